@@ -1,0 +1,101 @@
+/* C ABI of the B200 QAFold commit+open library (libparcomm_qafold.so).
+ *
+ * Each entry point replaces one public call of the reference Rust prover
+ * (qafold/f65521/src/protocol.rs, tbv.rs, main.rs).  Every call returns 0 or
+ * a negative QF_E_* code; qf_last_error() returns the message of the last
+ * failure on the calling thread (the reference's `check` strings and
+ * mikros_qafold::Error variants, vendor/qafold/src/lib.rs:20-35).
+ *
+ * Wire formats
+ *   points : per matrix, in shape order: row point then column point, each
+ *            coordinate a 16-byte canonical extension element; the row
+ *            point has log2(next_pow2(rows)) coordinates, the column point
+ *            log2(next_pow2(cols)) (tbv.rs:128-142).
+ *   claims : per matrix: row point, column point, value (16 bytes each).
+ *   proof  : the reference's bincode-fixint Proof (protocol.rs:88-107).
+ */
+#ifndef PARCOMM_QAFOLD_H
+#define PARCOMM_QAFOLD_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QF_FIELD_F65521 1    /* F65521^8, signed 8-bit weights */
+#define QF_FIELD_KOALABEAR 2 /* KoalaBear^4, signed 16-bit payloads */
+
+#define QF_OK 0
+#define QF_E_ENCODING -1
+#define QF_E_HASHING -2
+#define QF_E_INVALID_COMMITMENT -3
+#define QF_E_INVALID_NUMBER_OF_VARIABLES -4
+#define QF_E_INVALID_PARAMETERS -5
+#define QF_E_TRANSCRIPT -6
+#define QF_E_PROTOCOL -7
+#define QF_E_CUDA -8
+#define QF_E_ARGUMENT -9
+#define QF_E_NO_DEVICE -10
+
+typedef struct qf_params qf_params;       /* Parameters (protocol.rs:41-46) */
+typedef struct qf_committed qf_committed; /* Committed, device-resident (protocol.rs:47-51) */
+
+typedef struct {
+  uint64_t rows, cols;
+} qf_shape; /* layout::Shape (layout.rs:4-8) */
+
+typedef struct {
+  uint32_t chunk_log, packed_log, query_rf_bits;
+} qf_config; /* protocol::Config (protocol.rs:18-32) */
+
+typedef struct {
+  double commit_ms, upload_ms, eo_ms, projection_ms, folding_ms, sumcheck_ms, binding_ms, native_opening_ms, decide_ms,
+      open_ms;
+  uint64_t kernel_launches;
+} qf_profile; /* ProverProfile (protocol.rs:67-80), milliseconds */
+
+/* Parameters::new(shapes, config) (protocol.rs:109-130). Setup runs on the host. */
+int qf_params_new(int field, const qf_shape* shapes, size_t n_shapes, const qf_config* config, qf_params** out);
+void qf_params_free(qf_params* params);
+/* Layout facts and Commitment::parameter_digest (layout.rs:56-114, packed.rs:161). */
+int qf_params_info(const qf_params* params, uint64_t* active, uint64_t* logical, uint64_t* blocks, uint64_t* buckets,
+                   uint8_t parameter_digest[32]);
+
+/* Parameters::commit / commit_recomputed (protocol.rs:131-185): validates the
+ * BVA padding, keeps the weights and codewords in HBM and writes the block
+ * roots (blocks * 32 bytes).  `bva` holds `n_values` signed entries (int8 for
+ * F65521, int16 for KoalaBear) in host memory, or in device memory when
+ * `bva_on_device` is nonzero.  Both cache modes produce identical bytes. */
+int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int bva_on_device, qf_committed** out,
+              uint8_t* roots_out);
+void qf_committed_free(qf_committed* committed);
+
+/* serde_json of the Commitment statement (protocol.rs:33-40), as absorbed. */
+int qf_statement_json(const qf_params* params, const uint8_t* roots, char* buf, size_t cap, size_t* len);
+
+/* The demo/benchmark points of main.rs:190-204 derived from the statement. */
+int qf_benchmark_points(const qf_params* params, const uint8_t* roots, uint8_t* points, size_t cap, size_t* len);
+
+/* tbv::evaluate_claims (tbv.rs:143-185) over the committed weights. */
+int qf_eval_claims(const qf_params* params, const qf_committed* committed, const uint8_t* points, size_t points_len,
+                   uint8_t* claims, size_t cap, size_t* len);
+
+/* Parameters::prove + Proof::to_bytes (protocol.rs:201-263, 88-96).  The
+ * proof buffer is allocated by the library; release it with qf_free_bytes.
+ * The committed state is consumed (as in the reference) and must still be
+ * released with qf_committed_free. */
+int qf_prove(const qf_params* params, qf_committed* committed, const uint8_t* claims, size_t claims_len, uint8_t** proof,
+             size_t* proof_len, qf_profile* profile);
+
+/* Proof::from_bytes + Parameters::verify (protocol.rs:97-107, 266-320). Host only. */
+int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,
+              size_t proof_len);
+
+void qf_free_bytes(uint8_t* bytes);
+size_t qf_last_error(char* buf, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

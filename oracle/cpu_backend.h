@@ -148,8 +148,8 @@ struct CpuBackend : Backend<F>, SingleBackend<F>, EoBackend<F> {
     write_codeword_rows(w, *folded, sel);
     return std::move(w.out);
   }
-  const Codeword<F>& folded_codeword() override { return *folded; }
-  const Codeword<F>& codeword() override { return *blocks[0]; }
+  const CodewordView<F>& folded_codeword() override { return *folded; }
+  const CodewordView<F>& codeword() override { return *blocks[0]; }
   std::vector<F> folded_row_projection(const std::vector<F>& rw) override {
     return systematic_row_projection(*folded, P.pcs.pp->top_rows(), rw);
   }

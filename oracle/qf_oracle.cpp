@@ -1,0 +1,194 @@
+// ORACLE (test infrastructure only): C entry points over the CPU restatement
+// in cpu_backend.h, used by tests/, __graft_entry__.smoke() and the bench's
+// CPU-baseline leg as the checker.  Never linked into the product library.
+//
+// Pinned by the reference's own golden vectors:
+//   * demo proof (qafold/f65521/src/main.rs:108-145, validation/qafold8-smoke-final/run.log)
+//   * native opening + Decide wire fixture (qafold_short_pc.rs:3605-3647)
+#include <chrono>
+#include <cstdlib>
+#include <string>
+
+#include "cpu_backend.h"
+
+using namespace qf;
+using F = Fp8;
+
+namespace {
+thread_local std::string g_err;
+template <class Fn>
+int guarded(Fn&& fn) {
+  try {
+    fn();
+    return 0;
+  } catch (const QfError& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return -7;
+  }
+}
+uint8_t* dup(const std::vector<uint8_t>& v) {
+  uint8_t* p = static_cast<uint8_t*>(std::malloc(v.size() ? v.size() : 1));
+  if (!v.empty()) std::memcpy(p, v.data(), v.size());
+  return p;
+}
+F sample_uniform(StdRng& rng) {
+  for (;;) {
+    uint8_t b[16];
+    uint64_t a = rng.next_u64(), c = rng.next_u64();
+    for (int i = 0; i < 8; ++i) { b[i] = uint8_t(a >> (8 * i)); b[8 + i] = uint8_t(c >> (8 * i)); }
+    F v;
+    if (F::from_uniform_bytes(b, v)) return v;
+  }
+}
+std::vector<Shape> shapes_of(const uint64_t* s, size_t n) {
+  std::vector<Shape> out;
+  for (size_t i = 0; i < n; ++i) out.push_back({size_t(s[2 * i]), size_t(s[2 * i + 1])});
+  return out;
+}
+}  // namespace
+
+extern "C" {
+
+const char* qfo_last_error() { return g_err.c_str(); }
+void qfo_free(void* p) { std::free(p); }
+
+// Full prover over a BVA.  `claims` may be null: the benchmark points of
+// main.rs:190-204 are then used.  Outputs (malloc'd): roots (blocks*32),
+// claims (claims wire), proof (bincode).  `times_ms` = {commit, open}.
+int qfo_prove(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+              const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint8_t** roots,
+              size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len,
+              double* times_ms) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<F>(shapes_of(shapes, n_shapes), c);
+    std::vector<Claim<F>> given;
+    if (claims_in) {
+      ByteReader r(claims_in, claims_len);
+      for (const Shape& s : P->layout.shapes) {
+        Claim<F> cl;
+        for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) cl.row.push_back(r.field<F>());
+        for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) cl.col.push_back(r.field<F>());
+        cl.value = r.field<F>();
+        given.push_back(cl);
+      }
+    }
+    auto res = qf_oracle::prove_all<F, int8_t>(*P, bva, n_values, claims_in == nullptr, claims_in ? &given : nullptr);
+    ByteWriter rw, cw;
+    for (const auto& d : res.statement.roots) rw.digest(d);
+    for (const auto& cl : res.claims) {
+      for (const F& v : cl.row) cw.field(v);
+      for (const F& v : cl.col) cw.field(v);
+      cw.field(cl.value);
+    }
+    *roots = dup(rw.out);
+    *roots_len = rw.out.size();
+    *claims_out = dup(cw.out);
+    *claims_out_len = cw.out.size();
+    *proof = dup(res.wire);
+    *proof_len = res.wire.size();
+    if (times_ms) { times_ms[0] = res.commit_ms; times_ms[1] = res.open_ms; }
+  });
+}
+
+// Commitment roots only (protocol.rs:131-185).
+int qfo_commit_roots(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                     const int8_t* bva, uint64_t n_values, uint8_t* roots_out, size_t cap) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<F>(shapes_of(shapes, n_shapes), c);
+    validate_values(P->layout, bva, n_values);
+    if (cap < 32 * P->blocks()) fail(-9, "roots buffer too small");
+    qf_oracle::CpuBackend<F, int8_t> be(*P, bva, n_values);
+    for (size_t b = 0; b < P->blocks(); ++b) {
+      Digest d = be.commit_block(b);
+      std::memcpy(roots_out + 32 * b, d.data(), 32);
+    }
+  });
+}
+
+// Golden vector 1: the demo bundle's proof digest and length.
+int qfo_demo(uint8_t digest_out[32], uint64_t* proof_len, uint64_t* statement_json_len) {
+  return guarded([&] {
+    std::vector<Shape> shapes = {{31, 37}, {65, 17}, {1, 7}, {9, 1}};
+    Config c;
+    c.chunk_log = 10;
+    c.packed_log = 4;
+    auto P = make_parameters<F>(shapes, c);
+    std::vector<std::vector<int8_t>> mats;
+    for (size_t i = 0; i < shapes.size(); ++i) {
+      std::vector<int8_t> m(shapes[i].rows * shapes[i].cols);
+      for (size_t e = 0; e < m.size(); ++e) m[e] = int8_t(uint8_t(e * 73 + i * 19));
+      mats.push_back(m);
+    }
+    auto vals = layout_encode<int8_t>(P->layout, mats);
+    auto res = qf_oracle::prove_all<F, int8_t>(*P, vals.data(), vals.size(), true);
+    Digest d = blake2s(res.wire.data(), res.wire.size());
+    std::memcpy(digest_out, d.data(), 32);
+    *proof_len = res.wire.size();
+    *statement_json_len = commitment_json(res.statement).size();
+  });
+}
+
+// Golden vector 2: BLAKE2s(root || opening || decide) of the native-opening
+// wire fixture (ShortQaFoldPC::new(1 << 16, 16, 2, 80), seed 0x706172616c6c656c).
+int qfo_wire_fixture(uint8_t digest_out[32]) {
+  return guarded([&] {
+    StdRng rng = StdRng::seed_from_u64(0x706172616c6c656cull);
+    auto pp = pcs_setup<F>(1u << 16, 16, 80, rng);
+    std::vector<F> witness(1u << 16);
+    for (auto& w : witness) w = sample_uniform(rng);
+    std::vector<F> point(16);
+    for (auto& p : point) p = sample_uniform(rng);
+    Codeword<F> cw = encode_and_commit(pp->seq.top(), witness, pp->extension_columns, kLeafBaseDomain);
+    const size_t col_log = ilog2(pp->extension_columns);
+    std::vector<F> rw = tensor_weights(std::vector<F>(point.begin() + col_log, point.end()));
+    std::vector<F> op = cw.project_rows(pp->top_rows(), rw);
+    F claimed = inner_product(op, tensor_weights(std::vector<F>(point.begin(), point.begin() + col_log)));
+    auto res = open_with_reduction(*pp, cw, point, op, claimed, rw);
+    auto dec = prove_decide(*pp, res.reduction);
+    auto red = verify_opening_reduction(*pp, cw.root(), point, claimed, opening_from_bytes<F>(opening_to_bytes(res.proof).data(), opening_to_bytes(res.proof).size()));
+    if (!red.ok || !(red.pending == res.reduction.pending) || !verify_decide(*pp, red, dec)) fail(-3, "fixture self-verification");
+    Blake2s h;
+    h.update(cw.root());
+    h.update(opening_to_bytes(res.proof));
+    h.update(decide_to_bytes(dec));
+    Digest d = h.finalize();
+    std::memcpy(digest_out, d.data(), 32);
+  });
+}
+
+// Independent verification of a proof (protocol.rs:266-320).
+int qfo_verify(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+               const uint8_t* roots, const uint8_t* claims_in, size_t claims_len, const uint8_t* proof, size_t proof_len) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<F>(shapes_of(shapes, n_shapes), c);
+    std::vector<Digest> rs(P->blocks());
+    for (size_t b = 0; b < rs.size(); ++b) std::memcpy(rs[b].data(), roots + 32 * b, 32);
+    ByteReader r(claims_in, claims_len);
+    std::vector<Claim<F>> cl;
+    for (const Shape& s : P->layout.shapes) {
+      Claim<F> x;
+      for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) x.row.push_back(r.field<F>());
+      for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) x.col.push_back(r.field<F>());
+      x.value = r.field<F>();
+      cl.push_back(x);
+    }
+    verify_proof(*P, make_statement(*P, rs), cl, proof_from_bytes<F>(proof, proof_len));
+  });
+}
+
+}  // extern "C"

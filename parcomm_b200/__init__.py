@@ -1,0 +1,318 @@
+"""B200 QAFold commit+open: Python mirror of the reference prover's public API.
+
+The reference crate `parcomm-qafold` exposes `Parameters::{new, commit,
+commit_recomputed, prove, verify}`, `Proof::{to_bytes, from_bytes}` and
+`tbv::evaluate_claims` (qafold/f65521/src/protocol.rs:108-321, tbv.rs:143-185).
+This module exposes the same calls over the C ABI of libparcomm_qafold.so
+(include/parcomm_qafold.h).  Proving runs on the GPU through hand-written
+sm_100a kernels; there is no CPU fallback: without a CUDA device `commit`
+raises `QfError(QF_E_NO_DEVICE)`.  Verification is host-only, as in the
+reference (its verifier always runs on one thread, main.rs:215-217).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from pathlib import Path
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "_lib" / "libparcomm_qafold.so"
+
+FIELD_F65521 = 1
+FIELD_KOALABEAR = 2
+ERRORS = {
+    -1: "EncodingError", -2: "HashingError", -3: "InvalidCommitment", -4: "InvalidNumberOfVariables",
+    -5: "InvalidParameters", -6: "TranscriptError", -7: "ProtocolError", -8: "CudaError", -9: "ArgumentError",
+    -10: "NoDevice",
+}
+QF_E_NO_DEVICE = -10
+
+
+class QfError(RuntimeError):
+    """A rejected call: `code` is the QF_E_* value, the message the reference's check string."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class _Shape(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_uint64), ("cols", ctypes.c_uint64)]
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("chunk_log", ctypes.c_uint32), ("packed_log", ctypes.c_uint32), ("query_rf_bits", ctypes.c_uint32)]
+
+
+class _Profile(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "commit_ms", "upload_ms", "eo_ms", "projection_ms", "folding_ms", "sumcheck_ms", "binding_ms",
+        "native_opening_ms", "decide_ms", "open_ms")] + [("kernel_launches", ctypes.c_uint64)]
+
+
+_lib = None
+
+EXPORTED = (
+    "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
+    "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
+)
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the in-tree library (built by `parcomm_b200.build`)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise QfError(-9, f"{LIB_PATH} is missing; run `python -m parcomm_b200.build`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        P, S, U64, U32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint32
+        BP = ctypes.POINTER(ctypes.c_uint8)
+        L.qf_params_new.argtypes = [ctypes.c_int, ctypes.POINTER(_Shape), S, ctypes.POINTER(_Config), ctypes.POINTER(P)]
+        L.qf_params_free.argtypes = [P]
+        L.qf_params_free.restype = None
+        L.qf_params_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64),
+                                     ctypes.POINTER(U64), ctypes.c_char_p]
+        L.qf_commit.argtypes = [P, P, U64, ctypes.c_int, ctypes.POINTER(P), ctypes.c_char_p]
+        L.qf_committed_free.argtypes = [P]
+        L.qf_committed_free.restype = None
+        L.qf_statement_json.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.POINTER(S)]
+        L.qf_benchmark_points.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.POINTER(S)]
+        L.qf_eval_claims.argtypes = [P, P, ctypes.c_char_p, S, ctypes.c_char_p, S, ctypes.POINTER(S)]
+        L.qf_prove.argtypes = [P, P, ctypes.c_char_p, S, ctypes.POINTER(BP), ctypes.POINTER(S), ctypes.POINTER(_Profile)]
+        L.qf_verify.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
+        L.qf_free_bytes.argtypes = [P]
+        L.qf_free_bytes.restype = None
+        L.qf_last_error.argtypes = [ctypes.c_char_p, S]
+        L.qf_last_error.restype = S
+        for name in EXPORTED:
+            if not hasattr(L, name):
+                raise QfError(-9, f"library does not export {name}")
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        buf = ctypes.create_string_buffer(4096)
+        lib().qf_last_error(buf, 4096)
+        raise QfError(rc, buf.value.decode(errors="replace"))
+
+
+@dataclasses.dataclass(frozen=True)
+class Shape:
+    rows: int
+    cols: int
+
+
+@dataclasses.dataclass(frozen=True)
+class Config:
+    """protocol::Config (protocol.rs:18-32)."""
+    chunk_log: int = 30
+    packed_log: int = 4
+    query_rf_bits: int = 100
+
+
+@dataclasses.dataclass
+class Claim:
+    """tbv::Claim: row/col points and value, 16-byte canonical scalars each."""
+    row: List[bytes]
+    col: List[bytes]
+    value: bytes
+
+
+@dataclasses.dataclass
+class ProverProfile:
+    commit_ms: float
+    upload_ms: float
+    eo_ms: float
+    projection_ms: float
+    folding_ms: float
+    sumcheck_ms: float
+    binding_ms: float
+    native_opening_ms: float
+    decide_ms: float
+    open_ms: float
+    kernel_launches: int
+
+
+def _row_bits(n: int) -> int:
+    return (n - 1).bit_length() if n > 1 else 0
+
+
+def claims_to_bytes(claims: Sequence[Claim]) -> bytes:
+    out = bytearray()
+    for c in claims:
+        for v in c.row:
+            out += v
+        for v in c.col:
+            out += v
+        out += c.value
+    return bytes(out)
+
+
+def claims_from_bytes(shapes: Sequence[Shape], data: bytes, with_value: bool = True) -> List[Claim]:
+    claims, off = [], 0
+    for s in shapes:
+        r = [data[off + 16 * i: off + 16 * i + 16] for i in range(_row_bits(s.rows))]
+        off += 16 * len(r)
+        c = [data[off + 16 * i: off + 16 * i + 16] for i in range(_row_bits(s.cols))]
+        off += 16 * len(c)
+        v = b"\x00" * 16
+        if with_value:
+            v = data[off: off + 16]
+            off += 16
+        claims.append(Claim(r, c, v))
+    if off != len(data):
+        raise QfError(-9, "claims length mismatch")
+    return claims
+
+
+class Committed:
+    """Committed state: weights, codewords and Merkle trees resident in HBM."""
+
+    def __init__(self, params: "Parameters", handle: int, roots: List[bytes]):
+        self.params = params
+        self._h = ctypes.c_void_p(handle)
+        self.roots = roots
+        self.consumed = False
+
+    @property
+    def statement(self) -> "Commitment":
+        return Commitment(self.params, list(self.roots))
+
+    def close(self) -> None:
+        if self._h:
+            lib().qf_committed_free(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclasses.dataclass
+class Commitment:
+    """protocol::Commitment: version 2, config, shapes, parameter digest, block roots."""
+    params: "Parameters"
+    roots: List[bytes]
+
+    def to_json(self) -> bytes:
+        return self.params.statement_json(self.roots)
+
+
+class Proof:
+    """The bincode-fixint wire of protocol::Proof (protocol.rs:88-107)."""
+
+    def __init__(self, data: bytes):
+        self.data = bytes(data)
+
+    def to_bytes(self) -> bytes:
+        return self.data
+
+    @staticmethod
+    def from_bytes(data: bytes) -> "Proof":
+        if len(data) > 256 * 1024 * 1024:
+            raise QfError(-7, "oversize ParComm proof")
+        return Proof(data)
+
+
+class Parameters:
+    """protocol::Parameters::new(shapes, config) for the F65521^8 field."""
+
+    def __init__(self, shapes: Sequence[Tuple[int, int]] | Sequence[Shape], config: Config = Config(),
+                 field: int = FIELD_F65521):
+        self.shapes = [s if isinstance(s, Shape) else Shape(int(s[0]), int(s[1])) for s in shapes]
+        self.config = config
+        self.field = field
+        arr = (_Shape * len(self.shapes))(*[_Shape(s.rows, s.cols) for s in self.shapes])
+        cfg = _Config(config.chunk_log, config.packed_log, config.query_rf_bits)
+        h = ctypes.c_void_p()
+        _check(lib().qf_params_new(field, arr, len(self.shapes), ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        a, l, b, k = (ctypes.c_uint64() for _ in range(4))
+        dig = ctypes.create_string_buffer(32)
+        _check(lib().qf_params_info(self._h, ctypes.byref(a), ctypes.byref(l), ctypes.byref(b), ctypes.byref(k), dig))
+        self.active, self.logical, self.blocks, self.buckets = a.value, l.value, b.value, k.value
+        self.parameter_digest = dig.raw
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().qf_params_free(self._h)
+        except Exception:
+            pass
+
+    # -- commit (protocol.rs:131-185); cached and recompute modes give identical bytes
+    def commit(self, values, on_device: bool = False) -> Committed:
+        if on_device:
+            ptr, n = int(values.data_ptr()), int(values.numel())
+        else:
+            arr = np.ascontiguousarray(values, dtype=np.int8)
+            ptr, n = arr.ctypes.data, arr.size
+        h = ctypes.c_void_p()
+        roots = ctypes.create_string_buffer(32 * max(self.blocks, 1))
+        _check(lib().qf_commit(self._h, ctypes.c_void_p(ptr), n, int(on_device), ctypes.byref(h), roots))
+        return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)])
+
+    commit_recomputed = commit
+
+    def statement_json(self, roots: Sequence[bytes]) -> bytes:
+        r = b"".join(roots)
+        n = ctypes.c_size_t()
+        _check(lib().qf_statement_json(self._h, r, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        _check(lib().qf_statement_json(self._h, r, buf, n.value, ctypes.byref(n)))
+        return buf.raw[: n.value]
+
+    def benchmark_points(self, roots: Sequence[bytes]) -> bytes:
+        """The points of main.rs:190-204 (transcript over the statement)."""
+        r = b"".join(roots)
+        n = ctypes.c_size_t()
+        _check(lib().qf_benchmark_points(self._h, r, None, 0, ctypes.byref(n)))
+        buf = ctypes.create_string_buffer(max(n.value, 1))
+        _check(lib().qf_benchmark_points(self._h, r, buf, n.value, ctypes.byref(n)))
+        return buf.raw[: n.value]
+
+    def evaluate_claims(self, committed: Committed, points: bytes) -> List[Claim]:
+        """tbv::evaluate_claims over the committed weights (on the GPU)."""
+        n = ctypes.c_size_t()
+        cap = len(points) + 16 * len(self.shapes)
+        buf = ctypes.create_string_buffer(cap)
+        _check(lib().qf_eval_claims(self._h, committed._h, points, len(points), buf, cap, ctypes.byref(n)))
+        return claims_from_bytes(self.shapes, buf.raw[: n.value])
+
+    def prove(self, committed: Committed, claims: Sequence[Claim]) -> Tuple[Proof, ProverProfile]:
+        cb = claims_to_bytes(claims)
+        out = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_size_t()
+        prof = _Profile()
+        _check(lib().qf_prove(self._h, committed._h, cb, len(cb), ctypes.byref(out), ctypes.byref(n), ctypes.byref(prof)))
+        try:
+            data = ctypes.string_at(out, n.value)
+        finally:
+            lib().qf_free_bytes(ctypes.cast(out, ctypes.c_void_p))
+        committed.consumed = True
+        return Proof(data), ProverProfile(*[getattr(prof, f) for f, _ in _Profile._fields_])
+
+    def verify(self, statement: Commitment | Sequence[bytes], claims: Sequence[Claim], proof: Proof | bytes) -> None:
+        """Raises QfError when the proof is rejected (protocol.rs:266-320)."""
+        roots = statement.roots if isinstance(statement, Commitment) else list(statement)
+        pb = proof.to_bytes() if isinstance(proof, Proof) else bytes(proof)
+        cb = claims_to_bytes(claims)
+        _check(lib().qf_verify(self._h, b"".join(roots), cb, len(cb), pb, len(pb)))
+
+
+def demo_shapes() -> List[Shape]:
+    """The demo collection of main.rs:108-115."""
+    return [Shape(31, 37), Shape(65, 17), Shape(1, 7), Shape(9, 1)]
+
+
+def encode_bva(layout_params: Parameters, matrices: Sequence[np.ndarray]) -> np.ndarray:
+    """Layout::encode (layout.rs:115-135): dense matrices -> BVA of `active` entries."""
+    from .layout import encode
+    return encode(layout_params.shapes, matrices)

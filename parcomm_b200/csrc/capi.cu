@@ -1,0 +1,326 @@
+// extern "C" boundary of libparcomm_qafold.so (declared in include/parcomm_qafold.h).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdlib>
+#include <string>
+
+#include "../../include/parcomm_qafold.h"
+#include "gpu_backend.cuh"
+
+using namespace qf;
+using qfg::DBuf;
+using qfg::GpuBackend;
+using F = Fp8;
+
+namespace {
+thread_local std::string g_last_error;
+
+int set_error(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+template <class Fn>
+int guarded(Fn&& fn) {
+  try {
+    fn();
+    return QF_OK;
+  } catch (const QfError& e) {
+    return set_error(e.code, e.what());
+  } catch (const std::bad_alloc&) {
+    return set_error(QF_E_ARGUMENT, "host allocation failed");
+  } catch (const std::exception& e) {
+    return set_error(QF_E_PROTOCOL, e.what());
+  }
+}
+
+// Any zero-padding entry that is nonzero sets the flag (Layout::validate_values, layout.rs:136-155).
+__global__ void k_check_zero_segments(const int8_t* __restrict__ bva, const uint64_t* __restrict__ seg, uint32_t n_seg,
+                                      unsigned int* __restrict__ flag) {
+  for (uint32_t s = blockIdx.x; s < n_seg; s += gridDim.x) {
+    const uint64_t a = seg[2 * s], b = seg[2 * s + 1];
+    for (uint64_t i = a + threadIdx.x; i < b; i += blockDim.x)
+      if (bva[i] != 0) atomicOr(flag, 1u);
+  }
+}
+
+void require_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(QF_E_NO_DEVICE, "no CUDA device available");
+}
+
+}  // namespace
+
+struct qf_params {
+  int field = 0;
+  std::unique_ptr<Parameters<F>> P;
+};
+
+struct qf_committed {
+  const qf_params* params = nullptr;
+  cudaStream_t stream = nullptr;
+  DBuf<int8_t> bva;
+  uint64_t active = 0;
+  std::unique_ptr<GpuBackend> be;
+  std::vector<Digest> roots;
+  double commit_ms = 0, upload_ms = 0;
+  bool consumed = false;
+  ~qf_committed() {
+    be.reset();
+    bva.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+static std::vector<Claim<F>> parse_claims(const Parameters<F>& P, const uint8_t* d, size_t n, bool with_value) {
+  std::vector<Claim<F>> claims;
+  ByteReader r(d, n);
+  for (const Shape& s : P.layout.shapes) {
+    Claim<F> c;
+    for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) c.row.push_back(r.field<F>());
+    for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) c.col.push_back(r.field<F>());
+    c.value = with_value ? r.field<F>() : F::zero();
+    claims.push_back(std::move(c));
+  }
+  if (!r.empty()) fail(QF_E_ARGUMENT, "claims length mismatch");
+  return claims;
+}
+static std::vector<uint8_t> write_claims(const std::vector<Claim<F>>& claims, bool with_value) {
+  ByteWriter w;
+  for (const auto& c : claims) {
+    for (const F& v : c.row) w.field(v);
+    for (const F& v : c.col) w.field(v);
+    if (with_value) w.field(c.value);
+  }
+  return std::move(w.out);
+}
+static void copy_out(const std::vector<uint8_t>& src, uint8_t* dst, size_t cap, size_t* len) {
+  if (len) *len = src.size();
+  if (dst) {
+    if (cap < src.size()) fail(QF_E_ARGUMENT, "output buffer too small");
+    std::memcpy(dst, src.data(), src.size());
+  }
+}
+static std::vector<Digest> roots_from(const qf_params* p, const uint8_t* roots) {
+  std::vector<Digest> out(p->P->blocks());
+  for (size_t b = 0; b < out.size(); ++b) std::memcpy(out[b].data(), roots + 32 * b, 32);
+  return out;
+}
+
+// TBV claim values on the device (tbv::evaluate_claims, tbv.rs:143-185).
+static std::vector<Claim<F>> device_eval_claims(const Parameters<F>& P, GpuBackend& be, std::vector<Claim<F>> claims) {
+  validate_claims(P.layout, claims);
+  std::vector<Term<F>> terms;
+  for (const Bucket& b : P.layout.buckets) {
+    const auto& row = claims[b.matrix].row;
+    const auto& col = claims[b.matrix].col;
+    Term<F> t{b.offset, monomial_weight(b.row_offset, row.data(), row.size()) * monomial_weight(b.col_offset, col.data(), col.size()), {}};
+    for (int k = 0; k < ilog2(b.cols); ++k) t.factors.push_back({F::one(), col[k]});
+    for (int k = 0; k < ilog2(b.rows); ++k) t.factors.push_back({F::one(), row[k]});
+    terms.push_back(std::move(t));
+  }
+  for (auto& c : claims) c.value = F::zero();
+  // Group by lane width (terms with fewer than four factors use fewer lanes).
+  for (size_t lanes_log = 0; lanes_log <= 4; ++lanes_log) {
+    std::vector<const Term<F>*> group;
+    std::vector<size_t> which;
+    for (size_t i = 0; i < terms.size(); ++i)
+      if (std::min<size_t>(4, terms[i].factors.size()) == lanes_log) { group.push_back(&terms[i]); which.push_back(i); }
+    if (group.empty()) continue;
+    auto pr = be.project_terms(group, 16);
+    for (size_t g = 0; g < group.size(); ++g) {
+      std::vector<F> low = factor_weights(group[g]->factors.data(), lanes_log);
+      F v = F::zero();
+      for (size_t l = 0; l < pr[g].size(); ++l) v += pr[g][l] * low[l];
+      claims[P.layout.buckets[which[g]].matrix].value += v;
+    }
+  }
+  return claims;
+}
+
+extern "C" {
+
+int qf_params_new(int field, const qf_shape* shapes, size_t n_shapes, const qf_config* config, qf_params** out) {
+  return guarded([&] {
+    if (!out || !config || (!shapes && n_shapes)) fail(QF_E_ARGUMENT, "null argument");
+    if (field != QF_FIELD_F65521) fail(QF_E_INVALID_PARAMETERS, "field not supported by this library build");
+    std::vector<Shape> sh;
+    for (size_t i = 0; i < n_shapes; ++i) sh.push_back({size_t(shapes[i].rows), size_t(shapes[i].cols)});
+    Config c;
+    c.chunk_log = config->chunk_log;
+    c.packed_log = config->packed_log;
+    c.query_rf_bits = config->query_rf_bits;
+    auto p = std::make_unique<qf_params>();
+    p->field = field;
+    p->P = make_parameters<F>(sh, c);
+    *out = p.release();
+  });
+}
+
+void qf_params_free(qf_params* params) { delete params; }
+
+int qf_params_info(const qf_params* params, uint64_t* active, uint64_t* logical, uint64_t* blocks, uint64_t* buckets,
+                   uint8_t parameter_digest[32]) {
+  return guarded([&] {
+    if (!params) fail(QF_E_ARGUMENT, "null params");
+    const auto& P = *params->P;
+    if (active) *active = P.layout.active;
+    if (logical) *logical = P.layout.logical;
+    if (blocks) *blocks = P.blocks();
+    if (buckets) *buckets = P.layout.buckets.size();
+    if (parameter_digest) std::memcpy(parameter_digest, P.pcs.parameter_digest().data(), 32);
+  });
+}
+
+int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int bva_on_device, qf_committed** out,
+              uint8_t* roots_out) {
+  return guarded([&] {
+    if (!params || !out || (!bva && n_values)) fail(QF_E_ARGUMENT, "null argument");
+    require_device();
+    const auto& P = *params->P;
+    check(n_values == P.layout.active, "active BVA length mismatch");
+    auto c = std::make_unique<qf_committed>();
+    c->params = params;
+    c->active = n_values;
+    QF_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    auto t0 = std::chrono::steady_clock::now();
+    c->bva.alloc(std::max<uint64_t>(n_values, 8));
+    QF_CK(cudaMemcpyAsync(c->bva.p, bva, n_values, bva_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
+    QF_CK(cudaStreamSynchronize(c->stream));
+    c->upload_ms = ms_since(t0);
+    t0 = std::chrono::steady_clock::now();
+    // Padding must be zero (validate_values) — checked on the device.
+    std::vector<uint64_t> seg;
+    for (const Bucket& b : P.layout.buckets)
+      for (size_t r = 0; r < b.rows; ++r) {
+        size_t valid = r < b.physical_rows ? b.physical_cols : 0;
+        if (valid == b.cols) continue;
+        uint64_t a = b.offset + r * b.cols + valid, e = b.offset + (r + 1) * b.cols;
+        if (!seg.empty() && seg.back() == a) seg.back() = e;  // merge contiguous runs
+        else { seg.push_back(a); seg.push_back(e); }
+      }
+    if (!seg.empty()) {
+      DBuf<uint64_t> dseg(seg.size());
+      DBuf<unsigned int> flag(1);
+      QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      QF_CK(cudaMemsetAsync(flag.p, 0, 4, c->stream));
+      k_check_zero_segments<<<unsigned(std::min<size_t>(seg.size() / 2, 148 * 8)), 256, 0, c->stream>>>(
+          c->bva.p, dseg.p, uint32_t(seg.size() / 2), flag.p);
+      QF_CK(cudaGetLastError());
+      unsigned int h = 0;
+      QF_CK(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, c->stream));
+      QF_CK(cudaStreamSynchronize(c->stream));
+      check(h == 0, "nonzero boundary padding");
+    }
+    c->be = std::make_unique<GpuBackend>(P, c->bva.p, n_values, c->stream);
+    for (size_t b = 0; b < P.blocks(); ++b) c->roots.push_back(c->be->commit_block(b));
+    QF_CK(cudaStreamSynchronize(c->stream));
+    c->commit_ms = ms_since(t0);
+    if (roots_out)
+      for (size_t b = 0; b < c->roots.size(); ++b) std::memcpy(roots_out + 32 * b, c->roots[b].data(), 32);
+    *out = c.release();
+  });
+}
+
+void qf_committed_free(qf_committed* committed) { delete committed; }
+
+int qf_statement_json(const qf_params* params, const uint8_t* roots, char* buf, size_t cap, size_t* len) {
+  return guarded([&] {
+    if (!params || !roots) fail(QF_E_ARGUMENT, "null argument");
+    std::string j = commitment_json(make_statement(*params->P, roots_from(params, roots)));
+    copy_out(std::vector<uint8_t>(j.begin(), j.end()), reinterpret_cast<uint8_t*>(buf), cap, len);
+  });
+}
+
+int qf_benchmark_points(const qf_params* params, const uint8_t* roots, uint8_t* points, size_t cap, size_t* len) {
+  return guarded([&] {
+    if (!params || !roots) fail(QF_E_ARGUMENT, "null argument");
+    auto pts = benchmark_points<F>(make_statement(*params->P, roots_from(params, roots)));
+    ByteWriter w;
+    for (const auto& [r, c] : pts) {
+      for (const F& v : r) w.field(v);
+      for (const F& v : c) w.field(v);
+    }
+    copy_out(w.out, points, cap, len);
+  });
+}
+
+int qf_eval_claims(const qf_params* params, const qf_committed* committed, const uint8_t* points, size_t points_len,
+                   uint8_t* claims, size_t cap, size_t* len) {
+  return guarded([&] {
+    if (!params || !committed || !points) fail(QF_E_ARGUMENT, "null argument");
+    if (committed->consumed) fail(QF_E_ARGUMENT, "committed state already consumed by prove");
+    auto cl = parse_claims(*params->P, points, points_len, false);
+    auto out = device_eval_claims(*params->P, *committed->be, std::move(cl));
+    copy_out(write_claims(out, true), claims, cap, len);
+  });
+}
+
+int qf_prove(const qf_params* params, qf_committed* committed, const uint8_t* claims, size_t claims_len, uint8_t** proof,
+             size_t* proof_len, qf_profile* profile) {
+  return guarded([&] {
+    if (!params || !committed || !claims || !proof || !proof_len) fail(QF_E_ARGUMENT, "null argument");
+    if (committed->consumed) fail(QF_E_ARGUMENT, "committed state already consumed by prove");
+    committed->consumed = true;
+    const auto& P = *params->P;
+    auto cl = parse_claims(P, claims, claims_len, true);
+    auto t0 = std::chrono::steady_clock::now();
+    Commitment st = make_statement(P, committed->roots);
+    Transcript<F> t = statement_transcript(P, st, cl);
+    Query<F> q = compile(P.layout, cl, t);
+    auto [eo, term] = eo_prove<F>(*committed->be, P.layout.logical, size_t(1) << P.config.packed_log, q, t);
+    double eo_ms = ms_since(t0);
+    std::vector<uint8_t> ctx = opening_context(t.state, 0);
+    BatchOpening<F> op = committed->roots.size() > 1 ? open_batch(P.pcs, *committed->be, committed->roots, term.point_msb, ctx)
+                                                    : open_single(P.pcs, *committed->be, committed->roots[0], term.point_msb, ctx);
+    check(op.claimed_value * term.scale == term.value, "QAFold/EO terminal mismatch");
+    Proof<F> pr;
+    pr.eo = std::move(eo);
+    pr.opening_value = op.claimed_value;
+    pr.opening_proof = std::move(op.wire);
+    std::vector<uint8_t> bytes = proof_to_bytes(pr);
+    uint8_t* buf = static_cast<uint8_t*>(std::malloc(bytes.size()));
+    if (!buf) fail(QF_E_ARGUMENT, "host allocation failed");
+    std::memcpy(buf, bytes.data(), bytes.size());
+    *proof = buf;
+    *proof_len = bytes.size();
+    if (profile) {
+      profile->commit_ms = committed->commit_ms;
+      profile->upload_ms = committed->upload_ms;
+      profile->eo_ms = eo_ms;
+      profile->projection_ms = op.times.projection_ms;
+      profile->folding_ms = op.times.folding_ms;
+      profile->sumcheck_ms = op.times.sumcheck_ms;
+      profile->binding_ms = op.times.binding_ms;
+      profile->native_opening_ms = op.times.native_opening_ms;
+      profile->decide_ms = op.times.decide_ms;
+      profile->open_ms = ms_since(t0);
+      profile->kernel_launches = committed->be->launches;
+    }
+  });
+}
+
+int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,
+              size_t proof_len) {
+  return guarded([&] {
+    if (!params || !roots || !claims || !proof) fail(QF_E_ARGUMENT, "null argument");
+    const auto& P = *params->P;
+    auto cl = parse_claims(P, claims, claims_len, true);
+    Proof<F> pr = proof_from_bytes<F>(proof, proof_len);
+    verify_proof(P, make_statement(P, roots_from(params, roots)), cl, pr);
+  });
+}
+
+void qf_free_bytes(uint8_t* bytes) { std::free(bytes); }
+
+size_t qf_last_error(char* buf, size_t cap) {
+  if (buf && cap) {
+    size_t n = std::min(cap - 1, g_last_error.size());
+    std::memcpy(buf, g_last_error.data(), n);
+    buf[n] = 0;
+  }
+  return g_last_error.size();
+}
+
+}  // extern "C"

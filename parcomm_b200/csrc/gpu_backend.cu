@@ -1,0 +1,693 @@
+// CUDA backend for the F65521^8 packed PCS and EO (see gpu_backend.cuh).
+#include "gpu_backend.cuh"
+#include "kernels/commit.cuh"
+#include "kernels/open.cuh"
+
+#include <map>
+
+namespace qfg {
+
+static constexpr int kThreads = 256;
+
+qfd::LeafPrefix leaf_prefix(size_t n_cols) {
+  std::vector<uint8_t> pre;
+  append_frame(pre, "domain", kLeafBaseDomain, std::strlen(kLeafBaseDomain));
+  auto w = le64(n_cols);
+  append_frame(pre, "width", w.data(), 8);
+  if (pre.size() != 75) fail(QF_E_ENCODING, "leaf prefix length");
+  qfd::LeafPrefix lp;
+  uint32_t h[8];
+  for (int i = 0; i < 8; ++i) h[i] = kBlake2sIv[i];
+  h[0] ^= 0x01010000u ^ 32u;
+  blake2s_compress(h, pre.data(), 64, false);
+  for (int i = 0; i < 8; ++i) lp.mid[i] = h[i];
+  uint8_t tail[12] = {0};
+  std::memcpy(tail, pre.data() + 64, 11);
+  for (int i = 0; i < 3; ++i)
+    lp.tail[i] = uint32_t(tail[4 * i]) | (uint32_t(tail[4 * i + 1]) << 8) | (uint32_t(tail[4 * i + 2]) << 16) |
+                 (uint32_t(tail[4 * i + 3]) << 24);
+  return lp;
+}
+qfd::InnerPrefix inner_prefix() {
+  std::vector<uint8_t> pre;
+  append_frame(pre, "domain", kInnerDomain, std::strlen(kInnerDomain));
+  if (pre.size() != 50) fail(QF_E_ENCODING, "inner prefix length");
+  uint8_t b[52] = {0};
+  std::memcpy(b, pre.data(), 50);
+  qfd::InnerPrefix ip;
+  for (int i = 0; i < 13; ++i)
+    ip.w[i] = uint32_t(b[4 * i]) | (uint32_t(b[4 * i + 1]) << 8) | (uint32_t(b[4 * i + 2]) << 16) | (uint32_t(b[4 * i + 3]) << 24);
+  return ip;
+}
+
+static Digest digest_from_words(const uint4* d) {
+  Digest out;
+  uint32_t w[8] = {d[0].x, d[0].y, d[0].z, d[0].w, d[1].x, d[1].y, d[1].z, d[1].w};
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 4; ++j) out[4 * i + j] = uint8_t(w[i] >> (8 * j));
+  return out;
+}
+
+template <class K>
+static void set_smem(K kernel, size_t bytes) {
+  QF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+}
+
+// ---------------------------------------------------------------- codeword view
+std::vector<F> DeviceCodeword::fold_rows(size_t n_rows, const std::vector<F>& w) const {
+  DBuf<Fe> dw(n_cols), out(n_rows);
+  QF_CK(cudaMemcpyAsync(dw.p, w.data(), n_cols * 16, cudaMemcpyHostToDevice, stream));
+  qfd::k_row_fold<<<grid_for(n_rows, kThreads), kThreads, 0, stream>>>(cw.p, n_ext, n_rows, int(n_cols), dw.p, out.p);
+  QF_CK(cudaGetLastError());
+  std::vector<F> h(n_rows);
+  QF_CK(cudaMemcpyAsync(h.data(), out.p, n_rows * 16, cudaMemcpyDeviceToHost, stream));
+  QF_CK(cudaStreamSynchronize(stream));
+  return h;
+}
+
+std::vector<F> DeviceCodeword::project_rows(size_t n_rows, const std::vector<F>& w) const {
+  // The row weights arrive as a full table; upload it as the low table of a
+  // single-entry two-level product.
+  DBuf<Fe> lo(n_rows), hi(1);
+  F one = F::one();
+  QF_CK(cudaMemcpyAsync(lo.p, w.data(), n_rows * 16, cudaMemcpyHostToDevice, stream));
+  QF_CK(cudaMemcpyAsync(hi.p, &one, 16, cudaMemcpyHostToDevice, stream));
+  const int chunks = int(std::min<size_t>(64, (n_rows + kThreads - 1) / kThreads));
+  DBuf<Fe> part(n_cols * chunks);
+  dim3 grid(chunks, unsigned(n_cols));
+  qfd::k_row_project<<<grid, kThreads, 0, stream>>>(cw.p, n_ext, n_rows, hi.p, lo.p, ilog2(n_rows), part.p);
+  QF_CK(cudaGetLastError());
+  std::vector<F> hp(n_cols * chunks);
+  QF_CK(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 16, cudaMemcpyDeviceToHost, stream));
+  QF_CK(cudaStreamSynchronize(stream));
+  std::vector<F> out(n_cols, F::zero());
+  for (size_t c = 0; c < n_cols; ++c)
+    for (int k = 0; k < chunks; ++k) out[c] += hp[c * chunks + k];
+  return out;
+}
+
+std::vector<std::vector<F>> DeviceCodeword::rows(const std::vector<size_t>& idx) const {
+  std::vector<std::vector<F>> out;
+  if (idx.empty()) return out;
+  std::vector<uint64_t> id(idx.begin(), idx.end());
+  DBuf<uint64_t> did(id.size());
+  DBuf<Fe> dout(id.size() * n_cols);
+  QF_CK(cudaMemcpyAsync(did.p, id.data(), id.size() * 8, cudaMemcpyHostToDevice, stream));
+  qfd::k_gather_rows<<<grid_for(id.size() * n_cols, kThreads, 1 << 20), kThreads, 0, stream>>>(cw.p, n_ext, int(n_cols), did.p,
+                                                                                               uint32_t(id.size()), dout.p);
+  QF_CK(cudaGetLastError());
+  std::vector<F> h(id.size() * n_cols);
+  QF_CK(cudaMemcpyAsync(h.data(), dout.p, h.size() * 16, cudaMemcpyDeviceToHost, stream));
+  QF_CK(cudaStreamSynchronize(stream));
+  for (size_t q = 0; q < id.size(); ++q) out.emplace_back(h.begin() + q * n_cols, h.begin() + (q + 1) * n_cols);
+  return out;
+}
+
+std::vector<std::vector<Digest>> DeviceCodeword::paths(const std::vector<size_t>& idx) const {
+  std::vector<std::vector<Digest>> out;
+  if (idx.empty()) return out;
+  const int depth = ilog2(n_ext);
+  std::vector<uint64_t> id(idx.begin(), idx.end());
+  DBuf<uint64_t> did(id.size()), doff(level_off.size());
+  DBuf<uint4> dout(id.size() * depth * 2);
+  QF_CK(cudaMemcpyAsync(did.p, id.data(), id.size() * 8, cudaMemcpyHostToDevice, stream));
+  QF_CK(cudaMemcpyAsync(doff.p, level_off.data(), level_off.size() * 8, cudaMemcpyHostToDevice, stream));
+  if (depth > 0) {
+    qfd::k_gather_paths<<<grid_for(id.size() * depth, kThreads, 1 << 20), kThreads, 0, stream>>>(tree.p, doff.p, depth, did.p,
+                                                                                                 uint32_t(id.size()), dout.p);
+    QF_CK(cudaGetLastError());
+  }
+  std::vector<uint4> h(id.size() * depth * 2);
+  QF_CK(cudaMemcpyAsync(h.data(), dout.p, h.size() * 16, cudaMemcpyDeviceToHost, stream));
+  QF_CK(cudaStreamSynchronize(stream));
+  for (size_t q = 0; q < id.size(); ++q) {
+    std::vector<Digest> p;
+    for (int l = 0; l < depth; ++l) p.push_back(digest_from_words(&h[(q * depth + l) * 2]));
+    out.push_back(std::move(p));
+  }
+  return out;
+}
+
+std::vector<F> DeviceCodeword::entries() const {
+  std::vector<F> h(n_ext * n_cols);
+  QF_CK(cudaMemcpyAsync(h.data(), cw.p, h.size() * 16, cudaMemcpyDeviceToHost, stream));
+  QF_CK(cudaStreamSynchronize(stream));
+  return h;
+}
+
+// ---------------------------------------------------------------- backend
+GpuBackend::GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s)
+    : P_(p), bva_(d_bva), active_(active), s_(s) {
+  partials_.alloc(148 * 8 * 4);
+  result_.alloc(8);
+}
+GpuBackend::~GpuBackend() {}
+
+void GpuBackend::ensure_alpha() {
+  if (alpha1_.p) return;
+  const auto& top = P_.pcs.pp->seq.top();
+  alpha1_.alloc(top.message_len);
+  QF_CK(cudaMemcpyAsync(alpha1_.p, top.alphas[1].data(), top.message_len * 16, cudaMemcpyHostToDevice, s_));
+}
+
+void GpuBackend::mobius_rest(Fe* cw, int logm, int logR, int from) {
+  for (int lo = from; lo < logm;) {
+    int k = std::min(9, logm - lo);
+    size_t smem = size_t(8) << k << 4;
+    set_smem(qfd::k_butterfly_strided<qfd::kMobius>, smem);
+    qfd::k_butterfly_strided<qfd::kMobius><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(cw, logR, lo, k);
+    QF_CK(cudaGetLastError());
+    ++launches;
+    lo += k;
+  }
+}
+
+// Parity = WHT(alpha1 * WHT(message)) per column, then leaf hashes and tree.
+void GpuBackend::encode_and_hash(DeviceCodeword& out) {
+  ensure_alpha();
+  const int logm = ilog2(P_.pcs.packed_len());
+  const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+  const size_t R = size_t(1) << logR;
+  const int wl = std::min(12, logR);
+  const size_t tsmem = size_t(16) << wl;
+  set_smem(qfd::k_wht_tile, tsmem);
+  Fe* msg = out.cw.p;
+  Fe* par = out.cw.p + R;
+  for (int pass = 0; pass < 2; ++pass) {
+    qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), kThreads, tsmem, s_>>>(pass == 0 ? msg : par, par,
+                                                                              pass == 0 ? nullptr : alpha1_.p, logR, wl);
+    QF_CK(cudaGetLastError());
+    ++launches;
+    for (int lo = wl; lo < logR;) {
+      int k = std::min(9, logR - lo);
+      size_t smem = size_t(8) << k << 4;
+      set_smem(qfd::k_butterfly_strided<qfd::kWht>, smem);
+      qfd::k_butterfly_strided<qfd::kWht><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(par, logR, lo, k);
+      QF_CK(cudaGetLastError());
+      ++launches;
+      lo += k;
+    }
+  }
+  // Leaves and inner levels.
+  const uint64_t n_ext = 2 * R;
+  qfd::LeafPrefix lp = leaf_prefix(out.n_cols);
+  qfd::k_hash_leaves<<<unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads), qfd::kLeafThreads, 0, s_>>>(
+      out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  qfd::InnerPrefix ip = inner_prefix();
+  out.level_off.clear();
+  uint64_t off = 0, n = n_ext;
+  while (n > 1) {
+    out.level_off.push_back(off);
+    qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s_>>>(out.tree.p + 2 * off, n / 2, ip,
+                                                                                   out.tree.p + 2 * (off + n));
+    QF_CK(cudaGetLastError());
+    ++launches;
+    off += n;
+    n /= 2;
+  }
+  out.level_off.push_back(off);
+  uint4 r[2];
+  QF_CK(cudaMemcpyAsync(r, out.tree.p + 2 * off, 32, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  out.root_ = digest_from_words(r);
+}
+
+static std::unique_ptr<DeviceCodeword> alloc_codeword(size_t R, size_t cols, cudaStream_t s) {
+  auto cw = std::make_unique<DeviceCodeword>();
+  cw->stream = s;
+  cw->n_ext = 2 * R;
+  cw->n_cols = cols;
+  cw->cw.alloc(2 * R * cols);
+  cw->tree.alloc(2 * (2 * cw->n_ext));
+  return cw;
+}
+
+Digest GpuBackend::commit_block(size_t b) {
+  const int logm = ilog2(P_.pcs.packed_len());
+  const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+  // The implicit zero suffix repeats one codeword; reuse its root and state.
+  if (b * P_.block_len >= active_ && !blocks_.empty()) {
+    for (size_t k = 0; k < blocks_.size(); ++k)
+      if (k * P_.block_len >= active_ && blocks_[k]) {
+        if (blocks_.size() <= b) blocks_.resize(b + 1);
+        roots_.resize(std::max(roots_.size(), b + 1));
+        roots_[b] = roots_[k];
+        return roots_[b];
+      }
+  }
+  auto cw = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
+  const int l0 = std::min(12, logm);
+  const size_t smem = size_t(16) << l0;
+  set_smem(qfd::k_pack_mobius_tile, smem);
+  qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
+                                                                                    cw->cw.p, logR, l0);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  mobius_rest(cw->cw.p, logm, logR, l0);
+  encode_and_hash(*cw);
+  if (blocks_.size() <= b) blocks_.resize(b + 1);
+  roots_.resize(std::max(roots_.size(), b + 1));
+  roots_[b] = cw->root_;
+  blocks_[b] = std::move(cw);
+  return roots_[b];
+}
+
+std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n) {
+  switch (n) {
+    case 1: qfd::k_reduce_partials<1><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p); break;
+    case 2: qfd::k_reduce_partials<2><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p); break;
+    case 3: qfd::k_reduce_partials<3><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p); break;
+    default: fail(QF_E_ARGUMENT, "reduce arity");
+  }
+  QF_CK(cudaGetLastError());
+  ++launches;
+  std::vector<F> out(n);
+  QF_CK(cudaMemcpyAsync(out.data(), result_.p, n * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return out;
+}
+
+// Two-level equality table of an MSB-first point: low coordinates index the
+// low table (equality_table, packed.rs:525-545).
+static void eq_tables(const std::vector<F>& point, std::vector<F>& hi, std::vector<F>& lo, int& lb) {
+  const int n = int(point.size());
+  lb = std::min(10, n);
+  hi = equality_table(std::vector<F>(point.begin(), point.begin() + (n - lb)));
+  lo = equality_table(std::vector<F>(point.begin() + (n - lb), point.end()));
+}
+
+std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& outer, size_t nblocks) {
+  const uint64_t m = P_.pcs.packed_len();
+  std::vector<F> hi, lo;
+  int lb;
+  eq_tables(outer, hi, lo, lb);
+  DBuf<Fe> dhi(hi.size()), dlo(lo.size());
+  QF_CK(cudaMemcpyAsync(dhi.p, hi.data(), hi.size() * 16, cudaMemcpyHostToDevice, s_));
+  QF_CK(cudaMemcpyAsync(dlo.p, lo.data(), lo.size() * 16, cudaMemcpyHostToDevice, s_));
+  weights_.alloc(m);
+  qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, weights_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  DBuf<unsigned long long> raw(64 * nblocks);
+  QF_CK(cudaMemsetAsync(raw.p, 0, 64 * nblocks * 8, s_));
+  for (size_t b = 0; b < nblocks; ++b) {
+    if (b * P_.block_len >= active_) continue;  // zero block: all lanes vanish
+    qfd::k_eq_project<<<grid_for(m * 8, qfd::kProjThreads), qfd::kProjThreads, 0, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
+                                                                                        m, weights_.p, raw.p + 64 * b);
+    QF_CK(cudaGetLastError());
+    ++launches;
+  }
+  std::vector<unsigned long long> h(64 * nblocks);
+  QF_CK(cudaMemcpyAsync(h.data(), raw.p, h.size() * 8, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  std::vector<std::vector<F>> out(nblocks, std::vector<F>(8));
+  for (size_t b = 0; b < nblocks; ++b)
+    for (int j = 0; j < 8; ++j)
+      for (int k = 0; k < 8; ++k) {
+        int64_t v = int64_t(h[64 * b + 8 * j + k]);
+        int64_t r = v % int64_t(P65521);
+        out[b][j].c[k] = uint16_t(r < 0 ? r + P65521 : r);
+      }
+  sum_len_ = 0;
+  return out;
+}
+
+std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
+  std::vector<std::vector<F>> lanes = project_blocks(outer, 1);
+  // Packed values of the single block: the block fold with weight one.
+  const uint64_t m = P_.pcs.packed_len();
+  values_.alloc(m);
+  std::vector<F> T(8);
+  for (int j = 0; j < 8; ++j) T[j] = basis<F>(j);
+  DBuf<Fe> dT(8);
+  QF_CK(cudaMemcpyAsync(dT.p, T.data(), 8 * 16, cudaMemcpyHostToDevice, s_));
+  qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, 8 * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  sum_len_ = m;
+  msg_valid_ = false;
+  return lanes[0];
+}
+
+void GpuBackend::apply_images(const std::vector<F>& images) {
+  DBuf<Fe> di(8);
+  QF_CK(cudaMemcpyAsync(di.p, images.data(), 8 * 16, cudaMemcpyHostToDevice, s_));
+  qfd::k_apply_images<<<grid_for(weights_.n, kThreads), kThreads, 0, s_>>>(weights_.p, weights_.n, di.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  QF_CK(cudaStreamSynchronize(s_));
+  msg_valid_ = false;
+}
+
+Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
+  const uint64_t m = P_.pcs.packed_len();
+  const int logm = ilog2(m);
+  const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+  const int blocks = int(fw.size());
+  std::vector<F> T(size_t(blocks) * 8);
+  for (int b = 0; b < blocks; ++b)
+    for (int j = 0; j < 8; ++j) T[b * 8 + j] = fw[b] * basis<F>(j);
+  DBuf<Fe> dT(T.size());
+  QF_CK(cudaMemcpyAsync(dT.p, T.data(), T.size() * 16, cudaMemcpyHostToDevice, s_));
+  values_.alloc(m);
+  set_smem(qfd::k_block_fold, T.size() * 16);
+  qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
+                                                                          values_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
+  const int l0 = std::min(12, logm);
+  const size_t smem = size_t(16) << l0;
+  set_smem(qfd::k_copy_mobius_tile, smem);
+  qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  mobius_rest(folded_->cw.p, logm, logR, l0);
+  encode_and_hash(*folded_);
+  sum_len_ = m;
+  msg_valid_ = false;
+  return folded_->root_;
+}
+
+void GpuBackend::sumcheck_message(F m[2]) {
+  if (!msg_valid_) {
+    const int g = grid_for(sum_len_ / 2, kThreads);
+    qfd::k_sum_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, partials_.p);
+    QF_CK(cudaGetLastError());
+    ++launches;
+    std::vector<F> r = reduce_to_host(partials_, g, 2);
+    msg_[0] = r[0];
+    msg_[1] = r[1];
+    msg_valid_ = true;
+  }
+  m[0] = msg_[0];
+  m[1] = msg_[1];
+}
+
+void GpuBackend::sumcheck_fold(F ch) {
+  if (tmp_v_.n < sum_len_ / 2) { tmp_v_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); tmp_w_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); }
+  const int g = grid_for(std::max<uint64_t>(sum_len_ / 4, 1), kThreads);
+  qfd::k_sum_fold_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  std::swap(values_, tmp_v_);
+  std::swap(weights_, tmp_w_);
+  sum_len_ /= 2;
+  if (sum_len_ >= 2) {
+    std::vector<F> r = reduce_to_host(partials_, g, 2);
+    msg_[0] = r[0];
+    msg_[1] = r[1];
+    msg_valid_ = true;
+  } else {
+    msg_valid_ = false;
+  }
+}
+
+F GpuBackend::sumcheck_final_value() {
+  F v;
+  QF_CK(cudaMemcpyAsync(&v, values_.p, 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return v;
+}
+F GpuBackend::sumcheck_final_weight() {
+  F v;
+  QF_CK(cudaMemcpyAsync(&v, weights_.p, 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return v;
+}
+
+std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) {
+  ByteWriter w;
+  w.bytes("QAFOLDB1", 8);
+  w.len(roots.size());
+  auto emit = [&](const DeviceCodeword& cw) {
+    Rows<F> r;
+    if (sel.all) {
+      r.all = true;
+      r.n_rows = cw.n_ext;
+      r.n_cols = cw.n_cols;
+      r.encoded = cw.entries();
+    } else {
+      auto rws = cw.rows(sel.rows);
+      auto pth = cw.paths(sel.rows);
+      for (size_t i = 0; i < sel.rows.size(); ++i) {
+        RowQuery<F> q;
+        q.row = std::move(rws[i]);
+        q.path.siblings = std::move(pth[i]);
+        r.partial.push_back(std::move(q));
+      }
+    }
+    write_rows(w, r);
+  };
+  for (size_t b = 0; b < roots.size(); ++b) {
+    const DeviceCodeword* cw = b < blocks_.size() ? blocks_[b].get() : nullptr;
+    if (!cw) {  // a repeated zero block: the first committed zero block
+      for (size_t k = 0; k < blocks_.size() && !cw; ++k)
+        if (blocks_[k] && roots_[k] == roots[b]) cw = blocks_[k].get();
+    }
+    if (!cw || cw->root_ != roots[b]) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
+    emit(*cw);
+  }
+  emit(*folded_);
+  return std::move(w.out);
+}
+
+// ---------------------------------------------------------------- TBV / EO
+std::vector<int8_t> GpuBackend::windows(const std::vector<uint64_t>& starts, size_t stride) {
+  std::vector<int8_t> out(starts.size() * stride);
+  if (starts.empty()) return out;
+  DBuf<uint64_t> ds(starts.size());
+  DBuf<int8_t> dout(out.size());
+  QF_CK(cudaMemcpyAsync(ds.p, starts.data(), starts.size() * 8, cudaMemcpyHostToDevice, s_));
+  qfd::k_gather_windows<<<grid_for(out.size(), kThreads, 1 << 20), kThreads, 0, s_>>>(bva_, active_, ds.p, uint32_t(starts.size()),
+                                                                                     int(stride), dout.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  QF_CK(cudaMemcpyAsync(out.data(), dout.p, out.size(), cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return out;
+}
+
+// Lane projections (tbv.rs:288-352) of large terms: two-level weight tables
+// per term, one tile per high-table entry.
+std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Term<F>*>& terms, size_t stride) {
+  std::vector<std::vector<F>> out(terms.size());
+  std::vector<qfd::ProjTile> tiles;
+  std::vector<F> lo_all;
+  std::vector<uint32_t> seg(1, 0);
+  std::vector<size_t> lanes_of(terms.size());
+  size_t common_lanes = 0;
+  for (size_t t = 0; t < terms.size(); ++t) {
+    const Term<F>& term = *terms[t];
+    size_t low_bits = std::min<size_t>(ilog2(stride), term.factors.size());
+    size_t lanes = size_t(1) << low_bits;
+    lanes_of[t] = lanes;
+    out[t].assign(lanes, F::zero());
+    if (common_lanes == 0) common_lanes = lanes;
+    if (lanes != common_lanes) fail(QF_E_ARGUMENT, "mixed lane widths");
+    if (term.offset >= active_ || term.scale.is_zero()) { seg.push_back(uint32_t(tiles.size())); continue; }
+    const size_t nh = term.factors.size() - low_bits;
+    const int lb = int(std::min<size_t>(10, nh));
+    const size_t rows = std::min((active_ - term.offset + lanes - 1) / lanes, term.len() / lanes);
+    const size_t ntiles = (rows + (size_t(1) << lb) - 1) >> lb;
+    std::vector<F> lo = factor_weights(term.factors.data() + low_bits, lb);
+    // High table entries for the tiles that touch active values, times scale.
+    std::vector<F> hi(ntiles, term.scale);
+    const auto* hf = term.factors.data() + low_bits + lb;
+    for (size_t i = 0; i < ntiles; ++i)
+      for (size_t k = 0; k < nh - lb; ++k) hi[i] = hi[i] * hf[k][(i >> k) & 1];
+    const uint32_t lo_off = uint32_t(lo_all.size());
+    lo_all.insert(lo_all.end(), lo.begin(), lo.end());
+    for (size_t i = 0; i < ntiles; ++i) {
+      qfd::ProjTile pt;
+      pt.base = term.offset + (i << lb) * lanes;
+      pt.rows = uint32_t(std::min<size_t>(size_t(1) << lb, rows - (i << lb)));
+      pt.lo_off = lo_off;
+      pt.hi = to_fe(hi[i]);
+      tiles.push_back(pt);
+    }
+    seg.push_back(uint32_t(tiles.size()));
+  }
+  if (tiles.empty()) return out;
+  DBuf<qfd::ProjTile> dt(tiles.size());
+  DBuf<Fe> dlo(lo_all.size()), dtile(tiles.size() * common_lanes), dterm(terms.size() * common_lanes);
+  DBuf<uint32_t> dseg(seg.size());
+  QF_CK(cudaMemcpyAsync(dt.p, tiles.data(), tiles.size() * sizeof(qfd::ProjTile), cudaMemcpyHostToDevice, s_));
+  QF_CK(cudaMemcpyAsync(dlo.p, lo_all.data(), lo_all.size() * 16, cudaMemcpyHostToDevice, s_));
+  QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, s_));
+  for (size_t off = 0; off < tiles.size(); off += 1u << 30) {
+    size_t cnt = std::min<size_t>(tiles.size() - off, size_t(1) << 30);
+    qfd::k_project_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(bva_, active_, dt.p + off, dlo.p, int(common_lanes),
+                                                             dtile.p + off * common_lanes);
+    QF_CK(cudaGetLastError());
+    ++launches;
+  }
+  qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  std::vector<F> h(terms.size() * common_lanes);
+  QF_CK(cudaMemcpyAsync(h.data(), dterm.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  for (size_t t = 0; t < terms.size(); ++t)
+    for (size_t l = 0; l < common_lanes; ++l) out[t][l] = h[t * common_lanes + l];
+  return out;
+}
+
+void GpuBackend::cross_terms(const Query<F>& q, size_t stride, std::vector<F>& pos, std::vector<F>& neg) {
+  pos.assign(stride - 1, F::zero());
+  neg.assign(stride - 1, F::zero());
+  std::vector<const Term<F>*> big, small;
+  for (const auto& t : q.terms) (t.len() >= stride ? big : small).push_back(&t);
+  std::vector<std::vector<F>> pr = project_terms(big, stride);
+  for (size_t i = 0; i < big.size(); ++i) {
+    std::vector<F> low = factor_weights(big[i]->factors.data(), ilog2(stride));
+    for (size_t d = 1; d < stride; ++d)
+      for (size_t lane = 0; lane + d < stride; ++lane) {
+        pos[d - 1] += pr[i][lane] * low[lane + d];
+        neg[d - 1] += pr[i][lane + d] * low[lane];
+      }
+  }
+  std::vector<uint64_t> starts;
+  for (const auto* t : small) starts.push_back(t->offset / stride * stride);
+  std::vector<int8_t> win = windows(starts, stride);
+  for (size_t s = 0; s < small.size(); ++s) {
+    const Term<F>& term = *small[s];
+    const size_t start = starts[s];
+    std::vector<F> qv(stride, F::zero());
+    for (size_t i = 0; i < term.len(); ++i) qv[term.offset - start + i] = term.weight(i);
+    const int8_t* v = win.data() + s * stride;
+    for (size_t d = 1; d < stride; ++d)
+      for (size_t lane = 0; lane + d < stride; ++lane) {
+        pos[d - 1] += qv[lane + d].mul_prime(F::small(v[lane]));
+        neg[d - 1] += qv[lane].mul_prime(F::small(v[lane + d]));
+      }
+  }
+}
+
+F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t stride) {
+  const uint64_t rows = logical / stride;
+  eo_len_ = rows;
+  wit_.alloc(rows);
+  qv_.alloc(rows);
+  std::vector<F> pinv = consecutive_powers(inv, stride);
+  DBuf<Fe> dp(stride);
+  QF_CK(cudaMemcpyAsync(dp.p, pinv.data(), stride * 16, cudaMemcpyHostToDevice, s_));
+  qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  // Query fold (tbv.rs:393-428): zero, then two disjoint passes of large-term
+  // tiles, then the merged small-term contributions.
+  QF_CK(cudaMemsetAsync(qv_.p, 0, rows * 16, s_));
+  std::vector<F> powers = consecutive_powers(ch, stride);
+  const size_t ls = ilog2(stride);
+  std::vector<qfd::QueryTile> pass_tiles[2];
+  std::vector<F> lo_all;
+  std::map<uint64_t, F> sparse;
+  const size_t n_claim_terms = P_.layout.buckets.size();
+  for (size_t ti = 0; ti < q.terms.size(); ++ti) {
+    const Term<F>& term = q.terms[ti];
+    if (term.len() >= stride) {
+      std::vector<F> low = factor_weights(term.factors.data(), ls);
+      F sc = F::zero();
+      for (size_t j = 0; j < stride; ++j) sc += low[j] * powers[j];
+      sc = term.scale * sc;
+      if (sc.is_zero()) continue;
+      const size_t nh = term.factors.size() - ls;
+      const int lb = int(std::min<size_t>(10, nh));
+      const size_t n_rows = term.len() / stride;
+      const size_t ntiles = n_rows >> lb;
+      std::vector<F> lo = factor_weights(term.factors.data() + ls, lb);
+      const uint32_t lo_off = uint32_t(lo_all.size());
+      lo_all.insert(lo_all.end(), lo.begin(), lo.end());
+      const auto* hf = term.factors.data() + ls + lb;
+      // Claim and zero-suffix terms are disjoint; padding terms overlap claim terms.
+      const int pass = (ti < n_claim_terms || term.offset >= P_.layout.active) ? 0 : 1;
+      for (size_t i = 0; i < ntiles; ++i) {
+        F h = sc;
+        for (size_t k = 0; k < nh - lb; ++k) h = h * hf[k][(i >> k) & 1];
+        qfd::QueryTile qt;
+        qt.start = term.offset / stride + (i << lb);
+        qt.rows = uint32_t(size_t(1) << lb);
+        qt.lo_off = lo_off;
+        qt.hi = to_fe(h);
+        pass_tiles[pass].push_back(qt);
+      }
+    } else {
+      for (size_t i = 0; i < term.len(); ++i) {
+        auto it = sparse.find(term.offset / stride);
+        F add = term.weight(i) * powers[(term.offset + i) % stride];
+        if (it == sparse.end()) sparse[term.offset / stride] = add; else it->second += add;
+      }
+    }
+  }
+  DBuf<Fe> dlo(std::max<size_t>(lo_all.size(), 1));
+  if (!lo_all.empty()) QF_CK(cudaMemcpyAsync(dlo.p, lo_all.data(), lo_all.size() * 16, cudaMemcpyHostToDevice, s_));
+  for (int pass = 0; pass < 2; ++pass) {
+    auto& tl = pass_tiles[pass];
+    if (tl.empty()) continue;
+    DBuf<qfd::QueryTile> dt(tl.size());
+    QF_CK(cudaMemcpyAsync(dt.p, tl.data(), tl.size() * sizeof(qfd::QueryTile), cudaMemcpyHostToDevice, s_));
+    for (size_t off = 0; off < tl.size(); off += 1u << 30) {
+      size_t cnt = std::min<size_t>(tl.size() - off, size_t(1) << 30);
+      qfd::k_query_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(dt.p + off, dlo.p, 1, qv_.p);
+      QF_CK(cudaGetLastError());
+      ++launches;
+    }
+    QF_CK(cudaStreamSynchronize(s_));
+  }
+  if (!sparse.empty()) {
+    std::vector<uint64_t> idx;
+    std::vector<F> vals;
+    for (auto& [k, v] : sparse) { idx.push_back(k); vals.push_back(v); }
+    DBuf<uint64_t> di(idx.size());
+    DBuf<Fe> dv(vals.size());
+    QF_CK(cudaMemcpyAsync(di.p, idx.data(), idx.size() * 8, cudaMemcpyHostToDevice, s_));
+    QF_CK(cudaMemcpyAsync(dv.p, vals.data(), vals.size() * 16, cudaMemcpyHostToDevice, s_));
+    qfd::k_scatter_add<<<unsigned((idx.size() + kThreads - 1) / kThreads), kThreads, 0, s_>>>(di.p, dv.p, uint32_t(idx.size()), qv_.p);
+    QF_CK(cudaGetLastError());
+    ++launches;
+    QF_CK(cudaStreamSynchronize(s_));
+  }
+  const int g = grid_for(std::max<uint64_t>(rows / 2, 1), kThreads);
+  qfd::k_eo_dot_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  std::vector<F> r = reduce_to_host(partials_, g, 3);
+  cross_ = {r[1], r[2]};
+  if (rows == 1) {  // a single packed row has no binary rounds
+    F w0, q0;
+    QF_CK(cudaMemcpyAsync(&w0, wit_.p, 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaMemcpyAsync(&q0, qv_.p, 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaStreamSynchronize(s_));
+    return w0 * q0;
+  }
+  return r[0];
+}
+
+void GpuBackend::eo_round_fold(F inv, F ch) {
+  const uint64_t n = eo_len_;
+  if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
+  const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
+  qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p);
+  QF_CK(cudaGetLastError());
+  ++launches;
+  std::swap(wit_, wit2_);
+  std::swap(qv_, qv2_);
+  eo_len_ = n / 2;
+  if (eo_len_ >= 2) {
+    std::vector<F> r = reduce_to_host(partials_, g, 2);
+    cross_ = {r[0], r[1]};
+  }
+}
+
+std::array<F, 2> GpuBackend::eo_terminal() {
+  F w0, q0;
+  QF_CK(cudaMemcpyAsync(&w0, wit_.p, 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaMemcpyAsync(&q0, qv_.p, 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return {w0, q0};
+}
+
+}  // namespace qfg

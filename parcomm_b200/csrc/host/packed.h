@@ -164,7 +164,7 @@ struct Backend {
   // Binding payload for the sampled rows of every block and the folded codeword.
   virtual std::vector<uint8_t> binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) = 0;
   // The folded codeword, for the native opening.
-  virtual const Codeword<F>& folded_codeword() = 0;
+  virtual const CodewordView<F>& folded_codeword() = 0;
   // Top row projection of the folded codeword at a row-weight vector.
   virtual std::vector<F> folded_row_projection(const std::vector<F>& row_weights) = 0;
 };
@@ -309,7 +309,7 @@ BatchOpening<F> open_batch(const PackedPcs<F>& pcs, Backend<F>& be, const std::v
   std::vector<uint8_t> binding = be.binding_rows(sel, roots);
   out.times.binding_ms = ms_since(t0);
   t0 = std::chrono::steady_clock::now();
-  const Codeword<F>& folded = be.folded_codeword();
+  const CodewordView<F>& folded = be.folded_codeword();
   const size_t col_log = ilog2(pcs.pp->extension_columns);
   std::vector<F> rw = tensor_weights(std::vector<F>(reduced.begin() + col_log, reduced.end()));
   std::vector<F> opening_vec = be.folded_row_projection(rw);
@@ -471,7 +471,7 @@ struct SingleBackend {
   virtual void sumcheck_fold(F ch) = 0;
   virtual F sumcheck_final_value() = 0;
   virtual F sumcheck_final_weight() = 0;
-  virtual const Codeword<F>& codeword() = 0;
+  virtual const CodewordView<F>& codeword() = 0;
   virtual std::vector<F> row_projection(const std::vector<F>& row_weights) = 0;
 };
 
@@ -518,7 +518,7 @@ BatchOpening<F> open_single(const PackedPcs<F>& pcs, SingleBackend<F>& be, const
     fail(QF_E_INVALID_COMMITMENT, "sumcheck terminal");
   out.times.sumcheck_ms = ms_since(t0);
   t0 = std::chrono::steady_clock::now();
-  const Codeword<F>& cw = be.codeword();
+  const CodewordView<F>& cw = be.codeword();
   const size_t col_log = ilog2(pcs.pp->extension_columns);
   std::vector<F> rw = tensor_weights(std::vector<F>(reduced.begin() + col_log, reduced.end()));
   std::vector<F> opening_vec = be.row_projection(rw);

@@ -432,18 +432,51 @@ std::unique_ptr<PcsParams<F>> pcs_setup(size_t n_witness, size_t extension_colum
 }
 
 // ------------------------------------------------------------ encoded matrices
-// A committed column-major codeword with its row tree (top level or carry).
+// Read access to a committed column-major codeword (host- or device-resident).
 template <class F>
-struct Codeword {
+struct CodewordView {
+  virtual ~CodewordView() {}
+  virtual Digest root() const = 0;
+  virtual size_t ext_rows() const = 0;
+  virtual size_t cols() const = 0;
+  // Freivalds fold of the systematic half: out[r] = sum_c w[c] * entry(c, r), r < n_rows.
+  virtual std::vector<F> fold_rows(size_t n_rows, const std::vector<F>& w) const = 0;
+  // Row projection of the systematic half: out[c] = sum_r w[r] * entry(c, r), r < n_rows.
+  virtual std::vector<F> project_rows(size_t n_rows, const std::vector<F>& w) const = 0;
+  // Sampled rows and their authentication paths.
+  virtual std::vector<std::vector<F>> rows(const std::vector<size_t>& idx) const = 0;
+  virtual std::vector<std::vector<Digest>> paths(const std::vector<size_t>& idx) const = 0;
+  // Every entry, column-major (all-row payloads of small codewords).
+  virtual std::vector<F> entries() const = 0;
+};
+
+// A committed column-major codeword with its row tree, held on the host.
+template <class F>
+struct Codeword : CodewordView<F> {
   std::vector<F> encoded;  // encoded[col * n_ext_rows + row]
   size_t n_ext_rows = 0, n_cols = 0;
   MerkleTree tree;
-  Digest root() const { return tree.root(); }
+  Digest root() const override { return tree.root(); }
+  size_t ext_rows() const override { return n_ext_rows; }
+  size_t cols() const override { return n_cols; }
   std::vector<F> row(size_t r) const {
     std::vector<F> v(n_cols);
     for (size_t c = 0; c < n_cols; ++c) v[c] = encoded[c * n_ext_rows + r];
     return v;
   }
+  std::vector<F> fold_rows(size_t n_rows, const std::vector<F>& w) const override;
+  std::vector<F> project_rows(size_t n_rows, const std::vector<F>& w) const override;
+  std::vector<std::vector<F>> rows(const std::vector<size_t>& idx) const override {
+    std::vector<std::vector<F>> out;
+    for (size_t r : idx) out.push_back(row(r));
+    return out;
+  }
+  std::vector<std::vector<Digest>> paths(const std::vector<size_t>& idx) const override {
+    std::vector<std::vector<Digest>> out;
+    for (size_t r : idx) out.push_back(tree.path(r));
+    return out;
+  }
+  std::vector<F> entries() const override { return encoded; }
 };
 
 // Encode each message column and hash rows (commit_owned_inner and
@@ -595,30 +628,32 @@ std::optional<VerifiedRound<F>> verify_round_reductions(const QaCode<F>& code, c
   return VerifiedRound<F>{msg->b_value, msg->b_point, gen->b_value, gen->b_point, msg->a_point};
 }
 
-// Row projection of the systematic half: out[c] = sum_r entries[c][r] * w[r].
 template <class F>
-std::vector<F> systematic_row_projection(const Codeword<F>& cw, size_t n_rows, const std::vector<F>& w) {
-  std::vector<F> out(cw.n_cols, F::zero());
+std::vector<F> Codeword<F>::project_rows(size_t n_rows, const std::vector<F>& w) const {
+  std::vector<F> out(n_cols, F::zero());
 #pragma omp parallel for if (n_rows >= 4096)
-  for (long c = 0; c < long(cw.n_cols); ++c) {
+  for (long c = 0; c < long(n_cols); ++c) {
     F s = F::zero();
-    const F* col = cw.encoded.data() + c * cw.n_ext_rows;
+    const F* col = encoded.data() + c * n_ext_rows;
     for (size_t r = 0; r < n_rows; ++r) s += w[r] * col[r];
     out[c] = s;
   }
   return out;
 }
-// Freivalds fold of the systematic half: out[r] = sum_c weights[c] * entries[c][r].
 template <class F>
-std::vector<F> systematic_fold(const Codeword<F>& cw, size_t n_rows, const std::vector<F>& weights) {
+std::vector<F> Codeword<F>::fold_rows(size_t n_rows, const std::vector<F>& weights) const {
   std::vector<F> out(n_rows);
 #pragma omp parallel for if (n_rows >= 4096)
   for (long r = 0; r < long(n_rows); ++r) {
     F s = F::zero();
-    for (size_t c = 0; c < cw.n_cols; ++c) s += weights[c] * cw.encoded[c * cw.n_ext_rows + r];
+    for (size_t c = 0; c < n_cols; ++c) s += weights[c] * encoded[c * n_ext_rows + r];
     out[r] = s;
   }
   return out;
+}
+template <class F>
+std::vector<F> systematic_row_projection(const CodewordView<F>& cw, size_t n_rows, const std::vector<F>& w) {
+  return cw.project_rows(n_rows, w);
 }
 
 // One opening round (top or extension).  `next` is the next code, or null at
@@ -632,18 +667,17 @@ struct RoundOutput {
 };
 
 template <class F>
-RoundOutput<F> prove_round(const PcsParams<F>& pp, size_t level, const Codeword<F>& cw, const std::vector<F>& point,
-                           const std::vector<F>& opening, const std::vector<F>& row_weights, PcsTranscript<F>& t,
-                           Rows<F>* move_all_rows_from = nullptr) {
+RoundOutput<F> prove_round(const PcsParams<F>& pp, size_t level, const CodewordView<F>& cw, const std::vector<F>& point,
+                           const std::vector<F>& opening, const std::vector<F>& row_weights, PcsTranscript<F>& t) {
   const QaCode<F>& code = pp.seq.codes[level];
   const QaCode<F>* next = level > 0 ? &pp.seq.codes[level - 1] : nullptr;
-  const size_t n_rows = code.message_len, n_cols = cw.n_cols;
+  const size_t n_rows = code.message_len, n_cols = cw.cols(), n_ext = cw.ext_rows();
   t.absorb_digest("round-root", cw.root());
   for (const F& o : opening) t.push_response(o);
   std::vector<F> freivalds;
   for (size_t i = 0; i < n_cols; ++i) freivalds.push_back(t.challenge_ext("freivalds"));
   F freivalds_value = inner_product(opening, freivalds);
-  std::vector<F> folded = systematic_fold(cw, n_rows, freivalds);
+  std::vector<F> folded = cw.fold_rows(n_rows, freivalds);
   RoundOutput<F> out;
   if (next) {
     // Folded vector is the next level's column-major message (32 columns).
@@ -652,32 +686,34 @@ RoundOutput<F> prove_round(const PcsParams<F>& pp, size_t level, const Codeword<
   } else {
     absorb_next_layer(t, false, hash_terminal_vector(folded));
   }
-  size_t qc = pp.num_queries(level, cw.n_ext_rows);
+  size_t qc = pp.num_queries(level, n_ext);
   Digest seed = t.challenge_digest("row-selection");
-  RowSelection sel = make_selection(qc, cw.n_ext_rows, seed);
+  RowSelection sel = make_selection(qc, n_ext, seed);
   std::vector<F> sampled(sel.size());
   if (sel.all) {
-    for (size_t r = 0; r < cw.n_ext_rows; ++r) {
+    std::vector<F> all = cw.entries();
+    for (size_t r = 0; r < n_ext; ++r) {
       F s = F::zero();
-      for (size_t c = 0; c < n_cols; ++c) s += freivalds[c] * cw.encoded[c * cw.n_ext_rows + r];
+      for (size_t c = 0; c < n_cols; ++c) s += freivalds[c] * all[c * n_ext + r];
       sampled[r] = s;
     }
     out.rows.all = true;
-    out.rows.n_rows = cw.n_ext_rows;
+    out.rows.n_rows = n_ext;
     out.rows.n_cols = n_cols;
-    out.rows.encoded = cw.encoded;
+    out.rows.encoded = std::move(all);
   } else {
+    std::vector<std::vector<F>> rws = cw.rows(sel.rows);
+    std::vector<std::vector<Digest>> pths = cw.paths(sel.rows);
     for (size_t i = 0; i < sel.size(); ++i) {
       RowQuery<F> q;
-      q.row = cw.row(sel.rows[i]);
-      q.path.siblings = cw.tree.path(sel.rows[i]);
+      q.row = std::move(rws[i]);
+      q.path.siblings = std::move(pths[i]);
       F s = F::zero();
       for (size_t c = 0; c < n_cols; ++c) s += freivalds[c] * q.row[c];
       sampled[i] = s;
       out.rows.partial.push_back(std::move(q));
     }
   }
-  (void)move_all_rows_from;
   t.absorb_exts("sampled-values", sampled);
   out.reduction = prove_round_reductions(code, point, freivalds, freivalds_value, folded, row_weights, sel, sampled, t);
   if (!next) out.terminal = std::move(folded);
@@ -694,7 +730,7 @@ struct OpenResult {
 // open_with_reduction (qafold_short_pc.rs:578-730).  `opening` is the top row
 // projection (computed by the caller's backend) and `claimed` its value.
 template <class F>
-OpenResult<F> open_with_reduction(const PcsParams<F>& pp, const Codeword<F>& top, const std::vector<F>& point,
+OpenResult<F> open_with_reduction(const PcsParams<F>& pp, const CodewordView<F>& top, const std::vector<F>& point,
                                   const std::vector<F>& opening, F claimed, const std::vector<F>& row_weights) {
   if (point.size() != size_t(ilog2(pp.n_witness))) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "opening point length");
   PcsTranscript<F> t;

@@ -27,19 +27,19 @@ struct QfError : std::runtime_error {
 };
 // Error codes mirror mikros_qafold::Error (vendor lib.rs:20-35) plus the
 // protocol's static `check` strings.
-enum : int {
-  QF_OK = 0,
-  QF_E_ENCODING = -1,
-  QF_E_HASHING = -2,
-  QF_E_INVALID_COMMITMENT = -3,
-  QF_E_INVALID_NUMBER_OF_VARIABLES = -4,
-  QF_E_INVALID_PARAMETERS = -5,
-  QF_E_TRANSCRIPT = -6,
-  QF_E_PROTOCOL = -7,
-  QF_E_CUDA = -8,
-  QF_E_ARGUMENT = -9,
-  QF_E_NO_DEVICE = -10,
-};
+#ifndef QF_OK  // same values as include/parcomm_qafold.h
+#define QF_OK 0
+#define QF_E_ENCODING -1
+#define QF_E_HASHING -2
+#define QF_E_INVALID_COMMITMENT -3
+#define QF_E_INVALID_NUMBER_OF_VARIABLES -4
+#define QF_E_INVALID_PARAMETERS -5
+#define QF_E_TRANSCRIPT -6
+#define QF_E_PROTOCOL -7
+#define QF_E_CUDA -8
+#define QF_E_ARGUMENT -9
+#define QF_E_NO_DEVICE -10
+#endif
 [[noreturn]] inline void fail(int code, const std::string& msg) { throw QfError(code, msg); }
 inline void check(bool ok, const char* msg) { if (!ok) fail(QF_E_PROTOCOL, msg); }
 

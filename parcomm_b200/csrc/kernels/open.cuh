@@ -1,0 +1,432 @@
+// Opening kernels: EO lane projections / witness / query fold / binary
+// rounds, the batch opening's equality-table lane projection, weight images,
+// block fold and degree-2 sumcheck, plus row/path gathers and the top-round
+// row projection and Freivalds fold.
+//
+// Every sum is exact: small signed weights times canonical coefficients
+// accumulate in 32-bit registers within a bounded tile and in 64-bit across
+// threads, and are reduced mod p once (the reference's i64 / u64 raw-lane
+// accumulators, tbv.rs:288-352, packed.rs:569-592).  Evaluation order does not
+// change any canonical result.
+#pragma once
+#include <cstdint>
+
+#include "../device/f65521_dev.cuh"
+
+namespace qfd {
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ uint32_t mod_i64(int64_t v) {
+  int64_t r = v % int64_t(P);
+  return uint32_t(r < 0 ? r + int64_t(P) : r);
+}
+__device__ __forceinline__ Fr shfl_xor(const Fr& v, int m) {
+  Fr r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r.c[k] = __shfl_xor_sync(0xffffffffu, v.c[k], m);
+  return r;
+}
+// Sums N field elements across the CTA; thread 0 receives the totals.
+template <int N>
+__device__ void block_reduce(Fr (&v)[N]) {
+  __shared__ Fr red_s[32][N];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+    for (int n = 0; n < N; ++n) v[n] = add(v[n], shfl_xor(v[n], o));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int n = 0; n < N; ++n) red_s[warp][n] = v[n];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int warps = (blockDim.x + 31) >> 5;
+    for (int w = 1; w < warps; ++w)
+#pragma unroll
+      for (int n = 0; n < N; ++n) v[n] = add(v[n], red_s[w][n]);
+  }
+}
+// partials[blockIdx][N] -> out[N] (single CTA).
+template <int N>
+__global__ void k_reduce_partials(const Fe* __restrict__ partials, uint32_t count, Fe* __restrict__ out) {
+  Fr v[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) v[n] = zero();
+  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x)
+#pragma unroll
+    for (int n = 0; n < N; ++n) v[n] = add(v[n], load(partials + size_t(i) * N + n));
+  block_reduce<N>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int n = 0; n < N; ++n) store(out + n, v[n]);
+}
+
+// Two-level product table: t[i] = hi[i >> lb] * lo[i & (2^lb - 1)].
+__device__ __forceinline__ Fr table_at(const Fe* hi, const Fe* lo, int lb, uint64_t i) {
+  return mul(load(hi + (i >> lb)), load(lo + (i & ((uint64_t(1) << lb) - 1))));
+}
+
+// ---------------------------------------------------------------- TBV projections
+// One tile of a large tensor term: `rows` consecutive rows of `lanes` BVA
+// values starting at `base`, all sharing the high weight `hi`; the low
+// weights are lo[0 .. rows).  Output: lanes field elements
+//   out[lane] = hi * sum_r lo[r] * v[base + r * lanes + lane].
+struct ProjTile {
+  uint64_t base;
+  uint32_t rows;
+  uint32_t lo_off;  // offset of this term's low table
+  Fe hi;
+};
+
+__global__ void k_project_tiles(const int8_t* __restrict__ bva, uint64_t active, const ProjTile* __restrict__ tiles,
+                                const Fe* __restrict__ lo_tables, int lanes, Fe* __restrict__ out) {
+  __shared__ int64_t acc_s[256][8];
+  const ProjTile t = tiles[blockIdx.x];
+  const int lane = threadIdx.x % lanes, phase = threadIdx.x / lanes, phases = blockDim.x / lanes;
+  int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const Fe* lo = lo_tables + t.lo_off;
+  for (uint32_t r = phase; r < t.rows; r += phases) {
+    const uint64_t g = t.base + uint64_t(r) * lanes + lane;
+    const int v = g < active ? int(bva[g]) : 0;
+    if (v != 0) {
+      Fr w = load(lo + r);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] += int32_t(w.c[k]) * v;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc_s[threadIdx.x][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < lanes) {
+    int64_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int p = 0; p < phases; ++p)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) s[k] += acc_s[p * lanes + threadIdx.x][k];
+    Fr sum;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sum.c[k] = mod_i64(s[k]);
+    store(out + size_t(blockIdx.x) * lanes + threadIdx.x, mul(load(&t.hi), sum));
+  }
+}
+
+// Segmented sum of tile outputs: term k owns tiles [seg[k], seg[k+1]).
+__global__ void k_sum_segments(const Fe* __restrict__ tile_out, const uint32_t* __restrict__ seg, int lanes,
+                               Fe* __restrict__ term_out) {
+  const uint32_t a = seg[blockIdx.x], b = seg[blockIdx.x + 1];
+  for (int lane = 0; lane < lanes; ++lane) {
+    Fr v[1] = {zero()};
+    for (uint32_t t = a + threadIdx.x; t < b; t += blockDim.x) v[0] = add(v[0], load(tile_out + size_t(t) * lanes + lane));
+    block_reduce<1>(v);
+    if (threadIdx.x == 0) store(term_out + size_t(blockIdx.x) * lanes + lane, v[0]);
+    __syncthreads();
+  }
+}
+
+// Copies the aligned stride-wide BVA window of each small term.
+__global__ void k_gather_windows(const int8_t* __restrict__ bva, uint64_t active, const uint64_t* __restrict__ starts,
+                                 uint32_t count, int stride, int8_t* __restrict__ out) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= uint64_t(count) * stride) return;
+  const uint64_t g = starts[i / stride] + i % stride;
+  out[i] = g < active ? bva[g] : int8_t(0);
+}
+
+// ---------------------------------------------------------------- EO
+// witness[row] = sum_lane v[row * stride + lane] * inv^lane (eo.rs:119-132).
+__global__ void k_eo_witness(const int8_t* __restrict__ bva, uint64_t active, uint64_t rows, int stride,
+                             const Fe* __restrict__ inv_powers, Fe* __restrict__ witness) {
+  __shared__ Fe pw[64];
+  if (threadIdx.x < stride) pw[threadIdx.x] = inv_powers[threadIdx.x];
+  __syncthreads();
+  for (uint64_t row = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < rows; row += uint64_t(gridDim.x) * blockDim.x) {
+    int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint64_t g0 = row * stride;
+    if (g0 < active) {
+      for (int lane = 0; lane < stride; ++lane) {
+        const uint64_t g = g0 + lane;
+        const int v = g < active ? int(bva[g]) : 0;
+        if (v) {
+          Fr p = load(pw + lane);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc[k] += int32_t(p.c[k]) * v;
+        }
+      }
+    }
+    Fr w;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) w.c[k] = mod_i64(acc[k]);
+    store(witness + row, w);
+  }
+}
+
+// Query-fold tile of a large term: q[start + r] (=|+=) hi * lo[r], r < rows.
+struct QueryTile {
+  uint64_t start;
+  uint32_t rows;
+  uint32_t lo_off;
+  Fe hi;
+};
+__global__ void k_query_tiles(const QueryTile* __restrict__ tiles, const Fe* __restrict__ lo_tables, int accumulate,
+                              Fe* __restrict__ q) {
+  const QueryTile t = tiles[blockIdx.x];
+  const Fr hi = load(&t.hi);
+  for (uint32_t r = threadIdx.x; r < t.rows; r += blockDim.x) {
+    Fr v = mul(hi, load(lo_tables + t.lo_off + r));
+    if (accumulate) v = add(v, load(q + t.start + r));
+    store(q + t.start + r, v);
+  }
+}
+__global__ void k_scatter_add(const uint64_t* __restrict__ idx, const Fe* __restrict__ vals, uint32_t n, Fe* __restrict__ q) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) store(q + idx[i], add(load(q + idx[i]), load(vals + i)));  // indices are unique
+}
+
+// dot(w, q) and the first binary cross pair.
+__global__ void k_eo_dot_cross(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n, Fe* __restrict__ partials) {
+  Fr v[3] = {zero(), zero(), zero()};
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n / 2; j += uint64_t(gridDim.x) * blockDim.x) {
+    Fr w0 = load(w + 2 * j), w1 = load(w + 2 * j + 1), q0 = load(q + 2 * j), q1 = load(q + 2 * j + 1);
+    v[0] = add(v[0], add(mul(w0, q0), mul(w1, q1)));
+    v[1] = add(v[1], mul(w0, q1));
+    v[2] = add(v[2], mul(w1, q0));
+  }
+  block_reduce<3>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; ++k) store(partials + size_t(blockIdx.x) * 3 + k, v[k]);
+}
+// w'[i] = w[2i] + w[2i+1] * inv; q'[i] = q[2i] + q[2i+1] * ch, plus the next
+// cross pair of (w', q') (eo.rs:141-160, fold_in_place 57-79).
+__global__ void k_eo_fold_cross(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n, Fe inv, Fe ch,
+                                Fe* __restrict__ w_out, Fe* __restrict__ q_out, Fe* __restrict__ partials) {
+  const Fr fi = load(&inv), fc = load(&ch);
+  Fr v[2] = {zero(), zero()};
+  if (n == 2) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      store(w_out, add(load(w), mul(load(w + 1), fi)));
+      store(q_out, add(load(q), mul(load(q + 1), fc)));
+    }
+  } else {
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n / 4; j += uint64_t(gridDim.x) * blockDim.x) {
+      Fr a0 = add(load(w + 4 * j), mul(load(w + 4 * j + 1), fi));
+      Fr a1 = add(load(w + 4 * j + 2), mul(load(w + 4 * j + 3), fi));
+      Fr b0 = add(load(q + 4 * j), mul(load(q + 4 * j + 1), fc));
+      Fr b1 = add(load(q + 4 * j + 2), mul(load(q + 4 * j + 3), fc));
+      store(w_out + 2 * j, a0);
+      store(w_out + 2 * j + 1, a1);
+      store(q_out + 2 * j, b0);
+      store(q_out + 2 * j + 1, b1);
+      v[0] = add(v[0], mul(a0, b1));
+      v[1] = add(v[1], mul(a1, b0));
+    }
+  }
+  block_reduce<2>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) store(partials + size_t(blockIdx.x) * 2 + k, v[k]);
+}
+
+// ---------------------------------------------------------------- batch opening
+// weights[i] = hi[i >> lb] * lo[i & mask]  (an equality or tensor table).
+__global__ void k_table(const Fe* __restrict__ hi, const Fe* __restrict__ lo, int lb, uint64_t m, Fe* __restrict__ out) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x)
+    store(out + i, table_at(hi, lo, lb, i));
+}
+
+// Raw lane sums of one block against the equality weights
+// (project_lanes_from_fn, packed_batch.rs:25-41):
+//   raw[j * 8 + k] += sum_i v(b, 8i + j) * weights[i].c[k]
+// Eight threads share an element, one lane j each.
+constexpr int kProjThreads = 256;
+__global__ void __launch_bounds__(kProjThreads) k_eq_project(const int8_t* __restrict__ bva, uint64_t active,
+                                                            uint64_t block_base, uint64_t m, const Fe* __restrict__ weights,
+                                                            unsigned long long* __restrict__ raw) {
+  __shared__ int64_t warp_s[kProjThreads / 32][32][8];
+  const int j = threadIdx.x & 7;
+  int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int64_t tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int count = 0;
+  const uint64_t stride = (uint64_t(gridDim.x) * blockDim.x) >> 3;
+  for (uint64_t i = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 3; i < m; i += stride) {
+    const uint64_t g = block_base + 8 * i + j;
+    const int v = g < active ? int(bva[g]) : 0;
+    if (v) {
+      Fr w = load(weights + i);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] += v * int32_t(w.c[k]);
+    }
+    if (++count == 64) {  // 64 * 128 * 65520 < 2^31
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { tot[k] += acc[k]; acc[k] = 0; }
+      count = 0;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    tot[k] += acc[k];
+    tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], 8);
+    tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], 16);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane < 8)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) warp_s[warp][lane][k] = tot[k];
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    const int jj = threadIdx.x >> 3, kk = threadIdx.x & 7;
+    int64_t s = 0;
+    for (int w = 0; w < kProjThreads / 32; ++w) s += warp_s[w][jj][kk];
+    atomicAdd(raw + threadIdx.x, (unsigned long long)s);  // two's complement sum
+  }
+}
+
+// w <- sum_j w.c[j] * images[j]  (apply_weight_images, packed.rs:634-650).
+__global__ void k_apply_images(Fe* __restrict__ weights, uint64_t m, const Fe* __restrict__ images) {
+  __shared__ uint32_t img[8][8];
+  if (threadIdx.x < 64) img[threadIdx.x >> 3][threadIdx.x & 7] = images[threadIdx.x >> 3].c[threadIdx.x & 7];
+  __syncthreads();
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+    Fr w = load(weights + i);
+    Fr o;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      uint64_t s = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s += uint64_t(w.c[j]) * img[j][k];
+      o.c[k] = red64(s);
+    }
+    store(weights + i, o);
+  }
+}
+
+// values[i] = sum_b fold[b] * packed(b, i) = sum_{b,j} v(b, 8i+j) * T[b][j],
+// with T[b][j] = fold[b] * X^j precomputed (packed_batch.rs:213-222).
+__global__ void k_block_fold(const int8_t* __restrict__ bva, uint64_t active, uint64_t block_len, int blocks, uint64_t m,
+                             const Fe* __restrict__ T, Fe* __restrict__ values) {
+  extern __shared__ uint4 smem_u4[];
+  Fe* Ts = reinterpret_cast<Fe*>(smem_u4);
+  for (int t = threadIdx.x; t < blocks * 8; t += blockDim.x) Ts[t] = T[t];
+  __syncthreads();
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+    int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < blocks; ++b) {
+      const uint64_t g = uint64_t(b) * block_len + 8 * i;
+      if (g >= active) break;  // later blocks start even later
+      int8_t v[8];
+      if (g + 8 <= active) {
+        uint2 raw8 = *reinterpret_cast<const uint2*>(bva + g);
+        const int8_t* bb = reinterpret_cast<const int8_t*>(&raw8);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = bb[j];
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[j] = g + j < active ? bva[g + j] : int8_t(0);
+      }
+      int32_t a32[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (v[j] == 0) continue;
+        Fr t = load(Ts + b * 8 + j);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a32[k] += int32_t(v[j]) * int32_t(t.c[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] += a32[k];
+    }
+    Fr o;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) o.c[k] = mod_i64(acc[k]);
+    store(values + i, o);
+  }
+}
+
+// Degree-2 sumcheck message on (v, w) of length n: sum_{i<h} v_i w_i and
+// sum (v_{i+h} - v_i)(w_{i+h} - w_i) (round_message, packed.rs:652-667).
+__global__ void k_sum_message(const Fe* __restrict__ v, const Fe* __restrict__ w, uint64_t n, Fe* __restrict__ partials) {
+  const uint64_t h = n / 2;
+  Fr s[2] = {zero(), zero()};
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < h; i += uint64_t(gridDim.x) * blockDim.x) {
+    Fr a = load(v + i), b = load(w + i), c = load(v + i + h), d = load(w + i + h);
+    s[0] = add(s[0], mul(a, b));
+    s[1] = add(s[1], mul(sub(c, a), sub(d, b)));
+  }
+  block_reduce<2>(s);
+  if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
+}
+// Fold both vectors at ch (lo <- lo + ch (hi - lo), packed.rs:674-696) and
+// emit the next message of the folded vectors.  Thread i < n/4 produces
+// entries i and i + n/4 of the new length-n/2 vectors.
+__global__ void k_sum_fold_message(const Fe* __restrict__ v, const Fe* __restrict__ w, uint64_t n, Fe ch,
+                                   Fe* __restrict__ v_out, Fe* __restrict__ w_out, Fe* __restrict__ partials) {
+  const Fr c = load(&ch);
+  const uint64_t h = n / 2, q = n / 4;
+  Fr s[2] = {zero(), zero()};
+  if (n == 2) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      Fr a = load(v), b = load(v + 1);
+      store(v_out, add(a, mul(c, sub(b, a))));
+      Fr x = load(w), y = load(w + 1);
+      store(w_out, add(x, mul(c, sub(y, x))));
+    }
+  } else {
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < q; i += uint64_t(gridDim.x) * blockDim.x) {
+      Fr a0 = load(v + i), a1 = load(v + i + h), b0 = load(v + i + q), b1 = load(v + i + q + h);
+      Fr nv0 = add(a0, mul(c, sub(a1, a0))), nv1 = add(b0, mul(c, sub(b1, b0)));
+      Fr x0 = load(w + i), x1 = load(w + i + h), y0 = load(w + i + q), y1 = load(w + i + q + h);
+      Fr nw0 = add(x0, mul(c, sub(x1, x0))), nw1 = add(y0, mul(c, sub(y1, y0)));
+      store(v_out + i, nv0);
+      store(v_out + i + q, nv1);
+      store(w_out + i, nw0);
+      store(w_out + i + q, nw1);
+      s[0] = add(s[0], mul(nv0, nw0));
+      s[1] = add(s[1], mul(sub(nv1, nv0), sub(nw1, nw0)));
+    }
+  }
+  block_reduce<2>(s);
+  if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
+}
+
+// ---------------------------------------------------------------- codeword access
+__global__ void k_gather_rows(const Fe* __restrict__ cw, uint64_t n_ext, int n_cols, const uint64_t* __restrict__ idx,
+                              uint32_t count, Fe* __restrict__ out) {
+  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= uint64_t(count) * n_cols) return;
+  const uint64_t q = t / n_cols, c = t % n_cols;
+  out[t] = cw[c * n_ext + idx[q]];
+}
+// Sibling digests of each queried leaf, leaf level first.
+__global__ void k_gather_paths(const uint4* __restrict__ tree, const uint64_t* __restrict__ level_off, int depth,
+                               const uint64_t* __restrict__ idx, uint32_t count, uint4* __restrict__ out) {
+  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= uint64_t(count) * depth) return;
+  const uint64_t q = t / depth;
+  const int l = int(t % depth);
+  const uint64_t node = (idx[q] >> l) ^ 1;
+  const uint64_t off = level_off[l] + node;
+  out[2 * t] = tree[2 * off];
+  out[2 * t + 1] = tree[2 * off + 1];
+}
+// out[c] partials: sum_{r in chunk} w[r] * cw[c * n_ext + r], r < n_rows.
+__global__ void k_row_project(const Fe* __restrict__ cw, uint64_t n_ext, uint64_t n_rows, const Fe* __restrict__ hi,
+                              const Fe* __restrict__ lo, int lb, Fe* __restrict__ partials) {
+  const int c = blockIdx.y;
+  Fr s[1] = {zero()};
+  for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rows; r += uint64_t(gridDim.x) * blockDim.x)
+    s[0] = add(s[0], mul(table_at(hi, lo, lb, r), load(cw + uint64_t(c) * n_ext + r)));
+  block_reduce<1>(s);
+  if (threadIdx.x == 0) store(partials + size_t(c) * gridDim.x + blockIdx.x, s[0]);
+}
+// out[r] = sum_c fw[c] * cw[c * n_ext + r], r < n_rows (base_systematic_fold).
+__global__ void k_row_fold(const Fe* __restrict__ cw, uint64_t n_ext, uint64_t n_rows, int n_cols, const Fe* __restrict__ fw,
+                           Fe* __restrict__ out) {
+  __shared__ Fe f_s[64];
+  if (threadIdx.x < n_cols) f_s[threadIdx.x] = fw[threadIdx.x];
+  __syncthreads();
+  for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rows; r += uint64_t(gridDim.x) * blockDim.x) {
+    Fr s = zero();
+    for (int c = 0; c < n_cols; ++c) s = add(s, mul(load(f_s + c), load(cw + uint64_t(c) * n_ext + r)));
+    store(out + r, s);
+  }
+}
+
+}  // namespace qfd

@@ -1,0 +1,56 @@
+"""Regenerates reference_vectors.json from the reference's own files (read as text).
+
+Run in the development container where the reference checkout is mounted:
+    python tests/golden/extract_reference_vectors.py /path/to/reference
+Sources:
+  * validation/qafold8-smoke-final/run.log  (F65521 demo bundle: proof bytes,
+    proof BLAKE2s printed with `{:x?}` (no zero padding), commitment JSON size)
+  * validation/qafold16-smoke/run.log       (KoalaBear demo bundle)
+  * qafold/f65521/vendor/qafold/src/qafold_short_pc.rs  (native opening +
+    Decide wire fixture digest, test `native_opening_and_decide_wire_fixture`)
+"""
+import json
+import re
+import sys
+from pathlib import Path
+
+
+def smoke(path: Path) -> dict:
+    for line in path.read_text().splitlines():
+        if '"proof_blake2s"' in line:
+            rec = json.loads(line)
+            digest = "".join(f"{int(x, 16):02x}" for x in rec["proof_blake2s"].strip("[]").split(", "))
+            return {"proof_bytes": rec["proof_bytes"], "proof_blake2s": digest,
+                    "public_commitment_json_bytes": rec["public_commitment_json_bytes"],
+                    "active_entries": rec["active_entries"], "logical_entries": rec["logical_entries"],
+                    "bucket_count": rec["bucket_count"], "pcs_blocks": rec.get("verifier_profile", {}).get("authenticated_roots"),
+                    "source": str(path.relative_to(path.parents[2]))}
+    raise SystemExit(f"no proof record in {path}")
+
+
+def wire_fixture(path: Path) -> dict:
+    text = path.read_text()
+    i = text.index("fn native_opening_and_decide_wire_fixture")
+    block = text[i:]
+    arr = re.search(r"assert_eq!\(\s*digest,\s*\[(.*?)\]", block, re.S).group(1)
+    digest = "".join(f"{int(x, 16):02x}" for x in re.findall(r"0x([0-9a-fA-F]{2})", arr))
+    line = text[:i].count("\n") + 1
+    return {"blake2s_root_opening_decide": digest, "source": f"qafold/f65521/vendor/qafold/src/qafold_short_pc.rs:{line}",
+            "pcs": {"n_witness": 65536, "extension_columns": 16, "index": 2, "security_bits": 80},
+            "rng_seed_u64": "0x706172616c6c656c"}
+
+
+def main(ref: Path) -> None:
+    out = {
+        "f65521_demo": smoke(ref / "validation/qafold8-smoke-final/run.log"),
+        "koalabear_demo": smoke(ref / "validation/qafold16-smoke/run.log"),
+        "f65521_wire_fixture": wire_fixture(ref / "qafold/f65521/vendor/qafold/src/qafold_short_pc.rs"),
+        "demo_command": "demo --chunk-log 10 --packed-log 4 --cache-mode recompute",
+    }
+    dst = Path(__file__).with_name("reference_vectors.json")
+    dst.write_text(json.dumps(out, indent=2) + "\n")
+    print(dst)
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))

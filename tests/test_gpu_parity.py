@@ -1,0 +1,92 @@
+"""GPU proofs are byte-identical to the CPU oracle's (and to the reference's
+golden demo digest), through the C ABI.  Requires a B200."""
+import hashlib
+
+import numpy as np
+import pytest
+
+import oracle
+import parcomm_b200 as qf
+from parcomm_b200 import layout
+
+pytestmark = pytest.mark.gpu
+
+
+def blake2s(b: bytes) -> str:
+    return hashlib.blake2s(b, digest_size=32).hexdigest()
+
+
+def gaussian_i8(rng, n, sigma=20.0, forced=0.0):
+    v = np.clip(np.rint(rng.normal(0.0, sigma, n)), -127, 127).astype(np.int8)
+    if forced:
+        idx = rng.choice(n, max(1, int(n * forced)), replace=False)
+        v[idx] = np.where(rng.random(idx.size) < 0.5, -127, 127).astype(np.int8)
+    return v
+
+
+def run_both(shapes, chunk_log, packed_log, mats):
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=packed_log))
+    bva = layout.encode(p.shapes, mats)
+    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, packed_log, bva)
+    c = p.commit(bva)
+    assert b"".join(c.roots) == o_roots, "commitment roots differ"
+    claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
+    assert qf.claims_to_bytes(claims) == o_claims, "claims differ"
+    proof, prof = p.prove(c, claims)
+    assert proof.to_bytes() == o_proof, "proof bytes differ"
+    p.verify(c.roots, claims, proof)
+    assert oracle.verify(p.shapes, chunk_log, packed_log, o_roots, o_claims, proof.to_bytes())
+    c.close()
+    return proof, prof
+
+
+def test_demo_bundle_matches_reference_digest(vectors):
+    shapes = qf.demo_shapes()
+    proof, prof = run_both(shapes, 10, 4, layout.demo_matrices(shapes))
+    assert len(proof.to_bytes()) == vectors["f65521_demo"]["proof_bytes"]
+    assert blake2s(proof.to_bytes()) == vectors["f65521_demo"]["proof_blake2s"]
+    assert prof.kernel_launches > 0
+
+
+def test_smoke_config_1024x4096_chunk20():
+    rng = np.random.default_rng(0)
+    mats = [gaussian_i8(rng, 1024 * 4096).reshape(1024, 4096)]
+    run_both([(1024, 4096)], 20, 4, mats)
+
+
+@pytest.mark.parametrize("packed_log", [1, 4, 6])
+def test_ragged_shapes_multilevel(packed_log):
+    rng = np.random.default_rng(7 + packed_log)
+    shapes = [(300, 700), (129, 65), (1, 5000), (77, 1)]
+    mats = [gaussian_i8(rng, r * c, forced=0.001).reshape(r, c) for r, c in shapes]
+    run_both(shapes, 14, packed_log, mats)
+
+
+def test_single_block_opening():
+    rng = np.random.default_rng(3)
+    mats = [gaussian_i8(rng, 64 * 64).reshape(64, 64)]
+    run_both([(64, 64)], 12, 4, mats)
+
+
+def test_zero_suffix_blocks_share_one_commitment():
+    rng = np.random.default_rng(5)
+    shapes = [(1024, 1024), (1, 16)]
+    mats = [gaussian_i8(rng, r * c).reshape(r, c) for r, c in shapes]
+    proof, _ = run_both(shapes, 16, 4, mats)
+
+
+def test_extreme_values_and_all_zero():
+    shapes = [(256, 256), (3, 3)]
+    mats = [np.full((256, 256), -127, np.int8), np.zeros((3, 3), np.int8)]
+    mats[0][::7, ::3] = 127
+    run_both(shapes, 12, 3, mats)
+
+
+def test_nonzero_padding_rejected():
+    p = qf.Parameters([(31, 31)], qf.Config(chunk_log=10, packed_log=4))
+    bva = layout.encode(p.shapes, [np.ones((31, 31), np.int8)])
+    bs, _, _ = layout.buckets(p.shapes)
+    b = next(b for b in bs if b.cols > b.physical_cols)
+    bva[b.offset + b.physical_cols] = 1
+    with pytest.raises(qf.QfError, match="nonzero boundary padding"):
+        p.commit(bva)

@@ -1,0 +1,29 @@
+"""Layout of the 8B-shape collection (226 matrices) and the smoke matrix."""
+import parcomm_b200 as qf
+from parcomm_b200 import layout
+
+
+def shapes_8b():
+    s = []
+    for _ in range(32):
+        s += [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096), (14336, 4096), (14336, 4096), (4096, 14336)]
+    return [(128256, 4096)] + s + [(128256, 4096)]
+
+
+def test_8b_shape_layout():
+    bs, active, logical = layout.buckets(shapes_8b())
+    assert len(shapes_8b()) == 226
+    assert sum(r * c for r, c in shapes_8b()) == 8_029_995_008
+    assert (len(bs), active, logical) == (424, 8_053_063_680, 1 << 33)
+
+
+def test_python_layout_matches_library():
+    p = qf.Parameters(shapes_8b()[1:4] + [(31, 37)], qf.Config(chunk_log=20, packed_log=4))
+    bs, active, logical = layout.buckets(p.shapes)
+    assert (p.active, p.logical, p.buckets) == (active, logical, len(bs))
+
+
+def test_intervals_last_doubled():
+    assert layout.intervals(31) == [(0, 16), (16, 8), (24, 4), (28, 4)]
+    assert layout.intervals(37) == [(0, 32), (32, 4), (36, 1)]
+    assert layout.intervals(128256) == [(0, 65536), (65536, 32768), (98304, 16384), (114688, 16384)]
