@@ -1,0 +1,335 @@
+"""QAFold commit+open throughput on B200: the 8B-shape 8-bit batched workload.
+
+Workload (one step): commit every 2^30-entry PCS block of the 226-matrix
+8B-shape collection (int8 round(N(0, 20^2)) clipped to +-127, 0.1% of entries
+forced to +-127; F65521^8, chunk_log 30, packed_log 4) and prove the
+benchmark claims, producing the reference's proof bytes.  As in the reference
+prover timer (main.rs:176-210) a step is commit + prove + serialisation;
+setup and claim generation are outside it.  The claims are computed once
+(their points derive from the committed roots, identical every step).
+
+  value  : weights/s with the BVA already in HBM (Parameters.commit(on_device)).
+  e2e    : weights/s through the same public API from a pinned host BVA
+           (host->device copy of the weights and proof bytes back per step).
+
+`--impl reference` times the CPU restatement of the reference prover (the
+oracle; the Rust reference cannot be built in this image) with all host
+threads on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+WEIGHTS_8B = 8_029_995_008
+
+
+def shapes_8b():
+    s = []
+    for _ in range(32):
+        s += [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096), (14336, 4096), (14336, 4096), (4096, 14336)]
+    return [(128256, 4096)] + s + [(128256, 4096)]
+
+
+def make_bva_on_device(shapes, seed: int = 0):
+    """Deterministic synthetic int8 weights laid out as the BVA, generated on the GPU."""
+    import torch
+    from parcomm_b200 import layout
+
+    buckets, active, _ = layout.buckets(shapes)
+    out = torch.zeros(active, dtype=torch.int8, device="cuda")
+    by_matrix = {}
+    for b in buckets:
+        by_matrix.setdefault(b.matrix, []).append(b)
+    g = torch.Generator(device="cuda")
+    for m, (rows, cols) in enumerate(shapes):
+        g.manual_seed(seed * 100003 + m)
+        w = torch.randn(rows * cols, generator=g, device="cuda", dtype=torch.float32).mul_(20.0).round_().clamp_(-127, 127)
+        n_forced = max(1, (rows * cols) // 1000)
+        idx = torch.randint(0, rows * cols, (n_forced,), generator=g, device="cuda")
+        sign = torch.randint(0, 2, (n_forced,), generator=g, device="cuda").float().mul_(254.0).sub_(127.0)
+        w[idx] = sign
+        w = w.to(torch.int8).view(rows, cols)
+        for b in by_matrix[m]:
+            dst = out[b.offset: b.offset + b.rows * b.cols].view(b.rows, b.cols)
+            dst[: b.physical_rows, : b.physical_cols] = w[b.row_offset: b.row_offset + b.physical_rows,
+                                                           b.col_offset: b.col_offset + b.physical_cols]
+        del w
+    torch.cuda.synchronize()
+    return out, active
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, path: Path):
+        self.path = path
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self, device_index: int = 0):
+        if not self.path.exists():
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(device_index):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(kernel)
+
+
+def run_reference(args):
+    """CPU restatement of the reference prover on a bounded sample of the workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+    import oracle
+    from parcomm_b200 import layout
+
+    # One decoder layer's attention projections (4 matrices, 41.9M weights),
+    # chunk_log 24 so the sample keeps the batched multi-block opening.
+    shapes = [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096)]
+    rng = np.random.default_rng(0)
+    mats = []
+    for r, c in shapes:
+        w = np.clip(np.rint(rng.normal(0, 20, r * c)), -127, 127).astype(np.int8)
+        idx = rng.choice(r * c, (r * c) // 1000, replace=False)
+        w[idx] = np.where(rng.random(idx.size) < 0.5, -127, 127)
+        mats.append(w.reshape(r, c))
+    bva = layout.encode(shapes, mats)
+    weights = sum(r * c for r, c in shapes)
+    threads = os.cpu_count() or 1
+    times = []
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, 24, 4, bva)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append((commit_ms + open_ms) / 1000.0)
+    sec = statistics.mean(times)
+    value = weights / sec
+    sample = (f"4 matrices of one 8B decoder layer (q,k,v,o: {weights} weights), chunk_log 24, packed_log 4, "
+              f"C++ restatement of the reference CPU prover (OpenMP, {threads} threads)")
+    line = {
+        "impl": "reference", "metric": "QAFold commit+open weights/s", "value": value, "unit": "weights/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+        "data": "synthetic", "config": {"workload": "8B-shape 8-bit weights, batched (sample)", "field": "F65521^8",
+                                        "chunk_log": 24, "packed_log": 4, "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "weights/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "weights/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="8b8", choices=["8b8", "smoke"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--out", default=str(ROOT / "gpurun_out"))
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+
+    import torch
+    import parcomm_b200 as qf
+    from parcomm_b200.build import build
+
+    build()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    if args.workload == "8b8":
+        shapes, cfg, name = shapes_8b(), qf.Config(30, 4), "8B-shape 8-bit weights, batched (226 matrices)"
+    else:
+        shapes, cfg, name = [(1024, 4096)], qf.Config(20, 4), "smoke 1024x4096 int8"
+    weights = sum(r * c for r, c in shapes)
+
+    t0 = time.time()
+    params = qf.Parameters(shapes, cfg)
+    setup_s = time.time() - t0
+    bva_dev, active = make_bva_on_device(shapes, seed=rank)
+    bva_host = torch.empty(active, dtype=torch.int8, pin_memory=True)
+    bva_host.copy_(bva_dev)
+
+    # Claims once: their points derive from the (step-invariant) roots.
+    c = params.commit(bva_dev, on_device=True)
+    claims = params.evaluate_claims(c, params.benchmark_points(c.roots))
+    proof, prof = params.prove(c, claims)
+    c.close()
+    verify_s = None
+    if rank == 0:
+        t0 = time.time()
+        params.verify(c.roots, claims, proof)
+        verify_s = time.time() - t0
+    proof_bytes = len(proof.to_bytes())
+
+    def step(on_device: bool):
+        cc = params.commit(bva_dev if on_device else bva_host, on_device=on_device)
+        pr, pf = params.prove(cc, claims)
+        cc.close()
+        return pr, pf
+
+    for _ in range(max(args.warmup - 1, 0)):
+        step(True)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed(on_device: bool, steps: int):
+        barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = qf.kernel_launches()
+        ev0.record()
+        last = None
+        for _ in range(steps):
+            last = step(on_device)
+        ev1.record()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps, last, qf.kernel_launches() - launches0
+
+    out_dir = Path(args.out)
+    out_dir.mkdir(exist_ok=True)
+    with ClockSampler(out_dir / "bench_clocks.csv") as clocks:
+        ms_dev, (pr_dev, pf_dev), launches = timed(True, args.steps)
+    ms_e2e, (pr_e2e, pf_e2e), _ = timed(False, max(1, args.steps))
+    assert pr_dev.to_bytes() == proof.to_bytes() == pr_e2e.to_bytes(), "proof bytes changed between steps"
+
+    # Per-kernel device time (CUDA events on each launch's own stream), one extra step.
+    qf.kernel_timing(True)
+    step(True)
+    torch.cuda.synchronize()
+    stats = qf.kernel_stats()
+    qf.kernel_timing(False)
+    dominant = max(stats, key=lambda k: stats[k]["ms"])
+    d = stats[dominant]
+    achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = ncu_traffic(dominant)
+
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    cpu_baseline = None
+    if not args.no_cpu_baseline:
+        try:
+            r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
+                                "--warmup", "0"], capture_output=True, text=True, timeout=900)
+            cpu_baseline = json.loads(r.stdout.strip().splitlines()[-1])["cpu_baseline"]
+        except Exception as e:  # reported, not fatal
+            cpu_baseline = {"error": str(e)[:200]}
+    value = weights * world / (ms_dev / 1000.0)
+    line = {
+        "metric": "QAFold commit+open weights/s",
+        "value": value,
+        "unit": "weights/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_dev,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int8",
+        "data": "synthetic",
+        "config": {"workload": name, "field": "F65521^8", "chunk_log": cfg.chunk_log, "packed_log": cfg.packed_log,
+                   "weights": weights, "active_entries": active, "pcs_blocks": params.blocks,
+                   "l2": "inputs larger than L2 (8 GB BVA, 4 GiB codeword per block)",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "e2e": {"value": weights * world / (ms_e2e / 1000.0), "unit": "weights/s",
+                "h2d_bytes_per_step": active, "d2h_bytes_per_step": proof_bytes},
+        "gpu_launches": launches // max(args.steps, 1),
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic, "kernel_ms_per_step": d["ms"], "kernel_launches": d["launches"],
+                     "alg_bytes_per_launch": d["bytes"] / max(d["launches"], 1)},
+        "cpu_baseline": cpu_baseline,
+        "clocks": clocks.summary(local),
+        "proof_bytes": proof_bytes,
+        "stage_ms": {k: getattr(pf_dev, k) for k in ("commit_ms", "eo_ms", "projection_ms", "folding_ms", "sumcheck_ms",
+                                                     "binding_ms", "native_opening_ms", "decide_ms", "open_ms")},
+        "setup_s": setup_s,
+        "verify_s": verify_s,
+    }
+    (out_dir / "bench_kernels.json").write_text(json.dumps(stats, indent=1))
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -93,6 +93,15 @@ int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* clai
               size_t proof_len);
 
 void qf_free_bytes(uint8_t* bytes);
+
+/* Diagnostics (no reference counterpart): per-kernel device time measured with
+ * CUDA events on each kernel's launching stream.  qf_kernel_timing(1) resets
+ * and enables recording; qf_kernel_stats writes JSON
+ * {"kernel": {"launches": n, "ms": t}, ...}.  qf_kernel_launches counts every
+ * kernel launched by this library since load. */
+int qf_kernel_timing(int enable);
+int qf_kernel_stats(char* buf, size_t cap, size_t* len);
+uint64_t qf_kernel_launches(void);
 size_t qf_last_error(char* buf, size_t cap);
 
 #ifdef __cplusplus

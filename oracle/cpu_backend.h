@@ -150,10 +150,12 @@ struct CpuBackend : Backend<F>, SingleBackend<F>, EoBackend<F> {
   }
   const CodewordView<F>& folded_codeword() override { return *folded; }
   const CodewordView<F>& codeword() override { return *blocks[0]; }
-  std::vector<F> folded_row_projection(const std::vector<F>& rw) override {
+  std::vector<F> folded_opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
+    rw = tensor_weights(std::vector<F>(point.begin() + col_log, point.end()));
     return systematic_row_projection(*folded, P.pcs.pp->top_rows(), rw);
   }
-  std::vector<F> row_projection(const std::vector<F>& rw) override {
+  std::vector<F> opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
+    rw = tensor_weights(std::vector<F>(point.begin() + col_log, point.end()));
     return systematic_row_projection(*blocks[0], P.pcs.pp->top_rows(), rw);
   }
 

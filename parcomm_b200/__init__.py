@@ -58,6 +58,7 @@ _lib = None
 EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
+    "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches",
 )
 
 
@@ -87,6 +88,10 @@ def lib() -> ctypes.CDLL:
         L.qf_free_bytes.restype = None
         L.qf_last_error.argtypes = [ctypes.c_char_p, S]
         L.qf_last_error.restype = S
+        L.qf_kernel_timing.argtypes = [ctypes.c_int]
+        L.qf_kernel_stats.argtypes = [ctypes.c_char_p, S, ctypes.POINTER(S)]
+        L.qf_kernel_launches.argtypes = []
+        L.qf_kernel_launches.restype = U64
         for name in EXPORTED:
             if not hasattr(L, name):
                 raise QfError(-9, f"library does not export {name}")
@@ -305,6 +310,25 @@ class Parameters:
         pb = proof.to_bytes() if isinstance(proof, Proof) else bytes(proof)
         cb = claims_to_bytes(claims)
         _check(lib().qf_verify(self._h, b"".join(roots), cb, len(cb), pb, len(pb)))
+
+
+def kernel_timing(enable: bool) -> None:
+    """Enables per-kernel CUDA-event timing (diagnostics; adds event records per launch)."""
+    _check(lib().qf_kernel_timing(int(enable)))
+
+
+def kernel_stats() -> dict:
+    """{kernel: {"launches", "ms", "bytes"}} since the last kernel_timing(True)."""
+    import json
+    n = ctypes.c_size_t()
+    _check(lib().qf_kernel_stats(None, 0, ctypes.byref(n)))
+    buf = ctypes.create_string_buffer(n.value + 1)
+    _check(lib().qf_kernel_stats(buf, n.value + 1, ctypes.byref(n)))
+    return json.loads(buf.raw[: n.value].decode())
+
+
+def kernel_launches() -> int:
+    return int(lib().qf_kernel_launches())
 
 
 def demo_shapes() -> List[Shape]:

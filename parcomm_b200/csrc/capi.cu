@@ -296,7 +296,7 @@ int qf_prove(const qf_params* params, qf_committed* committed, const uint8_t* cl
       profile->native_opening_ms = op.times.native_opening_ms;
       profile->decide_ms = op.times.decide_ms;
       profile->open_ms = ms_since(t0);
-      profile->kernel_launches = committed->be->launches;
+      profile->kernel_launches = qfg::KernelClock::launches.load();
     }
   });
 }
@@ -313,6 +313,19 @@ int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* clai
 }
 
 void qf_free_bytes(uint8_t* bytes) { std::free(bytes); }
+
+int qf_kernel_timing(int enable) {
+  return guarded([&] { qfg::KernelClock::reset(enable != 0); });
+}
+
+int qf_kernel_stats(char* buf, size_t cap, size_t* len) {
+  return guarded([&] {
+    std::string j = qfg::KernelClock::stats_json();
+    copy_out(std::vector<uint8_t>(j.begin(), j.end()), reinterpret_cast<uint8_t*>(buf), cap, len);
+  });
+}
+
+uint64_t qf_kernel_launches(void) { return qfg::KernelClock::launches.load(); }
 
 size_t qf_last_error(char* buf, size_t cap) {
   if (buf && cap) {

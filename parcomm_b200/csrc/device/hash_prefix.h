@@ -5,11 +5,12 @@
 
 namespace qfd {
 
-// Leaf message = 75-byte prefix (framed domain and width) || row bytes.  The
-// first 64 bytes are absorbed into `mid`; `tail` holds prefix bytes 64..74.
+// Leaf message = prefix (framed domain and width; 75 bytes for base rows,
+// 80 for extension rows) || row bytes.  The first 64 bytes are absorbed into
+// `mid`; `tail` holds the remaining prefix bytes.
 struct LeafPrefix {
   uint32_t mid[8];
-  uint32_t tail[3];
+  uint32_t tail[4];  // 11 (base-row) or 16 (extension-row) bytes
 };
 
 // Inner message = 50-byte framed domain || left || right.

@@ -2,6 +2,7 @@
 #include "gpu_backend.cuh"
 #include "kernels/commit.cuh"
 #include "kernels/open.cuh"
+#include "kernels/vec.cuh"
 
 #include <map>
 
@@ -9,21 +10,74 @@ namespace qfg {
 
 static constexpr int kThreads = 256;
 
-qfd::LeafPrefix leaf_prefix(size_t n_cols) {
+bool KernelClock::enabled = false;
+std::mutex KernelClock::mu;
+std::vector<KernelClock::Rec> KernelClock::recs;
+std::atomic<uint64_t> KernelClock::launches{0};
+
+KernelClock::Scope::Scope(cudaStream_t s, const char* n, uint64_t b_) : stream(s), name(n), bytes(b_) {
+  if (enabled) {
+    QF_CK(cudaEventCreate(&a));
+    QF_CK(cudaEventCreate(&b));
+    QF_CK(cudaEventRecord(a, stream));
+  }
+}
+void KernelClock::Scope::done() {
+  ++launches;
+  if (enabled) {
+    QF_CK(cudaEventRecord(b, stream));
+    std::lock_guard<std::mutex> g(mu);
+    recs.push_back({name, a, b, bytes});
+  }
+}
+void KernelClock::reset(bool on) {
+  std::lock_guard<std::mutex> g(mu);
+  for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  recs.clear();
+  enabled = on;
+}
+std::string KernelClock::stats_json() {
+  QF_CK(cudaDeviceSynchronize());
+  std::lock_guard<std::mutex> g(mu);
+  struct Agg { uint64_t n = 0, bytes = 0; double ms = 0; };
+  std::map<std::string, Agg> agg;
+  for (auto& r : recs) {
+    float ms = 0;
+    QF_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    auto& e = agg[r.name];
+    e.n += 1;
+    e.ms += ms;
+    e.bytes += r.bytes;
+  }
+  std::string s = "{";
+  bool first = true;
+  for (auto& [k, v] : agg) {
+    if (!first) s += ",";
+    first = false;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu}", k.c_str(),
+                  (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
+    s += buf;
+  }
+  return s + "}";
+}
+
+qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain) {
   std::vector<uint8_t> pre;
-  append_frame(pre, "domain", kLeafBaseDomain, std::strlen(kLeafBaseDomain));
+  const char* dom = ext_domain ? kLeafExtDomain : kLeafBaseDomain;
+  append_frame(pre, "domain", dom, std::strlen(dom));
   auto w = le64(n_cols);
   append_frame(pre, "width", w.data(), 8);
-  if (pre.size() != 75) fail(QF_E_ENCODING, "leaf prefix length");
+  if (pre.size() != (ext_domain ? 80u : 75u)) fail(QF_E_ENCODING, "leaf prefix length");
   qfd::LeafPrefix lp;
   uint32_t h[8];
   for (int i = 0; i < 8; ++i) h[i] = kBlake2sIv[i];
   h[0] ^= 0x01010000u ^ 32u;
   blake2s_compress(h, pre.data(), 64, false);
   for (int i = 0; i < 8; ++i) lp.mid[i] = h[i];
-  uint8_t tail[12] = {0};
-  std::memcpy(tail, pre.data() + 64, 11);
-  for (int i = 0; i < 3; ++i)
+  uint8_t tail[16] = {0};
+  std::memcpy(tail, pre.data() + 64, pre.size() - 64);
+  for (int i = 0; i < 4; ++i)
     lp.tail[i] = uint32_t(tail[4 * i]) | (uint32_t(tail[4 * i + 1]) << 8) | (uint32_t(tail[4 * i + 2]) << 16) |
                  (uint32_t(tail[4 * i + 3]) << 24);
   return lp;
@@ -57,8 +111,7 @@ static void set_smem(K kernel, size_t bytes) {
 std::vector<F> DeviceCodeword::fold_rows(size_t n_rows, const std::vector<F>& w) const {
   DBuf<Fe> dw(n_cols), out(n_rows);
   QF_CK(cudaMemcpyAsync(dw.p, w.data(), n_cols * 16, cudaMemcpyHostToDevice, stream));
-  qfd::k_row_fold<<<grid_for(n_rows, kThreads), kThreads, 0, stream>>>(cw.p, n_ext, n_rows, int(n_cols), dw.p, out.p);
-  QF_CK(cudaGetLastError());
+  QF_LAUNCH(stream, "k_row_fold", uint64_t(n_rows) * n_cols * 16 + uint64_t(n_rows) * 16, qfd::k_row_fold<<<grid_for(n_rows, kThreads), kThreads, 0, stream>>>(cw.p, n_ext, n_rows, int(n_cols), dw.p, out.p));
   std::vector<F> h(n_rows);
   QF_CK(cudaMemcpyAsync(h.data(), out.p, n_rows * 16, cudaMemcpyDeviceToHost, stream));
   QF_CK(cudaStreamSynchronize(stream));
@@ -75,8 +128,7 @@ std::vector<F> DeviceCodeword::project_rows(size_t n_rows, const std::vector<F>&
   const int chunks = int(std::min<size_t>(64, (n_rows + kThreads - 1) / kThreads));
   DBuf<Fe> part(n_cols * chunks);
   dim3 grid(chunks, unsigned(n_cols));
-  qfd::k_row_project<<<grid, kThreads, 0, stream>>>(cw.p, n_ext, n_rows, hi.p, lo.p, ilog2(n_rows), part.p);
-  QF_CK(cudaGetLastError());
+  QF_LAUNCH(stream, "k_row_project", uint64_t(n_rows) * n_cols * 16 + uint64_t(n_rows) * 16, qfd::k_row_project<<<grid, kThreads, 0, stream>>>(cw.p, n_ext, n_rows, hi.p, lo.p, ilog2(n_rows), part.p));
   std::vector<F> hp(n_cols * chunks);
   QF_CK(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 16, cudaMemcpyDeviceToHost, stream));
   QF_CK(cudaStreamSynchronize(stream));
@@ -93,9 +145,8 @@ std::vector<std::vector<F>> DeviceCodeword::rows(const std::vector<size_t>& idx)
   DBuf<uint64_t> did(id.size());
   DBuf<Fe> dout(id.size() * n_cols);
   QF_CK(cudaMemcpyAsync(did.p, id.data(), id.size() * 8, cudaMemcpyHostToDevice, stream));
-  qfd::k_gather_rows<<<grid_for(id.size() * n_cols, kThreads, 1 << 20), kThreads, 0, stream>>>(cw.p, n_ext, int(n_cols), did.p,
-                                                                                               uint32_t(id.size()), dout.p);
-  QF_CK(cudaGetLastError());
+  QF_LAUNCH(stream, "k_gather_rows", uint64_t(id.size()) * n_cols * 32, qfd::k_gather_rows<<<grid_for(id.size() * n_cols, kThreads, 1 << 20), kThreads, 0, stream>>>(cw.p, n_ext, int(n_cols), did.p,
+                                                                                               uint32_t(id.size()), dout.p));
   std::vector<F> h(id.size() * n_cols);
   QF_CK(cudaMemcpyAsync(h.data(), dout.p, h.size() * 16, cudaMemcpyDeviceToHost, stream));
   QF_CK(cudaStreamSynchronize(stream));
@@ -113,9 +164,8 @@ std::vector<std::vector<Digest>> DeviceCodeword::paths(const std::vector<size_t>
   QF_CK(cudaMemcpyAsync(did.p, id.data(), id.size() * 8, cudaMemcpyHostToDevice, stream));
   QF_CK(cudaMemcpyAsync(doff.p, level_off.data(), level_off.size() * 8, cudaMemcpyHostToDevice, stream));
   if (depth > 0) {
-    qfd::k_gather_paths<<<grid_for(id.size() * depth, kThreads, 1 << 20), kThreads, 0, stream>>>(tree.p, doff.p, depth, did.p,
-                                                                                                 uint32_t(id.size()), dout.p);
-    QF_CK(cudaGetLastError());
+    QF_LAUNCH(stream, "k_gather_paths", uint64_t(id.size()) * depth * 64, qfd::k_gather_paths<<<grid_for(id.size() * depth, kThreads, 1 << 20), kThreads, 0, stream>>>(tree.p, doff.p, depth, did.p,
+                                                                                                 uint32_t(id.size()), dout.p));
   }
   std::vector<uint4> h(id.size() * depth * 2);
   QF_CK(cudaMemcpyAsync(h.data(), dout.p, h.size() * 16, cudaMemcpyDeviceToHost, stream));
@@ -155,18 +205,13 @@ void GpuBackend::mobius_rest(Fe* cw, int logm, int logR, int from) {
     int k = std::min(9, logm - lo);
     size_t smem = size_t(8) << k << 4;
     set_smem(qfd::k_butterfly_strided<qfd::kMobius>, smem);
-    qfd::k_butterfly_strided<qfd::kMobius><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(cw, logR, lo, k);
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_butterfly_strided", (uint64_t(2) << logm) * 16, qfd::k_butterfly_strided<qfd::kMobius><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(cw, logR, lo, k));
     lo += k;
   }
 }
 
-// Parity = WHT(alpha1 * WHT(message)) per column, then leaf hashes and tree.
-void GpuBackend::encode_and_hash(DeviceCodeword& out) {
-  ensure_alpha();
-  const int logm = ilog2(P_.pcs.packed_len());
-  const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+// Parity = WHT(alpha * WHT(message)) per column, then leaf hashes and tree.
+void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain) {
   const size_t R = size_t(1) << logR;
   const int wl = std::min(12, logR);
   const size_t tsmem = size_t(16) << wl;
@@ -174,36 +219,36 @@ void GpuBackend::encode_and_hash(DeviceCodeword& out) {
   Fe* msg = out.cw.p;
   Fe* par = out.cw.p + R;
   for (int pass = 0; pass < 2; ++pass) {
-    qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), kThreads, tsmem, s_>>>(pass == 0 ? msg : par, par,
-                                                                              pass == 0 ? nullptr : alpha1_.p, logR, wl);
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logm) * 16,
+              qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), kThreads, tsmem, s_>>>(pass == 0 ? msg : par, par,
+                                                                                        pass == 0 ? nullptr : alpha, logR, wl));
     for (int lo = wl; lo < logR;) {
       int k = std::min(9, logR - lo);
       size_t smem = size_t(8) << k << 4;
       set_smem(qfd::k_butterfly_strided<qfd::kWht>, smem);
-      qfd::k_butterfly_strided<qfd::kWht><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(par, logR, lo, k);
-      QF_CK(cudaGetLastError());
-      ++launches;
+      QF_LAUNCH(s_, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
+                qfd::k_butterfly_strided<qfd::kWht><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(par, logR, lo, k));
       lo += k;
     }
   }
   // Leaves and inner levels.
   const uint64_t n_ext = 2 * R;
-  qfd::LeafPrefix lp = leaf_prefix(out.n_cols);
-  qfd::k_hash_leaves<<<unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads), qfd::kLeafThreads, 0, s_>>>(
-      out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  qfd::LeafPrefix lp = leaf_prefix(out.n_cols, ext_domain);
+  const unsigned lgrid = unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads);
+  if (ext_domain)
+    QF_LAUNCH(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32,
+              qfd::k_hash_leaves<16><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
+  else
+    QF_LAUNCH(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32,
+              qfd::k_hash_leaves<11><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
   qfd::InnerPrefix ip = inner_prefix();
   out.level_off.clear();
   uint64_t off = 0, n = n_ext;
   while (n > 1) {
     out.level_off.push_back(off);
-    qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s_>>>(out.tree.p + 2 * off, n / 2, ip,
-                                                                                   out.tree.p + 2 * (off + n));
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_hash_inner", n * 32 + (n / 2) * 32,
+              qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s_>>>(out.tree.p + 2 * off, n / 2, ip,
+                                                                                             out.tree.p + 2 * (off + n)));
     off += n;
     n /= 2;
   }
@@ -241,12 +286,11 @@ Digest GpuBackend::commit_block(size_t b) {
   const int l0 = std::min(12, logm);
   const size_t smem = size_t(16) << l0;
   set_smem(qfd::k_pack_mobius_tile, smem);
-  qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
-                                                                                    cw->cw.p, logR, l0);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
+                                                                                    cw->cw.p, logR, l0));
   mobius_rest(cw->cw.p, logm, logR, l0);
-  encode_and_hash(*cw);
+  ensure_alpha();
+  encode_and_hash(*cw, alpha1_.p, logR, logm, false);
   if (blocks_.size() <= b) blocks_.resize(b + 1);
   roots_.resize(std::max(roots_.size(), b + 1));
   roots_[b] = cw->root_;
@@ -256,13 +300,11 @@ Digest GpuBackend::commit_block(size_t b) {
 
 std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n) {
   switch (n) {
-    case 1: qfd::k_reduce_partials<1><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p); break;
-    case 2: qfd::k_reduce_partials<2><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p); break;
-    case 3: qfd::k_reduce_partials<3><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p); break;
+    case 1: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 16, qfd::k_reduce_partials<1><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;
+    case 2: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 32, qfd::k_reduce_partials<2><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;
+    case 3: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 48, qfd::k_reduce_partials<3><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;
     default: fail(QF_E_ARGUMENT, "reduce arity");
   }
-  QF_CK(cudaGetLastError());
-  ++launches;
   std::vector<F> out(n);
   QF_CK(cudaMemcpyAsync(out.data(), result_.p, n * 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
@@ -287,17 +329,13 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   QF_CK(cudaMemcpyAsync(dhi.p, hi.data(), hi.size() * 16, cudaMemcpyHostToDevice, s_));
   QF_CK(cudaMemcpyAsync(dlo.p, lo.data(), lo.size() * 16, cudaMemcpyHostToDevice, s_));
   weights_.alloc(m);
-  qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, weights_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_table", m * 16, qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, weights_.p));
   DBuf<unsigned long long> raw(64 * nblocks);
   QF_CK(cudaMemsetAsync(raw.p, 0, 64 * nblocks * 8, s_));
   for (size_t b = 0; b < nblocks; ++b) {
     if (b * P_.block_len >= active_) continue;  // zero block: all lanes vanish
-    qfd::k_eq_project<<<grid_for(m * 8, qfd::kProjThreads), qfd::kProjThreads, 0, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
-                                                                                        m, weights_.p, raw.p + 64 * b);
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_eq_project", m * 24, qfd::k_eq_project<<<grid_for(m * 8, qfd::kProjThreads), qfd::kProjThreads, 0, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
+                                                                                        m, weights_.p, raw.p + 64 * b));
   }
   std::vector<unsigned long long> h(64 * nblocks);
   QF_CK(cudaMemcpyAsync(h.data(), raw.p, h.size() * 8, cudaMemcpyDeviceToHost, s_));
@@ -323,9 +361,7 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   for (int j = 0; j < 8; ++j) T[j] = basis<F>(j);
   DBuf<Fe> dT(8);
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), 8 * 16, cudaMemcpyHostToDevice, s_));
-  qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, 8 * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_block_fold", m * 24, qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, 8 * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p));
   sum_len_ = m;
   msg_valid_ = false;
   return lanes[0];
@@ -334,9 +370,7 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
 void GpuBackend::apply_images(const std::vector<F>& images) {
   DBuf<Fe> di(8);
   QF_CK(cudaMemcpyAsync(di.p, images.data(), 8 * 16, cudaMemcpyHostToDevice, s_));
-  qfd::k_apply_images<<<grid_for(weights_.n, kThreads), kThreads, 0, s_>>>(weights_.p, weights_.n, di.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_apply_images", uint64_t(weights_.n) * 32, qfd::k_apply_images<<<grid_for(weights_.n, kThreads), kThreads, 0, s_>>>(weights_.p, weights_.n, di.p));
   QF_CK(cudaStreamSynchronize(s_));
   msg_valid_ = false;
 }
@@ -353,19 +387,16 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), T.size() * 16, cudaMemcpyHostToDevice, s_));
   values_.alloc(m);
   set_smem(qfd::k_block_fold, T.size() * 16);
-  qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
-                                                                          values_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_block_fold", m * (8 * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
+                                                                          values_.p));
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(12, logm);
   const size_t smem = size_t(16) << l0;
   set_smem(qfd::k_copy_mobius_tile, smem);
-  qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0));
   mobius_rest(folded_->cw.p, logm, logR, l0);
-  encode_and_hash(*folded_);
+  ensure_alpha();
+  encode_and_hash(*folded_, alpha1_.p, logR, logm, false);
   sum_len_ = m;
   msg_valid_ = false;
   return folded_->root_;
@@ -374,9 +405,7 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
 void GpuBackend::sumcheck_message(F m[2]) {
   if (!msg_valid_) {
     const int g = grid_for(sum_len_ / 2, kThreads);
-    qfd::k_sum_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, partials_.p);
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_sum_message", sum_len_ * 32, qfd::k_sum_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, partials_.p));
     std::vector<F> r = reduce_to_host(partials_, g, 2);
     msg_[0] = r[0];
     msg_[1] = r[1];
@@ -389,9 +418,7 @@ void GpuBackend::sumcheck_message(F m[2]) {
 void GpuBackend::sumcheck_fold(F ch) {
   if (tmp_v_.n < sum_len_ / 2) { tmp_v_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); tmp_w_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); }
   const int g = grid_for(std::max<uint64_t>(sum_len_ / 4, 1), kThreads);
-  qfd::k_sum_fold_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_sum_fold_message", sum_len_ * 48, qfd::k_sum_fold_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p));
   std::swap(values_, tmp_v_);
   std::swap(weights_, tmp_w_);
   sum_len_ /= 2;
@@ -461,10 +488,8 @@ std::vector<int8_t> GpuBackend::windows(const std::vector<uint64_t>& starts, siz
   DBuf<uint64_t> ds(starts.size());
   DBuf<int8_t> dout(out.size());
   QF_CK(cudaMemcpyAsync(ds.p, starts.data(), starts.size() * 8, cudaMemcpyHostToDevice, s_));
-  qfd::k_gather_windows<<<grid_for(out.size(), kThreads, 1 << 20), kThreads, 0, s_>>>(bva_, active_, ds.p, uint32_t(starts.size()),
-                                                                                     int(stride), dout.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_gather_windows", uint64_t(out.size()) * 2, qfd::k_gather_windows<<<grid_for(out.size(), kThreads, 1 << 20), kThreads, 0, s_>>>(bva_, active_, ds.p, uint32_t(starts.size()),
+                                                                                     int(stride), dout.p));
   QF_CK(cudaMemcpyAsync(out.data(), dout.p, out.size(), cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
   return out;
@@ -476,6 +501,7 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
   std::vector<std::vector<F>> out(terms.size());
   std::vector<qfd::ProjTile> tiles;
   std::vector<F> lo_all;
+  uint64_t proj_bytes = 0;
   std::vector<uint32_t> seg(1, 0);
   std::vector<size_t> lanes_of(terms.size());
   size_t common_lanes = 0;
@@ -493,17 +519,17 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
     const size_t rows = std::min((active_ - term.offset + lanes - 1) / lanes, term.len() / lanes);
     const size_t ntiles = (rows + (size_t(1) << lb) - 1) >> lb;
     std::vector<F> lo = factor_weights(term.factors.data() + low_bits, lb);
-    // High table entries for the tiles that touch active values, times scale.
-    std::vector<F> hi(ntiles, term.scale);
-    const auto* hf = term.factors.data() + low_bits + lb;
-    for (size_t i = 0; i < ntiles; ++i)
-      for (size_t k = 0; k < nh - lb; ++k) hi[i] = hi[i] * hf[k][(i >> k) & 1];
+    // High table entries (one product per entry by doubling), times scale.
+    std::vector<F> hi = factor_weights(term.factors.data() + low_bits + lb, nh - lb);
+    hi.resize(ntiles);
+    for (auto& h : hi) h = h * term.scale;
     const uint32_t lo_off = uint32_t(lo_all.size());
     lo_all.insert(lo_all.end(), lo.begin(), lo.end());
     for (size_t i = 0; i < ntiles; ++i) {
       qfd::ProjTile pt;
       pt.base = term.offset + (i << lb) * lanes;
       pt.rows = uint32_t(std::min<size_t>(size_t(1) << lb, rows - (i << lb)));
+      proj_bytes += uint64_t(pt.rows) * lanes + 16;
       pt.lo_off = lo_off;
       pt.hi = to_fe(hi[i]);
       tiles.push_back(pt);
@@ -519,14 +545,10 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
   QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, s_));
   for (size_t off = 0; off < tiles.size(); off += 1u << 30) {
     size_t cnt = std::min<size_t>(tiles.size() - off, size_t(1) << 30);
-    qfd::k_project_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(bva_, active_, dt.p + off, dlo.p, int(common_lanes),
-                                                             dtile.p + off * common_lanes);
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_project_tiles", proj_bytes, qfd::k_project_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(bva_, active_, dt.p + off, dlo.p, int(common_lanes),
+                                                             dtile.p + off * common_lanes));
   }
-  qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_sum_segments", uint64_t(tiles.size()) * common_lanes * 16, qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p));
   std::vector<F> h(terms.size() * common_lanes);
   QF_CK(cudaMemcpyAsync(h.data(), dterm.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
@@ -574,15 +596,14 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
   std::vector<F> pinv = consecutive_powers(inv, stride);
   DBuf<Fe> dp(stride);
   QF_CK(cudaMemcpyAsync(dp.p, pinv.data(), stride * 16, cudaMemcpyHostToDevice, s_));
-  qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_eo_witness", std::min<uint64_t>(active_, rows * stride) + rows * 16, qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p));
   // Query fold (tbv.rs:393-428): zero, then two disjoint passes of large-term
   // tiles, then the merged small-term contributions.
   QF_CK(cudaMemsetAsync(qv_.p, 0, rows * 16, s_));
   std::vector<F> powers = consecutive_powers(ch, stride);
   const size_t ls = ilog2(stride);
   std::vector<qfd::QueryTile> pass_tiles[2];
+  uint64_t query_bytes[2] = {0, 0};
   std::vector<F> lo_all;
   std::map<uint64_t, F> sparse;
   const size_t n_claim_terms = P_.layout.buckets.size();
@@ -601,18 +622,18 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
       std::vector<F> lo = factor_weights(term.factors.data() + ls, lb);
       const uint32_t lo_off = uint32_t(lo_all.size());
       lo_all.insert(lo_all.end(), lo.begin(), lo.end());
-      const auto* hf = term.factors.data() + ls + lb;
+      std::vector<F> hi = factor_weights(term.factors.data() + ls + lb, nh - lb);
       // Claim and zero-suffix terms are disjoint; padding terms overlap claim terms.
       const int pass = (ti < n_claim_terms || term.offset >= P_.layout.active) ? 0 : 1;
       for (size_t i = 0; i < ntiles; ++i) {
-        F h = sc;
-        for (size_t k = 0; k < nh - lb; ++k) h = h * hf[k][(i >> k) & 1];
+        F h = sc * hi[i];
         qfd::QueryTile qt;
         qt.start = term.offset / stride + (i << lb);
         qt.rows = uint32_t(size_t(1) << lb);
         qt.lo_off = lo_off;
         qt.hi = to_fe(h);
         pass_tiles[pass].push_back(qt);
+        query_bytes[pass] += uint64_t(qt.rows) * 32;
       }
     } else {
       for (size_t i = 0; i < term.len(); ++i) {
@@ -631,9 +652,7 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
     QF_CK(cudaMemcpyAsync(dt.p, tl.data(), tl.size() * sizeof(qfd::QueryTile), cudaMemcpyHostToDevice, s_));
     for (size_t off = 0; off < tl.size(); off += 1u << 30) {
       size_t cnt = std::min<size_t>(tl.size() - off, size_t(1) << 30);
-      qfd::k_query_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(dt.p + off, dlo.p, 1, qv_.p);
-      QF_CK(cudaGetLastError());
-      ++launches;
+      QF_LAUNCH(s_, "k_query_tiles", query_bytes[pass], qfd::k_query_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(dt.p + off, dlo.p, 1, qv_.p));
     }
     QF_CK(cudaStreamSynchronize(s_));
   }
@@ -645,15 +664,11 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
     DBuf<Fe> dv(vals.size());
     QF_CK(cudaMemcpyAsync(di.p, idx.data(), idx.size() * 8, cudaMemcpyHostToDevice, s_));
     QF_CK(cudaMemcpyAsync(dv.p, vals.data(), vals.size() * 16, cudaMemcpyHostToDevice, s_));
-    qfd::k_scatter_add<<<unsigned((idx.size() + kThreads - 1) / kThreads), kThreads, 0, s_>>>(di.p, dv.p, uint32_t(idx.size()), qv_.p);
-    QF_CK(cudaGetLastError());
-    ++launches;
+    QF_LAUNCH(s_, "k_scatter_add", uint64_t(idx.size()) * 48, qfd::k_scatter_add<<<unsigned((idx.size() + kThreads - 1) / kThreads), kThreads, 0, s_>>>(di.p, dv.p, uint32_t(idx.size()), qv_.p));
     QF_CK(cudaStreamSynchronize(s_));
   }
   const int g = grid_for(std::max<uint64_t>(rows / 2, 1), kThreads);
-  qfd::k_eo_dot_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_eo_dot_cross", rows * 32, qfd::k_eo_dot_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p));
   std::vector<F> r = reduce_to_host(partials_, g, 3);
   cross_ = {r[1], r[2]};
   if (rows == 1) {  // a single packed row has no binary rounds
@@ -670,9 +685,7 @@ void GpuBackend::eo_round_fold(F inv, F ch) {
   const uint64_t n = eo_len_;
   if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
   const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
-  qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p);
-  QF_CK(cudaGetLastError());
-  ++launches;
+  QF_LAUNCH(s_, "k_eo_fold_cross", n * 48, qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p));
   std::swap(wit_, wit2_);
   std::swap(qv_, qv2_);
   eo_len_ = n / 2;
@@ -688,6 +701,351 @@ std::array<F, 2> GpuBackend::eo_terminal() {
   QF_CK(cudaMemcpyAsync(&q0, qv_.p, 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
   return {w0, q0};
+}
+
+
+// ---------------------------------------------------------------- top round / Decide on device
+const Fe* GpuBackend::level_alpha(size_t level, int which) {
+  auto& v = level_alpha_[which];
+  if (v.size() <= level) v.resize(level + 1);
+  if (!v[level].p) {
+    const auto& a = P_.pcs.pp->seq.codes[level].alphas[which];
+    v[level].alloc(a.size());
+    QF_CK(cudaMemcpyAsync(v[level].p, a.data(), a.size() * 16, cudaMemcpyHostToDevice, s_));
+  }
+  return v[level].p;
+}
+
+// MSB-first monomial tensor weights (tensor_weights, qafold_short_pc.rs:2826-2855):
+// the last <= 10 coordinates index a low table, the rest a high table.
+void GpuBackend::tensor_table(const std::vector<F>& point, DBuf<Fe>& out) {
+  const int n = int(point.size());
+  const int lb = std::min(10, n);
+  std::vector<F> hi = tensor_weights(std::vector<F>(point.begin(), point.begin() + (n - lb)));
+  std::vector<F> lo = tensor_weights(std::vector<F>(point.begin() + (n - lb), point.end()));
+  DBuf<Fe> dhi(hi.size()), dlo(lo.size());
+  QF_CK(cudaMemcpyAsync(dhi.p, hi.data(), hi.size() * 16, cudaMemcpyHostToDevice, s_));
+  QF_CK(cudaMemcpyAsync(dlo.p, lo.data(), lo.size() * 16, cudaMemcpyHostToDevice, s_));
+  const uint64_t m = uint64_t(1) << n;
+  if (out.n != m) out.alloc(m);
+  QF_LAUNCH(s_, "k_table", m * 16, qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, out.p));
+  QF_CK(cudaStreamSynchronize(s_));
+}
+
+// Unnormalised WHT of a device vector of 2^logn entries, optionally
+// multiplying by alpha first (one tile pass, then strided passes).
+void GpuBackend::wht_dev(Fe* v, int logn, const Fe* alpha) {
+  const int wl = std::min(12, logn);
+  const size_t tsmem = size_t(16) << wl;
+  set_smem(qfd::k_wht_tile, tsmem);
+  QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logn) * 16,
+            qfd::k_wht_tile<<<unsigned(size_t(1) << (logn - wl)), kThreads, tsmem, s_>>>(v, v, alpha, logn, wl));
+  for (int lo = wl; lo < logn;) {
+    int k = std::min(9, logn - lo);
+    size_t smem = size_t(8) << k << 4;
+    set_smem(qfd::k_butterfly_strided<qfd::kWht>, smem);
+    QF_LAUNCH(s_, "k_butterfly_strided", (uint64_t(2) << logn) * 16,
+              qfd::k_butterfly_strided<qfd::kWht><<<unsigned((size_t(1) << (logn - k)) / 8), kThreads, smem, s_>>>(v, logn, lo, k));
+    lo += k;
+  }
+}
+
+F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {
+  const int g = grid_for(n, kThreads);
+  QF_LAUNCH(s_, "k_dot", n * 32, qfd::k_dot<<<g, kThreads, 0, s_>>>(a, b, n, partials_.p));
+  return reduce_to_host(partials_, g, 1)[0];
+}
+
+std::array<F, 2> GpuBackend::lb_cross(const Fe* L, const Fe* R, uint64_t n) {
+  const int g = grid_for(std::max<uint64_t>(n / 2, 1), kThreads);
+  QF_LAUNCH(s_, "k_lb_cross", n * 32, qfd::k_lb_cross<<<g, kThreads, 0, s_>>>(L, R, n, partials_.p));
+  std::vector<F> r = reduce_to_host(partials_, g, 2);
+  return {r[0], r[1]};
+}
+
+// prove_litebullet (qafold_short_pc.rs:1895-1940) on device vectors; with
+// check_and_absorb = false it is the MultiEval row phase (no claim check, no
+// domain label) and `claimed` is the running right-hand side.
+LiteBullet<F> GpuBackend::litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, PcsTranscript<F>& t, const char* label,
+                                         const char* fold_label, bool check_and_absorb) {
+  if (check_and_absorb) {
+    if (n == 0 || !is_pow2(n) || dot_dev(L, R, n) != claimed) fail(QF_E_INVALID_COMMITMENT, "litebullet claim");
+    t.absorb_str("litebullet-domain", label);
+  }
+  F rhs = claimed;
+  LiteBullet<F> out;
+  std::array<F, 2> cr{F::zero(), F::zero()};
+  if (n > 1) cr = lb_cross(L, R, n);
+  while (n > 1) {
+    t.push_response(cr[0]);
+    t.push_response(cr[1]);
+    F ch = t.challenge_nonzero(fold_label);
+    F inv = ch.inverse();
+    rhs += cr[0] * ch + cr[1] * inv;
+    const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
+    QF_LAUNCH(s_, "k_lb_fold_cross", n * 48,
+              qfd::k_lb_fold_cross<<<g, kThreads, 0, s_>>>(L, R, n, to_fe(inv), to_fe(ch), partials_.p));
+    n /= 2;
+    if (n > 1) {
+      std::vector<F> r = reduce_to_host(partials_, g, 2);
+      cr = {r[0], r[1]};
+    }
+    out.a_point.push_back(inv);
+    out.b_point.push_back(ch);
+  }
+  QF_CK(cudaMemcpyAsync(&out.a_value, L, 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaMemcpyAsync(&out.b_value, R, 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  t.push_response(out.a_value);
+  t.push_response(out.b_value);
+  if (check_and_absorb && out.a_value * out.b_value != rhs) fail(QF_E_INVALID_COMMITMENT, "litebullet terminal");
+  lb_rhs_ = rhs;
+  return out;
+}
+
+// Row projection of the systematic half at tensor_weights(point[col_log..]),
+// keeping the row weights in HBM for the top round.
+std::vector<F> GpuBackend::open_top(const DeviceCodeword& cw, const std::vector<F>& point, size_t col_log) {
+  open_cw_ = &cw;
+  const uint64_t n_rows = cw.n_ext / 2;
+  tensor_table(std::vector<F>(point.begin() + col_log, point.end()), rw_d_);
+  if (rw_d_.n != n_rows) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "top row weights");
+  F one = F::one();
+  DBuf<Fe> hi(1);
+  QF_CK(cudaMemcpyAsync(hi.p, &one, 16, cudaMemcpyHostToDevice, s_));
+  const int chunks = int(std::min<uint64_t>(64, (n_rows + kThreads - 1) / kThreads));
+  DBuf<Fe> part(cw.n_cols * chunks);
+  dim3 grid(chunks, unsigned(cw.n_cols));
+  QF_LAUNCH(s_, "k_row_project", n_rows * cw.n_cols * 16 + n_rows * 16,
+            qfd::k_row_project<<<grid, kThreads, 0, s_>>>(cw.cw.p, cw.n_ext, n_rows, hi.p, rw_d_.p, ilog2(n_rows), part.p));
+  std::vector<F> hp(cw.n_cols * chunks);
+  QF_CK(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  std::vector<F> out(cw.n_cols, F::zero());
+  for (size_t c = 0; c < cw.n_cols; ++c)
+    for (int k = 0; k < chunks; ++k) out[c] += hp[c * chunks + k];
+  return out;
+}
+
+// prove_base_round_with_next_layer + prove_round_reductions
+// (qafold_short_pc.rs:1120-1280, 1454-1527) with the vectors in HBM.
+RoundOutput<F> GpuBackend::prove_top_round(const PcsParams<F>& pp, size_t level, const std::vector<F>& point,
+                                           const std::vector<F>& opening, PcsTranscript<F>& t) {
+  if (!open_cw_) fail(QF_E_ENCODING, "top round without an opened codeword");
+  const DeviceCodeword& cw = *open_cw_;
+  const QaCode<F>& code = pp.seq.codes[level];
+  const QaCode<F>* next = level > 0 ? &pp.seq.codes[level - 1] : nullptr;
+  const uint64_t n_rows = code.message_len, n_ext = cw.n_ext;
+  const size_t n_cols = cw.n_cols, col_log = ilog2(n_cols);
+  const int logR = ilog2(n_rows);
+  if (n_ext != 2 * n_rows || rw_d_.n != n_rows || point.size() != col_log + size_t(logR))
+    fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "top round dims");
+  t.absorb_digest("round-root", cw.root());
+  for (const F& o : opening) t.push_response(o);
+  std::vector<F> freivalds;
+  for (size_t i = 0; i < n_cols; ++i) freivalds.push_back(t.challenge_ext("freivalds"));
+  F fv = inner_product(opening, freivalds);
+  DBuf<Fe> folded(n_rows), dfw(n_cols);
+  QF_CK(cudaMemcpyAsync(dfw.p, freivalds.data(), n_cols * 16, cudaMemcpyHostToDevice, s_));
+  QF_LAUNCH(s_, "k_row_fold", n_rows * n_cols * 16 + n_rows * 16,
+            qfd::k_row_fold<<<grid_for(n_rows, kThreads), kThreads, 0, s_>>>(cw.cw.p, n_ext, n_rows, int(n_cols), dfw.p, folded.p));
+  RoundOutput<F> out;
+  if (next) {
+    // The folded vector is the next level's column-major message.
+    const uint64_t rn = next->message_len;
+    auto ncw = alloc_codeword(rn, n_cols, s_);
+    QF_LAUNCH(s_, "k_to_message_halves", n_rows * 32,
+              qfd::k_to_message_halves<<<grid_for(n_rows, kThreads), kThreads, 0, s_>>>(folded.p, n_rows, ilog2(rn), ncw->cw.p));
+    encode_and_hash(*ncw, level_alpha(level - 1, 1), ilog2(rn), logR, true);
+    absorb_next_layer(t, true, ncw->root());
+    out.next_cw = std::move(ncw);
+  } else {
+    std::vector<F> term(n_rows);
+    QF_CK(cudaMemcpyAsync(term.data(), folded.p, n_rows * 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaStreamSynchronize(s_));
+    absorb_next_layer(t, false, hash_terminal_vector(term));
+    out.terminal = std::move(term);
+  }
+  size_t qc = pp.num_queries(level, n_ext);
+  Digest seed = t.challenge_digest("row-selection");
+  RowSelection sel = make_selection(qc, n_ext, seed);
+  std::vector<F> sampled(sel.size());
+  std::vector<uint64_t> sel_rows;
+  if (sel.all) {
+    std::vector<F> all = cw.entries();
+    for (uint64_t r = 0; r < n_ext; ++r) {
+      F s = F::zero();
+      for (size_t c = 0; c < n_cols; ++c) s += freivalds[c] * all[c * n_ext + r];
+      sampled[r] = s;
+      sel_rows.push_back(r);
+    }
+    out.rows.all = true;
+    out.rows.n_rows = n_ext;
+    out.rows.n_cols = n_cols;
+    out.rows.encoded = std::move(all);
+  } else {
+    auto rws = cw.rows(sel.rows);
+    auto pth = cw.paths(sel.rows);
+    for (size_t i = 0; i < sel.size(); ++i) {
+      RowQuery<F> q;
+      q.row = std::move(rws[i]);
+      q.path.siblings = std::move(pth[i]);
+      F s = F::zero();
+      for (size_t c = 0; c < n_cols; ++c) s += freivalds[c] * q.row[c];
+      sampled[i] = s;
+      out.rows.partial.push_back(std::move(q));
+      sel_rows.push_back(sel.rows[i]);
+    }
+  }
+  t.absorb_exts("sampled-values", sampled);
+  // ---- round reductions
+  size_t sel_log = ilog2(next_pow2(sel.size()));
+  std::vector<F> sel_point;
+  for (size_t i = 0; i < sel_log; ++i) sel_point.push_back(t.challenge_ext("selection-left"));
+  std::vector<F> sw = tensor_weights_prefix(sel_point, sel.size());
+  F selected = inner_product(sw, sampled);
+  DBuf<Fe> pi(n_ext), comb(n_rows), gen_right(n_ext), tw;
+  {
+    DBuf<uint64_t> didx(sel_rows.size());
+    DBuf<Fe> dval(sw.size());
+    QF_CK(cudaMemsetAsync(pi.p, 0, n_ext * 16, s_));
+    QF_CK(cudaMemcpyAsync(didx.p, sel_rows.data(), sel_rows.size() * 8, cudaMemcpyHostToDevice, s_));
+    QF_CK(cudaMemcpyAsync(dval.p, sw.data(), sw.size() * 16, cudaMemcpyHostToDevice, s_));
+    QF_LAUNCH(s_, "k_scatter_set", uint64_t(sw.size()) * 24,
+              qfd::k_scatter_set<<<unsigned((sw.size() + kThreads - 1) / kThreads), kThreads, 0, s_>>>(pi.p, didx.p, dval.p,
+                                                                                                  uint32_t(sw.size())));
+    QF_CK(cudaStreamSynchronize(s_));
+  }
+  // generator_left_projection: WHT(alpha1 * WHT(pi[R..2R))) + pi[0..R)
+  QF_CK(cudaMemcpyAsync(comb.p, pi.p + n_rows, n_rows * 16, cudaMemcpyDeviceToDevice, s_));
+  wht_dev(comb.p, logR, nullptr);
+  wht_dev(comb.p, logR, level_alpha(level, 1));
+  QF_LAUNCH(s_, "k_add", n_rows * 48, qfd::k_add<<<grid_for(n_rows, kThreads), kThreads, 0, s_>>>(comb.p, pi.p, n_rows));
+  F rho = t.challenge_ext("opening-batch");
+  F combined_value = selected + rho * fv;
+  QF_LAUNCH(s_, "k_axpy", n_rows * 48, qfd::k_axpy<<<grid_for(n_rows, kThreads), kThreads, 0, s_>>>(comb.p, rw_d_.p, n_rows, to_fe(rho)));
+  LiteBullet<F> msg = litebullet_dev(combined_value, comb.p, folded.p, n_rows, t, "message-litebullet", "litebullet-fold", true);
+  std::vector<F> pt_rows(point.begin() + col_log, point.end());
+  F ole = tensor_inner_product(pt_rows, msg.a_point);
+  F sle = msg.a_value - rho * ole;
+  // generator_right_projection = encode(tensor_weights(a_point))
+  tensor_table(msg.a_point, tw);
+  QF_CK(cudaMemcpyAsync(gen_right.p, tw.p, n_rows * 16, cudaMemcpyDeviceToDevice, s_));
+  QF_CK(cudaMemcpyAsync(gen_right.p + n_rows, tw.p, n_rows * 16, cudaMemcpyDeviceToDevice, s_));
+  wht_dev(gen_right.p + n_rows, logR, nullptr);
+  wht_dev(gen_right.p + n_rows, logR, level_alpha(level, 1));
+  LiteBullet<F> gen = litebullet_dev(sle, pi.p, gen_right.p, n_ext, t, "generator-litebullet", "litebullet-fold", true);
+  out.reduction = {msg.b_value, msg.b_point, gen.b_value, gen.b_point, msg.a_point};
+  open_cw_ = nullptr;
+  return out;
+}
+
+// MultiEval over one level's alpha columns (qafold_short_decide.rs:466-536)
+// with the row vectors in HBM, followed by the direct-interleaved block fold.
+MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
+                                              size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) {
+  const QaCode<F>& code = pp.seq.codes[level];
+  const uint64_t rows = uint64_t(1) << log_rows;
+  const size_t real = code.alphas.size();
+  if (rows != code.message_len) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "multi-eval rows");
+  validate_multi_eval(claims, real, log_rows, log_cols);
+  absorb_multi_eval_statement(claims, log_rows, log_cols, t);
+  F rho = t.challenge_ext("multi-eval-batch");
+  std::vector<DBuf<Fe>> row_w(claims.size());
+  for (size_t i = 0; i < claims.size(); ++i) tensor_table(claims[i].row_point, row_w[i]);
+  std::vector<const Fe*> col(real);
+  for (size_t sidx = 0; sidx < real; ++sidx) col[sidx] = level_alpha(level, int(sidx));
+  std::vector<std::vector<F>> se(claims.size(), std::vector<F>(real));
+  for (size_t i = 0; i < claims.size(); ++i)
+    for (size_t sidx = 0; sidx < real; ++sidx) se[i][sidx] = dot_dev(row_w[i].p, col[sidx], rows);
+  MultiEvalColumns<F> mc = multi_eval_columns(claims, real, log_cols, rho, se, t);
+  DBuf<Fe> right(rows), folded(rows), left(rows);
+  QF_CK(cudaMemsetAsync(right.p, 0, rows * 16, s_));
+  QF_CK(cudaMemsetAsync(folded.p, 0, rows * 16, s_));
+  for (size_t i = 0; i < claims.size(); ++i)
+    QF_LAUNCH(s_, "k_axpy", rows * 48,
+              qfd::k_axpy<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(right.p, row_w[i].p, rows, to_fe(mc.row_scale[i])));
+  for (const auto& [src, coef] : mc.terms0)
+    QF_LAUNCH(s_, "k_axpy", rows * 48,
+              qfd::k_axpy<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(folded.p, col[src], rows, to_fe(coef)));
+  QF_CK(cudaMemcpyAsync(left.p, folded.p, rows * 16, cudaMemcpyDeviceToDevice, s_));
+  LiteBullet<F> lb = litebullet_dev(mc.rhs, left.p, right.p, rows, t, nullptr, "multi-eval-fold", false);
+  std::vector<F> a_point = mc.a_point, b_point = mc.b_point;
+  a_point.insert(a_point.end(), lb.a_point.begin(), lb.a_point.end());
+  b_point.insert(b_point.end(), lb.b_point.begin(), lb.b_point.end());
+  F ew = expected_weight_eval(claims, mc.powers, log_cols, b_point);
+  MultiEvalOut<F> out;
+  out.ok = (lb.a_value * lb.b_value == lb_rhs_) && (lb.b_value == ew);
+  out.reduced = {lb.a_value, a_point};
+  // Block fold at the first log2(row_factor) coordinates of the merged row point.
+  const int block_log = ilog2(row_factor);
+  if (a_point.size() < log_cols + size_t(block_log)) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "merged point");
+  std::vector<F> bw = tensor_weights(std::vector<F>(a_point.begin() + log_cols, a_point.begin() + log_cols + block_log));
+  const uint64_t trows = rows / row_factor;
+  DBuf<Fe> dbw(row_factor), rec(trows);
+  QF_CK(cudaMemcpyAsync(dbw.p, bw.data(), row_factor * 16, cudaMemcpyHostToDevice, s_));
+  QF_LAUNCH(s_, "k_block_combine", rows * 16 + trows * 16,
+            qfd::k_block_combine<<<grid_for(trows, kThreads), kThreads, 0, s_>>>(folded.p, trows, int(row_factor), dbw.p, rec.p));
+  out.folded_vector.resize(trows);
+  QF_CK(cudaMemcpyAsync(out.folded_vector.data(), rec.p, trows * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return out;
+}
+
+// prove_short_qa_direct_code_switch_carry (qafold_short_decide_carry.rs:940-1027)
+// with the message-length vectors in HBM.
+bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
+                               const std::vector<F>& iota, const std::vector<F>& folded_message, F merged_value,
+                               const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) {
+  const uint64_t n = target.message_len, n_enc = target.codeword_len();
+  if (n < 1024) return false;
+  const int logn = ilog2(n);
+  const size_t block_log = ilog2(row_factor);
+  std::vector<F> base_point(merged_left.begin() + block_log, merged_left.end());
+  if (folded_message.size() != n) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "switch message");
+  F ev;
+  if (!mle_eval(folded_message, base_point, ev) || ev != merged_value) fail(QF_E_INVALID_COMMITMENT, "switch merged value");
+  absorb_direct_switch(t, target, target_level, row_factor, sel, iota, merged_value, merged_left);
+  size_t sel_log = ilog2(next_pow2(sel.size()));
+  std::vector<F> slp;
+  for (size_t i = 0; i < sel_log; ++i) slp.push_back(t.challenge_ext("direct-code-switch-selection-left"));
+  std::vector<F> sl = tensor_weights_prefix(slp, sel.size());
+  F selected = inner_product(sl, iota);
+  std::vector<uint64_t> rows_idx;
+  for (size_t i = 0; i < sel.size(); ++i) rows_idx.push_back(sel.at(i));
+  DBuf<Fe> sparse(n_enc), comb(n), msg_d(n), ml, gr(n_enc), tw;
+  {
+    DBuf<uint64_t> didx(rows_idx.size());
+    DBuf<Fe> dval(sl.size());
+    QF_CK(cudaMemsetAsync(sparse.p, 0, n_enc * 16, s_));
+    QF_CK(cudaMemcpyAsync(didx.p, rows_idx.data(), rows_idx.size() * 8, cudaMemcpyHostToDevice, s_));
+    QF_CK(cudaMemcpyAsync(dval.p, sl.data(), sl.size() * 16, cudaMemcpyHostToDevice, s_));
+    QF_LAUNCH(s_, "k_scatter_set", uint64_t(sl.size()) * 24,
+              qfd::k_scatter_set<<<unsigned((sl.size() + kThreads - 1) / kThreads), kThreads, 0, s_>>>(sparse.p, didx.p, dval.p,
+                                                                                                  uint32_t(sl.size())));
+    QF_CK(cudaStreamSynchronize(s_));
+  }
+  const Fe* alpha = level_alpha(target_level, 1);
+  QF_CK(cudaMemcpyAsync(comb.p, sparse.p + n, n * 16, cudaMemcpyDeviceToDevice, s_));
+  wht_dev(comb.p, logn, nullptr);
+  wht_dev(comb.p, logn, alpha);
+  QF_LAUNCH(s_, "k_add", n * 48, qfd::k_add<<<grid_for(n, kThreads), kThreads, 0, s_>>>(comb.p, sparse.p, n));
+  F rho = t.challenge_ext("direct-code-switch-opening-batch");
+  tensor_table(base_point, ml);
+  F combined = selected + rho * merged_value;
+  QF_LAUNCH(s_, "k_axpy", n * 48, qfd::k_axpy<<<grid_for(n, kThreads), kThreads, 0, s_>>>(comb.p, ml.p, n, to_fe(rho)));
+  QF_CK(cudaMemcpyAsync(msg_d.p, folded_message.data(), n * 16, cudaMemcpyHostToDevice, s_));
+  LiteBullet<F> msg = litebullet_dev(combined, comb.p, msg_d.p, n, t, "decide-direct-carry-message-litebullet", "litebullet-fold", true);
+  F ole = tensor_inner_product(base_point, msg.a_point);
+  F sle = msg.a_value - rho * ole;
+  tensor_table(msg.a_point, tw);
+  QF_CK(cudaMemcpyAsync(gr.p, tw.p, n * 16, cudaMemcpyDeviceToDevice, s_));
+  QF_CK(cudaMemcpyAsync(gr.p + n, tw.p, n * 16, cudaMemcpyDeviceToDevice, s_));
+  wht_dev(gr.p + n, logn, nullptr);
+  wht_dev(gr.p + n, logn, alpha);
+  LiteBullet<F> gen = litebullet_dev(sle, sparse.p, gr.p, n_enc, t, "decide-direct-carry-generator-litebullet", "litebullet-fold", true);
+  out = {MatrixClaim<F>{gen.b_value, gen.b_point, msg.a_point}, EvalWithPoint<F>{msg.b_value, msg.b_point}};
+  return true;
 }
 
 }  // namespace qfg

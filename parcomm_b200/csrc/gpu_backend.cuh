@@ -4,7 +4,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <memory>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "host/protocol.h"
@@ -21,6 +24,34 @@ using qfd::Fe;
     cudaError_t e_ = (x);                                                                     \
     if (e_ != cudaSuccess)                                                                    \
       ::qf::fail(QF_E_CUDA, std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #x); \
+  } while (0)
+
+// Per-kernel device time: when enabled, every launch is bracketed by CUDA
+// events recorded on the launching stream; totals are read after a sync.
+struct KernelClock {
+  struct Rec { const char* name; cudaEvent_t a, b; uint64_t bytes; };
+  struct Scope {
+    cudaStream_t stream;
+    const char* name;
+    uint64_t bytes;  // algorithmic bytes moved by this launch
+    cudaEvent_t a = nullptr, b = nullptr;
+    Scope(cudaStream_t s, const char* n, uint64_t bytes);
+    void done();
+  };
+  static bool enabled;
+  static std::mutex mu;
+  static std::vector<Rec> recs;
+  static std::atomic<uint64_t> launches;
+  static void reset(bool on);
+  static std::string stats_json();
+};
+
+#define QF_LAUNCH(stream, name, bytes, ...)     \
+  do {                                          \
+    ::qfg::KernelClock::Scope qf_scope_(stream, name, bytes); \
+    __VA_ARGS__;                                \
+    QF_CK(cudaGetLastError());                  \
+    qf_scope_.done();                           \
   } while (0)
 
 template <class T>
@@ -54,7 +85,7 @@ inline int grid_for(uint64_t n, int threads, int max_blocks = 148 * 8) {
 }
 
 // Constant hash prefixes computed on the host.
-qfd::LeafPrefix leaf_prefix(size_t n_cols);
+qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain);
 qfd::InnerPrefix inner_prefix();
 
 // A committed codeword in HBM: column-major entries and all Merkle levels.
@@ -76,7 +107,11 @@ struct DeviceCodeword : CodewordView<F> {
   std::vector<F> entries() const override;
 };
 
-class GpuBackend : public Backend<F>, public SingleBackend<F>, public EoBackend<F> {
+class GpuBackend : public Backend<F>,
+                   public SingleBackend<F>,
+                   public EoBackend<F>,
+                   public TopRoundAccel<F>,
+                   public DecideAccel<F> {
  public:
   GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s);
   ~GpuBackend() override;
@@ -98,8 +133,30 @@ class GpuBackend : public Backend<F>, public SingleBackend<F>, public EoBackend<
   std::vector<uint8_t> binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) override;
   const CodewordView<F>& folded_codeword() override { return *folded_; }
   const CodewordView<F>& codeword() override { return *blocks_.at(0); }
-  std::vector<F> folded_row_projection(const std::vector<F>& rw) override { return folded_->project_rows(P_.pcs.pp->top_rows(), rw); }
-  std::vector<F> row_projection(const std::vector<F>& rw) override { return blocks_.at(0)->project_rows(P_.pcs.pp->top_rows(), rw); }
+  std::vector<F> folded_opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
+    return open_top(*folded_, point, col_log);
+  }
+  std::vector<F> opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
+    return open_top(*blocks_.at(0), point, col_log);
+  }
+  TopRoundAccel<F>* top_round_accel() override { return this; }
+  DecideAccel<F>* decide_accel() override { return this; }
+  // Top opening round with the message-length vectors in HBM.
+  RoundOutput<F> prove_top_round(const PcsParams<F>& pp, size_t level, const std::vector<F>& point,
+                                 const std::vector<F>& opening, PcsTranscript<F>& t) override;
+  bool open_round(const CodewordView<F>& cw, size_t n_rows, const std::vector<F>& point, size_t col_log,
+                  std::vector<F>& opening) override {
+    const auto* dc = dynamic_cast<const DeviceCodeword*>(&cw);
+    if (!dc || n_rows < 1024) return false;
+    opening = open_top(*dc, point, col_log);
+    return true;
+  }
+  // First Decide round (alpha columns only) with the row vectors in HBM.
+  MultiEvalOut<F> multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
+                                    size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) override;
+  bool direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
+                     const std::vector<F>& iota, const std::vector<F>& folded_message, F merged_value,
+                     const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) override;
 
   // EO
   void cross_terms(const Query<F>& q, size_t stride, std::vector<F>& pos, std::vector<F>& neg) override;
@@ -113,11 +170,20 @@ class GpuBackend : public Backend<F>, public SingleBackend<F>, public EoBackend<
   // Raw window values of small terms.
   std::vector<int8_t> windows(const std::vector<uint64_t>& starts, size_t stride);
 
-  // Kernel launches performed so far (for reporting).
-  uint64_t launches = 0;
 
  private:
-  void encode_and_hash(DeviceCodeword& out);
+  // Encode the message halves of `out` with alpha (parity = WHT(alpha * WHT(msg)))
+  // and build its row tree with the base- or extension-row leaf domain.
+  void encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain);
+  std::vector<F> open_top(const DeviceCodeword& cw, const std::vector<F>& point, size_t col_log);
+  void tensor_table(const std::vector<F>& point, DBuf<Fe>& out);
+  void wht_dev(Fe* v, int logn, const Fe* alpha);
+  F dot_dev(const Fe* a, const Fe* b, uint64_t n);
+  std::array<F, 2> lb_cross(const Fe* L, const Fe* R, uint64_t n);
+  // LiteBullet (or MultiEval row rounds) on device vectors, folded in place.
+  LiteBullet<F> litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, PcsTranscript<F>& t, const char* label,
+                               const char* fold_label, bool check_and_absorb);
+  const Fe* level_alpha(size_t level, int which);
   void mobius_rest(Fe* cw, int logm, int logR, int from);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
   void ensure_alpha();
@@ -130,6 +196,10 @@ class GpuBackend : public Backend<F>, public SingleBackend<F>, public EoBackend<
   std::vector<Digest> roots_;
   std::unique_ptr<DeviceCodeword> folded_;
   DBuf<Fe> alpha1_;
+  std::vector<DBuf<Fe>> level_alpha_[2];  // device copies of alphas[0], alphas[1] per level
+  const DeviceCodeword* open_cw_ = nullptr;  // codeword whose top round is being opened
+  DBuf<Fe> rw_d_;                            // its row weights
+  F lb_rhs_;                                 // running claim after the last device LiteBullet
   // opening state
   DBuf<Fe> weights_, values_, tmp_v_, tmp_w_;
   uint64_t sum_len_ = 0;

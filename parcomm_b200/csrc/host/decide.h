@@ -219,42 +219,31 @@ F expected_weight_eval(const std::vector<EvalClaim<F>>& claims, const std::vecto
   return sum;
 }
 
-// `columns` are the real columns (setup alphas first, then the carry column),
-// each of exactly `rows` entries.
+// Column phase of MultiEval (qafold_short_decide.rs:476-505): given the
+// source evaluations se[claim][source], folds the logical columns and the
+// claims' column weights, pushing the cross messages.  Afterwards the folded
+// matrix column is sum(coef * source) over `terms0`, and the row weight vector
+// is sum_i row_scale[i] * tensor_weights(claims[i].row_point).
 template <class F>
-MultiEvalOut<F> prove_multi_eval(const std::vector<EvalClaim<F>>& claims, const std::vector<const std::vector<F>*>& columns,
-                                 size_t log_rows, size_t log_cols, PcsTranscript<F>& t) {
-  const size_t rows = size_t(1) << log_rows, cols = size_t(1) << log_cols;
-  for (const auto& c : claims)
-    if (c.row_point.size() != log_rows || c.col_weight.empty() || c.col_weight.size() > cols)
-      fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "multi-eval claim");
-  const size_t real = columns.size();
-  if (real == 0 || real > cols) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "multi-eval columns");
+struct MultiEvalColumns {
+  F rhs;
+  std::vector<F> powers, row_scale, a_point, b_point;
+  std::vector<std::pair<size_t, F>> terms0;
+};
+template <class F>
+MultiEvalColumns<F> multi_eval_columns(const std::vector<EvalClaim<F>>& claims, size_t real, size_t log_cols, F rho,
+                                       const std::vector<std::vector<F>>& se, PcsTranscript<F>& t) {
+  const size_t cols = size_t(1) << log_cols;
+  MultiEvalColumns<F> out;
+  out.rhs = F::zero();
+  F power = F::one();
+  for (const auto& c : claims) { out.powers.push_back(power); out.rhs += power * c.value; power *= rho; }
   // Column terms: each logical column is a linear combination of sources.
   std::vector<std::vector<std::pair<size_t, F>>> terms(real);
   for (size_t c = 0; c < real; ++c) terms[c].push_back({c, F::one()});
-  absorb_multi_eval_statement(claims, log_rows, log_cols, t);
-  F rho = t.challenge_ext("multi-eval-batch");
-  F rhs = F::zero(), power = F::one();
-  std::vector<F> powers;
-  for (const auto& c : claims) { powers.push_back(power); rhs += power * c.value; power *= rho; }
-  std::vector<std::vector<F>> row_w;
-  for (const auto& c : claims) row_w.push_back(tensor_weights(c.row_point));
-  // source evaluations[claim][source]
-  std::vector<std::vector<F>> se(claims.size(), std::vector<F>(real, F::zero()));
-  for (size_t i = 0; i < claims.size(); ++i)
-#pragma omp parallel for if (rows >= 4096)
-    for (long s = 0; s < long(real); ++s) {
-      F acc = F::zero();
-      const std::vector<F>& col = *columns[s];
-      for (size_t r = 0; r < rows && r < col.size(); ++r) acc += row_w[i][r] * col[r];
-      se[i][s] = acc;
-    }
   std::vector<std::vector<F>> cw;  // column weight state per claim
   for (const auto& c : claims) cw.push_back(c.col_weight);
   size_t logical = cols;
-  MultiEvalOut<F> out;
-  std::vector<F> a_point, b_point;
   auto eval_at = [&](size_t column, size_t claim) {
     F s = F::zero();
     if (column < terms.size())
@@ -262,7 +251,7 @@ MultiEvalOut<F> prove_multi_eval(const std::vector<EvalClaim<F>>& claims, const 
     return s;
   };
   auto wval = [&](size_t claim, size_t column) {
-    return column < cw[claim].size() ? powers[claim] * cw[claim][column] : F::zero();
+    return column < cw[claim].size() ? out.powers[claim] * cw[claim][column] : F::zero();
   };
   for (size_t k = 0; k < log_cols; ++k) {
     size_t half = logical / 2;
@@ -277,7 +266,7 @@ MultiEvalOut<F> prove_multi_eval(const std::vector<EvalClaim<F>>& claims, const 
     t.push_response(rc);
     F ch = t.challenge_nonzero("multi-eval-fold");
     F inv = ch.inverse();
-    rhs += lc * ch + rc * inv;
+    out.rhs += lc * ch + rc * inv;
     // matrix.fold_columns(inv)
     {
       std::vector<std::vector<std::pair<size_t, F>>> upper;
@@ -297,21 +286,59 @@ MultiEvalOut<F> prove_multi_eval(const std::vector<EvalClaim<F>>& claims, const 
       }
     }
     logical = half;
-    a_point.push_back(inv);
-    b_point.push_back(ch);
+    out.a_point.push_back(inv);
+    out.b_point.push_back(ch);
   }
+  for (size_t i = 0; i < claims.size(); ++i) out.row_scale.push_back(out.powers[i] * cw[i][0]);
+  if (!terms.empty()) out.terms0 = terms[0];
+  return out;
+}
+
+template <class F>
+void validate_multi_eval(const std::vector<EvalClaim<F>>& claims, size_t real, size_t log_rows, size_t log_cols) {
+  const size_t cols = size_t(1) << log_cols;
+  for (const auto& c : claims)
+    if (c.row_point.size() != log_rows || c.col_weight.empty() || c.col_weight.size() > cols)
+      fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "multi-eval claim");
+  if (claims.empty() || real == 0 || real > cols) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "multi-eval columns");
+}
+
+// `columns` are the real columns (setup alphas first, then the carry column),
+// each of exactly `rows` entries (prove_multi_eval, qafold_short_decide.rs:466-536).
+template <class F>
+MultiEvalOut<F> prove_multi_eval(const std::vector<EvalClaim<F>>& claims, const std::vector<const std::vector<F>*>& columns,
+                                 size_t log_rows, size_t log_cols, PcsTranscript<F>& t) {
+  const size_t rows = size_t(1) << log_rows;
+  const size_t real = columns.size();
+  validate_multi_eval(claims, real, log_rows, log_cols);
+  absorb_multi_eval_statement(claims, log_rows, log_cols, t);
+  F rho = t.challenge_ext("multi-eval-batch");
+  std::vector<std::vector<F>> row_w;
+  for (const auto& c : claims) row_w.push_back(tensor_weights(c.row_point));
+  // source evaluations[claim][source]
+  std::vector<std::vector<F>> se(claims.size(), std::vector<F>(real, F::zero()));
+  for (size_t i = 0; i < claims.size(); ++i)
+#pragma omp parallel for if (rows >= 4096)
+    for (long s = 0; s < long(real); ++s) {
+      F acc = F::zero();
+      const std::vector<F>& col = *columns[s];
+      for (size_t r = 0; r < rows && r < col.size(); ++r) acc += row_w[i][r] * col[r];
+      se[i][s] = acc;
+    }
+  MultiEvalColumns<F> mc = multi_eval_columns(claims, real, log_cols, rho, se, t);
+  F rhs = mc.rhs;
+  std::vector<F> a_point = mc.a_point, b_point = mc.b_point;
   std::vector<F> right(rows, F::zero());
   for (size_t i = 0; i < claims.size(); ++i) {
-    F scale = powers[i] * cw[i][0];
+    F scale = mc.row_scale[i];
 #pragma omp parallel for if (rows >= 4096)
     for (long r = 0; r < long(rows); ++r) right[r] += scale * row_w[i][r];
   }
   std::vector<F> folded(rows, F::zero());
-  const auto& t0 = terms.empty() ? std::vector<std::pair<size_t, F>>() : terms[0];
 #pragma omp parallel for if (rows >= 4096)
   for (long r = 0; r < long(rows); ++r) {
     F s = F::zero();
-    for (const auto& [src, coef] : t0) {
+    for (const auto& [src, coef] : mc.terms0) {
       const std::vector<F>& col = *columns[src];
       if (size_t(r) < col.size()) s += col[r] * coef;
     }
@@ -336,7 +363,8 @@ MultiEvalOut<F> prove_multi_eval(const std::vector<EvalClaim<F>>& claims, const 
   F a = left[0], b = right[0];
   t.push_response(a);
   t.push_response(b);
-  F ew = expected_weight_eval(claims, powers, log_cols, b_point);
+  F ew = expected_weight_eval(claims, mc.powers, log_cols, b_point);
+  MultiEvalOut<F> out;
   out.ok = (a * b == rhs) && (b == ew);
   out.reduced = {a, a_point};
   out.folded_vector = std::move(folded);
@@ -657,8 +685,27 @@ std::optional<SwitchCarry<F>> verify_direct_switch(const QaCode<F>& target, size
 }
 
 // ------------------------------------------------------------ prove / verify
+// Runs a MultiEval whose columns are exactly one level's alpha columns (the
+// first Decide round, which has no carry) with the row vectors on a device.
+// Same transcript as prove_multi_eval; `folded_vector` is returned already
+// block-folded at the reduced point's first log2(row_factor) coordinates
+// (fold_short_direct_interleaved_witness), i.e. rows / row_factor entries.
 template <class F>
-DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red) {
+struct DecideAccel {
+  virtual ~DecideAccel() {}
+  virtual MultiEvalOut<F> multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
+                                            size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) = 0;
+  // prove_direct_switch with its message-length vectors on the device;
+  // returns false to keep the (small) switch on the host.
+  virtual bool direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
+                             const std::vector<F>& iota, const std::vector<F>& folded_message, F merged_value,
+                             const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) {
+    return false;
+  }
+};
+
+template <class F>
+DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, DecideAccel<F>* accel = nullptr) {
   const size_t L = pp.levels();
   PcsTranscript<F> t;
   auto h = prepare_pending_h(pp, red, t);
@@ -685,7 +732,9 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red) {
     std::vector<const std::vector<F>*> cols;
     for (const auto& a : code.alphas) cols.push_back(&a);
     if (carry) cols.push_back(&carry->message);
-    MultiEvalOut<F> me = prove_multi_eval(claims, cols, ps.log_rows, ps.log_cols, t);
+    const bool on_device = accel && !carry;
+    MultiEvalOut<F> me = on_device ? accel->multi_eval_alphas(pp, level, claims, ps.log_rows, ps.log_cols, pp.seq.switch_ratio, t)
+                                   : prove_multi_eval(claims, cols, ps.log_rows, ps.log_cols, t);
     if (!me.ok || me.reduced.point.size() != ps.log_cols + ps.log_rows) fail(QF_E_INVALID_COMMITMENT, "multi-eval");
     std::vector<F> col_point(me.reduced.point.begin(), me.reduced.point.begin() + ps.log_cols);
     std::vector<F> merged_left(me.reduced.point.begin() + ps.log_cols, me.reduced.point.end());
@@ -708,13 +757,19 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red) {
     for (const F& v : iota) t.push_response(v);
     // Fold the block coordinate of the logical witness.
     const size_t trows = target.message_len;
-    std::vector<F> bw = tensor_weights(std::vector<F>(merged_left.begin(), merged_left.begin() + ilog2(rf)));
-    std::vector<F> recursive(trows, F::zero());
-    for (size_t r = 0; r < trows; ++r) {
-      F s = F::zero();
-      for (size_t b = 0; b < rf; ++b) s += me.folded_vector[b * trows + r] * bw[b];
-      recursive[r] = s;
+    std::vector<F> recursive;
+    if (on_device) {
+      recursive = std::move(me.folded_vector);
+    } else {
+      std::vector<F> bw = tensor_weights(std::vector<F>(merged_left.begin(), merged_left.begin() + ilog2(rf)));
+      recursive.assign(trows, F::zero());
+      for (size_t r = 0; r < trows; ++r) {
+        F s = F::zero();
+        for (size_t b = 0; b < rf; ++b) s += me.folded_vector[b * trows + r] * bw[b];
+        recursive[r] = s;
+      }
     }
+    if (recursive.size() != trows) fail(QF_E_ENCODING, "recursive witness length");
     std::unique_ptr<Carry<F>> next_carry;
     std::optional<Digest> next_root;
     std::vector<F> terminal;
@@ -730,7 +785,9 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red) {
     }
     absorb_next_carry(t, next_root);
     const std::vector<F>& folded_for_switch = next_carry ? next_carry->message : terminal;
-    SwitchCarry<F> sc = prove_direct_switch(target, level - 1, rf, sel, iota, folded_for_switch, me.reduced.value, merged_left, t);
+    SwitchCarry<F> sc;
+    if (!(accel && accel->direct_switch(target, level - 1, rf, sel, iota, folded_for_switch, me.reduced.value, merged_left, t, sc)))
+      sc = prove_direct_switch(target, level - 1, rf, sel, iota, folded_for_switch, me.reduced.value, merged_left, t);
     if (level > 1) {
       h[level - 1].push_back(reduce_generator_claim(target.message_len, target.index, sc.generator_claim));
       w_claim = sc.folded_w;

@@ -165,8 +165,13 @@ struct Backend {
   virtual std::vector<uint8_t> binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) = 0;
   // The folded codeword, for the native opening.
   virtual const CodewordView<F>& folded_codeword() = 0;
-  // Top row projection of the folded codeword at a row-weight vector.
-  virtual std::vector<F> folded_row_projection(const std::vector<F>& row_weights) = 0;
+  // Top row projection of the folded codeword at tensor_weights(point[col_log..]);
+  // a host backend also returns that row-weight vector in `row_weights`.
+  virtual std::vector<F> folded_opening(const std::vector<F>& point, size_t col_log, std::vector<F>& row_weights) = 0;
+  // Device execution of the folded codeword's top opening round, if any.
+  virtual TopRoundAccel<F>* top_round_accel() { return nullptr; }
+  // Device execution of the first Decide round, if any.
+  virtual DecideAccel<F>* decide_accel() { return nullptr; }
 };
 
 // ------------------------------------------------------------ packed PCS
@@ -311,14 +316,14 @@ BatchOpening<F> open_batch(const PackedPcs<F>& pcs, Backend<F>& be, const std::v
   t0 = std::chrono::steady_clock::now();
   const CodewordView<F>& folded = be.folded_codeword();
   const size_t col_log = ilog2(pcs.pp->extension_columns);
-  std::vector<F> rw = tensor_weights(std::vector<F>(reduced.begin() + col_log, reduced.end()));
-  std::vector<F> opening_vec = be.folded_row_projection(rw);
+  std::vector<F> rw;
+  std::vector<F> opening_vec = be.folded_opening(reduced, col_log, rw);
   F actual = inner_product(opening_vec, tensor_weights(std::vector<F>(reduced.begin(), reduced.begin() + col_log)));
-  OpenResult<F> op = open_with_reduction(*pcs.pp, folded, reduced, opening_vec, actual, rw);
+  OpenResult<F> op = open_with_reduction(*pcs.pp, folded, reduced, opening_vec, actual, rw, be.top_round_accel());
   if (op.claimed != final_value || !op.reduction.ok) fail(QF_E_INVALID_COMMITMENT, "native opening value");
   out.times.native_opening_ms = ms_since(t0);
   t0 = std::chrono::steady_clock::now();
-  DecideProof<F> dp = prove_decide(*pcs.pp, op.reduction);
+  DecideProof<F> dp = prove_decide(*pcs.pp, op.reduction, be.decide_accel());
   out.times.decide_ms = ms_since(t0);
   ByteWriter w;
   w.bytes("QAPKBAT1", 8);
@@ -472,7 +477,9 @@ struct SingleBackend {
   virtual F sumcheck_final_value() = 0;
   virtual F sumcheck_final_weight() = 0;
   virtual const CodewordView<F>& codeword() = 0;
-  virtual std::vector<F> row_projection(const std::vector<F>& row_weights) = 0;
+  virtual std::vector<F> opening(const std::vector<F>& point, size_t col_log, std::vector<F>& row_weights) = 0;
+  virtual TopRoundAccel<F>* top_round_accel() { return nullptr; }
+  virtual DecideAccel<F>* decide_accel() { return nullptr; }
 };
 
 // PackedPcs::open (packed.rs:294-393).
@@ -520,14 +527,14 @@ BatchOpening<F> open_single(const PackedPcs<F>& pcs, SingleBackend<F>& be, const
   t0 = std::chrono::steady_clock::now();
   const CodewordView<F>& cw = be.codeword();
   const size_t col_log = ilog2(pcs.pp->extension_columns);
-  std::vector<F> rw = tensor_weights(std::vector<F>(reduced.begin() + col_log, reduced.end()));
-  std::vector<F> opening_vec = be.row_projection(rw);
+  std::vector<F> rw;
+  std::vector<F> opening_vec = be.opening(reduced, col_log, rw);
   F actual = inner_product(opening_vec, tensor_weights(std::vector<F>(reduced.begin(), reduced.begin() + col_log)));
-  OpenResult<F> op = open_with_reduction(*pcs.pp, cw, reduced, opening_vec, actual, rw);
+  OpenResult<F> op = open_with_reduction(*pcs.pp, cw, reduced, opening_vec, actual, rw, be.top_round_accel());
   if (op.claimed != final_value || !op.reduction.ok) fail(QF_E_INVALID_COMMITMENT, "native opening value");
   out.times.native_opening_ms = ms_since(t0);
   t0 = std::chrono::steady_clock::now();
-  DecideProof<F> dp = prove_decide(*pcs.pp, op.reduction);
+  DecideProof<F> dp = prove_decide(*pcs.pp, op.reduction, be.decide_accel());
   out.times.decide_ms = ms_since(t0);
   ByteWriter w;
   w.bytes(F::kPackedMagic, 8);

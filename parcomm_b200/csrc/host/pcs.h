@@ -663,7 +663,25 @@ struct RoundOutput {
   Rows<F> rows;
   std::optional<std::vector<F>> terminal;
   VerifiedRound<F> reduction;
-  std::unique_ptr<Codeword<F>> next_cw;
+  std::unique_ptr<CodewordView<F>> next_cw;
+};
+
+// Runs the top opening round with its message-length vectors (the Freivalds
+// fold, the next-level commitment, the generator projections and both
+// LiteBullets) resident on a device.  Same transcript and outputs as
+// prove_round; `opening` is the top row projection.
+template <class F>
+struct TopRoundAccel {
+  virtual ~TopRoundAccel() {}
+  virtual RoundOutput<F> prove_top_round(const PcsParams<F>& pp, size_t level, const std::vector<F>& point,
+                                         const std::vector<F>& opening, PcsTranscript<F>& t) = 0;
+  // For a codeword produced by this accelerator: computes the extension
+  // round's opening vector on the device and returns true, after which
+  // prove_top_round runs the round; false keeps the round on the host.
+  virtual bool open_round(const CodewordView<F>& cw, size_t n_rows, const std::vector<F>& point, size_t col_log,
+                          std::vector<F>& opening) {
+    return false;
+  }
 };
 
 template <class F>
@@ -731,7 +749,8 @@ struct OpenResult {
 // projection (computed by the caller's backend) and `claimed` its value.
 template <class F>
 OpenResult<F> open_with_reduction(const PcsParams<F>& pp, const CodewordView<F>& top, const std::vector<F>& point,
-                                  const std::vector<F>& opening, F claimed, const std::vector<F>& row_weights) {
+                                  const std::vector<F>& opening, F claimed, const std::vector<F>& row_weights,
+                                  TopRoundAccel<F>* accel = nullptr) {
   if (point.size() != size_t(ilog2(pp.n_witness))) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "opening point length");
   PcsTranscript<F> t;
   t.absorb_digest("parameters", pp.parameter_digest);
@@ -741,7 +760,8 @@ OpenResult<F> open_with_reduction(const PcsParams<F>& pp, const CodewordView<F>&
   const size_t L = pp.levels(), top_level = L - 1;
   OpenResult<F> res;
   res.claimed = claimed;
-  RoundOutput<F> r0 = prove_round(pp, top_level, top, point, opening, row_weights, t);
+  RoundOutput<F> r0 = accel ? accel->prove_top_round(pp, top_level, point, opening, t)
+                            : prove_round(pp, top_level, top, point, opening, row_weights, t);
   res.proof.top = std::move(r0.rows);
   if (top_level == 0) {
     if (evaluate_generator_mle(pp.seq.codes[0], r0.reduction.generator_left_point, r0.reduction.generator_right_point) !=
@@ -753,16 +773,21 @@ OpenResult<F> open_with_reduction(const PcsParams<F>& pp, const CodewordView<F>&
   F next_value = r0.reduction.next_value;
   std::vector<F> next_point = r0.reduction.next_point;
   std::optional<std::vector<F>> terminal = std::move(r0.terminal);
-  std::unique_ptr<Codeword<F>> prepared = std::move(r0.next_cw);
+  std::unique_ptr<CodewordView<F>> prepared = std::move(r0.next_cw);
   const size_t col_log = ilog2(pp.extension_columns);
   for (size_t level = top_level; level-- > 0;) {
     if (terminal || !prepared) fail(QF_E_ENCODING, "round sequencing");
     const QaCode<F>& code = pp.seq.codes[level];
-    std::vector<F> rw = tensor_weights(std::vector<F>(next_point.begin() + col_log, next_point.end()));
-    std::vector<F> opening_vec = systematic_row_projection(*prepared, code.message_len, rw);
+    std::vector<F> rw, opening_vec;
+    const bool on_device = accel && accel->open_round(*prepared, code.message_len, next_point, col_log, opening_vec);
+    if (!on_device) {
+      rw = tensor_weights(std::vector<F>(next_point.begin() + col_log, next_point.end()));
+      opening_vec = systematic_row_projection(*prepared, code.message_len, rw);
+    }
     std::vector<F> cw_pt(next_point.begin(), next_point.begin() + col_log);
     if (inner_product(opening_vec, tensor_weights(cw_pt)) != next_value) fail(QF_E_INVALID_COMMITMENT, "extension opening");
-    RoundOutput<F> r = prove_round(pp, level, *prepared, next_point, opening_vec, rw, t);
+    RoundOutput<F> r = on_device ? accel->prove_top_round(pp, level, next_point, opening_vec, t)
+                                 : prove_round(pp, level, *prepared, next_point, opening_vec, rw, t);
     res.proof.ext_rounds.push_back(ExtRound<F>{prepared->root(), std::move(r.rows)});
     if (level == 0) {
       if (evaluate_generator_mle(code, r.reduction.generator_left_point, r.reduction.generator_right_point) !=

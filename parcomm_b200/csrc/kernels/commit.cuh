@@ -104,7 +104,7 @@ __global__ void k_copy_mobius_tile(const Fe* __restrict__ src, Fe* __restrict__ 
 // WHT levels [0, levels) within a tile (levels <= logR so columns never mix).
 // Reads the message (or parity) half at src, optionally multiplies each row by
 // alpha[r] first, writes the parity half.
-__global__ void k_wht_tile(const Fe* __restrict__ src, Fe* __restrict__ dst, const Fe* __restrict__ alpha, int logR,
+__global__ void k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR,
                            int levels) {
   extern __shared__ uint4 smem_u4[];
   Fe* tile = reinterpret_cast<Fe*>(smem_u4);
@@ -162,8 +162,12 @@ constexpr int kLeafThreads = 64;
 constexpr int kRowWords = 128;  // 32 entries x 4 words
 constexpr int kRowStride = 129;  // padded: conflict-free per-thread rows
 
+// TAIL = prefix bytes after the 64-byte midstate: 11 for the 75-byte
+// base-row prefix, 16 for the 80-byte extension-row prefix.
+template <int TAIL>
 __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restrict__ cw, uint64_t n_rows, int n_cols,
                                                               LeafPrefix pre, uint4* __restrict__ leaves) {
+  static_assert(TAIL == 11 || TAIL == 16, "leaf prefix");
   __shared__ uint32_t rows_s[kLeafThreads * kRowStride];
   const uint64_t r = uint64_t(blockIdx.x) * kLeafThreads + threadIdx.x;
   uint32_t* mine = rows_s + threadIdx.x * kRowStride;
@@ -179,8 +183,8 @@ __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restri
   uint32_t h[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) h[i] = pre.mid[i];
-  // Stream after the midstate: 11 prefix bytes then the row; 64-byte blocks.
-  const uint32_t total = 75u + uint32_t(nw) * 4u;
+  // Stream after the midstate: TAIL prefix bytes then the row; 64-byte blocks.
+  const uint32_t total = 64u + TAIL + uint32_t(nw) * 4u;
   const int nblocks = int((total - 64 + 63) / 64);
   for (int j = 1; j <= nblocks; ++j) {
     uint32_t m[16];
@@ -188,9 +192,13 @@ __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restri
     for (int w = 0; w < 16; ++w) {
       const int s = 64 * (j - 1) + 4 * w;
       uint32_t word;
-      if (s < 8) word = pre.tail[w];
-      else if (s == 8) word = pre.tail[2] | (rw(0) << 24);
-      else {
+      if (TAIL == 16) {
+        word = s < 16 ? pre.tail[w] : rw((s - 16) >> 2);
+      } else if (s < 8) {
+        word = pre.tail[w];
+      } else if (s == 8) {
+        word = pre.tail[2] | (rw(0) << 24);
+      } else {
         const int q = (s - 12) >> 2;
         word = (rw(q) >> 8) | (rw(q + 1) << 24);
       }

@@ -11,7 +11,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 def declared_functions():
     text = (ROOT / "include" / "parcomm_qafold.h").read_text()
-    return sorted(set(re.findall(r"^(?:int|void|size_t)\s+(qf_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^(?:int|void|size_t|uint64_t)\s+(qf_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_reference_entry_points():
