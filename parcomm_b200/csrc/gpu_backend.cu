@@ -10,7 +10,53 @@ namespace qfg {
 
 static constexpr int kThreads = 256;
 
+namespace {
+std::mutex g_pool_mu;
+std::multimap<size_t, void*> g_pool;  // rounded bytes -> free device block
+}  // namespace
+
+void* DevicePool::get(size_t bytes) {
+  const size_t r = rounded(bytes);
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    auto it = g_pool.find(r);
+    if (it != g_pool.end()) {
+      void* p = it->second;
+      g_pool.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, r) != cudaSuccess) {
+    cudaGetLastError();
+    trim();
+    QF_CK(cudaMalloc(&p, r));
+  }
+  return p;
+}
+void DevicePool::put(void* p, size_t bytes) {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  g_pool.emplace(rounded(bytes), p);
+}
+void DevicePool::trim() {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  cudaDeviceSynchronize();
+  for (auto& [b, p] : g_pool) cudaFree(p);
+  g_pool.clear();
+}
+
 bool KernelClock::enabled = false;
+namespace {
+std::map<std::string, std::pair<uint64_t, double>> g_host_sections;
+}
+HostScope::~HostScope() {
+  if (!KernelClock::enabled) return;
+  double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  std::lock_guard<std::mutex> g(KernelClock::mu);
+  auto& e = g_host_sections[name];
+  e.first += 1;
+  e.second += ms;
+}
 std::mutex KernelClock::mu;
 std::vector<KernelClock::Rec> KernelClock::recs;
 std::atomic<uint64_t> KernelClock::launches{0};
@@ -34,6 +80,7 @@ void KernelClock::reset(bool on) {
   std::lock_guard<std::mutex> g(mu);
   for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   recs.clear();
+  g_host_sections.clear();
   enabled = on;
 }
 std::string KernelClock::stats_json() {
@@ -57,6 +104,14 @@ std::string KernelClock::stats_json() {
     char buf[256];
     std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu}", k.c_str(),
                   (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
+    s += buf;
+  }
+  for (auto& [k, v] : g_host_sections) {
+    if (!first) s += ",";
+    first = false;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "\"host:%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0}", k.c_str(),
+                  (unsigned long long)v.first, v.second);
     s += buf;
   }
   return s + "}";
@@ -270,6 +325,7 @@ static std::unique_ptr<DeviceCodeword> alloc_codeword(size_t R, size_t cols, cud
 }
 
 Digest GpuBackend::commit_block(size_t b) {
+  HostScope hs("commit_block");
   const int logm = ilog2(P_.pcs.packed_len());
   const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
   // The implicit zero suffix repeats one codeword; reuse its root and state.
@@ -498,6 +554,7 @@ std::vector<int8_t> GpuBackend::windows(const std::vector<uint64_t>& starts, siz
 // Lane projections (tbv.rs:288-352) of large terms: two-level weight tables
 // per term, one tile per high-table entry.
 std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Term<F>*>& terms, size_t stride) {
+  HostScope hs("project_terms");
   std::vector<std::vector<F>> out(terms.size());
   std::vector<qfd::ProjTile> tiles;
   std::vector<F> lo_all;
@@ -558,6 +615,7 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
 }
 
 void GpuBackend::cross_terms(const Query<F>& q, size_t stride, std::vector<F>& pos, std::vector<F>& neg) {
+  HostScope hs("eo_cross_terms");
   pos.assign(stride - 1, F::zero());
   neg.assign(stride - 1, F::zero());
   std::vector<const Term<F>*> big, small;
@@ -589,6 +647,7 @@ void GpuBackend::cross_terms(const Query<F>& q, size_t stride, std::vector<F>& p
 }
 
 F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t stride) {
+  HostScope hs("eo_build");
   const uint64_t rows = logical / stride;
   eo_len_ = rows;
   wit_.alloc(rows);
@@ -682,6 +741,7 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
 }
 
 void GpuBackend::eo_round_fold(F inv, F ch) {
+  HostScope hs("eo_round_fold");
   const uint64_t n = eo_len_;
   if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
   const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
@@ -831,6 +891,7 @@ std::vector<F> GpuBackend::open_top(const DeviceCodeword& cw, const std::vector<
 // (qafold_short_pc.rs:1120-1280, 1454-1527) with the vectors in HBM.
 RoundOutput<F> GpuBackend::prove_top_round(const PcsParams<F>& pp, size_t level, const std::vector<F>& point,
                                            const std::vector<F>& opening, PcsTranscript<F>& t) {
+  HostScope hs("opening_round");
   if (!open_cw_) fail(QF_E_ENCODING, "top round without an opened codeword");
   const DeviceCodeword& cw = *open_cw_;
   const QaCode<F>& code = pp.seq.codes[level];
@@ -944,6 +1005,7 @@ RoundOutput<F> GpuBackend::prove_top_round(const PcsParams<F>& pp, size_t level,
 // with the row vectors in HBM, followed by the direct-interleaved block fold.
 MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
                                               size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) {
+  HostScope hs("decide_multi_eval");
   const QaCode<F>& code = pp.seq.codes[level];
   const uint64_t rows = uint64_t(1) << log_rows;
   const size_t real = code.alphas.size();
@@ -997,6 +1059,7 @@ MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t lev
 bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
                                const std::vector<F>& iota, const std::vector<F>& folded_message, F merged_value,
                                const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) {
+  HostScope hs("decide_switch");
   const uint64_t n = target.message_len, n_enc = target.codeword_len();
   if (n < 1024) return false;
   const int logn = ilog2(n);

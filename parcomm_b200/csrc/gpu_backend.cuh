@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -46,6 +48,14 @@ struct KernelClock {
   static std::string stats_json();
 };
 
+// Host wall time of named sections (recorded while KernelClock is enabled).
+struct HostScope {
+  const char* name;
+  std::chrono::steady_clock::time_point t0;
+  explicit HostScope(const char* n) : name(n), t0(std::chrono::steady_clock::now()) {}
+  ~HostScope();
+};
+
 #define QF_LAUNCH(stream, name, bytes, ...)     \
   do {                                          \
     ::qfg::KernelClock::Scope qf_scope_(stream, name, bytes); \
@@ -53,6 +63,20 @@ struct KernelClock {
     QF_CK(cudaGetLastError());                  \
     qf_scope_.done();                           \
   } while (0)
+
+// Process-wide cache of device allocations: released buffers are kept, keyed
+// by their rounded size, and handed out again, so repeated commits/openings
+// of the same shapes pay no cudaMalloc/cudaFree.  A failed cudaMalloc first
+// returns the cache to the driver and retries.
+struct DevicePool {
+  static void* get(size_t bytes);
+  static void put(void* p, size_t bytes);
+  static void trim();
+  static size_t rounded(size_t bytes) {
+    const size_t g = bytes >= (size_t(1) << 20) ? (size_t(1) << 20) : 256;
+    return (bytes + g - 1) / g * g;
+  }
+};
 
 template <class T>
 struct DBuf {
@@ -67,10 +91,14 @@ struct DBuf {
   ~DBuf() { reset(); }
   void alloc(size_t count) {
     reset();
-    if (count) QF_CK(cudaMalloc(&p, count * sizeof(T)));
+    if (count) p = static_cast<T*>(DevicePool::get(count * sizeof(T)));
     n = count;
   }
-  void reset() { if (p) cudaFree(p); p = nullptr; n = 0; }
+  void reset() {
+    if (p) DevicePool::put(p, n * sizeof(T));
+    p = nullptr;
+    n = 0;
+  }
 };
 
 inline const Fe* as_fe(const F* p) { return reinterpret_cast<const Fe*>(p); }
