@@ -5,6 +5,8 @@
 #include "kernels/vec.cuh"
 
 #include <map>
+#include <mutex>
+#include <set>
 
 namespace qfg {
 
@@ -240,9 +242,28 @@ std::vector<F> DeviceCodeword::entries() const {
   return h;
 }
 
+// Planar tile kernels take up to 2^kMaxTileLog elements (128 KiB of shared
+// memory); the opt-in is set once per device.
+static void configure_tile_kernels() {
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  QF_CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  if (done.count(dev)) return;
+  const size_t bytes = qfd::kTileSmem;
+  set_smem(qfd::k_pack_mobius_tile, bytes);
+  set_smem(qfd::k_copy_mobius_tile, bytes);
+  set_smem(qfd::k_wht_tile, bytes);
+  set_smem(qfd::k_butterfly_strided<qfd::kMobius>, bytes);
+  set_smem(qfd::k_butterfly_strided<qfd::kWht>, bytes);
+  done.insert(dev);
+}
+
 // ---------------------------------------------------------------- backend
 GpuBackend::GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s)
     : P_(p), bva_(d_bva), active_(active), s_(s) {
+  configure_tile_kernels();
   partials_.alloc(148 * 8 * 4);
   result_.alloc(8);
 }
@@ -255,36 +276,37 @@ void GpuBackend::ensure_alpha() {
   QF_CK(cudaMemcpyAsync(alpha1_.p, top.alphas[1].data(), top.message_len * 16, cudaMemcpyHostToDevice, s_));
 }
 
-void GpuBackend::mobius_rest(Fe* cw, int logm, int logR, int from) {
-  for (int lo = from; lo < logm;) {
-    int k = std::min(9, logm - lo);
-    size_t smem = size_t(8) << k << 4;
-    set_smem(qfd::k_butterfly_strided<qfd::kMobius>, smem);
-    QF_LAUNCH(s_, "k_butterfly_strided", (uint64_t(2) << logm) * 16, qfd::k_butterfly_strided<qfd::kMobius><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(cw, logR, lo, k));
+// Butterfly levels [from, to) over a half (message or parity at `base`) of
+// 2^logm entries, in strided passes of at most 10 levels.  `to` is logR for
+// the per-column WHT and logm for the Mobius transform of the whole message.
+template <int OP>
+static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int from, int to) {
+  for (int lo = from; lo < to;) {
+    const int k = std::min(10, to - lo);
+    // 2^cb consecutive group bases per tile: 64-byte runs at k = 10, the
+    // full 4096-element tile below that.
+    const int cb = std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k);
+    const size_t smem = qfd::kTileSmem;
+    QF_LAUNCH(s, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
+              qfd::k_butterfly_strided<OP><<<unsigned(size_t(1) << (logm - k - cb)), qfd::kTileThreads, smem, s>>>(base, logR, lo, k, cb));
     lo += k;
   }
 }
 
+void GpuBackend::mobius_rest(Fe* cw, int logm, int logR, int from) { strided_passes<qfd::kMobius>(s_, cw, logR, logm, from, logm); }
+
 // Parity = WHT(alpha * WHT(message)) per column, then leaf hashes and tree.
 void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain) {
   const size_t R = size_t(1) << logR;
-  const int wl = std::min(12, logR);
-  const size_t tsmem = size_t(16) << wl;
-  set_smem(qfd::k_wht_tile, tsmem);
+  const int wl = std::min(qfd::kMaxTileLog, logR);
+  const size_t tsmem = qfd::kTileSmem;
   Fe* msg = out.cw.p;
   Fe* par = out.cw.p + R;
   for (int pass = 0; pass < 2; ++pass) {
     QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logm) * 16,
-              qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), kThreads, tsmem, s_>>>(pass == 0 ? msg : par, par,
-                                                                                        pass == 0 ? nullptr : alpha, logR, wl));
-    for (int lo = wl; lo < logR;) {
-      int k = std::min(9, logR - lo);
-      size_t smem = size_t(8) << k << 4;
-      set_smem(qfd::k_butterfly_strided<qfd::kWht>, smem);
-      QF_LAUNCH(s_, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
-                qfd::k_butterfly_strided<qfd::kWht><<<unsigned((size_t(1) << (logm - k)) / 8), kThreads, smem, s_>>>(par, logR, lo, k));
-      lo += k;
-    }
+              qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), qfd::kTileThreads, tsmem, s_>>>(
+                  pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, wl));
+    strided_passes<qfd::kWht>(s_, par, logR, logm, wl, logR);
   }
   // Leaves and inner levels.
   const uint64_t n_ext = 2 * R;
@@ -339,10 +361,9 @@ Digest GpuBackend::commit_block(size_t b) {
       }
   }
   auto cw = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
-  const int l0 = std::min(12, logm);
-  const size_t smem = size_t(16) << l0;
-  set_smem(qfd::k_pack_mobius_tile, smem);
-  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
+  const int l0 = std::min(qfd::kMaxTileLog, logm);
+  const size_t smem = qfd::kTileSmem;
+  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
                                                                                     cw->cw.p, logR, l0));
   mobius_rest(cw->cw.p, logm, logR, l0);
   ensure_alpha();
@@ -446,10 +467,9 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   QF_LAUNCH(s_, "k_block_fold", m * (8 * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
                                                                           values_.p));
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
-  const int l0 = std::min(12, logm);
-  const size_t smem = size_t(16) << l0;
-  set_smem(qfd::k_copy_mobius_tile, smem);
-  QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), kThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0));
+  const int l0 = std::min(qfd::kMaxTileLog, logm);
+  const size_t smem = qfd::kTileSmem;
+  QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0));
   mobius_rest(folded_->cw.p, logm, logR, l0);
   ensure_alpha();
   encode_and_hash(*folded_, alpha1_.p, logR, logm, false);
@@ -795,19 +815,10 @@ void GpuBackend::tensor_table(const std::vector<F>& point, DBuf<Fe>& out) {
 // Unnormalised WHT of a device vector of 2^logn entries, optionally
 // multiplying by alpha first (one tile pass, then strided passes).
 void GpuBackend::wht_dev(Fe* v, int logn, const Fe* alpha) {
-  const int wl = std::min(12, logn);
-  const size_t tsmem = size_t(16) << wl;
-  set_smem(qfd::k_wht_tile, tsmem);
+  const int wl = std::min(qfd::kMaxTileLog, logn);
   QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logn) * 16,
-            qfd::k_wht_tile<<<unsigned(size_t(1) << (logn - wl)), kThreads, tsmem, s_>>>(v, v, alpha, logn, wl));
-  for (int lo = wl; lo < logn;) {
-    int k = std::min(9, logn - lo);
-    size_t smem = size_t(8) << k << 4;
-    set_smem(qfd::k_butterfly_strided<qfd::kWht>, smem);
-    QF_LAUNCH(s_, "k_butterfly_strided", (uint64_t(2) << logn) * 16,
-              qfd::k_butterfly_strided<qfd::kWht><<<unsigned((size_t(1) << (logn - k)) / 8), kThreads, smem, s_>>>(v, logn, lo, k));
-    lo += k;
-  }
+            qfd::k_wht_tile<<<unsigned(size_t(1) << (logn - wl)), qfd::kTileThreads, qfd::kTileSmem, s_>>>(v, v, alpha, logn, wl));
+  strided_passes<qfd::kWht>(s_, v, logn, logn, wl, logn);
 }
 
 F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {

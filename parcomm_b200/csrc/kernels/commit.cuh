@@ -27,38 +27,151 @@ __device__ __forceinline__ size_t msg_addr(size_t i, int logR) {
 
 enum ButterflyOp { kMobius = 0, kWht = 1 };
 
-template <int OP>
-__device__ __forceinline__ void butterfly(Fe* lo, Fe* hi) {
-  Fr a = load(lo), b = load(hi);
-  if (OP == kMobius) {
-    store(hi, sub(b, a));
-  } else {
-    store(lo, add(a, b));
-    store(hi, sub(a, b));
-  }
+// ---------------------------------------------------------------- planar tiles
+// A shared-memory tile holds each of the 8 coefficients of its elements in a
+// separate 32-bit plane.  Entry e of a plane sits at e ^ swz(e >> 5), an XOR
+// of its bank bits with a GF(2)-linear image of bits 5..7 (columns 4, 9, 18):
+// every warp access of the butterfly stages below (groups at bit offsets 0,
+// 2 and 3, radix 2..8) and of the load/store loops then hits 32 distinct
+// banks.  Butterflies run in radix-8 register stages on lazily reduced
+// values: a value entering level l of a pass is < 2^l * p, a difference is
+// formed as a + 2^l p - b, so twelve levels stay below 2^28 and one
+// reduction per pass suffices.  Both transforms act coefficient-wise over F_p.
+constexpr int kTileThreads = 512;
+constexpr int kMaxTileLog = 12;                 // 4096 elements per tile
+constexpr int kPlane = 1 << kMaxTileLog;        // plane stride (words)
+constexpr size_t kTileSmem = size_t(8) * kPlane * 4;  // 128 KiB
+__device__ __forceinline__ int pidx(int e) {
+  // byte z of kSwz is swz(z); swz is linear over GF(2), so for index parts
+  // with disjoint bits pidx(x | y) = pidx(x) ^ pidx(y).
+  constexpr uint64_t kSwz = 0x1f1b16120d090400ull;
+  return e ^ int(__byte_perm(uint32_t(kSwz), uint32_t(kSwz >> 32), (e >> 5) & 7) & 31);
 }
 
-// In-shared-memory butterflies over `levels` low levels of a tile of 2^levels
-// consecutive elements.
-template <int OP>
-__device__ __forceinline__ void tile_levels(Fe* tile, int levels) {
-  const int n = 1 << levels;
-  for (int l = 0; l < levels; ++l) {
-    const int half = 1 << l;
-    for (int p = threadIdx.x; p < n / 2; p += blockDim.x) {
-      int lo = ((p >> l) << (l + 1)) | (p & (half - 1));
-      butterfly<OP>(tile + lo, tile + lo + half);
+__device__ __forceinline__ void planar_put_raw(uint32_t* planes, int e, uint4 u) {
+  const int q = pidx(e);
+  planes[0 * kPlane + q] = u.x & 0xffffu; planes[1 * kPlane + q] = u.x >> 16;
+  planes[2 * kPlane + q] = u.y & 0xffffu; planes[3 * kPlane + q] = u.y >> 16;
+  planes[4 * kPlane + q] = u.z & 0xffffu; planes[5 * kPlane + q] = u.z >> 16;
+  planes[6 * kPlane + q] = u.w & 0xffffu; planes[7 * kPlane + q] = u.w >> 16;
+}
+__device__ __forceinline__ void planar_put(uint32_t* planes, int e, const Fr& v) {
+  const int q = pidx(e);
+#pragma unroll
+  for (int c = 0; c < 8; ++c) planes[c * kPlane + q] = v.c[c];
+}
+// Values below 2^28 (at most twelve lazy levels) to canonical form, packed.
+__device__ __forceinline__ uint32_t red28(uint32_t v) {
+  const uint32_t f = (v & 0xffffu) + 15u * (v >> 16);  // < 2^16 + 15 * 2^12 < 2p
+  return min(f, f - P);
+}
+__device__ __forceinline__ uint4 planar_get_packed(const uint32_t* planes, int e) {
+  const int q = pidx(e);
+  uint32_t v[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) v[c] = red28(planes[c * kPlane + q]);
+  return make_uint4(v[0] | (v[1] << 16), v[2] | (v[3] << 16), v[4] | (v[5] << 16), v[6] | (v[7] << 16));
+}
+
+// One radix-2^R register stage: levels [lvl, lvl + R) of the pass, acting on
+// tile bits [b, b + R).  A thread takes a group of 2^R elements and runs it
+// through all 8 coefficient planes; the group's plane offsets are computed
+// once (pidx is XOR-linear over the disjoint base and level bits).
+template <int OP, int R>
+__device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b, int lvl) {
+  const int groups = 1 << (log_n - R);
+  const int bmask = (1 << b) - 1;
+  int off[1 << R];
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) off[j] = pidx(j << b);
+  for (int g = threadIdx.x; g < groups; g += blockDim.x) {
+    const int pb = pidx((g & bmask) | ((g & ~bmask) << R));
+    int q[1 << R];
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) q[j] = pb ^ off[j];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+      uint32_t* pl = planes + c * kPlane;
+      uint32_t v[1 << R];
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) v[j] = pl[q[j]];
+#pragma unroll
+      for (int sft = 0; sft < R; ++sft) {
+        const uint32_t B = P << (lvl + sft);  // bound entering this level
+#pragma unroll
+        for (int j = 0; j < (1 << R); ++j) {
+          if (j & (1 << sft)) continue;
+          const uint32_t lo = v[j], hi = v[j | (1 << sft)];
+          if (OP == kWht) {
+            v[j] = lo + hi;
+            v[j | (1 << sft)] = lo + B - hi;
+          } else {
+            v[j | (1 << sft)] = hi + B - lo;
+          }
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < (1 << R); ++j) pl[q[j]] = v[j];
     }
-    __syncthreads();
   }
+  __syncthreads();
+}
+
+// Levels act on tile bits [bit0, bit0 + levels) of the 2^log_n elements.
+template <int OP>
+__device__ __forceinline__ void planar_levels(uint32_t* planes, int log_n, int bit0, int levels) {
+  int l = 0;
+  for (; l + 3 <= levels; l += 3) planar_stage<OP, 3>(planes, log_n, bit0 + l, l);
+  if (levels - l == 2) planar_stage<OP, 2>(planes, log_n, bit0 + l, l);
+  if (levels - l == 1) planar_stage<OP, 1>(planes, log_n, bit0 + l, l);
+}
+
+// Gathers the n tile elements src[addr(t)] (times alpha[addr(t) & amask] when
+// alpha is given) into the planes.  Each thread issues up to kBatch 16-byte loads
+// before it writes shared memory, so a tile's loads are in flight together.
+constexpr int kBatch = 8;
+template <class Addr>
+__device__ __forceinline__ void tile_gather(uint32_t* planes, int n, const Fe* src, Addr addr, const Fe* __restrict__ alpha,
+                                            size_t amask) {
+  for (int t0 = threadIdx.x; t0 < n; t0 += kBatch * blockDim.x) {
+    uint4 raw[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int t = t0 + u * blockDim.x;
+      if (t < n) raw[u] = *reinterpret_cast<const uint4*>(src + addr(t));
+    }
+    if (alpha) {
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t < n) {
+          Fr v;
+          v.c[0] = raw[u].x & 0xffffu; v.c[1] = raw[u].x >> 16; v.c[2] = raw[u].y & 0xffffu; v.c[3] = raw[u].y >> 16;
+          v.c[4] = raw[u].z & 0xffffu; v.c[5] = raw[u].z >> 16; v.c[6] = raw[u].w & 0xffffu; v.c[7] = raw[u].w >> 16;
+          planar_put(planes, t, mul(v, load(alpha + (addr(t) & amask))));
+        }
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int t = t0 + u * blockDim.x;
+        if (t < n) planar_put_raw(planes, t, raw[u]);
+      }
+    }
+  }
+  __syncthreads();
+}
+template <class Addr>
+__device__ __forceinline__ void tile_scatter(const uint32_t* planes, int n, Fe* dst, Addr addr) {
+  for (int t = threadIdx.x; t < n; t += blockDim.x)
+    *reinterpret_cast<uint4*>(dst + addr(t)) = planar_get_packed(planes, t);
 }
 
 // Pack eight signed weights per element, then Mobius levels [0, levels) in a
 // tile; write into the message half.  `src_base` is the block's first BVA index.
-__global__ void k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t active, uint64_t src_base,
-                                   Fe* __restrict__ cw, int logR, int levels) {
-  extern __shared__ uint4 smem_u4[];
-  Fe* tile = reinterpret_cast<Fe*>(smem_u4);
+__global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t active,
+                                                                     uint64_t src_base, Fe* __restrict__ cw, int logR, int levels) {
+  extern __shared__ uint32_t planes_s[];
   const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
   for (int e = threadIdx.x; e < n; e += blockDim.x) {
@@ -66,9 +179,9 @@ __global__ void k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t acti
     int8_t v[8];
     if (g + 8 <= active) {
       uint2 raw = *reinterpret_cast<const uint2*>(bva + g);
-      const int8_t* b = reinterpret_cast<const int8_t*>(&raw);
+      const int8_t* bb = reinterpret_cast<const int8_t*>(&raw);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = b[k];
+      for (int k = 0; k < 8; ++k) v[k] = bb[k];
     } else {
 #pragma unroll
       for (int k = 0; k < 8; ++k) v[k] = (g + k < active) ? bva[g + k] : int8_t(0);
@@ -76,85 +189,60 @@ __global__ void k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t acti
     Fr r;
 #pragma unroll
     for (int k = 0; k < 8; ++k) r.c[k] = small(v[k]);
-    store(tile + e, r);
+    planar_put(planes_s, e, r);
   }
   __syncthreads();
-  tile_levels<kMobius>(tile, levels);
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const size_t i = first + e;
-    *reinterpret_cast<uint4*>(cw + msg_addr(i, logR)) = *reinterpret_cast<const uint4*>(tile + e);
-  }
+  planar_levels<kMobius>(planes_s, levels, 0, levels);
+  tile_scatter(planes_s, n, cw, [=](int t) { return msg_addr(first + t, logR); });
 }
 
-// Same as above but the packed values come from an element vector (the
-// block-folded table); the source is also left untouched for the sumcheck.
-__global__ void k_copy_mobius_tile(const Fe* __restrict__ src, Fe* __restrict__ cw, int logR, int levels) {
-  extern __shared__ uint4 smem_u4[];
-  Fe* tile = reinterpret_cast<Fe*>(smem_u4);
+// Same, but the packed values come from an element vector (the block-folded
+// table), which is left untouched for the sumcheck.
+__global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* __restrict__ src, Fe* __restrict__ cw, int logR,
+                                                                     int levels) {
+  extern __shared__ uint32_t planes_s[];
   const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
-  for (int e = threadIdx.x; e < n; e += blockDim.x)
-    *reinterpret_cast<uint4*>(tile + e) = *reinterpret_cast<const uint4*>(src + first + e);
-  __syncthreads();
-  tile_levels<kMobius>(tile, levels);
-  for (int e = threadIdx.x; e < n; e += blockDim.x)
-    *reinterpret_cast<uint4*>(cw + msg_addr(first + e, logR)) = *reinterpret_cast<const uint4*>(tile + e);
+  tile_gather(planes_s, n, src, [=](int t) { return first + t; }, nullptr, 0);
+  planar_levels<kMobius>(planes_s, levels, 0, levels);
+  tile_scatter(planes_s, n, cw, [=](int t) { return msg_addr(first + t, logR); });
 }
 
 // WHT levels [0, levels) within a tile (levels <= logR so columns never mix).
 // Reads the message (or parity) half at src, optionally multiplies each row by
-// alpha[r] first, writes the parity half.
-__global__ void k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR,
-                           int levels) {
-  extern __shared__ uint4 smem_u4[];
-  Fe* tile = reinterpret_cast<Fe*>(smem_u4);
+// alpha[r] first, writes the parity half (src may equal dst: a CTA reads its
+// whole tile before it writes).
+__global__ void __launch_bounds__(kTileThreads, 1) k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR,
+                                                             int levels) {
+  extern __shared__ uint32_t planes_s[];
   const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
+  // For a message-half address a = c * 2R + r, a & (R - 1) = r.
   const size_t rmask = (size_t(1) << logR) - 1;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const size_t i = first + e;
-    Fr v = load(src + msg_addr(i, logR));
-    if (alpha) v = mul(v, load(alpha + (i & rmask)));
-    store(tile + e, v);
-  }
-  __syncthreads();
-  tile_levels<kWht>(tile, levels);
-  for (int e = threadIdx.x; e < n; e += blockDim.x)
-    *reinterpret_cast<uint4*>(dst + msg_addr(first + e, logR)) = *reinterpret_cast<const uint4*>(tile + e);
+  tile_gather(planes_s, n, src, [=](int t) { return msg_addr(first + t, logR); }, alpha, rmask);
+  planar_levels<kWht>(planes_s, levels, 0, levels);
+  tile_scatter(planes_s, n, dst, [=](int t) { return msg_addr(first + t, logR); });
 }
 
-// Levels [lo, lo + k) over the logical index space of m elements, on the half
-// starting at `base` (cw for the message, cw + R for the parity).  Each CTA
-// owns 8 consecutive group bases (one 128-byte segment per row of the tile).
+// Levels [lo, lo + k) over the logical index space, on the half starting at
+// `base` (cw for the message, cw + R for the parity).  Each CTA owns 2^cb
+// consecutive group bases (64- or 128-byte runs in HBM for cb = 2, 3): tile
+// element t = (j << cb) + c is logical index base(g0 + c) + (j << lo), so the
+// levels act on tile bits [cb, cb + k).
 template <int OP>
-__global__ void k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k) {
-  extern __shared__ uint4 smem_u4[];
-  Fe* tile = reinterpret_cast<Fe*>(smem_u4);
-  const int rows = 1 << k;
-  const size_t g0 = size_t(blockIdx.x) * 8;
+__global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k, int cb) {
+  extern __shared__ uint32_t planes_s[];
+  const int n = 1 << (cb + k);
+  const size_t g0 = size_t(blockIdx.x) << cb;
   const size_t low_mask = (size_t(1) << lo) - 1;
-  for (int t = threadIdx.x; t < rows * 8; t += blockDim.x) {
-    const int c8 = t & 7, j = t >> 3;
-    const size_t g = g0 + c8;
-    const size_t i = (((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(j) << lo);
-    *reinterpret_cast<uint4*>(tile + t) = *reinterpret_cast<const uint4*>(base + msg_addr(i, logR));
-  }
-  __syncthreads();
-  for (int l = 0; l < k; ++l) {
-    const int half = 1 << l;
-    for (int q = threadIdx.x; q < rows * 4; q += blockDim.x) {
-      const int c8 = q & 7, pj = q >> 3;
-      const int jlo = ((pj >> l) << (l + 1)) | (pj & (half - 1));
-      butterfly<OP>(tile + jlo * 8 + c8, tile + (jlo + half) * 8 + c8);
-    }
-    __syncthreads();
-  }
-  for (int t = threadIdx.x; t < rows * 8; t += blockDim.x) {
-    const int c8 = t & 7, j = t >> 3;
-    const size_t g = g0 + c8;
-    const size_t i = (((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(j) << lo);
-    *reinterpret_cast<uint4*>(base + msg_addr(i, logR)) = *reinterpret_cast<const uint4*>(tile + t);
-  }
+  const int cmask = (1 << cb) - 1;
+  auto addr = [=](int t) {
+    const size_t g = g0 + (t & cmask);
+    return msg_addr((((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(t >> cb) << lo), logR);
+  };
+  tile_gather(planes_s, n, base, addr, nullptr, 0);
+  planar_levels<OP>(planes_s, cb + k, cb, k);
+  tile_scatter(planes_s, n, base, addr);
 }
 
 // ---------------------------------------------------------------- hashing
