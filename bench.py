@@ -183,7 +183,11 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="8b8", choices=["8b8", "smoke"])
+    ap.add_argument("--workload", default="8b8", choices=["8b8", "layers", "smoke"],
+                    help="8b8: the 8B shape set; layers: the first --layers transformer layers "
+                         "(7 matrices each) at --chunk-log, a small case for profiling")
+    ap.add_argument("--layers", type=int, default=2)
+    ap.add_argument("--chunk-log", type=int, default=28)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--out", default=str(ROOT / "gpurun_out"))
     args = ap.parse_args()
@@ -209,6 +213,10 @@ def main():
 
     if args.workload == "8b8":
         shapes, cfg, name = shapes_8b(), qf.Config(30, 4), "8B-shape 8-bit weights, batched (226 matrices)"
+    elif args.workload == "layers":
+        shapes = shapes_8b()[1:1 + 7 * args.layers]
+        cfg = qf.Config(args.chunk_log, 4)
+        name = f"8B-shape 8-bit weights, first {args.layers} layers, chunk 2^{args.chunk_log}"
     else:
         shapes, cfg, name = [(1024, 4096)], qf.Config(20, 4), "smoke 1024x4096 int8"
     weights = sum(r * c for r, c in shapes)
