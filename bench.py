@@ -134,6 +134,23 @@ def ncu_traffic(kernel: str):
     return d.get(kernel)
 
 
+def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
+    """Step time of the slowest rank (every rank calls this collectively)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(weights_per_rank: int, world: int, ms_per_step: float) -> float:
+    """Whole-job weights/s: every rank proves its own model of `weights_per_rank`."""
+    return weights_per_rank * world / (ms_per_step / 1000.0)
+
+
 def run_reference(args):
     """CPU restatement of the reference prover on a bounded sample of the workload."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -264,11 +281,7 @@ def main():
             last = step(on_device)
         ev1.record()
         barrier()
-        ms = ev0.elapsed_time(ev1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ev0.elapsed_time(ev1), world)
         return ms / steps, last, qf.kernel_launches() - launches0
 
     out_dir = Path(args.out)
@@ -303,7 +316,7 @@ def main():
             cpu_baseline = json.loads(r.stdout.strip().splitlines()[-1])["cpu_baseline"]
         except Exception as e:  # reported, not fatal
             cpu_baseline = {"error": str(e)[:200]}
-    value = weights * world / (ms_dev / 1000.0)
+    value = job_throughput(weights, world, ms_dev)
     line = {
         "metric": "QAFold commit+open weights/s",
         "value": value,
@@ -321,7 +334,7 @@ def main():
                    "weights": weights, "active_entries": active, "pcs_blocks": params.blocks,
                    "l2": "inputs larger than L2 (8 GB BVA, 4 GiB codeword per block)",
                    "parallelism": "replicas" if world > 1 else "single"},
-        "e2e": {"value": weights * world / (ms_e2e / 1000.0), "unit": "weights/s",
+        "e2e": {"value": job_throughput(weights, world, ms_e2e), "unit": "weights/s",
                 "h2d_bytes_per_step": active, "d2h_bytes_per_step": proof_bytes},
         "gpu_launches": launches // max(args.steps, 1),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
