@@ -104,6 +104,32 @@ int qf_kernel_stats(char* buf, size_t cap, size_t* len);
 uint64_t qf_kernel_launches(void);
 size_t qf_last_error(char* buf, size_t cap);
 
+/* No counterpart in the reference: a commitment entry point that allocates
+ * no device memory, for callers that cannot (a serving engine that reserves
+ * nearly all of HBM for its own pool; a latency-bound loop that cannot take
+ * the synchronisation cudaMalloc/cudaFree may imply).
+ *
+ * Writes the root of PCS block `block` (the bytes qf_commit writes at
+ * roots_out + 32 * block) to the 32 device bytes `d_root`, asynchronously on
+ * `stream` (a cudaStream_t; NULL is the legacy default stream).  `d_bva` is
+ * a device pointer to the n_values active int8 entries.  Unlike qf_commit it
+ * neither copies the weights nor checks the layout's zero padding.
+ *
+ * Limit: F65521 blocks of at most 2^QF_NOALLOC_MAX_CHUNK_LOG weights
+ * (config chunk_log <= 20); larger blocks return QF_E_ARGUMENT.  All working
+ * buffers live in one static device array of QF_NOALLOC_SCRATCH_BYTES, which
+ * every GPU that loads the library holds until the process exits.  The first
+ * call on a device looks up that array's address there (cudaGetSymbolAddress);
+ * make that first call before any stream capture.  Every call shares the
+ * array, which keeps the last call's contents (nothing in it has to start at
+ * zero: each word a call reads, the same call wrote first); calls that
+ * overlap on the GPU (other streams or host threads on the same device) race,
+ * so serialise them. */
+#define QF_NOALLOC_MAX_CHUNK_LOG 20
+#define QF_NOALLOC_SCRATCH_BYTES (5u << 20)
+int qf_commit_block_noalloc(const qf_params* params, const int8_t* d_bva, uint64_t n_values, uint64_t block,
+                            uint8_t* d_root, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,7 +58,7 @@ _lib = None
 EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
-    "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches",
+    "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc",
 )
 
 
@@ -92,6 +92,7 @@ def lib() -> ctypes.CDLL:
         L.qf_kernel_stats.argtypes = [ctypes.c_char_p, S, ctypes.POINTER(S)]
         L.qf_kernel_launches.argtypes = []
         L.qf_kernel_launches.restype = U64
+        L.qf_commit_block_noalloc.argtypes = [P, P, U64, U64, P, P]
         for name in EXPORTED:
             if not hasattr(L, name):
                 raise QfError(-9, f"library does not export {name}")
@@ -265,6 +266,14 @@ class Parameters:
         return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)])
 
     commit_recomputed = commit
+
+    def block_root_noalloc(self, bva, block: int, root, stream: int = 0) -> None:
+        """qf_commit_block_noalloc: the root of PCS block `block` of the
+        device BVA tensor `bva` (int8, active entries) into the 32-byte
+        device tensor `root`, asynchronously on the CUDA stream handle
+        `stream`, with no device allocation (blocks of at most 2^20 weights)."""
+        _check(lib().qf_commit_block_noalloc(self._h, ctypes.c_void_p(int(bva.data_ptr())), int(bva.numel()), int(block),
+                                             ctypes.c_void_p(int(root.data_ptr())), ctypes.c_void_p(int(stream))))
 
     def statement_json(self, roots: Sequence[bytes]) -> bytes:
         r = b"".join(roots)

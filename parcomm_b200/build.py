@@ -12,7 +12,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libparcomm_qafold.so"
-SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "gpu_backend.cu"]
+SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "gpu_backend.cu", PKG / "csrc" / "noalloc.cu"]
 HEADERS = sorted((PKG / "csrc").rglob("*.h")) + sorted((PKG / "csrc").rglob("*.cuh"))
 
 NVCC_FLAGS = [

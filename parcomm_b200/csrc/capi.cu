@@ -6,35 +6,18 @@
 #include <string>
 
 #include "../../include/parcomm_qafold.h"
+#include "capi_internal.h"
 #include "gpu_backend.cuh"
 
 using namespace qf;
 using qfg::DBuf;
 using qfg::GpuBackend;
 using F = Fp8;
+using qfc::guarded;
+using qfc::require_device;
+using qfc::set_error;
 
 namespace {
-thread_local std::string g_last_error;
-
-int set_error(int code, const std::string& msg) {
-  g_last_error = msg;
-  return code;
-}
-
-template <class Fn>
-int guarded(Fn&& fn) {
-  try {
-    fn();
-    return QF_OK;
-  } catch (const QfError& e) {
-    return set_error(e.code, e.what());
-  } catch (const std::bad_alloc&) {
-    return set_error(QF_E_ARGUMENT, "host allocation failed");
-  } catch (const std::exception& e) {
-    return set_error(QF_E_PROTOCOL, e.what());
-  }
-}
-
 // Any zero-padding entry that is nonzero sets the flag (Layout::validate_values, layout.rs:136-155).
 __global__ void k_check_zero_segments(const int8_t* __restrict__ bva, const uint64_t* __restrict__ seg, uint32_t n_seg,
                                       unsigned int* __restrict__ flag) {
@@ -45,17 +28,7 @@ __global__ void k_check_zero_segments(const int8_t* __restrict__ bva, const uint
   }
 }
 
-void require_device() {
-  int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) fail(QF_E_NO_DEVICE, "no CUDA device available");
-}
-
 }  // namespace
-
-struct qf_params {
-  int field = 0;
-  std::unique_ptr<Parameters<F>> P;
-};
 
 struct qf_committed {
   const qf_params* params = nullptr;
@@ -329,11 +302,11 @@ uint64_t qf_kernel_launches(void) { return qfg::KernelClock::launches.load(); }
 
 size_t qf_last_error(char* buf, size_t cap) {
   if (buf && cap) {
-    size_t n = std::min(cap - 1, g_last_error.size());
-    std::memcpy(buf, g_last_error.data(), n);
+    size_t n = std::min(cap - 1, qfc::g_last_error.size());
+    std::memcpy(buf, qfc::g_last_error.data(), n);
     buf[n] = 0;
   }
-  return g_last_error.size();
+  return qfc::g_last_error.size();
 }
 
 }  // extern "C"

@@ -375,6 +375,59 @@ Digest GpuBackend::commit_block(size_t b) {
   return roots_[b];
 }
 
+// The same kernels as commit_block + encode_and_hash, launched without the
+// per-launch timers and into caller-owned buffers.
+template <int OP>
+static void strided_passes_plain(cudaStream_t s, Fe* base, int logR, int logm, int from, int to) {
+  for (int lo = from; lo < to;) {
+    const int k = std::min(10, to - lo);
+    const int cb = std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k);
+    qfd::k_butterfly_strided<OP><<<unsigned(size_t(1) << (logm - k - cb)), qfd::kTileThreads, qfd::kTileSmem, s>>>(base, logR, lo, k, cb);
+    QF_CK(cudaGetLastError());
+    lo += k;
+  }
+}
+
+void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
+                       Fe* alpha, uint8_t* d_root, cudaStream_t s) {
+  configure_tile_kernels();
+  const int logm = ilog2(P.pcs.packed_len());
+  const size_t cols = P.pcs.pp->extension_columns;
+  const int logR = logm - ilog2(cols);
+  const size_t R = size_t(1) << logR;
+  const auto& top = P.pcs.pp->seq.top();
+  check(top.message_len == R, "alpha table length");
+  QF_CK(cudaMemcpyAsync(alpha, top.alphas[1].data(), R * 16, cudaMemcpyHostToDevice, s));
+  // Message half: pack + Mobius.
+  const int l0 = std::min(qfd::kMaxTileLog, logm);
+  qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
+      d_bva, active, uint64_t(b) * P.block_len, cw, logR, l0);
+  QF_CK(cudaGetLastError());
+  strided_passes_plain<qfd::kMobius>(s, cw, logR, logm, l0, logm);
+  // Parity half: WHT(alpha * WHT(message)) per column.
+  const int wl = std::min(qfd::kMaxTileLog, logR);
+  for (int pass = 0; pass < 2; ++pass) {
+    qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
+        pass == 0 ? cw : cw + R, cw + R, pass == 0 ? nullptr : alpha, logR, wl);
+    QF_CK(cudaGetLastError());
+    strided_passes_plain<qfd::kWht>(s, cw + R, logR, logm, wl, logR);
+  }
+  // Row leaves, inner levels, root.
+  const uint64_t n_ext = 2 * R;
+  qfd::k_hash_leaves<11><<<unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads), qfd::kLeafThreads, 0, s>>>(
+      cw, n_ext, int(cols), leaf_prefix(cols, false), tree);
+  QF_CK(cudaGetLastError());
+  const qfd::InnerPrefix ip = inner_prefix();
+  uint64_t off = 0, n = n_ext;
+  while (n > 1) {
+    qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s>>>(tree + 2 * off, n / 2, ip, tree + 2 * (off + n));
+    QF_CK(cudaGetLastError());
+    off += n;
+    n /= 2;
+  }
+  QF_CK(cudaMemcpyAsync(d_root, tree + 2 * off, 32, cudaMemcpyDeviceToDevice, s));
+}
+
 std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n) {
   switch (n) {
     case 1: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 16, qfd::k_reduce_partials<1><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;

@@ -135,6 +135,14 @@ struct DeviceCodeword : CodewordView<F> {
   std::vector<F> entries() const override;
 };
 
+// Commitment root of block `b` of a device BVA (`active` entries), computed
+// only in the caller's device buffers: `cw` holds 2R x cols entries, `tree`
+// 4 x 2R words (2 x 2R digests), `alpha` R entries (overwritten with the
+// code's alpha table).  Launches on `s`, writes the 32-byte root to the device
+// bytes `d_root` and returns without synchronising; allocates no device memory.
+void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
+                       Fe* alpha, uint8_t* d_root, cudaStream_t s);
+
 class GpuBackend : public Backend<F>,
                    public SingleBackend<F>,
                    public EoBackend<F>,
