@@ -125,13 +125,18 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, if any."""
+def ncu_traffic(kernel: str, alg_bytes_per_launch: float):
+    """Per-launch DRAM bytes of `kernel`: the committed ncu capture's ratio of
+    dram__bytes_read.sum + dram__bytes_write.sum to algorithmic bytes (taken
+    on a smaller case of the same kernel), times this run's algorithmic bytes
+    per launch; None without a capture."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text())
-    return d.get(kernel)
+    d = json.loads(p.read_text()).get(kernel)
+    if not d:
+        return None
+    return d["dram_bytes_per_alg_byte"] * alg_bytes_per_launch
 
 
 def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
@@ -302,7 +307,7 @@ def main():
     d = stats[dominant]
     achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic(dominant)
+    traffic = ncu_traffic(dominant, d["bytes"] / d["launches"])
 
     if world > 1:
         torch.distributed.destroy_process_group()
