@@ -624,61 +624,104 @@ std::vector<int8_t> GpuBackend::windows(const std::vector<uint64_t>& starts, siz
   return out;
 }
 
-// Lane projections (tbv.rs:288-352) of large terms: two-level weight tables
-// per term, one tile per high-table entry.
+// Factor-pair tables for the TBV term kernels, built on the device in one
+// launch (the host only gathers each table's factor pairs and scale).
+namespace {
+struct TableBuilder {
+  std::vector<Fe> factors;  // two entries per factor pair
+  std::vector<qfd::TableSpec> specs;
+  uint32_t total = 0;
+  uint32_t add(const std::array<F, 2>* f, size_t n_bits, size_t count, const F& scale) {
+    qfd::TableSpec sp;
+    sp.out_off = total;
+    sp.count = uint32_t(count);
+    sp.fac_off = uint32_t(factors.size() / 2);
+    sp.n_bits = uint32_t(n_bits);
+    sp.scale = to_fe(scale);
+    for (size_t k = 0; k < n_bits; ++k) {
+      factors.push_back(to_fe(f[k][0]));
+      factors.push_back(to_fe(f[k][1]));
+    }
+    specs.push_back(sp);
+    total += uint32_t(count);
+    return sp.out_off;
+  }
+  // Uploads and launches; the staging buffers live in the builder until the
+  // caller has synchronised the stream.
+  void build(cudaStream_t s, DBuf<Fe>& out) {
+    out.alloc(std::max<uint32_t>(total, 1));
+    if (specs.empty()) return;
+    dfac.alloc(std::max<size_t>(factors.size(), 1));
+    dspec.alloc(specs.size());
+    if (!factors.empty()) QF_CK(cudaMemcpyAsync(dfac.p, factors.data(), factors.size() * 16, cudaMemcpyHostToDevice, s));
+    QF_CK(cudaMemcpyAsync(dspec.p, specs.data(), specs.size() * sizeof(qfd::TableSpec), cudaMemcpyHostToDevice, s));
+    QF_LAUNCH(s, "k_factor_tables", uint64_t(total) * 16,
+              qfd::k_factor_tables<<<grid_for(total, kThreads), kThreads, 0, s>>>(dspec.p, int(specs.size()), dfac.p, total, out.p));
+  }
+  DBuf<Fe> dfac;
+  DBuf<qfd::TableSpec> dspec;
+};
+
+// One term's tiles: rows of 2^lb, high bits split into mid (<= 2^10) and top.
+qfd::TermTiles term_tiles(TableBuilder& tb, const std::array<F, 2>* f, size_t nh, uint64_t offset, uint64_t rows,
+                          uint32_t first_tile, const F& scale) {
+  qfd::TermTiles T;
+  const size_t lb = std::min<size_t>(10, nh);
+  const size_t mb = std::min<size_t>(10, nh - lb);
+  const uint64_t ntiles = (rows + (uint64_t(1) << lb) - 1) >> lb;
+  T.offset = offset;
+  T.rows = rows;
+  T.first_tile = first_tile;
+  T.lb = uint32_t(lb);
+  T.mb = uint32_t(mb);
+  T.lo_off = tb.add(f, lb, size_t(1) << lb, F::one());
+  T.mid_off = tb.add(f + lb, mb, size_t(1) << mb, F::one());
+  T.top_off = tb.add(f + lb + mb, nh - lb - mb, (ntiles + (uint64_t(1) << mb) - 1) >> mb, scale);
+  return T;
+}
+uint64_t term_tile_count(const qfd::TermTiles& T) { return (T.rows + (uint64_t(1) << T.lb) - 1) >> T.lb; }
+}  // namespace
+
+// Lane projections (tbv.rs:288-352) of large terms: one CTA per tile of up
+// to 1024 rows, tile weights from device-built factor tables.
 std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Term<F>*>& terms, size_t stride) {
   HostScope hs("project_terms");
   std::vector<std::vector<F>> out(terms.size());
-  std::vector<qfd::ProjTile> tiles;
-  std::vector<F> lo_all;
-  uint64_t proj_bytes = 0;
+  TableBuilder tb;
+  std::vector<qfd::TermTiles> tt;
   std::vector<uint32_t> seg(1, 0);
-  std::vector<size_t> lanes_of(terms.size());
+  uint64_t tiles = 0, proj_bytes = 0;
   size_t common_lanes = 0;
   for (size_t t = 0; t < terms.size(); ++t) {
     const Term<F>& term = *terms[t];
-    size_t low_bits = std::min<size_t>(ilog2(stride), term.factors.size());
-    size_t lanes = size_t(1) << low_bits;
-    lanes_of[t] = lanes;
+    const size_t low_bits = std::min<size_t>(ilog2(stride), term.factors.size());
+    const size_t lanes = size_t(1) << low_bits;
     out[t].assign(lanes, F::zero());
     if (common_lanes == 0) common_lanes = lanes;
     if (lanes != common_lanes) fail(QF_E_ARGUMENT, "mixed lane widths");
-    if (term.offset >= active_ || term.scale.is_zero()) { seg.push_back(uint32_t(tiles.size())); continue; }
-    const size_t nh = term.factors.size() - low_bits;
-    const int lb = int(std::min<size_t>(10, nh));
-    const size_t rows = std::min((active_ - term.offset + lanes - 1) / lanes, term.len() / lanes);
-    const size_t ntiles = (rows + (size_t(1) << lb) - 1) >> lb;
-    std::vector<F> lo = factor_weights(term.factors.data() + low_bits, lb);
-    // High table entries (one product per entry by doubling), times scale.
-    std::vector<F> hi = factor_weights(term.factors.data() + low_bits + lb, nh - lb);
-    hi.resize(ntiles);
-    for (auto& h : hi) h = h * term.scale;
-    const uint32_t lo_off = uint32_t(lo_all.size());
-    lo_all.insert(lo_all.end(), lo.begin(), lo.end());
-    for (size_t i = 0; i < ntiles; ++i) {
-      qfd::ProjTile pt;
-      pt.base = term.offset + (i << lb) * lanes;
-      pt.rows = uint32_t(std::min<size_t>(size_t(1) << lb, rows - (i << lb)));
-      proj_bytes += uint64_t(pt.rows) * lanes + 16;
-      pt.lo_off = lo_off;
-      pt.hi = to_fe(hi[i]);
-      tiles.push_back(pt);
+    check(lanes <= 64, "at most 64 projection lanes");
+    if (term.offset < active_ && !term.scale.is_zero()) {
+      const size_t nh = term.factors.size() - low_bits;
+      const uint64_t rows = std::min<uint64_t>((active_ - term.offset + lanes - 1) / lanes, term.len() / lanes);
+      qfd::TermTiles T = term_tiles(tb, term.factors.data() + low_bits, nh, term.offset, rows, uint32_t(tiles), term.scale);
+      tiles += term_tile_count(T);
+      proj_bytes += rows * lanes + term_tile_count(T) * 16;
+      tt.push_back(T);
     }
-    seg.push_back(uint32_t(tiles.size()));
+    check(tiles < (uint64_t(1) << 31), "projection tile count");
+    seg.push_back(uint32_t(tiles));
   }
-  if (tiles.empty()) return out;
-  DBuf<qfd::ProjTile> dt(tiles.size());
-  DBuf<Fe> dlo(lo_all.size()), dtile(tiles.size() * common_lanes), dterm(terms.size() * common_lanes);
+  if (tiles == 0) return out;
+  DBuf<Fe> tables, dtile(tiles * common_lanes), dterm(terms.size() * common_lanes);
+  tb.build(s_, tables);
+  DBuf<qfd::TermTiles> dtt(tt.size());
   DBuf<uint32_t> dseg(seg.size());
-  QF_CK(cudaMemcpyAsync(dt.p, tiles.data(), tiles.size() * sizeof(qfd::ProjTile), cudaMemcpyHostToDevice, s_));
-  QF_CK(cudaMemcpyAsync(dlo.p, lo_all.data(), lo_all.size() * 16, cudaMemcpyHostToDevice, s_));
+  QF_CK(cudaMemcpyAsync(dtt.p, tt.data(), tt.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
   QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, s_));
-  for (size_t off = 0; off < tiles.size(); off += 1u << 30) {
-    size_t cnt = std::min<size_t>(tiles.size() - off, size_t(1) << 30);
-    QF_LAUNCH(s_, "k_project_tiles", proj_bytes, qfd::k_project_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(bva_, active_, dt.p + off, dlo.p, int(common_lanes),
-                                                             dtile.p + off * common_lanes));
-  }
-  QF_LAUNCH(s_, "k_sum_segments", uint64_t(tiles.size()) * common_lanes * 16, qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p));
+  QF_LAUNCH(s_, "k_project_terms", proj_bytes,
+            qfd::k_project_terms<<<unsigned(tiles), qfd::kTermThreads, 0, s_>>>(bva_, active_, dtt.p, int(tt.size()), tables.p,
+                                                                                 int(common_lanes), dtile.p));
+  QF_LAUNCH(s_, "k_sum_segments", tiles * common_lanes * 16, qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p));
   std::vector<F> h(terms.size() * common_lanes);
   QF_CK(cudaMemcpyAsync(h.data(), dterm.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
@@ -734,9 +777,9 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
   QF_CK(cudaMemsetAsync(qv_.p, 0, rows * 16, s_));
   std::vector<F> powers = consecutive_powers(ch, stride);
   const size_t ls = ilog2(stride);
-  std::vector<qfd::QueryTile> pass_tiles[2];
-  uint64_t query_bytes[2] = {0, 0};
-  std::vector<F> lo_all;
+  TableBuilder tb;
+  std::vector<qfd::TermTiles> pass_terms[2];
+  uint64_t pass_tiles[2] = {0, 0}, query_bytes[2] = {0, 0};
   std::map<uint64_t, F> sparse;
   const size_t n_claim_terms = P_.layout.buckets.size();
   for (size_t ti = 0; ti < q.terms.size(); ++ti) {
@@ -747,26 +790,15 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
       for (size_t j = 0; j < stride; ++j) sc += low[j] * powers[j];
       sc = term.scale * sc;
       if (sc.is_zero()) continue;
-      const size_t nh = term.factors.size() - ls;
-      const int lb = int(std::min<size_t>(10, nh));
-      const size_t n_rows = term.len() / stride;
-      const size_t ntiles = n_rows >> lb;
-      std::vector<F> lo = factor_weights(term.factors.data() + ls, lb);
-      const uint32_t lo_off = uint32_t(lo_all.size());
-      lo_all.insert(lo_all.end(), lo.begin(), lo.end());
-      std::vector<F> hi = factor_weights(term.factors.data() + ls + lb, nh - lb);
       // Claim and zero-suffix terms are disjoint; padding terms overlap claim terms.
       const int pass = (ti < n_claim_terms || term.offset >= P_.layout.active) ? 0 : 1;
-      for (size_t i = 0; i < ntiles; ++i) {
-        F h = sc * hi[i];
-        qfd::QueryTile qt;
-        qt.start = term.offset / stride + (i << lb);
-        qt.rows = uint32_t(size_t(1) << lb);
-        qt.lo_off = lo_off;
-        qt.hi = to_fe(h);
-        pass_tiles[pass].push_back(qt);
-        query_bytes[pass] += uint64_t(qt.rows) * 32;
-      }
+      const size_t nh = term.factors.size() - ls;
+      qfd::TermTiles T = term_tiles(tb, term.factors.data() + ls, nh, term.offset / stride, term.len() / stride,
+                                    uint32_t(pass_tiles[pass]), sc);
+      pass_tiles[pass] += term_tile_count(T);
+      check(pass_tiles[pass] < (uint64_t(1) << 31), "query tile count");
+      query_bytes[pass] += T.rows * 32;
+      pass_terms[pass].push_back(T);
     } else {
       for (size_t i = 0; i < term.len(); ++i) {
         auto it = sparse.find(term.offset / stride);
@@ -775,18 +807,16 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
       }
     }
   }
-  DBuf<Fe> dlo(std::max<size_t>(lo_all.size(), 1));
-  if (!lo_all.empty()) QF_CK(cudaMemcpyAsync(dlo.p, lo_all.data(), lo_all.size() * 16, cudaMemcpyHostToDevice, s_));
+  DBuf<Fe> tables;
+  tb.build(s_, tables);
+  DBuf<qfd::TermTiles> dtt[2];
   for (int pass = 0; pass < 2; ++pass) {
-    auto& tl = pass_tiles[pass];
+    auto& tl = pass_terms[pass];
     if (tl.empty()) continue;
-    DBuf<qfd::QueryTile> dt(tl.size());
-    QF_CK(cudaMemcpyAsync(dt.p, tl.data(), tl.size() * sizeof(qfd::QueryTile), cudaMemcpyHostToDevice, s_));
-    for (size_t off = 0; off < tl.size(); off += 1u << 30) {
-      size_t cnt = std::min<size_t>(tl.size() - off, size_t(1) << 30);
-      QF_LAUNCH(s_, "k_query_tiles", query_bytes[pass], qfd::k_query_tiles<<<unsigned(cnt), kThreads, 0, s_>>>(dt.p + off, dlo.p, 1, qv_.p));
-    }
-    QF_CK(cudaStreamSynchronize(s_));
+    dtt[pass].alloc(tl.size());
+    QF_CK(cudaMemcpyAsync(dtt[pass].p, tl.data(), tl.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
+    QF_LAUNCH(s_, "k_query_terms", query_bytes[pass],
+              qfd::k_query_terms<<<unsigned(pass_tiles[pass]), kThreads, 0, s_>>>(dtt[pass].p, int(tl.size()), tables.p, qv_.p));
   }
   if (!sparse.empty()) {
     std::vector<uint64_t> idx;

@@ -71,41 +71,117 @@ __device__ __forceinline__ Fr table_at(const Fe* hi, const Fe* lo, int lb, uint6
 // values starting at `base`, all sharing the high weight `hi`; the low
 // weights are lo[0 .. rows).  Output: lanes field elements
 //   out[lane] = hi * sum_r lo[r] * v[base + r * lanes + lane].
-struct ProjTile {
-  uint64_t base;
-  uint32_t rows;
-  uint32_t lo_off;  // offset of this term's low table
-  Fe hi;
+// ---------------------------------------------------------------- TBV term tiles
+// Tensor weights of LSB-first factor pairs (tbv.rs:45-76), built on the
+// device: entry e of a table is scale * prod_k factors[k][bit k of e].
+struct TableSpec {
+  uint32_t out_off, count;  // entries [out_off, out_off + count) of the table array
+  uint32_t fac_off, n_bits; // factor pairs [fac_off, fac_off + n_bits)
+  Fe scale;
 };
-
-__global__ void k_project_tiles(const int8_t* __restrict__ bva, uint64_t active, const ProjTile* __restrict__ tiles,
-                                const Fe* __restrict__ lo_tables, int lanes, Fe* __restrict__ out) {
-  __shared__ int64_t acc_s[256][8];
-  const ProjTile t = tiles[blockIdx.x];
-  const int lane = threadIdx.x % lanes, phase = threadIdx.x / lanes, phases = blockDim.x / lanes;
-  int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  const Fe* lo = lo_tables + t.lo_off;
-  for (uint32_t r = phase; r < t.rows; r += phases) {
-    const uint64_t g = t.base + uint64_t(r) * lanes + lane;
-    const int v = g < active ? int(bva[g]) : 0;
-    if (v != 0) {
-      Fr w = load(lo + r);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc[k] += int32_t(w.c[k]) * v;
+__global__ void k_factor_tables(const TableSpec* __restrict__ specs, int n_specs, const Fe* __restrict__ factors,
+                                uint32_t total, Fe* __restrict__ out) {
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_specs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (specs[mid].out_off <= e) lo = mid; else hi = mid - 1;
     }
+    const TableSpec& s = specs[lo];
+    const uint32_t idx = e - s.out_off;
+    Fr v = load(&s.scale);
+    for (uint32_t k = 0; k < s.n_bits; ++k) v = mul(v, load(factors + 2 * (s.fac_off + k) + ((idx >> k) & 1)));
+    store(out + e, v);
   }
+}
+
+// The tiles of one TBV term: tile i covers rows [i << lb, (i + 1) << lb) of the
+// term (a row is `lanes` consecutive BVA entries from `offset` for the
+// projection, one packed row from `offset` for the query fold).  Its weight
+// is lo[r] * top[i >> mb] * mid[i & (2^mb - 1)], the term scale folded into top.
+struct TermTiles {
+  uint64_t offset, rows;
+  uint32_t first_tile;
+  uint32_t lo_off, mid_off, top_off;
+  uint32_t lb, mb;
+};
+__device__ __forceinline__ int find_term(const TermTiles* __restrict__ t, int n, uint32_t tile) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (t[mid].first_tile <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+__device__ __forceinline__ Fr tile_high(const TermTiles& T, const Fe* __restrict__ tables, uint64_t i) {
+  return mul(load(tables + T.top_off + (i >> T.mb)), load(tables + T.mid_off + (i & ((uint64_t(1) << T.mb) - 1))));
+}
+
+// Lane projections (tbv.rs:288-352): out[tile * lanes + l] = high(tile) *
+// sum_r lo[r] * bva[offset + row * lanes + l].  A thread takes min(4, lanes)
+// lanes of a row (one 32-bit load); products accumulate exactly in i32 (at
+// most 128 rows * 128 * 65520 < 2^31 per warp sum: tiles have <= 1024 rows),
+// then in i64 across warps, then reduce once.
+constexpr int kTermThreads = 256;
+__global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __restrict__ bva, uint64_t active,
+                                                                const TermTiles* __restrict__ terms, int n_terms,
+                                                                const Fe* __restrict__ tables, int lanes,
+                                                                Fe* __restrict__ out) {
+  __shared__ int t_sel;
+  __shared__ int64_t part_s[kTermThreads / 32][64][8];
+  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, blockIdx.x);
+  __syncthreads();
+  const TermTiles T = terms[t_sel];
+  const uint64_t i = blockIdx.x - T.first_tile;
+  const uint64_t row0 = i << T.lb;
+  const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
+  const int nrows = int(left < span ? left : span);
+  const int lpt = lanes < 4 ? lanes : 4;
+  const int tpr = lanes / lpt;
+  const int rpp = kTermThreads / tpr;
+  const int sub = threadIdx.x % tpr;
+  int32_t acc[4][8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) acc_s[threadIdx.x][k] = acc[k];
+  for (int j = 0; j < 4; ++j)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) acc[j][k] = 0;
+  const Fe* lo = tables + T.lo_off;
+  for (int r = threadIdx.x / tpr; r < nrows; r += rpp) {
+    const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
+    int v[4] = {0, 0, 0, 0};
+    if (lpt == 4 && g + 4 <= active && (g & 3) == 0) {
+      const uint32_t u = *reinterpret_cast<const uint32_t*>(bva + g);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[j] = int(int8_t(u >> (8 * j)));
+    } else {
+      for (int j = 0; j < lpt; ++j) v[j] = g + j < active ? int(bva[g + j]) : 0;
+    }
+    const Fr w = load(lo + r);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[j][k] += int32_t(w.c[k]) * v[j];
+  }
+  for (int o = tpr; o < 32; o <<= 1)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+  const int warp = threadIdx.x >> 5, lane_id = threadIdx.x & 31;
+  if (lane_id < tpr)
+    for (int j = 0; j < lpt; ++j)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) part_s[warp][lane_id * lpt + j][k] = acc[j][k];
   __syncthreads();
   if (threadIdx.x < lanes) {
     int64_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int p = 0; p < phases; ++p)
+    for (int w = 0; w < kTermThreads / 32; ++w)
 #pragma unroll
-      for (int k = 0; k < 8; ++k) s[k] += acc_s[p * lanes + threadIdx.x][k];
+      for (int k = 0; k < 8; ++k) s[k] += part_s[w][threadIdx.x][k];
     Fr sum;
 #pragma unroll
     for (int k = 0; k < 8; ++k) sum.c[k] = mod_i64(s[k]);
-    store(out + size_t(blockIdx.x) * lanes + threadIdx.x, mul(load(&t.hi), sum));
+    store(out + size_t(blockIdx.x) * lanes + threadIdx.x, mul(tile_high(T, tables, i), sum));
   }
 }
 
@@ -160,21 +236,21 @@ __global__ void k_eo_witness(const int8_t* __restrict__ bva, uint64_t active, ui
 }
 
 // Query-fold tile of a large term: q[start + r] (=|+=) hi * lo[r], r < rows.
-struct QueryTile {
-  uint64_t start;
-  uint32_t rows;
-  uint32_t lo_off;
-  Fe hi;
-};
-__global__ void k_query_tiles(const QueryTile* __restrict__ tiles, const Fe* __restrict__ lo_tables, int accumulate,
+// Query fold of large terms (tbv.rs:393-428): q[offset + row] += high(tile) *
+// lo[r] for the rows of each tile.  Terms within one launch are disjoint.
+__global__ void k_query_terms(const TermTiles* __restrict__ terms, int n_terms, const Fe* __restrict__ tables,
                               Fe* __restrict__ q) {
-  const QueryTile t = tiles[blockIdx.x];
-  const Fr hi = load(&t.hi);
-  for (uint32_t r = threadIdx.x; r < t.rows; r += blockDim.x) {
-    Fr v = mul(hi, load(lo_tables + t.lo_off + r));
-    if (accumulate) v = add(v, load(q + t.start + r));
-    store(q + t.start + r, v);
-  }
+  __shared__ int t_sel;
+  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, blockIdx.x);
+  __syncthreads();
+  const TermTiles T = terms[t_sel];
+  const uint64_t i = blockIdx.x - T.first_tile;
+  const uint64_t row0 = i << T.lb;
+  const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
+  const uint32_t nrows = uint32_t(left < span ? left : span);
+  const Fr hi = tile_high(T, tables, i);
+  Fe* dst = q + T.offset + row0;
+  for (uint32_t r = threadIdx.x; r < nrows; r += blockDim.x) store(dst + r, add(load(dst + r), mul(hi, load(tables + T.lo_off + r))));
 }
 __global__ void k_scatter_add(const uint64_t* __restrict__ idx, const Fe* __restrict__ vals, uint32_t n, Fe* __restrict__ q) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
