@@ -48,17 +48,6 @@ void DevicePool::trim() {
 }
 
 bool KernelClock::enabled = false;
-namespace {
-std::map<std::string, std::pair<uint64_t, double>> g_host_sections;
-}
-HostScope::~HostScope() {
-  if (!KernelClock::enabled) return;
-  double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-  std::lock_guard<std::mutex> g(KernelClock::mu);
-  auto& e = g_host_sections[name];
-  e.first += 1;
-  e.second += ms;
-}
 std::mutex KernelClock::mu;
 std::vector<KernelClock::Rec> KernelClock::recs;
 std::atomic<uint64_t> KernelClock::launches{0};
@@ -82,7 +71,7 @@ void KernelClock::reset(bool on) {
   std::lock_guard<std::mutex> g(mu);
   for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   recs.clear();
-  g_host_sections.clear();
+  ::qf::Sections::reset(on);
   enabled = on;
 }
 std::string KernelClock::stats_json() {
@@ -108,7 +97,8 @@ std::string KernelClock::stats_json() {
                   (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
     s += buf;
   }
-  for (auto& [k, v] : g_host_sections) {
+  std::lock_guard<std::mutex> gs(::qf::Sections::mu);
+  for (auto& [k, v] : ::qf::Sections::totals) {
     if (!first) s += ",";
     first = false;
     char buf[256];
@@ -254,7 +244,8 @@ static void configure_tile_kernels() {
   const size_t bytes = qfd::kTileSmem;
   set_smem(qfd::k_pack_mobius_tile, bytes);
   set_smem(qfd::k_copy_mobius_tile, bytes);
-  set_smem(qfd::k_wht_tile, bytes);
+  set_smem(qfd::k_wht_tile<false>, bytes);
+  set_smem(qfd::k_wht_tile<true>, bytes);
   set_smem(qfd::k_butterfly_strided<qfd::kMobius>, bytes);
   set_smem(qfd::k_butterfly_strided<qfd::kWht>, bytes);
   done.insert(dev);
@@ -274,6 +265,16 @@ void GpuBackend::ensure_alpha() {
   const auto& top = P_.pcs.pp->seq.top();
   alpha1_.alloc(top.message_len);
   QF_CK(cudaMemcpyAsync(alpha1_.p, top.alphas[1].data(), top.message_len * 16, cudaMemcpyHostToDevice, s_));
+}
+
+// The first min(12, logR) WHT levels of a 2^logm-entry half, optionally
+// multiplying by alpha first (a CTA size per variant).
+static void wht_tile_launch(cudaStream_t s, const Fe* src, Fe* dst, const Fe* alpha, int logR, int logm, int wl) {
+  const unsigned grid = unsigned(size_t(1) << (logm - wl));
+  if (alpha)
+    qfd::k_wht_tile<true><<<grid, qfd::kAlphaTileThreads, qfd::kTileSmem, s>>>(src, dst, alpha, logR, wl);
+  else
+    qfd::k_wht_tile<false><<<grid, qfd::kTileThreads, qfd::kTileSmem, s>>>(src, dst, nullptr, logR, wl);
 }
 
 // Butterfly levels [from, to) over a half (message or parity at `base`) of
@@ -299,13 +300,11 @@ void GpuBackend::mobius_rest(Fe* cw, int logm, int logR, int from) { strided_pas
 void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain) {
   const size_t R = size_t(1) << logR;
   const int wl = std::min(qfd::kMaxTileLog, logR);
-  const size_t tsmem = qfd::kTileSmem;
   Fe* msg = out.cw.p;
   Fe* par = out.cw.p + R;
   for (int pass = 0; pass < 2; ++pass) {
     QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logm) * 16,
-              qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), qfd::kTileThreads, tsmem, s_>>>(
-                  pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, wl));
+              wht_tile_launch(s_, pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, logm, wl));
     strided_passes<qfd::kWht>(s_, par, logR, logm, wl, logR);
   }
   // Leaves and inner levels.
@@ -407,8 +406,7 @@ void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t act
   // Parity half: WHT(alpha * WHT(message)) per column.
   const int wl = std::min(qfd::kMaxTileLog, logR);
   for (int pass = 0; pass < 2; ++pass) {
-    qfd::k_wht_tile<<<unsigned(size_t(1) << (logm - wl)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
-        pass == 0 ? cw : cw + R, cw + R, pass == 0 ? nullptr : alpha, logR, wl);
+    wht_tile_launch(s, pass == 0 ? cw : cw + R, cw + R, pass == 0 ? nullptr : alpha, logR, logm, wl);
     QF_CK(cudaGetLastError());
     strided_passes_plain<qfd::kWht>(s, cw + R, logR, logm, wl, logR);
   }
@@ -462,10 +460,14 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   QF_LAUNCH(s_, "k_table", m * 16, qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, weights_.p));
   DBuf<unsigned long long> raw(64 * nblocks);
   QF_CK(cudaMemsetAsync(raw.p, 0, 64 * nblocks * 8, s_));
-  for (size_t b = 0; b < nblocks; ++b) {
-    if (b * P_.block_len >= active_) continue;  // zero block: all lanes vanish
-    QF_LAUNCH(s_, "k_eq_project", m * 24, qfd::k_eq_project<<<grid_for(m * 8, qfd::kProjThreads), qfd::kProjThreads, 0, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
-                                                                                        m, weights_.p, raw.p + 64 * b));
+  // Zero blocks (the suffix past the active entries) have vanishing lanes.
+  const size_t live = std::min<size_t>(nblocks, (active_ + P_.block_len - 1) / P_.block_len);
+  const unsigned grid = unsigned(std::min<uint64_t>((m + qfd::kEqChunk - 1) / qfd::kEqChunk, 148 * 4));
+  for (size_t b0 = 0; b0 < live; b0 += qfd::kEqBlocks) {
+    const int nb = int(std::min<size_t>(qfd::kEqBlocks, live - b0));
+    QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * 8 * uint64_t(nb),
+              qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva_, active_, P_.block_len, b0, nb, m, weights_.p,
+                                                                         raw.p + 64 * b0));
   }
   std::vector<unsigned long long> h(64 * nblocks);
   QF_CK(cudaMemcpyAsync(h.data(), raw.p, h.size() * 8, cudaMemcpyDeviceToHost, s_));
@@ -899,8 +901,7 @@ void GpuBackend::tensor_table(const std::vector<F>& point, DBuf<Fe>& out) {
 // multiplying by alpha first (one tile pass, then strided passes).
 void GpuBackend::wht_dev(Fe* v, int logn, const Fe* alpha) {
   const int wl = std::min(qfd::kMaxTileLog, logn);
-  QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logn) * 16,
-            qfd::k_wht_tile<<<unsigned(size_t(1) << (logn - wl)), qfd::kTileThreads, qfd::kTileSmem, s_>>>(v, v, alpha, logn, wl));
+  QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logn) * 16, wht_tile_launch(s_, v, v, alpha, logn, logn, wl));
   strided_passes<qfd::kWht>(s_, v, logn, logn, wl, logn);
 }
 
@@ -1097,12 +1098,14 @@ RoundOutput<F> GpuBackend::prove_top_round(const PcsParams<F>& pp, size_t level,
 
 // MultiEval over one level's alpha columns (qafold_short_decide.rs:466-536)
 // with the row vectors in HBM, followed by the direct-interleaved block fold.
-MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
-                                              size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) {
-  HostScope hs("decide_multi_eval");
+bool GpuBackend::multi_eval(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
+                            const std::vector<F>* carry_message, size_t log_rows, size_t log_cols, size_t row_factor,
+                            PcsTranscript<F>& t, MultiEvalOut<F>& out) {
   const QaCode<F>& code = pp.seq.codes[level];
   const uint64_t rows = uint64_t(1) << log_rows;
-  const size_t real = code.alphas.size();
+  if (rows < 1024 || code.alphas.size() > 2) return false;
+  HostScope hs("decide_multi_eval");
+  const size_t real = code.alphas.size() + (carry_message ? 1 : 0);
   if (rows != code.message_len) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "multi-eval rows");
   validate_multi_eval(claims, real, log_rows, log_cols);
   absorb_multi_eval_statement(claims, log_rows, log_cols, t);
@@ -1110,7 +1113,16 @@ MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t lev
   std::vector<DBuf<Fe>> row_w(claims.size());
   for (size_t i = 0; i < claims.size(); ++i) tensor_table(claims[i].row_point, row_w[i]);
   std::vector<const Fe*> col(real);
-  for (size_t sidx = 0; sidx < real; ++sidx) col[sidx] = level_alpha(level, int(sidx));
+  for (size_t sidx = 0; sidx < code.alphas.size(); ++sidx) col[sidx] = level_alpha(level, int(sidx));
+  DBuf<Fe> carry_d;
+  if (carry_message) {
+    // Entries past the carried message's length count as zero.
+    if (carry_message->size() > rows) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "carry message length");
+    carry_d.alloc(rows);
+    QF_CK(cudaMemsetAsync(carry_d.p, 0, rows * 16, s_));
+    QF_CK(cudaMemcpyAsync(carry_d.p, carry_message->data(), carry_message->size() * 16, cudaMemcpyHostToDevice, s_));
+    col[real - 1] = carry_d.p;
+  }
   std::vector<std::vector<F>> se(claims.size(), std::vector<F>(real));
   for (size_t i = 0; i < claims.size(); ++i)
     for (size_t sidx = 0; sidx < real; ++sidx) se[i][sidx] = dot_dev(row_w[i].p, col[sidx], rows);
@@ -1130,7 +1142,7 @@ MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t lev
   a_point.insert(a_point.end(), lb.a_point.begin(), lb.a_point.end());
   b_point.insert(b_point.end(), lb.b_point.begin(), lb.b_point.end());
   F ew = expected_weight_eval(claims, mc.powers, log_cols, b_point);
-  MultiEvalOut<F> out;
+  out = MultiEvalOut<F>();
   out.ok = (lb.a_value * lb.b_value == lb_rhs_) && (lb.b_value == ew);
   out.reduced = {lb.a_value, a_point};
   // Block fold at the first log2(row_factor) coordinates of the merged row point.
@@ -1145,7 +1157,7 @@ MultiEvalOut<F> GpuBackend::multi_eval_alphas(const PcsParams<F>& pp, size_t lev
   out.folded_vector.resize(trows);
   QF_CK(cudaMemcpyAsync(out.folded_vector.data(), rec.p, trows * 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
-  return out;
+  return true;
 }
 
 // prove_short_qa_direct_code_switch_carry (qafold_short_decide_carry.rs:940-1027)

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "host/protocol.h"
+#include "host/sections.h"
 #include "device/f65521_dev.cuh"
 #include "device/hash_prefix.h"
 
@@ -49,12 +50,7 @@ struct KernelClock {
 };
 
 // Host wall time of named sections (recorded while KernelClock is enabled).
-struct HostScope {
-  const char* name;
-  std::chrono::steady_clock::time_point t0;
-  explicit HostScope(const char* n) : name(n), t0(std::chrono::steady_clock::now()) {}
-  ~HostScope();
-};
+using HostScope = ::qf::Section;
 
 #define QF_LAUNCH(stream, name, bytes, ...)     \
   do {                                          \
@@ -187,9 +183,11 @@ class GpuBackend : public Backend<F>,
     opening = open_top(*dc, point, col_log);
     return true;
   }
-  // First Decide round (alpha columns only) with the row vectors in HBM.
-  MultiEvalOut<F> multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
-                                    size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) override;
+  // Decide MultiEval (alpha columns, plus the carried message) with the row
+  // vectors in HBM; declines below 1024 rows.
+  bool multi_eval(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
+                  const std::vector<F>* carry_message, size_t log_rows, size_t log_cols, size_t row_factor,
+                  PcsTranscript<F>& t, MultiEvalOut<F>& out) override;
   bool direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
                      const std::vector<F>& iota, const std::vector<F>& folded_message, F merged_value,
                      const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) override;

@@ -685,16 +685,19 @@ std::optional<SwitchCarry<F>> verify_direct_switch(const QaCode<F>& target, size
 }
 
 // ------------------------------------------------------------ prove / verify
-// Runs a MultiEval whose columns are exactly one level's alpha columns (the
-// first Decide round, which has no carry) with the row vectors on a device.
-// Same transcript as prove_multi_eval; `folded_vector` is returned already
-// block-folded at the reduced point's first log2(row_factor) coordinates
-// (fold_short_direct_interleaved_witness), i.e. rows / row_factor entries.
+// Runs a MultiEval over one level's alpha columns, plus the carried message
+// as the last column when `carry_message` is given, with the row vectors on
+// a device.  Same transcript as prove_multi_eval; `folded_vector` is returned
+// already block-folded at the reduced point's first log2(row_factor)
+// coordinates (fold_short_direct_interleaved_witness), i.e. rows / row_factor
+// entries.  Returns false, before touching the transcript, to leave a small
+// MultiEval on the host.
 template <class F>
 struct DecideAccel {
   virtual ~DecideAccel() {}
-  virtual MultiEvalOut<F> multi_eval_alphas(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
-                                            size_t log_rows, size_t log_cols, size_t row_factor, PcsTranscript<F>& t) = 0;
+  virtual bool multi_eval(const PcsParams<F>& pp, size_t level, const std::vector<EvalClaim<F>>& claims,
+                          const std::vector<F>* carry_message, size_t log_rows, size_t log_cols, size_t row_factor,
+                          PcsTranscript<F>& t, MultiEvalOut<F>& out) = 0;
   // prove_direct_switch with its message-length vectors on the device;
   // returns false to keep the (small) switch on the host.
   virtual bool direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
@@ -708,7 +711,11 @@ template <class F>
 DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, DecideAccel<F>* accel = nullptr) {
   const size_t L = pp.levels();
   PcsTranscript<F> t;
-  auto h = prepare_pending_h(pp, red, t);
+  std::vector<std::vector<MatrixClaim<F>>> h;
+  {
+    Section sec("decide_pending_h");
+    h = prepare_pending_h(pp, red, t);
+  }
   DecideProof<F> proof;
   if (L <= 1) {
     for (auto& v : h) if (!v.empty()) fail(QF_E_INVALID_COMMITMENT, "base-level claims");
@@ -732,9 +739,13 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, Dec
     std::vector<const std::vector<F>*> cols;
     for (const auto& a : code.alphas) cols.push_back(&a);
     if (carry) cols.push_back(&carry->message);
-    const bool on_device = accel && !carry;
-    MultiEvalOut<F> me = on_device ? accel->multi_eval_alphas(pp, level, claims, ps.log_rows, ps.log_cols, pp.seq.switch_ratio, t)
-                                   : prove_multi_eval(claims, cols, ps.log_rows, ps.log_cols, t);
+    MultiEvalOut<F> me;
+    const bool on_device = accel && accel->multi_eval(pp, level, claims, carry ? &carry->message : nullptr, ps.log_rows,
+                                                      ps.log_cols, pp.seq.switch_ratio, t, me);
+    if (!on_device) {
+      Section sec("decide_multi_eval_host");
+      me = prove_multi_eval(claims, cols, ps.log_rows, ps.log_cols, t);
+    }
     if (!me.ok || me.reduced.point.size() != ps.log_cols + ps.log_rows) fail(QF_E_INVALID_COMMITMENT, "multi-eval");
     std::vector<F> col_point(me.reduced.point.begin(), me.reduced.point.begin() + ps.log_cols);
     std::vector<F> merged_left(me.reduced.point.begin() + ps.log_cols, me.reduced.point.end());
@@ -747,13 +758,20 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, Dec
     RowSelection sel = make_selection(qc, n_enc, seed);
     DecideRound<F> round;
     round.level = level;
-    round.setup_rows = open_setup_rows(sl, sel);
-    if (carry) round.carry_rows = open_codeword_rows(carry->cw, sel);
+    {
+      Section sec("decide_open_rows");
+      round.setup_rows = open_setup_rows(sl, sel);
+      if (carry) round.carry_rows = open_codeword_rows(carry->cw, sel);
+    }
     std::vector<F> iw = iota_weights(col_w, ps.setup_cols, ps.carry_cols, merged_left, rf);
     size_t auth_carry_cols = ps.carry_cols * rf;
     if (iw.size() != next_pow2(sl.shape.total_cols() + auth_carry_cols)) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "iota weights");
     absorb_iota_statement(t, level, sl, carry_root, auth_carry_cols, sel, iw);
-    std::vector<F> iota = compute_iota(sl, round.setup_rows, round.carry_rows, auth_carry_cols, sel, iw);
+    std::vector<F> iota;
+    {
+      Section sec("decide_iota");
+      iota = compute_iota(sl, round.setup_rows, round.carry_rows, auth_carry_cols, sel, iw);
+    }
     for (const F& v : iota) t.push_response(v);
     // Fold the block coordinate of the logical witness.
     const size_t trows = target.message_len;
@@ -778,6 +796,7 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, Dec
       if (trows != nt.message_len * rf) fail(QF_E_ENCODING, "carry rows");
       next_carry = std::make_unique<Carry<F>>();
       next_carry->message = recursive;
+      Section sec("decide_carry_commit");
       next_carry->cw = encode_and_commit(nt, recursive, rf, kLeafExtDomain);
       next_root = next_carry->cw.root();
     } else {
@@ -786,8 +805,10 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, Dec
     absorb_next_carry(t, next_root);
     const std::vector<F>& folded_for_switch = next_carry ? next_carry->message : terminal;
     SwitchCarry<F> sc;
-    if (!(accel && accel->direct_switch(target, level - 1, rf, sel, iota, folded_for_switch, me.reduced.value, merged_left, t, sc)))
+    if (!(accel && accel->direct_switch(target, level - 1, rf, sel, iota, folded_for_switch, me.reduced.value, merged_left, t, sc))) {
+      Section sec("decide_switch_host");
       sc = prove_direct_switch(target, level - 1, rf, sel, iota, folded_for_switch, me.reduced.value, merged_left, t);
+    }
     if (level > 1) {
       h[level - 1].push_back(reduce_generator_claim(target.message_len, target.index, sc.generator_claim));
       w_claim = sc.folded_w;

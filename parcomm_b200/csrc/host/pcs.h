@@ -15,6 +15,7 @@
 #include "field65521.h"
 #include "merkle.h"
 #include "qacode.h"
+#include "sections.h"
 
 namespace qf {
 
@@ -786,8 +787,13 @@ OpenResult<F> open_with_reduction(const PcsParams<F>& pp, const CodewordView<F>&
     }
     std::vector<F> cw_pt(next_point.begin(), next_point.begin() + col_log);
     if (inner_product(opening_vec, tensor_weights(cw_pt)) != next_value) fail(QF_E_INVALID_COMMITMENT, "extension opening");
-    RoundOutput<F> r = on_device ? accel->prove_top_round(pp, level, next_point, opening_vec, t)
-                                 : prove_round(pp, level, *prepared, next_point, opening_vec, rw, t);
+    RoundOutput<F> r;
+    if (on_device) {
+      r = accel->prove_top_round(pp, level, next_point, opening_vec, t);
+    } else {
+      Section sec("opening_round_host");
+      r = prove_round(pp, level, *prepared, next_point, opening_vec, rw, t);
+    }
     res.proof.ext_rounds.push_back(ExtRound<F>{prepared->root(), std::move(r.rows)});
     if (level == 0) {
       if (evaluate_generator_mle(code, r.reduction.generator_left_point, r.reduction.generator_right_point) !=

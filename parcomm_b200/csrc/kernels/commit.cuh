@@ -37,7 +37,8 @@ enum ButterflyOp { kMobius = 0, kWht = 1 };
 // values: a value entering level l of a pass is < 2^l * p, a difference is
 // formed as a + 2^l p - b, so twelve levels stay below 2^28 and one
 // reduction per pass suffices.  Both transforms act coefficient-wise over F_p.
-constexpr int kTileThreads = 512;
+constexpr int kTileThreads = 512;       // CTA size of the tile kernels
+constexpr int kAlphaTileThreads = 512;  // the WHT tile that multiplies by alpha
 constexpr int kMaxTileLog = 12;                 // 4096 elements per tile
 constexpr int kPlane = 1 << kMaxTileLog;        // plane stride (words)
 constexpr size_t kTileSmem = size_t(8) * kPlane * 4;  // 128 KiB
@@ -74,24 +75,31 @@ __device__ __forceinline__ uint4 planar_get_packed(const uint32_t* planes, int e
 }
 
 // One radix-2^R register stage: levels [lvl, lvl + R) of the pass, acting on
-// tile bits [b, b + R).  A thread takes a group of 2^R elements and runs it
-// through all 8 coefficient planes; the group's plane offsets are computed
-// once (pidx is XOR-linear over the disjoint base and level bits).
+// tile bits [b, b + R).  A work item is a group of 2^R elements and a run of
+// coefficient planes (all 8, or fewer when the CTA has more threads than
+// groups); its plane offsets are computed once (pidx is XOR-linear over the
+// disjoint base and level bits).  Consecutive threads take consecutive groups
+// of the same planes.
 template <int OP, int R>
 __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b, int lvl) {
-  const int groups = 1 << (log_n - R);
+  const int lg = log_n - R;
+  int split = 0;
+  while (split < 3 && (1 << (lg + split)) < int(blockDim.x)) ++split;
+  const int ppi = 8 >> split;  // planes per item
   const int bmask = (1 << b) - 1;
   int off[1 << R];
 #pragma unroll
   for (int j = 0; j < (1 << R); ++j) off[j] = pidx(j << b);
-  for (int g = threadIdx.x; g < groups; g += blockDim.x) {
+  for (int item = threadIdx.x; item < (1 << (lg + split)); item += blockDim.x) {
+    const int g = item & ((1 << lg) - 1), c0 = (item >> lg) * ppi;
     const int pb = pidx((g & bmask) | ((g & ~bmask) << R));
     int q[1 << R];
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) q[j] = pb ^ off[j];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      uint32_t* pl = planes + c * kPlane;
+    for (int cc = 0; cc < 8; ++cc) {
+      if (cc >= ppi) break;
+      uint32_t* pl = planes + (c0 + cc) * kPlane;
       uint32_t v[1 << R];
 #pragma unroll
       for (int j = 0; j < (1 << R); ++j) v[j] = pl[q[j]];
@@ -129,7 +137,7 @@ __device__ __forceinline__ void planar_levels(uint32_t* planes, int log_n, int b
 // Gathers the n tile elements src[addr(t)] (times alpha[addr(t) & amask] when
 // alpha is given) into the planes.  Each thread issues up to kBatch 16-byte loads
 // before it writes shared memory, so a tile's loads are in flight together.
-constexpr int kBatch = 8;
+constexpr int kBatch = 4;
 template <class Addr>
 __device__ __forceinline__ void tile_gather(uint32_t* planes, int n, const Fe* src, Addr addr, const Fe* __restrict__ alpha,
                                             size_t amask) {
@@ -209,17 +217,18 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* 
 }
 
 // WHT levels [0, levels) within a tile (levels <= logR so columns never mix).
-// Reads the message (or parity) half at src, optionally multiplies each row by
-// alpha[r] first, writes the parity half (src may equal dst: a CTA reads its
-// whole tile before it writes).
-__global__ void __launch_bounds__(kTileThreads, 1) k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR,
-                                                             int levels) {
+// Reads the message (or parity) half at src, with ALPHA multiplies each row
+// by alpha[r] first, writes the parity half (src may equal dst: a CTA reads
+// its whole tile before it writes).
+template <bool ALPHA>
+__global__ void __launch_bounds__(ALPHA ? kAlphaTileThreads : kTileThreads, 1)
+    k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR, int levels) {
   extern __shared__ uint32_t planes_s[];
   const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
   // For a message-half address a = c * 2R + r, a & (R - 1) = r.
   const size_t rmask = (size_t(1) << logR) - 1;
-  tile_gather(planes_s, n, src, [=](int t) { return msg_addr(first + t, logR); }, alpha, rmask);
+  tile_gather(planes_s, n, src, [=](int t) { return msg_addr(first + t, logR); }, ALPHA ? alpha : nullptr, rmask);
   planar_levels<kWht>(planes_s, levels, 0, levels);
   tile_scatter(planes_s, n, dst, [=](int t) { return msg_addr(first + t, logR); });
 }

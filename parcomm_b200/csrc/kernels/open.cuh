@@ -309,51 +309,85 @@ __global__ void k_table(const Fe* __restrict__ hi, const Fe* __restrict__ lo, in
     store(out + i, table_at(hi, lo, lb, i));
 }
 
-// Raw lane sums of one block against the equality weights
-// (project_lanes_from_fn, packed_batch.rs:25-41):
-//   raw[j * 8 + k] += sum_i v(b, 8i + j) * weights[i].c[k]
-// Eight threads share an element, one lane j each.
-constexpr int kProjThreads = 256;
-__global__ void __launch_bounds__(kProjThreads) k_eq_project(const int8_t* __restrict__ bva, uint64_t active,
-                                                            uint64_t block_base, uint64_t m, const Fe* __restrict__ weights,
-                                                            unsigned long long* __restrict__ raw) {
-  __shared__ int64_t warp_s[kProjThreads / 32][32][8];
-  const int j = threadIdx.x & 7;
-  int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int64_t tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int count = 0;
-  const uint64_t stride = (uint64_t(gridDim.x) * blockDim.x) >> 3;
-  for (uint64_t i = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 3; i < m; i += stride) {
-    const uint64_t g = block_base + 8 * i + j;
-    const int v = g < active ? int(bva[g]) : 0;
-    if (v) {
-      Fr w = load(weights + i);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc[k] += v * int32_t(w.c[k]);
-    }
-    if (++count == 64) {  // 64 * 128 * 65520 < 2^31
-#pragma unroll
-      for (int k = 0; k < 8; ++k) { tot[k] += acc[k]; acc[k] = 0; }
-      count = 0;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    tot[k] += acc[k];
-    tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], 8);
-    tot[k] += __shfl_xor_sync(0xffffffffu, tot[k], 16);
-  }
+// Raw lane sums of up to kEqBlocks consecutive blocks against the equality
+// weights (project_lanes_from_fn, packed_batch.rs:25-41):
+//   raw[b][j * 8 + k] += sum_i v(b, 8i + j) * weights[i].c[k]
+// A CTA stages a chunk of kEqChunk weights in shared memory and runs every
+// block over it, so the table is read from HBM once for all blocks.  A thread
+// takes 8 elements per block (one 8-byte load each) into 64 i32 sums; a warp
+// reduce-scatter leaves lane l with entries 2l and 2l + 1 (each a sum of 256
+// products, |sum| <= 256 * 128 * 65520 < 2^31), and the CTA keeps i64 totals
+// per block that reach `raw` with one atomic add per entry at the end.
+constexpr int kEqThreads = 256, kEqChunk = 2048, kEqBlocks = 8;
+__global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_t* __restrict__ bva, uint64_t active,
+                                                                    uint64_t block_len, uint64_t first_block, int nb,
+                                                                    uint64_t m, const Fe* __restrict__ weights,
+                                                                    unsigned long long* __restrict__ raw) {
+  __shared__ uint4 w_s[kEqChunk];
+  __shared__ int32_t stage_s[kEqThreads / 32][64];
+  __shared__ long long tot_s[kEqBlocks][64];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane < 8)
+  for (int t = threadIdx.x; t < kEqBlocks * 64; t += kEqThreads) tot_s[t >> 6][t & 63] = 0;
+  for (uint64_t c0 = uint64_t(blockIdx.x) * kEqChunk; c0 < m; c0 += uint64_t(gridDim.x) * kEqChunk) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kEqChunk; e += kEqThreads)
+      w_s[e] = c0 + e < m ? *reinterpret_cast<const uint4*>(weights + c0 + e) : make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    for (int b = 0; b < nb; ++b) {
+      const uint64_t bbase = (first_block + b) * block_len;
+      int32_t acc[64];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) warp_s[warp][lane][k] = tot[k];
-  __syncthreads();
-  if (threadIdx.x < 64) {
-    const int jj = threadIdx.x >> 3, kk = threadIdx.x & 7;
-    int64_t s = 0;
-    for (int w = 0; w < kProjThreads / 32; ++w) s += warp_s[w][jj][kk];
-    atomicAdd(raw + threadIdx.x, (unsigned long long)s);  // two's complement sum
+      for (int q = 0; q < 64; ++q) acc[q] = 0;
+#pragma unroll 2
+      for (int u = 0; u < kEqChunk / kEqThreads; ++u) {
+        const int e = threadIdx.x + u * kEqThreads;
+        const uint64_t g = bbase + 8 * (c0 + e);
+        uint2 v8 = make_uint2(0, 0);
+        if (c0 + e < m) {
+          if (g + 8 <= active) {
+            v8 = *reinterpret_cast<const uint2*>(bva + g);
+          } else {
+            uint32_t w[2] = {0, 0};
+            for (int j = 0; j < 8; ++j)
+              if (g + j < active) w[j >> 2] |= uint32_t(uint8_t(bva[g + j])) << (8 * (j & 3));
+            v8 = make_uint2(w[0], w[1]);
+          }
+        }
+        const uint4 wq = w_s[e];
+        const uint32_t wc[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int v = int(int8_t(((j < 4 ? v8.x : v8.y) >> (8 * (j & 3))) & 0xffu));
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc[j * 8 + k] += v * int32_t((wc[k >> 1] >> (16 * (k & 1))) & 0xffffu);
+        }
+      }
+      // Reduce-scatter over the warp: after offset o the lane keeps the half
+      // of its entries selected by (lane & o).
+#pragma unroll
+      for (int o = 16, n = 64; o >= 1; o >>= 1, n >>= 1) {
+        const bool upper = lane & o;
+#pragma unroll
+        for (int q = 0; q < n / 2; ++q) {
+          const int32_t send = upper ? acc[q] : acc[q + n / 2];
+          const int32_t keep = upper ? acc[q + n / 2] : acc[q];
+          acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      stage_s[warp][2 * lane] = acc[0];
+      stage_s[warp][2 * lane + 1] = acc[1];
+      __syncthreads();
+      if (threadIdx.x < 64) {
+        long long t = 0;
+#pragma unroll
+        for (int w = 0; w < kEqThreads / 32; ++w) t += stage_s[w][threadIdx.x];
+        tot_s[b][threadIdx.x] += t;
+      }
+      __syncthreads();
+    }
   }
+  for (int t = threadIdx.x; t < nb * 64; t += kEqThreads)
+    atomicAdd(raw + t, (unsigned long long)tot_s[t >> 6][t & 63]);  // two's complement sum
 }
 
 // w <- sum_j w.c[j] * images[j]  (apply_weight_images, packed.rs:634-650).
