@@ -125,6 +125,7 @@ int qf_params_new(int field, const qf_shape* shapes, size_t n_shapes, const qf_c
     c.packed_log = config->packed_log;
     c.query_rf_bits = config->query_rf_bits;
     auto p = std::make_unique<qf_params>();
+    p->tables = std::make_shared<qfg::DeviceTables>();
     p->field = field;
     p->P = make_parameters<F>(sh, c);
     *out = p.release();
@@ -186,7 +187,7 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
       QF_CK(cudaStreamSynchronize(c->stream));
       check(h == 0, "nonzero boundary padding");
     }
-    c->be = std::make_unique<GpuBackend>(P, c->bva.p, n_values, c->stream);
+    c->be = std::make_unique<GpuBackend>(P, c->bva.p, n_values, c->stream, params->tables.get());
     for (size_t b = 0; b < P.blocks(); ++b) c->roots.push_back(c->be->commit_block(b));
     QF_CK(cudaStreamSynchronize(c->stream));
     c->commit_ms = ms_since(t0);

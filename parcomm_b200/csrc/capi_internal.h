@@ -11,9 +11,14 @@
 
 #include "host/protocol.h"
 
+namespace qfg {
+class DeviceTables;
+}
+
 struct qf_params {
   int field = 0;
   std::unique_ptr<qf::Parameters<qf::Fp8>> P;
+  std::shared_ptr<qfg::DeviceTables> tables;  // device code tables shared by its commitments
 };
 
 namespace qfc {

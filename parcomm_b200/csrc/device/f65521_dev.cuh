@@ -8,6 +8,9 @@
 #pragma once
 #include <cstdint>
 
+// Host-callable too, so the arithmetic can be checked against the host field on a CPU.
+#define QFD_HD __host__ __device__ __forceinline__
+
 namespace qfd {
 
 constexpr uint32_t P = 65521u;
@@ -21,20 +24,20 @@ struct Fr {
   uint32_t c[8];
 };
 
-__device__ __forceinline__ uint32_t red32(uint32_t v) {
+QFD_HD uint32_t red32(uint32_t v) {
   uint32_t f = (v & 0xffffu) + 15u * (v >> 16);
   f = (f & 0xffffu) + 15u * (f >> 16);
   return f >= P ? f - P : f;
 }
-__device__ __forceinline__ uint32_t red64(uint64_t v) {  // v < 2^48
+QFD_HD uint32_t red64(uint64_t v) {  // v < 2^48
   uint64_t f = (v & 0xffffu) + 15ull * (v >> 16);
   uint32_t g = uint32_t((f & 0xffffu) + 15ull * (f >> 16));
   return red32(g);
 }
-__device__ __forceinline__ uint32_t addp(uint32_t a, uint32_t b) { uint32_t s = a + b; return s >= P ? s - P : s; }
-__device__ __forceinline__ uint32_t subp(uint32_t a, uint32_t b) { return a >= b ? a - b : a + P - b; }
+QFD_HD uint32_t addp(uint32_t a, uint32_t b) { uint32_t s = a + b; return s >= P ? s - P : s; }
+QFD_HD uint32_t subp(uint32_t a, uint32_t b) { return a >= b ? a - b : a + P - b; }
 
-__device__ __forceinline__ Fr load(const Fe* p) {
+QFD_HD Fr load(const Fe* p) {
   uint4 u = *reinterpret_cast<const uint4*>(p);
   Fr r;
   r.c[0] = u.x & 0xffffu; r.c[1] = u.x >> 16;
@@ -43,7 +46,7 @@ __device__ __forceinline__ Fr load(const Fe* p) {
   r.c[6] = u.w & 0xffffu; r.c[7] = u.w >> 16;
   return r;
 }
-__device__ __forceinline__ void store(Fe* p, const Fr& r) {
+QFD_HD void store(Fe* p, const Fr& r) {
   uint4 u;
   u.x = r.c[0] | (r.c[1] << 16);
   u.y = r.c[2] | (r.c[3] << 16);
@@ -51,33 +54,44 @@ __device__ __forceinline__ void store(Fe* p, const Fr& r) {
   u.w = r.c[6] | (r.c[7] << 16);
   *reinterpret_cast<uint4*>(p) = u;
 }
-__device__ __forceinline__ Fr zero() { Fr r; for (int i = 0; i < 8; ++i) r.c[i] = 0; return r; }
-__device__ __forceinline__ Fr add(const Fr& a, const Fr& b) { Fr r; for (int i = 0; i < 8; ++i) r.c[i] = addp(a.c[i], b.c[i]); return r; }
-__device__ __forceinline__ Fr sub(const Fr& a, const Fr& b) { Fr r; for (int i = 0; i < 8; ++i) r.c[i] = subp(a.c[i], b.c[i]); return r; }
-__device__ __forceinline__ Fr mul(const Fr& a, const Fr& b) {
-  // Low and high product halves accumulate separately; the high half is
-  // folded with X^8 = 17.  Each half-sum is < 8 * 65520^2 < 2^35.
-  uint64_t lo[8], hi[8];
+QFD_HD Fr zero() { Fr r; for (int i = 0; i < 8; ++i) r.c[i] = 0; return r; }
+QFD_HD Fr add(const Fr& a, const Fr& b) { Fr r; for (int i = 0; i < 8; ++i) r.c[i] = addp(a.c[i], b.c[i]); return r; }
+QFD_HD Fr sub(const Fr& a, const Fr& b) { Fr r; for (int i = 0; i < 8; ++i) r.c[i] = subp(a.c[i], b.c[i]); return r; }
+// v < 2^40 to canonical: two 2^16 = 15 folds (< 2^28 + 2^16, then < 2p) and
+// one conditional subtraction.
+QFD_HD uint32_t red40(uint64_t v) {
+  uint32_t f = uint32_t(v & 0xffffu) + 15u * uint32_t(v >> 16);
+  f = (f & 0xffffu) + 15u * (f >> 16);
+  return f >= P ? f - P : f;
+}
+QFD_HD Fr mul(const Fr& a, const Fr& b) {
+  // X^8 = 17: the wrap-around products take 17 * b_j (< 2^21, unreduced), so
+  // output coefficient k is one sum of eight products a_i * b'_j < 2^37,
+  // accumulated with 64-bit multiply-adds (< 2^40) and reduced once.
+  uint32_t b17[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) { lo[k] = 0; hi[k] = 0; }
+  for (int j = 0; j < 8; ++j) b17[j] = 17u * b.c[j];
+  uint64_t r[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r[k] = 0;
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-      uint32_t p = a.c[i] * b.c[j];
-      if (i + j < 8) lo[i + j] += p; else hi[i + j - 8] += p;
+      if (i + j < 8) r[i + j] += uint64_t(a.c[i]) * b.c[j];
+      else r[i + j - 8] += uint64_t(a.c[i]) * b17[j];
     }
-  Fr r;
+  Fr out;
 #pragma unroll
-  for (int k = 0; k < 8; ++k) r.c[k] = red64(lo[k] + 17ull * hi[k]);
-  return r;
+  for (int k = 0; k < 8; ++k) out.c[k] = red40(r[k]);
+  return out;
 }
-__device__ __forceinline__ Fr mul_base(const Fr& a, uint32_t s) {
+QFD_HD Fr mul_base(const Fr& a, uint32_t s) {
   Fr r;
   for (int i = 0; i < 8; ++i) r.c[i] = red32(a.c[i] * s);
   return r;
 }
 // small signed integer -> canonical F_65521 (field.rs:24-26)
-__device__ __forceinline__ uint32_t small(int v) { return v < 0 ? uint32_t(v + int(P)) : uint32_t(v); }
+QFD_HD uint32_t small(int v) { return v < 0 ? uint32_t(v + int(P)) : uint32_t(v); }
 
 }  // namespace qfd

@@ -4,6 +4,7 @@
 #include "kernels/open.cuh"
 #include "kernels/vec.cuh"
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <set>
@@ -96,6 +97,29 @@ std::string KernelClock::stats_json() {
     std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu}", k.c_str(),
                   (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
     s += buf;
+  }
+  // Idle time between consecutive recorded launches (in launch order), with
+  // the largest gaps named by the kernels on either side.
+  if (recs.size() > 1) {
+    struct Gap { double ms; const char* before; const char* after; };
+    std::vector<Gap> gaps;
+    double total = 0;
+    for (size_t i = 1; i < recs.size(); ++i) {
+      float ms = 0;
+      QF_CK(cudaEventElapsedTime(&ms, recs[i - 1].b, recs[i].a));
+      if (ms > 0) { gaps.push_back({ms, recs[i - 1].name, recs[i].name}); total += ms; }
+    }
+    std::sort(gaps.begin(), gaps.end(), [](const Gap& x, const Gap& y) { return x.ms > y.ms; });
+    if (!first) s += ",";
+    first = false;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "\"_gaps\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0,\"top\":[", (unsigned long long)gaps.size(), total);
+    s += buf;
+    for (size_t i = 0; i < gaps.size() && i < 40; ++i) {
+      std::snprintf(buf, sizeof buf, "%s[\"%s\",\"%s\",%.4f]", i ? "," : "", gaps[i].before, gaps[i].after, gaps[i].ms);
+      s += buf;
+    }
+    s += "]}";
   }
   std::lock_guard<std::mutex> gs(::qf::Sections::mu);
   for (auto& [k, v] : ::qf::Sections::totals) {
@@ -252,19 +276,27 @@ static void configure_tile_kernels() {
 }
 
 // ---------------------------------------------------------------- backend
-GpuBackend::GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s)
-    : P_(p), bva_(d_bva), active_(active), s_(s) {
+GpuBackend::GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s, DeviceTables* tables)
+    : P_(p), bva_(d_bva), active_(active), s_(s), tables_(tables ? tables : &own_tables_) {
   configure_tile_kernels();
   partials_.alloc(148 * 8 * 4);
   result_.alloc(8);
 }
 GpuBackend::~GpuBackend() {}
 
-void GpuBackend::ensure_alpha() {
-  if (alpha1_.p) return;
-  const auto& top = P_.pcs.pp->seq.top();
-  alpha1_.alloc(top.message_len);
-  QF_CK(cudaMemcpyAsync(alpha1_.p, top.alphas[1].data(), top.message_len * 16, cudaMemcpyHostToDevice, s_));
+const Fe* DeviceTables::alpha(const PcsParams<F>& pp, size_t level, int which) {
+  int dev = 0;
+  QF_CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu_);
+  auto key = std::make_tuple(dev, level, which);
+  auto it = bufs_.find(key);
+  if (it == bufs_.end()) {
+    const auto& a = pp.seq.codes.at(level).alphas.at(size_t(which));
+    DBuf<Fe> b(a.size());
+    QF_CK(cudaMemcpy(b.p, a.data(), a.size() * 16, cudaMemcpyHostToDevice));
+    it = bufs_.emplace(key, std::move(b)).first;
+  }
+  return it->second.p;
 }
 
 // The first min(12, logR) WHT levels of a 2^logm-entry half, optionally
@@ -365,8 +397,7 @@ Digest GpuBackend::commit_block(size_t b) {
   QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
                                                                                     cw->cw.p, logR, l0));
   mobius_rest(cw->cw.p, logm, logR, l0);
-  ensure_alpha();
-  encode_and_hash(*cw, alpha1_.p, logR, logm, false);
+  encode_and_hash(*cw, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
   if (blocks_.size() <= b) blocks_.resize(b + 1);
   roots_.resize(std::max(roots_.size(), b + 1));
   roots_[b] = cw->root_;
@@ -439,25 +470,36 @@ std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t cou
   return out;
 }
 
-// Two-level equality table of an MSB-first point: low coordinates index the
-// low table (equality_table, packed.rs:525-545).
-static void eq_tables(const std::vector<F>& point, std::vector<F>& hi, std::vector<F>& lo, int& lb) {
+// Device table of the 2^n weights of an MSB-first point, `weights` giving the
+// host table of a coordinate slice (equality_table, packed.rs:525-545, or
+// tensor_weights, qafold_short_pc.rs:2826-2855; both factor over slices).
+// The last <= 10 coordinates index a low table, the next <= 10 a middle
+// table and the rest a high table; the high x middle product is formed on the
+// device, then the full table.  Synchronises the stream before returning.
+template <class W>
+static void device_point_table(cudaStream_t s, const std::vector<F>& point, W weights, DBuf<Fe>& out) {
   const int n = int(point.size());
-  lb = std::min(10, n);
-  hi = equality_table(std::vector<F>(point.begin(), point.begin() + (n - lb)));
-  lo = equality_table(std::vector<F>(point.begin() + (n - lb), point.end()));
+  const int lb = std::min(10, n), mb = std::min(10, n - lb), hb = n - lb - mb;
+  std::vector<F> hi = weights(std::vector<F>(point.begin(), point.begin() + hb));
+  std::vector<F> mid = weights(std::vector<F>(point.begin() + hb, point.begin() + hb + mb));
+  std::vector<F> lo = weights(std::vector<F>(point.begin() + hb + mb, point.end()));
+  DBuf<Fe> dhi(hi.size()), dmid(mid.size()), dlo(lo.size()), upper(size_t(1) << (hb + mb));
+  QF_CK(cudaMemcpyAsync(dhi.p, hi.data(), hi.size() * 16, cudaMemcpyHostToDevice, s));
+  QF_CK(cudaMemcpyAsync(dmid.p, mid.data(), mid.size() * 16, cudaMemcpyHostToDevice, s));
+  QF_CK(cudaMemcpyAsync(dlo.p, lo.data(), lo.size() * 16, cudaMemcpyHostToDevice, s));
+  const uint64_t mu = uint64_t(1) << (hb + mb), m = uint64_t(1) << n;
+  QF_LAUNCH(s, "k_table", mu * 16, qfd::k_table<<<grid_for(mu, kThreads), kThreads, 0, s>>>(dhi.p, dmid.p, mb, mu, upper.p));
+  if (out.n != m) out.alloc(m);
+  QF_LAUNCH(s, "k_table", m * 16, qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s>>>(upper.p, dlo.p, lb, m, out.p));
+  QF_CK(cudaStreamSynchronize(s));
 }
+static std::vector<F> eq_slice(const std::vector<F>& p) { return equality_table(p); }
+static std::vector<F> tensor_slice(const std::vector<F>& p) { return tensor_weights(p); }
 
 std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& outer, size_t nblocks) {
   const uint64_t m = P_.pcs.packed_len();
-  std::vector<F> hi, lo;
-  int lb;
-  eq_tables(outer, hi, lo, lb);
-  DBuf<Fe> dhi(hi.size()), dlo(lo.size());
-  QF_CK(cudaMemcpyAsync(dhi.p, hi.data(), hi.size() * 16, cudaMemcpyHostToDevice, s_));
-  QF_CK(cudaMemcpyAsync(dlo.p, lo.data(), lo.size() * 16, cudaMemcpyHostToDevice, s_));
-  weights_.alloc(m);
-  QF_LAUNCH(s_, "k_table", m * 16, qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, weights_.p));
+  if (outer.size() != size_t(ilog2(m))) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "outer point");
+  device_point_table(s_, outer, eq_slice, weights_);
   DBuf<unsigned long long> raw(64 * nblocks);
   QF_CK(cudaMemsetAsync(raw.p, 0, 64 * nblocks * 8, s_));
   // Zero blocks (the suffix past the active entries) have vanishing lanes.
@@ -526,8 +568,7 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   const size_t smem = qfd::kTileSmem;
   QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0));
   mobius_rest(folded_->cw.p, logm, logR, l0);
-  ensure_alpha();
-  encode_and_hash(*folded_, alpha1_.p, logR, logm, false);
+  encode_and_hash(*folded_, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
   sum_len_ = m;
   msg_valid_ = false;
   return folded_->root_;
@@ -870,32 +911,11 @@ std::array<F, 2> GpuBackend::eo_terminal() {
 
 
 // ---------------------------------------------------------------- top round / Decide on device
-const Fe* GpuBackend::level_alpha(size_t level, int which) {
-  auto& v = level_alpha_[which];
-  if (v.size() <= level) v.resize(level + 1);
-  if (!v[level].p) {
-    const auto& a = P_.pcs.pp->seq.codes[level].alphas[which];
-    v[level].alloc(a.size());
-    QF_CK(cudaMemcpyAsync(v[level].p, a.data(), a.size() * 16, cudaMemcpyHostToDevice, s_));
-  }
-  return v[level].p;
-}
+const Fe* GpuBackend::level_alpha(size_t level, int which) { return tables_->alpha(*P_.pcs.pp, level, which); }
 
 // MSB-first monomial tensor weights (tensor_weights, qafold_short_pc.rs:2826-2855):
 // the last <= 10 coordinates index a low table, the rest a high table.
-void GpuBackend::tensor_table(const std::vector<F>& point, DBuf<Fe>& out) {
-  const int n = int(point.size());
-  const int lb = std::min(10, n);
-  std::vector<F> hi = tensor_weights(std::vector<F>(point.begin(), point.begin() + (n - lb)));
-  std::vector<F> lo = tensor_weights(std::vector<F>(point.begin() + (n - lb), point.end()));
-  DBuf<Fe> dhi(hi.size()), dlo(lo.size());
-  QF_CK(cudaMemcpyAsync(dhi.p, hi.data(), hi.size() * 16, cudaMemcpyHostToDevice, s_));
-  QF_CK(cudaMemcpyAsync(dlo.p, lo.data(), lo.size() * 16, cudaMemcpyHostToDevice, s_));
-  const uint64_t m = uint64_t(1) << n;
-  if (out.n != m) out.alloc(m);
-  QF_LAUNCH(s_, "k_table", m * 16, qfd::k_table<<<grid_for(m, kThreads), kThreads, 0, s_>>>(dhi.p, dlo.p, lb, m, out.p));
-  QF_CK(cudaStreamSynchronize(s_));
-}
+void GpuBackend::tensor_table(const std::vector<F>& point, DBuf<Fe>& out) { device_point_table(s_, point, tensor_slice, out); }
 
 // Unnormalised WHT of a device vector of 2^logn entries, optionally
 // multiplying by alpha first (one tile pass, then strided passes).
@@ -1171,9 +1191,12 @@ bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, siz
   const int logn = ilog2(n);
   const size_t block_log = ilog2(row_factor);
   std::vector<F> base_point(merged_left.begin() + block_log, merged_left.end());
-  if (folded_message.size() != n) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "switch message");
-  F ev;
-  if (!mle_eval(folded_message, base_point, ev) || ev != merged_value) fail(QF_E_INVALID_COMMITMENT, "switch merged value");
+  if (folded_message.size() != n || base_point.size() != size_t(logn)) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "switch message");
+  // The merged value is the message's MLE at the base point: <message, tensor weights>.
+  DBuf<Fe> sparse(n_enc), comb(n), msg_d(n), ml, gr(n_enc), tw;
+  QF_CK(cudaMemcpyAsync(msg_d.p, folded_message.data(), n * 16, cudaMemcpyHostToDevice, s_));
+  tensor_table(base_point, ml);
+  if (dot_dev(msg_d.p, ml.p, n) != merged_value) fail(QF_E_INVALID_COMMITMENT, "switch merged value");
   absorb_direct_switch(t, target, target_level, row_factor, sel, iota, merged_value, merged_left);
   size_t sel_log = ilog2(next_pow2(sel.size()));
   std::vector<F> slp;
@@ -1182,7 +1205,6 @@ bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, siz
   F selected = inner_product(sl, iota);
   std::vector<uint64_t> rows_idx;
   for (size_t i = 0; i < sel.size(); ++i) rows_idx.push_back(sel.at(i));
-  DBuf<Fe> sparse(n_enc), comb(n), msg_d(n), ml, gr(n_enc), tw;
   {
     DBuf<uint64_t> didx(rows_idx.size());
     DBuf<Fe> dval(sl.size());
@@ -1200,10 +1222,8 @@ bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, siz
   wht_dev(comb.p, logn, alpha);
   QF_LAUNCH(s_, "k_add", n * 48, qfd::k_add<<<grid_for(n, kThreads), kThreads, 0, s_>>>(comb.p, sparse.p, n));
   F rho = t.challenge_ext("direct-code-switch-opening-batch");
-  tensor_table(base_point, ml);
   F combined = selected + rho * merged_value;
   QF_LAUNCH(s_, "k_axpy", n * 48, qfd::k_axpy<<<grid_for(n, kThreads), kThreads, 0, s_>>>(comb.p, ml.p, n, to_fe(rho)));
-  QF_CK(cudaMemcpyAsync(msg_d.p, folded_message.data(), n * 16, cudaMemcpyHostToDevice, s_));
   LiteBullet<F> msg = litebullet_dev(combined, comb.p, msg_d.p, n, t, "decide-direct-carry-message-litebullet", "litebullet-fold", true);
   F ole = tensor_inner_product(base_point, msg.a_point);
   F sle = msg.a_value - rho * ole;

@@ -10,6 +10,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "host/protocol.h"
@@ -108,6 +109,20 @@ inline int grid_for(uint64_t n, int threads, int max_blocks = 148 * 8) {
   return int(b);
 }
 
+// Device copies of a parameter set's code alphas (alphas[0] and alphas[1] of
+// every level), uploaded once per device and shared by every commitment and
+// opening made with that parameter set.  Thread-safe; an upload completes
+// before the pointer is returned, so any stream may read it.
+class DeviceTables {
+ public:
+  const Fe* alpha(const PcsParams<F>& pp, size_t level, int which);
+  const Fe* top_alpha1(const PcsParams<F>& pp) { return alpha(pp, pp.seq.codes.size() - 1, 1); }
+
+ private:
+  std::mutex mu_;
+  std::map<std::tuple<int, size_t, int>, DBuf<Fe>> bufs_;  // (device, level, which)
+};
+
 // Constant hash prefixes computed on the host.
 qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain);
 qfd::InnerPrefix inner_prefix();
@@ -145,7 +160,8 @@ class GpuBackend : public Backend<F>,
                    public TopRoundAccel<F>,
                    public DecideAccel<F> {
  public:
-  GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s);
+  // `tables` (optional, not owned) shares uploaded code tables across backends.
+  GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s, DeviceTables* tables = nullptr);
   ~GpuBackend() override;
 
   // commit
@@ -220,7 +236,6 @@ class GpuBackend : public Backend<F>,
   const Fe* level_alpha(size_t level, int which);
   void mobius_rest(Fe* cw, int logm, int logR, int from);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
-  void ensure_alpha();
 
   const Parameters<F>& P_;
   const int8_t* bva_;
@@ -229,8 +244,8 @@ class GpuBackend : public Backend<F>,
   std::vector<std::unique_ptr<DeviceCodeword>> blocks_;
   std::vector<Digest> roots_;
   std::unique_ptr<DeviceCodeword> folded_;
-  DBuf<Fe> alpha1_;
-  std::vector<DBuf<Fe>> level_alpha_[2];  // device copies of alphas[0], alphas[1] per level
+  DeviceTables own_tables_;
+  DeviceTables* tables_;
   const DeviceCodeword* open_cw_ = nullptr;  // codeword whose top round is being opened
   DBuf<Fe> rw_d_;                            // its row weights
   F lb_rhs_;                                 // running claim after the last device LiteBullet
