@@ -762,8 +762,8 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
   QF_CK(cudaMemcpyAsync(dtt.p, tt.data(), tt.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
   QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, s_));
   QF_LAUNCH(s_, "k_project_terms", proj_bytes,
-            qfd::k_project_terms<<<unsigned(tiles), qfd::kTermThreads, 0, s_>>>(bva_, active_, dtt.p, int(tt.size()), tables.p,
-                                                                                 int(common_lanes), dtile.p));
+            qfd::k_project_terms<<<unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0, s_>>>(
+                bva_, active_, dtt.p, int(tt.size()), uint32_t(tiles), tables.p, int(common_lanes), dtile.p));
   QF_LAUNCH(s_, "k_sum_segments", tiles * common_lanes * 16, qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p));
   std::vector<F> h(terms.size() * common_lanes);
   QF_CK(cudaMemcpyAsync(h.data(), dterm.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
@@ -780,13 +780,26 @@ void GpuBackend::cross_terms(const Query<F>& q, size_t stride, std::vector<F>& p
   std::vector<const Term<F>*> big, small;
   for (const auto& t : q.terms) (t.len() >= stride ? big : small).push_back(&t);
   std::vector<std::vector<F>> pr = project_terms(big, stride);
-  for (size_t i = 0; i < big.size(); ++i) {
-    std::vector<F> low = factor_weights(big[i]->factors.data(), ilog2(stride));
-    for (size_t d = 1; d < stride; ++d)
-      for (size_t lane = 0; lane + d < stride; ++lane) {
-        pos[d - 1] += pr[i][lane] * low[lane + d];
-        neg[d - 1] += pr[i][lane + d] * low[lane];
-      }
+  if (!big.empty() && stride > 1) {
+    std::vector<F> prs(big.size() * stride), lows(big.size() * stride);
+    for (size_t i = 0; i < big.size(); ++i) {
+      if (pr[i].size() != stride) fail(QF_E_ARGUMENT, "projection lanes");
+      std::vector<F> low = factor_weights(big[i]->factors.data(), ilog2(stride));
+      std::copy(pr[i].begin(), pr[i].end(), prs.begin() + i * stride);
+      std::copy(low.begin(), low.end(), lows.begin() + i * stride);
+    }
+    DBuf<Fe> dpr(prs.size()), dlow(lows.size()), dout(2 * (stride - 1));
+    QF_CK(cudaMemcpyAsync(dpr.p, prs.data(), prs.size() * 16, cudaMemcpyHostToDevice, s_));
+    QF_CK(cudaMemcpyAsync(dlow.p, lows.data(), lows.size() * 16, cudaMemcpyHostToDevice, s_));
+    QF_LAUNCH(s_, "k_laurent_cross", uint64_t(prs.size()) * 32,
+              qfd::k_laurent_cross<<<unsigned(2 * (stride - 1)), kThreads, 0, s_>>>(dpr.p, dlow.p, int(big.size()), int(stride), dout.p));
+    std::vector<F> h(2 * (stride - 1));
+    QF_CK(cudaMemcpyAsync(h.data(), dout.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaStreamSynchronize(s_));
+    for (size_t d = 1; d < stride; ++d) {
+      pos[d - 1] += h[d - 1];
+      neg[d - 1] += h[stride - 2 + d];
+    }
   }
   std::vector<uint64_t> starts;
   for (const auto* t : small) starts.push_back(t->offset / stride * stride);
@@ -859,7 +872,8 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
     dtt[pass].alloc(tl.size());
     QF_CK(cudaMemcpyAsync(dtt[pass].p, tl.data(), tl.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
     QF_LAUNCH(s_, "k_query_terms", query_bytes[pass],
-              qfd::k_query_terms<<<unsigned(pass_tiles[pass]), kThreads, 0, s_>>>(dtt[pass].p, int(tl.size()), tables.p, qv_.p));
+              qfd::k_query_terms<<<unsigned((pass_tiles[pass] + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), kThreads, 0, s_>>>(
+                  dtt[pass].p, int(tl.size()), uint32_t(pass_tiles[pass]), tables.p, qv_.p));
   }
   if (!sparse.empty()) {
     std::vector<uint64_t> idx;

@@ -20,6 +20,28 @@ __device__ __forceinline__ uint32_t mod_i64(int64_t v) {
   int64_t r = v % int64_t(P);
   return uint32_t(r < 0 ? r + int64_t(P) : r);
 }
+// |v| < 2^31: v + 32768 p is in [0, 2^32), then the 2^16 = 15 fold.
+__device__ __forceinline__ uint32_t mod_i32(int32_t v) {
+  return red32(uint32_t(int64_t(v) + int64_t(P) * 32768));
+}
+// Four signed 8-bit lanes of a times four unsigned 8-bit lanes of b, plus c.
+__device__ __forceinline__ int32_t dp4a_su(uint32_t a, uint32_t b, int32_t c) {
+  int32_t d;
+  asm("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+// Byte planes of the coefficient k of four elements e[0..3]: lo = the low
+// bytes, hi = the high bytes, lane i in byte i.
+__device__ __forceinline__ void byte_planes(const Fe* e, int k, uint32_t& lo, uint32_t& hi) {
+  lo = 0;
+  hi = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t c = e[i].c[k];
+    lo |= (c & 0xffu) << (8 * i);
+    hi |= (c >> 8) << (8 * i);
+  }
+}
 __device__ __forceinline__ Fr shfl_xor(const Fr& v, int m) {
   Fr r;
 #pragma unroll
@@ -66,11 +88,6 @@ __device__ __forceinline__ Fr table_at(const Fe* hi, const Fe* lo, int lb, uint6
   return mul(load(hi + (i >> lb)), load(lo + (i & ((uint64_t(1) << lb) - 1))));
 }
 
-// ---------------------------------------------------------------- TBV projections
-// One tile of a large tensor term: `rows` consecutive rows of `lanes` BVA
-// values starting at `base`, all sharing the high weight `hi`; the low
-// weights are lo[0 .. rows).  Output: lanes field elements
-//   out[lane] = hi * sum_r lo[r] * v[base + r * lanes + lane].
 // ---------------------------------------------------------------- TBV term tiles
 // Tensor weights of LSB-first factor pairs (tbv.rs:45-76), built on the
 // device: entry e of a table is scale * prod_k factors[k][bit k of e].
@@ -123,65 +140,72 @@ __device__ __forceinline__ Fr tile_high(const TermTiles& T, const Fe* __restrict
 // most 128 rows * 128 * 65520 < 2^31 per warp sum: tiles have <= 1024 rows),
 // then in i64 across warps, then reduce once.
 constexpr int kTermThreads = 256;
+constexpr int kTilesPerCta = 4;  // consecutive tiles per CTA: one term search, then a forward scan
 __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __restrict__ bva, uint64_t active,
                                                                 const TermTiles* __restrict__ terms, int n_terms,
-                                                                const Fe* __restrict__ tables, int lanes,
-                                                                Fe* __restrict__ out) {
+                                                                uint32_t n_tiles, const Fe* __restrict__ tables,
+                                                                int lanes, Fe* __restrict__ out) {
   __shared__ int t_sel;
   __shared__ int64_t part_s[kTermThreads / 32][64][8];
-  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, blockIdx.x);
+  const uint32_t tile0 = blockIdx.x * kTilesPerCta;
+  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, tile0);
   __syncthreads();
-  const TermTiles T = terms[t_sel];
-  const uint64_t i = blockIdx.x - T.first_tile;
-  const uint64_t row0 = i << T.lb;
-  const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
-  const int nrows = int(left < span ? left : span);
+  int ti = t_sel;
   const int lpt = lanes < 4 ? lanes : 4;
   const int tpr = lanes / lpt;
   const int rpp = kTermThreads / tpr;
   const int sub = threadIdx.x % tpr;
-  int32_t acc[4][8];
-#pragma unroll
-  for (int j = 0; j < 4; ++j)
-#pragma unroll
-    for (int k = 0; k < 8; ++k) acc[j][k] = 0;
-  const Fe* lo = tables + T.lo_off;
-  for (int r = threadIdx.x / tpr; r < nrows; r += rpp) {
-    const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
-    int v[4] = {0, 0, 0, 0};
-    if (lpt == 4 && g + 4 <= active && (g & 3) == 0) {
-      const uint32_t u = *reinterpret_cast<const uint32_t*>(bva + g);
-#pragma unroll
-      for (int j = 0; j < 4; ++j) v[j] = int(int8_t(u >> (8 * j)));
-    } else {
-      for (int j = 0; j < lpt; ++j) v[j] = g + j < active ? int(bva[g + j]) : 0;
-    }
-    const Fr w = load(lo + r);
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc[j][k] += int32_t(w.c[k]) * v[j];
-  }
-  for (int o = tpr; o < 32; o <<= 1)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
   const int warp = threadIdx.x >> 5, lane_id = threadIdx.x & 31;
-  if (lane_id < tpr)
-    for (int j = 0; j < lpt; ++j)
+  for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
+    while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
+    const TermTiles T = terms[ti];
+    const uint64_t i = tile - T.first_tile;
+    const uint64_t row0 = i << T.lb;
+    const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
+    const int nrows = int(left < span ? left : span);
+    int32_t acc[4][8];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) part_s[warp][lane_id * lpt + j][k] = acc[j][k];
-  __syncthreads();
-  if (threadIdx.x < lanes) {
-    int64_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (int w = 0; w < kTermThreads / 32; ++w)
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int k = 0; k < 8; ++k) s[k] += part_s[w][threadIdx.x][k];
-    Fr sum;
+      for (int k = 0; k < 8; ++k) acc[j][k] = 0;
+    const Fe* lo = tables + T.lo_off;
+    for (int r = threadIdx.x / tpr; r < nrows; r += rpp) {
+      const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
+      int v[4] = {0, 0, 0, 0};
+      if (lpt == 4 && g + 4 <= active && (g & 3) == 0) {
+        const uint32_t u = *reinterpret_cast<const uint32_t*>(bva + g);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) sum.c[k] = mod_i64(s[k]);
-    store(out + size_t(blockIdx.x) * lanes + threadIdx.x, mul(tile_high(T, tables, i), sum));
+        for (int j = 0; j < 4; ++j) v[j] = int(int8_t(u >> (8 * j)));
+      } else {
+        for (int j = 0; j < lpt; ++j) v[j] = g + j < active ? int(bva[g + j]) : 0;
+      }
+      const Fr w = load(lo + r);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[j][k] += int32_t(w.c[k]) * v[j];
+    }
+    for (int o = tpr; o < 32; o <<= 1)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+    if (lane_id < tpr)
+      for (int j = 0; j < lpt; ++j)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) part_s[warp][lane_id * lpt + j][k] = acc[j][k];
+    __syncthreads();
+    if (threadIdx.x < lanes) {
+      int64_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int w = 0; w < kTermThreads / 32; ++w)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) s[k] += part_s[w][threadIdx.x][k];
+      Fr sum;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) sum.c[k] = mod_i64(s[k]);
+      store(out + size_t(tile) * lanes + threadIdx.x, mul(tile_high(T, tables, i), sum));
+    }
+    __syncthreads();
   }
 }
 
@@ -198,6 +222,25 @@ __global__ void k_sum_segments(const Fe* __restrict__ tile_out, const uint32_t* 
   }
 }
 
+// Laurent cross sums of the large terms (Query::cross_terms, tbv.rs:353-392):
+// block d - 1 (d = 1 .. stride - 1) sums pr[t][lane] * low[t][lane + d], block
+// stride - 2 + d sums pr[t][lane + d] * low[t][lane], over terms t and lanes.
+__global__ void k_laurent_cross(const Fe* __restrict__ pr, const Fe* __restrict__ low, int n_terms, int stride,
+                                Fe* __restrict__ out) {
+  const int d = int(blockIdx.x) % (stride - 1) + 1;
+  const bool negative = int(blockIdx.x) >= stride - 1;
+  const int per = stride - d;
+  Fr acc[1] = {zero()};
+  for (int e = threadIdx.x; e < n_terms * per; e += blockDim.x) {
+    const int t = e / per, lane = e % per;
+    const Fe* a = pr + size_t(t) * stride;
+    const Fe* b = low + size_t(t) * stride;
+    acc[0] = add(acc[0], negative ? mul(load(a + lane + d), load(b + lane)) : mul(load(a + lane), load(b + lane + d)));
+  }
+  block_reduce<1>(acc);
+  if (threadIdx.x == 0) store(out + blockIdx.x, acc[0]);
+}
+
 // Copies the aligned stride-wide BVA window of each small term.
 __global__ void k_gather_windows(const int8_t* __restrict__ bva, uint64_t active, const uint64_t* __restrict__ starts,
                                  uint32_t count, int stride, int8_t* __restrict__ out) {
@@ -209,48 +252,75 @@ __global__ void k_gather_windows(const int8_t* __restrict__ bva, uint64_t active
 
 // ---------------------------------------------------------------- EO
 // witness[row] = sum_lane v[row * stride + lane] * inv^lane (eo.rs:119-132).
+// Packed EO witness (eo.rs:119-132): witness[row] = sum_lane v(row * stride +
+// lane) * inv_powers[lane].  For stride 16 a row is one 16-byte load and each
+// coefficient two chains of four dp4a (signed weights against the low and
+// high bytes of the powers, held in registers); |sum| < 16 * 128 * 65520.
 __global__ void k_eo_witness(const int8_t* __restrict__ bva, uint64_t active, uint64_t rows, int stride,
                              const Fe* __restrict__ inv_powers, Fe* __restrict__ witness) {
   __shared__ Fe pw[64];
   if (threadIdx.x < stride) pw[threadIdx.x] = inv_powers[threadIdx.x];
   __syncthreads();
+  uint32_t plo[8][4], phi[8][4];
+  if (stride == 16) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) byte_planes(pw + 4 * q, k, plo[k][q], phi[k][q]);
+  }
   for (uint64_t row = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < rows; row += uint64_t(gridDim.x) * blockDim.x) {
     int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const uint64_t g0 = row * stride;
-    if (g0 < active) {
+    if (stride == 16 && g0 + 16 <= active) {
+      const uint4 raw = *reinterpret_cast<const uint4*>(bva + g0);
+      const uint32_t a[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        int32_t lo = 0, hi = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          lo = dp4a_su(a[q], plo[k][q], lo);
+          hi = dp4a_su(a[q], phi[k][q], hi);
+        }
+        acc[k] = lo + hi * 256;
+      }
+    } else if (g0 < active) {
       for (int lane = 0; lane < stride; ++lane) {
         const uint64_t g = g0 + lane;
         const int v = g < active ? int(bva[g]) : 0;
-        if (v) {
-          Fr p = load(pw + lane);
+        const Fr p = load(pw + lane);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) acc[k] += int32_t(p.c[k]) * v;
-        }
+        for (int k = 0; k < 8; ++k) acc[k] += int32_t(p.c[k]) * v;
       }
     }
     Fr w;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) w.c[k] = mod_i64(acc[k]);
+    for (int k = 0; k < 8; ++k) w.c[k] = mod_i32(acc[k]);
     store(witness + row, w);
   }
 }
 
-// Query-fold tile of a large term: q[start + r] (=|+=) hi * lo[r], r < rows.
 // Query fold of large terms (tbv.rs:393-428): q[offset + row] += high(tile) *
 // lo[r] for the rows of each tile.  Terms within one launch are disjoint.
-__global__ void k_query_terms(const TermTiles* __restrict__ terms, int n_terms, const Fe* __restrict__ tables,
-                              Fe* __restrict__ q) {
+__global__ void k_query_terms(const TermTiles* __restrict__ terms, int n_terms, uint32_t n_tiles,
+                              const Fe* __restrict__ tables, Fe* __restrict__ q) {
   __shared__ int t_sel;
-  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, blockIdx.x);
+  const uint32_t tile0 = blockIdx.x * kTilesPerCta;
+  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, tile0);
   __syncthreads();
-  const TermTiles T = terms[t_sel];
-  const uint64_t i = blockIdx.x - T.first_tile;
-  const uint64_t row0 = i << T.lb;
-  const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
-  const uint32_t nrows = uint32_t(left < span ? left : span);
-  const Fr hi = tile_high(T, tables, i);
-  Fe* dst = q + T.offset + row0;
-  for (uint32_t r = threadIdx.x; r < nrows; r += blockDim.x) store(dst + r, add(load(dst + r), mul(hi, load(tables + T.lo_off + r))));
+  int ti = t_sel;
+  for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
+    while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
+    const TermTiles T = terms[ti];
+    const uint64_t i = tile - T.first_tile;
+    const uint64_t row0 = i << T.lb;
+    const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
+    const uint32_t nrows = uint32_t(left < span ? left : span);
+    const Fr hi = tile_high(T, tables, i);
+    Fe* dst = q + T.offset + row0;
+    for (uint32_t r = threadIdx.x; r < nrows; r += blockDim.x)
+      store(dst + r, add(load(dst + r), mul(hi, load(tables + T.lo_off + r))));
+  }
 }
 __global__ void k_scatter_add(const uint64_t* __restrict__ idx, const Fe* __restrict__ vals, uint32_t n, Fe* __restrict__ q) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -411,41 +481,53 @@ __global__ void k_apply_images(Fe* __restrict__ weights, uint64_t m, const Fe* _
 
 // values[i] = sum_b fold[b] * packed(b, i) = sum_{b,j} v(b, 8i+j) * T[b][j],
 // with T[b][j] = fold[b] * X^j precomputed (packed_batch.rs:213-222).
+// Block fold of the packed weights (packed_batch.rs:213-236):
+// values[i] = sum_b sum_j v(b * block_len + 8i + j) * T[b * 8 + j], T[b * 8 + j] =
+// (c^-1)^b * X^j.  Each block's T rows are held as byte planes in shared
+// memory; a block contributes two dp4a per byte plane and coefficient.  Sums
+// of 8 blocks stay below 8 * 8 * 128 * 65520 < 2^31 and move to i64 totals.
 __global__ void k_block_fold(const int8_t* __restrict__ bva, uint64_t active, uint64_t block_len, int blocks, uint64_t m,
                              const Fe* __restrict__ T, Fe* __restrict__ values) {
   extern __shared__ uint4 smem_u4[];
-  Fe* Ts = reinterpret_cast<Fe*>(smem_u4);
-  for (int t = threadIdx.x; t < blocks * 8; t += blockDim.x) Ts[t] = T[t];
+  // planes[b][k] = {lo(j 0..3), lo(j 4..7), hi(j 0..3), hi(j 4..7)}
+  uint4* planes = smem_u4;
+  for (int t = threadIdx.x; t < blocks * 8; t += blockDim.x) {
+    const int b = t >> 3, k = t & 7;
+    uint4 pl;
+    byte_planes(T + b * 8, k, pl.x, pl.z);
+    byte_planes(T + b * 8 + 4, k, pl.y, pl.w);
+    planes[t] = pl;
+  }
   __syncthreads();
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (int b = 0; b < blocks; ++b) {
+      if (b && (b & 7) == 0)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { tot[k] += acc[k]; acc[k] = 0; }
       const uint64_t g = uint64_t(b) * block_len + 8 * i;
       if (g >= active) break;  // later blocks start even later
-      int8_t v[8];
+      uint2 v8;
       if (g + 8 <= active) {
-        uint2 raw8 = *reinterpret_cast<const uint2*>(bva + g);
-        const int8_t* bb = reinterpret_cast<const int8_t*>(&raw8);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = bb[j];
+        v8 = *reinterpret_cast<const uint2*>(bva + g);
       } else {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) v[j] = g + j < active ? bva[g + j] : int8_t(0);
-      }
-      int32_t a32[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (v[j] == 0) continue;
-        Fr t = load(Ts + b * 8 + j);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) a32[k] += int32_t(v[j]) * int32_t(t.c[k]);
+        uint32_t w[2] = {0, 0};
+        for (int j = 0; j < 8; ++j)
+          if (g + j < active) w[j >> 2] |= uint32_t(uint8_t(bva[g + j])) << (8 * (j & 3));
+        v8 = make_uint2(w[0], w[1]);
       }
 #pragma unroll
-      for (int k = 0; k < 8; ++k) acc[k] += a32[k];
+      for (int k = 0; k < 8; ++k) {
+        const uint4 pl = planes[b * 8 + k];
+        const int32_t lo = dp4a_su(v8.y, pl.y, dp4a_su(v8.x, pl.x, 0));
+        const int32_t hi = dp4a_su(v8.y, pl.w, dp4a_su(v8.x, pl.z, 0));
+        acc[k] += lo + hi * 256;
+      }
     }
     Fr o;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) o.c[k] = mod_i64(acc[k]);
+    for (int k = 0; k < 8; ++k) o.c[k] = blocks > 8 ? mod_i64(tot[k] + acc[k]) : mod_i32(acc[k]);
     store(values + i, o);
   }
 }
