@@ -13,7 +13,10 @@
 #pragma once
 #include <cmath>
 #include <cstdint>
+#include <map>
+#include <mutex>
 #include <stdexcept>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -104,7 +107,7 @@ inline bool qa_bound_at(size_t message_len, size_t index, double distance, doubl
   return true;
 }
 // qafold.rs:75-131.  Returns false for "InvalidParameters" (no admissible distance).
-inline bool qa_distance_bound(size_t message_len, size_t index, size_t security_bits, double modulus_log2, double& rel) {
+inline bool qa_distance_bound_uncached(size_t message_len, size_t index, size_t security_bits, double modulus_log2, double& rel) {
   if (message_len == 0 || !is_pow2(message_len) || index <= 1 || !is_pow2(index) || security_bits == 0 ||
       !std::isfinite(modulus_log2) || modulus_log2 <= 0.0)
     fail(QF_E_ENCODING, "qa distance arguments");
@@ -132,6 +135,27 @@ inline bool qa_distance_bound(size_t message_len, size_t index, size_t security_
   if (!qa_bound_at(message_len, index, relative, ln_p, e, lf)) fail(QF_E_ENCODING, "qa bound");
   rel = relative;
   return true;
+}
+// The bound depends only on its arguments; provers and verifiers ask for the
+// same few codes many times, so results are memoised (thread-safe).
+inline bool qa_distance_bound(size_t message_len, size_t index, size_t security_bits, double modulus_log2, double& rel) {
+  static std::mutex mu;
+  static std::map<std::tuple<size_t, size_t, size_t, double>, std::pair<bool, double>> memo;
+  const auto key = std::make_tuple(message_len, index, security_bits, modulus_log2);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = memo.find(key);
+    if (it != memo.end()) {
+      rel = it->second.second;
+      return it->second.first;
+    }
+  }
+  double r = 0.0;
+  const bool ok = qa_distance_bound_uncached(message_len, index, security_bits, modulus_log2, r);
+  std::lock_guard<std::mutex> g(mu);
+  memo[key] = {ok, r};
+  rel = r;
+  return ok;
 }
 // brakefold.rs:4-20.
 inline size_t queries_for_relative_distance(size_t security_bits, double distance) {

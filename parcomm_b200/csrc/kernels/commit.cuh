@@ -49,13 +49,6 @@ __device__ __forceinline__ int pidx(int e) {
   return e ^ int(__byte_perm(uint32_t(kSwz), uint32_t(kSwz >> 32), (e >> 5) & 7) & 31);
 }
 
-__device__ __forceinline__ void planar_put_raw(uint32_t* planes, int e, uint4 u) {
-  const int q = pidx(e);
-  planes[0 * kPlane + q] = u.x & 0xffffu; planes[1 * kPlane + q] = u.x >> 16;
-  planes[2 * kPlane + q] = u.y & 0xffffu; planes[3 * kPlane + q] = u.y >> 16;
-  planes[4 * kPlane + q] = u.z & 0xffffu; planes[5 * kPlane + q] = u.z >> 16;
-  planes[6 * kPlane + q] = u.w & 0xffffu; planes[7 * kPlane + q] = u.w >> 16;
-}
 __device__ __forceinline__ void planar_put(uint32_t* planes, int e, const Fr& v) {
   const int q = pidx(e);
 #pragma unroll
@@ -125,54 +118,129 @@ __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b,
   __syncthreads();
 }
 
-// Levels act on tile bits [bit0, bit0 + levels) of the 2^log_n elements.
+// Levels act on tile bits [bit0, bit0 + levels) of the 2^log_n elements; the
+// first of them is level lvl0 of the pass (for the lazy bounds).
 template <int OP>
-__device__ __forceinline__ void planar_levels(uint32_t* planes, int log_n, int bit0, int levels) {
+__device__ __forceinline__ void planar_levels(uint32_t* planes, int log_n, int bit0, int levels, int lvl0 = 0) {
   int l = 0;
-  for (; l + 3 <= levels; l += 3) planar_stage<OP, 3>(planes, log_n, bit0 + l, l);
-  if (levels - l == 2) planar_stage<OP, 2>(planes, log_n, bit0 + l, l);
-  if (levels - l == 1) planar_stage<OP, 1>(planes, log_n, bit0 + l, l);
+  for (; l + 3 <= levels; l += 3) planar_stage<OP, 3>(planes, log_n, bit0 + l, lvl0 + l);
+  if (levels - l == 2) planar_stage<OP, 2>(planes, log_n, bit0 + l, lvl0 + l);
+  if (levels - l == 1) planar_stage<OP, 1>(planes, log_n, bit0 + l, lvl0 + l);
 }
 
-// Gathers the n tile elements src[addr(t)] (times alpha[addr(t) & amask] when
-// alpha is given) into the planes.  Each thread issues up to kBatch 16-byte loads
-// before it writes shared memory, so a tile's loads are in flight together.
-constexpr int kBatch = 4;
-template <class Addr>
-__device__ __forceinline__ void tile_gather(uint32_t* planes, int n, const Fe* src, Addr addr, const Fe* __restrict__ alpha,
-                                            size_t amask) {
-  for (int t0 = threadIdx.x; t0 < n; t0 += kBatch * blockDim.x) {
-    uint4 raw[kBatch];
+// ---------------------------------------------------------------- tile passes
+// A pass applies the levels on tile bits [b0, log_n) of a 2^log_n-element
+// tile.  ld(t) returns the canonical value of tile element t (from HBM) and
+// st(t, u) stores element t packed.  For a full 4096-element tile with at
+// least three levels, the levels on tile bits 9..11 run in registers right
+// after the loads (pass_head) and the last one to three levels right before
+// the stores (pass_tail): a thread owns 8 (or 4, 2) elements with all 8
+// coefficients, and consecutive threads take consecutive elements, so every
+// load and store instruction of a warp stays coalesced.  The levels between
+// run as planar shared-memory stages.  Smaller tiles run every level in
+// shared memory.
+
+// R levels across the elements held in registers, starting at level lvl.
+template <int OP, int R>
+__device__ __forceinline__ void reg_levels(uint32_t (&v)[1 << R][8], int lvl) {
 #pragma unroll
-    for (int u = 0; u < kBatch; ++u) {
-      const int t = t0 + u * blockDim.x;
-      if (t < n) raw[u] = *reinterpret_cast<const uint4*>(src + addr(t));
-    }
-    if (alpha) {
+  for (int sft = 0; sft < R; ++sft) {
+    const uint32_t B = P << (lvl + sft);
 #pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        const int t = t0 + u * blockDim.x;
-        if (t < n) {
-          Fr v;
-          v.c[0] = raw[u].x & 0xffffu; v.c[1] = raw[u].x >> 16; v.c[2] = raw[u].y & 0xffffu; v.c[3] = raw[u].y >> 16;
-          v.c[4] = raw[u].z & 0xffffu; v.c[5] = raw[u].z >> 16; v.c[6] = raw[u].w & 0xffffu; v.c[7] = raw[u].w >> 16;
-          planar_put(planes, t, mul(v, load(alpha + (addr(t) & amask))));
+    for (int j = 0; j < (1 << R); ++j) {
+      if (j & (1 << sft)) continue;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const uint32_t lo = v[j][c], hi = v[j | (1 << sft)][c];
+        if (OP == kWht) {
+          v[j][c] = lo + hi;
+          v[j | (1 << sft)][c] = lo + B - hi;
+        } else {
+          v[j | (1 << sft)][c] = hi + B - lo;
         }
-      }
-    } else {
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        const int t = t0 + u * blockDim.x;
-        if (t < n) planar_put_raw(planes, t, raw[u]);
       }
     }
   }
+}
+
+// Loads, levels 0..2 on tile bits 9..11, planes.  Thread g (512 per CTA) owns
+// tile elements g + (j << 9), j < 8.
+template <int OP, class Ld>
+__device__ __forceinline__ void pass_head(uint32_t* planes, Ld ld) {
+  const int g = threadIdx.x;
+  uint32_t v[8][8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const Fr e = ld(g + (j << 9));
+#pragma unroll
+    for (int c = 0; c < 8; ++c) v[j][c] = e.c[c];
+  }
+  reg_levels<OP, 3>(v, 0);
+  const int pb = pidx(g);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int q = pb ^ pidx(j << 9);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) planes[c * kPlane + q] = v[j][c];
+  }
   __syncthreads();
 }
-template <class Addr>
-__device__ __forceinline__ void tile_scatter(const uint32_t* planes, int n, Fe* dst, Addr addr) {
-  for (int t = threadIdx.x; t < n; t += blockDim.x)
-    *reinterpret_cast<uint4*>(dst + addr(t)) = planar_get_packed(planes, t);
+
+// Planes, the last R levels (tile bits [zb, zb + R), the first of them level
+// lvl of the pass), reduction, stores.
+template <int OP, int R, class St>
+__device__ __forceinline__ void pass_tail(const uint32_t* planes, int zb, int lvl, St st) {
+  constexpr int kGroups = (1 << kMaxTileLog) >> R;
+  for (int g = threadIdx.x; g < kGroups; g += blockDim.x) {
+    const int base = (g & ((1 << zb) - 1)) | ((g >> zb) << (zb + R));
+    const int pb = pidx(base);
+    uint32_t v[1 << R][8];
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      const int q = pb ^ pidx(j << zb);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v[j][c] = planes[c * kPlane + q];
+    }
+    reg_levels<OP, R>(v, lvl);
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      uint32_t w[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) w[c] = red28(v[j][c]);
+      st(base + (j << zb), make_uint4(w[0] | (w[1] << 16), w[2] | (w[3] << 16), w[4] | (w[5] << 16), w[6] | (w[7] << 16)));
+    }
+  }
+}
+
+template <int OP, class Ld, class St>
+__device__ __forceinline__ void tile_pass(uint32_t* planes, int log_n, int b0, Ld ld, St st) {
+  const int n = 1 << log_n;
+  if (log_n == kMaxTileLog && log_n - b0 >= 3 && blockDim.x == kTileThreads) {
+    pass_head<OP>(planes, ld);
+    const int rem = 9 - b0;  // level bits [b0, 9) are left
+    const int rz = rem < 3 ? rem : 3;
+    const int rm = rem - rz;
+    planar_levels<OP>(planes, log_n, b0, rm, 3);
+    switch (rz) {
+      case 3: pass_tail<OP, 3>(planes, 9 - 3, 3 + rm, st); break;
+      case 2: pass_tail<OP, 2>(planes, 9 - 2, 3 + rm, st); break;
+      case 1: pass_tail<OP, 1>(planes, 9 - 1, 3 + rm, st); break;
+      default:
+        for (int t = threadIdx.x; t < n; t += blockDim.x) st(t, planar_get_packed(planes, t));
+    }
+    return;
+  }
+  for (int t = threadIdx.x; t < n; t += blockDim.x) planar_put(planes, t, ld(t));
+  __syncthreads();
+  planar_levels<OP>(planes, log_n, b0, log_n - b0);
+  for (int t = threadIdx.x; t < n; t += blockDim.x) st(t, planar_get_packed(planes, t));
+}
+
+__device__ __forceinline__ Fr unpack(uint4 u) {
+  Fr v;
+  v.c[0] = u.x & 0xffffu; v.c[1] = u.x >> 16; v.c[2] = u.y & 0xffffu; v.c[3] = u.y >> 16;
+  v.c[4] = u.z & 0xffffu; v.c[5] = u.z >> 16; v.c[6] = u.w & 0xffffu; v.c[7] = u.w >> 16;
+  return v;
 }
 
 // Pack eight signed weights per element, then Mobius levels [0, levels) in a
@@ -180,28 +248,25 @@ __device__ __forceinline__ void tile_scatter(const uint32_t* planes, int n, Fe* 
 __global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t active,
                                                                      uint64_t src_base, Fe* __restrict__ cw, int logR, int levels) {
   extern __shared__ uint32_t planes_s[];
-  const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
-  for (int e = threadIdx.x; e < n; e += blockDim.x) {
-    const uint64_t g = src_base + 8ull * (first + e);
-    int8_t v[8];
+  auto ld = [=](int t) {
+    const uint64_t g = src_base + 8ull * (first + t);
+    uint2 raw = make_uint2(0, 0);
     if (g + 8 <= active) {
-      uint2 raw = *reinterpret_cast<const uint2*>(bva + g);
-      const int8_t* bb = reinterpret_cast<const int8_t*>(&raw);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = bb[k];
+      raw = *reinterpret_cast<const uint2*>(bva + g);
     } else {
-#pragma unroll
-      for (int k = 0; k < 8; ++k) v[k] = (g + k < active) ? bva[g + k] : int8_t(0);
+      uint32_t w[2] = {0, 0};
+      for (int k = 0; k < 8; ++k)
+        if (g + k < active) w[k >> 2] |= uint32_t(uint8_t(bva[g + k])) << (8 * (k & 3));
+      raw = make_uint2(w[0], w[1]);
     }
     Fr r;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) r.c[k] = small(v[k]);
-    planar_put(planes_s, e, r);
-  }
-  __syncthreads();
-  planar_levels<kMobius>(planes_s, levels, 0, levels);
-  tile_scatter(planes_s, n, cw, [=](int t) { return msg_addr(first + t, logR); });
+    for (int k = 0; k < 8; ++k) r.c[k] = small(int(int8_t(((k < 4 ? raw.x : raw.y) >> (8 * (k & 3))) & 0xffu)));
+    return r;
+  };
+  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(cw + msg_addr(first + t, logR)) = u; };
+  tile_pass<kMobius>(planes_s, levels, 0, ld, st);
 }
 
 // Same, but the packed values come from an element vector (the block-folded
@@ -209,11 +274,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const int8
 __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* __restrict__ src, Fe* __restrict__ cw, int logR,
                                                                      int levels) {
   extern __shared__ uint32_t planes_s[];
-  const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
-  tile_gather(planes_s, n, src, [=](int t) { return first + t; }, nullptr, 0);
-  planar_levels<kMobius>(planes_s, levels, 0, levels);
-  tile_scatter(planes_s, n, cw, [=](int t) { return msg_addr(first + t, logR); });
+  auto ld = [=](int t) { return load(src + first + t); };
+  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(cw + msg_addr(first + t, logR)) = u; };
+  tile_pass<kMobius>(planes_s, levels, 0, ld, st);
 }
 
 // WHT levels [0, levels) within a tile (levels <= logR so columns never mix).
@@ -224,24 +288,26 @@ template <bool ALPHA>
 __global__ void __launch_bounds__(ALPHA ? kAlphaTileThreads : kTileThreads, 1)
     k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR, int levels) {
   extern __shared__ uint32_t planes_s[];
-  const int n = 1 << levels;
   const size_t first = size_t(blockIdx.x) << levels;
   // For a message-half address a = c * 2R + r, a & (R - 1) = r.
   const size_t rmask = (size_t(1) << logR) - 1;
-  tile_gather(planes_s, n, src, [=](int t) { return msg_addr(first + t, logR); }, ALPHA ? alpha : nullptr, rmask);
-  planar_levels<kWht>(planes_s, levels, 0, levels);
-  tile_scatter(planes_s, n, dst, [=](int t) { return msg_addr(first + t, logR); });
+  auto ld = [=](int t) {
+    const size_t a = msg_addr(first + t, logR);
+    const Fr v = unpack(*reinterpret_cast<const uint4*>(src + a));
+    return ALPHA ? mul(v, load(alpha + (a & rmask))) : v;
+  };
+  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(dst + msg_addr(first + t, logR)) = u; };
+  tile_pass<kWht>(planes_s, levels, 0, ld, st);
 }
 
 // Levels [lo, lo + k) over the logical index space, on the half starting at
 // `base` (cw for the message, cw + R for the parity).  Each CTA owns 2^cb
-// consecutive group bases (64- or 128-byte runs in HBM for cb = 2, 3): tile
-// element t = (j << cb) + c is logical index base(g0 + c) + (j << lo), so the
-// levels act on tile bits [cb, cb + k).
+// consecutive group bases (64-byte runs in HBM at cb = 2, longer above):
+// tile element t = (j << cb) + c is logical index base(g0 + c) + (j << lo),
+// so the levels act on tile bits [cb, cb + k).
 template <int OP>
 __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k, int cb) {
   extern __shared__ uint32_t planes_s[];
-  const int n = 1 << (cb + k);
   const size_t g0 = size_t(blockIdx.x) << cb;
   const size_t low_mask = (size_t(1) << lo) - 1;
   const int cmask = (1 << cb) - 1;
@@ -249,9 +315,9 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __res
     const size_t g = g0 + (t & cmask);
     return msg_addr((((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(t >> cb) << lo), logR);
   };
-  tile_gather(planes_s, n, base, addr, nullptr, 0);
-  planar_levels<OP>(planes_s, cb + k, cb, k);
-  tile_scatter(planes_s, n, base, addr);
+  auto ld = [=](int t) { return unpack(*reinterpret_cast<const uint4*>(base + addr(t))); };
+  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(base + addr(t)) = u; };
+  tile_pass<OP>(planes_s, cb + k, cb, ld, st);
 }
 
 // ---------------------------------------------------------------- hashing

@@ -169,21 +169,35 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __
 #pragma unroll
       for (int k = 0; k < 8; ++k) acc[j][k] = 0;
     const Fe* lo = tables + T.lo_off;
-    for (int r = threadIdx.x / tpr; r < nrows; r += rpp) {
-      const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
-      int v[4] = {0, 0, 0, 0};
-      if (lpt == 4 && g + 4 <= active && (g & 3) == 0) {
-        const uint32_t u = *reinterpret_cast<const uint32_t*>(bva + g);
+    // Four rows per iteration: their loads are issued before any is used.
+    for (int r0 = threadIdx.x / tpr; r0 < nrows; r0 += 4 * rpp) {
+      uint32_t u[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) v[j] = int(int8_t(u >> (8 * j)));
-      } else {
-        for (int j = 0; j < lpt; ++j) v[j] = g + j < active ? int(bva[g + j]) : 0;
+      for (int q = 0; q < 4; ++q) {
+        const int r = r0 + q * rpp;
+        const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
+        u[q] = 0;
+        if (r < nrows) {
+          if (lpt == 4 && g + 4 <= active && (g & 3) == 0) {
+            u[q] = *reinterpret_cast<const uint32_t*>(bva + g);
+          } else {
+            for (int j = 0; j < lpt; ++j)
+              if (g + j < active) u[q] |= uint32_t(uint8_t(bva[g + j])) << (8 * j);
+          }
+        }
       }
-      const Fr w = load(lo + r);
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+      for (int q = 0; q < 4; ++q) {
+        const int r = r0 + q * rpp;
+        if (r >= nrows) break;
+        const Fr w = load(lo + r);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[j][k] += int32_t(w.c[k]) * v[j];
+        for (int j = 0; j < 4; ++j) {
+          const int v = int(int8_t(u[q] >> (8 * j)));
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc[j][k] += int32_t(w.c[k]) * v;
+        }
+      }
     }
     for (int o = tpr; o < 32; o <<= 1)
 #pragma unroll
