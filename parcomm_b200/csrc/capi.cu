@@ -18,14 +18,28 @@ using qfc::require_device;
 using qfc::set_error;
 
 namespace {
-// Any zero-padding entry that is nonzero sets the flag (Layout::validate_values, layout.rs:136-155).
+// Any zero-padding entry that is nonzero sets the flag (Layout::validate_values,
+// layout.rs:136-155).  Segments are at most kZeroPiece bytes; a CTA checks one
+// with 16-byte loads over its aligned middle and byte loads at the ends.
+constexpr uint64_t kZeroPiece = 4096;
 __global__ void k_check_zero_segments(const int8_t* __restrict__ bva, const uint64_t* __restrict__ seg, uint32_t n_seg,
                                       unsigned int* __restrict__ flag) {
+  bool bad = false;
   for (uint32_t s = blockIdx.x; s < n_seg; s += gridDim.x) {
     const uint64_t a = seg[2 * s], b = seg[2 * s + 1];
-    for (uint64_t i = a + threadIdx.x; i < b; i += blockDim.x)
-      if (bva[i] != 0) atomicOr(flag, 1u);
+    const uint64_t a16 = (a + 15) & ~uint64_t(15), b16 = b & ~uint64_t(15);
+    if (a16 >= b16) {
+      for (uint64_t i = a + threadIdx.x; i < b; i += blockDim.x) bad |= bva[i] != 0;
+    } else {
+      for (uint64_t i = a + threadIdx.x; i < a16; i += blockDim.x) bad |= bva[i] != 0;
+      for (uint64_t i = b16 + threadIdx.x; i < b; i += blockDim.x) bad |= bva[i] != 0;
+      for (uint64_t i = a16 + 16 * uint64_t(threadIdx.x); i < b16; i += 16 * uint64_t(blockDim.x)) {
+        const uint4 u = *reinterpret_cast<const uint4*>(bva + i);
+        bad |= (u.x | u.y | u.z | u.w) != 0;
+      }
+    }
   }
+  if (bad) atomicOr(flag, 1u);
 }
 
 }  // namespace
@@ -165,23 +179,31 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
     c->upload_ms = ms_since(t0);
     t0 = std::chrono::steady_clock::now();
     // Padding must be zero (validate_values) — checked on the device.
-    std::vector<uint64_t> seg;
-    for (const Bucket& b : P.layout.buckets)
-      for (size_t r = 0; r < b.rows; ++r) {
-        size_t valid = r < b.physical_rows ? b.physical_cols : 0;
-        if (valid == b.cols) continue;
-        uint64_t a = b.offset + r * b.cols + valid, e = b.offset + (r + 1) * b.cols;
-        if (!seg.empty() && seg.back() == a) seg.back() = e;  // merge contiguous runs
-        else { seg.push_back(a); seg.push_back(e); }
+    std::vector<uint64_t> runs;
+    auto add_run = [&](uint64_t a, uint64_t e) {
+      if (a >= e) return;
+      if (!runs.empty() && runs.back() == a) runs.back() = e;  // merge contiguous runs
+      else { runs.push_back(a); runs.push_back(e); }
+    };
+    for (const Bucket& b : P.layout.buckets) {
+      if (b.physical_cols < b.cols)  // the padded tail of every real row
+        for (size_t r = 0; r < b.physical_rows; ++r) add_run(b.offset + r * b.cols + b.physical_cols, b.offset + (r + 1) * b.cols);
+      add_run(b.offset + b.physical_rows * b.cols, b.offset + b.rows * b.cols);  // padding rows
+    }
+    std::vector<uint64_t> seg;  // runs cut into pieces of at most kZeroPiece bytes
+    for (size_t i = 0; i < runs.size(); i += 2)
+      for (uint64_t a = runs[i]; a < runs[i + 1]; a += kZeroPiece) {
+        seg.push_back(a);
+        seg.push_back(std::min(a + kZeroPiece, runs[i + 1]));
       }
     if (!seg.empty()) {
       DBuf<uint64_t> dseg(seg.size());
       DBuf<unsigned int> flag(1);
       QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, c->stream));
       QF_CK(cudaMemsetAsync(flag.p, 0, 4, c->stream));
-      k_check_zero_segments<<<unsigned(std::min<size_t>(seg.size() / 2, 148 * 8)), 256, 0, c->stream>>>(
-          c->bva.p, dseg.p, uint32_t(seg.size() / 2), flag.p);
-      QF_CK(cudaGetLastError());
+      QF_LAUNCH(c->stream, "k_check_zero_segments", 0,
+                k_check_zero_segments<<<unsigned(std::min<size_t>(seg.size() / 2, 148 * 8)), 256, 0, c->stream>>>(
+                    c->bva.p, dseg.p, uint32_t(seg.size() / 2), flag.p));
       unsigned int h = 0;
       QF_CK(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, c->stream));
       QF_CK(cudaStreamSynchronize(c->stream));

@@ -299,14 +299,25 @@ const Fe* DeviceTables::alpha(const PcsParams<F>& pp, size_t level, int which) {
   return it->second.p;
 }
 
+// Grid of a persistent tile kernel: at most one CTA per SM (a CTA's 128 KiB of
+// tile planes leaves room for one), each looping over its tiles.
+static unsigned tile_grid(uint64_t n_tiles) {
+  static const int sms = [] {
+    int d = 0, n = 148;
+    if (cudaGetDevice(&d) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d) != cudaSuccess) n = 148;
+    return n;
+  }();
+  return unsigned(std::min<uint64_t>(n_tiles, uint64_t(sms)));
+}
+
 // The first min(12, logR) WHT levels of a 2^logm-entry half, optionally
 // multiplying by alpha first (a CTA size per variant).
 static void wht_tile_launch(cudaStream_t s, const Fe* src, Fe* dst, const Fe* alpha, int logR, int logm, int wl) {
-  const unsigned grid = unsigned(size_t(1) << (logm - wl));
+  const uint32_t tiles = uint32_t(size_t(1) << (logm - wl));
   if (alpha)
-    qfd::k_wht_tile<true><<<grid, qfd::kAlphaTileThreads, qfd::kTileSmem, s>>>(src, dst, alpha, logR, wl);
+    qfd::k_wht_tile<true><<<tile_grid(tiles), qfd::kAlphaTileThreads, qfd::kTileSmem, s>>>(src, dst, alpha, logR, wl, tiles);
   else
-    qfd::k_wht_tile<false><<<grid, qfd::kTileThreads, qfd::kTileSmem, s>>>(src, dst, nullptr, logR, wl);
+    qfd::k_wht_tile<false><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(src, dst, nullptr, logR, wl, tiles);
 }
 
 // Butterfly levels [from, to) over a half (message or parity at `base`) of
@@ -321,7 +332,8 @@ static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int fro
     const int cb = std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k);
     const size_t smem = qfd::kTileSmem;
     QF_LAUNCH(s, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
-              qfd::k_butterfly_strided<OP><<<unsigned(size_t(1) << (logm - k - cb)), qfd::kTileThreads, smem, s>>>(base, logR, lo, k, cb));
+              qfd::k_butterfly_strided<OP><<<tile_grid(uint64_t(1) << (logm - k - cb)), qfd::kTileThreads, smem, s>>>(
+                  base, logR, lo, k, cb, uint32_t(uint64_t(1) << (logm - k - cb))));
     lo += k;
   }
 }
@@ -394,8 +406,8 @@ Digest GpuBackend::commit_block(size_t b) {
   auto cw = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
-  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(bva_, active_, uint64_t(b) * P_.block_len,
-                                                                                    cw->cw.p, logR, l0));
+  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
+                bva_, active_, uint64_t(b) * P_.block_len, cw->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
   mobius_rest(cw->cw.p, logm, logR, l0);
   encode_and_hash(*cw, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
   if (blocks_.size() <= b) blocks_.resize(b + 1);
@@ -412,7 +424,8 @@ static void strided_passes_plain(cudaStream_t s, Fe* base, int logR, int logm, i
   for (int lo = from; lo < to;) {
     const int k = std::min(10, to - lo);
     const int cb = std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k);
-    qfd::k_butterfly_strided<OP><<<unsigned(size_t(1) << (logm - k - cb)), qfd::kTileThreads, qfd::kTileSmem, s>>>(base, logR, lo, k, cb);
+    qfd::k_butterfly_strided<OP><<<tile_grid(uint64_t(1) << (logm - k - cb)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
+        base, logR, lo, k, cb, uint32_t(uint64_t(1) << (logm - k - cb)));
     QF_CK(cudaGetLastError());
     lo += k;
   }
@@ -430,8 +443,8 @@ void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t act
   QF_CK(cudaMemcpyAsync(alpha, top.alphas[1].data(), R * 16, cudaMemcpyHostToDevice, s));
   // Message half: pack + Mobius.
   const int l0 = std::min(qfd::kMaxTileLog, logm);
-  qfd::k_pack_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
-      d_bva, active, uint64_t(b) * P.block_len, cw, logR, l0);
+  qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
+      d_bva, active, uint64_t(b) * P.block_len, cw, logR, l0, uint32_t(uint64_t(1) << (logm - l0)));
   QF_CK(cudaGetLastError());
   strided_passes_plain<qfd::kMobius>(s, cw, logR, logm, l0, logm);
   // Parity half: WHT(alpha * WHT(message)) per column.
@@ -566,7 +579,8 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
-  QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<unsigned(size_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(values_.p, folded_->cw.p, logR, l0));
+  QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
+                values_.p, folded_->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
   mobius_rest(folded_->cw.p, logm, logR, l0);
   encode_and_hash(*folded_, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
   sum_len_ = m;

@@ -133,7 +133,7 @@ __device__ __forceinline__ void planar_levels(uint32_t* planes, int log_n, int b
 // tile.  ld(t) returns the canonical value of tile element t (from HBM) and
 // st(t, u) stores element t packed.  For a full 4096-element tile with at
 // least three levels, the levels on tile bits 9..11 run in registers right
-// after the loads (pass_head) and the last one to three levels right before
+// after the loads (head_levels) and the last one to three levels right before
 // the stores (pass_tail): a thread owns 8 (or 4, 2) elements with all 8
 // coefficients, and consecutive threads take consecutive elements, so every
 // load and store instruction of a warp stays coalesced.  The levels between
@@ -163,18 +163,11 @@ __device__ __forceinline__ void reg_levels(uint32_t (&v)[1 << R][8], int lvl) {
   }
 }
 
-// Loads, levels 0..2 on tile bits 9..11, planes.  Thread g (512 per CTA) owns
-// tile elements g + (j << 9), j < 8.
-template <int OP, class Ld>
-__device__ __forceinline__ void pass_head(uint32_t* planes, Ld ld) {
+// Levels 0..2 on tile bits 9..11 from values already loaded, into the
+// planes.  Thread g (512 per CTA) owns tile elements g + (j << 9), j < 8.
+template <int OP>
+__device__ __forceinline__ void head_levels(uint32_t* planes, uint32_t (&v)[8][8]) {
   const int g = threadIdx.x;
-  uint32_t v[8][8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const Fr e = ld(g + (j << 9));
-#pragma unroll
-    for (int c = 0; c < 8; ++c) v[j][c] = e.c[c];
-  }
   reg_levels<OP, 3>(v, 0);
   const int pb = pidx(g);
 #pragma unroll
@@ -212,28 +205,64 @@ __device__ __forceinline__ void pass_tail(const uint32_t* planes, int zb, int lv
   }
 }
 
-template <int OP, class Ld, class St>
-__device__ __forceinline__ void tile_pass(uint32_t* planes, int log_n, int b0, Ld ld, St st) {
+// Runs the pass on tiles blockIdx.x, blockIdx.x + gridDim.x, ... < n_tiles.
+//   fetch(tile, t) -> Raw     the global load of tile element t
+//   conv(tile, t, raw) -> Fr  its canonical value
+//   st(tile, t, uint4)        the store of the packed result
+// Full 4096-element tiles with at least three levels take the register head
+// and tail, and the loads of a CTA's next tile are issued right after the
+// current tile's head, so they land while its middle and tail stages run.
+// A tile is read and written only by the CTA that owns it, so in-place
+// passes (src == dst) stay race free.
+template <int OP, class Raw, class Fetch, class Conv, class St>
+__device__ __forceinline__ void tile_loop(uint32_t* planes, int log_n, int b0, uint32_t n_tiles, Fetch fetch, Conv conv,
+                                          St st) {
   const int n = 1 << log_n;
   if (log_n == kMaxTileLog && log_n - b0 >= 3 && blockDim.x == kTileThreads) {
-    pass_head<OP>(planes, ld);
-    const int rem = 9 - b0;  // level bits [b0, 9) are left
+    const int g = threadIdx.x;
+    const int rem = 9 - b0;  // level bits [b0, 9) follow the head
     const int rz = rem < 3 ? rem : 3;
     const int rm = rem - rz;
-    planar_levels<OP>(planes, log_n, b0, rm, 3);
-    switch (rz) {
-      case 3: pass_tail<OP, 3>(planes, 9 - 3, 3 + rm, st); break;
-      case 2: pass_tail<OP, 2>(planes, 9 - 2, 3 + rm, st); break;
-      case 1: pass_tail<OP, 1>(planes, 9 - 1, 3 + rm, st); break;
-      default:
-        for (int t = threadIdx.x; t < n; t += blockDim.x) st(t, planar_get_packed(planes, t));
+    Raw raw[8];
+    uint32_t tile = blockIdx.x;
+    if (tile < n_tiles)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+    for (; tile < n_tiles; tile += gridDim.x) {
+      {
+        uint32_t v[8][8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const Fr e = conv(tile, g + (j << 9), raw[j]);
+#pragma unroll
+          for (int c = 0; c < 8; ++c) v[j][c] = e.c[c];
+        }
+        head_levels<OP>(planes, v);
+      }
+      const uint32_t next = tile + gridDim.x;
+      if (next < n_tiles)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
+      planar_levels<OP>(planes, log_n, b0, rm, 3);
+      auto st_t = [&](int t, uint4 u) { st(tile, t, u); };
+      switch (rz) {
+        case 3: pass_tail<OP, 3>(planes, 9 - 3, 3 + rm, st_t); break;
+        case 2: pass_tail<OP, 2>(planes, 9 - 2, 3 + rm, st_t); break;
+        case 1: pass_tail<OP, 1>(planes, 9 - 1, 3 + rm, st_t); break;
+        default:
+          for (int t = threadIdx.x; t < n; t += blockDim.x) st(tile, t, planar_get_packed(planes, t));
+      }
+      __syncthreads();  // the next head overwrites the planes
     }
     return;
   }
-  for (int t = threadIdx.x; t < n; t += blockDim.x) planar_put(planes, t, ld(t));
-  __syncthreads();
-  planar_levels<OP>(planes, log_n, b0, log_n - b0);
-  for (int t = threadIdx.x; t < n; t += blockDim.x) st(t, planar_get_packed(planes, t));
+  for (uint32_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    for (int t = threadIdx.x; t < n; t += blockDim.x) planar_put(planes, t, conv(tile, t, fetch(tile, t)));
+    __syncthreads();
+    planar_levels<OP>(planes, log_n, b0, log_n - b0);
+    for (int t = threadIdx.x; t < n; t += blockDim.x) st(tile, t, planar_get_packed(planes, t));
+    __syncthreads();
+  }
 }
 
 __device__ __forceinline__ Fr unpack(uint4 u) {
@@ -243,81 +272,84 @@ __device__ __forceinline__ Fr unpack(uint4 u) {
   return v;
 }
 
-// Pack eight signed weights per element, then Mobius levels [0, levels) in a
-// tile; write into the message half.  `src_base` is the block's first BVA index.
+// Pack eight signed weights per element, then Mobius levels [0, levels) in
+// tiles of 2^levels elements; write into the message half.  `src_base` is
+// the block's first BVA index.
 __global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t active,
-                                                                     uint64_t src_base, Fe* __restrict__ cw, int logR, int levels) {
+                                                                     uint64_t src_base, Fe* __restrict__ cw, int logR, int levels,
+                                                                     uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  const size_t first = size_t(blockIdx.x) << levels;
-  auto ld = [=](int t) {
-    const uint64_t g = src_base + 8ull * (first + t);
-    uint2 raw = make_uint2(0, 0);
-    if (g + 8 <= active) {
-      raw = *reinterpret_cast<const uint2*>(bva + g);
-    } else {
-      uint32_t w[2] = {0, 0};
-      for (int k = 0; k < 8; ++k)
-        if (g + k < active) w[k >> 2] |= uint32_t(uint8_t(bva[g + k])) << (8 * (k & 3));
-      raw = make_uint2(w[0], w[1]);
-    }
+  auto fetch = [=](uint32_t tile, int t) {
+    const uint64_t g = src_base + 8ull * ((uint64_t(tile) << levels) + t);
+    if (g + 8 <= active) return *reinterpret_cast<const uint2*>(bva + g);
+    uint32_t w[2] = {0, 0};
+    for (int k = 0; k < 8; ++k)
+      if (g + k < active) w[k >> 2] |= uint32_t(uint8_t(bva[g + k])) << (8 * (k & 3));
+    return make_uint2(w[0], w[1]);
+  };
+  auto conv = [](uint32_t, int, uint2 raw) {
     Fr r;
 #pragma unroll
     for (int k = 0; k < 8; ++k) r.c[k] = small(int(int8_t(((k < 4 ? raw.x : raw.y) >> (8 * (k & 3))) & 0xffu)));
     return r;
   };
-  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(cw + msg_addr(first + t, logR)) = u; };
-  tile_pass<kMobius>(planes_s, levels, 0, ld, st);
+  auto st = [=](uint32_t tile, int t, uint4 u) {
+    *reinterpret_cast<uint4*>(cw + msg_addr((size_t(tile) << levels) + t, logR)) = u;
+  };
+  tile_loop<kMobius, uint2>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
 // Same, but the packed values come from an element vector (the block-folded
 // table), which is left untouched for the sumcheck.
 __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* __restrict__ src, Fe* __restrict__ cw, int logR,
-                                                                     int levels) {
+                                                                     int levels, uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  const size_t first = size_t(blockIdx.x) << levels;
-  auto ld = [=](int t) { return load(src + first + t); };
-  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(cw + msg_addr(first + t, logR)) = u; };
-  tile_pass<kMobius>(planes_s, levels, 0, ld, st);
+  auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + (size_t(tile) << levels) + t); };
+  auto conv = [](uint32_t, int, uint4 raw) { return unpack(raw); };
+  auto st = [=](uint32_t tile, int t, uint4 u) {
+    *reinterpret_cast<uint4*>(cw + msg_addr((size_t(tile) << levels) + t, logR)) = u;
+  };
+  tile_loop<kMobius, uint4>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
-// WHT levels [0, levels) within a tile (levels <= logR so columns never mix).
+// WHT levels [0, levels) within tiles (levels <= logR so columns never mix).
 // Reads the message (or parity) half at src, with ALPHA multiplies each row
-// by alpha[r] first, writes the parity half (src may equal dst: a CTA reads
-// its whole tile before it writes).
+// by alpha[r] first, writes the parity half (src may equal dst).
 template <bool ALPHA>
 __global__ void __launch_bounds__(ALPHA ? kAlphaTileThreads : kTileThreads, 1)
-    k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR, int levels) {
+    k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR, int levels, uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  const size_t first = size_t(blockIdx.x) << levels;
   // For a message-half address a = c * 2R + r, a & (R - 1) = r.
   const size_t rmask = (size_t(1) << logR) - 1;
-  auto ld = [=](int t) {
-    const size_t a = msg_addr(first + t, logR);
-    const Fr v = unpack(*reinterpret_cast<const uint4*>(src + a));
-    return ALPHA ? mul(v, load(alpha + (a & rmask))) : v;
+  auto addr = [=](uint32_t tile, int t) { return msg_addr((size_t(tile) << levels) + t, logR); };
+  auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + addr(tile, t)); };
+  auto conv = [=](uint32_t tile, int t, uint4 raw) {
+    const Fr v = unpack(raw);
+    return ALPHA ? mul(v, load(alpha + (addr(tile, t) & rmask))) : v;
   };
-  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(dst + msg_addr(first + t, logR)) = u; };
-  tile_pass<kWht>(planes_s, levels, 0, ld, st);
+  auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(dst + addr(tile, t)) = u; };
+  tile_loop<kWht, uint4>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
 // Levels [lo, lo + k) over the logical index space, on the half starting at
-// `base` (cw for the message, cw + R for the parity).  Each CTA owns 2^cb
-// consecutive group bases (64-byte runs in HBM at cb = 2, longer above):
-// tile element t = (j << cb) + c is logical index base(g0 + c) + (j << lo),
-// so the levels act on tile bits [cb, cb + k).
+// `base` (cw for the message, cw + R for the parity).  Tile `tile` owns 2^cb
+// consecutive group bases g0 = tile << cb (64-byte runs in HBM at cb = 2,
+// longer above): tile element t = (j << cb) + c is logical index
+// base(g0 + c) + (j << lo), so the levels act on tile bits [cb, cb + k).
 template <int OP>
-__global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k, int cb) {
+__global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k, int cb,
+                                                                      uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  const size_t g0 = size_t(blockIdx.x) << cb;
   const size_t low_mask = (size_t(1) << lo) - 1;
   const int cmask = (1 << cb) - 1;
-  auto addr = [=](int t) {
-    const size_t g = g0 + (t & cmask);
+  auto addr = [=](uint32_t tile, int t) {
+    const size_t g = (size_t(tile) << cb) + (t & cmask);
     return msg_addr((((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(t >> cb) << lo), logR);
   };
-  auto ld = [=](int t) { return unpack(*reinterpret_cast<const uint4*>(base + addr(t))); };
-  auto st = [=](int t, uint4 u) { *reinterpret_cast<uint4*>(base + addr(t)) = u; };
-  tile_pass<OP>(planes_s, cb + k, cb, ld, st);
+  auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(base + addr(tile, t)); };
+  auto conv = [](uint32_t, int, uint4 raw) { return unpack(raw); };
+  auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(base + addr(tile, t)) = u; };
+  tile_loop<OP, uint4>(planes_s, cb + k, cb, n_tiles, fetch, conv, st);
 }
 
 // ---------------------------------------------------------------- hashing
