@@ -44,6 +44,29 @@ __global__ void k_check_zero_segments(const int8_t* __restrict__ bva, const uint
 
 }  // namespace
 
+// A side stream for the weight transfer, with one event per block.
+struct CopyPipeline {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t begin = nullptr, end = nullptr;
+  std::vector<cudaEvent_t> landed;
+  explicit CopyPipeline(size_t blocks) : landed(blocks, nullptr) {
+    QF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    QF_CK(cudaEventCreate(&begin));
+    QF_CK(cudaEventCreate(&end));
+    for (auto& e : landed) QF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  ~CopyPipeline() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& e : landed)
+      if (e) cudaEventDestroy(e);
+    if (begin) cudaEventDestroy(begin);
+    if (end) cudaEventDestroy(end);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  CopyPipeline(const CopyPipeline&) = delete;
+  CopyPipeline& operator=(const CopyPipeline&) = delete;
+};
+
 struct qf_committed {
   const qf_params* params = nullptr;
   cudaStream_t stream = nullptr;
@@ -174,10 +197,29 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
     QF_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     auto t0 = std::chrono::steady_clock::now();
     c->bva.alloc(std::max<uint64_t>(n_values, 8));
-    QF_CK(cudaMemcpyAsync(c->bva.p, bva, n_values, bva_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->stream));
-    QF_CK(cudaStreamSynchronize(c->stream));
-    c->upload_ms = ms_since(t0);
-    t0 = std::chrono::steady_clock::now();
+    // The weights arrive block by block on a copy stream; block b is committed
+    // as soon as its bytes have landed, so the transfer of block b + 1
+    // overlaps the encoding and hashing of block b.
+    const size_t live = std::min<size_t>(P.blocks(), (n_values + P.block_len - 1) / P.block_len);
+    CopyPipeline copies(live);
+    const cudaMemcpyKind kind = bva_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    QF_CK(cudaEventRecord(copies.begin, copies.stream));
+    for (size_t b = 0; b < live; ++b) {
+      const uint64_t a = uint64_t(b) * P.block_len, e = std::min<uint64_t>(a + P.block_len, n_values);
+      QF_CK(cudaMemcpyAsync(c->bva.p + a, static_cast<const int8_t*>(bva) + a, e - a, kind, copies.stream));
+      QF_CK(cudaEventRecord(copies.landed[b], copies.stream));
+    }
+    QF_CK(cudaEventRecord(copies.end, copies.stream));
+    c->be = std::make_unique<GpuBackend>(P, c->bva.p, n_values, c->stream, params->tables.get());
+    for (size_t b = 0; b < P.blocks(); ++b) {
+      if (b < live) QF_CK(cudaStreamWaitEvent(c->stream, copies.landed[b], 0));
+      c->roots.push_back(c->be->commit_block(b));
+    }
+    QF_CK(cudaStreamWaitEvent(c->stream, copies.end, 0));
+    QF_CK(cudaEventSynchronize(copies.end));
+    float up = 0;
+    QF_CK(cudaEventElapsedTime(&up, copies.begin, copies.end));
+    c->upload_ms = up;
     // Padding must be zero (validate_values) — checked on the device.
     std::vector<uint64_t> runs;
     auto add_run = [&](uint64_t a, uint64_t e) {
@@ -209,8 +251,6 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
       QF_CK(cudaStreamSynchronize(c->stream));
       check(h == 0, "nonzero boundary padding");
     }
-    c->be = std::make_unique<GpuBackend>(P, c->bva.p, n_values, c->stream, params->tables.get());
-    for (size_t b = 0; b < P.blocks(); ++b) c->roots.push_back(c->be->commit_block(b));
     QF_CK(cudaStreamSynchronize(c->stream));
     c->commit_ms = ms_since(t0);
     if (roots_out)
