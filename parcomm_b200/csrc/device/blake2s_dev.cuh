@@ -9,15 +9,23 @@ __constant__ uint32_t kIv[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0xA54FF53
                                 0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
 
 __device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
+// a + b as a 32-bit multiply-add by `one` (a runtime 1 from the kernel's
+// arguments): it issues to the FMA pipe, leaving the ALU pipe, which the
+// XORs and rotations keep busy, to them.
+__device__ __forceinline__ uint32_t add_fma(uint32_t a, uint32_t b, uint32_t one) {
+  uint32_t d;
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(b), "r"(one), "r"(a));
+  return d;
+}
 
-#define QFD_G(a, b, c, d, x, y)          \
-  v[a] = v[a] + v[b] + (x);              \
-  v[d] = rotr(v[d] ^ v[a], 16);          \
-  v[c] = v[c] + v[d];                    \
-  v[b] = rotr(v[b] ^ v[c], 12);          \
-  v[a] = v[a] + v[b] + (y);              \
-  v[d] = rotr(v[d] ^ v[a], 8);           \
-  v[c] = v[c] + v[d];                    \
+#define QFD_G(a, b, c, d, x, y)                         \
+  v[a] = add_fma(add_fma(v[a], v[b], one), (x), one);   \
+  v[d] = rotr(v[d] ^ v[a], 16);                         \
+  v[c] = add_fma(v[c], v[d], one);                      \
+  v[b] = rotr(v[b] ^ v[c], 12);                         \
+  v[a] = add_fma(add_fma(v[a], v[b], one), (y), one);   \
+  v[d] = rotr(v[d] ^ v[a], 8);                          \
+  v[c] = add_fma(v[c], v[d], one);                      \
   v[b] = rotr(v[b] ^ v[c], 7);
 
 #define QFD_ROUND(s0, s1, s2, s3, s4, s5, s6, s7, s8, s9, s10, s11, s12, s13, s14, s15) \
@@ -30,9 +38,9 @@ __device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return __funnelshi
   QFD_G(2, 7, 8, 13, m[s12], m[s13]);                                                   \
   QFD_G(3, 4, 9, 14, m[s14], m[s15]);
 
-// h <- compress(h, m, t, last).  The sigma schedule is unrolled so every
-// message index is a compile-time constant.
-__device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], uint32_t t, bool last) {
+// h <- compress(h, m, t, last); `one` must be 1.  The sigma schedule is
+// unrolled so every message index is a compile-time constant.
+__device__ __forceinline__ void compress(uint32_t h[8], const uint32_t m[16], uint32_t t, bool last, uint32_t one) {
   uint32_t v[16];
 #pragma unroll
   for (int i = 0; i < 8; ++i) { v[i] = h[i]; v[i + 8] = kIv[i]; }

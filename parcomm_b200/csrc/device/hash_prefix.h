@@ -11,11 +11,13 @@ namespace qfd {
 struct LeafPrefix {
   uint32_t mid[8];
   uint32_t tail[4];  // 11 (base-row) or 16 (extension-row) bytes
+  uint32_t one = 1;  // the multiplier of the compression's multiply-add additions
 };
 
 // Inner message = 50-byte framed domain || left || right.
 struct InnerPrefix {
   uint32_t w[13];  // last word holds 2 bytes
+  uint32_t one = 1;  // the multiplier of the compression's multiply-add additions
 };
 
 }  // namespace qfd

@@ -400,7 +400,7 @@ __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restri
       m[w] = word;
     }
     const bool last = j == nblocks;
-    compress(h, m, last ? total : 64u + 64u * uint32_t(j), last);
+    compress(h, m, last ? total : 64u + 64u * uint32_t(j), last, pre.one);
   }
   leaves[2 * r] = make_uint4(h[0], h[1], h[2], h[3]);
   leaves[2 * r + 1] = make_uint4(h[4], h[5], h[6], h[7]);
@@ -429,8 +429,8 @@ __global__ void k_hash_inner(const uint4* __restrict__ children, uint64_t n_pare
 #pragma unroll
   for (int k = 0; k < 8; ++k) h[k] = kIv[k];
   h[0] ^= 0x01010020u;
-  compress(h, buf, 64u, false);
-  compress(h, buf + 16, 114u, true);
+  compress(h, buf, 64u, false, pre.one);
+  compress(h, buf + 16, 114u, true, pre.one);
   parents[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
   parents[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
