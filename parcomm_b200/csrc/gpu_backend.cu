@@ -293,7 +293,10 @@ const Fe* DeviceTables::alpha(const PcsParams<F>& pp, size_t level, int which) {
   if (it == bufs_.end()) {
     const auto& a = pp.seq.codes.at(level).alphas.at(size_t(which));
     DBuf<Fe> b(a.size());
+    // A copy from pageable memory may return before its DMA has landed, and
+    // the readers run on non-blocking streams: wait for the legacy stream.
     QF_CK(cudaMemcpy(b.p, a.data(), a.size() * 16, cudaMemcpyHostToDevice));
+    QF_CK(cudaStreamSynchronize(0));
     it = bufs_.emplace(key, std::move(b)).first;
   }
   return it->second.p;

@@ -62,6 +62,16 @@ def test_ragged_shapes_multilevel(packed_log):
     run_both(shapes, 14, packed_log, mats)
 
 
+@pytest.mark.parametrize("rows,chunk_log", [(4096, 24), (2048, 23), (4096, 25)])
+def test_single_matrix_deep_code_sequences(rows, chunk_log):
+    """One matrix per statement, as in the per-matrix path: chunk 23-25 give
+    code sequences whose Decide levels with a carried codeword have 2^10 to
+    2^12 rows, run on the device."""
+    rng = np.random.default_rng(rows + chunk_log)
+    mats = [gaussian_i8(rng, rows * 4096, forced=0.001).reshape(rows, 4096)]
+    run_both([(rows, 4096)], chunk_log, 4, mats)
+
+
 def test_single_block_opening():
     rng = np.random.default_rng(3)
     mats = [gaussian_i8(rng, 64 * 64).reshape(64, 64)]
