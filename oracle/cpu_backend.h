@@ -313,7 +313,7 @@ ProveResult<F, T> prove_all(const Parameters<F>& P, const T* values, size_t n, b
   Transcript<F> t = statement_transcript(P, out.statement, out.claims);
   Query<F> q = compile(P.layout, out.claims, t);
   auto [eo, term] = eo_prove<F>(be, P.layout.logical, size_t(1) << P.config.packed_log, q, t);
-  std::vector<uint8_t> ctx = opening_context(t.state, 0);
+  std::vector<uint8_t> ctx = opening_context<F>(t.state, 0);
   BatchOpening<F> op = roots.size() > 1 ? open_batch(P.pcs, be, roots, term.point_msb, ctx)
                                         : open_single(P.pcs, be, roots[0], term.point_msb, ctx);
   check(op.claimed_value * term.scale == term.value, "QAFold/EO terminal mismatch");

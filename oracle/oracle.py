@@ -32,15 +32,19 @@ def lib() -> ctypes.CDLL:
         L.qfo_last_error.restype = ctypes.c_char_p
         L.qfo_free.argtypes = [P]
         L.qfo_free.restype = None
-        L.qfo_prove.argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
-                                P, ctypes.c_uint64, ctypes.c_char_p, S, BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S),
-                                BPP, ctypes.POINTER(S), ctypes.POINTER(ctypes.c_double)]
-        L.qfo_commit_roots.argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
-                                       ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S]
-        L.qfo_demo.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+        for name in ("qfo_prove", "qfo_prove_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, BPP, ctypes.POINTER(S),
+                                         BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S), ctypes.POINTER(ctypes.c_double)]
+        for name in ("qfo_commit_roots", "qfo_commit_roots_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S]
+        for name in ("qfo_demo", "qfo_demo_kb"):
+            getattr(L, name).argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
         L.qfo_wire_fixture.argtypes = [ctypes.c_char_p]
-        L.qfo_verify.argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
-                                 ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
+        for name in ("qfo_verify", "qfo_verify_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
         _lib = L
     return _lib
 
@@ -69,31 +73,40 @@ def _take(p, n):
         lib().qfo_free(ctypes.cast(p, ctypes.c_void_p))
 
 
-def prove(shapes, chunk_log, packed_log, values, claims: bytes | None = None, rf_bits=100):
+# field: "f65521" (F65521^8, signed 8-bit weights) or "koalabear" (KoalaBear^4,
+# signed 16-bit payloads).
+_SUFFIX = {"f65521": ("", np.int8), "koalabear": ("_kb", np.int16)}
+
+
+def prove(shapes, chunk_log, packed_log, values, claims: bytes | None = None, rf_bits=100, field="f65521"):
     """Returns (roots, claims, proof, (commit_ms, open_ms)) from the CPU restatement."""
+    sfx, dt = _SUFFIX[field]
     arr, n = _shapes(shapes)
-    v = np.ascontiguousarray(values, dtype=np.int8)
+    v = np.ascontiguousarray(values, dtype=dt)
     outs = [ctypes.POINTER(ctypes.c_uint8)() for _ in range(3)]
     lens = [ctypes.c_size_t() for _ in range(3)]
     t = (ctypes.c_double * 2)()
-    _check(lib().qfo_prove(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size, claims,
-                           len(claims) if claims else 0, ctypes.byref(outs[0]), ctypes.byref(lens[0]),
-                           ctypes.byref(outs[1]), ctypes.byref(lens[1]), ctypes.byref(outs[2]), ctypes.byref(lens[2]), t))
+    _check(getattr(lib(), "qfo_prove" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size, claims,
+                                            len(claims) if claims else 0, ctypes.byref(outs[0]), ctypes.byref(lens[0]),
+                                            ctypes.byref(outs[1]), ctypes.byref(lens[1]), ctypes.byref(outs[2]),
+                                            ctypes.byref(lens[2]), t))
     return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2]), (t[0], t[1])
 
 
-def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100):
+def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):
+    sfx, dt = _SUFFIX[field]
     arr, n = _shapes(shapes)
-    v = np.ascontiguousarray(values, dtype=np.int8)
+    v = np.ascontiguousarray(values, dtype=dt)
     buf = ctypes.create_string_buffer(32 * 128)
-    _check(lib().qfo_commit_roots(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size, buf, 32 * 128))
+    _check(getattr(lib(), "qfo_commit_roots" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size, buf,
+                                                   32 * 128))
     return buf.raw
 
 
-def demo():
+def demo(field="f65521"):
     d = ctypes.create_string_buffer(32)
     pl, jl = ctypes.c_uint64(), ctypes.c_uint64()
-    _check(lib().qfo_demo(d, ctypes.byref(pl), ctypes.byref(jl)))
+    _check(getattr(lib(), "qfo_demo" + _SUFFIX[field][0])(d, ctypes.byref(pl), ctypes.byref(jl)))
     return d.raw, pl.value, jl.value
 
 
@@ -103,7 +116,8 @@ def wire_fixture():
     return d.raw
 
 
-def verify(shapes, chunk_log, packed_log, roots: bytes, claims: bytes, proof: bytes, rf_bits=100) -> bool:
+def verify(shapes, chunk_log, packed_log, roots: bytes, claims: bytes, proof: bytes, rf_bits=100, field="f65521") -> bool:
     arr, n = _shapes(shapes)
-    rc = lib().qfo_verify(arr, n, chunk_log, packed_log, rf_bits, roots, claims, len(claims), proof, len(proof))
+    rc = getattr(lib(), "qfo_verify" + _SUFFIX[field][0])(arr, n, chunk_log, packed_log, rf_bits, roots, claims,
+                                                         len(claims), proof, len(proof))
     return rc == 0

@@ -34,13 +34,14 @@ uint8_t* dup(const std::vector<uint8_t>& v) {
   if (!v.empty()) std::memcpy(p, v.data(), v.size());
   return p;
 }
-F sample_uniform(StdRng& rng) {
+template <class G = F>
+G sample_uniform(StdRng& rng) {
   for (;;) {
     uint8_t b[16];
     uint64_t a = rng.next_u64(), c = rng.next_u64();
     for (int i = 0; i < 8; ++i) { b[i] = uint8_t(a >> (8 * i)); b[8 + i] = uint8_t(c >> (8 * i)); }
-    F v;
-    if (F::from_uniform_bytes(b, v)) return v;
+    G v;
+    if (G::from_uniform_bytes(b, v)) return v;
   }
 }
 std::vector<Shape> shapes_of(const uint64_t* s, size_t n) {
@@ -48,43 +49,34 @@ std::vector<Shape> shapes_of(const uint64_t* s, size_t n) {
   for (size_t i = 0; i < n; ++i) out.push_back({size_t(s[2 * i]), size_t(s[2 * i + 1])});
   return out;
 }
-}  // namespace
-
-extern "C" {
-
-const char* qfo_last_error() { return g_err.c_str(); }
-void qfo_free(void* p) { std::free(p); }
-
-// Full prover over a BVA.  `claims` may be null: the benchmark points of
-// main.rs:190-204 are then used.  Outputs (malloc'd): roots (blocks*32),
-// claims (claims wire), proof (bincode).  `times_ms` = {commit, open}.
-int qfo_prove(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
-              const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint8_t** roots,
-              size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len,
-              double* times_ms) {
+template <class G, class T>
+int prove_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+               const T* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint8_t** roots,
+               size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len,
+               double* times_ms) {
   return guarded([&] {
     Config c;
     c.chunk_log = chunk_log;
     c.packed_log = packed_log;
     c.query_rf_bits = rf_bits;
-    auto P = make_parameters<F>(shapes_of(shapes, n_shapes), c);
-    std::vector<Claim<F>> given;
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
+    std::vector<Claim<G>> given;
     if (claims_in) {
       ByteReader r(claims_in, claims_len);
       for (const Shape& s : P->layout.shapes) {
-        Claim<F> cl;
-        for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) cl.row.push_back(r.field<F>());
-        for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) cl.col.push_back(r.field<F>());
-        cl.value = r.field<F>();
+        Claim<G> cl;
+        for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) cl.row.push_back(r.field<G>());
+        for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) cl.col.push_back(r.field<G>());
+        cl.value = r.field<G>();
         given.push_back(cl);
       }
     }
-    auto res = qf_oracle::prove_all<F, int8_t>(*P, bva, n_values, claims_in == nullptr, claims_in ? &given : nullptr);
+    auto res = qf_oracle::prove_all<G, T>(*P, bva, n_values, claims_in == nullptr, claims_in ? &given : nullptr);
     ByteWriter rw, cw;
     for (const auto& d : res.statement.roots) rw.digest(d);
     for (const auto& cl : res.claims) {
-      for (const F& v : cl.row) cw.field(v);
-      for (const F& v : cl.col) cw.field(v);
+      for (const G& v : cl.row) cw.field(v);
+      for (const G& v : cl.col) cw.field(v);
       cw.field(cl.value);
     }
     *roots = dup(rw.out);
@@ -97,18 +89,18 @@ int qfo_prove(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint3
   });
 }
 
-// Commitment roots only (protocol.rs:131-185).
-int qfo_commit_roots(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
-                     const int8_t* bva, uint64_t n_values, uint8_t* roots_out, size_t cap) {
+template <class G, class T>
+int commit_roots_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                      const T* bva, uint64_t n_values, uint8_t* roots_out, size_t cap) {
   return guarded([&] {
     Config c;
     c.chunk_log = chunk_log;
     c.packed_log = packed_log;
     c.query_rf_bits = rf_bits;
-    auto P = make_parameters<F>(shapes_of(shapes, n_shapes), c);
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
     validate_values(P->layout, bva, n_values);
     if (cap < 32 * P->blocks()) fail(-9, "roots buffer too small");
-    qf_oracle::CpuBackend<F, int8_t> be(*P, bva, n_values);
+    qf_oracle::CpuBackend<G, T> be(*P, bva, n_values);
     for (size_t b = 0; b < P->blocks(); ++b) {
       Digest d = be.commit_block(b);
       std::memcpy(roots_out + 32 * b, d.data(), 32);
@@ -116,27 +108,98 @@ int qfo_commit_roots(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log
   });
 }
 
-// Golden vector 1: the demo bundle's proof digest and length.
-int qfo_demo(uint8_t digest_out[32], uint64_t* proof_len, uint64_t* statement_json_len) {
+// The demo bundle (main.rs:108-145): shapes 31x37, 65x17, 1x7, 9x1, entry
+// (e * 73 + i * 19) truncated to the payload width, chunk 10, packed_log 4.
+template <class G, class T, class U>
+int demo_impl(uint8_t digest_out[32], uint64_t* proof_len, uint64_t* statement_json_len) {
   return guarded([&] {
     std::vector<Shape> shapes = {{31, 37}, {65, 17}, {1, 7}, {9, 1}};
     Config c;
     c.chunk_log = 10;
     c.packed_log = 4;
-    auto P = make_parameters<F>(shapes, c);
-    std::vector<std::vector<int8_t>> mats;
+    auto P = make_parameters<G>(shapes, c);
+    std::vector<std::vector<T>> mats;
     for (size_t i = 0; i < shapes.size(); ++i) {
-      std::vector<int8_t> m(shapes[i].rows * shapes[i].cols);
-      for (size_t e = 0; e < m.size(); ++e) m[e] = int8_t(uint8_t(e * 73 + i * 19));
+      std::vector<T> m(shapes[i].rows * shapes[i].cols);
+      for (size_t e = 0; e < m.size(); ++e) m[e] = T(U(e * 73 + i * 19));
       mats.push_back(m);
     }
-    auto vals = layout_encode<int8_t>(P->layout, mats);
-    auto res = qf_oracle::prove_all<F, int8_t>(*P, vals.data(), vals.size(), true);
+    auto vals = layout_encode<T>(P->layout, mats);
+    auto res = qf_oracle::prove_all<G, T>(*P, vals.data(), vals.size(), true);
     Digest d = blake2s(res.wire.data(), res.wire.size());
     std::memcpy(digest_out, d.data(), 32);
     *proof_len = res.wire.size();
     *statement_json_len = commitment_json(res.statement).size();
   });
+}
+
+template <class G>
+int verify_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                const uint8_t* roots, const uint8_t* claims_in, size_t claims_len, const uint8_t* proof, size_t proof_len) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
+    std::vector<Digest> rs(P->blocks());
+    for (size_t b = 0; b < rs.size(); ++b) std::memcpy(rs[b].data(), roots + 32 * b, 32);
+    ByteReader r(claims_in, claims_len);
+    std::vector<Claim<G>> cl;
+    for (const Shape& s : P->layout.shapes) {
+      Claim<G> x;
+      for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) x.row.push_back(r.field<G>());
+      for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) x.col.push_back(r.field<G>());
+      x.value = r.field<G>();
+      cl.push_back(x);
+    }
+    verify_proof(*P, make_statement(*P, rs), cl, proof_from_bytes<G>(proof, proof_len));
+  });
+}
+}  // namespace
+
+extern "C" {
+
+const char* qfo_last_error() { return g_err.c_str(); }
+void qfo_free(void* p) { std::free(p); }
+
+// Full prover over a BVA.  `claims` may be null: the benchmark points of
+// main.rs:190-204 are then used.  Outputs (malloc'd): roots (blocks*32),
+// claims (claims wire), proof (bincode).  `times_ms` = {commit, open}.
+// F65521^8 with signed 8-bit weights; the _kb variants take KoalaBear^4 and
+// signed 16-bit payloads (qafold/koalabear).
+int qfo_prove(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+              const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint8_t** roots,
+              size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len,
+              double* times_ms) {
+  return prove_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in, claims_len, roots,
+                                 roots_len, claims_out, claims_out_len, proof, proof_len, times_ms);
+}
+int qfo_prove_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                 const int16_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint8_t** roots,
+                 size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len,
+                 double* times_ms) {
+  return prove_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in, claims_len, roots,
+                                  roots_len, claims_out, claims_out_len, proof, proof_len, times_ms);
+}
+
+// Commitment roots only (protocol.rs:131-185).
+int qfo_commit_roots(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                     const int8_t* bva, uint64_t n_values, uint8_t* roots_out, size_t cap) {
+  return commit_roots_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, roots_out, cap);
+}
+int qfo_commit_roots_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                        const int16_t* bva, uint64_t n_values, uint8_t* roots_out, size_t cap) {
+  return commit_roots_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, roots_out, cap);
+}
+
+// Golden vector 1: the F65521 demo bundle's proof digest and length.
+int qfo_demo(uint8_t digest_out[32], uint64_t* proof_len, uint64_t* statement_json_len) {
+  return demo_impl<Fp8, int8_t, uint8_t>(digest_out, proof_len, statement_json_len);
+}
+// Golden vector G2: the KoalaBear demo bundle (entries truncated to u16, read as i16).
+int qfo_demo_kb(uint8_t digest_out[32], uint64_t* proof_len, uint64_t* statement_json_len) {
+  return demo_impl<Kb4, int16_t, uint16_t>(digest_out, proof_len, statement_json_len);
 }
 
 // Golden vector 2: BLAKE2s(root || opening || decide) of the native-opening
@@ -170,25 +233,11 @@ int qfo_wire_fixture(uint8_t digest_out[32]) {
 // Independent verification of a proof (protocol.rs:266-320).
 int qfo_verify(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
                const uint8_t* roots, const uint8_t* claims_in, size_t claims_len, const uint8_t* proof, size_t proof_len) {
-  return guarded([&] {
-    Config c;
-    c.chunk_log = chunk_log;
-    c.packed_log = packed_log;
-    c.query_rf_bits = rf_bits;
-    auto P = make_parameters<F>(shapes_of(shapes, n_shapes), c);
-    std::vector<Digest> rs(P->blocks());
-    for (size_t b = 0; b < rs.size(); ++b) std::memcpy(rs[b].data(), roots + 32 * b, 32);
-    ByteReader r(claims_in, claims_len);
-    std::vector<Claim<F>> cl;
-    for (const Shape& s : P->layout.shapes) {
-      Claim<F> x;
-      for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) x.row.push_back(r.field<F>());
-      for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) x.col.push_back(r.field<F>());
-      x.value = r.field<F>();
-      cl.push_back(x);
-    }
-    verify_proof(*P, make_statement(*P, rs), cl, proof_from_bytes<F>(proof, proof_len));
-  });
+  return verify_impl<Fp8>(shapes, n_shapes, chunk_log, packed_log, rf_bits, roots, claims_in, claims_len, proof, proof_len);
+}
+int qfo_verify_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                  const uint8_t* roots, const uint8_t* claims_in, size_t claims_len, const uint8_t* proof, size_t proof_len) {
+  return verify_impl<Kb4>(shapes, n_shapes, chunk_log, packed_log, rf_bits, roots, claims_in, claims_len, proof, proof_len);
 }
 
 }  // extern "C"

@@ -307,7 +307,7 @@ int qf_prove(const qf_params* params, qf_committed* committed, const uint8_t* cl
     Query<F> q = compile(P.layout, cl, t);
     auto [eo, term] = eo_prove<F>(*committed->be, P.layout.logical, size_t(1) << P.config.packed_log, q, t);
     double eo_ms = ms_since(t0);
-    std::vector<uint8_t> ctx = opening_context(t.state, 0);
+    std::vector<uint8_t> ctx = opening_context<F>(t.state, 0);
     BatchOpening<F> op = committed->roots.size() > 1 ? open_batch(P.pcs, *committed->be, committed->roots, term.point_msb, ctx)
                                                     : open_single(P.pcs, *committed->be, committed->roots[0], term.point_msb, ctx);
     check(op.claimed_value * term.scale == term.value, "QAFold/EO terminal mismatch");

@@ -51,6 +51,9 @@ struct Fp8 {
   // Packed-PCS transcript domain and single-block proof magic (packed.rs:19, 442).
   static constexpr const char* kPackedDomain = "mikros/qafold-f65521-ext8/packed-boolean-mle/v1";
   static constexpr const char* kPackedMagic = "QA655PK1";
+  // Outer protocol transcript and opening-context domains (transcript.rs:15, protocol.rs:323).
+  static constexpr const char* kPublicDomain = "parcomm-qafold/public/v1";
+  static constexpr const char* kTerminalDomain = "parcomm/qafold/terminal/v2";
   static uint32_t base_mul(uint32_t a, uint32_t b) { return fp_mul(a, b); }
   static uint32_t base_inv(uint32_t a) { return fp_inv(a % P65521); }
   // The primitive 8th root of unity 17^((p-1)/8) used by the lane DFT, inverted.

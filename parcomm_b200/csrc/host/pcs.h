@@ -13,6 +13,7 @@
 
 #include "chacha.h"
 #include "field65521.h"
+#include "fieldkb.h"
 #include "merkle.h"
 #include "qacode.h"
 #include "sections.h"

@@ -161,7 +161,7 @@ template <class F>
 struct Transcript {
   Digest state;
   uint64_t counter = 0;
-  Transcript() { const char* d = "parcomm-qafold/public/v1"; state = blake2s(d, std::strlen(d)); }
+  Transcript() { const char* d = F::kPublicDomain; state = blake2s(d, std::strlen(d)); }
   void bytes(const char* label, const void* b, size_t n) {
     Blake2s h;
     h.update(state);
@@ -502,8 +502,9 @@ Proof<F> proof_from_bytes(const uint8_t* d, size_t n) {
   return p;
 }
 
-inline std::vector<uint8_t> opening_context(const Digest& state, size_t block) {
-  const char* d = "parcomm/qafold/terminal/v2";
+template <class F>
+std::vector<uint8_t> opening_context(const Digest& state, size_t block) {
+  const char* d = F::kTerminalDomain;
   std::vector<uint8_t> b(d, d + std::strlen(d));
   b.insert(b.end(), state.begin(), state.end());
   auto bl = le64(block);
@@ -571,7 +572,7 @@ bool verify_proof(const Parameters<F>& P, const Commitment& st, const std::vecto
   Transcript<F> t = statement_transcript(P, st, claims);
   Query<F> q = compile(P.layout, claims, t);
   Terminal<F> term = eo_verify(proof.eo, P.layout.logical, size_t(1) << P.config.packed_log, q, t);
-  std::vector<uint8_t> ctx = opening_context(t.state, 0);
+  std::vector<uint8_t> ctx = opening_context<F>(t.state, 0);
   bool ok;
   if (st.roots.size() > 1)
     ok = verify_batch(P.pcs, st.roots, term.point_msb, proof.opening_value, proof.opening_proof.data(), proof.opening_proof.size(), ctx);

@@ -67,11 +67,14 @@ def encode(shapes, matrices: Sequence[np.ndarray], dtype=np.int8) -> np.ndarray:
     return out
 
 
-def demo_matrices(shapes) -> List[np.ndarray]:
-    """The demo weights of main.rs:139-141: (entry * 73 + index * 19) as u8 as i8."""
+def demo_matrices(shapes, dtype=np.int8) -> List[np.ndarray]:
+    """The demo weights of main.rs:139-141: (entry * 73 + index * 19) truncated
+    to the payload width (as u8 as i8; for 16-bit payloads as u16 as i16)."""
     mats = []
+    unsigned = {np.dtype(np.int8): np.uint8, np.dtype(np.int16): np.uint16}[np.dtype(dtype)]
+    mask = np.iinfo(unsigned).max
     for i, s in enumerate(shapes):
         rows, cols = (s.rows, s.cols) if hasattr(s, "rows") else s
         e = np.arange(rows * cols, dtype=np.int64)
-        mats.append(((e * 73 + i * 19) & 0xFF).astype(np.uint8).view(np.int8).reshape(rows, cols))
+        mats.append(((e * 73 + i * 19) & mask).astype(unsigned).view(dtype).reshape(rows, cols))
     return mats

@@ -1,4 +1,6 @@
 """The CPU oracle is pinned to the reference's own golden vectors."""
+import numpy as np
+
 import oracle
 
 import parcomm_b200 as qf
@@ -29,3 +31,23 @@ def test_demo_proof_verifies_in_oracle():
     roots, claims, proof, _ = oracle.prove(shapes, 10, 4, bva)
     assert len(roots) == 4 * 32
     assert oracle.verify(shapes, 10, 4, roots, claims, proof)
+
+
+def test_koalabear_demo_proof_digest_matches_reference(vectors):
+    """G2: the KoalaBear^4 / signed-i16 demo bundle (qafold/koalabear main.rs)."""
+    digest, proof_len, json_len = oracle.demo("koalabear")
+    g = vectors["koalabear_demo"]
+    assert proof_len == g["proof_bytes"]
+    assert json_len == g["public_commitment_json_bytes"]
+    assert digest.hex() == g["proof_blake2s"]
+
+
+def test_koalabear_demo_proof_verifies_and_tampering_is_rejected():
+    shapes = qf.demo_shapes()
+    bva = layout.encode(shapes, layout.demo_matrices(shapes, np.int16), np.int16)
+    roots, claims, proof, _ = oracle.prove(shapes, 10, 4, bva, field="koalabear")
+    assert oracle.verify(shapes, 10, 4, roots, claims, proof, field="koalabear")
+    bad = bytearray(proof)
+    bad[len(bad) // 2] ^= 1
+    assert not oracle.verify(shapes, 10, 4, roots, claims, bytes(bad), field="koalabear")
+    assert not oracle.verify(shapes, 10, 4, roots, claims, proof, field="f65521")
