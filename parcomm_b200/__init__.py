@@ -228,13 +228,18 @@ class Proof:
 
 
 class Parameters:
-    """protocol::Parameters::new(shapes, config) for the F65521^8 field."""
+    """protocol::Parameters::new(shapes, config).
+
+    `field` picks the message field: FIELD_F65521 (F65521^8, signed 8-bit
+    weights; qafold/f65521) or FIELD_KOALABEAR (KoalaBear^4, signed 16-bit
+    payloads; qafold/koalabear)."""
 
     def __init__(self, shapes: Sequence[Tuple[int, int]] | Sequence[Shape], config: Config = Config(),
                  field: int = FIELD_F65521):
         self.shapes = [s if isinstance(s, Shape) else Shape(int(s[0]), int(s[1])) for s in shapes]
         self.config = config
         self.field = field
+        self.weight_dtype = np.int16 if field == FIELD_KOALABEAR else np.int8
         arr = (_Shape * len(self.shapes))(*[_Shape(s.rows, s.cols) for s in self.shapes])
         cfg = _Config(config.chunk_log, config.packed_log, config.query_rf_bits)
         h = ctypes.c_void_p()
@@ -256,9 +261,11 @@ class Parameters:
     # -- commit (protocol.rs:131-185); cached and recompute modes give identical bytes
     def commit(self, values, on_device: bool = False) -> Committed:
         if on_device:
+            if int(values.element_size()) != np.dtype(self.weight_dtype).itemsize:
+                raise QfError(-9, f"device weights must be {np.dtype(self.weight_dtype).name}")
             ptr, n = int(values.data_ptr()), int(values.numel())
         else:
-            arr = np.ascontiguousarray(values, dtype=np.int8)
+            arr = np.ascontiguousarray(values, dtype=self.weight_dtype)
             ptr, n = arr.ctypes.data, arr.size
         h = ctypes.c_void_p()
         roots = ctypes.create_string_buffer(32 * max(self.blocks, 1))
@@ -348,4 +355,4 @@ def demo_shapes() -> List[Shape]:
 def encode_bva(layout_params: Parameters, matrices: Sequence[np.ndarray]) -> np.ndarray:
     """Layout::encode (layout.rs:115-135): dense matrices -> BVA of `active` entries."""
     from .layout import encode
-    return encode(layout_params.shapes, matrices)
+    return encode(layout_params.shapes, matrices, layout_params.weight_dtype)

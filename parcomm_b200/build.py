@@ -12,7 +12,11 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 LIB_DIR = PKG / "_lib"
 LIB = LIB_DIR / "libparcomm_qafold.so"
-SOURCES = [PKG / "csrc" / "capi.cu", PKG / "csrc" / "gpu_backend.cu", PKG / "csrc" / "noalloc.cu"]
+# gpu_backend_kb.cu / capi_field_kb.cu recompile gpu_backend.cu / capi_field.cu
+# for KoalaBear^4 (QF_FIELD_KB); the others are F65521^8 or field-independent.
+SOURCES = [PKG / "csrc" / n for n in ("capi.cu", "gpu_common.cu", "gpu_backend.cu", "capi_field.cu", "noalloc.cu",
+                                      "gpu_backend_kb.cu", "capi_field_kb.cu")]
+OBJ_DIR = PKG / "_build"
 HEADERS = sorted((PKG / "csrc").rglob("*.h")) + sorted((PKG / "csrc").rglob("*.cuh"))
 
 NVCC_FLAGS = [
@@ -20,7 +24,6 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17",
     "-Xcompiler", "-fPIC,-fopenmp,-O2,-ffp-contract=off",
     "--expt-relaxed-constexpr",
-    "-shared",
 ]
 
 
@@ -39,10 +42,25 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compiles each source to an object (in parallel), then links the library."""
     if not force and not stale():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
     LIB_DIR.mkdir(exist_ok=True)
-    cmd = [nvcc(), *NVCC_FLAGS, *map(str, SOURCES), "-o", str(LIB), "-lgomp"]
+    OBJ_DIR.mkdir(exist_ok=True)
+
+    def compile_one(src: Path) -> Path:
+        obj = OBJ_DIR / (src.stem + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 1)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *map(str, objs), "-o", str(LIB), "-lgomp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -1,0 +1,296 @@
+// The field-specific half of the extern "C" boundary (see capi.cu): the
+// bodies of commit, claims, prove and verify for the field picked by
+// field_select.h.  This file is compiled once per field (capi_field_kb.cu
+// defines QF_FIELD_KB and includes it); each compilation exports its table as
+// QFB_NS::kFieldApi.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "capi_internal.h"
+#include "gpu_backend.cuh"
+
+namespace QFB_NS {
+namespace {
+
+const Parameters<F>& params_of(const qf_params* p) { return *static_cast<const Parameters<F>*>(p->P.get()); }
+
+// Any zero-padding entry that is nonzero sets the flag (Layout::validate_values,
+// layout.rs:136-155).  Segments are at most kZeroPiece bytes; a CTA checks one
+// with 16-byte loads over its aligned middle and byte loads at the ends.
+constexpr uint64_t kZeroPiece = 4096;
+__global__ void k_check_zero_segments(const uint8_t* __restrict__ bva, const uint64_t* __restrict__ seg, uint32_t n_seg,
+                                      unsigned int* __restrict__ flag) {
+  bool bad = false;
+  for (uint32_t s = blockIdx.x; s < n_seg; s += gridDim.x) {
+    const uint64_t a = seg[2 * s], b = seg[2 * s + 1];
+    const uint64_t a16 = (a + 15) & ~uint64_t(15), b16 = b & ~uint64_t(15);
+    if (a16 >= b16) {
+      for (uint64_t i = a + threadIdx.x; i < b; i += blockDim.x) bad |= bva[i] != 0;
+    } else {
+      for (uint64_t i = a + threadIdx.x; i < a16; i += blockDim.x) bad |= bva[i] != 0;
+      for (uint64_t i = b16 + threadIdx.x; i < b; i += blockDim.x) bad |= bva[i] != 0;
+      for (uint64_t i = a16 + 16 * uint64_t(threadIdx.x); i < b16; i += 16 * uint64_t(blockDim.x)) {
+        const uint4 u = *reinterpret_cast<const uint4*>(bva + i);
+        bad |= (u.x | u.y | u.z | u.w) != 0;
+      }
+    }
+  }
+  if (bad) atomicOr(flag, 1u);
+}
+
+
+// A side stream for the weight transfer, with one event per block.
+struct CopyPipeline {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t begin = nullptr, end = nullptr;
+  std::vector<cudaEvent_t> landed;
+  explicit CopyPipeline(size_t blocks) : landed(blocks, nullptr) {
+    QF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    QF_CK(cudaEventCreate(&begin));
+    QF_CK(cudaEventCreate(&end));
+    for (auto& e : landed) QF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  ~CopyPipeline() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& e : landed)
+      if (e) cudaEventDestroy(e);
+    if (begin) cudaEventDestroy(begin);
+    if (end) cudaEventDestroy(end);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  CopyPipeline(const CopyPipeline&) = delete;
+  CopyPipeline& operator=(const CopyPipeline&) = delete;
+};
+
+struct FieldCommitted : qf_committed_state {
+  cudaStream_t stream = nullptr;
+  DBuf<W> bva;
+  uint64_t active = 0;
+  std::unique_ptr<GpuBackend> be;
+  std::vector<Digest> roots;
+  double commit_ms = 0, upload_ms = 0;
+  ~FieldCommitted() override {
+    be.reset();
+    bva.reset();
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+static std::vector<Claim<F>> parse_claims(const Parameters<F>& P, const uint8_t* d, size_t n, bool with_value) {
+  std::vector<Claim<F>> claims;
+  ByteReader r(d, n);
+  for (const Shape& s : P.layout.shapes) {
+    Claim<F> c;
+    for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) c.row.push_back(r.field<F>());
+    for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) c.col.push_back(r.field<F>());
+    c.value = with_value ? r.field<F>() : F::zero();
+    claims.push_back(std::move(c));
+  }
+  if (!r.empty()) fail(QF_E_ARGUMENT, "claims length mismatch");
+  return claims;
+}
+static std::vector<uint8_t> write_claims(const std::vector<Claim<F>>& claims, bool with_value) {
+  ByteWriter w;
+  for (const auto& c : claims) {
+    for (const F& v : c.row) w.field(v);
+    for (const F& v : c.col) w.field(v);
+    if (with_value) w.field(c.value);
+  }
+  return std::move(w.out);
+}
+static std::vector<Digest> roots_from(const qf_params* p, const uint8_t* roots) {
+  std::vector<Digest> out(params_of(p).blocks());
+  for (size_t b = 0; b < out.size(); ++b) std::memcpy(out[b].data(), roots + 32 * b, 32);
+  return out;
+}
+
+// TBV claim values on the device (tbv::evaluate_claims, tbv.rs:143-185).
+static std::vector<Claim<F>> device_eval_claims(const Parameters<F>& P, GpuBackend& be, std::vector<Claim<F>> claims) {
+  validate_claims(P.layout, claims);
+  std::vector<Term<F>> terms;
+  for (const Bucket& b : P.layout.buckets) {
+    const auto& row = claims[b.matrix].row;
+    const auto& col = claims[b.matrix].col;
+    Term<F> t{b.offset, monomial_weight(b.row_offset, row.data(), row.size()) * monomial_weight(b.col_offset, col.data(), col.size()), {}};
+    for (int k = 0; k < ilog2(b.cols); ++k) t.factors.push_back({F::one(), col[k]});
+    for (int k = 0; k < ilog2(b.rows); ++k) t.factors.push_back({F::one(), row[k]});
+    terms.push_back(std::move(t));
+  }
+  for (auto& c : claims) c.value = F::zero();
+  // Group by lane width (terms with fewer than four factors use fewer lanes).
+  for (size_t lanes_log = 0; lanes_log <= 4; ++lanes_log) {
+    std::vector<const Term<F>*> group;
+    std::vector<size_t> which;
+    for (size_t i = 0; i < terms.size(); ++i)
+      if (std::min<size_t>(4, terms[i].factors.size()) == lanes_log) { group.push_back(&terms[i]); which.push_back(i); }
+    if (group.empty()) continue;
+    auto pr = be.project_terms(group, 16);
+    for (size_t g = 0; g < group.size(); ++g) {
+      std::vector<F> low = factor_weights(group[g]->factors.data(), lanes_log);
+      F v = F::zero();
+      for (size_t l = 0; l < pr[g].size(); ++l) v += pr[g][l] * low[l];
+      claims[P.layout.buckets[which[g]].matrix].value += v;
+    }
+  }
+  return claims;
+}
+
+void make_params(qf_params* out, const std::vector<Shape>& shapes, const Config& config) {
+  out->P = std::shared_ptr<Parameters<F>>(make_parameters<F>(shapes, config).release());
+  out->tables = std::make_shared<DeviceTables>();
+}
+
+void info(const qf_params* params, uint64_t* active, uint64_t* logical, uint64_t* blocks, uint64_t* buckets,
+          uint8_t parameter_digest[32]) {
+  const auto& P = params_of(params);
+  if (active) *active = P.layout.active;
+  if (logical) *logical = P.layout.logical;
+  if (blocks) *blocks = P.blocks();
+  if (buckets) *buckets = P.layout.buckets.size();
+  if (parameter_digest) std::memcpy(parameter_digest, P.pcs.parameter_digest().data(), 32);
+}
+
+void commit(const qf_params* params, const void* bva, uint64_t n_values, int bva_on_device, qf_committed* out,
+            uint8_t* roots_out) {
+    const auto& P = params_of(params);
+    check(n_values == P.layout.active, "active BVA length mismatch");
+    auto c = std::make_unique<FieldCommitted>();
+    c->active = n_values;
+    QF_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    auto t0 = std::chrono::steady_clock::now();
+    c->bva.alloc(std::max<uint64_t>(n_values, 8));
+    // The weights arrive block by block on a copy stream; block b is committed
+    // as soon as its bytes have landed, so the transfer of block b + 1
+    // overlaps the encoding and hashing of block b.
+    const size_t live = std::min<size_t>(P.blocks(), (n_values + P.block_len - 1) / P.block_len);
+    CopyPipeline copies(live);
+    const cudaMemcpyKind kind = bva_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    QF_CK(cudaEventRecord(copies.begin, copies.stream));
+    for (size_t b = 0; b < live; ++b) {
+      const uint64_t a = uint64_t(b) * P.block_len, e = std::min<uint64_t>(a + P.block_len, n_values);
+      QF_CK(cudaMemcpyAsync(c->bva.p + a, static_cast<const W*>(bva) + a, (e - a) * sizeof(W), kind, copies.stream));
+      QF_CK(cudaEventRecord(copies.landed[b], copies.stream));
+    }
+    QF_CK(cudaEventRecord(copies.end, copies.stream));
+    c->be = std::make_unique<GpuBackend>(P, c->bva.p, n_values, c->stream, static_cast<DeviceTables*>(params->tables.get()));
+    for (size_t b = 0; b < P.blocks(); ++b) {
+      if (b < live) QF_CK(cudaStreamWaitEvent(c->stream, copies.landed[b], 0));
+      c->roots.push_back(c->be->commit_block(b));
+    }
+    QF_CK(cudaStreamWaitEvent(c->stream, copies.end, 0));
+    QF_CK(cudaEventSynchronize(copies.end));
+    float up = 0;
+    QF_CK(cudaEventElapsedTime(&up, copies.begin, copies.end));
+    c->upload_ms = up;
+    // Padding must be zero (validate_values) — checked on the device.
+    std::vector<uint64_t> runs;
+    auto add_run = [&](uint64_t a, uint64_t e) {
+      if (a >= e) return;
+      if (!runs.empty() && runs.back() == a) runs.back() = e;  // merge contiguous runs
+      else { runs.push_back(a); runs.push_back(e); }
+    };
+    for (const Bucket& b : P.layout.buckets) {
+      if (b.physical_cols < b.cols)  // the padded tail of every real row
+        for (size_t r = 0; r < b.physical_rows; ++r) add_run(b.offset + r * b.cols + b.physical_cols, b.offset + (r + 1) * b.cols);
+      add_run(b.offset + b.physical_rows * b.cols, b.offset + b.rows * b.cols);  // padding rows
+    }
+    std::vector<uint64_t> seg;  // runs, as byte ranges cut into pieces of at most kZeroPiece bytes
+    for (size_t i = 0; i < runs.size(); i += 2)
+      for (uint64_t a = runs[i] * sizeof(W); a < runs[i + 1] * sizeof(W); a += kZeroPiece) {
+        seg.push_back(a);
+        seg.push_back(std::min<uint64_t>(a + kZeroPiece, runs[i + 1] * sizeof(W)));
+      }
+    if (!seg.empty()) {
+      DBuf<uint64_t> dseg(seg.size());
+      DBuf<unsigned int> flag(1);
+      QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, c->stream));
+      QF_CK(cudaMemsetAsync(flag.p, 0, 4, c->stream));
+      QF_LAUNCH(c->stream, "k_check_zero_segments", 0,
+                k_check_zero_segments<<<unsigned(std::min<size_t>(seg.size() / 2, 148 * 8)), 256, 0, c->stream>>>(
+                    reinterpret_cast<const uint8_t*>(c->bva.p), dseg.p, uint32_t(seg.size() / 2), flag.p));
+      unsigned int h = 0;
+      QF_CK(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, c->stream));
+      QF_CK(cudaStreamSynchronize(c->stream));
+      check(h == 0, "nonzero boundary padding");
+    }
+    QF_CK(cudaStreamSynchronize(c->stream));
+    c->commit_ms = ms_since(t0);
+    if (roots_out)
+      for (size_t b = 0; b < c->roots.size(); ++b) std::memcpy(roots_out + 32 * b, c->roots[b].data(), 32);
+    out->state = std::move(c);
+}
+
+std::string statement_json(const qf_params* params, const uint8_t* roots) {
+  return commitment_json(make_statement(params_of(params), roots_from(params, roots)));
+}
+
+std::vector<uint8_t> benchmark_points_bytes(const qf_params* params, const uint8_t* roots) {
+  auto pts = benchmark_points<F>(make_statement(params_of(params), roots_from(params, roots)));
+  ByteWriter w;
+  for (const auto& [r, c] : pts) {
+    for (const F& v : r) w.field(v);
+    for (const F& v : c) w.field(v);
+  }
+  return std::move(w.out);
+}
+
+std::vector<uint8_t> eval_claims(const qf_params* params, const qf_committed* committed, const uint8_t* points, size_t len) {
+  const auto* fc = static_cast<const FieldCommitted*>(committed->state.get());
+  auto cl = parse_claims(params_of(params), points, len, false);
+  return write_claims(device_eval_claims(params_of(params), *fc->be, std::move(cl)), true);
+}
+
+std::vector<uint8_t> prove(const qf_params* params, qf_committed* committed, const uint8_t* claims, size_t claims_len,
+                           qf_profile* profile) {
+    auto* fc = static_cast<FieldCommitted*>(committed->state.get());
+    const auto& P = params_of(params);
+    auto cl = parse_claims(P, claims, claims_len, true);
+    auto t0 = std::chrono::steady_clock::now();
+    Commitment st = make_statement(P, fc->roots);
+    Transcript<F> t = statement_transcript(P, st, cl);
+    Query<F> q = compile(P.layout, cl, t);
+    auto [eo, term] = eo_prove<F>(*fc->be, P.layout.logical, size_t(1) << P.config.packed_log, q, t);
+    double eo_ms = ms_since(t0);
+    std::vector<uint8_t> ctx = opening_context<F>(t.state, 0);
+    BatchOpening<F> op = fc->roots.size() > 1 ? open_batch(P.pcs, *fc->be, fc->roots, term.point_msb, ctx)
+                                                    : open_single(P.pcs, *fc->be, fc->roots[0], term.point_msb, ctx);
+    check(op.claimed_value * term.scale == term.value, "QAFold/EO terminal mismatch");
+    Proof<F> pr;
+    pr.eo = std::move(eo);
+    pr.opening_value = op.claimed_value;
+    pr.opening_proof = std::move(op.wire);
+    std::vector<uint8_t> bytes = proof_to_bytes(pr);
+    if (profile) {
+      profile->commit_ms = fc->commit_ms;
+      profile->upload_ms = fc->upload_ms;
+      profile->eo_ms = eo_ms;
+      profile->projection_ms = op.times.projection_ms;
+      profile->folding_ms = op.times.folding_ms;
+      profile->sumcheck_ms = op.times.sumcheck_ms;
+      profile->binding_ms = op.times.binding_ms;
+      profile->native_opening_ms = op.times.native_opening_ms;
+      profile->decide_ms = op.times.decide_ms;
+      profile->open_ms = ms_since(t0);
+      profile->kernel_launches = qfg::KernelClock::launches.load();
+    }
+    return bytes;
+}
+
+void verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,
+            size_t proof_len) {
+    const auto& P = params_of(params);
+    auto cl = parse_claims(P, claims, claims_len, true);
+    Proof<F> pr = proof_from_bytes<F>(proof, proof_len);
+    verify_proof(P, make_statement(P, roots_from(params, roots)), cl, pr);
+}
+
+}  // namespace
+
+const qfc::FieldApi kFieldApi = {sizeof(W), make_params, info, commit, statement_json, benchmark_points_bytes,
+                                 eval_claims, prove, verify};
+
+}  // namespace QFB_NS

@@ -1,6 +1,7 @@
-// Shared pieces of the extern "C" boundary: the parameter handle, the
-// per-thread last-error message and the exception guard that turns a QfError
-// into its QF_E_* return code.
+// Shared pieces of the extern "C" boundary: the parameter and commitment
+// handles (field-independent, with the field's own state behind them), the
+// per-field function table, the per-thread last-error message and the
+// exception guard that turns a QfError into its QF_E_* return code.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -8,20 +9,46 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
+#include "../../include/parcomm_qafold.h"
 #include "host/protocol.h"
 
-namespace qfg {
-class DeviceTables;
-}
+// State of one commitment, owned by the field's implementation.
+struct qf_committed_state {
+  virtual ~qf_committed_state() {}
+};
 
 struct qf_params {
   int field = 0;
-  std::unique_ptr<qf::Parameters<qf::Fp8>> P;
-  std::shared_ptr<qfg::DeviceTables> tables;  // device code tables shared by its commitments
+  std::shared_ptr<void> P;       // qf::Parameters<F> of the field
+  std::shared_ptr<void> tables;  // the field's device code tables, shared by its commitments
+};
+
+struct qf_committed {
+  const qf_params* params = nullptr;
+  std::unique_ptr<qf_committed_state> state;
+  bool consumed = false;
 };
 
 namespace qfc {
+
+// One field's implementation of the C ABI calls (capi_field.cu, compiled once
+// per field).  Arguments are already checked for null.
+struct FieldApi {
+  size_t weight_bytes;  // bytes of one BVA entry
+  void (*make_params)(qf_params* out, const std::vector<qf::Shape>& shapes, const qf::Config& config);
+  void (*info)(const qf_params* p, uint64_t* active, uint64_t* logical, uint64_t* blocks, uint64_t* buckets,
+               uint8_t digest[32]);
+  void (*commit)(const qf_params* p, const void* bva, uint64_t n_values, int on_device, qf_committed* c,
+                 uint8_t* roots_out);
+  std::string (*statement_json)(const qf_params* p, const uint8_t* roots);
+  std::vector<uint8_t> (*benchmark_points)(const qf_params* p, const uint8_t* roots);
+  std::vector<uint8_t> (*eval_claims)(const qf_params* p, const qf_committed* c, const uint8_t* points, size_t len);
+  std::vector<uint8_t> (*prove)(const qf_params* p, qf_committed* c, const uint8_t* claims, size_t len, qf_profile* profile);
+  void (*verify)(const qf_params* p, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,
+                 size_t proof_len);
+};
 
 inline thread_local std::string g_last_error;
 
@@ -50,3 +77,10 @@ inline void require_device() {
 }
 
 }  // namespace qfc
+
+namespace qfg {
+extern const qfc::FieldApi kFieldApi;  // F65521^8, int8 weights
+}
+namespace qfgkb {
+extern const qfc::FieldApi kFieldApi;  // KoalaBear^4, int16 payloads
+}

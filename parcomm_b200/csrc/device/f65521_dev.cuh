@@ -14,6 +14,8 @@
 namespace qfd {
 
 constexpr uint32_t P = 65521u;
+constexpr int kC = 8;   // coefficients per element
+using Wt = int8_t;      // one BVA entry
 
 struct __align__(16) Fe {
   uint16_t c[8];
@@ -91,7 +93,42 @@ QFD_HD Fr mul_base(const Fr& a, uint32_t s) {
   for (int i = 0; i < 8; ++i) r.c[i] = red32(a.c[i] * s);
   return r;
 }
+// Σ of kC products of canonical values (< 2^35) to canonical.
+QFD_HD uint32_t red_sum(uint64_t v) { return red64(v); }
+QFD_HD Fr unpack_fe(uint4 u) {
+  Fr v;
+  v.c[0] = u.x & 0xffffu; v.c[1] = u.x >> 16; v.c[2] = u.y & 0xffffu; v.c[3] = u.y >> 16;
+  v.c[4] = u.z & 0xffffu; v.c[5] = u.z >> 16; v.c[6] = u.w & 0xffffu; v.c[7] = u.w >> 16;
+  return v;
+}
+QFD_HD uint4 pack_fe(const Fr& r) {
+  return make_uint4(r.c[0] | (r.c[1] << 16), r.c[2] | (r.c[3] << 16), r.c[4] | (r.c[5] << 16), r.c[6] | (r.c[7] << 16));
+}
+
+// Planar transform tiles use lazy reduction: a value entering level l of a
+// pass is below tile_bound(l) = 2^l p, a difference is formed as a + 2^l p - b,
+// so twelve levels stay below 2^28 and tile_final reduces once per pass.
+QFD_HD uint32_t tile_bound(int lvl) { return P << lvl; }
+QFD_HD void bfly_wht(uint32_t& lo, uint32_t& hi, uint32_t B) {
+  const uint32_t a = lo, b = hi;
+  lo = a + b;
+  hi = a + B - b;
+}
+QFD_HD void bfly_mobius(uint32_t lo, uint32_t& hi, uint32_t B) { hi = hi + B - lo; }
+// Values below 2^28 (at most twelve lazy levels) to canonical form.
+QFD_HD uint32_t tile_final(uint32_t v) {
+  const uint32_t f = (v & 0xffffu) + 15u * (v >> 16);  // < 2^16 + 15 * 2^12 < 2p
+  return f >= P ? f - P : f;
+}
+
 // small signed integer -> canonical F_65521 (field.rs:24-26)
 QFD_HD uint32_t small(int v) { return v < 0 ? uint32_t(v + int(P)) : uint32_t(v); }
+// Eight signed 8-bit weights (8 bytes) to the packed element.
+QFD_HD Fr weights_to_fr(uint2 raw) {
+  Fr r;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) r.c[k] = small(int(int8_t(((k < 4 ? raw.x : raw.y) >> (8 * (k & 3))) & 0xffu)));
+  return r;
+}
 
 }  // namespace qfd

@@ -1,4 +1,4 @@
-// CUDA backend for the F65521^8 packed PCS and EO (see gpu_backend.cuh).
+// CUDA backend for the packed PCS and EO of one field (see gpu_backend.cuh).
 #include "gpu_backend.cuh"
 #include "kernels/commit.cuh"
 #include "kernels/open.cuh"
@@ -9,169 +9,9 @@
 #include <mutex>
 #include <set>
 
-namespace qfg {
+namespace QFB_NS {
 
 static constexpr int kThreads = 256;
-
-namespace {
-std::mutex g_pool_mu;
-std::multimap<size_t, void*> g_pool;  // rounded bytes -> free device block
-}  // namespace
-
-void* DevicePool::get(size_t bytes) {
-  const size_t r = rounded(bytes);
-  {
-    std::lock_guard<std::mutex> g(g_pool_mu);
-    auto it = g_pool.find(r);
-    if (it != g_pool.end()) {
-      void* p = it->second;
-      g_pool.erase(it);
-      return p;
-    }
-  }
-  void* p = nullptr;
-  if (cudaMalloc(&p, r) != cudaSuccess) {
-    cudaGetLastError();
-    trim();
-    QF_CK(cudaMalloc(&p, r));
-  }
-  return p;
-}
-void DevicePool::put(void* p, size_t bytes) {
-  std::lock_guard<std::mutex> g(g_pool_mu);
-  g_pool.emplace(rounded(bytes), p);
-}
-void DevicePool::trim() {
-  std::lock_guard<std::mutex> g(g_pool_mu);
-  cudaDeviceSynchronize();
-  for (auto& [b, p] : g_pool) cudaFree(p);
-  g_pool.clear();
-}
-
-bool KernelClock::enabled = false;
-std::mutex KernelClock::mu;
-std::vector<KernelClock::Rec> KernelClock::recs;
-std::atomic<uint64_t> KernelClock::launches{0};
-
-KernelClock::Scope::Scope(cudaStream_t s, const char* n, uint64_t b_) : stream(s), name(n), bytes(b_) {
-  if (enabled) {
-    QF_CK(cudaEventCreate(&a));
-    QF_CK(cudaEventCreate(&b));
-    QF_CK(cudaEventRecord(a, stream));
-  }
-}
-void KernelClock::Scope::done() {
-  ++launches;
-  if (enabled) {
-    QF_CK(cudaEventRecord(b, stream));
-    std::lock_guard<std::mutex> g(mu);
-    recs.push_back({name, a, b, bytes});
-  }
-}
-void KernelClock::reset(bool on) {
-  std::lock_guard<std::mutex> g(mu);
-  for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
-  recs.clear();
-  ::qf::Sections::reset(on);
-  enabled = on;
-}
-std::string KernelClock::stats_json() {
-  QF_CK(cudaDeviceSynchronize());
-  std::lock_guard<std::mutex> g(mu);
-  struct Agg { uint64_t n = 0, bytes = 0; double ms = 0; };
-  std::map<std::string, Agg> agg;
-  for (auto& r : recs) {
-    float ms = 0;
-    QF_CK(cudaEventElapsedTime(&ms, r.a, r.b));
-    auto& e = agg[r.name];
-    e.n += 1;
-    e.ms += ms;
-    e.bytes += r.bytes;
-  }
-  std::string s = "{";
-  bool first = true;
-  for (auto& [k, v] : agg) {
-    if (!first) s += ",";
-    first = false;
-    char buf[256];
-    std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu}", k.c_str(),
-                  (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
-    s += buf;
-  }
-  // Idle time between consecutive recorded launches (in launch order), with
-  // the largest gaps named by the kernels on either side.
-  if (recs.size() > 1) {
-    struct Gap { double ms; const char* before; const char* after; };
-    std::vector<Gap> gaps;
-    double total = 0;
-    for (size_t i = 1; i < recs.size(); ++i) {
-      float ms = 0;
-      QF_CK(cudaEventElapsedTime(&ms, recs[i - 1].b, recs[i].a));
-      if (ms > 0) { gaps.push_back({ms, recs[i - 1].name, recs[i].name}); total += ms; }
-    }
-    std::sort(gaps.begin(), gaps.end(), [](const Gap& x, const Gap& y) { return x.ms > y.ms; });
-    if (!first) s += ",";
-    first = false;
-    char buf[256];
-    std::snprintf(buf, sizeof buf, "\"_gaps\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0,\"top\":[", (unsigned long long)gaps.size(), total);
-    s += buf;
-    for (size_t i = 0; i < gaps.size() && i < 40; ++i) {
-      std::snprintf(buf, sizeof buf, "%s[\"%s\",\"%s\",%.4f]", i ? "," : "", gaps[i].before, gaps[i].after, gaps[i].ms);
-      s += buf;
-    }
-    s += "]}";
-  }
-  std::lock_guard<std::mutex> gs(::qf::Sections::mu);
-  for (auto& [k, v] : ::qf::Sections::totals) {
-    if (!first) s += ",";
-    first = false;
-    char buf[256];
-    std::snprintf(buf, sizeof buf, "\"host:%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0}", k.c_str(),
-                  (unsigned long long)v.first, v.second);
-    s += buf;
-  }
-  return s + "}";
-}
-
-qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain) {
-  std::vector<uint8_t> pre;
-  const char* dom = ext_domain ? kLeafExtDomain : kLeafBaseDomain;
-  append_frame(pre, "domain", dom, std::strlen(dom));
-  auto w = le64(n_cols);
-  append_frame(pre, "width", w.data(), 8);
-  if (pre.size() != (ext_domain ? 80u : 75u)) fail(QF_E_ENCODING, "leaf prefix length");
-  qfd::LeafPrefix lp;
-  uint32_t h[8];
-  for (int i = 0; i < 8; ++i) h[i] = kBlake2sIv[i];
-  h[0] ^= 0x01010000u ^ 32u;
-  blake2s_compress(h, pre.data(), 64, false);
-  for (int i = 0; i < 8; ++i) lp.mid[i] = h[i];
-  uint8_t tail[16] = {0};
-  std::memcpy(tail, pre.data() + 64, pre.size() - 64);
-  for (int i = 0; i < 4; ++i)
-    lp.tail[i] = uint32_t(tail[4 * i]) | (uint32_t(tail[4 * i + 1]) << 8) | (uint32_t(tail[4 * i + 2]) << 16) |
-                 (uint32_t(tail[4 * i + 3]) << 24);
-  return lp;
-}
-qfd::InnerPrefix inner_prefix() {
-  std::vector<uint8_t> pre;
-  append_frame(pre, "domain", kInnerDomain, std::strlen(kInnerDomain));
-  if (pre.size() != 50) fail(QF_E_ENCODING, "inner prefix length");
-  uint8_t b[52] = {0};
-  std::memcpy(b, pre.data(), 50);
-  qfd::InnerPrefix ip;
-  for (int i = 0; i < 13; ++i)
-    ip.w[i] = uint32_t(b[4 * i]) | (uint32_t(b[4 * i + 1]) << 8) | (uint32_t(b[4 * i + 2]) << 16) | (uint32_t(b[4 * i + 3]) << 24);
-  return ip;
-}
-
-static Digest digest_from_words(const uint4* d) {
-  Digest out;
-  uint32_t w[8] = {d[0].x, d[0].y, d[0].z, d[0].w, d[1].x, d[1].y, d[1].z, d[1].w};
-  for (int i = 0; i < 8; ++i)
-    for (int j = 0; j < 4; ++j) out[4 * i + j] = uint8_t(w[i] >> (8 * j));
-  return out;
-}
 
 template <class K>
 static void set_smem(K kernel, size_t bytes) {
@@ -276,7 +116,7 @@ static void configure_tile_kernels() {
 }
 
 // ---------------------------------------------------------------- backend
-GpuBackend::GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s, DeviceTables* tables)
+GpuBackend::GpuBackend(const Parameters<F>& p, const W* d_bva, size_t active, cudaStream_t s, DeviceTables* tables)
     : P_(p), bva_(d_bva), active_(active), s_(s), tables_(tables ? tables : &own_tables_) {
   configure_tile_kernels();
   partials_.alloc(148 * 8 * 4);
@@ -356,7 +196,7 @@ void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR,
   }
   // Leaves and inner levels.
   const uint64_t n_ext = 2 * R;
-  qfd::LeafPrefix lp = leaf_prefix(out.n_cols, ext_domain);
+  ::qfd::LeafPrefix lp = leaf_prefix(out.n_cols, ext_domain);
   const unsigned lgrid = unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads);
   if (ext_domain)
     QF_LAUNCH(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32,
@@ -364,7 +204,7 @@ void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR,
   else
     QF_LAUNCH(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32,
               qfd::k_hash_leaves<11><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
-  qfd::InnerPrefix ip = inner_prefix();
+  ::qfd::InnerPrefix ip = inner_prefix();
   out.level_off.clear();
   uint64_t off = 0, n = n_ext;
   while (n > 1) {
@@ -434,7 +274,7 @@ static void strided_passes_plain(cudaStream_t s, Fe* base, int logR, int logm, i
   }
 }
 
-void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
+void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
                        Fe* alpha, uint8_t* d_root, cudaStream_t s) {
   configure_tile_kernels();
   const int logm = ilog2(P.pcs.packed_len());
@@ -462,7 +302,7 @@ void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t act
   qfd::k_hash_leaves<11><<<unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads), qfd::kLeafThreads, 0, s>>>(
       cw, n_ext, int(cols), leaf_prefix(cols, false), tree);
   QF_CK(cudaGetLastError());
-  const qfd::InnerPrefix ip = inner_prefix();
+  const ::qfd::InnerPrefix ip = inner_prefix();
   uint64_t off = 0, n = n_ext;
   while (n > 1) {
     qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s>>>(tree + 2 * off, n / 2, ip, tree + 2 * (off + n));
@@ -516,27 +356,30 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   const uint64_t m = P_.pcs.packed_len();
   if (outer.size() != size_t(ilog2(m))) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "outer point");
   device_point_table(s_, outer, eq_slice, weights_);
-  DBuf<unsigned long long> raw(64 * nblocks);
-  QF_CK(cudaMemsetAsync(raw.p, 0, 64 * nblocks * 8, s_));
+  constexpr int L = F::kLanes, kRaw = qfd::kEqRaw;
+  static_assert(kRaw == L * qfd::kC, "raw lane sums per block");
+  DBuf<unsigned long long> raw(kRaw * nblocks);
+  QF_CK(cudaMemsetAsync(raw.p, 0, kRaw * nblocks * 8, s_));
   // Zero blocks (the suffix past the active entries) have vanishing lanes.
   const size_t live = std::min<size_t>(nblocks, (active_ + P_.block_len - 1) / P_.block_len);
   const unsigned grid = unsigned(std::min<uint64_t>((m + qfd::kEqChunk - 1) / qfd::kEqChunk, 148 * 4));
   for (size_t b0 = 0; b0 < live; b0 += qfd::kEqBlocks) {
     const int nb = int(std::min<size_t>(qfd::kEqBlocks, live - b0));
-    QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * 8 * uint64_t(nb),
+    QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W) * uint64_t(nb),
               qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva_, active_, P_.block_len, b0, nb, m, weights_.p,
-                                                                         raw.p + 64 * b0));
+                                                                         raw.p + kRaw * b0));
   }
-  std::vector<unsigned long long> h(64 * nblocks);
+  std::vector<unsigned long long> h(kRaw * nblocks);
   QF_CK(cudaMemcpyAsync(h.data(), raw.p, h.size() * 8, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
-  std::vector<std::vector<F>> out(nblocks, std::vector<F>(8));
+  // Entries are two's complement sums of exact signed totals below 2^63.
+  std::vector<std::vector<F>> out(nblocks, std::vector<F>(L));
   for (size_t b = 0; b < nblocks; ++b)
-    for (int j = 0; j < 8; ++j)
-      for (int k = 0; k < 8; ++k) {
-        int64_t v = int64_t(h[64 * b + 8 * j + k]);
-        int64_t r = v % int64_t(P65521);
-        out[b][j].c[k] = uint16_t(r < 0 ? r + P65521 : r);
+    for (int j = 0; j < L; ++j)
+      for (int k = 0; k < qfd::kC; ++k) {
+        const int64_t v = int64_t(h[kRaw * b + qfd::kC * j + k]);
+        const int64_t r = v % int64_t(F::kPrime);
+        out[b][j].c[k] = typename F::Coeff(r < 0 ? r + int64_t(F::kPrime) : r);
       }
   sum_len_ = 0;
   return out;
@@ -547,19 +390,21 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   // Packed values of the single block: the block fold with weight one.
   const uint64_t m = P_.pcs.packed_len();
   values_.alloc(m);
-  std::vector<F> T(8);
-  for (int j = 0; j < 8; ++j) T[j] = basis<F>(j);
-  DBuf<Fe> dT(8);
-  QF_CK(cudaMemcpyAsync(dT.p, T.data(), 8 * 16, cudaMemcpyHostToDevice, s_));
-  QF_LAUNCH(s_, "k_block_fold", m * 24, qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, 8 * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p));
+  constexpr int L = F::kLanes;
+  std::vector<F> T(L);
+  for (int j = 0; j < L; ++j) T[j] = basis<F>(j);
+  DBuf<Fe> dT(L);
+  QF_CK(cudaMemcpyAsync(dT.p, T.data(), L * 16, cudaMemcpyHostToDevice, s_));
+  QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p));
   sum_len_ = m;
   msg_valid_ = false;
   return lanes[0];
 }
 
 void GpuBackend::apply_images(const std::vector<F>& images) {
-  DBuf<Fe> di(8);
-  QF_CK(cudaMemcpyAsync(di.p, images.data(), 8 * 16, cudaMemcpyHostToDevice, s_));
+  check(images.size() == size_t(F::kLanes), "weight images");
+  DBuf<Fe> di(F::kLanes);
+  QF_CK(cudaMemcpyAsync(di.p, images.data(), F::kLanes * 16, cudaMemcpyHostToDevice, s_));
   QF_LAUNCH(s_, "k_apply_images", uint64_t(weights_.n) * 32, qfd::k_apply_images<<<grid_for(weights_.n, kThreads), kThreads, 0, s_>>>(weights_.p, weights_.n, di.p));
   QF_CK(cudaStreamSynchronize(s_));
   msg_valid_ = false;
@@ -570,14 +415,15 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   const int logm = ilog2(m);
   const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
   const int blocks = int(fw.size());
-  std::vector<F> T(size_t(blocks) * 8);
+  constexpr int L = F::kLanes;
+  std::vector<F> T(size_t(blocks) * L);
   for (int b = 0; b < blocks; ++b)
-    for (int j = 0; j < 8; ++j) T[b * 8 + j] = fw[b] * basis<F>(j);
+    for (int j = 0; j < L; ++j) T[b * L + j] = fw[b] * basis<F>(j);
   DBuf<Fe> dT(T.size());
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), T.size() * 16, cudaMemcpyHostToDevice, s_));
   values_.alloc(m);
   set_smem(qfd::k_block_fold, T.size() * 16);
-  QF_LAUNCH(s_, "k_block_fold", m * (8 * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
+  QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
                                                                           values_.p));
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
@@ -671,15 +517,15 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
 }
 
 // ---------------------------------------------------------------- TBV / EO
-std::vector<int8_t> GpuBackend::windows(const std::vector<uint64_t>& starts, size_t stride) {
-  std::vector<int8_t> out(starts.size() * stride);
+std::vector<W> GpuBackend::windows(const std::vector<uint64_t>& starts, size_t stride) {
+  std::vector<W> out(starts.size() * stride);
   if (starts.empty()) return out;
   DBuf<uint64_t> ds(starts.size());
-  DBuf<int8_t> dout(out.size());
+  DBuf<W> dout(out.size());
   QF_CK(cudaMemcpyAsync(ds.p, starts.data(), starts.size() * 8, cudaMemcpyHostToDevice, s_));
   QF_LAUNCH(s_, "k_gather_windows", uint64_t(out.size()) * 2, qfd::k_gather_windows<<<grid_for(out.size(), kThreads, 1 << 20), kThreads, 0, s_>>>(bva_, active_, ds.p, uint32_t(starts.size()),
                                                                                      int(stride), dout.p));
-  QF_CK(cudaMemcpyAsync(out.data(), dout.p, out.size(), cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaMemcpyAsync(out.data(), dout.p, out.size() * sizeof(W), cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
   return out;
 }
@@ -765,7 +611,7 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
       const uint64_t rows = std::min<uint64_t>((active_ - term.offset + lanes - 1) / lanes, term.len() / lanes);
       qfd::TermTiles T = term_tiles(tb, term.factors.data() + low_bits, nh, term.offset, rows, uint32_t(tiles), term.scale);
       tiles += term_tile_count(T);
-      proj_bytes += rows * lanes + term_tile_count(T) * 16;
+      proj_bytes += rows * lanes * sizeof(W) + term_tile_count(T) * 16;
       tt.push_back(T);
     }
     check(tiles < (uint64_t(1) << 31), "projection tile count");
@@ -820,13 +666,13 @@ void GpuBackend::cross_terms(const Query<F>& q, size_t stride, std::vector<F>& p
   }
   std::vector<uint64_t> starts;
   for (const auto* t : small) starts.push_back(t->offset / stride * stride);
-  std::vector<int8_t> win = windows(starts, stride);
+  std::vector<W> win = windows(starts, stride);
   for (size_t s = 0; s < small.size(); ++s) {
     const Term<F>& term = *small[s];
     const size_t start = starts[s];
     std::vector<F> qv(stride, F::zero());
     for (size_t i = 0; i < term.len(); ++i) qv[term.offset - start + i] = term.weight(i);
-    const int8_t* v = win.data() + s * stride;
+    const W* v = win.data() + s * stride;
     for (size_t d = 1; d < stride; ++d)
       for (size_t lane = 0; lane + d < stride; ++lane) {
         pos[d - 1] += qv[lane + d].mul_prime(F::small(v[lane]));
@@ -844,7 +690,7 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
   std::vector<F> pinv = consecutive_powers(inv, stride);
   DBuf<Fe> dp(stride);
   QF_CK(cudaMemcpyAsync(dp.p, pinv.data(), stride * 16, cudaMemcpyHostToDevice, s_));
-  QF_LAUNCH(s_, "k_eo_witness", std::min<uint64_t>(active_, rows * stride) + rows * 16, qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p));
+  QF_LAUNCH(s_, "k_eo_witness", std::min<uint64_t>(active_, rows * stride) * sizeof(W) + rows * 16, qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p));
   // Query fold (tbv.rs:393-428): zero, then two disjoint passes of large-term
   // tiles, then the merged small-term contributions.
   QF_CK(cudaMemsetAsync(qv_.p, 0, rows * 16, s_));
@@ -1268,4 +1114,4 @@ bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, siz
   return true;
 }
 
-}  // namespace qfg
+}  // namespace QFB_NS

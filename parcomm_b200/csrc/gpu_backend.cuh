@@ -1,113 +1,22 @@
-// CUDA implementation of the packed-PCS / EO backend for F65521^8 with int8
-// weights.  All bulk data (BVA, codewords, Merkle trees, EO and sumcheck
-// vectors) stays in HBM; only transcript-sized values cross to the host.
+// CUDA implementation of the packed-PCS / EO backend for one field: F65521^8
+// with int8 weights, or KoalaBear^4 with int16 payloads when QF_FIELD_KB is
+// defined (the translation unit that includes this header picks one).  All bulk
+// data (BVA, codewords, Merkle trees, EO and sumcheck vectors) stays in HBM;
+// only transcript-sized values cross to the host.
 #pragma once
-#include <cuda_runtime.h>
+#include "device/field_dev.cuh"
+#include "field_select.h"
+#include "gpu_common.cuh"
 
-#include <atomic>
-#include <chrono>
-#include <map>
-#include <memory>
-#include <mutex>
-#include <string>
-#include <tuple>
-#include <vector>
-
-#include "host/protocol.h"
-#include "host/sections.h"
-#include "device/f65521_dev.cuh"
-#include "device/hash_prefix.h"
-
-namespace qfg {
+namespace QFB_NS {
 using namespace qf;
-using F = Fp8;
+using namespace qfg;
+namespace qfd = ::QFD_NS;
 using qfd::Fe;
-
-#define QF_CK(x)                                                                              \
-  do {                                                                                        \
-    cudaError_t e_ = (x);                                                                     \
-    if (e_ != cudaSuccess)                                                                    \
-      ::qf::fail(QF_E_CUDA, std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #x); \
-  } while (0)
-
-// Per-kernel device time: when enabled, every launch is bracketed by CUDA
-// events recorded on the launching stream; totals are read after a sync.
-struct KernelClock {
-  struct Rec { const char* name; cudaEvent_t a, b; uint64_t bytes; };
-  struct Scope {
-    cudaStream_t stream;
-    const char* name;
-    uint64_t bytes;  // algorithmic bytes moved by this launch
-    cudaEvent_t a = nullptr, b = nullptr;
-    Scope(cudaStream_t s, const char* n, uint64_t bytes);
-    void done();
-  };
-  static bool enabled;
-  static std::mutex mu;
-  static std::vector<Rec> recs;
-  static std::atomic<uint64_t> launches;
-  static void reset(bool on);
-  static std::string stats_json();
-};
-
-// Host wall time of named sections (recorded while KernelClock is enabled).
-using HostScope = ::qf::Section;
-
-#define QF_LAUNCH(stream, name, bytes, ...)     \
-  do {                                          \
-    ::qfg::KernelClock::Scope qf_scope_(stream, name, bytes); \
-    __VA_ARGS__;                                \
-    QF_CK(cudaGetLastError());                  \
-    qf_scope_.done();                           \
-  } while (0)
-
-// Process-wide cache of device allocations: released buffers are kept, keyed
-// by their rounded size, and handed out again, so repeated commits/openings
-// of the same shapes pay no cudaMalloc/cudaFree.  A failed cudaMalloc first
-// returns the cache to the driver and retries.
-struct DevicePool {
-  static void* get(size_t bytes);
-  static void put(void* p, size_t bytes);
-  static void trim();
-  static size_t rounded(size_t bytes) {
-    const size_t g = bytes >= (size_t(1) << 20) ? (size_t(1) << 20) : 256;
-    return (bytes + g - 1) / g * g;
-  }
-};
-
-template <class T>
-struct DBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DBuf() = default;
-  explicit DBuf(size_t count) { alloc(count); }
-  DBuf(const DBuf&) = delete;
-  DBuf& operator=(const DBuf&) = delete;
-  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
-  DBuf& operator=(DBuf&& o) noexcept { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; return *this; }
-  ~DBuf() { reset(); }
-  void alloc(size_t count) {
-    reset();
-    if (count) p = static_cast<T*>(DevicePool::get(count * sizeof(T)));
-    n = count;
-  }
-  void reset() {
-    if (p) DevicePool::put(p, n * sizeof(T));
-    p = nullptr;
-    n = 0;
-  }
-};
 
 inline const Fe* as_fe(const F* p) { return reinterpret_cast<const Fe*>(p); }
 inline Fe to_fe(const F& v) { Fe e; std::memcpy(&e, &v, 16); return e; }
 inline F from_fe(const Fe& e) { F v; std::memcpy(&v, &e, 16); return v; }
-
-inline int grid_for(uint64_t n, int threads, int max_blocks = 148 * 8) {
-  uint64_t b = (n + threads - 1) / threads;
-  if (b < 1) b = 1;
-  if (b > uint64_t(max_blocks)) b = max_blocks;
-  return int(b);
-}
 
 // Device copies of a parameter set's code alphas (alphas[0] and alphas[1] of
 // every level), uploaded once per device and shared by every commitment and
@@ -123,9 +32,6 @@ class DeviceTables {
   std::map<std::tuple<int, size_t, int>, DBuf<Fe>> bufs_;  // (device, level, which)
 };
 
-// Constant hash prefixes computed on the host.
-qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain);
-qfd::InnerPrefix inner_prefix();
 
 // A committed codeword in HBM: column-major entries and all Merkle levels.
 struct DeviceCodeword : CodewordView<F> {
@@ -151,7 +57,7 @@ struct DeviceCodeword : CodewordView<F> {
 // 4 x 2R words (2 x 2R digests), `alpha` R entries (overwritten with the
 // code's alpha table).  Launches on `s`, writes the 32-byte root to the device
 // bytes `d_root` and returns without synchronising; allocates no device memory.
-void commit_block_into(const Parameters<F>& P, const int8_t* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
+void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
                        Fe* alpha, uint8_t* d_root, cudaStream_t s);
 
 class GpuBackend : public Backend<F>,
@@ -161,7 +67,7 @@ class GpuBackend : public Backend<F>,
                    public DecideAccel<F> {
  public:
   // `tables` (optional, not owned) shares uploaded code tables across backends.
-  GpuBackend(const Parameters<F>& p, const int8_t* d_bva, size_t active, cudaStream_t s, DeviceTables* tables = nullptr);
+  GpuBackend(const Parameters<F>& p, const W* d_bva, size_t active, cudaStream_t s, DeviceTables* tables = nullptr);
   ~GpuBackend() override;
 
   // commit
@@ -218,7 +124,7 @@ class GpuBackend : public Backend<F>,
   // Lane projections of arbitrary tensor terms (TBV claims and EO cross terms).
   std::vector<std::vector<F>> project_terms(const std::vector<const Term<F>*>& terms, size_t stride);
   // Raw window values of small terms.
-  std::vector<int8_t> windows(const std::vector<uint64_t>& starts, size_t stride);
+  std::vector<W> windows(const std::vector<uint64_t>& starts, size_t stride);
 
 
  private:
@@ -238,7 +144,7 @@ class GpuBackend : public Backend<F>,
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
 
   const Parameters<F>& P_;
-  const int8_t* bva_;
+  const W* bva_;
   size_t active_;
   cudaStream_t s_;
   std::vector<std::unique_ptr<DeviceCodeword>> blocks_;
@@ -261,4 +167,4 @@ class GpuBackend : public Backend<F>,
   DBuf<Fe> partials_, result_;
 };
 
-}  // namespace qfg
+}  // namespace QFB_NS

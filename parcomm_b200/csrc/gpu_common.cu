@@ -1,0 +1,163 @@
+// Field-independent CUDA infrastructure (see gpu_common.cuh).
+#include "gpu_common.cuh"
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+
+namespace qfg {
+
+namespace {
+std::mutex g_pool_mu;
+std::multimap<size_t, void*> g_pool;  // rounded bytes -> free device block
+}  // namespace
+
+void* DevicePool::get(size_t bytes) {
+  const size_t r = rounded(bytes);
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    auto it = g_pool.find(r);
+    if (it != g_pool.end()) {
+      void* p = it->second;
+      g_pool.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, r) != cudaSuccess) {
+    cudaGetLastError();
+    trim();
+    QF_CK(cudaMalloc(&p, r));
+  }
+  return p;
+}
+void DevicePool::put(void* p, size_t bytes) {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  g_pool.emplace(rounded(bytes), p);
+}
+void DevicePool::trim() {
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  cudaDeviceSynchronize();
+  for (auto& [b, p] : g_pool) cudaFree(p);
+  g_pool.clear();
+}
+
+bool KernelClock::enabled = false;
+std::mutex KernelClock::mu;
+std::vector<KernelClock::Rec> KernelClock::recs;
+std::atomic<uint64_t> KernelClock::launches{0};
+
+KernelClock::Scope::Scope(cudaStream_t s, const char* n, uint64_t b_) : stream(s), name(n), bytes(b_) {
+  if (enabled) {
+    QF_CK(cudaEventCreate(&a));
+    QF_CK(cudaEventCreate(&b));
+    QF_CK(cudaEventRecord(a, stream));
+  }
+}
+void KernelClock::Scope::done() {
+  ++launches;
+  if (enabled) {
+    QF_CK(cudaEventRecord(b, stream));
+    std::lock_guard<std::mutex> g(mu);
+    recs.push_back({name, a, b, bytes});
+  }
+}
+void KernelClock::reset(bool on) {
+  std::lock_guard<std::mutex> g(mu);
+  for (auto& r : recs) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  recs.clear();
+  ::qf::Sections::reset(on);
+  enabled = on;
+}
+std::string KernelClock::stats_json() {
+  QF_CK(cudaDeviceSynchronize());
+  std::lock_guard<std::mutex> g(mu);
+  struct Agg { uint64_t n = 0, bytes = 0; double ms = 0; };
+  std::map<std::string, Agg> agg;
+  for (auto& r : recs) {
+    float ms = 0;
+    QF_CK(cudaEventElapsedTime(&ms, r.a, r.b));
+    auto& e = agg[r.name];
+    e.n += 1;
+    e.ms += ms;
+    e.bytes += r.bytes;
+  }
+  std::string s = "{";
+  bool first = true;
+  for (auto& [k, v] : agg) {
+    if (!first) s += ",";
+    first = false;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu}", k.c_str(),
+                  (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
+    s += buf;
+  }
+  // Idle time between consecutive recorded launches (in launch order), with
+  // the largest gaps named by the kernels on either side.
+  if (recs.size() > 1) {
+    struct Gap { double ms; const char* before; const char* after; };
+    std::vector<Gap> gaps;
+    double total = 0;
+    for (size_t i = 1; i < recs.size(); ++i) {
+      float ms = 0;
+      QF_CK(cudaEventElapsedTime(&ms, recs[i - 1].b, recs[i].a));
+      if (ms > 0) { gaps.push_back({ms, recs[i - 1].name, recs[i].name}); total += ms; }
+    }
+    std::sort(gaps.begin(), gaps.end(), [](const Gap& x, const Gap& y) { return x.ms > y.ms; });
+    if (!first) s += ",";
+    first = false;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "\"_gaps\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0,\"top\":[", (unsigned long long)gaps.size(), total);
+    s += buf;
+    for (size_t i = 0; i < gaps.size() && i < 40; ++i) {
+      std::snprintf(buf, sizeof buf, "%s[\"%s\",\"%s\",%.4f]", i ? "," : "", gaps[i].before, gaps[i].after, gaps[i].ms);
+      s += buf;
+    }
+    s += "]}";
+  }
+  std::lock_guard<std::mutex> gs(::qf::Sections::mu);
+  for (auto& [k, v] : ::qf::Sections::totals) {
+    if (!first) s += ",";
+    first = false;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "\"host:%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0}", k.c_str(),
+                  (unsigned long long)v.first, v.second);
+    s += buf;
+  }
+  return s + "}";
+}
+
+qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain) {
+  std::vector<uint8_t> pre;
+  const char* dom = ext_domain ? kLeafExtDomain : kLeafBaseDomain;
+  append_frame(pre, "domain", dom, std::strlen(dom));
+  auto w = le64(n_cols);
+  append_frame(pre, "width", w.data(), 8);
+  if (pre.size() != (ext_domain ? 80u : 75u)) fail(QF_E_ENCODING, "leaf prefix length");
+  qfd::LeafPrefix lp;
+  uint32_t h[8];
+  for (int i = 0; i < 8; ++i) h[i] = kBlake2sIv[i];
+  h[0] ^= 0x01010000u ^ 32u;
+  blake2s_compress(h, pre.data(), 64, false);
+  for (int i = 0; i < 8; ++i) lp.mid[i] = h[i];
+  uint8_t tail[16] = {0};
+  std::memcpy(tail, pre.data() + 64, pre.size() - 64);
+  for (int i = 0; i < 4; ++i)
+    lp.tail[i] = uint32_t(tail[4 * i]) | (uint32_t(tail[4 * i + 1]) << 8) | (uint32_t(tail[4 * i + 2]) << 16) |
+                 (uint32_t(tail[4 * i + 3]) << 24);
+  return lp;
+}
+qfd::InnerPrefix inner_prefix() {
+  std::vector<uint8_t> pre;
+  append_frame(pre, "domain", kInnerDomain, std::strlen(kInnerDomain));
+  if (pre.size() != 50) fail(QF_E_ENCODING, "inner prefix length");
+  uint8_t b[52] = {0};
+  std::memcpy(b, pre.data(), 50);
+  qfd::InnerPrefix ip;
+  for (int i = 0; i < 13; ++i)
+    ip.w[i] = uint32_t(b[4 * i]) | (uint32_t(b[4 * i + 1]) << 8) | (uint32_t(b[4 * i + 2]) << 16) | (uint32_t(b[4 * i + 3]) << 24);
+  return ip;
+}
+
+
+}  // namespace qfg

@@ -1,0 +1,119 @@
+// Field-independent CUDA infrastructure of the library: error checks, the
+// per-kernel timer, the device memory pool, device buffers, launch sizing and
+// the constant BLAKE2s prefixes of the Merkle hashing.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "device/hash_prefix.h"
+#include "host/protocol.h"
+#include "host/sections.h"
+
+namespace qfg {
+using namespace qf;
+
+#define QF_CK(x)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (x);                                                                     \
+    if (e_ != cudaSuccess)                                                                    \
+      ::qf::fail(QF_E_CUDA, std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #x); \
+  } while (0)
+
+// Per-kernel device time: when enabled, every launch is bracketed by CUDA
+// events recorded on the launching stream; totals are read after a sync.
+struct KernelClock {
+  struct Rec { const char* name; cudaEvent_t a, b; uint64_t bytes; };
+  struct Scope {
+    cudaStream_t stream;
+    const char* name;
+    uint64_t bytes;  // algorithmic bytes moved by this launch
+    cudaEvent_t a = nullptr, b = nullptr;
+    Scope(cudaStream_t s, const char* n, uint64_t bytes);
+    void done();
+  };
+  static bool enabled;
+  static std::mutex mu;
+  static std::vector<Rec> recs;
+  static std::atomic<uint64_t> launches;
+  static void reset(bool on);
+  static std::string stats_json();
+};
+
+// Host wall time of named sections (recorded while KernelClock is enabled).
+using HostScope = ::qf::Section;
+
+#define QF_LAUNCH(stream, name, bytes, ...)     \
+  do {                                          \
+    ::qfg::KernelClock::Scope qf_scope_(stream, name, bytes); \
+    __VA_ARGS__;                                \
+    QF_CK(cudaGetLastError());                  \
+    qf_scope_.done();                           \
+  } while (0)
+
+// Process-wide cache of device allocations: released buffers are kept, keyed
+// by their rounded size, and handed out again, so repeated commits/openings
+// of the same shapes pay no cudaMalloc/cudaFree.  A failed cudaMalloc first
+// returns the cache to the driver and retries.
+struct DevicePool {
+  static void* get(size_t bytes);
+  static void put(void* p, size_t bytes);
+  static void trim();
+  static size_t rounded(size_t bytes) {
+    const size_t g = bytes >= (size_t(1) << 20) ? (size_t(1) << 20) : 256;
+    return (bytes + g - 1) / g * g;
+  }
+};
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  explicit DBuf(size_t count) { alloc(count); }
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DBuf& operator=(DBuf&& o) noexcept { reset(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; return *this; }
+  ~DBuf() { reset(); }
+  void alloc(size_t count) {
+    reset();
+    if (count) p = static_cast<T*>(DevicePool::get(count * sizeof(T)));
+    n = count;
+  }
+  void reset() {
+    if (p) DevicePool::put(p, n * sizeof(T));
+    p = nullptr;
+    n = 0;
+  }
+};
+
+inline int grid_for(uint64_t n, int threads, int max_blocks = 148 * 8) {
+  uint64_t b = (n + threads - 1) / threads;
+  if (b < 1) b = 1;
+  if (b > uint64_t(max_blocks)) b = max_blocks;
+  return int(b);
+}
+
+// Constant hash prefixes computed on the host.
+qfd::LeafPrefix leaf_prefix(size_t n_cols, bool ext_domain);
+qfd::InnerPrefix inner_prefix();
+
+// A digest held as two uint4 words (the Merkle tree layout in device memory).
+inline Digest digest_from_words(const uint4* d) {
+  Digest out;
+  uint32_t w[8] = {d[0].x, d[0].y, d[0].z, d[0].w, d[1].x, d[1].y, d[1].z, d[1].w};
+  for (int i = 0; i < 8; ++i)
+    for (int j = 0; j < 4; ++j) out[4 * i + j] = uint8_t(w[i] >> (8 * j));
+  return out;
+}
+
+}  // namespace qfg

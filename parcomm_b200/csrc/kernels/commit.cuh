@@ -16,10 +16,10 @@
 #include <cstdint>
 
 #include "../device/blake2s_dev.cuh"
-#include "../device/f65521_dev.cuh"
+#include "../device/field_dev.cuh"
 #include "../device/hash_prefix.h"
 
-namespace qfd {
+namespace QFD_NS {
 
 __device__ __forceinline__ size_t msg_addr(size_t i, int logR) {
   return ((i >> logR) << (logR + 1)) | (i & ((size_t(1) << logR) - 1));
@@ -41,7 +41,8 @@ constexpr int kTileThreads = 512;       // CTA size of the tile kernels
 constexpr int kAlphaTileThreads = 512;  // the WHT tile that multiplies by alpha
 constexpr int kMaxTileLog = 12;                 // 4096 elements per tile
 constexpr int kPlane = 1 << kMaxTileLog;        // plane stride (words)
-constexpr size_t kTileSmem = size_t(8) * kPlane * 4;  // 128 KiB
+constexpr size_t kTileSmem = size_t(kC) * kPlane * 4;  // kC planes: 128 KiB (F65521), 64 KiB (KoalaBear)
+constexpr int kCLog = kC == 8 ? 3 : 2;
 __device__ __forceinline__ int pidx(int e) {
   // byte z of kSwz is swz(z); swz is linear over GF(2), so for index parts
   // with disjoint bits pidx(x | y) = pidx(x) ^ pidx(y).
@@ -52,19 +53,15 @@ __device__ __forceinline__ int pidx(int e) {
 __device__ __forceinline__ void planar_put(uint32_t* planes, int e, const Fr& v) {
   const int q = pidx(e);
 #pragma unroll
-  for (int c = 0; c < 8; ++c) planes[c * kPlane + q] = v.c[c];
+  for (int c = 0; c < kC; ++c) planes[c * kPlane + q] = v.c[c];
 }
-// Values below 2^28 (at most twelve lazy levels) to canonical form, packed.
-__device__ __forceinline__ uint32_t red28(uint32_t v) {
-  const uint32_t f = (v & 0xffffu) + 15u * (v >> 16);  // < 2^16 + 15 * 2^12 < 2p
-  return min(f, f - P);
-}
+// The element at plane position e, reduced to canonical form and packed.
 __device__ __forceinline__ uint4 planar_get_packed(const uint32_t* planes, int e) {
   const int q = pidx(e);
-  uint32_t v[8];
+  Fr v;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) v[c] = red28(planes[c * kPlane + q]);
-  return make_uint4(v[0] | (v[1] << 16), v[2] | (v[3] << 16), v[4] | (v[5] << 16), v[6] | (v[7] << 16));
+  for (int c = 0; c < kC; ++c) v.c[c] = tile_final(planes[c * kPlane + q]);
+  return pack_fe(v);
 }
 
 // One radix-2^R register stage: levels [lvl, lvl + R) of the pass, acting on
@@ -77,8 +74,8 @@ template <int OP, int R>
 __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b, int lvl) {
   const int lg = log_n - R;
   int split = 0;
-  while (split < 3 && (1 << (lg + split)) < int(blockDim.x)) ++split;
-  const int ppi = 8 >> split;  // planes per item
+  while (split < kCLog && (1 << (lg + split)) < int(blockDim.x)) ++split;
+  const int ppi = kC >> split;  // planes per item
   const int bmask = (1 << b) - 1;
   int off[1 << R];
 #pragma unroll
@@ -90,7 +87,7 @@ __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b,
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) q[j] = pb ^ off[j];
 #pragma unroll
-    for (int cc = 0; cc < 8; ++cc) {
+    for (int cc = 0; cc < kC; ++cc) {
       if (cc >= ppi) break;
       uint32_t* pl = planes + (c0 + cc) * kPlane;
       uint32_t v[1 << R];
@@ -98,17 +95,12 @@ __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b,
       for (int j = 0; j < (1 << R); ++j) v[j] = pl[q[j]];
 #pragma unroll
       for (int sft = 0; sft < R; ++sft) {
-        const uint32_t B = P << (lvl + sft);  // bound entering this level
+        const uint32_t B = tile_bound(lvl + sft);  // bound entering this level
 #pragma unroll
         for (int j = 0; j < (1 << R); ++j) {
           if (j & (1 << sft)) continue;
-          const uint32_t lo = v[j], hi = v[j | (1 << sft)];
-          if (OP == kWht) {
-            v[j] = lo + hi;
-            v[j | (1 << sft)] = lo + B - hi;
-          } else {
-            v[j | (1 << sft)] = hi + B - lo;
-          }
+          if (OP == kWht) bfly_wht(v[j], v[j | (1 << sft)], B);
+          else bfly_mobius(v[j], v[j | (1 << sft)], B);
         }
       }
 #pragma unroll
@@ -142,22 +134,17 @@ __device__ __forceinline__ void planar_levels(uint32_t* planes, int log_n, int b
 
 // R levels across the elements held in registers, starting at level lvl.
 template <int OP, int R>
-__device__ __forceinline__ void reg_levels(uint32_t (&v)[1 << R][8], int lvl) {
+__device__ __forceinline__ void reg_levels(uint32_t (&v)[1 << R][kC], int lvl) {
 #pragma unroll
   for (int sft = 0; sft < R; ++sft) {
-    const uint32_t B = P << (lvl + sft);
+    const uint32_t B = tile_bound(lvl + sft);
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       if (j & (1 << sft)) continue;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        const uint32_t lo = v[j][c], hi = v[j | (1 << sft)][c];
-        if (OP == kWht) {
-          v[j][c] = lo + hi;
-          v[j | (1 << sft)][c] = lo + B - hi;
-        } else {
-          v[j | (1 << sft)][c] = hi + B - lo;
-        }
+      for (int c = 0; c < kC; ++c) {
+        if (OP == kWht) bfly_wht(v[j][c], v[j | (1 << sft)][c], B);
+        else bfly_mobius(v[j][c], v[j | (1 << sft)][c], B);
       }
     }
   }
@@ -166,7 +153,7 @@ __device__ __forceinline__ void reg_levels(uint32_t (&v)[1 << R][8], int lvl) {
 // Levels 0..2 on tile bits 9..11 from values already loaded, into the
 // planes.  Thread g (512 per CTA) owns tile elements g + (j << 9), j < 8.
 template <int OP>
-__device__ __forceinline__ void head_levels(uint32_t* planes, uint32_t (&v)[8][8]) {
+__device__ __forceinline__ void head_levels(uint32_t* planes, uint32_t (&v)[8][kC]) {
   const int g = threadIdx.x;
   reg_levels<OP, 3>(v, 0);
   const int pb = pidx(g);
@@ -174,7 +161,7 @@ __device__ __forceinline__ void head_levels(uint32_t* planes, uint32_t (&v)[8][8
   for (int j = 0; j < 8; ++j) {
     const int q = pb ^ pidx(j << 9);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) planes[c * kPlane + q] = v[j][c];
+    for (int c = 0; c < kC; ++c) planes[c * kPlane + q] = v[j][c];
   }
   __syncthreads();
 }
@@ -187,20 +174,20 @@ __device__ __forceinline__ void pass_tail(const uint32_t* planes, int zb, int lv
   for (int g = threadIdx.x; g < kGroups; g += blockDim.x) {
     const int base = (g & ((1 << zb) - 1)) | ((g >> zb) << (zb + R));
     const int pb = pidx(base);
-    uint32_t v[1 << R][8];
+    uint32_t v[1 << R][kC];
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
       const int q = pb ^ pidx(j << zb);
 #pragma unroll
-      for (int c = 0; c < 8; ++c) v[j][c] = planes[c * kPlane + q];
+      for (int c = 0; c < kC; ++c) v[j][c] = planes[c * kPlane + q];
     }
     reg_levels<OP, R>(v, lvl);
 #pragma unroll
     for (int j = 0; j < (1 << R); ++j) {
-      uint32_t w[8];
+      Fr w;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) w[c] = red28(v[j][c]);
-      st(base + (j << zb), make_uint4(w[0] | (w[1] << 16), w[2] | (w[3] << 16), w[4] | (w[5] << 16), w[6] | (w[7] << 16)));
+      for (int c = 0; c < kC; ++c) w.c[c] = tile_final(v[j][c]);
+      st(base + (j << zb), pack_fe(w));
     }
   }
 }
@@ -230,12 +217,12 @@ __device__ __forceinline__ void tile_loop(uint32_t* planes, int log_n, int b0, u
       for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
     for (; tile < n_tiles; tile += gridDim.x) {
       {
-        uint32_t v[8][8];
+        uint32_t v[8][kC];
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
           const Fr e = conv(tile, g + (j << 9), raw[j]);
 #pragma unroll
-          for (int c = 0; c < 8; ++c) v[j][c] = e.c[c];
+          for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
         }
         head_levels<OP>(planes, v);
       }
@@ -265,34 +252,26 @@ __device__ __forceinline__ void tile_loop(uint32_t* planes, int log_n, int b0, u
   }
 }
 
-__device__ __forceinline__ Fr unpack(uint4 u) {
-  Fr v;
-  v.c[0] = u.x & 0xffffu; v.c[1] = u.x >> 16; v.c[2] = u.y & 0xffffu; v.c[3] = u.y >> 16;
-  v.c[4] = u.z & 0xffffu; v.c[5] = u.z >> 16; v.c[6] = u.w & 0xffffu; v.c[7] = u.w >> 16;
-  return v;
-}
 
 // Pack eight signed weights per element, then Mobius levels [0, levels) in
 // tiles of 2^levels elements; write into the message half.  `src_base` is
 // the block's first BVA index.
-__global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const int8_t* __restrict__ bva, uint64_t active,
+__global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const Wt* __restrict__ bva, uint64_t active,
                                                                      uint64_t src_base, Fe* __restrict__ cw, int logR, int levels,
                                                                      uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
+  // kC entries (8 bytes) per element; entries at or past `active` are zero.
   auto fetch = [=](uint32_t tile, int t) {
-    const uint64_t g = src_base + 8ull * ((uint64_t(tile) << levels) + t);
-    if (g + 8 <= active) return *reinterpret_cast<const uint2*>(bva + g);
+    const uint64_t g = src_base + uint64_t(kC) * ((uint64_t(tile) << levels) + t);
+    if (g + kC <= active) return *reinterpret_cast<const uint2*>(bva + g);
+    constexpr int kPer = 4 / int(sizeof(Wt));      // entries per 32-bit word
+    constexpr uint32_t kMask = (1u << (8 * sizeof(Wt))) - 1u;
     uint32_t w[2] = {0, 0};
-    for (int k = 0; k < 8; ++k)
-      if (g + k < active) w[k >> 2] |= uint32_t(uint8_t(bva[g + k])) << (8 * (k & 3));
+    for (int k = 0; k < kC; ++k)
+      if (g + k < active) w[k / kPer] |= (uint32_t(bva[g + k]) & kMask) << (8 * int(sizeof(Wt)) * (k % kPer));
     return make_uint2(w[0], w[1]);
   };
-  auto conv = [](uint32_t, int, uint2 raw) {
-    Fr r;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) r.c[k] = small(int(int8_t(((k < 4 ? raw.x : raw.y) >> (8 * (k & 3))) & 0xffu)));
-    return r;
-  };
+  auto conv = [](uint32_t, int, uint2 raw) { return weights_to_fr(raw); };
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + msg_addr((size_t(tile) << levels) + t, logR)) = u;
   };
@@ -305,7 +284,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* 
                                                                      int levels, uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
   auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + (size_t(tile) << levels) + t); };
-  auto conv = [](uint32_t, int, uint4 raw) { return unpack(raw); };
+  auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + msg_addr((size_t(tile) << levels) + t, logR)) = u;
   };
@@ -324,7 +303,7 @@ __global__ void __launch_bounds__(ALPHA ? kAlphaTileThreads : kTileThreads, 1)
   auto addr = [=](uint32_t tile, int t) { return msg_addr((size_t(tile) << levels) + t, logR); };
   auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + addr(tile, t)); };
   auto conv = [=](uint32_t tile, int t, uint4 raw) {
-    const Fr v = unpack(raw);
+    const Fr v = unpack_fe(raw);
     return ALPHA ? mul(v, load(alpha + (addr(tile, t) & rmask))) : v;
   };
   auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(dst + addr(tile, t)) = u; };
@@ -347,7 +326,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __res
     return msg_addr((((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(t >> cb) << lo), logR);
   };
   auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(base + addr(tile, t)); };
-  auto conv = [](uint32_t, int, uint4 raw) { return unpack(raw); };
+  auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
   auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(base + addr(tile, t)) = u; };
   tile_loop<OP, uint4>(planes_s, cb + k, cb, n_tiles, fetch, conv, st);
 }
@@ -361,7 +340,7 @@ constexpr int kRowStride = 129;  // padded: conflict-free per-thread rows
 // base-row prefix, 16 for the 80-byte extension-row prefix.
 template <int TAIL>
 __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restrict__ cw, uint64_t n_rows, int n_cols,
-                                                              LeafPrefix pre, uint4* __restrict__ leaves) {
+                                                              ::qfd::LeafPrefix pre, uint4* __restrict__ leaves) {
   static_assert(TAIL == 11 || TAIL == 16, "leaf prefix");
   __shared__ uint32_t rows_s[kLeafThreads * kRowStride];
   const uint64_t r = uint64_t(blockIdx.x) * kLeafThreads + threadIdx.x;
@@ -400,14 +379,14 @@ __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restri
       m[w] = word;
     }
     const bool last = j == nblocks;
-    compress(h, m, last ? total : 64u + 64u * uint32_t(j), last, pre.one);
+    ::qfd::compress(h, m, last ? total : 64u + 64u * uint32_t(j), last, pre.one);
   }
   leaves[2 * r] = make_uint4(h[0], h[1], h[2], h[3]);
   leaves[2 * r + 1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
 // Inner node = BLAKE2s(50-byte prefix || left || right), 114 bytes.
-__global__ void k_hash_inner(const uint4* __restrict__ children, uint64_t n_parents, InnerPrefix pre, uint4* __restrict__ parents) {
+__global__ void k_hash_inner(const uint4* __restrict__ children, uint64_t n_parents, ::qfd::InnerPrefix pre, uint4* __restrict__ parents) {
   const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= n_parents) return;
   uint32_t d[16];
@@ -427,12 +406,12 @@ __global__ void k_hash_inner(const uint4* __restrict__ children, uint64_t n_pare
   for (int k = 29; k < 32; ++k) buf[k] = 0;
   uint32_t h[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) h[k] = kIv[k];
+  for (int k = 0; k < 8; ++k) h[k] = ::qfd::kIv[k];
   h[0] ^= 0x01010020u;
-  compress(h, buf, 64u, false, pre.one);
-  compress(h, buf + 16, 114u, true, pre.one);
+  ::qfd::compress(h, buf, 64u, false, pre.one);
+  ::qfd::compress(h, buf + 16, 114u, true, pre.one);
   parents[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
   parents[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
-}  // namespace qfd
+}  // namespace QFD_NS

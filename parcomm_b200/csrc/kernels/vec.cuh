@@ -5,9 +5,9 @@
 #pragma once
 #include <cstdint>
 
-#include "../device/f65521_dev.cuh"
+#include "../device/field_dev.cuh"
 
-namespace qfd {
+namespace QFD_NS {
 
 // a[i] += s * b[i]
 __global__ void k_axpy(Fe* __restrict__ a, const Fe* __restrict__ b, uint64_t n, Fe s) {
@@ -91,4 +91,4 @@ __global__ void k_to_message_halves(const Fe* __restrict__ src, uint64_t m, int 
     cw[((i >> logR) << (logR + 1)) | (i & ((uint64_t(1) << logR) - 1))] = src[i];
 }
 
-}  // namespace qfd
+}  // namespace QFD_NS

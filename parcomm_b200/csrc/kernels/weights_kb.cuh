@@ -1,0 +1,252 @@
+// BVA-reading opening kernels for KoalaBear^4 with signed 16-bit payloads:
+// TBV lane projections, the packed EO witness, the batch opening's
+// equality-table lane projection and the block fold.
+//
+// A payload (|v| <= 2^15) times a canonical coefficient (< 2^31) is below
+// 2^46 in magnitude, so every per-thread and per-warp sum below stays inside
+// a signed 64-bit accumulator (the reference keeps u128 raw lanes for the
+// same sums, packed_koalabear.rs); each sum is reduced mod p once, and the
+// CTA-level totals are kept as canonical residues.
+#pragma once
+#include <cstdint>
+
+#include "open.cuh"
+
+namespace QFD_NS {
+
+// Four consecutive payloads from entry g (zero at or past `active`); one
+// 8-byte load when the four lie inside and g is 4-aligned.
+__device__ __forceinline__ uint2 load4(const Wt* __restrict__ bva, uint64_t active, uint64_t g) {
+  if (g + 4 <= active && (g & 3) == 0) return *reinterpret_cast<const uint2*>(bva + g);
+  uint32_t w[2] = {0, 0};
+  for (int j = 0; j < 4; ++j)
+    if (g + j < active) w[j >> 1] |= (uint32_t(bva[g + j]) & 0xffffu) << (16 * (j & 1));
+  return make_uint2(w[0], w[1]);
+}
+// Payload j (0..3) of a load4 word pair.
+__device__ __forceinline__ int lane_of(uint2 u, int j) { return int(int16_t(((j < 2 ? u.x : u.y) >> (16 * (j & 1))) & 0xffffu)); }
+
+// Lane projections (tbv.rs:288-352): out[tile * lanes + l] = high(tile) *
+// sum_r lo[r] * bva[offset + row * lanes + l].  A thread takes min(4, lanes)
+// lanes of a row; a tile has at most 1024 rows, so a lane's sum is below
+// 2^56 before the single reduction.
+__global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __restrict__ bva, uint64_t active,
+                                                                const TermTiles* __restrict__ terms, int n_terms,
+                                                                uint32_t n_tiles, const Fe* __restrict__ tables,
+                                                                int lanes, Fe* __restrict__ out) {
+  __shared__ int t_sel;
+  __shared__ long long part_s[kTermThreads / 32][64][kC];
+  const uint32_t tile0 = blockIdx.x * kTilesPerCta;
+  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, tile0);
+  __syncthreads();
+  int ti = t_sel;
+  const int lpt = lanes < 4 ? lanes : 4;
+  const int tpr = lanes / lpt;
+  const int rpp = kTermThreads / tpr;
+  const int sub = threadIdx.x % tpr;
+  const int warp = threadIdx.x >> 5, lane_id = threadIdx.x & 31;
+  for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
+    while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
+    const TermTiles T = terms[ti];
+    const uint64_t i = tile - T.first_tile;
+    const uint64_t row0 = i << T.lb;
+    const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
+    const int nrows = int(left < span ? left : span);
+    long long acc[4][kC];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < kC; ++k) acc[j][k] = 0;
+    const Fe* lo = tables + T.lo_off;
+    for (int r0 = threadIdx.x / tpr; r0 < nrows; r0 += 2 * rpp) {
+      uint2 u[2];
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int r = r0 + q * rpp;
+        const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
+        u[q] = make_uint2(0, 0);
+        if (r < nrows) {
+          if (lpt == 4) {
+            u[q] = load4(bva, active, g);
+          } else {
+            for (int j = 0; j < lpt; ++j)
+              if (g + j < active) (j < 2 ? u[q].x : u[q].y) |= (uint32_t(bva[g + j]) & 0xffffu) << (16 * (j & 1));
+          }
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const int r = r0 + q * rpp;
+        if (r >= nrows) break;
+        const Fr w = load(lo + r);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const long long v = lane_of(u[q], j);
+#pragma unroll
+          for (int k = 0; k < kC; ++k) acc[j][k] += (long long)w.c[k] * v;
+        }
+      }
+    }
+    for (int o = tpr; o < 32; o <<= 1)
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < kC; ++k) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+    if (lane_id < tpr)
+      for (int j = 0; j < lpt; ++j)
+#pragma unroll
+        for (int k = 0; k < kC; ++k) part_s[warp][lane_id * lpt + j][k] = acc[j][k];
+    __syncthreads();
+    if (threadIdx.x < lanes) {
+      long long s[kC];
+#pragma unroll
+      for (int k = 0; k < kC; ++k) s[k] = 0;
+      for (int w = 0; w < kTermThreads / 32; ++w)
+#pragma unroll
+        for (int k = 0; k < kC; ++k) s[k] += part_s[w][threadIdx.x][k];
+      Fr sum;
+#pragma unroll
+      for (int k = 0; k < kC; ++k) sum.c[k] = mod_i64(s[k]);
+      store(out + size_t(tile) * lanes + threadIdx.x, mul(tile_high(T, tables, i), sum));
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- EO
+// Packed EO witness (eo.rs:119-132): witness[row] = sum_lane v(row * stride +
+// lane) * inv_powers[lane], stride <= 64, so a sum is below 2^52.
+__global__ void k_eo_witness(const Wt* __restrict__ bva, uint64_t active, uint64_t rows, int stride,
+                             const Fe* __restrict__ inv_powers, Fe* __restrict__ witness) {
+  __shared__ Fe pw[64];
+  if (threadIdx.x < stride) pw[threadIdx.x] = inv_powers[threadIdx.x];
+  __syncthreads();
+  for (uint64_t row = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < rows; row += uint64_t(gridDim.x) * blockDim.x) {
+    long long acc[kC];
+#pragma unroll
+    for (int k = 0; k < kC; ++k) acc[k] = 0;
+    const uint64_t g0 = row * stride;
+    if (g0 < active) {
+      for (int l0 = 0; l0 < stride; l0 += 4) {
+        const int n = stride - l0 < 4 ? stride - l0 : 4;
+        const uint2 u = n == 4 ? load4(bva, active, g0 + l0) : make_uint2(0, 0);
+        for (int j = 0; j < n; ++j) {
+          const uint64_t g = g0 + l0 + j;
+          const long long v = n == 4 ? lane_of(u, j) : (g < active ? int(bva[g]) : 0);
+          const Fr p = load(pw + l0 + j);
+#pragma unroll
+          for (int k = 0; k < kC; ++k) acc[k] += (long long)p.c[k] * v;
+        }
+      }
+    }
+    Fr w;
+#pragma unroll
+    for (int k = 0; k < kC; ++k) w.c[k] = mod_i64(acc[k]);
+    store(witness + row, w);
+  }
+}
+
+// ---------------------------------------------------------------- batch opening
+// Raw lane sums of up to kEqBlocks consecutive blocks against the equality
+// weights (project_lanes_from_fn, packed_batch.rs:25-41):
+//   raw[b][j * 4 + k] += sum_i v(b, 4i + j) * weights[i].c[k]
+// A CTA stages kEqChunk weights in shared memory and runs every block over
+// them.  A thread takes 8 elements per block into 16 i64 sums (< 2^49); a
+// warp reduce-scatter leaves each lane pair with one entry (< 2^54), the CTA
+// sum (< 2^57) is reduced to a residue and added to the block's residue
+// total, and `raw` receives one atomic add per entry at the end (a sum of
+// residues over the grid, far below 2^63).
+__global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const Wt* __restrict__ bva, uint64_t active,
+                                                                    uint64_t block_len, uint64_t first_block, int nb,
+                                                                    uint64_t m, const Fe* __restrict__ weights,
+                                                                    unsigned long long* __restrict__ raw) {
+  __shared__ uint4 w_s[kEqChunk];
+  __shared__ long long stage_s[kEqThreads / 32][kEqRaw];
+  __shared__ unsigned long long tot_s[kEqBlocks][kEqRaw];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int t = threadIdx.x; t < kEqBlocks * kEqRaw; t += kEqThreads) tot_s[t / kEqRaw][t % kEqRaw] = 0;
+  for (uint64_t c0 = uint64_t(blockIdx.x) * kEqChunk; c0 < m; c0 += uint64_t(gridDim.x) * kEqChunk) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < kEqChunk; e += kEqThreads)
+      w_s[e] = c0 + e < m ? *reinterpret_cast<const uint4*>(weights + c0 + e) : make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    for (int b = 0; b < nb; ++b) {
+      const uint64_t bbase = (first_block + b) * block_len;
+      long long acc[kEqRaw];
+#pragma unroll
+      for (int q = 0; q < kEqRaw; ++q) acc[q] = 0;
+#pragma unroll 2
+      for (int u = 0; u < kEqChunk / kEqThreads; ++u) {
+        const int e = threadIdx.x + u * kEqThreads;
+        const uint2 v4 = c0 + e < m ? load4(bva, active, bbase + 4 * (c0 + e)) : make_uint2(0, 0);
+        const uint4 wq = w_s[e];
+        const uint32_t wc[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const long long v = lane_of(v4, j);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc[j * 4 + k] += v * (long long)wc[k];
+        }
+      }
+      // Reduce-scatter: after offset o the lane keeps the half of its entries
+      // selected by (lane & o); after o = 2 lane l holds entry l >> 1, and
+      // the o = 1 exchange completes the sum in both lanes of the pair.
+#pragma unroll
+      for (int o = 16, n = kEqRaw; o >= 2; o >>= 1, n >>= 1) {
+        const bool upper = lane & o;
+#pragma unroll
+        for (int q = 0; q < n / 2; ++q) {
+          const long long send = upper ? acc[q] : acc[q + n / 2];
+          const long long keep = upper ? acc[q + n / 2] : acc[q];
+          acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+      }
+      acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
+      if ((lane & 1) == 0) stage_s[warp][lane >> 1] = acc[0];
+      __syncthreads();
+      if (threadIdx.x < kEqRaw) {
+        long long t = 0;
+#pragma unroll
+        for (int w = 0; w < kEqThreads / 32; ++w) t += stage_s[w][threadIdx.x];
+        tot_s[b][threadIdx.x] = (tot_s[b][threadIdx.x] + mod_i64(t)) % P;
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < nb * kEqRaw; t += kEqThreads) atomicAdd(raw + t, tot_s[t / kEqRaw][t % kEqRaw]);
+}
+
+// Block fold of the packed payloads (packed_batch.rs:213-236): values[i] =
+// sum_b sum_j v(b * block_len + 4i + j) * T[b * 4 + j], T[b * 4 + j] =
+// (c^-1)^b * X^j, held in shared memory.  At most 128 blocks: a sum of 512
+// products stays below 2^55.
+__global__ void k_block_fold(const Wt* __restrict__ bva, uint64_t active, uint64_t block_len, int blocks, uint64_t m,
+                             const Fe* __restrict__ T, Fe* __restrict__ values) {
+  extern __shared__ uint4 smem_u4[];
+  Fe* t_s = reinterpret_cast<Fe*>(smem_u4);
+  for (int t = threadIdx.x; t < blocks * kC; t += blockDim.x) t_s[t] = T[t];
+  __syncthreads();
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
+    long long acc[kC];
+#pragma unroll
+    for (int k = 0; k < kC; ++k) acc[k] = 0;
+    for (int b = 0; b < blocks; ++b) {
+      const uint64_t g = uint64_t(b) * block_len + 4 * i;
+      if (g >= active) break;  // later blocks start even later
+      const uint2 v4 = load4(bva, active, g);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const long long v = lane_of(v4, j);
+        const Fr t = load(t_s + b * kC + j);
+#pragma unroll
+        for (int k = 0; k < kC; ++k) acc[k] += v * (long long)t.c[k];
+      }
+    }
+    Fr o;
+#pragma unroll
+    for (int k = 0; k < kC; ++k) o.c[k] = mod_i64(acc[k]);
+    store(values + i, o);
+  }
+}
+
+}  // namespace QFD_NS

@@ -73,8 +73,8 @@ extern "C" int qf_commit_block_noalloc(const qf_params* params, const int8_t* d_
                                        uint8_t* d_root, void* stream) {
   return qfc::guarded([&] {
     if (!params || !d_root || (!d_bva && n_values)) fail(QF_E_ARGUMENT, "null argument");
-    const auto& P = *params->P;
     if (params->field != QF_FIELD_F65521) fail(QF_E_ARGUMENT, "qf_commit_block_noalloc supports F65521 only");
+    const auto& P = *static_cast<const qf::Parameters<qf::Fp8>*>(params->P.get());
     if (P.chunk_log() > kMaxChunkLog)
       fail(QF_E_ARGUMENT, "qf_commit_block_noalloc: block of 2^" + std::to_string(P.chunk_log()) +
                               " weights exceeds the limit of 2^" + std::to_string(kMaxChunkLog) + " (" +

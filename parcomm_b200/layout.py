@@ -56,8 +56,11 @@ def buckets(shapes) -> Tuple[List[Bucket], int, int]:
     return out, active, logical
 
 
-def encode(shapes, matrices: Sequence[np.ndarray], dtype=np.int8) -> np.ndarray:
+def encode(shapes, matrices: Sequence[np.ndarray], dtype=None) -> np.ndarray:
+    """`dtype` defaults to the first matrix's (int8 weights or int16 payloads)."""
     bs, active, _ = buckets(shapes)
+    if dtype is None:
+        dtype = np.asarray(matrices[0]).dtype if len(matrices) else np.int8
     out = np.zeros(active, dtype=dtype)
     for b in bs:
         m = np.asarray(matrices[b.matrix])

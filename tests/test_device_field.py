@@ -18,10 +18,11 @@ def nvcc():
 
 
 @pytest.mark.skipif(nvcc() is None, reason="nvcc not available")
-def test_device_field_matches_host_field(tmp_path):
+@pytest.mark.parametrize("source", ["device_field_check.cu", "device_field_check_kb.cu"])
+def test_device_field_matches_host_field(tmp_path, source):
     exe = tmp_path / "device_field_check"
     subprocess.run([nvcc(), "-std=c++17", "-O2", "--expt-relaxed-constexpr", "-Xcompiler", "-ffp-contract=off",
-                    str(ROOT / "device_field_check.cu"), "-o", str(exe)], check=True)
+                    str(ROOT / source), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     out = json.loads(r.stdout.strip().splitlines()[-1])
     assert r.returncode == 0 and out["mismatches"] == 0, out

@@ -24,10 +24,21 @@ def gaussian_i8(rng, n, sigma=20.0, forced=0.0):
     return v
 
 
-def run_both(shapes, chunk_log, packed_log, mats):
-    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=packed_log))
+def gaussian_i16(rng, n, sigma=3000.0, forced=0.0):
+    v = np.clip(np.rint(rng.normal(0.0, sigma, n)), -32768, 32767).astype(np.int16)
+    if forced:
+        idx = rng.choice(n, max(1, int(n * forced)), replace=False)
+        v[idx] = np.where(rng.random(idx.size) < 0.5, -32768, 32767).astype(np.int16)
+    return v
+
+
+FIELDS = {"f65521": qf.FIELD_F65521, "koalabear": qf.FIELD_KOALABEAR}
+
+
+def run_both(shapes, chunk_log, packed_log, mats, field="f65521"):
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=packed_log), field=FIELDS[field])
     bva = layout.encode(p.shapes, mats)
-    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, packed_log, bva)
+    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, packed_log, bva, field=field)
     c = p.commit(bva)
     assert b"".join(c.roots) == o_roots, "commitment roots differ"
     claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
@@ -35,7 +46,7 @@ def run_both(shapes, chunk_log, packed_log, mats):
     proof, prof = p.prove(c, claims)
     assert proof.to_bytes() == o_proof, "proof bytes differ"
     p.verify(c.roots, claims, proof)
-    assert oracle.verify(p.shapes, chunk_log, packed_log, o_roots, o_claims, proof.to_bytes())
+    assert oracle.verify(p.shapes, chunk_log, packed_log, o_roots, o_claims, proof.to_bytes(), field=field)
     c.close()
     return proof, prof
 
@@ -95,6 +106,61 @@ def test_extreme_values_and_all_zero():
 def test_nonzero_padding_rejected():
     p = qf.Parameters([(31, 31)], qf.Config(chunk_log=10, packed_log=4))
     bva = layout.encode(p.shapes, [np.ones((31, 31), np.int8)])
+    bs, _, _ = layout.buckets(p.shapes)
+    b = next(b for b in bs if b.cols > b.physical_cols)
+    bva[b.offset + b.physical_cols] = 1
+    with pytest.raises(qf.QfError, match="nonzero boundary padding"):
+        p.commit(bva)
+
+
+# ---------------------------------------------------------------- KoalaBear^4, signed 16-bit payloads
+def test_koalabear_demo_bundle_matches_reference_digest(vectors):
+    shapes = qf.demo_shapes()
+    proof, prof = run_both(shapes, 10, 4, layout.demo_matrices(shapes, dtype=np.int16), field="koalabear")
+    assert len(proof.to_bytes()) == vectors["koalabear_demo"]["proof_bytes"]
+    assert blake2s(proof.to_bytes()) == vectors["koalabear_demo"]["proof_blake2s"]
+    assert prof.kernel_launches > 0
+
+
+@pytest.mark.parametrize("packed_log", [1, 4, 6])
+def test_koalabear_ragged_shapes_multilevel(packed_log):
+    rng = np.random.default_rng(70 + packed_log)
+    shapes = [(300, 700), (129, 65), (1, 5000), (77, 1)]
+    mats = [gaussian_i16(rng, r * c, forced=0.001).reshape(r, c) for r, c in shapes]
+    run_both(shapes, 14, packed_log, mats, field="koalabear")
+
+
+def test_koalabear_1024x4096_chunk20():
+    rng = np.random.default_rng(11)
+    mats = [gaussian_i16(rng, 1024 * 4096).reshape(1024, 4096)]
+    run_both([(1024, 4096)], 20, 4, mats, field="koalabear")
+
+
+@pytest.mark.parametrize("rows,chunk_log", [(2048, 23), (4096, 24)])
+def test_koalabear_single_matrix_deep_code_sequences(rows, chunk_log):
+    rng = np.random.default_rng(rows + chunk_log + 1)
+    mats = [gaussian_i16(rng, rows * 4096, forced=0.001).reshape(rows, 4096)]
+    run_both([(rows, 4096)], chunk_log, 4, mats, field="koalabear")
+
+
+def test_koalabear_single_block_and_zero_suffix():
+    rng = np.random.default_rng(13)
+    run_both([(64, 64)], 12, 4, [gaussian_i16(rng, 64 * 64).reshape(64, 64)], field="koalabear")
+    shapes = [(1024, 1024), (1, 16)]
+    mats = [gaussian_i16(rng, r * c).reshape(r, c) for r, c in shapes]
+    run_both(shapes, 16, 4, mats, field="koalabear")
+
+
+def test_koalabear_extreme_values_and_all_zero():
+    shapes = [(256, 256), (3, 3)]
+    mats = [np.full((256, 256), -32768, np.int16), np.zeros((3, 3), np.int16)]
+    mats[0][::7, ::3] = 32767
+    run_both(shapes, 12, 3, mats, field="koalabear")
+
+
+def test_koalabear_nonzero_padding_rejected():
+    p = qf.Parameters([(31, 31)], qf.Config(chunk_log=10, packed_log=4), field=qf.FIELD_KOALABEAR)
+    bva = layout.encode(p.shapes, [np.ones((31, 31), np.int16)])
     bs, _, _ = layout.buckets(p.shapes)
     b = next(b for b in bs if b.cols > b.physical_cols)
     bva[b.offset + b.physical_cols] = 1
