@@ -1,9 +1,12 @@
-"""QAFold commit+open throughput on B200: the 8B-shape 8-bit batched workload.
+"""QAFold commit+open throughput on B200: the 8B-shape batched workloads.
 
 Workload (one step): commit every 2^30-entry PCS block of the 226-matrix
-8B-shape collection (int8 round(N(0, 20^2)) clipped to +-127, 0.1% of entries
-forced to +-127; F65521^8, chunk_log 30, packed_log 4) and prove the
-benchmark claims, producing the reference's proof bytes.  As in the reference
+8B-shape collection and prove the benchmark claims, producing the
+reference's proof bytes.  `--workload 8b8` (the default): int8 round(N(0,
+20^2)) clipped to +-127 with 0.1% of entries forced to +-127, F65521^8,
+chunk_log 30, packed_log 4.  `--workload 8b16`: the raw 16-bit payloads of
+BF16 values drawn from N(0, 0.02^2) (the embedding from N(0, 1)),
+KoalaBear^4, chunk_log 30, packed_log 4.  As in the reference
 prover timer (main.rs:176-210) a step is commit + prove + serialisation;
 setup and claim generation are outside it.  The claims are computed once
 (their points derive from the committed roots, identical every step).
@@ -40,25 +43,33 @@ def shapes_8b():
     return [(128256, 4096)] + s + [(128256, 4096)]
 
 
-def make_bva_on_device(shapes, seed: int = 0):
-    """Deterministic synthetic int8 weights laid out as the BVA, generated on the GPU."""
+def make_bva_on_device(shapes, seed: int = 0, bf16: bool = False, embedding_first: bool = False):
+    """Deterministic synthetic weights laid out as the BVA, generated on the GPU:
+    int8 round(N(0, 20^2)) clipped to +-127 with 0.1% forced to +-127, or (bf16)
+    the int16 bit patterns of BF16 values from N(0, 0.02^2), matrix 0 from N(0, 1)
+    when `embedding_first`."""
     import torch
     from parcomm_b200 import layout
 
     buckets, active, _ = layout.buckets(shapes)
-    out = torch.zeros(active, dtype=torch.int8, device="cuda")
+    out = torch.zeros(active, dtype=torch.int16 if bf16 else torch.int8, device="cuda")
     by_matrix = {}
     for b in buckets:
         by_matrix.setdefault(b.matrix, []).append(b)
     g = torch.Generator(device="cuda")
     for m, (rows, cols) in enumerate(shapes):
         g.manual_seed(seed * 100003 + m)
-        w = torch.randn(rows * cols, generator=g, device="cuda", dtype=torch.float32).mul_(20.0).round_().clamp_(-127, 127)
-        n_forced = max(1, (rows * cols) // 1000)
-        idx = torch.randint(0, rows * cols, (n_forced,), generator=g, device="cuda")
-        sign = torch.randint(0, 2, (n_forced,), generator=g, device="cuda").float().mul_(254.0).sub_(127.0)
-        w[idx] = sign
-        w = w.to(torch.int8).view(rows, cols)
+        w = torch.randn(rows * cols, generator=g, device="cuda", dtype=torch.float32)
+        if bf16:
+            sigma = 1.0 if (embedding_first and m == 0) else 0.02
+            w = w.mul_(sigma).to(torch.bfloat16).view(torch.int16).view(rows, cols)
+        else:
+            w = w.mul_(20.0).round_().clamp_(-127, 127)
+            n_forced = max(1, (rows * cols) // 1000)
+            idx = torch.randint(0, rows * cols, (n_forced,), generator=g, device="cuda")
+            sign = torch.randint(0, 2, (n_forced,), generator=g, device="cuda").float().mul_(254.0).sub_(127.0)
+            w[idx] = sign
+            w = w.to(torch.int8).view(rows, cols)
         for b in by_matrix[m]:
             dst = out[b.offset: b.offset + b.rows * b.cols].view(b.rows, b.cols)
             dst[: b.physical_rows, : b.physical_cols] = w[b.row_offset: b.row_offset + b.physical_rows,
@@ -158,7 +169,7 @@ def job_throughput(weights_per_rank: int, world: int, ms_per_step: float) -> flo
     return weights_per_rank * world / (ms_per_step / 1000.0)
 
 
-def per_matrix_path(qf, shapes, seed_base: int):
+def per_matrix_path(qf, shapes, seed_base: int, field: int, bf16: bool):
     """The plain per-matrix path: every matrix committed and proven as its own
     single-matrix statement (its own layout, parameters and proof), one after
     another, through the same library.  Returns (timed seconds of one pass over
@@ -171,11 +182,11 @@ def per_matrix_path(qf, shapes, seed_base: int):
     params = {}
     for s in shapes:
         if s not in params:
-            params[s] = qf.Parameters([s], qf.Config(30, 4))
+            params[s] = qf.Parameters([s], qf.Config(30, 4), field=field)
     setup_s = time.time() - t0
     jobs = []
     for m, s in enumerate(shapes):
-        bva, _ = make_bva_on_device([s], seed=seed_base + m)
+        bva, _ = make_bva_on_device([s], seed=seed_base + m, bf16=bf16, embedding_first=bf16 and m == 0)
         p = params[s]
         c = p.commit(bva, on_device=True)
         claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
@@ -202,12 +213,21 @@ def run_reference(args):
     # One decoder layer's attention projections (4 matrices, 41.9M weights),
     # chunk_log 24 so the sample keeps the batched multi-block opening.
     shapes = [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096)]
+    sixteen = args.workload in ("8b16", "layers16")
+    field = "koalabear" if sixteen else "f65521"
     rng = np.random.default_rng(0)
     mats = []
     for r, c in shapes:
-        w = np.clip(np.rint(rng.normal(0, 20, r * c)), -127, 127).astype(np.int8)
-        idx = rng.choice(r * c, (r * c) // 1000, replace=False)
-        w[idx] = np.where(rng.random(idx.size) < 0.5, -127, 127)
+        if sixteen:
+            f = rng.normal(0, 0.02, r * c).astype(np.float32)
+            # BF16 bit pattern: the high half of the f32 word, rounded to nearest even.
+            u = f.view(np.uint32).astype(np.uint64)
+            u = (u + 0x7FFF + ((u >> 16) & 1)) >> 16
+            w = u.astype(np.uint16).view(np.int16)
+        else:
+            w = np.clip(np.rint(rng.normal(0, 20, r * c)), -127, 127).astype(np.int8)
+            idx = rng.choice(r * c, (r * c) // 1000, replace=False)
+            w[idx] = np.where(rng.random(idx.size) < 0.5, -127, 127)
         mats.append(w.reshape(r, c))
     bva = layout.encode(shapes, mats)
     weights = sum(r * c for r, c in shapes)
@@ -215,19 +235,21 @@ def run_reference(args):
     times = []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, 24, 4, bva)
+        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, 24, 4, bva, field=field)
         dt = time.perf_counter() - t0
         if step >= args.warmup:
             times.append((commit_ms + open_ms) / 1000.0)
     sec = statistics.mean(times)
     value = weights / sec
-    sample = (f"4 matrices of one 8B decoder layer (q,k,v,o: {weights} weights), chunk_log 24, packed_log 4, "
+    sample = (f"4 matrices of one 8B decoder layer (q,k,v,o: {weights} "
+              f"{'BF16 payloads' if sixteen else 'int8 weights'}), chunk_log 24, packed_log 4, "
               f"C++ restatement of the reference CPU prover (OpenMP, {threads} threads)")
     line = {
         "impl": "reference", "metric": "QAFold commit+open weights/s", "value": value, "unit": "weights/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
-        "data": "synthetic", "config": {"workload": "8B-shape 8-bit weights, batched (sample)", "field": "F65521^8",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16" if sixteen else "int8",
+        "data": "synthetic", "config": {"workload": f"8B-shape {16 if sixteen else 8}-bit weights, batched (sample)",
+                                        "field": "KoalaBear^4" if sixteen else "F65521^8",
                                         "chunk_log": 24, "packed_log": 4, "sample": sample},
         "cpu_baseline": {"value": value, "unit": "weights/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "weights/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -241,8 +263,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="8b8", choices=["8b8", "layers", "smoke"],
-                    help="8b8: the 8B shape set; layers: the first --layers transformer layers "
+    ap.add_argument("--workload", default="8b8", choices=["8b8", "8b16", "layers", "layers16", "smoke"],
+                    help="8b8 / 8b16: the 8B shape set with 8-bit weights (F65521^8) or 16-bit BF16 "
+                         "payloads (KoalaBear^4); layers / layers16: the first --layers transformer layers "
                          "(7 matrices each) at --chunk-log, a small case for profiling")
     ap.add_argument("--layers", type=int, default=2)
     ap.add_argument("--chunk-log", type=int, default=28)
@@ -271,21 +294,24 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    if args.workload == "8b8":
-        shapes, cfg, name = shapes_8b(), qf.Config(30, 4), "8B-shape 8-bit weights, batched (226 matrices)"
-    elif args.workload == "layers":
+    sixteen = args.workload in ("8b16", "layers16")
+    field = qf.FIELD_KOALABEAR if sixteen else qf.FIELD_F65521
+    bits = 16 if sixteen else 8
+    if args.workload in ("8b8", "8b16"):
+        shapes, cfg, name = shapes_8b(), qf.Config(30, 4), f"8B-shape {bits}-bit weights, batched (226 matrices)"
+    elif args.workload in ("layers", "layers16"):
         shapes = shapes_8b()[1:1 + 7 * args.layers]
         cfg = qf.Config(args.chunk_log, 4)
-        name = f"8B-shape 8-bit weights, first {args.layers} layers, chunk 2^{args.chunk_log}"
+        name = f"8B-shape {bits}-bit weights, first {args.layers} layers, chunk 2^{args.chunk_log}"
     else:
         shapes, cfg, name = [(1024, 4096)], qf.Config(20, 4), "smoke 1024x4096 int8"
     weights = sum(r * c for r, c in shapes)
 
     t0 = time.time()
-    params = qf.Parameters(shapes, cfg)
+    params = qf.Parameters(shapes, cfg, field=field)
     setup_s = time.time() - t0
-    bva_dev, active = make_bva_on_device(shapes, seed=rank)
-    bva_host = torch.empty(active, dtype=torch.int8, pin_memory=True)
+    bva_dev, active = make_bva_on_device(shapes, seed=rank, bf16=sixteen, embedding_first=args.workload == "8b16")
+    bva_host = torch.empty(active, dtype=bva_dev.dtype, pin_memory=True)
     bva_host.copy_(bva_dev)
 
     # Claims once: their points derive from the (step-invariant) roots.
@@ -349,9 +375,9 @@ def main():
     traffic = ncu_traffic(dominant, d["bytes"] / d["launches"])
 
     per_matrix = None
-    if not args.no_per_matrix and args.workload == "8b8":
+    if not args.no_per_matrix and args.workload in ("8b8", "8b16"):
         del bva_host
-        pm_s, pm_setup = per_matrix_path(qf, [(r, c) for r, c in shapes], 1_000_003 * (rank + 1))
+        pm_s, pm_setup = per_matrix_path(qf, [(r, c) for r, c in shapes], 1_000_003 * (rank + 1), field, sixteen)
         pm_ms = max_over_ranks(pm_s * 1000.0, world)
         per_matrix = {"value": job_throughput(weights, world, pm_ms), "unit": "weights/s", "ms_per_pass": pm_ms,
                       "proofs_per_pass": len(shapes), "setup_s": pm_setup,
@@ -368,7 +394,8 @@ def main():
     if not args.no_cpu_baseline:
         try:
             r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1",
-                                "--warmup", "0"], capture_output=True, text=True, timeout=900)
+                                "--warmup", "0", "--workload", args.workload], capture_output=True, text=True,
+                               timeout=900)
             cpu_baseline = json.loads(r.stdout.strip().splitlines()[-1])["cpu_baseline"]
         except Exception as e:  # reported, not fatal
             cpu_baseline = {"error": str(e)[:200]}
@@ -384,14 +411,14 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "int8",
+        "dtype": "int16" if sixteen else "int8",
         "data": "synthetic",
-        "config": {"workload": name, "field": "F65521^8", "chunk_log": cfg.chunk_log, "packed_log": cfg.packed_log,
-                   "weights": weights, "active_entries": active, "pcs_blocks": params.blocks,
-                   "l2": "inputs larger than L2 (8 GB BVA, 4 GiB codeword per block)",
+        "config": {"workload": name, "field": "KoalaBear^4" if sixteen else "F65521^8", "chunk_log": cfg.chunk_log,
+                   "packed_log": cfg.packed_log, "weights": weights, "active_entries": active, "pcs_blocks": params.blocks,
+                   "l2": "inputs larger than L2 (BVA of 8 or 16 GB, 4 or 8 GiB codeword per block)",
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": {"value": job_throughput(weights, world, ms_e2e), "unit": "weights/s",
-                "h2d_bytes_per_step": active, "d2h_bytes_per_step": proof_bytes},
+                "h2d_bytes_per_step": active * bva_dev.element_size(), "d2h_bytes_per_step": proof_bytes},
         "gpu_launches": launches // max(args.steps, 1),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
