@@ -42,9 +42,19 @@ QFD_HD uint32_t red64(uint64_t v) {
   if (r >= P) r -= P;
   return uint32_t(r);
 }
+QFD_HD uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 QFD_HD uint32_t red32(uint32_t v) { return v >= P ? v - P : v; }  // v < 2p
-QFD_HD uint32_t addp(uint32_t a, uint32_t b) { uint32_t s = a + b; return s >= P ? s - P : s; }
-QFD_HD uint32_t subp(uint32_t a, uint32_t b) { return a >= b ? a - b : a + P - b; }
+// Canonical a, b < p < 2^31.  The sum is below 2^32, and s - p wraps above
+// s exactly when s < p, so the unsigned minimum picks the reduced value; for
+// the difference, a - b wraps above a - b + p exactly when a < b.
+QFD_HD uint32_t addp(uint32_t a, uint32_t b) {
+  const uint32_t s = a + b;
+  return umin32(s, s - P);
+}
+QFD_HD uint32_t subp(uint32_t a, uint32_t b) {
+  const uint32_t d = a - b;
+  return umin32(d, d + P);
+}
 
 QFD_HD Fr unpack_fe(uint4 u) { Fr r; r.c[0] = u.x; r.c[1] = u.y; r.c[2] = u.z; r.c[3] = u.w; return r; }
 QFD_HD uint4 pack_fe(const Fr& r) { return make_uint4(r.c[0], r.c[1], r.c[2], r.c[3]); }

@@ -23,6 +23,13 @@ __device__ __forceinline__ uint2 load4(const Wt* __restrict__ bva, uint64_t acti
     if (g + j < active) w[j >> 1] |= (uint32_t(bva[g + j]) & 0xffffu) << (16 * (j & 1));
   return make_uint2(w[0], w[1]);
 }
+// c + a * b for a 32-bit signed a and b (a canonical coefficient is below
+// 2^31, so it is one): a single widening multiply-add into 64 bits.
+__device__ __forceinline__ long long mad_wide(int a, int b, long long c) {
+  long long d;
+  asm("mad.wide.s32 %0, %1, %2, %3;" : "=l"(d) : "r"(a), "r"(b), "l"(c));
+  return d;
+}
 // Payload j (0..3) of a load4 word pair.
 __device__ __forceinline__ int lane_of(uint2 u, int j) { return int(int16_t(((j < 2 ? u.x : u.y) >> (16 * (j & 1))) & 0xffffu)); }
 
@@ -81,9 +88,9 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __rest
         const Fr w = load(lo + r);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const long long v = lane_of(u[q], j);
+          const int v = lane_of(u[q], j);
 #pragma unroll
-          for (int k = 0; k < kC; ++k) acc[j][k] += (long long)w.c[k] * v;
+          for (int k = 0; k < kC; ++k) acc[j][k] = mad_wide(int(w.c[k]), v, acc[j][k]);
         }
       }
     }
@@ -132,10 +139,10 @@ __global__ void k_eo_witness(const Wt* __restrict__ bva, uint64_t active, uint64
         const uint2 u = n == 4 ? load4(bva, active, g0 + l0) : make_uint2(0, 0);
         for (int j = 0; j < n; ++j) {
           const uint64_t g = g0 + l0 + j;
-          const long long v = n == 4 ? lane_of(u, j) : (g < active ? int(bva[g]) : 0);
+          const int v = n == 4 ? lane_of(u, j) : (g < active ? int(bva[g]) : 0);
           const Fr p = load(pw + l0 + j);
 #pragma unroll
-          for (int k = 0; k < kC; ++k) acc[k] += (long long)p.c[k] * v;
+          for (int k = 0; k < kC; ++k) acc[k] = mad_wide(int(p.c[k]), v, acc[k]);
         }
       }
     }
@@ -183,9 +190,9 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const Wt* _
         const uint32_t wc[4] = {wq.x, wq.y, wq.z, wq.w};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const long long v = lane_of(v4, j);
+          const int v = lane_of(v4, j);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) acc[j * 4 + k] += v * (long long)wc[k];
+          for (int k = 0; k < 4; ++k) acc[j * 4 + k] = mad_wide(int(wc[k]), v, acc[j * 4 + k]);
         }
       }
       // Reduce-scatter: after offset o the lane keeps the half of its entries
@@ -236,10 +243,10 @@ __global__ void k_block_fold(const Wt* __restrict__ bva, uint64_t active, uint64
       const uint2 v4 = load4(bva, active, g);
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
-        const long long v = lane_of(v4, j);
+        const int v = lane_of(v4, j);
         const Fr t = load(t_s + b * kC + j);
 #pragma unroll
-        for (int k = 0; k < kC; ++k) acc[k] += v * (long long)t.c[k];
+        for (int k = 0; k < kC; ++k) acc[k] = mad_wide(int(t.c[k]), v, acc[k]);
       }
     }
     Fr o;
