@@ -71,6 +71,19 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
               uint8_t* roots_out);
 void qf_committed_free(qf_committed* committed);
 
+/* Parameters::commit_recomputed (protocol.rs:131-185, the reference's
+ * `--cache-mode recompute`) for weight sets larger than HBM: `host_bva`
+ * (n_values entries in host memory; page-locked memory lets the copies
+ * overlap the compute) stays owned by the caller and must stay valid and
+ * unchanged until the committed handle is freed.  Every pass that reads the
+ * weights (commit, EO cross terms and witness, projection, block fold) stages
+ * them into HBM one PCS block at a time, and binding re-encodes each block
+ * and checks its root.  The first resident_bytes / (2^chunk_log * entry size)
+ * blocks are kept in HBM after the first pass.  Needs at least two PCS
+ * blocks.  Writes the same roots, claims and proof bytes as qf_commit. */
+int qf_commit_streamed(const qf_params* params, const void* host_bva, uint64_t n_values, uint64_t resident_bytes,
+                       qf_committed** out, uint8_t* roots_out);
+
 /* serde_json of the Commitment statement (protocol.rs:33-40), as absorbed. */
 int qf_statement_json(const qf_params* params, const uint8_t* roots, char* buf, size_t cap, size_t* len);
 

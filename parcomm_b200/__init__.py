@@ -58,7 +58,7 @@ _lib = None
 EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
-    "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc",
+    "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
 )
 
 
@@ -77,6 +77,7 @@ def lib() -> ctypes.CDLL:
         L.qf_params_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64),
                                      ctypes.POINTER(U64), ctypes.c_char_p]
         L.qf_commit.argtypes = [P, P, U64, ctypes.c_int, ctypes.POINTER(P), ctypes.c_char_p]
+        L.qf_commit_streamed.argtypes = [P, P, U64, U64, ctypes.POINTER(P), ctypes.c_char_p]
         L.qf_committed_free.argtypes = [P]
         L.qf_committed_free.restype = None
         L.qf_statement_json.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.POINTER(S)]
@@ -177,13 +178,15 @@ def claims_from_bytes(shapes: Sequence[Shape], data: bytes, with_value: bool = T
 
 
 class Committed:
-    """Committed state: weights, codewords and Merkle trees resident in HBM."""
+    """Committed state: weights, codewords and Merkle trees resident in HBM,
+    or (recompute mode) the roots only, over weights kept in host memory."""
 
-    def __init__(self, params: "Parameters", handle: int, roots: List[bytes]):
+    def __init__(self, params: "Parameters", handle: int, roots: List[bytes], keep=None):
         self.params = params
         self._h = ctypes.c_void_p(handle)
         self.roots = roots
         self.consumed = False
+        self._keep = keep  # host weights the handle streams from
 
     @property
     def statement(self) -> "Commitment":
@@ -272,7 +275,27 @@ class Parameters:
         _check(lib().qf_commit(self._h, ctypes.c_void_p(ptr), n, int(on_device), ctypes.byref(h), roots))
         return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)])
 
-    commit_recomputed = commit
+    def commit_recomputed(self, values, resident_bytes: int = 0) -> Committed:
+        """Parameters::commit_recomputed: the reference's recompute mode.  Host
+        weights (a numpy array, or a CPU tensor, ideally in pinned memory) stay
+        where they are and are streamed into HBM one PCS block at a time for
+        every pass; only the roots stay on the device and binding re-encodes
+        each block.  `resident_bytes` of leading blocks are kept in HBM after
+        the first pass.  Device tensors take the cached path (`commit`).  The
+        roots, claims and proof bytes equal those of `commit`."""
+        if hasattr(values, "is_cuda") and values.is_cuda:
+            return self.commit(values, on_device=True)
+        if hasattr(values, "data_ptr"):
+            if int(values.element_size()) != np.dtype(self.weight_dtype).itemsize or not values.is_contiguous():
+                raise QfError(-9, f"host weights must be contiguous {np.dtype(self.weight_dtype).name}")
+            keep, ptr, n = values, int(values.data_ptr()), int(values.numel())
+        else:
+            keep = np.ascontiguousarray(values, dtype=self.weight_dtype)
+            ptr, n = keep.ctypes.data, keep.size
+        h = ctypes.c_void_p()
+        roots = ctypes.create_string_buffer(32 * max(self.blocks, 1))
+        _check(lib().qf_commit_streamed(self._h, ctypes.c_void_p(ptr), n, int(resident_bytes), ctypes.byref(h), roots))
+        return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)], keep=keep)
 
     def block_root_noalloc(self, bva, block: int, root, stream: int = 0) -> None:
         """qf_commit_block_noalloc: the root of PCS block `block` of the

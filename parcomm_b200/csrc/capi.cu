@@ -74,6 +74,18 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
   });
 }
 
+int qf_commit_streamed(const qf_params* params, const void* host_bva, uint64_t n_values, uint64_t resident_bytes,
+                       qf_committed** out, uint8_t* roots_out) {
+  return guarded([&] {
+    if (!params || !out || (!host_bva && n_values)) fail(QF_E_ARGUMENT, "null argument");
+    require_device();
+    auto c = std::make_unique<qf_committed>();
+    c->params = params;
+    api(params->field).commit_streamed(params, host_bva, n_values, resident_bytes, c.get(), roots_out);
+    *out = c.release();
+  });
+}
+
 void qf_committed_free(qf_committed* committed) { delete committed; }
 
 int qf_statement_json(const qf_params* params, const uint8_t* roots, char* buf, size_t cap, size_t* len) {

@@ -43,6 +43,33 @@ __global__ void k_check_zero_segments(const uint8_t* __restrict__ bva, const uin
 }
 
 
+// The entries of the layout's zero padding (Layout::validate_values,
+// layout.rs:136-155) inside [lo, hi), as byte ranges relative to lo, cut into
+// pieces of at most kZeroPiece bytes.
+static std::vector<uint64_t> padding_segments(const Parameters<F>& P, uint64_t lo, uint64_t hi) {
+  std::vector<uint64_t> runs;
+  auto add_run = [&](uint64_t a, uint64_t e) {
+    a = std::max(a, lo);
+    e = std::min(e, hi);
+    if (a >= e) return;
+    if (!runs.empty() && runs.back() == a) runs.back() = e;  // merge contiguous runs
+    else { runs.push_back(a); runs.push_back(e); }
+  };
+  for (const Bucket& b : P.layout.buckets) {
+    if (b.offset + b.rows * b.cols <= lo || b.offset >= hi) continue;
+    if (b.physical_cols < b.cols)  // the padded tail of every real row
+      for (size_t r = 0; r < b.physical_rows; ++r) add_run(b.offset + r * b.cols + b.physical_cols, b.offset + (r + 1) * b.cols);
+    add_run(b.offset + b.physical_rows * b.cols, b.offset + b.rows * b.cols);  // padding rows
+  }
+  std::vector<uint64_t> seg;
+  for (size_t i = 0; i < runs.size(); i += 2)
+    for (uint64_t a = (runs[i] - lo) * sizeof(W); a < (runs[i + 1] - lo) * sizeof(W); a += kZeroPiece) {
+      seg.push_back(a);
+      seg.push_back(std::min<uint64_t>(a + kZeroPiece, (runs[i + 1] - lo) * sizeof(W)));
+    }
+  return seg;
+}
+
 // A side stream for the weight transfer, with one event per block.
 struct CopyPipeline {
   cudaStream_t stream = nullptr;
@@ -68,13 +95,15 @@ struct CopyPipeline {
 
 struct FieldCommitted : qf_committed_state {
   cudaStream_t stream = nullptr;
-  DBuf<W> bva;
+  DBuf<W> bva;                       // resident weights
+  std::unique_ptr<BlockStream> src;  // or streamed weights
   uint64_t active = 0;
   std::unique_ptr<GpuBackend> be;
   std::vector<Digest> roots;
   double commit_ms = 0, upload_ms = 0;
   ~FieldCommitted() override {
     be.reset();
+    src.reset();
     bva.reset();
     if (stream) cudaStreamDestroy(stream);
   }
@@ -121,21 +150,29 @@ static std::vector<Claim<F>> device_eval_claims(const Parameters<F>& P, GpuBacke
     terms.push_back(std::move(t));
   }
   for (auto& c : claims) c.value = F::zero();
-  // Group by lane width (terms with fewer than four factors use fewer lanes).
+  // Group by lane width (terms with fewer than four factors use fewer lanes);
+  // all groups go through one pass over the weights.
+  std::vector<std::vector<const Term<F>*>> groups;
+  std::vector<std::vector<size_t>> which;
+  std::vector<size_t> group_log;
   for (size_t lanes_log = 0; lanes_log <= 4; ++lanes_log) {
     std::vector<const Term<F>*> group;
-    std::vector<size_t> which;
+    std::vector<size_t> w;
     for (size_t i = 0; i < terms.size(); ++i)
-      if (std::min<size_t>(4, terms[i].factors.size()) == lanes_log) { group.push_back(&terms[i]); which.push_back(i); }
+      if (std::min<size_t>(4, terms[i].factors.size()) == lanes_log) { group.push_back(&terms[i]); w.push_back(i); }
     if (group.empty()) continue;
-    auto pr = be.project_terms(group, 16);
-    for (size_t g = 0; g < group.size(); ++g) {
-      std::vector<F> low = factor_weights(group[g]->factors.data(), lanes_log);
-      F v = F::zero();
-      for (size_t l = 0; l < pr[g].size(); ++l) v += pr[g][l] * low[l];
-      claims[P.layout.buckets[which[g]].matrix].value += v;
-    }
+    groups.push_back(std::move(group));
+    which.push_back(std::move(w));
+    group_log.push_back(lanes_log);
   }
+  auto pr = be.project_term_groups(groups, 16);
+  for (size_t k = 0; k < groups.size(); ++k)
+    for (size_t g = 0; g < groups[k].size(); ++g) {
+      std::vector<F> low = factor_weights(groups[k][g]->factors.data(), group_log[k]);
+      F v = F::zero();
+      for (size_t l = 0; l < pr[k][g].size(); ++l) v += pr[k][g][l] * low[l];
+      claims[P.layout.buckets[which[k][g]].matrix].value += v;
+    }
   return claims;
 }
 
@@ -187,23 +224,7 @@ void commit(const qf_params* params, const void* bva, uint64_t n_values, int bva
     QF_CK(cudaEventElapsedTime(&up, copies.begin, copies.end));
     c->upload_ms = up;
     // Padding must be zero (validate_values) — checked on the device.
-    std::vector<uint64_t> runs;
-    auto add_run = [&](uint64_t a, uint64_t e) {
-      if (a >= e) return;
-      if (!runs.empty() && runs.back() == a) runs.back() = e;  // merge contiguous runs
-      else { runs.push_back(a); runs.push_back(e); }
-    };
-    for (const Bucket& b : P.layout.buckets) {
-      if (b.physical_cols < b.cols)  // the padded tail of every real row
-        for (size_t r = 0; r < b.physical_rows; ++r) add_run(b.offset + r * b.cols + b.physical_cols, b.offset + (r + 1) * b.cols);
-      add_run(b.offset + b.physical_rows * b.cols, b.offset + b.rows * b.cols);  // padding rows
-    }
-    std::vector<uint64_t> seg;  // runs, as byte ranges cut into pieces of at most kZeroPiece bytes
-    for (size_t i = 0; i < runs.size(); i += 2)
-      for (uint64_t a = runs[i] * sizeof(W); a < runs[i + 1] * sizeof(W); a += kZeroPiece) {
-        seg.push_back(a);
-        seg.push_back(std::min<uint64_t>(a + kZeroPiece, runs[i + 1] * sizeof(W)));
-      }
+    std::vector<uint64_t> seg = padding_segments(P, 0, n_values);
     if (!seg.empty()) {
       DBuf<uint64_t> dseg(seg.size());
       DBuf<unsigned int> flag(1);
@@ -222,6 +243,52 @@ void commit(const qf_params* params, const void* bva, uint64_t n_values, int bva
     if (roots_out)
       for (size_t b = 0; b < c->roots.size(); ++b) std::memcpy(roots_out + 32 * b, c->roots[b].data(), 32);
     out->state = std::move(c);
+}
+
+// Recompute mode over weights that stay in host memory (`host` must outlive
+// the committed handle): one streamed pass commits every block and checks
+// the padding; the first `resident_bytes` worth of blocks stay in HBM.
+void commit_streamed(const qf_params* params, const void* host, uint64_t n_values, uint64_t resident_bytes,
+                     qf_committed* out, uint8_t* roots_out) {
+  const auto& P = params_of(params);
+  check(n_values == P.layout.active, "active BVA length mismatch");
+  auto c = std::make_unique<FieldCommitted>();
+  c->active = n_values;
+  QF_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  auto t0 = std::chrono::steady_clock::now();
+  const size_t resident = size_t(resident_bytes / (P.block_len * sizeof(W)));
+  c->src = std::make_unique<BlockStream>(static_cast<const W*>(host), n_values, P.block_len, resident, 3);
+  c->be = std::make_unique<GpuBackend>(P, c->src.get(), c->stream, static_cast<DeviceTables*>(params->tables.get()));
+  // Padding segments of every live block, relative to the block, uploaded once.
+  const size_t live = c->src->live_blocks();
+  std::vector<uint64_t> seg;
+  std::vector<size_t> seg_at(live + 1, 0);
+  for (size_t b = 0; b < live; ++b) {
+    const uint64_t lo = uint64_t(b) * P.block_len;
+    std::vector<uint64_t> s = padding_segments(P, lo, std::min<uint64_t>(lo + P.block_len, n_values));
+    seg.insert(seg.end(), s.begin(), s.end());
+    seg_at[b + 1] = seg.size();
+  }
+  DBuf<uint64_t> dseg(std::max<size_t>(seg.size(), 1));
+  DBuf<unsigned int> flag(1);
+  if (!seg.empty()) QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, c->stream));
+  QF_CK(cudaMemsetAsync(flag.p, 0, 4, c->stream));
+  c->roots = c->be->commit_streamed([&](size_t b, const W* d, uint64_t) {
+    const size_t ns = (seg_at[b + 1] - seg_at[b]) / 2;
+    if (!ns) return;
+    QF_LAUNCH(c->stream, "k_check_zero_segments", 0,
+              k_check_zero_segments<<<unsigned(std::min<size_t>(ns, 148 * 8)), 256, 0, c->stream>>>(
+                  reinterpret_cast<const uint8_t*>(d), dseg.p + seg_at[b], uint32_t(ns), flag.p));
+  });
+  unsigned int h = 0;
+  QF_CK(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, c->stream));
+  QF_CK(cudaStreamSynchronize(c->stream));
+  check(h == 0, "nonzero boundary padding");
+  c->commit_ms = ms_since(t0);
+  c->upload_ms = 0;
+  if (roots_out)
+    for (size_t b = 0; b < c->roots.size(); ++b) std::memcpy(roots_out + 32 * b, c->roots[b].data(), 32);
+  out->state = std::move(c);
 }
 
 std::string statement_json(const qf_params* params, const uint8_t* roots) {
@@ -290,7 +357,7 @@ void verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims
 
 }  // namespace
 
-const qfc::FieldApi kFieldApi = {sizeof(W), make_params, info, commit, statement_json, benchmark_points_bytes,
-                                 eval_claims, prove, verify};
+const qfc::FieldApi kFieldApi = {sizeof(W), make_params, info, commit, commit_streamed, statement_json,
+                                 benchmark_points_bytes, eval_claims, prove, verify};
 
 }  // namespace QFB_NS

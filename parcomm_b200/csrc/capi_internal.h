@@ -42,6 +42,8 @@ struct FieldApi {
                uint8_t digest[32]);
   void (*commit)(const qf_params* p, const void* bva, uint64_t n_values, int on_device, qf_committed* c,
                  uint8_t* roots_out);
+  void (*commit_streamed)(const qf_params* p, const void* host_bva, uint64_t n_values, uint64_t resident_bytes,
+                          qf_committed* c, uint8_t* roots_out);
   std::string (*statement_json)(const qf_params* p, const uint8_t* roots);
   std::vector<uint8_t> (*benchmark_points)(const qf_params* p, const uint8_t* roots);
   std::vector<uint8_t> (*eval_claims)(const qf_params* p, const qf_committed* c, const uint8_t* points, size_t len);

@@ -122,7 +122,68 @@ GpuBackend::GpuBackend(const Parameters<F>& p, const W* d_bva, size_t active, cu
   partials_.alloc(148 * 8 * 4);
   result_.alloc(8);
 }
+GpuBackend::GpuBackend(const Parameters<F>& p, BlockStream* src, cudaStream_t s, DeviceTables* tables)
+    : P_(p), bva_(nullptr), src_(src), active_(src->active()), s_(s), tables_(tables ? tables : &own_tables_) {
+  configure_tile_kernels();
+  check(P_.blocks() >= 2, "streamed weights need at least two PCS blocks");
+  check(src->block_len() == P_.block_len, "block length of the weight stream");
+  partials_.alloc(148 * 8 * 4);
+  result_.alloc(8);
+}
 GpuBackend::~GpuBackend() {}
+
+// ---------------------------------------------------------------- streamed weights
+BlockStream::BlockStream(const W* host, uint64_t active, uint64_t block_len, size_t resident, int slots)
+    : host_(host), active_(active), block_len_(block_len) {
+  check(slots >= 2, "at least two staging slots");
+  live_ = size_t((active + block_len - 1) / block_len);
+  resident_ = std::min(resident, live_);
+  if (resident_) resident_buf_.alloc(resident_ * block_len);
+  const size_t streamed = live_ - resident_;
+  slot_buf_.resize(std::min<size_t>(size_t(slots), streamed));
+  for (auto& b : slot_buf_) b.alloc(block_len);
+  QF_CK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
+  landed_.assign(live_, nullptr);
+  for (auto& e : landed_) QF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  freed_.assign(slot_buf_.size(), nullptr);
+  for (auto& e : freed_) QF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+BlockStream::~BlockStream() {
+  if (copy_) cudaStreamSynchronize(copy_);
+  for (auto& e : landed_)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : freed_)
+    if (e) cudaEventDestroy(e);
+  if (copy_) cudaStreamDestroy(copy_);
+}
+
+void BlockStream::for_each(cudaStream_t s, const BlockFn& fn) {
+  const size_t K = slot_buf_.size();
+  auto n_of = [&](size_t b) { return std::min<uint64_t>(block_len_, active_ - uint64_t(b) * block_len_); };
+  auto dev_of = [&](size_t b) -> W* {
+    return b < resident_ ? resident_buf_.p + uint64_t(b) * block_len_ : slot_buf_[(b - resident_) % K].p;
+  };
+  // Block j goes to its resident place or to slot (j - resident) % K, whose
+  // previous block is j - K: the copy waits until that block's launches are
+  // done.  Copies run up to K blocks ahead of the compute position.
+  auto issue = [&](size_t j) {
+    if (j < resident_ && resident_ready_) return;
+    if (j >= resident_) QF_CK(cudaStreamWaitEvent(copy_, freed_[(j - resident_) % K], 0));
+    const uint64_t n = n_of(j);
+    QF_CK(cudaMemcpyAsync(dev_of(j), host_ + uint64_t(j) * block_len_, n * sizeof(W), cudaMemcpyHostToDevice, copy_));
+    QF_CK(cudaEventRecord(landed_[j], copy_));
+    copied_ += n * sizeof(W);
+  };
+  const size_t ahead = std::max<size_t>(K, 1);
+  size_t issued = 0;
+  for (size_t i = 0; i < live_; ++i) {
+    while (issued < live_ && issued < i + ahead) issue(issued++);
+    if (!(i < resident_ && resident_ready_)) QF_CK(cudaStreamWaitEvent(s, landed_[i], 0));
+    fn(i, dev_of(i), n_of(i));
+    if (i >= resident_) QF_CK(cudaEventRecord(freed_[(i - resident_) % K], s));
+  }
+  if (resident_) resident_ready_ = true;
+}
 
 const Fe* DeviceTables::alpha(const PcsParams<F>& pp, size_t level, int which) {
   int dev = 0;
@@ -232,8 +293,31 @@ static std::unique_ptr<DeviceCodeword> alloc_codeword(size_t R, size_t cols, cud
   return cw;
 }
 
+Digest GpuBackend::encode_block(const W* bva, uint64_t active, uint64_t src_base, DeviceCodeword& cw) {
+  const int logm = ilog2(P_.pcs.packed_len());
+  const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+  const int l0 = std::min(qfd::kMaxTileLog, logm);
+  const size_t smem = qfd::kTileSmem;
+  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * (F::kLanes * sizeof(W) + 16),
+            qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
+                bva, active, src_base, cw.cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
+  mobius_rest(cw.cw.p, logm, logR, l0);
+  encode_and_hash(cw, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
+  return cw.root_;
+}
+
+DeviceCodeword& GpuBackend::scratch_codeword() {
+  if (!scratch_) {
+    const int logm = ilog2(P_.pcs.packed_len());
+    const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+    scratch_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
+  }
+  return *scratch_;
+}
+
 Digest GpuBackend::commit_block(size_t b) {
   HostScope hs("commit_block");
+  check(!src_, "commit_block on streamed weights");
   const int logm = ilog2(P_.pcs.packed_len());
   const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
   // The implicit zero suffix repeats one codeword; reuse its root and state.
@@ -247,17 +331,28 @@ Digest GpuBackend::commit_block(size_t b) {
       }
   }
   auto cw = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
-  const int l0 = std::min(qfd::kMaxTileLog, logm);
-  const size_t smem = qfd::kTileSmem;
-  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * 24, qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
-                bva_, active_, uint64_t(b) * P_.block_len, cw->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
-  mobius_rest(cw->cw.p, logm, logR, l0);
-  encode_and_hash(*cw, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
+  encode_block(bva_, active_, uint64_t(b) * P_.block_len, *cw);
   if (blocks_.size() <= b) blocks_.resize(b + 1);
   roots_.resize(std::max(roots_.size(), b + 1));
   roots_[b] = cw->root_;
   blocks_[b] = std::move(cw);
   return roots_[b];
+}
+
+std::vector<Digest> GpuBackend::commit_streamed(const BlockStream::BlockFn& per_block) {
+  HostScope hs("commit_streamed");
+  check(src_ != nullptr, "commit_streamed needs streamed weights");
+  DeviceCodeword& cw = scratch_codeword();
+  roots_.assign(P_.blocks(), Digest{});
+  src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+    roots_[b] = encode_block(d, n, 0, cw);
+    if (per_block) per_block(b, d, n);
+  });
+  if (src_->live_blocks() < P_.blocks()) {  // the zero suffix: one codeword for all
+    const Digest z = encode_block(nullptr, 0, 0, cw);
+    for (size_t b = src_->live_blocks(); b < P_.blocks(); ++b) roots_[b] = z;
+  }
+  return roots_;
 }
 
 // The same kernels as commit_block + encode_and_hash, launched without the
@@ -363,7 +458,15 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   // Zero blocks (the suffix past the active entries) have vanishing lanes.
   const size_t live = std::min<size_t>(nblocks, (active_ + P_.block_len - 1) / P_.block_len);
   const unsigned grid = unsigned(std::min<uint64_t>((m + qfd::kEqChunk - 1) / qfd::kEqChunk, 148 * 4));
-  for (size_t b0 = 0; b0 < live; b0 += qfd::kEqBlocks) {
+  if (src_) {  // one block per launch, as each lands in HBM
+    src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+      if (b >= nblocks) return;
+      QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W),
+                qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(d, n, P_.block_len, 0, 1, m, weights_.p,
+                                                                           raw.p + kRaw * b));
+    });
+  }
+  for (size_t b0 = 0; !src_ && b0 < live; b0 += qfd::kEqBlocks) {
     const int nb = int(std::min<size_t>(qfd::kEqBlocks, live - b0));
     QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W) * uint64_t(nb),
               qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva_, active_, P_.block_len, b0, nb, m, weights_.p,
@@ -386,6 +489,7 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
 }
 
 std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
+  check(!src_, "single-block opening of streamed weights");
   std::vector<std::vector<F>> lanes = project_blocks(outer, 1);
   // Packed values of the single block: the block fold with weight one.
   const uint64_t m = P_.pcs.packed_len();
@@ -395,7 +499,7 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   for (int j = 0; j < L; ++j) T[j] = basis<F>(j);
   DBuf<Fe> dT(L);
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), L * 16, cudaMemcpyHostToDevice, s_));
-  QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p));
+  QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p, 0));
   sum_len_ = m;
   msg_valid_ = false;
   return lanes[0];
@@ -422,9 +526,19 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   DBuf<Fe> dT(T.size());
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), T.size() * 16, cudaMemcpyHostToDevice, s_));
   values_.alloc(m);
-  set_smem(qfd::k_block_fold, T.size() * 16);
-  QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
-                                                                          values_.p));
+  if (src_) {  // accumulate block by block; the zero blocks add nothing
+    QF_CK(cudaMemsetAsync(values_.p, 0, m * 16, s_));
+    src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+      if (b >= size_t(blocks)) return;
+      QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 32),
+                qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(d, n, P_.block_len, 1, m, dT.p + b * L,
+                                                                                  values_.p, 1));
+    });
+  } else {
+    set_smem(qfd::k_block_fold, T.size() * 16);
+    QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
+                                                                            values_.p, 0));
+  }
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
@@ -503,6 +617,28 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
     }
     write_rows(w, r);
   };
+  if (src_) {
+    // Recompute mode: re-encode every live block as its weights land, check
+    // its root, then the zero suffix once.
+    DeviceCodeword& cw = scratch_codeword();
+    check(roots.size() == P_.blocks(), "block roots");
+    src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+      if (encode_block(d, n, 0, cw) != roots[b]) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
+      emit(cw);
+    });
+    if (src_->live_blocks() < roots.size()) {
+      const Digest z = encode_block(nullptr, 0, 0, cw);
+      const size_t at = w.out.size();
+      emit(cw);
+      const std::vector<uint8_t> zero_rows(w.out.begin() + at, w.out.end());
+      for (size_t b = src_->live_blocks(); b < roots.size(); ++b) {
+        if (roots[b] != z) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
+        if (b > src_->live_blocks()) w.out.insert(w.out.end(), zero_rows.begin(), zero_rows.end());
+      }
+    }
+    emit(*folded_);
+    return std::move(w.out);
+  }
   for (size_t b = 0; b < roots.size(); ++b) {
     const DeviceCodeword* cw = b < blocks_.size() ? blocks_[b].get() : nullptr;
     if (!cw) {  // a repeated zero block: the first committed zero block
@@ -520,6 +656,14 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
 std::vector<W> GpuBackend::windows(const std::vector<uint64_t>& starts, size_t stride) {
   std::vector<W> out(starts.size() * stride);
   if (starts.empty()) return out;
+  if (src_) {  // a few entries each: read them where the weights live
+    for (size_t i = 0; i < starts.size(); ++i)
+      for (size_t k = 0; k < stride; ++k) {
+        const uint64_t g = starts[i] + k;
+        out[i * stride + k] = g < active_ ? src_->host()[g] : W(0);
+      }
+    return out;
+  }
   DBuf<uint64_t> ds(starts.size());
   DBuf<W> dout(out.size());
   QF_CK(cudaMemcpyAsync(ds.p, starts.data(), starts.size() * 8, cudaMemcpyHostToDevice, s_));
@@ -568,16 +712,18 @@ struct TableBuilder {
   DBuf<qfd::TableSpec> dspec;
 };
 
-// One term's tiles: rows of 2^lb, high bits split into mid (<= 2^10) and top.
+// One term's tiles: rows of 2^lb (lb <= max_lb), high bits split into mid
+// (<= 2^10) and top.
 qfd::TermTiles term_tiles(TableBuilder& tb, const std::array<F, 2>* f, size_t nh, uint64_t offset, uint64_t rows,
-                          uint32_t first_tile, const F& scale) {
+                          uint32_t first_tile, const F& scale, size_t max_lb = 10) {
   qfd::TermTiles T;
-  const size_t lb = std::min<size_t>(10, nh);
+  const size_t lb = std::min<size_t>(std::min<size_t>(10, max_lb), nh);
   const size_t mb = std::min<size_t>(10, nh - lb);
   const uint64_t ntiles = (rows + (uint64_t(1) << lb) - 1) >> lb;
   T.offset = offset;
   T.rows = rows;
   T.first_tile = first_tile;
+  T.tile_skip = 0;
   T.lb = uint32_t(lb);
   T.mb = uint32_t(mb);
   T.lo_off = tb.add(f, lb, size_t(1) << lb, F::one());
@@ -590,7 +736,120 @@ uint64_t term_tile_count(const qfd::TermTiles& T) { return (T.rows + (uint64_t(1
 
 // Lane projections (tbv.rs:288-352) of large terms: one CTA per tile of up
 // to 1024 rows, tile weights from device-built factor tables.
+std::vector<std::vector<std::vector<F>>> GpuBackend::project_term_groups(
+    const std::vector<std::vector<const Term<F>*>>& groups, size_t stride) {
+  if (src_) return project_groups_streamed(groups, stride);
+  std::vector<std::vector<std::vector<F>>> out;
+  for (const auto& g : groups) out.push_back(project_terms(g, stride));
+  return out;
+}
+
+// Streamed weights: every group's tiles are cut at block boundaries (a term
+// is aligned to its power-of-two length, so it lies inside one block or
+// covers whole blocks, and tiles no longer than a block never straddle one);
+// each block's pieces run as its weights land, and the pieces of a term are
+// summed at the end.
+std::vector<std::vector<std::vector<F>>> GpuBackend::project_groups_streamed(
+    const std::vector<std::vector<const Term<F>*>>& groups, size_t stride) {
+  HostScope hs("project_terms");
+  const uint64_t bl = P_.block_len;
+  const size_t live = src_->live_blocks(), G = groups.size();
+  std::vector<std::vector<std::vector<F>>> out(G);
+  TableBuilder tb;
+  std::vector<size_t> lanes_of(G, 0);
+  // pieces[b][g]: launch-local tiles of block b for group g; term_of: each piece's term
+  std::vector<std::vector<std::vector<qfd::TermTiles>>> pieces(live, std::vector<std::vector<qfd::TermTiles>>(G));
+  std::vector<std::vector<std::vector<size_t>>> term_of(live, std::vector<std::vector<size_t>>(G));
+  std::vector<std::vector<uint64_t>> tiles_bg(live, std::vector<uint64_t>(G, 0));
+  for (size_t g = 0; g < G; ++g) {
+    out[g].resize(groups[g].size());
+    for (size_t t = 0; t < groups[g].size(); ++t) {
+      const Term<F>& term = *groups[g][t];
+      const size_t low_bits = std::min<size_t>(ilog2(stride), term.factors.size());
+      const size_t lanes = size_t(1) << low_bits;
+      out[g][t].assign(lanes, F::zero());
+      if (lanes_of[g] == 0) lanes_of[g] = lanes;
+      if (lanes != lanes_of[g]) fail(QF_E_ARGUMENT, "mixed lane widths");
+      check(lanes <= 64 && lanes <= bl, "at most 64 projection lanes");
+      if (term.offset >= active_ || term.scale.is_zero()) continue;
+      const size_t nh = term.factors.size() - low_bits;
+      const uint64_t rows = std::min<uint64_t>((active_ - term.offset + lanes - 1) / lanes, term.len() / lanes);
+      const qfd::TermTiles T = term_tiles(tb, term.factors.data() + low_bits, nh, term.offset, rows, 0, term.scale,
+                                          size_t(ilog2(bl / lanes)));
+      const uint64_t span = (uint64_t(1) << T.lb) * lanes, ntiles = term_tile_count(T);
+      check(term.offset % span == 0, "projection term alignment");
+      for (uint64_t i = 0; i < ntiles;) {
+        const uint64_t e0 = term.offset + i * span, b = e0 / bl;
+        check(b < live, "projection tile past the live blocks");
+        const uint64_t i1 = std::min<uint64_t>(ntiles, i + ((b + 1) * bl - e0) / span);
+        qfd::TermTiles piece = T;
+        piece.offset = term.offset - b * bl;  // modulo 2^64: the kernel adds the tile's rows back
+        piece.tile_skip = uint32_t(i);
+        piece.first_tile = uint32_t(tiles_bg[b][g]);
+        pieces[b][g].push_back(piece);
+        term_of[b][g].push_back(t);
+        tiles_bg[b][g] += i1 - i;
+        check(tiles_bg[b][g] < (uint64_t(1) << 31), "projection tile count");
+        i = i1;
+      }
+    }
+  }
+  DBuf<Fe> tables;
+  tb.build(s_, tables);
+  // One device array of all pieces, block-major then group; each group's tile
+  // outputs block-major too, so a piece's tiles are one segment.
+  std::vector<qfd::TermTiles> all;
+  std::vector<std::vector<size_t>> piece_at(live, std::vector<size_t>(G));
+  std::vector<std::vector<uint64_t>> tile_base(live, std::vector<uint64_t>(G));
+  std::vector<uint64_t> tiles_g(G, 0);
+  std::vector<std::vector<uint32_t>> seg(G, std::vector<uint32_t>(1, 0));
+  std::vector<std::vector<size_t>> seg_term(G);
+  for (size_t b = 0; b < live; ++b)
+    for (size_t g = 0; g < G; ++g) {
+      piece_at[b][g] = all.size();
+      tile_base[b][g] = tiles_g[g];
+      for (size_t k = 0; k < pieces[b][g].size(); ++k) {
+        all.push_back(pieces[b][g][k]);
+        const uint64_t end = k + 1 < pieces[b][g].size() ? pieces[b][g][k + 1].first_tile : tiles_bg[b][g];
+        seg[g].push_back(uint32_t(tiles_g[g] + end));
+        seg_term[g].push_back(term_of[b][g][k]);
+      }
+      tiles_g[g] += tiles_bg[b][g];
+    }
+  if (all.empty()) return out;
+  DBuf<qfd::TermTiles> dall(all.size());
+  QF_CK(cudaMemcpyAsync(dall.p, all.data(), all.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
+  std::vector<DBuf<Fe>> dtile(G);
+  for (size_t g = 0; g < G; ++g) dtile[g].alloc(std::max<uint64_t>(tiles_g[g] * lanes_of[g], 1));
+  src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+    for (size_t g = 0; g < G; ++g) {
+      const uint64_t tiles = tiles_bg[b][g];
+      if (!tiles) continue;
+      QF_LAUNCH(s_, "k_project_terms", n * sizeof(W),
+                qfd::k_project_terms<<<unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0, s_>>>(
+                    d, n, dall.p + piece_at[b][g], int(pieces[b][g].size()), uint32_t(tiles), tables.p, int(lanes_of[g]),
+                    dtile[g].p + tile_base[b][g] * lanes_of[g]));
+    }
+  });
+  for (size_t g = 0; g < G; ++g) {
+    const size_t np = seg_term[g].size();
+    if (!np) continue;
+    DBuf<uint32_t> dseg(seg[g].size());
+    DBuf<Fe> dpiece(np * lanes_of[g]);
+    QF_CK(cudaMemcpyAsync(dseg.p, seg[g].data(), seg[g].size() * 4, cudaMemcpyHostToDevice, s_));
+    QF_LAUNCH(s_, "k_sum_segments", tiles_g[g] * lanes_of[g] * 16,
+              qfd::k_sum_segments<<<unsigned(np), kThreads, 0, s_>>>(dtile[g].p, dseg.p, int(lanes_of[g]), dpiece.p));
+    std::vector<F> h(np * lanes_of[g]);
+    QF_CK(cudaMemcpyAsync(h.data(), dpiece.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaStreamSynchronize(s_));
+    for (size_t k = 0; k < np; ++k)
+      for (size_t l = 0; l < lanes_of[g]; ++l) out[g][seg_term[g][k]][l] += h[k * lanes_of[g] + l];
+  }
+  return out;
+}
+
 std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Term<F>*>& terms, size_t stride) {
+  if (src_) return project_groups_streamed({terms}, stride)[0];
   HostScope hs("project_terms");
   std::vector<std::vector<F>> out(terms.size());
   TableBuilder tb;
@@ -690,7 +949,21 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
   std::vector<F> pinv = consecutive_powers(inv, stride);
   DBuf<Fe> dp(stride);
   QF_CK(cudaMemcpyAsync(dp.p, pinv.data(), stride * 16, cudaMemcpyHostToDevice, s_));
-  QF_LAUNCH(s_, "k_eo_witness", std::min<uint64_t>(active_, rows * stride) * sizeof(W) + rows * 16, qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p));
+  if (src_) {
+    // Rows of each block as its weights land; rows past the live blocks are zero.
+    check(P_.block_len % stride == 0, "block length and EO stride");
+    const uint64_t rpb = P_.block_len / stride;
+    QF_CK(cudaMemsetAsync(wit_.p, 0, rows * 16, s_));
+    src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+      const uint64_t r0 = uint64_t(b) * rpb;
+      if (r0 >= rows) return;
+      const uint64_t rb = std::min(rpb, rows - r0);
+      QF_LAUNCH(s_, "k_eo_witness", n * sizeof(W) + rb * 16,
+                qfd::k_eo_witness<<<grid_for(rb, kThreads), kThreads, 0, s_>>>(d, n, rb, int(stride), dp.p, wit_.p + r0));
+    });
+  } else {
+    QF_LAUNCH(s_, "k_eo_witness", std::min<uint64_t>(active_, rows * stride) * sizeof(W) + rows * 16, qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p));
+  }
   // Query fold (tbv.rs:393-428): zero, then two disjoint passes of large-term
   // tiles, then the merged small-term contributions.
   QF_CK(cudaMemsetAsync(qv_.p, 0, rows * 16, s_));

@@ -4,6 +4,8 @@
 // data (BVA, codewords, Merkle trees, EO and sumcheck vectors) stays in HBM;
 // only transcript-sized values cross to the host.
 #pragma once
+#include <functional>
+
 #include "device/field_dev.cuh"
 #include "field_select.h"
 #include "gpu_common.cuh"
@@ -52,6 +54,43 @@ struct DeviceCodeword : CodewordView<F> {
   std::vector<F> entries() const override;
 };
 
+// Weights held in host memory (the caller's buffer; pinned memory lets the
+// copies run at full speed and ahead of the compute) and staged into HBM one
+// PCS block at a time for every pass that reads them: the reference's
+// recompute mode, for weight sets larger than HBM.  The first `resident`
+// blocks are copied on the first pass and stay in HBM; the others cycle
+// through `slots` staging buffers, copied on a side stream while earlier
+// blocks are processed.
+class BlockStream {
+ public:
+  BlockStream(const W* host, uint64_t active, uint64_t block_len, size_t resident, int slots);
+  ~BlockStream();
+  BlockStream(const BlockStream&) = delete;
+  BlockStream& operator=(const BlockStream&) = delete;
+  uint64_t active() const { return active_; }
+  uint64_t block_len() const { return block_len_; }
+  size_t live_blocks() const { return live_; }
+  size_t resident_blocks() const { return resident_; }
+  const W* host() const { return host_; }
+  uint64_t h2d_bytes() const { return copied_; }
+  // fn(b, d, n) for every live block b in order, with its launches on `s`: d
+  // is the device copy of entries [b * block_len, b * block_len + n).
+  using BlockFn = std::function<void(size_t b, const W* d, uint64_t n)>;
+  void for_each(cudaStream_t s, const BlockFn& fn);
+
+ private:
+  const W* host_;
+  uint64_t active_, block_len_;
+  size_t live_, resident_;
+  bool resident_ready_ = false;
+  DBuf<W> resident_buf_;
+  std::vector<DBuf<W>> slot_buf_;
+  std::vector<cudaEvent_t> landed_;  // per live block: its copy has landed
+  std::vector<cudaEvent_t> freed_;   // per slot: the compute on its last block is done
+  cudaStream_t copy_ = nullptr;
+  uint64_t copied_ = 0;
+};
+
 // Commitment root of block `b` of a device BVA (`active` entries), computed
 // only in the caller's device buffers: `cw` holds 2R x cols entries, `tree`
 // 4 x 2R words (2 x 2R digests), `alpha` R entries (overwritten with the
@@ -68,6 +107,12 @@ class GpuBackend : public Backend<F>,
  public:
   // `tables` (optional, not owned) shares uploaded code tables across backends.
   GpuBackend(const Parameters<F>& p, const W* d_bva, size_t active, cudaStream_t s, DeviceTables* tables = nullptr);
+  // Streamed weights (not owned): only block roots stay in HBM, and binding
+  // re-encodes every block.
+  GpuBackend(const Parameters<F>& p, BlockStream* src, cudaStream_t s, DeviceTables* tables = nullptr);
+  // Commits every block of a streamed backend in one pass over the weights;
+  // `per_block` runs after each live block's launches (same stream).
+  std::vector<Digest> commit_streamed(const BlockStream::BlockFn& per_block);
   ~GpuBackend() override;
 
   // commit
@@ -123,6 +168,10 @@ class GpuBackend : public Backend<F>,
 
   // Lane projections of arbitrary tensor terms (TBV claims and EO cross terms).
   std::vector<std::vector<F>> project_terms(const std::vector<const Term<F>*>& terms, size_t stride);
+  // The same for several groups of terms (each group with one lane width), in
+  // one pass over streamed weights.
+  std::vector<std::vector<std::vector<F>>> project_term_groups(const std::vector<std::vector<const Term<F>*>>& groups,
+                                                               size_t stride);
   // Raw window values of small terms.
   std::vector<W> windows(const std::vector<uint64_t>& starts, size_t stride);
 
@@ -140,11 +189,19 @@ class GpuBackend : public Backend<F>,
   LiteBullet<F> litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, PcsTranscript<F>& t, const char* label,
                                const char* fold_label, bool check_and_absorb);
   const Fe* level_alpha(size_t level, int which);
+  // Pack + Mobius + encode + hash of the block whose entries [src_base,
+  // src_base + 2^chunk) are read from `bva` (zero at or past `active`).
+  Digest encode_block(const W* bva, uint64_t active, uint64_t src_base, DeviceCodeword& cw);
+  DeviceCodeword& scratch_codeword();
+  std::vector<std::vector<std::vector<F>>> project_groups_streamed(const std::vector<std::vector<const Term<F>*>>& groups,
+                                                                   size_t stride);
   void mobius_rest(Fe* cw, int logm, int logR, int from);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
 
   const Parameters<F>& P_;
-  const W* bva_;
+  const W* bva_;              // resident weights, or null
+  BlockStream* src_ = nullptr;  // streamed weights, or null
+  std::unique_ptr<DeviceCodeword> scratch_;  // re-encoded block of a streamed backend
   size_t active_;
   cudaStream_t s_;
   std::vector<std::unique_ptr<DeviceCodeword>> blocks_;

@@ -97,6 +97,7 @@ __global__ void k_factor_tables(const TableSpec* __restrict__ specs, int n_specs
 struct TermTiles {
   uint64_t offset, rows;
   uint32_t first_tile;
+  uint32_t tile_skip;  // the term's tiles before the first one of this list entry (0 unless a term is split)
   uint32_t lo_off, mid_off, top_off;
   uint32_t lb, mb;
 };
@@ -169,7 +170,7 @@ __global__ void k_query_terms(const TermTiles* __restrict__ terms, int n_terms, 
   for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
     while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
     const TermTiles T = terms[ti];
-    const uint64_t i = tile - T.first_tile;
+    const uint64_t i = tile - T.first_tile + T.tile_skip;
     const uint64_t row0 = i << T.lb;
     const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
     const uint32_t nrows = uint32_t(left < span ? left : span);

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __
   for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
     while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
     const TermTiles T = terms[ti];
-    const uint64_t i = tile - T.first_tile;
+    const uint64_t i = tile - T.first_tile + T.tile_skip;
     const uint64_t row0 = i << T.lb;
     const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
     const int nrows = int(left < span ? left : span);
@@ -250,15 +250,15 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
     atomicAdd(raw + t, (unsigned long long)tot_s[t >> 6][t & 63]);  // two's complement sum
 }
 
-// values[i] = sum_b fold[b] * packed(b, i) = sum_{b,j} v(b, 8i+j) * T[b][j],
-// with T[b][j] = fold[b] * X^j precomputed (packed_batch.rs:213-222).
 // Block fold of the packed weights (packed_batch.rs:213-236):
 // values[i] = sum_b sum_j v(b * block_len + 8i + j) * T[b * 8 + j], T[b * 8 + j] =
-// (c^-1)^b * X^j.  Each block's T rows are held as byte planes in shared
-// memory; a block contributes two dp4a per byte plane and coefficient.  Sums
-// of 8 blocks stay below 8 * 8 * 128 * 65520 < 2^31 and move to i64 totals.
+// (c^-1)^b * X^j; with `accumulate` the sum is added to values[i] (blocks
+// folded one launch at a time).  Each block's T rows are held as byte planes
+// in shared memory; a block contributes two dp4a per byte plane and
+// coefficient.  Sums of 8 blocks stay below 8 * 8 * 128 * 65520 < 2^31 and
+// move to i64 totals.
 __global__ void k_block_fold(const int8_t* __restrict__ bva, uint64_t active, uint64_t block_len, int blocks, uint64_t m,
-                             const Fe* __restrict__ T, Fe* __restrict__ values) {
+                             const Fe* __restrict__ T, Fe* __restrict__ values, int accumulate) {
   extern __shared__ uint4 smem_u4[];
   // planes[b][k] = {lo(j 0..3), lo(j 4..7), hi(j 0..3), hi(j 4..7)}
   uint4* planes = smem_u4;
@@ -299,7 +299,7 @@ __global__ void k_block_fold(const int8_t* __restrict__ bva, uint64_t active, ui
     Fr o;
 #pragma unroll
     for (int k = 0; k < 8; ++k) o.c[k] = blocks > 8 ? mod_i64(tot[k] + acc[k]) : mod_i32(acc[k]);
-    store(values + i, o);
+    store(values + i, accumulate ? add(load(values + i), o) : o);
   }
 }
 

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __rest
   for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
     while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
     const TermTiles T = terms[ti];
-    const uint64_t i = tile - T.first_tile;
+    const uint64_t i = tile - T.first_tile + T.tile_skip;
     const uint64_t row0 = i << T.lb;
     const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
     const int nrows = int(left < span ? left : span);
@@ -225,10 +225,10 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const Wt* _
 
 // Block fold of the packed payloads (packed_batch.rs:213-236): values[i] =
 // sum_b sum_j v(b * block_len + 4i + j) * T[b * 4 + j], T[b * 4 + j] =
-// (c^-1)^b * X^j, held in shared memory.  At most 128 blocks: a sum of 512
-// products stays below 2^55.
+// (c^-1)^b * X^j, held in shared memory; with `accumulate` the sum is added
+// to values[i].  At most 128 blocks: a sum of 512 products stays below 2^55.
 __global__ void k_block_fold(const Wt* __restrict__ bva, uint64_t active, uint64_t block_len, int blocks, uint64_t m,
-                             const Fe* __restrict__ T, Fe* __restrict__ values) {
+                             const Fe* __restrict__ T, Fe* __restrict__ values, int accumulate) {
   extern __shared__ uint4 smem_u4[];
   Fe* t_s = reinterpret_cast<Fe*>(smem_u4);
   for (int t = threadIdx.x; t < blocks * kC; t += blockDim.x) t_s[t] = T[t];
@@ -252,7 +252,7 @@ __global__ void k_block_fold(const Wt* __restrict__ bva, uint64_t active, uint64
     Fr o;
 #pragma unroll
     for (int k = 0; k < kC; ++k) o.c[k] = mod_i64(acc[k]);
-    store(values + i, o);
+    store(values + i, accumulate ? add(load(values + i), o) : o);
   }
 }
 

@@ -166,3 +166,77 @@ def test_koalabear_nonzero_padding_rejected():
     bva[b.offset + b.physical_cols] = 1
     with pytest.raises(qf.QfError, match="nonzero boundary padding"):
         p.commit(bva)
+
+
+# ---------------------------------------------------------------- recompute mode over streamed host weights
+def run_streamed(shapes, chunk_log, packed_log, mats, field="f65521", resident_bytes=0, pinned=False):
+    """commit_recomputed: the weights stay in host memory and every pass
+    streams them block by block; the bytes must equal the oracle's."""
+    import torch
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=packed_log), field=FIELDS[field])
+    bva = layout.encode(p.shapes, mats)
+    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, packed_log, bva, field=field)
+    host = torch.from_numpy(bva).pin_memory() if pinned else bva
+    c = p.commit_recomputed(host, resident_bytes=resident_bytes)
+    assert b"".join(c.roots) == o_roots, "commitment roots differ"
+    claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
+    assert qf.claims_to_bytes(claims) == o_claims, "claims differ"
+    proof, _ = p.prove(c, claims)
+    assert proof.to_bytes() == o_proof, "proof bytes differ"
+    p.verify(c.roots, claims, proof)
+    c.close()
+    return proof
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_streamed_demo_bundle_matches_reference_digest(vectors, field):
+    shapes = qf.demo_shapes()
+    dt = np.int16 if field == "koalabear" else np.int8
+    proof = run_streamed(shapes, 10, 4, layout.demo_matrices(shapes, dtype=dt), field=field)
+    assert blake2s(proof.to_bytes()) == vectors[f"{field}_demo"]["proof_blake2s"]
+
+
+@pytest.mark.parametrize("field,packed_log,resident,pinned", [
+    ("f65521", 4, 0, True), ("f65521", 6, 3, False), ("koalabear", 4, 0, False), ("koalabear", 6, 2, True)])
+def test_streamed_ragged_shapes_many_blocks(field, packed_log, resident, pinned):
+    rng = np.random.default_rng(100 + packed_log + resident)
+    shapes = [(300, 700), (129, 65), (1, 5000), (77, 1)]
+    gen = gaussian_i16 if field == "koalabear" else gaussian_i8
+    mats = [gen(rng, r * c, forced=0.001).reshape(r, c) for r, c in shapes]
+    w = 2 if field == "koalabear" else 1
+    run_streamed(shapes, 14, packed_log, mats, field=field, resident_bytes=resident * (1 << 14) * w, pinned=pinned)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_streamed_terms_spanning_blocks_and_zero_suffix(field):
+    """A 2^20-entry bucket spans 16 blocks of 2^16; 15 of 32 blocks are the zero suffix."""
+    rng = np.random.default_rng(17)
+    shapes = [(1024, 1024), (1, 16)]
+    gen = gaussian_i16 if field == "koalabear" else gaussian_i8
+    mats = [gen(rng, r * c).reshape(r, c) for r, c in shapes]
+    run_streamed(shapes, 16, 4, mats, field=field, resident_bytes=0, pinned=True)
+
+
+def test_streamed_matches_resident_commit_smoke_config():
+    rng = np.random.default_rng(0)
+    mats = [gaussian_i8(rng, 1024 * 4096).reshape(1024, 4096)]
+    p = qf.Parameters([(1024, 4096)], qf.Config(chunk_log=20, packed_log=4))
+    bva = layout.encode(p.shapes, mats)
+    a = p.commit(bva)
+    b = p.commit_recomputed(bva, resident_bytes=1 << 20)
+    assert a.roots == b.roots
+    claims = p.evaluate_claims(a, p.benchmark_points(a.roots))
+    assert qf.claims_to_bytes(p.evaluate_claims(b, p.benchmark_points(b.roots))) == qf.claims_to_bytes(claims)
+    pa, _ = p.prove(a, claims)
+    pb, _ = p.prove(b, claims)
+    assert pa.to_bytes() == pb.to_bytes()
+
+
+def test_streamed_nonzero_padding_rejected():
+    p = qf.Parameters([(31, 31), (40, 40)], qf.Config(chunk_log=10, packed_log=4))
+    bva = layout.encode(p.shapes, [np.ones((31, 31), np.int8), np.ones((40, 40), np.int8)])
+    bs, _, _ = layout.buckets(p.shapes)
+    b = next(b for b in bs if b.cols > b.physical_cols)
+    bva[b.offset + b.physical_cols] = 1
+    with pytest.raises(qf.QfError, match="nonzero boundary padding"):
+        p.commit_recomputed(bva)
