@@ -6,7 +6,12 @@ reference's proof bytes.  `--workload 8b8` (the default): int8 round(N(0,
 20^2)) clipped to +-127 with 0.1% of entries forced to +-127, F65521^8,
 chunk_log 30, packed_log 4.  `--workload 8b16`: the raw 16-bit payloads of
 BF16 values drawn from N(0, 0.02^2) (the embedding from N(0, 1)),
-KoalaBear^4, chunk_log 30, packed_log 4.  As in the reference
+KoalaBear^4, chunk_log 30, packed_log 4.  `--workload 70b16`: the 562 shapes
+of the 70B set, BF16 payloads from N(0, 0.02^2) (141 GB), KoalaBear^4,
+chunk_log 30, packed_log 6; the weights exceed HBM, so they stay in pinned
+host memory and every pass streams them (the recompute mode,
+Parameters.commit_recomputed), `--resident-gb` of leading blocks staying in
+HBM after the first pass.  As in the reference
 prover timer (main.rs:176-210) a step is commit + prove + serialisation;
 setup and claim generation are outside it.  The claims are computed once
 (their points derive from the committed roots, identical every step).
@@ -41,6 +46,47 @@ def shapes_8b():
     for _ in range(32):
         s += [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096), (14336, 4096), (14336, 4096), (4096, 14336)]
     return [(128256, 4096)] + s + [(128256, 4096)]
+
+
+def shapes_70b():
+    s = []
+    for _ in range(80):
+        s += [(8192, 8192), (1024, 8192), (1024, 8192), (8192, 8192), (28672, 8192), (28672, 8192), (8192, 28672)]
+    return [(128256, 8192)] + s + [(128256, 8192)]
+
+
+def make_bva_on_host(shapes, seed: int = 0, sigma: float = 0.02):
+    """BF16 payloads of N(0, sigma^2) laid out as the BVA in pinned host memory,
+    generated on the GPU one matrix at a time."""
+    import torch
+    from parcomm_b200 import layout
+
+    buckets, active, _ = layout.buckets(shapes)
+    # Page-locked by registration: torch's pinned allocator rounds a request up
+    # to a power of two, which 141 GB does not survive.
+    out = torch.empty(active, dtype=torch.int16)
+    pinned = int(torch.cuda.cudart().cudaHostRegister(out.data_ptr(), out.numel() * 2, 0)) == 0
+    by_matrix = {}
+    for b in buckets:
+        by_matrix.setdefault(b.matrix, []).append(b)
+    covered = 0
+    g = torch.Generator(device="cuda")
+    for m, (rows, cols) in enumerate(shapes):
+        g.manual_seed(seed * 100003 + m)
+        w = torch.randn(rows * cols, generator=g, device="cuda", dtype=torch.float32)
+        w = w.mul_(sigma).to(torch.bfloat16).view(torch.int16).view(rows, cols)
+        for b in by_matrix[m]:
+            blk = torch.zeros(b.rows, b.cols, dtype=torch.int16, device="cuda")
+            blk[: b.physical_rows, : b.physical_cols] = w[b.row_offset: b.row_offset + b.physical_rows,
+                                                         b.col_offset: b.col_offset + b.physical_cols]
+            out[b.offset: b.offset + b.rows * b.cols].copy_(blk.view(-1))
+            covered += b.rows * b.cols
+            del blk
+        del w
+    assert covered == active
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return out, active, pinned
 
 
 def make_bva_on_device(shapes, seed: int = 0, bf16: bool = False, embedding_first: bool = False):
@@ -164,6 +210,25 @@ def max_over_ranks(ms: float, world: int, device: str = "cuda") -> float:
     return float(t.item())
 
 
+def measure_h2d_gbs(nbytes: int = 1 << 31, reps: int = 3) -> float:
+    """Pinned host -> device copy bandwidth (best of `reps` copies of 2 GiB),
+    the bound of a workload streamed from host memory."""
+    import torch
+    src = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    dst = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    best = 0.0
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dst.copy_(src, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, nbytes / (e0.elapsed_time(e1) / 1000.0) / 1e9)
+    del src, dst
+    torch.cuda.empty_cache()
+    return best
+
+
 def job_throughput(weights_per_rank: int, world: int, ms_per_step: float) -> float:
     """Whole-job weights/s: every rank proves its own model of `weights_per_rank`."""
     return weights_per_rank * world / (ms_per_step / 1000.0)
@@ -213,8 +278,11 @@ def run_reference(args):
     # One decoder layer's attention projections (4 matrices, 41.9M weights),
     # chunk_log 24 so the sample keeps the batched multi-block opening.
     shapes = [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096)]
-    sixteen = args.workload in ("8b16", "layers16")
+    sixteen = args.workload in ("8b16", "layers16", "70b16")
     field = "koalabear" if sixteen else "f65521"
+    packed_log = 6 if args.workload == "70b16" else 4
+    if args.workload == "70b16":  # one 70B decoder layer's attention projections
+        shapes = [(8192, 8192), (1024, 8192), (1024, 8192)]
     rng = np.random.default_rng(0)
     mats = []
     for r, c in shapes:
@@ -235,22 +303,25 @@ def run_reference(args):
     times = []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, 24, 4, bva, field=field)
+        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, 24, packed_log, bva, field=field)
         dt = time.perf_counter() - t0
         if step >= args.warmup:
             times.append((commit_ms + open_ms) / 1000.0)
     sec = statistics.mean(times)
     value = weights / sec
-    sample = (f"4 matrices of one 8B decoder layer (q,k,v,o: {weights} "
-              f"{'BF16 payloads' if sixteen else 'int8 weights'}), chunk_log 24, packed_log 4, "
+    layer = "3 matrices of one 70B decoder layer (q,k,v" if args.workload == "70b16" else \
+        "4 matrices of one 8B decoder layer (q,k,v,o"
+    sample = (f"{layer}: {weights} "
+              f"{'BF16 payloads' if sixteen else 'int8 weights'}), chunk_log 24, packed_log {packed_log}, "
               f"C++ restatement of the reference CPU prover (OpenMP, {threads} threads)")
     line = {
         "impl": "reference", "metric": "QAFold commit+open weights/s", "value": value, "unit": "weights/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16" if sixteen else "int8",
-        "data": "synthetic", "config": {"workload": f"8B-shape {16 if sixteen else 8}-bit weights, batched (sample)",
+        "data": "synthetic", "config": {"workload": ("70B-shape 16-bit weights, streamed (sample)" if args.workload == "70b16"
+                                                     else f"8B-shape {16 if sixteen else 8}-bit weights, batched (sample)"),
                                         "field": "KoalaBear^4" if sixteen else "F65521^8",
-                                        "chunk_log": 24, "packed_log": 4, "sample": sample},
+                                        "chunk_log": 24, "packed_log": packed_log, "sample": sample},
         "cpu_baseline": {"value": value, "unit": "weights/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "weights/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -263,11 +334,15 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="8b8", choices=["8b8", "8b16", "layers", "layers16", "smoke"],
+    ap.add_argument("--workload", default="8b8",
+                    choices=["8b8", "8b16", "70b16", "layers", "layers16", "layers70", "smoke"],
                     help="8b8 / 8b16: the 8B shape set with 8-bit weights (F65521^8) or 16-bit BF16 "
                          "payloads (KoalaBear^4); layers / layers16: the first --layers transformer layers "
                          "(7 matrices each) at --chunk-log, a small case for profiling")
     ap.add_argument("--layers", type=int, default=2)
+    ap.add_argument("--resident-gb", type=float, default=None,
+                    help="70b16 / layers70: GB of leading weight blocks kept in HBM after the first streamed pass "
+                         "(default: what free HBM allows next to the proof's own peak)")
     ap.add_argument("--chunk-log", type=int, default=28)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-matrix", action="store_true",
@@ -294,11 +369,18 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    sixteen = args.workload in ("8b16", "layers16")
+    sixteen = args.workload in ("8b16", "layers16", "70b16", "layers70")
+    streamed = args.workload in ("70b16", "layers70")
     field = qf.FIELD_KOALABEAR if sixteen else qf.FIELD_F65521
     bits = 16 if sixteen else 8
     if args.workload in ("8b8", "8b16"):
         shapes, cfg, name = shapes_8b(), qf.Config(30, 4), f"8B-shape {bits}-bit weights, batched (226 matrices)"
+    elif args.workload == "70b16":
+        shapes, cfg = shapes_70b(), qf.Config(30, 6)
+        name = "70B-shape 16-bit weights, streamed from pinned host memory (562 matrices)"
+    elif args.workload == "layers70":
+        shapes, cfg = shapes_70b()[1:1 + 7 * args.layers], qf.Config(args.chunk_log, 6)
+        name = f"70B-shape 16-bit weights, first {args.layers} layers, chunk 2^{args.chunk_log}, streamed"
     elif args.workload in ("layers", "layers16"):
         shapes = shapes_8b()[1:1 + 7 * args.layers]
         cfg = qf.Config(args.chunk_log, 4)
@@ -310,12 +392,27 @@ def main():
     t0 = time.time()
     params = qf.Parameters(shapes, cfg, field=field)
     setup_s = time.time() - t0
-    bva_dev, active = make_bva_on_device(shapes, seed=rank, bf16=sixteen, embedding_first=args.workload == "8b16")
-    bva_host = torch.empty(active, dtype=bva_dev.dtype, pin_memory=True)
-    bva_host.copy_(bva_dev)
+    t0 = time.time()
+    host_pinned = True
+    if streamed:
+        bva_host, active, host_pinned = make_bva_on_host(shapes, seed=rank)
+        bva_dev = None
+        resident = None if args.resident_gb is None else int(args.resident_gb * 1e9)
+
+        def commit(on_device: bool):
+            return params.commit_recomputed(bva_host, resident_bytes=resident)
+    else:
+        bva_dev, active = make_bva_on_device(shapes, seed=rank, bf16=sixteen, embedding_first=args.workload == "8b16")
+        bva_host = torch.empty(active, dtype=bva_dev.dtype, pin_memory=True)
+        bva_host.copy_(bva_dev)
+
+        def commit(on_device: bool):
+            return params.commit(bva_dev if on_device else bva_host, on_device=on_device)
+    entry_bytes = bva_host.element_size()
+    input_s = time.time() - t0
 
     # Claims once: their points derive from the (step-invariant) roots.
-    c = params.commit(bva_dev, on_device=True)
+    c = commit(True)
     claims = params.evaluate_claims(c, params.benchmark_points(c.roots))
     proof, prof = params.prove(c, claims)
     c.close()
@@ -326,11 +423,17 @@ def main():
         verify_s = time.time() - t0
     proof_bytes = len(proof.to_bytes())
 
+    res_blocks = [0, 0]
+
     def step(on_device: bool):
-        cc = params.commit(bva_dev if on_device else bva_host, on_device=on_device)
+        cc = commit(on_device)
         pr, pf = params.prove(cc, claims)
+        if streamed:
+            h2d, res_blocks[0], res_blocks[1] = cc.stream_info()
+        else:
+            h2d = 0 if on_device else active * entry_bytes
         cc.close()
-        return pr, pf
+        return pr, pf, h2d
 
     for _ in range(max(args.warmup - 1, 0)):
         step(True)
@@ -356,8 +459,11 @@ def main():
     out_dir = Path(args.out)
     out_dir.mkdir(exist_ok=True)
     with ClockSampler(out_dir / "bench_clocks.csv") as clocks:
-        ms_dev, (pr_dev, pf_dev), launches = timed(True, args.steps)
-    ms_e2e, (pr_e2e, pf_e2e), _ = timed(False, max(1, args.steps))
+        ms_dev, (pr_dev, pf_dev, h2d_dev), launches = timed(True, args.steps)
+    if streamed:  # the weights only exist in host memory: the timed run is already end to end
+        ms_e2e, pr_e2e, h2d_e2e = ms_dev, pr_dev, h2d_dev
+    else:
+        ms_e2e, (pr_e2e, pf_e2e, h2d_e2e), _ = timed(False, max(1, args.steps))
     assert pr_dev.to_bytes() == proof.to_bytes() == pr_e2e.to_bytes(), "proof bytes changed between steps"
 
     # Per-kernel device time (CUDA events on each launch's own stream), one extra step.
@@ -373,6 +479,14 @@ def main():
     achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
     traffic = ncu_traffic(dominant, d["bytes"] / d["launches"])
+
+    link = None
+    if streamed:  # the host link bounds a streamed step: bytes copied per step against a measured copy
+        h2d_peak = measure_h2d_gbs()
+        h2d_achieved = h2d_dev / (ms_dev / 1000.0) / 1e9
+        link = {"bound": "h2d", "achieved": h2d_achieved, "peak": h2d_peak, "unit": "GB/s",
+                "frac": h2d_achieved / h2d_peak, "bytes_per_step": h2d_dev,
+                "peak_source": "pinned 2 GiB host->device copy, best of 3, measured in this run"}
 
     per_matrix = None
     if not args.no_per_matrix and args.workload in ("8b8", "8b16"):
@@ -415,15 +529,20 @@ def main():
         "data": "synthetic",
         "config": {"workload": name, "field": "KoalaBear^4" if sixteen else "F65521^8", "chunk_log": cfg.chunk_log,
                    "packed_log": cfg.packed_log, "weights": weights, "active_entries": active, "pcs_blocks": params.blocks,
-                   "l2": "inputs larger than L2 (BVA of 8 or 16 GB, 4 or 8 GiB codeword per block)",
+                   "l2": "inputs larger than L2 (BVA of 8 to 141 GB, 4 or 8 GiB codeword per block)",
+                   "weights_in": (("pinned" if host_pinned else "pageable") + " host memory, streamed per pass, "
+                                  + (f"{args.resident_gb} GB of blocks resident" if args.resident_gb is not None
+                                     else f"{res_blocks[0]} of {res_blocks[1]} live blocks resident (auto)")
+                                  if streamed else "HBM (value); pinned host memory (e2e)"),
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": {"value": job_throughput(weights, world, ms_e2e), "unit": "weights/s",
-                "h2d_bytes_per_step": active * bva_dev.element_size(), "d2h_bytes_per_step": proof_bytes},
+                "h2d_bytes_per_step": h2d_e2e, "d2h_bytes_per_step": proof_bytes},
         "gpu_launches": launches // max(args.steps, 1),
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "kernel_ms_per_step": d["ms"], "kernel_launches": d["launches"],
                      "alg_bytes_per_launch": d["bytes"] / max(d["launches"], 1)},
+        "link_roofline": link,
         "cpu_baseline": cpu_baseline,
         "per_matrix": per_matrix,
         "clocks": clocks.summary(local),
@@ -431,6 +550,7 @@ def main():
         "stage_ms": {k: getattr(pf_dev, k) for k in ("commit_ms", "eo_ms", "projection_ms", "folding_ms", "sumcheck_ms",
                                                      "binding_ms", "native_opening_ms", "decide_ms", "open_ms")},
         "setup_s": setup_s,
+        "input_s": input_s,
         "verify_s": verify_s,
     }
     (out_dir / "bench_kernels.json").write_text(json.dumps(stats, indent=1))

@@ -79,10 +79,19 @@ void qf_committed_free(qf_committed* committed);
  * weights (commit, EO cross terms and witness, projection, block fold) stages
  * them into HBM one PCS block at a time, and binding re-encodes each block
  * and checks its root.  The first resident_bytes / (2^chunk_log * entry size)
- * blocks are kept in HBM after the first pass.  Needs at least two PCS
- * blocks.  Writes the same roots, claims and proof bytes as qf_commit. */
+ * blocks are kept in HBM after the first pass; QF_RESIDENT_AUTO sizes that
+ * from the device's free memory less the proof's own peak.  Needs at least
+ * two PCS blocks.  Writes the same roots, claims and proof bytes as
+ * qf_commit. */
+#define QF_RESIDENT_AUTO UINT64_MAX
 int qf_commit_streamed(const qf_params* params, const void* host_bva, uint64_t n_values, uint64_t resident_bytes,
                        qf_committed** out, uint8_t* roots_out);
+/* For a qf_commit_streamed handle: bytes of weights copied host->device so
+ * far, and the PCS blocks kept in HBM out of the blocks holding weights (all
+ * 0 for qf_commit handles).  Any output pointer may be NULL.  No reference
+ * counterpart. */
+int qf_committed_stream_info(const qf_committed* committed, uint64_t* h2d_bytes, uint64_t* resident_blocks,
+                             uint64_t* live_blocks);
 
 /* serde_json of the Commitment statement (protocol.rs:33-40), as absorbed. */
 int qf_statement_json(const qf_params* params, const uint8_t* roots, char* buf, size_t cap, size_t* len);

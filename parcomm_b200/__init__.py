@@ -23,6 +23,7 @@ LIB_PATH = _PKG / "_lib" / "libparcomm_qafold.so"
 
 FIELD_F65521 = 1
 FIELD_KOALABEAR = 2
+RESIDENT_AUTO = (1 << 64) - 1  # QF_RESIDENT_AUTO
 ERRORS = {
     -1: "EncodingError", -2: "HashingError", -3: "InvalidCommitment", -4: "InvalidNumberOfVariables",
     -5: "InvalidParameters", -6: "TranscriptError", -7: "ProtocolError", -8: "CudaError", -9: "ArgumentError",
@@ -59,6 +60,7 @@ EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
     "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
+    "qf_committed_stream_info",
 )
 
 
@@ -78,6 +80,7 @@ def lib() -> ctypes.CDLL:
                                      ctypes.POINTER(U64), ctypes.c_char_p]
         L.qf_commit.argtypes = [P, P, U64, ctypes.c_int, ctypes.POINTER(P), ctypes.c_char_p]
         L.qf_commit_streamed.argtypes = [P, P, U64, U64, ctypes.POINTER(P), ctypes.c_char_p]
+        L.qf_committed_stream_info.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64), ctypes.POINTER(U64)]
         L.qf_committed_free.argtypes = [P]
         L.qf_committed_free.restype = None
         L.qf_statement_json.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.POINTER(S)]
@@ -192,6 +195,16 @@ class Committed:
     def statement(self) -> "Commitment":
         return Commitment(self.params, list(self.roots))
 
+    def stream_info(self) -> Tuple[int, int, int]:
+        """Recompute mode: (host->device bytes of weights copied so far,
+        blocks kept in HBM, blocks holding weights)."""
+        v = [ctypes.c_uint64() for _ in range(3)]
+        _check(lib().qf_committed_stream_info(self._h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def stream_bytes(self) -> int:
+        return self.stream_info()[0]
+
     def close(self) -> None:
         if self._h:
             lib().qf_committed_free(self._h)
@@ -275,14 +288,16 @@ class Parameters:
         _check(lib().qf_commit(self._h, ctypes.c_void_p(ptr), n, int(on_device), ctypes.byref(h), roots))
         return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)])
 
-    def commit_recomputed(self, values, resident_bytes: int = 0) -> Committed:
+    def commit_recomputed(self, values, resident_bytes: Optional[int] = 0) -> Committed:
         """Parameters::commit_recomputed: the reference's recompute mode.  Host
         weights (a numpy array, or a CPU tensor, ideally in pinned memory) stay
         where they are and are streamed into HBM one PCS block at a time for
         every pass; only the roots stay on the device and binding re-encodes
         each block.  `resident_bytes` of leading blocks are kept in HBM after
-        the first pass.  Device tensors take the cached path (`commit`).  The
-        roots, claims and proof bytes equal those of `commit`."""
+        the first pass (None: as many as the device's free memory allows next
+        to the proof's own peak).  Device tensors take the cached path
+        (`commit`).  The roots, claims and proof bytes equal those of
+        `commit`."""
         if hasattr(values, "is_cuda") and values.is_cuda:
             return self.commit(values, on_device=True)
         if hasattr(values, "data_ptr"):
@@ -294,7 +309,8 @@ class Parameters:
             ptr, n = keep.ctypes.data, keep.size
         h = ctypes.c_void_p()
         roots = ctypes.create_string_buffer(32 * max(self.blocks, 1))
-        _check(lib().qf_commit_streamed(self._h, ctypes.c_void_p(ptr), n, int(resident_bytes), ctypes.byref(h), roots))
+        budget = RESIDENT_AUTO if resident_bytes is None else int(resident_bytes)
+        _check(lib().qf_commit_streamed(self._h, ctypes.c_void_p(ptr), n, budget, ctypes.byref(h), roots))
         return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)], keep=keep)
 
     def block_root_noalloc(self, bva, block: int, root, stream: int = 0) -> None:

@@ -88,6 +88,19 @@ int qf_commit_streamed(const qf_params* params, const void* host_bva, uint64_t n
 
 void qf_committed_free(qf_committed* committed) { delete committed; }
 
+int qf_committed_stream_info(const qf_committed* committed, uint64_t* h2d_bytes, uint64_t* resident_blocks,
+                             uint64_t* live_blocks) {
+  return guarded([&] {
+    if (!committed) fail(QF_E_ARGUMENT, "null argument");
+    if (committed->state) {
+      api(committed->params->field).stream_info(committed, h2d_bytes, resident_blocks, live_blocks);
+    } else {
+      for (uint64_t* p : {h2d_bytes, resident_blocks, live_blocks})
+        if (p) *p = 0;
+    }
+  });
+}
+
 int qf_statement_json(const qf_params* params, const uint8_t* roots, char* buf, size_t cap, size_t* len) {
   return guarded([&] {
     if (!params || !roots) fail(QF_E_ARGUMENT, "null argument");

@@ -245,6 +245,23 @@ void commit(const qf_params* params, const void* bva, uint64_t n_values, int bva
     out->state = std::move(c);
 }
 
+// HBM for resident weight blocks.  QF_RESIDENT_AUTO takes what the device
+// has free now (the pool's cache included) less the proof's own peak: the EO round vectors (2.5 x
+// N/stride elements) or the batch opening's tables and codewords (about 7.5 x
+// packed_len elements), whichever is larger, plus the staging slots and 4 GiB.
+static uint64_t resident_budget(const Parameters<F>& P, uint64_t requested) {
+  if (requested != QF_RESIDENT_AUTO) return requested;
+  // Blocks cached by the pool count as free: a repeated proof of the same
+  // shapes finds its buffers there, and a short allocation trims the cache.
+  size_t free_b = 0, total_b = 0;
+  QF_CK(cudaMemGetInfo(&free_b, &total_b));
+  free_b += DevicePool::cached_bytes();
+  const uint64_t el = 16, m = P.pcs.packed_len(), rows = P.layout.logical >> P.config.packed_log;
+  const uint64_t eo = rows * el * 5 / 2, opening = m * el * 15 / 2;
+  const uint64_t need = std::max(eo, opening) + 3 * P.block_len * sizeof(W) + (uint64_t(4) << 30);
+  return free_b > need ? free_b - need : 0;
+}
+
 // Recompute mode over weights that stay in host memory (`host` must outlive
 // the committed handle): one streamed pass commits every block and checks
 // the padding; the first `resident_bytes` worth of blocks stay in HBM.
@@ -256,7 +273,7 @@ void commit_streamed(const qf_params* params, const void* host, uint64_t n_value
   c->active = n_values;
   QF_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   auto t0 = std::chrono::steady_clock::now();
-  const size_t resident = size_t(resident_bytes / (P.block_len * sizeof(W)));
+  const size_t resident = size_t(resident_budget(P, resident_bytes) / (P.block_len * sizeof(W)));
   c->src = std::make_unique<BlockStream>(static_cast<const W*>(host), n_values, P.block_len, resident, 3);
   c->be = std::make_unique<GpuBackend>(P, c->src.get(), c->stream, static_cast<DeviceTables*>(params->tables.get()));
   // Padding segments of every live block, relative to the block, uploaded once.
@@ -355,9 +372,17 @@ void verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims
     verify_proof(P, make_statement(P, roots_from(params, roots)), cl, pr);
 }
 
+
+void stream_info(const qf_committed* committed, uint64_t* h2d_bytes, uint64_t* resident_blocks, uint64_t* live_blocks) {
+  const auto* fc = static_cast<const FieldCommitted*>(committed->state.get());
+  if (h2d_bytes) *h2d_bytes = fc->src ? fc->src->h2d_bytes() : 0;
+  if (resident_blocks) *resident_blocks = fc->src ? fc->src->resident_blocks() : 0;
+  if (live_blocks) *live_blocks = fc->src ? fc->src->live_blocks() : 0;
+}
+
 }  // namespace
 
 const qfc::FieldApi kFieldApi = {sizeof(W), make_params, info, commit, commit_streamed, statement_json,
-                                 benchmark_points_bytes, eval_claims, prove, verify};
+                                 benchmark_points_bytes, eval_claims, prove, verify, stream_info};
 
 }  // namespace QFB_NS

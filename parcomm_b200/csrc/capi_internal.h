@@ -50,6 +50,8 @@ struct FieldApi {
   std::vector<uint8_t> (*prove)(const qf_params* p, qf_committed* c, const uint8_t* claims, size_t len, qf_profile* profile);
   void (*verify)(const qf_params* p, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,
                  size_t proof_len);
+  // Streamed weights: host->device bytes copied so far, resident and live blocks.
+  void (*stream_info)(const qf_committed* c, uint64_t* h2d_bytes, uint64_t* resident_blocks, uint64_t* live_blocks);
 };
 
 inline thread_local std::string g_last_error;

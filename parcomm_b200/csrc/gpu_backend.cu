@@ -165,7 +165,8 @@ void BlockStream::for_each(cudaStream_t s, const BlockFn& fn) {
   };
   // Block j goes to its resident place or to slot (j - resident) % K, whose
   // previous block is j - K: the copy waits until that block's launches are
-  // done.  Copies run up to K blocks ahead of the compute position.
+  // done.  Copies run up to K blocks ahead of the compute position, and the
+  // first K streamed blocks are copied while the resident ones are processed.
   auto issue = [&](size_t j) {
     if (j < resident_ && resident_ready_) return;
     if (j >= resident_) QF_CK(cudaStreamWaitEvent(copy_, freed_[(j - resident_) % K], 0));
@@ -177,7 +178,8 @@ void BlockStream::for_each(cudaStream_t s, const BlockFn& fn) {
   const size_t ahead = std::max<size_t>(K, 1);
   size_t issued = 0;
   for (size_t i = 0; i < live_; ++i) {
-    while (issued < live_ && issued < i + ahead) issue(issued++);
+    const size_t horizon = (resident_ready_ ? std::max(i, resident_) : i) + ahead;
+    while (issued < live_ && issued < horizon) issue(issued++);
     if (!(i < resident_ && resident_ready_)) QF_CK(cudaStreamWaitEvent(s, landed_[i], 0));
     fn(i, dev_of(i), n_of(i));
     if (i >= resident_) QF_CK(cudaEventRecord(freed_[(i - resident_) % K], s));
@@ -352,6 +354,7 @@ std::vector<Digest> GpuBackend::commit_streamed(const BlockStream::BlockFn& per_
     const Digest z = encode_block(nullptr, 0, 0, cw);
     for (size_t b = src_->live_blocks(); b < P_.blocks(); ++b) roots_[b] = z;
   }
+  scratch_.reset();  // back to the pool until binding needs it again
   return roots_;
 }
 
@@ -1039,11 +1042,23 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
 void GpuBackend::eo_round_fold(F inv, F ch) {
   HostScope hs("eo_round_fold");
   const uint64_t n = eo_len_;
-  if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
   const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
-  QF_LAUNCH(s_, "k_eo_fold_cross", n * 48, qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p));
-  std::swap(wit_, wit2_);
-  std::swap(qv_, qv2_);
+  if (n >= (uint64_t(1) << 26)) {
+    // Large rounds fold the two vectors one after the other: the full-length
+    // witness goes back to the pool before the query's output is allocated,
+    // so the round holds 2.5 rather than 3 vector lengths.
+    DBuf<Fe> w2(n / 2);
+    QF_LAUNCH(s_, "k_eo_fold_vec", n * 24, qfd::k_eo_fold_vec<<<grid_for(n / 2, kThreads), kThreads, 0, s_>>>(wit_.p, n, to_fe(inv), w2.p));
+    wit_ = std::move(w2);
+    DBuf<Fe> q2(n / 2);
+    QF_LAUNCH(s_, "k_eo_fold_query_cross", n * 32, qfd::k_eo_fold_query_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch), q2.p, partials_.p));
+    qv_ = std::move(q2);
+  } else {
+    if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
+    QF_LAUNCH(s_, "k_eo_fold_cross", n * 48, qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p));
+    std::swap(wit_, wit2_);
+    std::swap(qv_, qv2_);
+  }
   eo_len_ = n / 2;
   if (eo_len_ >= 2) {
     std::vector<F> r = reduce_to_host(partials_, g, 2);
@@ -1056,6 +1071,12 @@ std::array<F, 2> GpuBackend::eo_terminal() {
   QF_CK(cudaMemcpyAsync(&w0, wit_.p, 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaMemcpyAsync(&q0, qv_.p, 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
+  // The EO vectors (up to 2 x 1.5 x N/stride elements) are done: give their
+  // memory back before the batch opening allocates its own.
+  wit_.reset();
+  qv_.reset();
+  wit2_.reset();
+  qv2_.reset();
   return {w0, q0};
 }
 

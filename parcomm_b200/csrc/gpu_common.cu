@@ -9,14 +9,20 @@ namespace qfg {
 
 namespace {
 std::mutex g_pool_mu;
-std::multimap<size_t, void*> g_pool;  // rounded bytes -> free device block
+std::multimap<std::pair<int, size_t>, void*> g_pool;  // (device, rounded bytes) -> free device block
+int current_device() {
+  int d = 0;
+  QF_CK(cudaGetDevice(&d));
+  return d;
+}
 }  // namespace
 
 void* DevicePool::get(size_t bytes) {
   const size_t r = rounded(bytes);
+  const int dev = current_device();
   {
     std::lock_guard<std::mutex> g(g_pool_mu);
-    auto it = g_pool.find(r);
+    auto it = g_pool.find({dev, r});
     if (it != g_pool.end()) {
       void* p = it->second;
       g_pool.erase(it);
@@ -32,14 +38,31 @@ void* DevicePool::get(size_t bytes) {
   return p;
 }
 void DevicePool::put(void* p, size_t bytes) {
+  const int dev = current_device();
   std::lock_guard<std::mutex> g(g_pool_mu);
-  g_pool.emplace(rounded(bytes), p);
+  g_pool.emplace(std::make_pair(dev, rounded(bytes)), p);
 }
+// Frees the current device's cached blocks.
 void DevicePool::trim() {
+  const int dev = current_device();
   std::lock_guard<std::mutex> g(g_pool_mu);
   cudaDeviceSynchronize();
-  for (auto& [b, p] : g_pool) cudaFree(p);
-  g_pool.clear();
+  for (auto it = g_pool.begin(); it != g_pool.end();) {
+    if (it->first.first == dev) {
+      cudaFree(it->second);
+      it = g_pool.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+size_t DevicePool::cached_bytes() {
+  const int dev = current_device();
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  size_t n = 0;
+  for (auto& [k, p] : g_pool)
+    if (k.first == dev) n += k.second;
+  return n;
 }
 
 bool KernelClock::enabled = false;

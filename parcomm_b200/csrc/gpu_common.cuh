@@ -60,13 +60,14 @@ using HostScope = ::qf::Section;
   } while (0)
 
 // Process-wide cache of device allocations: released buffers are kept, keyed
-// by their rounded size, and handed out again, so repeated commits/openings
+// by device and rounded size, and handed out again, so repeated commits/openings
 // of the same shapes pay no cudaMalloc/cudaFree.  A failed cudaMalloc first
 // returns the cache to the driver and retries.
 struct DevicePool {
   static void* get(size_t bytes);
   static void put(void* p, size_t bytes);
   static void trim();
+  static size_t cached_bytes();  // held in the cache for the current device
   static size_t rounded(size_t bytes) {
     const size_t g = bytes >= (size_t(1) << 20) ? (size_t(1) << 20) : 256;
     return (bytes + g - 1) / g * g;

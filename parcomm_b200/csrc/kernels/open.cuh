@@ -230,6 +230,38 @@ __global__ void k_eo_fold_cross(const Fe* __restrict__ w, const Fe* __restrict__
     for (int k = 0; k < 2; ++k) store(partials + size_t(blockIdx.x) * 2 + k, v[k]);
 }
 
+// The same fold as k_eo_fold_cross, one vector at a time, so the full-length
+// witness can be released before the query's half-length output exists:
+// w'[i] = w[2i] + w[2i+1] * inv, then q'[i] = q[2i] + q[2i+1] * ch with the
+// next cross pair of (w', q').
+__global__ void k_eo_fold_vec(const Fe* __restrict__ w, uint64_t n, Fe f, Fe* __restrict__ out) {
+  const Fr ff = load(&f);
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n / 2; i += uint64_t(gridDim.x) * blockDim.x)
+    store(out + i, add(load(w + 2 * i), mul(load(w + 2 * i + 1), ff)));
+}
+__global__ void k_eo_fold_query_cross(const Fe* __restrict__ wf, const Fe* __restrict__ q, uint64_t n, Fe ch,
+                                      Fe* __restrict__ q_out, Fe* __restrict__ partials) {
+  const Fr fc = load(&ch);
+  Fr v[2] = {zero(), zero()};
+  if (n == 2) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) store(q_out, add(load(q), mul(load(q + 1), fc)));
+  } else {
+    for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n / 4; j += uint64_t(gridDim.x) * blockDim.x) {
+      const Fr a0 = load(wf + 2 * j), a1 = load(wf + 2 * j + 1);
+      const Fr b0 = add(load(q + 4 * j), mul(load(q + 4 * j + 1), fc));
+      const Fr b1 = add(load(q + 4 * j + 2), mul(load(q + 4 * j + 3), fc));
+      store(q_out + 2 * j, b0);
+      store(q_out + 2 * j + 1, b1);
+      v[0] = add(v[0], mul(a0, b1));
+      v[1] = add(v[1], mul(a1, b0));
+    }
+  }
+  block_reduce<2>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 2; ++k) store(partials + size_t(blockIdx.x) * 2 + k, v[k]);
+}
+
 // ---------------------------------------------------------------- batch opening
 // weights[i] = hi[i >> lb] * lo[i & mask]  (an equality or tensor table).
 __global__ void k_table(const Fe* __restrict__ hi, const Fe* __restrict__ lo, int lb, uint64_t m, Fe* __restrict__ out) {

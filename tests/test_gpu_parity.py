@@ -178,6 +178,10 @@ def run_streamed(shapes, chunk_log, packed_log, mats, field="f65521", resident_b
     o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, packed_log, bva, field=field)
     host = torch.from_numpy(bva).pin_memory() if pinned else bva
     c = p.commit_recomputed(host, resident_bytes=resident_bytes)
+    h2d, resident, live = c.stream_info()
+    assert h2d == bva.nbytes and live == -(-bva.size // (1 << chunk_log))
+    if resident_bytes is None:
+        assert resident == live
     assert b"".join(c.roots) == o_roots, "commitment roots differ"
     claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
     assert qf.claims_to_bytes(claims) == o_claims, "claims differ"
@@ -207,14 +211,15 @@ def test_streamed_ragged_shapes_many_blocks(field, packed_log, resident, pinned)
     run_streamed(shapes, 14, packed_log, mats, field=field, resident_bytes=resident * (1 << 14) * w, pinned=pinned)
 
 
-@pytest.mark.parametrize("field", ["f65521", "koalabear"])
-def test_streamed_terms_spanning_blocks_and_zero_suffix(field):
-    """A 2^20-entry bucket spans 16 blocks of 2^16; 15 of 32 blocks are the zero suffix."""
+@pytest.mark.parametrize("field,resident", [("f65521", 0), ("koalabear", None)])
+def test_streamed_terms_spanning_blocks_and_zero_suffix(field, resident):
+    """A 2^20-entry bucket spans 16 blocks of 2^16; 15 of 32 blocks are the
+    zero suffix.  resident None: the automatic budget keeps every block."""
     rng = np.random.default_rng(17)
     shapes = [(1024, 1024), (1, 16)]
     gen = gaussian_i16 if field == "koalabear" else gaussian_i8
     mats = [gen(rng, r * c).reshape(r, c) for r, c in shapes]
-    run_streamed(shapes, 16, 4, mats, field=field, resident_bytes=0, pinned=True)
+    run_streamed(shapes, 16, 4, mats, field=field, resident_bytes=resident, pinned=True)
 
 
 def test_streamed_matches_resident_commit_smoke_config():
