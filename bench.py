@@ -184,15 +184,16 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel: str, alg_bytes_per_launch: float):
+def ncu_traffic(kernel: str, alg_bytes_per_launch: float, field: str = ""):
     """Per-launch DRAM bytes of `kernel`: the committed ncu capture's ratio of
     dram__bytes_read.sum + dram__bytes_write.sum to algorithmic bytes (taken
-    on a smaller case of the same kernel), times this run's algorithmic bytes
-    per launch; None without a capture."""
+    on a smaller case of the same kernel and field), times this run's
+    algorithmic bytes per launch; None without a capture."""
     p = ROOT / "profiles" / "ncu_traffic.json"
     if not p.exists():
         return None
-    d = json.loads(p.read_text()).get(kernel)
+    table = json.loads(p.read_text())
+    d = table.get(f"{kernel}/{field}") if field else table.get(kernel)
     if not d:
         return None
     return d["dram_bytes_per_alg_byte"] * alg_bytes_per_launch
@@ -478,7 +479,7 @@ def main():
     d = stats[dominant]
     achieved = d["bytes"] / (d["ms"] / 1000.0) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = ncu_traffic(dominant, d["bytes"] / d["launches"])
+    traffic = ncu_traffic(dominant, d["bytes"] / d["launches"], "koalabear" if sixteen else "")
 
     link = None
     if streamed:  # the host link bounds a streamed step: bytes copied per step against a measured copy
