@@ -72,10 +72,12 @@ int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int b
 void qf_committed_free(qf_committed* committed);
 
 /* Parameters::commit_recomputed (protocol.rs:131-185, the reference's
- * `--cache-mode recompute`) for weight sets larger than HBM: `host_bva`
- * (n_values entries in host memory; page-locked memory lets the copies
- * overlap the compute) stays owned by the caller and must stay valid and
- * unchanged until the committed handle is freed.  Every pass that reads the
+ * `--cache-mode recompute`): only the block roots stay in HBM, and binding
+ * re-encodes every block.  `host_bva` holds n_values entries in host memory
+ * (for weight sets larger than HBM; page-locked memory lets the copies
+ * overlap the compute) or in device memory (weights resident, codewords
+ * recomputed: a pool of many commitments).  It stays owned by the caller and
+ * must stay valid and unchanged until the committed handle is freed.  Every pass that reads the
  * weights (commit, EO cross terms and witness, projection, block fold) stages
  * them into HBM one PCS block at a time, and binding re-encodes each block
  * and checks its root.  The first resident_bytes / (2^chunk_log * entry size)
@@ -109,6 +111,13 @@ int qf_eval_claims(const qf_params* params, const qf_committed* committed, const
  * released with qf_committed_free. */
 int qf_prove(const qf_params* params, qf_committed* committed, const uint8_t* claims, size_t claims_len, uint8_t** proof,
              size_t* proof_len, qf_profile* profile);
+
+/* Like qf_prove, but leaves the committed handle usable for further
+ * openings (a serving pool answers many claims on one commitment).  Calls on
+ * one handle must not overlap; handles are independent.  No reference
+ * counterpart: the reference's prove consumes Committed. */
+int qf_open(const qf_params* params, const qf_committed* committed, const uint8_t* claims, size_t claims_len,
+            uint8_t** proof, size_t* proof_len, qf_profile* profile);
 
 /* Proof::from_bytes + Parameters::verify (protocol.rs:97-107, 266-320). Host only. */
 int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,

@@ -60,7 +60,7 @@ EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
     "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
-    "qf_committed_stream_info",
+    "qf_committed_stream_info", "qf_open",
 )
 
 
@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
         L.qf_eval_claims.argtypes = [P, P, ctypes.c_char_p, S, ctypes.c_char_p, S, ctypes.POINTER(S)]
         L.qf_prove.argtypes = [P, P, ctypes.c_char_p, S, ctypes.POINTER(BP), ctypes.POINTER(S), ctypes.POINTER(_Profile)]
         L.qf_verify.argtypes = [P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
+        L.qf_open.argtypes = [P, P, ctypes.c_char_p, S, ctypes.POINTER(BP), ctypes.POINTER(S), ctypes.POINTER(_Profile)]
         L.qf_free_bytes.argtypes = [P]
         L.qf_free_bytes.restype = None
         L.qf_last_error.argtypes = [ctypes.c_char_p, S]
@@ -289,17 +290,15 @@ class Parameters:
         return Committed(self, h.value, [roots.raw[32 * i: 32 * i + 32] for i in range(self.blocks)])
 
     def commit_recomputed(self, values, resident_bytes: Optional[int] = 0) -> Committed:
-        """Parameters::commit_recomputed: the reference's recompute mode.  Host
+        """Parameters::commit_recomputed: the reference's recompute mode: only
+        the roots stay on the device and binding re-encodes each block.  Host
         weights (a numpy array, or a CPU tensor, ideally in pinned memory) stay
         where they are and are streamed into HBM one PCS block at a time for
-        every pass; only the roots stay on the device and binding re-encodes
-        each block.  `resident_bytes` of leading blocks are kept in HBM after
+        every pass; `resident_bytes` of leading blocks are kept in HBM after
         the first pass (None: as many as the device's free memory allows next
-        to the proof's own peak).  Device tensors take the cached path
-        (`commit`).  The roots, claims and proof bytes equal those of
-        `commit`."""
-        if hasattr(values, "is_cuda") and values.is_cuda:
-            return self.commit(values, on_device=True)
+        to the proof's own peak).  A CUDA tensor stays where it is and is read
+        in place.  The weights must stay unchanged while the handle lives.
+        The roots, claims and proof bytes equal those of `commit`."""
         if hasattr(values, "data_ptr"):
             if int(values.element_size()) != np.dtype(self.weight_dtype).itemsize or not values.is_contiguous():
                 raise QfError(-9, f"host weights must be contiguous {np.dtype(self.weight_dtype).name}")
@@ -357,6 +356,21 @@ class Parameters:
         finally:
             lib().qf_free_bytes(ctypes.cast(out, ctypes.c_void_p))
         committed.consumed = True
+        return Proof(data), ProverProfile(*[getattr(prof, f) for f, _ in _Profile._fields_])
+
+    def open(self, committed: Committed, claims: Sequence[Claim]) -> Tuple[Proof, ProverProfile]:
+        """`prove` without consuming the commitment (qf_open): a pool answers
+        many claims on one commitment.  Calls on one commitment must not
+        overlap."""
+        cb = claims_to_bytes(claims)
+        out = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_size_t()
+        prof = _Profile()
+        _check(lib().qf_open(self._h, committed._h, cb, len(cb), ctypes.byref(out), ctypes.byref(n), ctypes.byref(prof)))
+        try:
+            data = ctypes.string_at(out, n.value)
+        finally:
+            lib().qf_free_bytes(ctypes.cast(out, ctypes.c_void_p))
         return Proof(data), ProverProfile(*[getattr(prof, f) for f, _ in _Profile._fields_])
 
     def verify(self, statement: Commitment | Sequence[bytes], claims: Sequence[Claim], proof: Proof | bytes) -> None:

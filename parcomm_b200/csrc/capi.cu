@@ -148,6 +148,21 @@ int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* clai
   });
 }
 
+int qf_open(const qf_params* params, const qf_committed* committed, const uint8_t* claims, size_t claims_len,
+            uint8_t** proof, size_t* proof_len, qf_profile* profile) {
+  return guarded([&] {
+    if (!params || !committed || !claims || !proof || !proof_len) fail(QF_E_ARGUMENT, "null argument");
+    if (committed->consumed) fail(QF_E_ARGUMENT, "committed state already consumed by prove");
+    std::vector<uint8_t> bytes =
+        api(params->field).prove(params, const_cast<qf_committed*>(committed), claims, claims_len, profile);
+    uint8_t* buf = static_cast<uint8_t*>(std::malloc(bytes.size()));
+    if (!buf) fail(QF_E_ARGUMENT, "host allocation failed");
+    std::memcpy(buf, bytes.data(), bytes.size());
+    *proof = buf;
+    *proof_len = bytes.size();
+  });
+}
+
 void qf_free_bytes(uint8_t* bytes) { std::free(bytes); }
 
 int qf_kernel_timing(int enable) {

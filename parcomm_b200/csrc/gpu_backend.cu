@@ -125,8 +125,8 @@ GpuBackend::GpuBackend(const Parameters<F>& p, const W* d_bva, size_t active, cu
 GpuBackend::GpuBackend(const Parameters<F>& p, BlockStream* src, cudaStream_t s, DeviceTables* tables)
     : P_(p), bva_(nullptr), src_(src), active_(src->active()), s_(s), tables_(tables ? tables : &own_tables_) {
   configure_tile_kernels();
-  check(P_.blocks() >= 2, "streamed weights need at least two PCS blocks");
   check(src->block_len() == P_.block_len, "block length of the weight stream");
+  if (src->on_device()) bva_ = src->host();  // gathers read the resident weights directly
   partials_.alloc(148 * 8 * 4);
   result_.alloc(8);
 }
@@ -137,6 +137,13 @@ BlockStream::BlockStream(const W* host, uint64_t active, uint64_t block_len, siz
     : host_(host), active_(active), block_len_(block_len) {
   check(slots >= 2, "at least two staging slots");
   live_ = size_t((active + block_len - 1) / block_len);
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, host) == cudaSuccess && attr.type == cudaMemoryTypeDevice) {
+    device_ = true;
+    resident_ = live_;
+    return;
+  }
+  cudaGetLastError();
   resident_ = std::min(resident, live_);
   if (resident_) resident_buf_.alloc(resident_ * block_len);
   const size_t streamed = live_ - resident_;
@@ -158,6 +165,11 @@ BlockStream::~BlockStream() {
 }
 
 void BlockStream::for_each(cudaStream_t s, const BlockFn& fn) {
+  if (device_) {
+    for (size_t i = 0; i < live_; ++i)
+      fn(i, host_ + uint64_t(i) * block_len_, std::min<uint64_t>(block_len_, active_ - uint64_t(i) * block_len_));
+    return;
+  }
   const size_t K = slot_buf_.size();
   auto n_of = [&](size_t b) { return std::min<uint64_t>(block_len_, active_ - uint64_t(b) * block_len_); };
   auto dev_of = [&](size_t b) -> W* {
@@ -461,7 +473,7 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   // Zero blocks (the suffix past the active entries) have vanishing lanes.
   const size_t live = std::min<size_t>(nblocks, (active_ + P_.block_len - 1) / P_.block_len);
   const unsigned grid = unsigned(std::min<uint64_t>((m + qfd::kEqChunk - 1) / qfd::kEqChunk, 148 * 4));
-  if (src_) {  // one block per launch, as each lands in HBM
+  if (streaming()) {  // one block per launch, as each lands in HBM
     src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
       if (b >= nblocks) return;
       QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W),
@@ -469,7 +481,7 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
                                                                            raw.p + kRaw * b));
     });
   }
-  for (size_t b0 = 0; !src_ && b0 < live; b0 += qfd::kEqBlocks) {
+  for (size_t b0 = 0; !streaming() && b0 < live; b0 += qfd::kEqBlocks) {
     const int nb = int(std::min<size_t>(qfd::kEqBlocks, live - b0));
     QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W) * uint64_t(nb),
               qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva_, active_, P_.block_len, b0, nb, m, weights_.p,
@@ -491,8 +503,23 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   return out;
 }
 
+const DeviceCodeword& GpuBackend::single_codeword() {
+  if (!src_) return *blocks_.at(0);
+  if (!single_cw_) {
+    DeviceCodeword& cw = scratch_codeword();
+    Digest r{};
+    if (src_->live_blocks() == 0) r = encode_block(nullptr, 0, 0, cw);
+    src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+      if (b == 0) r = encode_block(d, n, 0, cw);
+    });
+    if (r != roots_.at(0)) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
+    single_cw_ = &cw;
+  }
+  return *single_cw_;
+}
+
 std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
-  check(!src_, "single-block opening of streamed weights");
+  single_cw_ = nullptr;  // a new opening
   std::vector<std::vector<F>> lanes = project_blocks(outer, 1);
   // Packed values of the single block: the block fold with weight one.
   const uint64_t m = P_.pcs.packed_len();
@@ -502,7 +529,16 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   for (int j = 0; j < L; ++j) T[j] = basis<F>(j);
   DBuf<Fe> dT(L);
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), L * 16, cudaMemcpyHostToDevice, s_));
-  QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p, 0));
+  if (streaming()) {
+    QF_CK(cudaMemsetAsync(values_.p, 0, m * 16, s_));
+    src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
+      if (b == 0)
+        QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 32),
+                  qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(d, n, P_.block_len, 1, m, dT.p, values_.p, 1));
+    });
+  } else {
+    QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p, 0));
+  }
   sum_len_ = m;
   msg_valid_ = false;
   return lanes[0];
@@ -529,7 +565,7 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   DBuf<Fe> dT(T.size());
   QF_CK(cudaMemcpyAsync(dT.p, T.data(), T.size() * 16, cudaMemcpyHostToDevice, s_));
   values_.alloc(m);
-  if (src_) {  // accumulate block by block; the zero blocks add nothing
+  if (streaming()) {  // accumulate block by block; the zero blocks add nothing
     QF_CK(cudaMemsetAsync(values_.p, 0, m * 16, s_));
     src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
       if (b >= size_t(blocks)) return;
@@ -659,7 +695,7 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
 std::vector<W> GpuBackend::windows(const std::vector<uint64_t>& starts, size_t stride) {
   std::vector<W> out(starts.size() * stride);
   if (starts.empty()) return out;
-  if (src_) {  // a few entries each: read them where the weights live
+  if (src_ && !src_->on_device()) {  // a few entries each: read them in host memory
     for (size_t i = 0; i < starts.size(); ++i)
       for (size_t k = 0; k < stride; ++k) {
         const uint64_t g = starts[i] + k;
@@ -741,7 +777,7 @@ uint64_t term_tile_count(const qfd::TermTiles& T) { return (T.rows + (uint64_t(1
 // to 1024 rows, tile weights from device-built factor tables.
 std::vector<std::vector<std::vector<F>>> GpuBackend::project_term_groups(
     const std::vector<std::vector<const Term<F>*>>& groups, size_t stride) {
-  if (src_) return project_groups_streamed(groups, stride);
+  if (streaming()) return project_groups_streamed(groups, stride);
   std::vector<std::vector<std::vector<F>>> out;
   for (const auto& g : groups) out.push_back(project_terms(g, stride));
   return out;
@@ -852,7 +888,7 @@ std::vector<std::vector<std::vector<F>>> GpuBackend::project_groups_streamed(
 }
 
 std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Term<F>*>& terms, size_t stride) {
-  if (src_) return project_groups_streamed({terms}, stride)[0];
+  if (streaming()) return project_groups_streamed({terms}, stride)[0];
   HostScope hs("project_terms");
   std::vector<std::vector<F>> out(terms.size());
   TableBuilder tb;
@@ -952,7 +988,7 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
   std::vector<F> pinv = consecutive_powers(inv, stride);
   DBuf<Fe> dp(stride);
   QF_CK(cudaMemcpyAsync(dp.p, pinv.data(), stride * 16, cudaMemcpyHostToDevice, s_));
-  if (src_) {
+  if (streaming()) {
     // Rows of each block as its weights land; rows past the live blocks are zero.
     check(P_.block_len % stride == 0, "block length and EO stride");
     const uint64_t rpb = P_.block_len / stride;

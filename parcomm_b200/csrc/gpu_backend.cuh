@@ -69,9 +69,12 @@ class BlockStream {
   BlockStream& operator=(const BlockStream&) = delete;
   uint64_t active() const { return active_; }
   uint64_t block_len() const { return block_len_; }
+  // The weights are already in HBM (a device pointer): every block is used in
+  // place and nothing is copied.
+  bool on_device() const { return device_; }
   size_t live_blocks() const { return live_; }
   size_t resident_blocks() const { return resident_; }
-  const W* host() const { return host_; }
+  const W* host() const { return host_; }  // the weights (device memory when on_device())
   uint64_t h2d_bytes() const { return copied_; }
   // fn(b, d, n) for every live block b in order, with its launches on `s`: d
   // is the device copy of entries [b * block_len, b * block_len + n).
@@ -82,6 +85,7 @@ class BlockStream {
   const W* host_;
   uint64_t active_, block_len_;
   size_t live_, resident_;
+  bool device_ = false;
   bool resident_ready_ = false;
   DBuf<W> resident_buf_;
   std::vector<DBuf<W>> slot_buf_;
@@ -131,12 +135,12 @@ class GpuBackend : public Backend<F>,
   F sumcheck_final_weight() override;
   std::vector<uint8_t> binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) override;
   const CodewordView<F>& folded_codeword() override { return *folded_; }
-  const CodewordView<F>& codeword() override { return *blocks_.at(0); }
+  const CodewordView<F>& codeword() override { return single_codeword(); }
   std::vector<F> folded_opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
     return open_top(*folded_, point, col_log);
   }
   std::vector<F> opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
-    return open_top(*blocks_.at(0), point, col_log);
+    return open_top(single_codeword(), point, col_log);
   }
   TopRoundAccel<F>* top_round_accel() override { return this; }
   DecideAccel<F>* decide_accel() override { return this; }
@@ -193,6 +197,12 @@ class GpuBackend : public Backend<F>,
   // src_base + 2^chunk) are read from `bva` (zero at or past `active`).
   Digest encode_block(const W* bva, uint64_t active, uint64_t src_base, DeviceCodeword& cw);
   DeviceCodeword& scratch_codeword();
+  // Weights that reach HBM block by block (host memory); resident weights,
+  // streamed or not, take the whole-array launches.
+  bool streaming() const { return src_ && !src_->on_device(); }
+  // The codeword of a single-block statement (re-encoded once per opening
+  // for streamed weights).
+  const DeviceCodeword& single_codeword();
   std::vector<std::vector<std::vector<F>>> project_groups_streamed(const std::vector<std::vector<const Term<F>*>>& groups,
                                                                    size_t stride);
   void mobius_rest(Fe* cw, int logm, int logR, int from);
@@ -202,6 +212,7 @@ class GpuBackend : public Backend<F>,
   const W* bva_;              // resident weights, or null
   BlockStream* src_ = nullptr;  // streamed weights, or null
   std::unique_ptr<DeviceCodeword> scratch_;  // re-encoded block of a streamed backend
+  const DeviceCodeword* single_cw_ = nullptr;  // this opening's re-encoded single block
   size_t active_;
   cudaStream_t s_;
   std::vector<std::unique_ptr<DeviceCodeword>> blocks_;

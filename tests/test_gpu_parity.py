@@ -245,3 +245,57 @@ def test_streamed_nonzero_padding_rejected():
     bva[b.offset + b.physical_cols] = 1
     with pytest.raises(qf.QfError, match="nonzero boundary padding"):
         p.commit_recomputed(bva)
+
+
+@pytest.mark.parametrize("field,shapes,chunk_log", [
+    ("f65521", [(300, 700), (129, 65), (1, 5000), (77, 1)], 14),   # many blocks
+    ("koalabear", [(512, 1024)], 20),                              # one block
+    ("f65521", [(64, 64)], 12)])                                   # one block
+def test_recompute_mode_device_and_host_weights(field, shapes, chunk_log):
+    """commit_recomputed over device-resident weights (read in place) and over
+    host weights; single-block statements re-encode their block for the
+    opening.  Both equal the oracle's bytes."""
+    import torch
+    rng = np.random.default_rng(23 + chunk_log)
+    gen = gaussian_i16 if field == "koalabear" else gaussian_i8
+    mats = [gen(rng, r * c, forced=0.001).reshape(r, c) for r, c in shapes]
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=4), field=FIELDS[field])
+    bva = layout.encode(p.shapes, mats)
+    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, 4, bva, field=field)
+    for weights in (torch.from_numpy(bva).cuda(), bva):
+        c = p.commit_recomputed(weights)
+        assert b"".join(c.roots) == o_roots
+        claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
+        assert qf.claims_to_bytes(claims) == o_claims
+        proof, _ = p.prove(c, claims)
+        assert proof.to_bytes() == o_proof
+        c.close()
+
+
+@pytest.mark.parametrize("mode", ["cache", "recompute_device", "recompute_host"])
+def test_open_keeps_the_commitment_for_repeated_claims(mode):
+    """qf_open answers several claims on one commitment; each proof equals the
+    oracle's proof for those claims (fresh points per opening)."""
+    import torch
+    rng = np.random.default_rng(31)
+    shapes = [(300, 700), (129, 65)]
+    chunk_log = 14 if mode != "cache" else 16
+    mats = [gaussian_i8(rng, r * c).reshape(r, c) for r, c in shapes]
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=4))
+    bva = layout.encode(p.shapes, mats)
+    if mode == "cache":
+        c = p.commit(bva)
+    elif mode == "recompute_device":
+        c = p.commit_recomputed(torch.from_numpy(bva).cuda())
+    else:
+        c = p.commit_recomputed(bva)
+    for k in range(3):
+        n_coords = len(p.benchmark_points(c.roots)) // 16
+        pts = rng.integers(0, 65521, n_coords * 8).astype("<u2").tobytes()  # canonical F65521^8 coordinates
+        claims = p.evaluate_claims(c, pts)
+        proof, _ = p.open(c, claims)
+        _, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, 4, bva, claims=qf.claims_to_bytes(claims))
+        assert qf.claims_to_bytes(claims) == o_claims
+        assert proof.to_bytes() == o_proof, f"opening {k} differs"
+        p.verify(c.roots, claims, proof)
+    c.close()
