@@ -12,6 +12,9 @@
 // implementation in the product library; a plain CPU restatement in the
 // oracle).  Everything here is sequential protocol logic.
 #pragma once
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <chrono>
 #include <functional>
 #include <memory>
@@ -178,15 +181,31 @@ struct Backend {
 template <class F>
 struct PackedPcs {
   size_t log_n = 0;  // base values per block, log2
-  std::unique_ptr<PcsParams<F>> pp;
+  std::shared_ptr<PcsParams<F>> pp;
   size_t packed_len() const { return size_t(1) << (log_n - ilog2(F::kLanes)); }
 
+  // The setup depends only on (log_n, columns, security bits, seed), so one
+  // process builds each distinct setup once and shares it between parameter
+  // sets (a pool of many shapes with few distinct block sizes).
   static PackedPcs create(size_t log_n, size_t columns, size_t security_bits, const std::array<uint8_t, 32>& seed) {
     if (log_n < 4 || log_n > 30) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "packed log_n");
+    static std::mutex mu;
+    static std::map<std::tuple<size_t, size_t, size_t, std::array<uint8_t, 32>>, std::shared_ptr<PcsParams<F>>> cache;
     PackedPcs p;
     p.log_n = log_n;
+    const auto key = std::make_tuple(log_n, columns, security_bits, seed);
+    {
+      std::lock_guard<std::mutex> g(mu);
+      auto it = cache.find(key);
+      if (it != cache.end()) {
+        p.pp = it->second;
+        return p;
+      }
+    }
     StdRng rng(seed);
-    p.pp = pcs_setup<F>(size_t(1) << (log_n - ilog2(F::kLanes)), columns, security_bits, rng);
+    std::shared_ptr<PcsParams<F>> pp(pcs_setup<F>(size_t(1) << (log_n - ilog2(F::kLanes)), columns, security_bits, rng).release());
+    std::lock_guard<std::mutex> g(mu);
+    p.pp = cache.emplace(key, pp).first->second;
     return p;
   }
   const Digest& parameter_digest() const { return pp->parameter_digest; }
