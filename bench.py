@@ -269,6 +269,105 @@ def per_matrix_path(qf, shapes, seed_base: int, field: int, bf16: bool):
     return time.perf_counter() - t0, setup_s
 
 
+def int8_matrix(rows: int, cols: int, seed: int):
+    """int8 round(N(0, 20^2)) clipped to +-127 with 0.1% forced to +-127, on the GPU."""
+    import torch
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    w = torch.randn(rows * cols, generator=g, device="cuda", dtype=torch.float32).mul_(20.0).round_().clamp_(-127, 127)
+    n_forced = max(1, (rows * cols) // 1000)
+    idx = torch.randint(0, rows * cols, (n_forced,), generator=g, device="cuda")
+    w[idx] = torch.randint(0, 2, (n_forced,), generator=g, device="cuda").float().mul_(254.0).sub_(127.0)
+    return w.to(torch.int8).view(rows, cols)
+
+
+def run_serve(args):
+    """The serving loop: a device-resident pool of the 8B-shape 8-bit set
+    (226 single-matrix commitments in cache mode: weights, codewords and
+    trees resident) and the 70B-shape 8-bit set (562 single-matrix
+    commitments in recompute mode: weights resident, each opening re-encodes;
+    F65521^8, packed_log 6).  Seeded Poisson arrivals per rate: 90% opening
+    requests of 1-64 random pooled matrices at fresh uniform points, 10%
+    commits of new int8 matrices (1024-28672 rows x 4096 or 8192 columns).
+    Each rate runs the same requests twice: through the engine (continuous
+    batching over --slots workers under the HBM budget) and one plain
+    request at a time.  Prints one JSON line."""
+    import numpy as np
+    import torch
+    import parcomm_b200 as qf
+    from parcomm_b200 import serving
+    from parcomm_b200.build import build
+
+    build()
+    torch.cuda.set_device(0)
+    t0 = time.time()
+    pool = serving.Pool()
+    sets = [("8B-shape 8-bit", shapes_8b(), qf.Config(30, 4), False),
+            ("70B-shape 8-bit", shapes_70b(), qf.Config(30, 6), True)]
+    if args.serve_scale < 1.0:  # a subset of each set, for quick runs
+        sets = [(n, sh[:max(1, int(len(sh) * args.serve_scale))], c, r) for n, sh, c, r in sets]
+    pool_weights = 0
+    for si, (_, shapes, cfg, recompute) in enumerate(sets):
+        for m, (r, c) in enumerate(shapes):
+            pool.commit(int8_matrix(r, c, 1000 * si + m), cfg, recompute)
+            pool_weights += r * c
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    load_s = time.time() - t0
+    free_b, total_b = torch.cuda.mem_get_info()
+    budget = int(free_b - (8 << 30))  # headroom for torch and the library's own tables
+    keys = pool.keys()
+
+    def make_requests(n, seed):
+        rng = np.random.default_rng(seed)
+        out = []
+        for k in range(n):
+            if rng.random() < 0.1:
+                rows, cols = int(rng.integers(1024, 28673)), int(rng.choice([4096, 8192]))
+                out.append(serving.CommitRequest(int8_matrix(rows, cols, 777_000 + seed * 1000 + k), qf.Config(30, 4), True))
+            else:
+                pick = list(rng.choice(keys, size=min(len(keys), int(rng.integers(1, 65))), replace=False))
+                out.append(serving.OpenRequest(pick, [serving.random_points(pool.get(m).params, rng) for m in pick]))
+        return out
+
+    # Warm-up: one request of each kind through the engine.
+    eng = serving.Engine(pool, slots=args.slots, hbm_budget=budget)
+    for q in make_requests(4, 12345):
+        eng.submit(q)
+    eng.drain()
+    eng.close()
+    rates = []
+    for ri, rate in enumerate(args.serve_rates):
+        reqs = make_requests(args.serve_requests, 100 + ri)
+        offsets = serving.poisson_arrivals(rate, len(reqs), args.serve_seed + ri)
+        row = {"rate_per_s": rate}
+        for name, slots in (("engine", args.slots), ("one_at_a_time", 1)):
+            eng = serving.Engine(pool, slots=slots, hbm_budget=budget)
+            res, span = serving.run_arrivals(eng, reqs, offsets)
+            eng.close()
+            row[name] = serving.summarize(res, span)
+            row[name]["peak_tasks_in_flight"] = eng.peak_running
+        row["p99_speedup"] = row["one_at_a_time"]["p99_ms"] / row["engine"]["p99_ms"]
+        rates.append(row)
+        print(json.dumps({"progress": row}), file=sys.stderr)
+    line = {
+        "metric": "QAFold serving: opening latency p50/p99 and throughput under Poisson load",
+        "unit": "ms (latency), weights/s and requests/s (throughput)",
+        "n_gpus": 1,
+        "data": "synthetic",
+        "dtype": "int8",
+        "config": {"workload": "serving loop (C5)", "pool": [n for n, *_ in sets], "pool_matrices": len(pool),
+                   "pool_weights": pool_weights, "field": "F65521^8", "slots": args.slots,
+                   "hbm_budget_bytes": budget, "requests_per_rate": args.serve_requests,
+                   "open": "1-64 random pooled matrices, fresh uniform points, one proof each (qf_open)",
+                   "commit": "10%: new int8 matrix, 1024-28672 rows x 4096/8192 cols, recompute mode",
+                   "scale": args.serve_scale},
+        "load_s": load_s,
+        "rates": rates,
+    }
+    print(json.dumps(line))
+
+
 def run_reference(args):
     """CPU restatement of the reference prover on a bounded sample of the workload."""
     sys.path.insert(0, str(ROOT / "oracle"))
@@ -336,11 +435,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="8b8",
-                    choices=["8b8", "8b16", "70b16", "layers", "layers16", "layers70", "smoke"],
+                    choices=["8b8", "8b16", "70b16", "layers", "layers16", "layers70", "smoke", "serve"],
                     help="8b8 / 8b16: the 8B shape set with 8-bit weights (F65521^8) or 16-bit BF16 "
                          "payloads (KoalaBear^4); layers / layers16: the first --layers transformer layers "
                          "(7 matrices each) at --chunk-log, a small case for profiling")
     ap.add_argument("--layers", type=int, default=2)
+    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent tasks")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[1.0, 5.0, 20.0, 50.0])
+    ap.add_argument("--serve-requests", type=int, default=10, help="serve: requests per rate")
+    ap.add_argument("--serve-seed", type=int, default=0)
+    ap.add_argument("--serve-scale", type=float, default=1.0, help="serve: fraction of each pool set to load")
     ap.add_argument("--resident-gb", type=float, default=None,
                     help="70b16 / layers70: GB of leading weight blocks kept in HBM after the first streamed pass "
                          "(default: what free HBM allows next to the proof's own peak)")
@@ -354,6 +458,10 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "serve":
+        if rank == 0:
+            run_serve(args)
+        return
     if args.impl == "reference":
         if rank == 0:
             run_reference(args)

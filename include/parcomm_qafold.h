@@ -66,7 +66,9 @@ int qf_params_info(const qf_params* params, uint64_t* active, uint64_t* logical,
  * BVA padding, keeps the weights and codewords in HBM and writes the block
  * roots (blocks * 32 bytes).  `bva` holds `n_values` signed entries (int8 for
  * F65521, int16 for KoalaBear) in host memory, or in device memory when
- * `bva_on_device` is nonzero.  Both cache modes produce identical bytes. */
+ * `bva_on_device` is nonzero.  The library reads device weights on its own
+ * streams: the caller's writes to them must be complete (synchronise the
+ * stream that produced them) before the call.  Both cache modes produce identical bytes. */
 int qf_commit(const qf_params* params, const void* bva, uint64_t n_values, int bva_on_device, qf_committed** out,
               uint8_t* roots_out);
 void qf_committed_free(qf_committed* committed);
@@ -76,8 +78,9 @@ void qf_committed_free(qf_committed* committed);
  * re-encodes every block.  `host_bva` holds n_values entries in host memory
  * (for weight sets larger than HBM; page-locked memory lets the copies
  * overlap the compute) or in device memory (weights resident, codewords
- * recomputed: a pool of many commitments).  It stays owned by the caller and
- * must stay valid and unchanged until the committed handle is freed.  Every pass that reads the
+ * recomputed: a pool of many commitments; its producer must have finished
+ * writing it, as for qf_commit).  It stays owned by the caller and must stay
+ * valid and unchanged until the committed handle is freed.  Every pass that reads the
  * weights (commit, EO cross terms and witness, projection, block fold) stages
  * them into HBM one PCS block at a time, and binding re-encodes each block
  * and checks its root.  The first resident_bytes / (2^chunk_log * entry size)

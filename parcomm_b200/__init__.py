@@ -105,6 +105,14 @@ def lib() -> ctypes.CDLL:
     return _lib
 
 
+def _ready(t) -> None:
+    """The library reads device weights on its own streams: the stream that
+    produced a CUDA tensor must have finished writing it."""
+    if getattr(t, "is_cuda", False):
+        import torch
+        torch.cuda.current_stream(t.device).synchronize()
+
+
 def _check(rc: int) -> None:
     if rc != 0:
         buf = ctypes.create_string_buffer(4096)
@@ -280,6 +288,7 @@ class Parameters:
         if on_device:
             if int(values.element_size()) != np.dtype(self.weight_dtype).itemsize:
                 raise QfError(-9, f"device weights must be {np.dtype(self.weight_dtype).name}")
+            _ready(values)
             ptr, n = int(values.data_ptr()), int(values.numel())
         else:
             arr = np.ascontiguousarray(values, dtype=self.weight_dtype)
@@ -302,6 +311,7 @@ class Parameters:
         if hasattr(values, "data_ptr"):
             if int(values.element_size()) != np.dtype(self.weight_dtype).itemsize or not values.is_contiguous():
                 raise QfError(-9, f"host weights must be contiguous {np.dtype(self.weight_dtype).name}")
+            _ready(values)
             keep, ptr, n = values, int(values.data_ptr()), int(values.numel())
         else:
             keep = np.ascontiguousarray(values, dtype=self.weight_dtype)

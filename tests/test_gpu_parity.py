@@ -299,3 +299,22 @@ def test_open_keeps_the_commitment_for_repeated_claims(mode):
         assert proof.to_bytes() == o_proof, f"opening {k} differs"
         p.verify(c.roots, claims, proof)
     c.close()
+
+
+def test_device_weights_written_just_before_commit():
+    """Weights produced by torch kernels still in flight: the commit must see
+    the finished tensor (the mirror synchronises the producer stream)."""
+    import torch
+    p = qf.Parameters([(4096, 4096)], qf.Config(chunk_log=22, packed_log=4))
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    roots = []
+    for mode in ("cache", "recompute"):
+        w = torch.randint(-127, 128, (4096 * 4096,), generator=g, device="cuda", dtype=torch.int32)
+        w = (w * 3 + 1).clamp_(-127, 127).to(torch.int8)  # more work queued on torch's stream
+        c = p.commit(w, on_device=True) if mode == "cache" else p.commit_recomputed(w)
+        ref = p.commit(w.cpu().numpy())
+        assert c.roots == ref.roots, mode
+        roots.append(c.roots)
+        c.close()
+        ref.close()
