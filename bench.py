@@ -314,8 +314,12 @@ def run_serve(args):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     load_s = time.time() - t0
+    # The engine budgets HBM itself: bound the library's cache of released
+    # buffers and keep it, plus headroom for torch, outside the budget.
+    cache = 16 << 30
+    qf.device_cache_limit(cache)
     free_b, total_b = torch.cuda.mem_get_info()
-    budget = int(free_b - (8 << 30))  # headroom for torch and the library's own tables
+    budget = int(free_b - cache - (8 << 30))
     keys = pool.keys()
 
     def make_requests(n, seed):
@@ -358,7 +362,8 @@ def run_serve(args):
         "dtype": "int8",
         "config": {"workload": "serving loop (C5)", "pool": [n for n, *_ in sets], "pool_matrices": len(pool),
                    "pool_weights": pool_weights, "field": "F65521^8", "slots": args.slots,
-                   "hbm_budget_bytes": budget, "requests_per_rate": args.serve_requests,
+                   "hbm_budget_bytes": budget, "device_cache_limit_bytes": cache,
+                   "requests_per_rate": args.serve_requests,
                    "open": "1-64 random pooled matrices, fresh uniform points, one proof each (qf_open)",
                    "commit": "10%: new int8 matrix, 1024-28672 rows x 4096/8192 cols, recompute mode",
                    "scale": args.serve_scale},

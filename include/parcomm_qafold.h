@@ -136,6 +136,14 @@ void qf_free_bytes(uint8_t* bytes);
 int qf_kernel_timing(int enable);
 int qf_kernel_stats(char* buf, size_t cap, size_t* len);
 uint64_t qf_kernel_launches(void);
+
+/* Device buffers released by the library are cached for reuse (no cudaMalloc
+ * on repeated proofs); at most `bytes` stay cached, the rest is freed at once
+ * (default: unlimited).  A request that does not fit frees the cache and
+ * retries, waiting up to half a second for concurrent work to release memory.
+ * A caller that budgets HBM itself (a serving loop) sets a limit.  No
+ * reference counterpart. */
+int qf_device_cache_limit(uint64_t bytes);
 size_t qf_last_error(char* buf, size_t cap);
 
 /* No counterpart in the reference: a commitment entry point that allocates

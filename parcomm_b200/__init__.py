@@ -60,7 +60,7 @@ EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
     "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
-    "qf_committed_stream_info", "qf_open",
+    "qf_committed_stream_info", "qf_open", "qf_device_cache_limit",
 )
 
 
@@ -97,6 +97,7 @@ def lib() -> ctypes.CDLL:
         L.qf_kernel_stats.argtypes = [ctypes.c_char_p, S, ctypes.POINTER(S)]
         L.qf_kernel_launches.argtypes = []
         L.qf_kernel_launches.restype = U64
+        L.qf_device_cache_limit.argtypes = [U64]
         L.qf_commit_block_noalloc.argtypes = [P, P, U64, U64, P, P]
         for name in EXPORTED:
             if not hasattr(L, name):
@@ -404,6 +405,11 @@ def kernel_stats() -> dict:
     buf = ctypes.create_string_buffer(n.value + 1)
     _check(lib().qf_kernel_stats(buf, n.value + 1, ctypes.byref(n)))
     return json.loads(buf.raw[: n.value].decode())
+
+
+def device_cache_limit(nbytes: int) -> None:
+    """At most `nbytes` of released device buffers stay cached for reuse."""
+    _check(lib().qf_device_cache_limit(int(nbytes)))
 
 
 def kernel_launches() -> int:

@@ -178,6 +178,10 @@ int qf_kernel_stats(char* buf, size_t cap, size_t* len) {
 
 uint64_t qf_kernel_launches(void) { return qfg::KernelClock::launches.load(); }
 
+int qf_device_cache_limit(uint64_t bytes) {
+  return guarded([&] { qfg::DevicePool::set_limit(size_t(bytes)); });
+}
+
 size_t qf_last_error(char* buf, size_t cap) {
   if (buf && cap) {
     size_t n = std::min(cap - 1, qfc::g_last_error.size());

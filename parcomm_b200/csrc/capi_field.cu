@@ -342,6 +342,7 @@ std::vector<uint8_t> prove(const qf_params* params, qf_committed* committed, con
     std::vector<uint8_t> ctx = opening_context<F>(t.state, 0);
     BatchOpening<F> op = fc->roots.size() > 1 ? open_batch(P.pcs, *fc->be, fc->roots, term.point_msb, ctx)
                                                     : open_single(P.pcs, *fc->be, fc->roots[0], term.point_msb, ctx);
+    fc->be->release_opening_state();
     check(op.claimed_value * term.scale == term.value, "QAFold/EO terminal mismatch");
     Proof<F> pr;
     pr.eo = std::move(eo);

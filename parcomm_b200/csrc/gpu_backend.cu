@@ -132,6 +132,18 @@ GpuBackend::GpuBackend(const Parameters<F>& p, BlockStream* src, cudaStream_t s,
 }
 GpuBackend::~GpuBackend() {}
 
+void GpuBackend::release_opening_state() {
+  QF_CK(cudaStreamSynchronize(s_));
+  for (DBuf<Fe>* b : {&weights_, &values_, &tmp_v_, &tmp_w_, &wit_, &qv_, &wit2_, &qv2_, &rw_d_}) b->reset();
+  folded_.reset();
+  scratch_.reset();
+  single_cw_ = nullptr;
+  open_cw_ = nullptr;
+  sum_len_ = 0;
+  eo_len_ = 0;
+  msg_valid_ = false;
+}
+
 // ---------------------------------------------------------------- streamed weights
 BlockStream::BlockStream(const W* host, uint64_t active, uint64_t block_len, size_t resident, int slots)
     : host_(host), active_(active), block_len_(block_len) {

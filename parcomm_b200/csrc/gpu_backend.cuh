@@ -117,6 +117,11 @@ class GpuBackend : public Backend<F>,
   // Commits every block of a streamed backend in one pass over the weights;
   // `per_block` runs after each live block's launches (same stream).
   std::vector<Digest> commit_streamed(const BlockStream::BlockFn& per_block);
+  // Returns the buffers of the last opening (tables, folded codeword, the
+  // sumcheck and EO vectors, a re-encoded block) to the pool: a commitment
+  // that waits for its next opening keeps only its own weights, codewords
+  // and trees.
+  void release_opening_state();
   ~GpuBackend() override;
 
   // commit

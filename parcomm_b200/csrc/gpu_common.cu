@@ -2,14 +2,18 @@
 #include "gpu_common.cuh"
 
 #include <algorithm>
+#include <chrono>
 #include <map>
 #include <mutex>
+#include <thread>
 
 namespace qfg {
 
 namespace {
 std::mutex g_pool_mu;
 std::multimap<std::pair<int, size_t>, void*> g_pool;  // (device, rounded bytes) -> free device block
+size_t g_pool_bytes = 0;                               // cached, all devices
+size_t g_pool_limit = ~size_t(0);
 int current_device() {
   int d = 0;
   QF_CK(cudaGetDevice(&d));
@@ -26,21 +30,41 @@ void* DevicePool::get(size_t bytes) {
     if (it != g_pool.end()) {
       void* p = it->second;
       g_pool.erase(it);
+      g_pool_bytes -= r;
       return p;
     }
   }
+  // On failure: return the cache to the driver and retry; then, for up to
+  // half a second, wait for buffers that concurrent work is about to release.
   void* p = nullptr;
-  if (cudaMalloc(&p, r) != cudaSuccess) {
+  for (int attempt = 0;; ++attempt) {
+    const cudaError_t e = cudaMalloc(&p, r);
+    if (e == cudaSuccess) return p;
     cudaGetLastError();
-    trim();
-    QF_CK(cudaMalloc(&p, r));
+    if (attempt >= 100) QF_CK(e);
+    if (attempt == 0 || cached_bytes() > 0) trim();
+    else std::this_thread::sleep_for(std::chrono::milliseconds(5));
   }
-  return p;
 }
 void DevicePool::put(void* p, size_t bytes) {
   const int dev = current_device();
-  std::lock_guard<std::mutex> g(g_pool_mu);
-  g_pool.emplace(std::make_pair(dev, rounded(bytes)), p);
+  const size_t r = rounded(bytes);
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    if (g_pool_bytes + r <= g_pool_limit) {
+      g_pool.emplace(std::make_pair(dev, r), p);
+      g_pool_bytes += r;
+      return;
+    }
+  }
+  cudaFree(p);  // over the cache limit
+}
+void DevicePool::set_limit(size_t bytes) {
+  {
+    std::lock_guard<std::mutex> g(g_pool_mu);
+    g_pool_limit = bytes;
+  }
+  if (cached_bytes() > bytes) trim();
 }
 // Frees the current device's cached blocks.
 void DevicePool::trim() {
@@ -50,6 +74,7 @@ void DevicePool::trim() {
   for (auto it = g_pool.begin(); it != g_pool.end();) {
     if (it->first.first == dev) {
       cudaFree(it->second);
+      g_pool_bytes -= it->first.second;
       it = g_pool.erase(it);
     } else {
       ++it;

@@ -68,6 +68,9 @@ struct DevicePool {
   static void put(void* p, size_t bytes);
   static void trim();
   static size_t cached_bytes();  // held in the cache for the current device
+  // At most `bytes` stay cached (all devices); further released blocks are
+  // freed at once.  Unlimited by default.
+  static void set_limit(size_t bytes);
   static size_t rounded(size_t bytes) {
     const size_t g = bytes >= (size_t(1) << 20) ? (size_t(1) << 20) : 256;
     return (bytes + g - 1) / g * g;

@@ -107,7 +107,8 @@ class Pool:
         p = self.params_for(shape, config)
         bva = layout_bva(p, weights)
         c = p.commit_recomputed(bva) if recompute else p.commit(bva, on_device=True)
-        e = PoolEntry(next(self._keys), shape, p, c, recompute, bva)
+        # Cache mode copies the weights into the commitment; recompute mode reads them in place.
+        e = PoolEntry(next(self._keys), shape, p, c, recompute, bva if recompute else None)
         with self._mu:
             self._entries[e.key] = e
         return e
