@@ -250,20 +250,119 @@ static void wht_tile_launch(cudaStream_t s, const Fe* src, Fe* dst, const Fe* al
     qfd::k_wht_tile<false><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(src, dst, nullptr, logR, wl, tiles);
 }
 
+// 2^cb consecutive group bases per tile of a k-level strided pass: 64-byte
+// runs at k = 10, the full 4096-element tile below that.
+static int strided_cb(int k, int logm) { return std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k); }
+
+// ---------------------------------------------------------------- pass autotuner
+// How many levels each strided pass takes is a choice: one deep pass is
+// issue-bound (its middle stages run on the ALU and shared memory), a shallow
+// one runs near copy speed but adds a pass over HBM.  The tuner times one
+// pass of every depth k = 1..10 of each transform once per process, on a
+// 2^24-element proxy half (256 MiB, past L2) with the access pattern of the
+// real passes, and splits a span of levels into the cheapest sequence of
+// depths (dynamic programming over the measured costs).  Any split gives the
+// same bytes.  QF_TUNE=0 keeps the greedy split (depth 10, then the rest).
+namespace {
+struct PassTuner {
+  std::mutex mu;
+  std::atomic<bool> ready{false};
+  float ms[2][11] = {};  // [op][k]: one pass over the proxy
+  std::map<std::pair<int, int>, std::vector<int>> plans;  // (op, span) -> depths
+
+  static bool enabled() {
+    const char* e = std::getenv("QF_TUNE");
+    return !(e && e[0] == '0');
+  }
+
+  template <int OP>
+  float time_pass(cudaStream_t s, Fe* buf, int k) {
+    constexpr int kLogm = 24, kLo = 12;
+    const int cb = strided_cb(k, kLogm);
+    const uint32_t tiles = uint32_t(uint64_t(1) << (kLogm - k - cb));
+    cudaEvent_t a, b;
+    QF_CK(cudaEventCreate(&a));
+    QF_CK(cudaEventCreate(&b));
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      QF_CK(cudaEventRecord(a, s));
+      qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(buf, kLogm, kLo, k, cb, tiles);
+      QF_CK(cudaGetLastError());
+      QF_CK(cudaEventRecord(b, s));
+      QF_CK(cudaEventSynchronize(b));
+      float t = 0;
+      QF_CK(cudaEventElapsedTime(&t, a, b));
+      if (rep) best = std::min(best, t);  // the first run warms up
+    }
+    QF_CK(cudaEventDestroy(a));
+    QF_CK(cudaEventDestroy(b));
+    return best;
+  }
+
+  void tune(cudaStream_t s) {
+    std::lock_guard<std::mutex> g(mu);
+    if (ready) return;
+    DBuf<Fe> buf(size_t(1) << 24);
+    QF_CK(cudaMemsetAsync(buf.p, 0, (size_t(1) << 24) * 16, s));
+    std::string note;
+    for (int k = 1; k <= 10; ++k) {
+      ms[qfd::kMobius][k] = time_pass<qfd::kMobius>(s, buf.p, k);
+      ms[qfd::kWht][k] = time_pass<qfd::kWht>(s, buf.p, k);
+      char b[96];
+      std::snprintf(b, sizeof b, "%s\"%d\":[%.4f,%.4f]", k > 1 ? "," : "", k, ms[qfd::kMobius][k], ms[qfd::kWht][k]);
+      note += b;
+    }
+    KernelClock::note("strided_pass_ms_per_2^24_mobius_wht", "{" + note + "}");
+    ready = true;
+  }
+
+  // Depths for `span` levels: measured optimum, or greedy before tuning.
+  std::vector<int> plan(int op, int span) {
+    std::vector<int> greedy;
+    for (int left = span; left > 0; left -= std::min(10, left)) greedy.push_back(std::min(10, left));
+    if (!ready) return greedy;
+    std::lock_guard<std::mutex> g(mu);
+    auto key = std::make_pair(op, span);
+    auto it = plans.find(key);
+    if (it != plans.end()) return it->second;
+    std::vector<float> best(span + 1, 1e30f);
+    std::vector<int> pick(span + 1, 0);
+    best[0] = 0;
+    for (int s = 1; s <= span; ++s)
+      for (int k = 1; k <= std::min(10, s); ++k)
+        if (best[s - k] + ms[op][k] < best[s]) { best[s] = best[s - k] + ms[op][k]; pick[s] = k; }
+    std::vector<int> out;
+    for (int s = span; s > 0; s -= pick[s]) out.push_back(pick[s]);
+    std::string desc;
+    for (int k : out) desc += (desc.empty() ? "" : "+") + std::to_string(k);
+    KernelClock::note(std::string(op == qfd::kMobius ? "plan_mobius_" : "plan_wht_") + std::to_string(span), "\"" + desc + "\"");
+    return plans.emplace(key, out).first->second;
+  }
+};
+PassTuner g_tuner;
+}  // namespace
+
 // Butterfly levels [from, to) over a half (message or parity at `base`) of
-// 2^logm entries, in strided passes of at most 10 levels.  `to` is logR for
-// the per-column WHT and logm for the Mobius transform of the whole message.
+// 2^logm entries, in strided passes of at most 10 levels (the tuner's split).
+// `to` is logR for the per-column WHT and logm for the Mobius transform of the
+// whole message.  `allow_tuning` is false on the allocation-free path.
 template <int OP>
-static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int from, int to) {
-  for (int lo = from; lo < to;) {
-    const int k = std::min(10, to - lo);
-    // 2^cb consecutive group bases per tile: 64-byte runs at k = 10, the
-    // full 4096-element tile below that.
-    const int cb = std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k);
-    const size_t smem = qfd::kTileSmem;
-    QF_LAUNCH(s, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
-              qfd::k_butterfly_strided<OP><<<tile_grid(uint64_t(1) << (logm - k - cb)), qfd::kTileThreads, smem, s>>>(
-                  base, logR, lo, k, cb, uint32_t(uint64_t(1) << (logm - k - cb))));
+static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int from, int to, bool timed = true,
+                           bool allow_tuning = true) {
+  if (to <= from) return;
+  if (allow_tuning && PassTuner::enabled() && !g_tuner.ready) g_tuner.tune(s);
+  int lo = from;
+  for (int k : g_tuner.plan(OP, to - from)) {
+    const int cb = strided_cb(k, logm);
+    const uint32_t tiles = uint32_t(uint64_t(1) << (logm - k - cb));
+    if (timed) {
+      QF_LAUNCH(s, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
+                qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(
+                    base, logR, lo, k, cb, tiles));
+    } else {
+      qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(base, logR, lo, k, cb, tiles);
+      QF_CK(cudaGetLastError());
+    }
     lo += k;
   }
 }
@@ -386,14 +485,7 @@ std::vector<Digest> GpuBackend::commit_streamed(const BlockStream::BlockFn& per_
 // per-launch timers and into caller-owned buffers.
 template <int OP>
 static void strided_passes_plain(cudaStream_t s, Fe* base, int logR, int logm, int from, int to) {
-  for (int lo = from; lo < to;) {
-    const int k = std::min(10, to - lo);
-    const int cb = std::min(k >= 10 ? 2 : qfd::kMaxTileLog - k, logm - k);
-    qfd::k_butterfly_strided<OP><<<tile_grid(uint64_t(1) << (logm - k - cb)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
-        base, logR, lo, k, cb, uint32_t(uint64_t(1) << (logm - k - cb)));
-    QF_CK(cudaGetLastError());
-    lo += k;
-  }
+  strided_passes<OP>(s, base, logR, logm, from, to, false, false);
 }
 
 void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,

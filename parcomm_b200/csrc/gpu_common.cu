@@ -117,6 +117,15 @@ void KernelClock::reset(bool on) {
   ::qf::Sections::reset(on);
   enabled = on;
 }
+namespace {
+std::mutex g_notes_mu;
+std::map<std::string, std::string> g_notes;
+}  // namespace
+void KernelClock::note(const std::string& key, const std::string& json_value) {
+  std::lock_guard<std::mutex> g(g_notes_mu);
+  g_notes[key] = json_value;
+}
+
 std::string KernelClock::stats_json() {
   QF_CK(cudaDeviceSynchronize());
   std::lock_guard<std::mutex> g(mu);
@@ -171,6 +180,18 @@ std::string KernelClock::stats_json() {
     std::snprintf(buf, sizeof buf, "\"host:%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":0}", k.c_str(),
                   (unsigned long long)v.first, v.second);
     s += buf;
+  }
+  std::lock_guard<std::mutex> gn(g_notes_mu);
+  if (!g_notes.empty()) {
+    if (!first) s += ",";
+    first = false;
+    s += "\"_notes\":{";
+    bool f2 = true;
+    for (auto& [k, v] : g_notes) {
+      s += (f2 ? "\"" : ",\"") + k + "\":" + v;
+      f2 = false;
+    }
+    s += "}";
   }
   return s + "}";
 }

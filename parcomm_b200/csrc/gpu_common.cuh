@@ -46,6 +46,8 @@ struct KernelClock {
   static std::atomic<uint64_t> launches;
   static void reset(bool on);
   static std::string stats_json();
+  // A named JSON value reported under "_notes" in stats_json (tuning results).
+  static void note(const std::string& key, const std::string& json_value);
 };
 
 // Host wall time of named sections (recorded while KernelClock is enabled).
