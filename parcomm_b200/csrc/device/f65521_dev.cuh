@@ -88,6 +88,36 @@ QFD_HD Fr mul(const Fr& a, const Fr& b) {
   for (int k = 0; k < 8; ++k) out.c[k] = red40(r[k]);
   return out;
 }
+// Lazy sums of products: a product adds at most eight terms below 2^36.1 to
+// each raw coefficient (below 2^39.1), so a 64-bit accumulator takes 2^24
+// products before it could overflow; it is reduced once at the end (two
+// folds of 2^16 = 15 bring any u64 below 2^40, then red40).
+struct Acc {
+  uint64_t c[8];
+};
+QFD_HD Acc acc_zero() { Acc r; for (int k = 0; k < 8; ++k) r.c[k] = 0; return r; }
+QFD_HD void mul_acc(Acc& r, const Fr& a, const Fr& b) {
+  uint32_t b17[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) b17[j] = 17u * b.c[j];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (i + j < 8) r.c[i + j] += uint64_t(a.c[i]) * b.c[j];
+      else r.c[i + j - 8] += uint64_t(a.c[i]) * b17[j];
+    }
+}
+QFD_HD Fr acc_reduce(const Acc& r) {
+  Fr out;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    uint64_t v = (r.c[k] & 0xffffu) + 15u * (r.c[k] >> 16);
+    v = (v & 0xffffu) + 15u * (v >> 16);
+    out.c[k] = red40(v);
+  }
+  return out;
+}
 QFD_HD Fr mul_base(const Fr& a, uint32_t s) {
   Fr r;
   for (int i = 0; i < 8; ++i) r.c[i] = red32(a.c[i] * s);

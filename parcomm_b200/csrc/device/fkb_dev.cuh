@@ -82,6 +82,14 @@ QFD_HD Fr mul(const Fr& a, const Fr& b) {
   for (int k = 0; k < 4; ++k) out.c[k] = red64(r[k]);
   return out;
 }
+// Sums of products: one product already fills a 64-bit raw coefficient, so
+// each product is reduced and added (the F65521 header keeps them lazy).
+struct Acc {
+  Fr v;
+};
+QFD_HD Acc acc_zero() { Acc r; r.v = zero(); return r; }
+QFD_HD void mul_acc(Acc& r, const Fr& a, const Fr& b) { r.v = add(r.v, mul(a, b)); }
+QFD_HD Fr acc_reduce(const Acc& r) { return r.v; }
 QFD_HD Fr mul_base(const Fr& a, uint32_t s) {
   Fr r;
   for (int i = 0; i < 4; ++i) r.c[i] = red64(uint64_t(a.c[i]) * s);

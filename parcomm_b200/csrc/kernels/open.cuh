@@ -187,13 +187,15 @@ __global__ void k_scatter_add(const uint64_t* __restrict__ idx, const Fe* __rest
 
 // dot(w, q) and the first binary cross pair.
 __global__ void k_eo_dot_cross(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n, Fe* __restrict__ partials) {
-  Fr v[3] = {zero(), zero(), zero()};
+  Acc acc[3] = {acc_zero(), acc_zero(), acc_zero()};
   for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < n / 2; j += uint64_t(gridDim.x) * blockDim.x) {
     Fr w0 = load(w + 2 * j), w1 = load(w + 2 * j + 1), q0 = load(q + 2 * j), q1 = load(q + 2 * j + 1);
-    v[0] = add(v[0], add(mul(w0, q0), mul(w1, q1)));
-    v[1] = add(v[1], mul(w0, q1));
-    v[2] = add(v[2], mul(w1, q0));
+    mul_acc(acc[0], w0, q0);
+    mul_acc(acc[0], w1, q1);
+    mul_acc(acc[1], w0, q1);
+    mul_acc(acc[2], w1, q0);
   }
+  Fr v[3] = {acc_reduce(acc[0]), acc_reduce(acc[1]), acc_reduce(acc[2])};
   block_reduce<3>(v);
   if (threadIdx.x == 0)
 #pragma unroll
@@ -204,7 +206,7 @@ __global__ void k_eo_dot_cross(const Fe* __restrict__ w, const Fe* __restrict__ 
 __global__ void k_eo_fold_cross(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n, Fe inv, Fe ch,
                                 Fe* __restrict__ w_out, Fe* __restrict__ q_out, Fe* __restrict__ partials) {
   const Fr fi = load(&inv), fc = load(&ch);
-  Fr v[2] = {zero(), zero()};
+  Acc acc[2] = {acc_zero(), acc_zero()};
   if (n == 2) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       store(w_out, add(load(w), mul(load(w + 1), fi)));
@@ -220,10 +222,11 @@ __global__ void k_eo_fold_cross(const Fe* __restrict__ w, const Fe* __restrict__
       store(w_out + 2 * j + 1, a1);
       store(q_out + 2 * j, b0);
       store(q_out + 2 * j + 1, b1);
-      v[0] = add(v[0], mul(a0, b1));
-      v[1] = add(v[1], mul(a1, b0));
+      mul_acc(acc[0], a0, b1);
+      mul_acc(acc[1], a1, b0);
     }
   }
+  Fr v[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(v);
   if (threadIdx.x == 0)
 #pragma unroll
@@ -242,7 +245,7 @@ __global__ void k_eo_fold_vec(const Fe* __restrict__ w, uint64_t n, Fe f, Fe* __
 __global__ void k_eo_fold_query_cross(const Fe* __restrict__ wf, const Fe* __restrict__ q, uint64_t n, Fe ch,
                                       Fe* __restrict__ q_out, Fe* __restrict__ partials) {
   const Fr fc = load(&ch);
-  Fr v[2] = {zero(), zero()};
+  Acc acc[2] = {acc_zero(), acc_zero()};
   if (n == 2) {
     if (blockIdx.x == 0 && threadIdx.x == 0) store(q_out, add(load(q), mul(load(q + 1), fc)));
   } else {
@@ -252,10 +255,11 @@ __global__ void k_eo_fold_query_cross(const Fe* __restrict__ wf, const Fe* __res
       const Fr b1 = add(load(q + 4 * j + 2), mul(load(q + 4 * j + 3), fc));
       store(q_out + 2 * j, b0);
       store(q_out + 2 * j + 1, b1);
-      v[0] = add(v[0], mul(a0, b1));
-      v[1] = add(v[1], mul(a1, b0));
+      mul_acc(acc[0], a0, b1);
+      mul_acc(acc[1], a1, b0);
     }
   }
+  Fr v[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(v);
   if (threadIdx.x == 0)
 #pragma unroll
@@ -296,12 +300,13 @@ __global__ void k_apply_images(Fe* __restrict__ weights, uint64_t m, const Fe* _
 // sum (v_{i+h} - v_i)(w_{i+h} - w_i) (round_message, packed.rs:652-667).
 __global__ void k_sum_message(const Fe* __restrict__ v, const Fe* __restrict__ w, uint64_t n, Fe* __restrict__ partials) {
   const uint64_t h = n / 2;
-  Fr s[2] = {zero(), zero()};
+  Acc acc[2] = {acc_zero(), acc_zero()};
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < h; i += uint64_t(gridDim.x) * blockDim.x) {
     Fr a = load(v + i), b = load(w + i), c = load(v + i + h), d = load(w + i + h);
-    s[0] = add(s[0], mul(a, b));
-    s[1] = add(s[1], mul(sub(c, a), sub(d, b)));
+    mul_acc(acc[0], a, b);
+    mul_acc(acc[1], sub(c, a), sub(d, b));
   }
+  Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
   if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
 }
@@ -312,7 +317,7 @@ __global__ void k_sum_fold_message(const Fe* __restrict__ v, const Fe* __restric
                                    Fe* __restrict__ v_out, Fe* __restrict__ w_out, Fe* __restrict__ partials) {
   const Fr c = load(&ch);
   const uint64_t h = n / 2, q = n / 4;
-  Fr s[2] = {zero(), zero()};
+  Acc acc[2] = {acc_zero(), acc_zero()};
   if (n == 2) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       Fr a = load(v), b = load(v + 1);
@@ -330,10 +335,11 @@ __global__ void k_sum_fold_message(const Fe* __restrict__ v, const Fe* __restric
       store(v_out + i + q, nv1);
       store(w_out + i, nw0);
       store(w_out + i + q, nw1);
-      s[0] = add(s[0], mul(nv0, nw0));
-      s[1] = add(s[1], mul(sub(nv1, nv0), sub(nw1, nw0)));
+      mul_acc(acc[0], nv0, nw0);
+      mul_acc(acc[1], sub(nv1, nv0), sub(nw1, nw0));
     }
   }
+  Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
   if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
 }
@@ -362,9 +368,10 @@ __global__ void k_gather_paths(const uint4* __restrict__ tree, const uint64_t* _
 __global__ void k_row_project(const Fe* __restrict__ cw, uint64_t n_ext, uint64_t n_rows, const Fe* __restrict__ hi,
                               const Fe* __restrict__ lo, int lb, Fe* __restrict__ partials) {
   const int c = blockIdx.y;
-  Fr s[1] = {zero()};
+  Acc acc = acc_zero();
   for (uint64_t r = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < n_rows; r += uint64_t(gridDim.x) * blockDim.x)
-    s[0] = add(s[0], mul(table_at(hi, lo, lb, r), load(cw + uint64_t(c) * n_ext + r)));
+    mul_acc(acc, table_at(hi, lo, lb, r), load(cw + uint64_t(c) * n_ext + r));
+  Fr s[1] = {acc_reduce(acc)};
   block_reduce<1>(s);
   if (threadIdx.x == 0) store(partials + size_t(c) * gridDim.x + blockIdx.x, s[0]);
 }

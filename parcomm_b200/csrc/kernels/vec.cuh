@@ -27,20 +27,22 @@ __global__ void k_scatter_set(Fe* __restrict__ dst, const uint64_t* __restrict__
 }
 // partial sums of sum_i a[i] * b[i]
 __global__ void k_dot(const Fe* __restrict__ a, const Fe* __restrict__ b, uint64_t n, Fe* __restrict__ partials) {
-  Fr s[1] = {zero()};
+  Acc acc = acc_zero();
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
-    s[0] = add(s[0], mul(load(a + i), load(b + i)));
+    mul_acc(acc, load(a + i), load(b + i));
+  Fr s[1] = {acc_reduce(acc)};
   block_reduce<1>(s);
   if (threadIdx.x == 0) store(partials + blockIdx.x, s[0]);
 }
 // LiteBullet cross pair of (L, R) with half h: sum L[i] R[h+i], sum L[h+i] R[i].
 __global__ void k_lb_cross(const Fe* __restrict__ L, const Fe* __restrict__ R, uint64_t n, Fe* __restrict__ partials) {
   const uint64_t h = n / 2;
-  Fr s[2] = {zero(), zero()};
+  Acc acc[2] = {acc_zero(), acc_zero()};
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < h; i += uint64_t(gridDim.x) * blockDim.x) {
-    s[0] = add(s[0], mul(load(L + i), load(R + h + i)));
-    s[1] = add(s[1], mul(load(L + h + i), load(R + i)));
+    mul_acc(acc[0], load(L + i), load(R + h + i));
+    mul_acc(acc[1], load(L + h + i), load(R + i));
   }
+  Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
   if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
 }
@@ -50,7 +52,7 @@ __global__ void k_lb_cross(const Fe* __restrict__ L, const Fe* __restrict__ R, u
 __global__ void k_lb_fold_cross(Fe* __restrict__ L, Fe* __restrict__ R, uint64_t n, Fe wl, Fe wr, Fe* __restrict__ partials) {
   const Fr fl = load(&wl), fr = load(&wr);
   const uint64_t h = n / 2, q = n / 4;
-  Fr s[2] = {zero(), zero()};
+  Acc acc[2] = {acc_zero(), acc_zero()};
   if (n == 2) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       store(L, add(load(L), mul(load(L + 1), fl)));
@@ -66,10 +68,11 @@ __global__ void k_lb_fold_cross(Fe* __restrict__ L, Fe* __restrict__ R, uint64_t
       store(L + i + q, l1);
       store(R + i, r0);
       store(R + i + q, r1);
-      s[0] = add(s[0], mul(l0, r1));
-      s[1] = add(s[1], mul(l1, r0));
+      mul_acc(acc[0], l0, r1);
+      mul_acc(acc[1], l1, r0);
     }
   }
+  Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
   if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
 }

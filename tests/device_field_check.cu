@@ -52,6 +52,21 @@ int main() {
     bad += qfd::red32(w) != w % 65521u;
     n += 6;
   }
+  // Lazy sums of products: short random runs, and 2^20 products of all-(p-1)
+  // operands (the largest raw coefficient growth) reduced once.
+  for (int run = 0; run < 2000; ++run) {
+    const int len = run < 1999 ? 1 + int(next() % 64) : (1 << 20);
+    const int mode = run == 1999 ? 1 : (run < 200 ? 2 : 0);
+    qfd::Acc acc = qfd::acc_zero();
+    qf::Fp8 want = qf::Fp8::zero();
+    for (int i = 0; i < len; ++i) {
+      const qf::Fp8 a = sample(mode), b = sample(mode);
+      qfd::mul_acc(acc, to_fr(a), to_fr(b));
+      want += a * b;
+    }
+    bad += !same(qfd::acc_reduce(acc), want);
+    ++n;
+  }
   std::printf("{\"checked\": %ld, \"mismatches\": %ld}\n", n, bad);
   return bad != 0;
 }

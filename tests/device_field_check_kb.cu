@@ -66,6 +66,18 @@ int main() {
     for (int k = 0; k < 4; ++k) bad += w.c[k] != qf::Kb4::small(e[k]);
     n += 11;
   }
+  for (int run = 0; run < 500; ++run) {
+    const int len = 1 + int(next() % 64);
+    qfdkb::Acc acc = qfdkb::acc_zero();
+    qf::Kb4 want = qf::Kb4::zero();
+    for (int i = 0; i < len; ++i) {
+      const qf::Kb4 a = sample(run < 50 ? 1 : 0), b = sample(run < 50 ? 1 : 0);
+      qfdkb::mul_acc(acc, to_fr(a), to_fr(b));
+      want += a * b;
+    }
+    bad += !same(qfdkb::acc_reduce(acc), want);
+    ++n;
+  }
   std::printf("{\"checked\": %ld, \"mismatches\": %ld}\n", n, bad);
   return bad != 0;
 }
