@@ -157,70 +157,67 @@ __global__ void k_eo_witness(const Wt* __restrict__ bva, uint64_t active, uint64
 // Raw lane sums of up to kEqBlocks consecutive blocks against the equality
 // weights (project_lanes_from_fn, packed_batch.rs:25-41):
 //   raw[b][j * 4 + k] += sum_i v(b, 4i + j) * weights[i].c[k]
-// A CTA stages kEqChunk weights in shared memory and runs every block over
-// them.  A thread takes 8 elements per block into 16 i64 sums (< 2^49); a
-// warp reduce-scatter leaves each lane pair with one entry (< 2^54), the CTA
-// sum (< 2^57) is reduced to a residue and added to the block's residue
-// total, and `raw` receives one atomic add per entry at the end (a sum of
-// residues over the grid, far below 2^63).
-__global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const Wt* __restrict__ bva, uint64_t active,
-                                                                    uint64_t block_len, uint64_t first_block, int nb,
-                                                                    uint64_t m, const Fe* __restrict__ weights,
-                                                                    unsigned long long* __restrict__ raw) {
-  __shared__ uint4 w_s[kEqChunk];
-  __shared__ long long stage_s[kEqThreads / 32][kEqRaw];
-  __shared__ unsigned long long tot_s[kEqBlocks][kEqRaw];
+// Blocks go two at a time: a thread keeps both blocks' 16 sums in registers
+// over its whole grid-stride range (each weight read once per pair), and the
+// CTA reduces once per pair.  A thread handles at most m / (grid x 256)
+// elements (below 2^11 for the grids the host launches), so a sum stays below
+// 2^57 and a warp sum below 2^62; each warp's sum is reduced to a residue
+// before the warps are added, and `raw` receives one atomic add per entry and
+// CTA (a sum of residues, far below 2^63).
+__global__ void __launch_bounds__(kEqThreads) k_eq_project_blocks(const Wt* __restrict__ bva, uint64_t active,
+                                                                 uint64_t block_len, uint64_t first_block, int nb,
+                                                                 uint64_t m, const Fe* __restrict__ weights,
+                                                                 unsigned long long* __restrict__ raw) {
+  __shared__ long long stage_s[kEqThreads / 32][2 * kEqRaw];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int t = threadIdx.x; t < kEqBlocks * kEqRaw; t += kEqThreads) tot_s[t / kEqRaw][t % kEqRaw] = 0;
-  for (uint64_t c0 = uint64_t(blockIdx.x) * kEqChunk; c0 < m; c0 += uint64_t(gridDim.x) * kEqChunk) {
-    __syncthreads();
-    for (int e = threadIdx.x; e < kEqChunk; e += kEqThreads)
-      w_s[e] = c0 + e < m ? *reinterpret_cast<const uint4*>(weights + c0 + e) : make_uint4(0, 0, 0, 0);
-    __syncthreads();
-    for (int b = 0; b < nb; ++b) {
-      const uint64_t bbase = (first_block + b) * block_len;
-      long long acc[kEqRaw];
+  for (int b0 = 0; b0 < nb; b0 += 2) {
+    const bool two = b0 + 1 < nb;
+    const uint64_t base0 = (first_block + b0) * block_len, base1 = base0 + block_len;
+    long long acc[2][kEqRaw];
 #pragma unroll
-      for (int q = 0; q < kEqRaw; ++q) acc[q] = 0;
-#pragma unroll 2
-      for (int u = 0; u < kEqChunk / kEqThreads; ++u) {
-        const int e = threadIdx.x + u * kEqThreads;
-        const uint2 v4 = c0 + e < m ? load4(bva, active, bbase + 4 * (c0 + e)) : make_uint2(0, 0);
-        const uint4 wq = w_s[e];
-        const uint32_t wc[4] = {wq.x, wq.y, wq.z, wq.w};
+    for (int q = 0; q < kEqRaw; ++q) acc[0][q] = acc[1][q] = 0;
+    for (uint64_t i = uint64_t(blockIdx.x) * kEqThreads + threadIdx.x; i < m; i += uint64_t(gridDim.x) * kEqThreads) {
+      const uint4 wq = *reinterpret_cast<const uint4*>(weights + i);
+      const uint32_t wc[4] = {wq.x, wq.y, wq.z, wq.w};
+      const uint2 v0 = load4(bva, active, base0 + 4 * i);
+      const uint2 v1 = two ? load4(bva, active, base1 + 4 * i) : make_uint2(0, 0);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int v = lane_of(v4, j);
+      for (int j = 0; j < 4; ++j) {
+        const int a = lane_of(v0, j), b = lane_of(v1, j);
 #pragma unroll
-          for (int k = 0; k < 4; ++k) acc[j * 4 + k] = mad_wide(int(wc[k]), v, acc[j * 4 + k]);
+        for (int k = 0; k < 4; ++k) {
+          acc[0][j * 4 + k] = mad_wide(int(wc[k]), a, acc[0][j * 4 + k]);
+          acc[1][j * 4 + k] = mad_wide(int(wc[k]), b, acc[1][j * 4 + k]);
         }
       }
-      // Reduce-scatter: after offset o the lane keeps the half of its entries
-      // selected by (lane & o); after o = 2 lane l holds entry l >> 1, and
-      // the o = 1 exchange completes the sum in both lanes of the pair.
+    }
+    // Reduce-scatter per block: after offset o the lane keeps the half of its
+    // entries selected by (lane & o); after o = 2 lane l holds entry l >> 1,
+    // and the o = 1 exchange completes the sum in both lanes of the pair.
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
 #pragma unroll
       for (int o = 16, n = kEqRaw; o >= 2; o >>= 1, n >>= 1) {
         const bool upper = lane & o;
 #pragma unroll
         for (int q = 0; q < n / 2; ++q) {
-          const long long send = upper ? acc[q] : acc[q + n / 2];
-          const long long keep = upper ? acc[q + n / 2] : acc[q];
-          acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+          const long long send = upper ? acc[h][q] : acc[h][q + n / 2];
+          const long long keep = upper ? acc[h][q + n / 2] : acc[h][q];
+          acc[h][q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
         }
       }
-      acc[0] += __shfl_xor_sync(0xffffffffu, acc[0], 1);
-      if ((lane & 1) == 0) stage_s[warp][lane >> 1] = acc[0];
-      __syncthreads();
-      if (threadIdx.x < kEqRaw) {
-        long long t = 0;
-#pragma unroll
-        for (int w = 0; w < kEqThreads / 32; ++w) t += stage_s[w][threadIdx.x];
-        tot_s[b][threadIdx.x] = (tot_s[b][threadIdx.x] + mod_i64(t)) % P;
-      }
-      __syncthreads();
+      acc[h][0] += __shfl_xor_sync(0xffffffffu, acc[h][0], 1);
+      if ((lane & 1) == 0) stage_s[warp][h * kEqRaw + (lane >> 1)] = acc[h][0];
     }
+    __syncthreads();
+    if (threadIdx.x < (two ? 2 : 1) * kEqRaw) {
+      unsigned long long t = 0;
+#pragma unroll
+      for (int w = 0; w < kEqThreads / 32; ++w) t += mod_i64(stage_s[w][threadIdx.x]);
+      atomicAdd(raw + uint64_t(b0) * kEqRaw + threadIdx.x, t % P);
+    }
+    __syncthreads();
   }
-  for (int t = threadIdx.x; t < nb * kEqRaw; t += kEqThreads) atomicAdd(raw + t, tot_s[t / kEqRaw][t % kEqRaw]);
 }
 
 // Block fold of the packed payloads (packed_batch.rs:213-236): values[i] =
