@@ -66,6 +66,16 @@ QFD_HD uint32_t red40(uint64_t v) {
   f = (f & 0xffffu) + 15u * (f >> 16);
   return f >= P ? f - P : f;
 }
+// A signed v with |v| < 2^62: adding kBias (the multiple of p just above
+// 2^62) gives an unsigned value below 2^64 with the same residue; two folds
+// of 2^16 = 15 bring it below 2^40 for red40.
+constexpr uint64_t kBias = ((uint64_t(1) << 62) / P + 1) * P;
+QFD_HD uint32_t red_signed(int64_t v) {
+  uint64_t u = uint64_t(v) + kBias;
+  u = (u & 0xffffu) + 15u * (u >> 16);
+  u = (u & 0xffffu) + 15u * (u >> 16);
+  return red40(u);
+}
 QFD_HD Fr mul(const Fr& a, const Fr& b) {
   // X^8 = 17: the wrap-around products take 17 * b_j (< 2^21, unreduced), so
   // output coefficient k is one sum of eight products a_i * b'_j < 2^37,

@@ -44,6 +44,10 @@ QFD_HD uint32_t red64(uint64_t v) {
 }
 QFD_HD uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 QFD_HD uint32_t red32(uint32_t v) { return v >= P ? v - P : v; }  // v < 2p
+// A signed v with |v| < 2^62: adding kBias (the multiple of p just above
+// 2^62) gives the same residue as an unsigned value below 2^64.
+constexpr uint64_t kBias = ((uint64_t(1) << 62) / P + 1) * P;
+QFD_HD uint32_t red_signed(int64_t v) { return red64(uint64_t(v) + kBias); }
 // Canonical a, b < p < 2^31.  The sum is below 2^32, and s - p wraps above
 // s exactly when s < p, so the unsigned minimum picks the reduced value; for
 // the difference, a - b wraps above a - b + p exactly when a < b.

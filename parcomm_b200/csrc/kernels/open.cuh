@@ -16,10 +16,8 @@
 namespace QFD_NS {
 
 // ---------------------------------------------------------------- reductions
-__device__ __forceinline__ uint32_t mod_i64(int64_t v) {
-  int64_t r = v % int64_t(P);
-  return uint32_t(r < 0 ? r + int64_t(P) : r);
-}
+// Exact signed sums to canonical form; every caller keeps |v| < 2^62.
+__device__ __forceinline__ uint32_t mod_i64(int64_t v) { return red_signed(v); }
 __device__ __forceinline__ Fr shfl_xor(const Fr& v, int m) {
   Fr r;
 #pragma unroll

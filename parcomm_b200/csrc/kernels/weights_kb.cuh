@@ -121,10 +121,39 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __rest
 }
 
 // ---------------------------------------------------------------- EO
+// One full row of L payloads (L a multiple of 8, the row 16-byte aligned):
+// 16-byte loads of eight payloads, two accumulator chains (even and odd
+// lanes) so consecutive multiply-adds do not wait on each other.
+template <int L>
+__device__ __forceinline__ void witness_row(const Wt* __restrict__ row, const Fe* pw, long long (&acc)[kC]) {
+  long long a2[kC];
+#pragma unroll
+  for (int k = 0; k < kC; ++k) a2[k] = 0;
+#pragma unroll 2
+  for (int c = 0; c < L / 8; ++c) {
+    const uint4 u = *reinterpret_cast<const uint4*>(row + 8 * c);
+    const uint2 lo = make_uint2(u.x, u.y), hi = make_uint2(u.z, u.w);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int v = lane_of(j < 4 ? lo : hi, j & 3);
+      const Fr p = load(pw + 8 * c + j);
+#pragma unroll
+      for (int k = 0; k < kC; ++k) {
+        if (j & 1) a2[k] = mad_wide(int(p.c[k]), v, a2[k]);
+        else acc[k] = mad_wide(int(p.c[k]), v, acc[k]);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kC; ++k) acc[k] += a2[k];
+}
+
 // Packed EO witness (eo.rs:119-132): witness[row] = sum_lane v(row * stride +
-// lane) * inv_powers[lane], stride <= 64, so a sum is below 2^52.
-__global__ void k_eo_witness(const Wt* __restrict__ bva, uint64_t active, uint64_t rows, int stride,
-                             const Fe* __restrict__ inv_powers, Fe* __restrict__ witness) {
+// lane) * inv_powers[lane], stride <= 64, so a sum is below 2^52.  Full rows
+// of 16 or 64 payloads take the unrolled path; the rest the generic loop.
+__global__ void __launch_bounds__(256, 2) k_eo_witness(const Wt* __restrict__ bva, uint64_t active, uint64_t rows,
+                                                       int stride, const Fe* __restrict__ inv_powers,
+                                                       Fe* __restrict__ witness) {
   __shared__ Fe pw[64];
   if (threadIdx.x < stride) pw[threadIdx.x] = inv_powers[threadIdx.x];
   __syncthreads();
@@ -133,7 +162,11 @@ __global__ void k_eo_witness(const Wt* __restrict__ bva, uint64_t active, uint64
 #pragma unroll
     for (int k = 0; k < kC; ++k) acc[k] = 0;
     const uint64_t g0 = row * stride;
-    if (g0 < active) {
+    if (stride == 16 && g0 + 16 <= active) {
+      witness_row<16>(bva + g0, pw, acc);
+    } else if (stride == 64 && g0 + 64 <= active) {
+      witness_row<64>(bva + g0, pw, acc);
+    } else if (g0 < active) {
       for (int l0 = 0; l0 < stride; l0 += 4) {
         const int n = stride - l0 < 4 ? stride - l0 : 4;
         const uint2 u = n == 4 ? load4(bva, active, g0 + l0) : make_uint2(0, 0);
@@ -231,24 +264,33 @@ __global__ void k_block_fold(const Wt* __restrict__ bva, uint64_t active, uint64
   for (int t = threadIdx.x; t < blocks * kC; t += blockDim.x) t_s[t] = T[t];
   __syncthreads();
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
-    long long acc[kC];
+    // Four blocks' loads are issued before their products; even and odd
+    // lanes feed two accumulator chains.
+    long long acc[2][kC];
 #pragma unroll
-    for (int k = 0; k < kC; ++k) acc[k] = 0;
-    for (int b = 0; b < blocks; ++b) {
-      const uint64_t g = uint64_t(b) * block_len + 4 * i;
-      if (g >= active) break;  // later blocks start even later
-      const uint2 v4 = load4(bva, active, g);
+    for (int k = 0; k < kC; ++k) acc[0][k] = acc[1][k] = 0;
+    for (int b = 0; b < blocks && uint64_t(b) * block_len + 4 * i < active; b += 4) {
+      uint2 v4[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int v = lane_of(v4, j);
-        const Fr t = load(t_s + b * kC + j);
+      for (int q = 0; q < 4; ++q) {
+        const uint64_t g = uint64_t(b + q) * block_len + 4 * i;
+        v4[q] = (b + q < blocks && g < active) ? load4(bva, active, g) : make_uint2(0, 0);
+      }
 #pragma unroll
-        for (int k = 0; k < kC; ++k) acc[k] = mad_wide(int(t.c[k]), v, acc[k]);
+      for (int q = 0; q < 4; ++q) {
+        if (b + q >= blocks) break;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int v = lane_of(v4[q], j);
+          const Fr t = load(t_s + (b + q) * kC + j);
+#pragma unroll
+          for (int k = 0; k < kC; ++k) acc[j & 1][k] = mad_wide(int(t.c[k]), v, acc[j & 1][k]);
+        }
       }
     }
     Fr o;
 #pragma unroll
-    for (int k = 0; k < kC; ++k) o.c[k] = mod_i64(acc[k]);
+    for (int k = 0; k < kC; ++k) o.c[k] = mod_i64(acc[0][k] + acc[1][k]);
     store(values + i, accumulate ? add(load(values + i), o) : o);
   }
 }

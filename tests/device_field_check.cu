@@ -52,6 +52,15 @@ int main() {
     bad += qfd::red32(w) != w % 65521u;
     n += 6;
   }
+  // Signed sums below 2^62 in magnitude.
+  for (int it = 0; it < 200000; ++it) {
+    int64_t v = int64_t(next() >> 2) * ((next() & 1) ? 1 : -1);
+    if (it < 4) v = (it & 1 ? -1 : 1) * ((int64_t(1) << 62) - 1 - it / 2);
+    int64_t want = v % int64_t(65521);
+    if (want < 0) want += 65521;
+    bad += qfd::red_signed(v) != uint32_t(want);
+    ++n;
+  }
   // Lazy sums of products: short random runs, and 2^20 products of all-(p-1)
   // operands (the largest raw coefficient growth) reduced once.
   for (int run = 0; run < 2000; ++run) {

@@ -66,6 +66,14 @@ int main() {
     for (int k = 0; k < 4; ++k) bad += w.c[k] != qf::Kb4::small(e[k]);
     n += 11;
   }
+  for (int it = 0; it < 200000; ++it) {
+    int64_t v = int64_t(next() >> 2) * ((next() & 1) ? 1 : -1);
+    if (it < 4) v = (it & 1 ? -1 : 1) * ((int64_t(1) << 62) - 1 - it / 2);
+    int64_t want = v % int64_t(P);
+    if (want < 0) want += P;
+    bad += qfdkb::red_signed(v) != uint32_t(want);
+    ++n;
+  }
   for (int run = 0; run < 500; ++run) {
     const int len = 1 + int(next() % 64);
     qfdkb::Acc acc = qfdkb::acc_zero();
