@@ -855,12 +855,13 @@ struct TableBuilder {
   DBuf<qfd::TableSpec> dspec;
 };
 
-// One term's tiles: rows of 2^lb (lb <= max_lb), high bits split into mid
-// (<= 2^10) and top.
+// One term's tiles: rows of 2^lb (lb <= min(12, max_lb)), high bits split
+// into mid (<= 2^10) and top.  4096-row tiles amortise each tile's
+// cross-thread reduction over enough products.
 qfd::TermTiles term_tiles(TableBuilder& tb, const std::array<F, 2>* f, size_t nh, uint64_t offset, uint64_t rows,
-                          uint32_t first_tile, const F& scale, size_t max_lb = 10) {
+                          uint32_t first_tile, const F& scale, size_t max_lb = 12) {
   qfd::TermTiles T;
-  const size_t lb = std::min<size_t>(std::min<size_t>(10, max_lb), nh);
+  const size_t lb = std::min<size_t>(std::min<size_t>(12, max_lb), nh);
   const size_t mb = std::min<size_t>(10, nh - lb);
   const uint64_t ntiles = (rows + (uint64_t(1) << lb) - 1) >> lb;
   T.offset = offset;
@@ -878,7 +879,7 @@ uint64_t term_tile_count(const qfd::TermTiles& T) { return (T.rows + (uint64_t(1
 }  // namespace
 
 // Lane projections (tbv.rs:288-352) of large terms: one CTA per tile of up
-// to 1024 rows, tile weights from device-built factor tables.
+// to 4096 rows, tile weights from device-built factor tables.
 std::vector<std::vector<std::vector<F>>> GpuBackend::project_term_groups(
     const std::vector<std::vector<const Term<F>*>>& groups, size_t stride) {
   if (streaming()) return project_groups_streamed(groups, stride);

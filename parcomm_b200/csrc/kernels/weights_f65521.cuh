@@ -33,11 +33,14 @@ __device__ __forceinline__ void byte_planes(const Fe* e, int k, uint32_t& lo, ui
   }
 }
 
+constexpr int kRowBatch = 8;  // rows whose weight loads a projection thread keeps in flight (measured)
+
 // Lane projections (tbv.rs:288-352): out[tile * lanes + l] = high(tile) *
 // sum_r lo[r] * bva[offset + row * lanes + l].  A thread takes min(4, lanes)
-// lanes of a row (one 32-bit load); products accumulate exactly in i32 (at
-// most 128 rows * 128 * 65520 < 2^31 per warp sum: tiles have <= 1024 rows),
-// then in i64 across warps, then reduce once.
+// lanes of a row (one 32-bit load); products accumulate exactly in i32 per
+// thread (a tile has at most 4096 rows, so a thread sums at most 64 rows:
+// 64 * 128 * 65520 < 2^30), then in i64 across threads and warps, then
+// reduce once.
 __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __restrict__ bva, uint64_t active,
                                                                 const TermTiles* __restrict__ terms, int n_terms,
                                                                 uint32_t n_tiles, const Fe* __restrict__ tables,
@@ -66,11 +69,11 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __
 #pragma unroll
       for (int k = 0; k < 8; ++k) acc[j][k] = 0;
     const Fe* lo = tables + T.lo_off;
-    // Four rows per iteration: their loads are issued before any is used.
-    for (int r0 = threadIdx.x / tpr; r0 < nrows; r0 += 4 * rpp) {
-      uint32_t u[4];
+    // kRowBatch rows per iteration: their loads are issued before any is used.
+    for (int r0 = threadIdx.x / tpr; r0 < nrows; r0 += kRowBatch * rpp) {
+      uint32_t u[kRowBatch];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kRowBatch; ++q) {
         const int r = r0 + q * rpp;
         const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
         u[q] = 0;
@@ -84,7 +87,7 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __
         }
       }
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kRowBatch; ++q) {
         const int r = r0 + q * rpp;
         if (r >= nrows) break;
         const Fr w = load(lo + r);
@@ -96,15 +99,20 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __
         }
       }
     }
+    int64_t wide[4][8];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int k = 0; k < 8; ++k) wide[j][k] = acc[j][k];
     for (int o = tpr; o < 32; o <<= 1)
 #pragma unroll
       for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc[j][k] += __shfl_xor_sync(0xffffffffu, acc[j][k], o);
+        for (int k = 0; k < 8; ++k) wide[j][k] += __shfl_xor_sync(0xffffffffu, wide[j][k], o);
     if (lane_id < tpr)
       for (int j = 0; j < lpt; ++j)
 #pragma unroll
-        for (int k = 0; k < 8; ++k) part_s[warp][lane_id * lpt + j][k] = acc[j][k];
+        for (int k = 0; k < 8; ++k) part_s[warp][lane_id * lpt + j][k] = wide[j][k];
     __syncthreads();
     if (threadIdx.x < lanes) {
       int64_t s[8] = {0, 0, 0, 0, 0, 0, 0, 0};

@@ -33,10 +33,12 @@ __device__ __forceinline__ long long mad_wide(int a, int b, long long c) {
 // Payload j (0..3) of a load4 word pair.
 __device__ __forceinline__ int lane_of(uint2 u, int j) { return int(int16_t(((j < 2 ? u.x : u.y) >> (16 * (j & 1))) & 0xffffu)); }
 
+constexpr int kRowBatch = 2;  // rows whose payload loads a projection thread keeps in flight (measured)
+
 // Lane projections (tbv.rs:288-352): out[tile * lanes + l] = high(tile) *
 // sum_r lo[r] * bva[offset + row * lanes + l].  A thread takes min(4, lanes)
-// lanes of a row; a tile has at most 1024 rows, so a lane's sum is below
-// 2^56 before the single reduction.
+// lanes of a row; a tile has at most 4096 rows, so a lane's sum is below
+// 2^58 before the single reduction.
 __global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __restrict__ bva, uint64_t active,
                                                                 const TermTiles* __restrict__ terms, int n_terms,
                                                                 uint32_t n_tiles, const Fe* __restrict__ tables,
@@ -65,10 +67,10 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __rest
 #pragma unroll
       for (int k = 0; k < kC; ++k) acc[j][k] = 0;
     const Fe* lo = tables + T.lo_off;
-    for (int r0 = threadIdx.x / tpr; r0 < nrows; r0 += 2 * rpp) {
-      uint2 u[2];
+    for (int r0 = threadIdx.x / tpr; r0 < nrows; r0 += kRowBatch * rpp) {
+      uint2 u[kRowBatch];
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < kRowBatch; ++q) {
         const int r = r0 + q * rpp;
         const uint64_t g = T.offset + (row0 + r) * lanes + sub * lpt;
         u[q] = make_uint2(0, 0);
@@ -82,7 +84,7 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const Wt* __rest
         }
       }
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < kRowBatch; ++q) {
         const int r = r0 + q * rpp;
         if (r >= nrows) break;
         const Fr w = load(lo + r);
