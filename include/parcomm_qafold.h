@@ -139,8 +139,9 @@ uint64_t qf_kernel_launches(void);
 
 /* Device buffers released by the library are cached for reuse (no cudaMalloc
  * on repeated proofs); at most `bytes` stay cached, the rest is freed at once
- * (default: unlimited).  A request that does not fit frees the cache and
- * retries, waiting up to half a second for concurrent work to release memory.
+ * (default: unlimited).  A request that does not fit frees cached blocks,
+ * largest first, until it fits, then waits up to half a second for
+ * concurrent work to release memory.
  * A caller that budgets HBM itself (a serving loop) sets a limit.  No
  * reference counterpart. */
 int qf_device_cache_limit(uint64_t bytes);

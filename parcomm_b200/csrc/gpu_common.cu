@@ -34,17 +34,32 @@ void* DevicePool::get(size_t bytes) {
       return p;
     }
   }
-  // On failure: return the cache to the driver and retry; then, for up to
-  // half a second, wait for buffers that concurrent work is about to release.
+  // On failure: free this device's cached blocks, largest first, only until
+  // the request fits (the rest stays cached for the allocations that follow);
+  // then, for up to half a second, wait for buffers that concurrent work is
+  // about to release.
   void* p = nullptr;
   for (int attempt = 0;; ++attempt) {
     const cudaError_t e = cudaMalloc(&p, r);
     if (e == cudaSuccess) return p;
     cudaGetLastError();
     if (attempt >= 100) QF_CK(e);
-    if (attempt == 0 || cached_bytes() > 0) trim();
-    else std::this_thread::sleep_for(std::chrono::milliseconds(5));
+    if (!evict_one()) std::this_thread::sleep_for(std::chrono::milliseconds(5));
   }
+}
+// Frees the current device's largest cached block; false when none is left.
+bool DevicePool::evict_one() {
+  const int dev = current_device();
+  std::lock_guard<std::mutex> g(g_pool_mu);
+  auto best = g_pool.end();
+  for (auto it = g_pool.begin(); it != g_pool.end(); ++it)
+    if (it->first.first == dev && (best == g_pool.end() || it->first.second > best->first.second)) best = it;
+  if (best == g_pool.end()) return false;
+  cudaDeviceSynchronize();
+  cudaFree(best->second);
+  g_pool_bytes -= best->first.second;
+  g_pool.erase(best);
+  return true;
 }
 void DevicePool::put(void* p, size_t bytes) {
   const int dev = current_device();

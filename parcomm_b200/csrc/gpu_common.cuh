@@ -63,12 +63,13 @@ using HostScope = ::qf::Section;
 
 // Process-wide cache of device allocations: released buffers are kept, keyed
 // by device and rounded size, and handed out again, so repeated commits/openings
-// of the same shapes pay no cudaMalloc/cudaFree.  A failed cudaMalloc first
-// returns the cache to the driver and retries.
+// of the same shapes pay no cudaMalloc/cudaFree.  A failed cudaMalloc frees
+// cached blocks, largest first, until the request fits.
 struct DevicePool {
   static void* get(size_t bytes);
   static void put(void* p, size_t bytes);
   static void trim();
+  static bool evict_one();  // frees the largest cached block of the current device
   static size_t cached_bytes();  // held in the cache for the current device
   // At most `bytes` stay cached (all devices); further released blocks are
   // freed at once.  Unlimited by default.
