@@ -56,3 +56,28 @@ def test_commit_without_device_fails_loudly():
     with pytest.raises(qf.QfError) as e:
         p.commit(np.zeros(p.active, dtype=np.int8))
     assert e.value.code == qf.QF_E_NO_DEVICE
+
+
+def test_koalabear_params_and_recompute_mode_without_gpu(vectors):
+    """The KoalaBear^4 parameter set mirrors the reference's layout facts, and
+    every commit mode refuses to run without a device (no CPU fallback)."""
+    import torch
+    import numpy as np
+    p = qf.Parameters(qf.demo_shapes(), qf.Config(chunk_log=10, packed_log=4), field=qf.FIELD_KOALABEAR)
+    g = vectors["koalabear_demo"]
+    assert (p.active, p.logical, p.blocks) == (g["active_entries"], g["logical_entries"], g["pcs_blocks"])
+    assert p.weight_dtype == np.int16
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    for commit in (lambda: p.commit(np.zeros(p.active, dtype=np.int16)),
+                   lambda: p.commit_recomputed(np.zeros(p.active, dtype=np.int16))):
+        with pytest.raises(qf.QfError) as e:
+            commit()
+        assert e.value.code == qf.QF_E_NO_DEVICE
+
+
+def test_wrong_weight_width_rejected():
+    import torch
+    p = qf.Parameters(qf.demo_shapes(), qf.Config(chunk_log=10, packed_log=4), field=qf.FIELD_KOALABEAR)
+    with pytest.raises(qf.QfError, match="int16"):
+        p.commit_recomputed(torch.zeros(p.active, dtype=torch.int8))
