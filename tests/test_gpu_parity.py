@@ -318,3 +318,42 @@ def test_device_weights_written_just_before_commit():
         roots.append(c.roots)
         c.close()
         ref.close()
+
+
+@pytest.mark.parametrize("field,shapes,chunk_log,packed_log", [
+    ("f65521", [(1, 70000), (70000, 1), (1, 1)], 16, 4),       # one row, one column, one entry
+    ("koalabear", [(1, 70000), (3, 3)], 16, 1),
+    ("koalabear", [(257, 513), (2, 65537)], 17, 6),
+    ("f65521", [(1025, 1023)], 15, 2)])
+def test_edge_shapes_every_mode(field, shapes, chunk_log, packed_log):
+    """Thin and tiny shapes (buckets of one row or column, ragged padding on
+    both axes) in cache mode and in recompute mode over device and host
+    weights: the same bytes as the oracle."""
+    import torch
+    rng = np.random.default_rng(chunk_log * 10 + packed_log)
+    gen = gaussian_i16 if field == "koalabear" else gaussian_i8
+    mats = [gen(rng, r * c, forced=0.01).reshape(r, c) for r, c in shapes]
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=packed_log), field=FIELDS[field])
+    bva = layout.encode(p.shapes, mats)
+    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, chunk_log, packed_log, bva, field=field)
+    for mode in ("cache", "device", "host"):
+        c = (p.commit(bva) if mode == "cache" else
+             p.commit_recomputed(torch.from_numpy(bva).cuda() if mode == "device" else bva))
+        assert b"".join(c.roots) == o_roots, mode
+        claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
+        assert qf.claims_to_bytes(claims) == o_claims, mode
+        proof, _ = p.prove(c, claims)
+        assert proof.to_bytes() == o_proof, mode
+        c.close()
+
+
+def test_all_zero_weights_streamed():
+    shapes = [(512, 512), (100, 3)]
+    p = qf.Parameters(shapes, qf.Config(chunk_log=14, packed_log=4), field=qf.FIELD_KOALABEAR)
+    bva = layout.encode(p.shapes, [np.zeros(s, np.int16) for s in shapes])
+    o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, 14, 4, bva, field="koalabear")
+    c = p.commit_recomputed(bva)
+    assert b"".join(c.roots) == o_roots
+    claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
+    proof, _ = p.prove(c, claims)
+    assert proof.to_bytes() == o_proof
