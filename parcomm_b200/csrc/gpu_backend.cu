@@ -161,6 +161,7 @@ BlockStream::BlockStream(const W* host, uint64_t active, uint64_t block_len, siz
   const size_t streamed = live_ - resident_;
   slot_buf_.resize(std::min<size_t>(size_t(slots), streamed));
   for (auto& b : slot_buf_) b.alloc(block_len);
+  slot_block_.assign(slot_buf_.size(), ~size_t(0));
   QF_CK(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking));
   landed_.assign(live_, nullptr);
   for (auto& e : landed_) QF_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -184,29 +185,81 @@ void BlockStream::for_each(cudaStream_t s, const BlockFn& fn) {
   }
   const size_t K = slot_buf_.size();
   auto n_of = [&](size_t b) { return std::min<uint64_t>(block_len_, active_ - uint64_t(b) * block_len_); };
+  // Visiting order.  The first pass goes in ascending order (it also copies
+  // the resident blocks).  Later passes start with the streamed blocks the
+  // previous pass left in the staging slots (no copy), then spread the other
+  // streamed blocks evenly among the resident ones, so that their copies
+  // overlap the resident blocks' launches.
+  std::vector<size_t> order;
+  if (!resident_ready_ || K == 0) {
+    for (size_t t = 0; t < live_; ++t) order.push_back(t);
+  } else {
+    std::vector<bool> staged(live_, false);
+    for (size_t k = 0; k < K; ++k)
+      if (slot_block_[k] < live_ && slot_block_[k] >= resident_ && !staged[slot_block_[k]]) {
+        staged[slot_block_[k]] = true;
+        order.push_back(slot_block_[k]);
+      }
+    std::vector<size_t> rest;
+    for (size_t b = resident_; b < live_; ++b)
+      if (!staged[b]) rest.push_back(b);
+    const size_t ns = rest.size(), nr = resident_;
+    for (size_t q = 0, a = 0, r = 0; q < ns + nr; ++q) {
+      if (a < ns && (r >= nr || a * (ns + nr) <= q * ns)) order.push_back(rest[a++]);
+      else order.push_back(r++);
+    }
+  }
+  // The t-th streamed block of the pass takes slot cycle[t % K]: the first K
+  // keep the slots that already hold them, the others take the free slots;
+  // ps[p] counts the streamed blocks before visiting position p.
+  std::vector<size_t> ps(live_ + 1, 0), streamed;
+  for (size_t p = 0; p < live_; ++p) {
+    ps[p + 1] = ps[p] + (order[p] >= resident_ ? 1 : 0);
+    if (order[p] >= resident_) streamed.push_back(order[p]);
+  }
+  std::vector<int> cycle(K, -1), slot_of(live_, -1);
+  std::vector<bool> taken(K, false);
+  for (size_t t = 0; t < std::min(K, streamed.size()); ++t)
+    for (size_t k = 0; k < K; ++k)
+      if (!taken[k] && slot_block_[k] == streamed[t]) { cycle[t] = int(k); taken[k] = true; break; }
+  for (size_t t = 0; t < K; ++t)
+    for (size_t k = 0; cycle[t] < 0 && k < K; ++k)
+      if (!taken[k]) { cycle[t] = int(k); taken[k] = true; }
+  for (size_t t = 0; t < streamed.size(); ++t) slot_of[streamed[t]] = cycle[t % K];
   auto dev_of = [&](size_t b) -> W* {
-    return b < resident_ ? resident_buf_.p + uint64_t(b) * block_len_ : slot_buf_[(b - resident_) % K].p;
+    return b < resident_ ? resident_buf_.p + uint64_t(b) * block_len_ : slot_buf_[size_t(slot_of[b])].p;
   };
-  // Block j goes to its resident place or to slot (j - resident) % K, whose
-  // previous block is j - K: the copy waits until that block's launches are
-  // done.  Copies run up to K blocks ahead of the compute position, and the
-  // first K streamed blocks are copied while the resident ones are processed.
-  auto issue = [&](size_t j) {
-    if (j < resident_ && resident_ready_) return;
-    if (j >= resident_) QF_CK(cudaStreamWaitEvent(copy_, freed_[(j - resident_) % K], 0));
-    const uint64_t n = n_of(j);
-    QF_CK(cudaMemcpyAsync(dev_of(j), host_ + uint64_t(j) * block_len_, n * sizeof(W), cudaMemcpyHostToDevice, copy_));
-    QF_CK(cudaEventRecord(landed_[j], copy_));
+  // A slot's new copy waits until the launches on its previous block are
+  // done (freed_); a block still staged from the previous pass is not copied.
+  auto issue = [&](size_t b) {
+    if (b < resident_ && resident_ready_) return;
+    if (b >= resident_) {
+      const size_t k = size_t(slot_of[b]);
+      if (slot_block_[k] == b) return;
+      QF_CK(cudaStreamWaitEvent(copy_, freed_[k], 0));
+      slot_block_[k] = b;
+    }
+    const uint64_t n = n_of(b);
+    QF_CK(cudaMemcpyAsync(dev_of(b), host_ + uint64_t(b) * block_len_, n * sizeof(W), cudaMemcpyHostToDevice, copy_));
+    QF_CK(cudaEventRecord(landed_[b], copy_));
     copied_ += n * sizeof(W);
   };
+  // Streamed copies run up to K streamed blocks ahead of the compute
+  // position (so a slot is reused only after its previous block's launches
+  // were enqueued); on the first pass the resident ones up to K positions.
   const size_t ahead = std::max<size_t>(K, 1);
   size_t issued = 0;
   for (size_t i = 0; i < live_; ++i) {
-    const size_t horizon = (resident_ready_ ? std::max(i, resident_) : i) + ahead;
-    while (issued < live_ && issued < horizon) issue(issued++);
-    if (!(i < resident_ && resident_ready_)) QF_CK(cudaStreamWaitEvent(s, landed_[i], 0));
-    fn(i, dev_of(i), n_of(i));
-    if (i >= resident_) QF_CK(cudaEventRecord(freed_[(i - resident_) % K], s));
+    while (issued < live_) {
+      const size_t b = order[issued];
+      if (b >= resident_ ? ps[issued] >= ps[i] + K : (!resident_ready_ && issued >= i + ahead)) break;
+      issue(b);
+      ++issued;
+    }
+    const size_t b = order[i];
+    if (!(b < resident_ && resident_ready_)) QF_CK(cudaStreamWaitEvent(s, landed_[b], 0));
+    fn(b, dev_of(b), n_of(b));
+    if (b >= resident_) QF_CK(cudaEventRecord(freed_[size_t(slot_of[b])], s));
   }
   if (resident_) resident_ready_ = true;
 }
@@ -741,7 +794,7 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
   ByteWriter w;
   w.bytes("QAFOLDB1", 8);
   w.len(roots.size());
-  auto emit = [&](const DeviceCodeword& cw) {
+  auto emit_into = [&](ByteWriter& w, const DeviceCodeword& cw) {
     Rows<F> r;
     if (sel.all) {
       r.all = true;
@@ -760,15 +813,22 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
     }
     write_rows(w, r);
   };
+  auto emit = [&](const DeviceCodeword& cw) { emit_into(w, cw); };
   if (src_) {
     // Recompute mode: re-encode every live block as its weights land, check
     // its root, then the zero suffix once.
     DeviceCodeword& cw = scratch_codeword();
     check(roots.size() == P_.blocks(), "block roots");
+    // Passes may visit the blocks in either direction: each block's rows are
+    // kept apart and appended in block order.
+    std::vector<std::vector<uint8_t>> per_block(src_->live_blocks());
     src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
       if (encode_block(d, n, 0, cw) != roots[b]) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
-      emit(cw);
+      ByteWriter bw;
+      emit_into(bw, cw);
+      per_block[b] = std::move(bw.out);
     });
+    for (const auto& v : per_block) w.out.insert(w.out.end(), v.begin(), v.end());
     if (src_->live_blocks() < roots.size()) {
       const Digest z = encode_block(nullptr, 0, 0, cw);
       const size_t at = w.out.size();

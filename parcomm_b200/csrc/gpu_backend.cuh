@@ -76,8 +76,12 @@ class BlockStream {
   size_t resident_blocks() const { return resident_; }
   const W* host() const { return host_; }  // the weights (device memory when on_device())
   uint64_t h2d_bytes() const { return copied_; }
-  // fn(b, d, n) for every live block b in order, with its launches on `s`: d
-  // is the device copy of entries [b * block_len, b * block_len + n).
+  // fn(b, d, n) for every live block b, with its launches on `s`: d is the
+  // device copy of entries [b * block_len, b * block_len + n).  After the
+  // first (ascending) pass, a pass starts with the blocks the previous pass
+  // left staged and interleaves the other streamed blocks with the resident
+  // ones; callers must not depend on the order.  Weights already in HBM are
+  // visited in ascending order.
   using BlockFn = std::function<void(size_t b, const W* d, uint64_t n)>;
   void for_each(cudaStream_t s, const BlockFn& fn);
 
@@ -91,6 +95,7 @@ class BlockStream {
   std::vector<DBuf<W>> slot_buf_;
   std::vector<cudaEvent_t> landed_;  // per live block: its copy has landed
   std::vector<cudaEvent_t> freed_;   // per slot: the compute on its last block is done
+  std::vector<size_t> slot_block_;   // per slot: the block its last copy staged
   cudaStream_t copy_ = nullptr;
   uint64_t copied_ = 0;
 };
