@@ -9,6 +9,8 @@
 // (qafold_short_decide_wire.rs).  Only DirectInterleavedV1 is reachable for
 // the supported fields, so the RF-code branches are not restated.
 #pragma once
+#include <exception>
+#include <mutex>
 #include <optional>
 #include <vector>
 
@@ -579,17 +581,36 @@ F carry_row_value(const Rows<F>& rows, size_t n_enc, size_t n_cols, size_t ordin
   }
   return s;
 }
+// body(i) for i in [0, n) on the OpenMP threads when n >= min_n; the first
+// exception any iteration throws is rethrown on the calling thread (none may
+// leave a parallel region).
+template <class Fn>
+void parallel_rows(size_t n, size_t min_n, Fn&& body) {
+  std::exception_ptr err;
+  std::mutex mu;
+#pragma omp parallel for if (n >= min_n) schedule(static)
+  for (long i = 0; i < long(n); ++i) {
+    try {
+      body(size_t(i));
+    } catch (...) {
+      std::lock_guard<std::mutex> g(mu);
+      if (!err) err = std::current_exception();
+    }
+  }
+  if (err) std::rethrow_exception(err);
+}
+
 template <class F>
 std::vector<F> compute_iota(const SetupLevel<F>& sl, const SetupRows<F>& srows, const std::optional<Rows<F>>& crows,
                             size_t carry_cols, const RowSelection& sel, const std::vector<F>& w) {
   const size_t tc = sl.shape.total_cols();
   std::vector<F> iota(sel.size());
-  for (size_t i = 0; i < sel.size(); ++i) {
+  parallel_rows(sel.size(), 64, [&](size_t i) {
     size_t row = sel.at(i);
     F v = setup_row_value(srows, sl.shape, i, row, w);
     if (crows) v += carry_row_value(*crows, sl.shape.encoded_rows, carry_cols, i, row, w.data() + tc);
     iota[i] = v;
-  }
+  });
   return iota;
 }
 
@@ -599,25 +620,27 @@ SetupRows<F> open_setup_rows(const SetupLevel<F>& sl, const RowSelection& sel) {
   out.shape = sl.shape;
   if (sel.all) { out.all = true; out.encoded = sl.encoded; return out; }
   const size_t tc = sl.shape.total_cols();
-  for (size_t r : sel.rows) {
-    SetupRowQuery<F> q;
+  out.partial.resize(sel.rows.size());
+  parallel_rows(sel.rows.size(), 64, [&](size_t i) {
+    const size_t r = sel.rows[i];
+    SetupRowQuery<F>& q = out.partial[i];
     q.row_index = r;
-    for (size_t c = 0; c < tc; ++c) q.row.push_back(sl.encoded[c * sl.shape.encoded_rows + r]);
+    q.row.resize(tc);
+    for (size_t c = 0; c < tc; ++c) q.row[c] = sl.encoded[c * sl.shape.encoded_rows + r];
     q.path.siblings = sl.tree.path(r);
-    out.partial.push_back(std::move(q));
-  }
+  });
   return out;
 }
 template <class F>
 Rows<F> open_codeword_rows(const Codeword<F>& cw, const RowSelection& sel) {
   Rows<F> out;
   if (sel.all) { out.all = true; out.n_rows = cw.n_ext_rows; out.n_cols = cw.n_cols; out.encoded = cw.encoded; return out; }
-  for (size_t r : sel.rows) {
-    RowQuery<F> q;
-    q.row = cw.row(r);
-    q.path.siblings = cw.tree.path(r);
-    out.partial.push_back(std::move(q));
-  }
+  out.partial.resize(sel.rows.size());
+  parallel_rows(sel.rows.size(), 64, [&](size_t i) {
+    const size_t r = sel.rows[i];
+    out.partial[i].row = cw.row(r);
+    out.partial[i].path.siblings = cw.tree.path(r);
+  });
   return out;
 }
 
