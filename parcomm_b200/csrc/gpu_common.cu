@@ -39,12 +39,13 @@ void* DevicePool::get(size_t bytes) {
   // then, for up to half a second, wait for buffers that concurrent work is
   // about to release.
   void* p = nullptr;
-  for (int attempt = 0;; ++attempt) {
+  for (int waits = 0;;) {
     const cudaError_t e = cudaMalloc(&p, r);
     if (e == cudaSuccess) return p;
     cudaGetLastError();
-    if (attempt >= 100) QF_CK(e);
-    if (!evict_one()) std::this_thread::sleep_for(std::chrono::milliseconds(5));
+    if (evict_one()) continue;
+    if (++waits > 100) QF_CK(e);
+    std::this_thread::sleep_for(std::chrono::milliseconds(5));
   }
 }
 // Frees the current device's largest cached block; false when none is left.
