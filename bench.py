@@ -21,6 +21,8 @@ setup and claim generation are outside it.  The claims are computed once
            (host->device copy of the weights and proof bytes back per step).
   per_matrix : the plain per-matrix path for comparison: the same 226 shapes,
            each committed and proven as its own single-matrix statement.
+  range_audit : the LogUp range audit of the same weights (Committed.range_audit),
+           a check beside the proof, timed once outside the step.
 
 `--impl reference` times the CPU restatement of the reference prover (the
 oracle; the Rust reference cannot be built in this image) with all host
@@ -457,6 +459,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-matrix", action="store_true",
                     help="skip the per-matrix comparison (each matrix proven on its own)")
+    ap.add_argument("--no-audit", action="store_true", help="skip the LogUp range audit measurement")
     ap.add_argument("--out", default=str(ROOT / "gpurun_out"))
     args = ap.parse_args()
 
@@ -602,6 +605,30 @@ def main():
                 "frac": h2d_achieved / h2d_peak, "bytes_per_step": h2d_dev,
                 "peak_source": "pinned 2 GiB host->device copy, best of 3, measured in this run"}
 
+    # LogUp range audit of the same weights (beside the proof, outside the
+    # timed region): one warm-up call, then one timed call.
+    range_audit = None
+    if not args.no_audit and not streamed:
+        ca = commit(True)
+        ca.range_audit()
+        torch.cuda.synchronize()
+        qf.kernel_timing(True)
+        t0 = time.perf_counter()
+        ra = ca.range_audit()
+        audit_s = time.perf_counter() - t0
+        ks = qf.kernel_stats().get("k_range_audit", {})
+        qf.kernel_timing(False)
+        ca.close()
+        k_ms = ks.get("ms")
+        range_audit = {
+            "holds": ra.holds, "values": active, "ms": audit_s * 1000.0, "values_per_s": active / audit_s,
+            "kernel_ms": k_ms, "kernel_launches": ks.get("launches"),
+            "kernel_values_per_s": active / (k_ms / 1000.0) if k_ms else None,
+            "kernel_hbm_frac": (active * entry_bytes / (k_ms / 1000.0) / 1e9) / peak if k_ms else None,
+            "nonzero_bins": int((ra.multiplicities > 0).sum()),
+            "what": "LogUp range audit beside the proof (never in it): per-value fraction sum and multiplicities "
+                    "on the device, the table side on the host"}
+
     per_matrix = None
     if not args.no_per_matrix and args.workload in ("8b8", "8b16"):
         del bva_host
@@ -659,6 +686,7 @@ def main():
         "link_roofline": link,
         "cpu_baseline": cpu_baseline,
         "per_matrix": per_matrix,
+        "range_audit": range_audit,
         "clocks": clocks.summary(local),
         "proof_bytes": proof_bytes,
         "stage_ms": {k: getattr(pf_dev, k) for k in ("commit_ms", "eo_ms", "projection_ms", "folding_ms", "sumcheck_ms",

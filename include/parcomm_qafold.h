@@ -126,6 +126,26 @@ int qf_open(const qf_params* params, const qf_committed* committed, const uint8_
 int qf_verify(const qf_params* params, const uint8_t* roots, const uint8_t* claims, size_t claims_len, const uint8_t* proof,
               size_t proof_len);
 
+/* LogUp range audit of committed weights over the entry type's table: the
+ * 256 values -128..127 for int8 weights, the 65536 values -32768..32767 for
+ * int16 payloads.  It is a check beside the proof: nothing of it enters a
+ * transcript or the proof bytes, and it has no reference counterpart (the
+ * values enter the field through field::small, field.rs:24-29).
+ *
+ * alpha is an extension element outside the base field, drawn from `seed` by
+ * BLAKE2s (domain "parcomm-b200/logup-range-audit/v1"; bind it to the
+ * commitment by hashing the roots into the seed).  On the device, one pass
+ * over the committed weights accumulates lhs = sum_i 1 / (alpha - v_i) value by
+ * value and counts each table value's multiplicity m_t; then rhs =
+ * sum_t m_t / (alpha - t).  Writes the multiplicities (n_bins must be 256 or
+ * 65536 to match the field; bin k counts the value k - 128 or k - 32768),
+ * alpha, lhs and rhs (16 canonical bytes each) and *holds = 1 when lhs == rhs
+ * and the multiplicities add up to the active entries, else 0.  Any output
+ * pointer may be NULL.  Works on qf_commit and qf_commit_streamed handles
+ * (streamed weights are staged block by block as in the proof's passes). */
+int qf_range_audit(const qf_params* params, const qf_committed* committed, const uint8_t seed[32], uint64_t* multiplicities,
+                   size_t n_bins, uint8_t alpha[16], uint8_t lhs[16], uint8_t rhs[16], int* holds);
+
 void qf_free_bytes(uint8_t* bytes);
 
 /* Diagnostics (no reference counterpart): per-kernel device time measured with

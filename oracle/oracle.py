@@ -45,6 +45,9 @@ def lib() -> ctypes.CDLL:
         for name in ("qfo_verify", "qfo_verify_kb"):
             getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
+        for name in ("qfo_range_audit", "qfo_range_audit_kb"):
+            getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
+                                         ctypes.c_char_p]
         _lib = L
     return _lib
 
@@ -121,3 +124,16 @@ def verify(shapes, chunk_log, packed_log, roots: bytes, claims: bytes, proof: by
     rc = getattr(lib(), "qfo_verify" + _SUFFIX[field][0])(arr, n, chunk_log, packed_log, rf_bits, roots, claims,
                                                          len(claims), proof, len(proof))
     return rc == 0
+
+
+def range_audit(values, seed: bytes, field="f65521"):
+    """LogUp range audit of BVA values: (multiplicities, alpha, lhs, rhs), the
+    field elements as 16 canonical bytes; bin k counts the value k - 128
+    (int8) or k - 32768 (int16)."""
+    sfx, dt = _SUFFIX[field]
+    v = np.ascontiguousarray(values, dtype=dt)
+    mult = np.zeros(256 if dt == np.int8 else 65536, dtype=np.uint64)
+    a, l, r = (ctypes.create_string_buffer(16) for _ in range(3))
+    assert len(seed) == 32
+    _check(getattr(lib(), "qfo_range_audit" + sfx)(v.ctypes.data, v.size, seed, mult.ctypes.data, a, l, r))
+    return mult, a.raw, l.raw, r.raw

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "cpu_backend.h"
+#include "../parcomm_b200/csrc/host/range_audit.h"
 
 using namespace qf;
 using F = Fp8;
@@ -48,6 +49,41 @@ std::vector<Shape> shapes_of(const uint64_t* s, size_t n) {
   std::vector<Shape> out;
   for (size_t i = 0; i < n; ++i) out.push_back({size_t(s[2 * i]), size_t(s[2 * i + 1])});
   return out;
+}
+// LogUp range audit, from the definitions: m_t counts the values equal to t;
+// lhs = sum over the values of (alpha - v)^-1, each distinct value's inverse
+// computed once; rhs = sum_t m_t (alpha - t)^-1 with one inversion per term.
+// alpha comes from the same seed derivation as the library's.
+template <class G, class T>
+int range_audit_impl(const T* values, uint64_t n, const uint8_t seed[32], uint64_t* mult_out, uint8_t alpha_out[16],
+                     uint8_t lhs_out[16], uint8_t rhs_out[16]) {
+  return guarded([&] {
+    using Tab = RangeTable<T>;
+    const G alpha = range_audit_alpha<G>(seed);
+    std::vector<uint64_t> mult(Tab::kBins, 0);
+    std::vector<G> inv(Tab::kBins);
+    std::vector<bool> have(Tab::kBins, false);
+    G lhs = G::zero();
+    for (uint64_t i = 0; i < n; ++i) {
+      const size_t k = size_t(int64_t(values[i]) - Tab::kMin);
+      ++mult[k];
+      if (!have[k]) {
+        inv[k] = (alpha - G::from_base(G::small(int(values[i])))).inverse();
+        have[k] = true;
+      }
+      lhs += inv[k];
+    }
+    G rhs = G::zero();
+    for (size_t k = 0; k < Tab::kBins; ++k)
+      if (mult[k]) {
+        const G d = alpha - G::from_base(G::small(int(int64_t(k) + Tab::kMin)));
+        rhs += d.inverse() * G::from_base(uint32_t(mult[k] % G::modulus_u64()));
+      }
+    std::memcpy(mult_out, mult.data(), mult.size() * 8);
+    alpha.to_bytes(alpha_out);
+    lhs.to_bytes(lhs_out);
+    rhs.to_bytes(rhs_out);
+  });
 }
 template <class G, class T>
 int prove_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
@@ -238,6 +274,16 @@ int qfo_verify(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint
 int qfo_verify_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
                   const uint8_t* roots, const uint8_t* claims_in, size_t claims_len, const uint8_t* proof, size_t proof_len) {
   return verify_impl<Kb4>(shapes, n_shapes, chunk_log, packed_log, rf_bits, roots, claims_in, claims_len, proof, proof_len);
+}
+
+// LogUp range audit of `n` BVA values (multiplicities: 256 or 65536 bins).
+int qfo_range_audit(const int8_t* values, uint64_t n, const uint8_t seed[32], uint64_t* mult, uint8_t alpha[16],
+                    uint8_t lhs[16], uint8_t rhs[16]) {
+  return range_audit_impl<Fp8, int8_t>(values, n, seed, mult, alpha, lhs, rhs);
+}
+int qfo_range_audit_kb(const int16_t* values, uint64_t n, const uint8_t seed[32], uint64_t* mult, uint8_t alpha[16],
+                       uint8_t lhs[16], uint8_t rhs[16]) {
+  return range_audit_impl<Kb4, int16_t>(values, n, seed, mult, alpha, lhs, rhs);
 }
 
 }  // extern "C"

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import hashlib
 from pathlib import Path
 from typing import List, Optional, Sequence, Tuple
 
@@ -29,6 +30,7 @@ ERRORS = {
     -5: "InvalidParameters", -6: "TranscriptError", -7: "ProtocolError", -8: "CudaError", -9: "ArgumentError",
     -10: "NoDevice",
 }
+QF_E_ARGUMENT = -9
 QF_E_NO_DEVICE = -10
 
 
@@ -60,7 +62,7 @@ EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
     "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
-    "qf_committed_stream_info", "qf_open", "qf_device_cache_limit",
+    "qf_committed_stream_info", "qf_open", "qf_device_cache_limit", "qf_range_audit",
 )
 
 
@@ -99,6 +101,8 @@ def lib() -> ctypes.CDLL:
         L.qf_kernel_launches.restype = U64
         L.qf_device_cache_limit.argtypes = [U64]
         L.qf_commit_block_noalloc.argtypes = [P, P, U64, U64, P, P]
+        L.qf_range_audit.argtypes = [P, P, ctypes.c_char_p, P, S, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                     ctypes.POINTER(ctypes.c_int)]
         for name in EXPORTED:
             if not hasattr(L, name):
                 raise QfError(-9, f"library does not export {name}")
@@ -215,6 +219,22 @@ class Committed:
     def stream_bytes(self) -> int:
         return self.stream_info()[0]
 
+    def range_audit(self, seed: Optional[bytes] = None) -> "RangeAudit":
+        """LogUp range audit of the committed weights over the entry type's
+        table (qf_range_audit); not part of the proof.  The default seed is
+        BLAKE2s of the concatenated roots, which ties alpha to the
+        commitment."""
+        if seed is None:
+            seed = hashlib.blake2s(b"".join(self.roots)).digest()
+        if len(seed) != 32:
+            raise QfError(QF_E_ARGUMENT, "range audit seed must be 32 bytes")
+        bins = 256 if self.params.field == FIELD_F65521 else 65536
+        mult = np.zeros(bins, dtype=np.uint64)
+        a, l, r = (ctypes.create_string_buffer(16) for _ in range(3))
+        holds = ctypes.c_int()
+        _check(lib().qf_range_audit(self.params._h, self._h, seed, mult.ctypes.data, bins, a, l, r, ctypes.byref(holds)))
+        return RangeAudit(mult, a.raw, l.raw, r.raw, bool(holds.value))
+
     def close(self) -> None:
         if self._h:
             lib().qf_committed_free(self._h)
@@ -228,6 +248,19 @@ class Committed:
 
 
 @dataclasses.dataclass
+@dataclasses.dataclass
+class RangeAudit:
+    """Result of Committed.range_audit: multiplicities (bin k counts the value
+    k - 128 for int8, k - 32768 for int16), alpha, lhs = sum_i 1/(alpha - v_i),
+    rhs = sum_t m_t/(alpha - t) (16 canonical bytes each), and whether the
+    identity holds."""
+    multiplicities: np.ndarray
+    alpha: bytes
+    lhs: bytes
+    rhs: bytes
+    holds: bool
+
+
 class Commitment:
     """protocol::Commitment: version 2, config, shapes, parameter digest, block roots."""
     params: "Parameters"

@@ -163,6 +163,16 @@ int qf_open(const qf_params* params, const qf_committed* committed, const uint8_
   });
 }
 
+int qf_range_audit(const qf_params* params, const qf_committed* committed, const uint8_t seed[32], uint64_t* multiplicities,
+                   size_t n_bins, uint8_t alpha[16], uint8_t lhs[16], uint8_t rhs[16], int* holds) {
+  return guarded([&] {
+    if (!params || !committed || !seed) fail(QF_E_ARGUMENT, "null argument");
+    if (committed->consumed) fail(QF_E_ARGUMENT, "committed state already consumed by prove");
+    require_device();
+    api(params->field).range_audit(params, committed, seed, multiplicities, n_bins, alpha, lhs, rhs, holds);
+  });
+}
+
 void qf_free_bytes(uint8_t* bytes) { std::free(bytes); }
 
 int qf_kernel_timing(int enable) {

@@ -12,6 +12,7 @@
 
 #include "capi_internal.h"
 #include "gpu_backend.cuh"
+#include "host/range_audit.h"
 
 namespace QFB_NS {
 namespace {
@@ -383,7 +384,27 @@ void stream_info(const qf_committed* committed, uint64_t* h2d_bytes, uint64_t* r
 
 }  // namespace
 
+// LogUp range audit: alpha from the seed, the weights' fraction sum on the
+// device, the table side from the multiplicities.
+void range_audit(const qf_params* params, const qf_committed* committed, const uint8_t seed[32], uint64_t* mult_out,
+                 size_t n_bins, uint8_t alpha_out[16], uint8_t lhs_out[16], uint8_t rhs_out[16], int* holds) {
+  const auto* fc = static_cast<const FieldCommitted*>(committed->state.get());
+  check(!mult_out || n_bins == RangeTable<W>::kBins, "range audit: multiplicities need 256 (int8) or 65536 (int16) bins");
+  const F alpha = range_audit_alpha<F>(seed);
+  std::vector<uint64_t> mult;
+  const std::array<F, 2> frac = fc->be->range_audit(alpha, mult);
+  const F lhs = frac[0] * frac[1].inverse();
+  const F rhs = logup_table_sum<F, W>(alpha, mult);
+  uint64_t total = 0;
+  for (uint64_t m : mult) total += m;
+  if (mult_out) std::memcpy(mult_out, mult.data(), mult.size() * 8);
+  if (alpha_out) alpha.to_bytes(alpha_out);
+  if (lhs_out) lhs.to_bytes(lhs_out);
+  if (rhs_out) rhs.to_bytes(rhs_out);
+  if (holds) *holds = (lhs == rhs && total == fc->active) ? 1 : 0;
+}
+
 const qfc::FieldApi kFieldApi = {sizeof(W), make_params, info, commit, commit_streamed, statement_json,
-                                 benchmark_points_bytes, eval_claims, prove, verify, stream_info};
+                                 benchmark_points_bytes, eval_claims, prove, verify, stream_info, range_audit};
 
 }  // namespace QFB_NS

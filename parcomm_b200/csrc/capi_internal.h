@@ -52,6 +52,9 @@ struct FieldApi {
                  size_t proof_len);
   // Streamed weights: host->device bytes copied so far, resident and live blocks.
   void (*stream_info)(const qf_committed* c, uint64_t* h2d_bytes, uint64_t* resident_blocks, uint64_t* live_blocks);
+  // LogUp range audit of the committed weights (not part of the proof).
+  void (*range_audit)(const qf_params* p, const qf_committed* c, const uint8_t seed[32], uint64_t* mult, size_t n_bins,
+                      uint8_t alpha[16], uint8_t lhs[16], uint8_t rhs[16], int* holds);
 };
 
 inline thread_local std::string g_last_error;

@@ -3,6 +3,7 @@
 #include "kernels/commit.cuh"
 #include "kernels/open.cuh"
 #include "kernels/vec.cuh"
+#include "kernels/audit.cuh"
 
 #include <algorithm>
 #include <map>
@@ -1607,6 +1608,53 @@ bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, siz
   LiteBullet<F> gen = litebullet_dev(sle, sparse.p, gr.p, n_enc, t, "decide-direct-carry-generator-litebullet", "litebullet-fold", true);
   out = {MatrixClaim<F>{gen.b_value, gen.b_point, msg.a_point}, EvalWithPoint<F>{msg.b_value, msg.b_point}};
   return true;
+}
+
+// ---------------------------------------------------------------- range audit
+std::array<F, 2> GpuBackend::range_audit(const F& alpha, std::vector<uint64_t>& mult) {
+  HostScope hs("range_audit");
+  static std::mutex mu;
+  static std::set<int> configured;
+  int dev = 0;
+  QF_CK(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (!configured.count(dev)) {
+      set_smem(qfd::k_range_audit, qfd::kAuditSmem);
+      configured.insert(dev);
+    }
+  }
+  // A warp's int8 counters are 32-bit: each warp takes at most
+  // ceil(n / (16 * 512 * grid)) * 512 values of one launch.
+  check(active_ < (uint64_t(1) << 40), "range audit: more than 2^40 values");
+  qfd::AlphaPowers ap;
+  F pw = alpha;
+  for (int k = 0; k < 4; ++k) { ap.p[k] = to_fe(pw); pw = pw * alpha; }
+  const unsigned grid = tile_grid(~uint64_t(0));  // one CTA per SM
+  const size_t launches = src_ ? src_->live_blocks() : 1;
+  DBuf<unsigned long long> hist(qfd::kAuditBins);
+  DBuf<Fe> part(2 * size_t(grid) * std::max<size_t>(launches, 1));
+  QF_CK(cudaMemsetAsync(hist.p, 0, hist.n * 8, s_));
+  size_t li = 0;
+  auto run = [&](const W* d, uint64_t n) {
+    check(reinterpret_cast<uintptr_t>(d) % 16 == 0, "range audit: weights must be 16-byte aligned");
+    QF_LAUNCH(s_, "k_range_audit", n * sizeof(W),
+              qfd::k_range_audit<<<grid, qfd::kAuditThreads, qfd::kAuditSmem, s_>>>(d, n, ap, hist.p, part.p + 2 * size_t(grid) * li));
+    ++li;
+  };
+  if (src_) src_->for_each(s_, [&](size_t, const W* d, uint64_t n) { run(d, n); });
+  else if (active_) run(bva_, active_);
+  mult.assign(qfd::kAuditBins, 0);
+  std::vector<F> h(2 * size_t(grid) * li);
+  QF_CK(cudaMemcpyAsync(mult.data(), hist.p, mult.size() * 8, cudaMemcpyDeviceToHost, s_));
+  if (!h.empty()) QF_CK(cudaMemcpyAsync(h.data(), part.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  F num = F::zero(), den = F::one();
+  for (size_t i = 0; i < h.size(); i += 2) {
+    num = num * h[i + 1] + h[i] * den;
+    den = den * h[i + 1];
+  }
+  return {num, den};
 }
 
 }  // namespace QFB_NS

@@ -188,6 +188,10 @@ class GpuBackend : public Backend<F>,
                                                                size_t stride);
   // Raw window values of small terms.
   std::vector<W> windows(const std::vector<uint64_t>& starts, size_t stride);
+  // LogUp range audit (not part of the proof): sum_i 1 / (alpha - v_i) over
+  // the weights as {numerator, denominator}, and `mult` = the multiplicity of
+  // each table value (bin k: the value k - 128 for int8, k - 32768 for int16).
+  std::array<F, 2> range_audit(const F& alpha, std::vector<uint64_t>& mult);
 
 
  private:
