@@ -1629,7 +1629,10 @@ std::array<F, 2> GpuBackend::range_audit(const F& alpha, std::vector<uint64_t>& 
   check(active_ < (uint64_t(1) << 40), "range audit: more than 2^40 values");
   qfd::AlphaPowers ap;
   F pw = alpha;
-  for (int k = 0; k < 4; ++k) { ap.p[k] = to_fe(pw); pw = pw * alpha; }
+  for (int k = 0; k < qfd::kAuditGroup; ++k) {
+    for (int j = 0; j < qfd::kC; ++j) ap.c[k][j] = uint32_t(pw.c[j]);
+    pw = pw * alpha;
+  }
   const unsigned grid = tile_grid(~uint64_t(0));  // one CTA per SM
   const size_t launches = src_ ? src_->live_blocks() : 1;
   DBuf<unsigned long long> hist(qfd::kAuditBins);

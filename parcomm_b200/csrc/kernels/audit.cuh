@@ -3,17 +3,21 @@
 // multiplicity over the entry type's table (int8: 256 values, int16: 65536).
 //
 // The fraction sum is formed per value, without the multiplicities: for each
-// group of four values the polynomial P(x) = prod (x - v_j) is built with
-// exact integer coefficients (elementary symmetric sums, |e_4| < 2^61 for
-// int16), so that sum_j 1 / (alpha - v_j) = P'(alpha) / P(alpha).  P(alpha)
-// and P'(alpha) take three base-by-extension products per coefficient lane
-// from alpha^1..alpha^4, and the running fraction n / d absorbs the group
-// with three extension products: (n P + P' d) / (d P).
+// group of G values (8 int8 entries, 4 int16 entries) the polynomial
+// P(x) = prod (x - v_j) is built with exact integer coefficients (|c_k| below
+// 2^57 for eight int8 values, 2^61 for four int16 values), so that
+// sum_j 1 / (alpha - v_j) = P'(alpha) / P(alpha).  P(alpha) and P'(alpha) take
+// G base-by-extension products per coefficient lane from alpha^1..alpha^G
+// (kernel parameters: constant-bank operands), and a running fraction n / d
+// absorbs the group with three extension products: (n P + P' d) / (d P).
+// Each thread keeps two running fractions (even and odd groups) so that two
+// chains of extension products overlap.
 //
 // Multiplicities go to shared memory.  For int8, each warp keeps its own 256
 // 32-bit counters.  The 65536 int16 counters are 16-bit halves of 32768
-// words (128 KB); a CTA adds at most 61,447 values between flushes to the
-// global 64-bit histogram, so a half never carries into its neighbour.
+// words (128 KB); a CTA of 384 threads adds at most 64,519 values between
+// flushes to the global 64-bit histogram, so a half never carries into its
+// neighbour.
 #pragma once
 #include <cstdint>
 
@@ -22,7 +26,8 @@
 
 namespace QFD_NS {
 
-constexpr int kAuditThreads = 512;
+// 384 threads: the two product chains fit in registers (no spills).
+constexpr int kAuditThreads = 384;
 constexpr int kAuditPerChunk = 16 / int(sizeof(Wt));  // values per 16-byte load
 constexpr int kAuditBins = sizeof(Wt) == 1 ? 256 : 65536;
 constexpr int kAuditMin = sizeof(Wt) == 1 ? -128 : -32768;
@@ -35,8 +40,11 @@ static_assert(sizeof(Wt) == 1 || size_t(kAuditEpochRounds) * kAuditThreads * kAu
               "an epoch must stay below 2^16 values per CTA");
 static_assert(kAuditSmemWords >= size_t(kAuditWarps) * 4 * kC, "fraction reduction reuses the counters");
 
+constexpr int kAuditGroup = sizeof(Wt) == 1 ? 8 : 4;  // values per polynomial
+
+// alpha^1 .. alpha^G as canonical 32-bit coefficient lanes.
 struct AlphaPowers {
-  Fe p[4];  // alpha^1 .. alpha^4
+  uint32_t c[kAuditGroup][kC];
 };
 
 struct Frac {
@@ -50,21 +58,61 @@ __device__ __forceinline__ Frac frac_add(const Frac& a, const Frac& b) {
   return {acc_reduce(t), mul(a.d, b.d)};
 }
 
-// n / d += sum_j 1 / (alpha - v_j) over four values.
-__device__ __forceinline__ void audit_group(Frac& f, const Fr (&a)[4], int v0, int v1, int v2, int v3) {
-  const long long a1 = v0 + v1, a2 = (long long)v0 * v1, b1 = v2 + v3, b2 = (long long)v2 * v3;
-  const long long e1 = a1 + b1, e2 = a2 + b2 + a1 * b1, e3 = a1 * b2 + a2 * b1, e4 = a2 * b2;
-  // P(x) = x^4 - e1 x^3 + e2 x^2 - e3 x + e4, P'(x) = 4 x^3 - 3 e1 x^2 + 2 e2 x - e3.
-  const uint32_t k3 = red_signed(-e1), k2 = red_signed(e2), k1 = red_signed(-e3), k0 = red_signed(e4);
-  const uint32_t d2 = red_signed(-3 * e1), d1 = red_signed(2 * e2);
+// Coefficients q[0..4] of the monic quartic prod_{j<4} (x - v_j).
+__device__ __forceinline__ void quartic(const int* v, long long* q) {
+  const long long a1 = v[0] + v[1], a2 = (long long)v[0] * v[1], b1 = v[2] + v[3], b2 = (long long)v[2] * v[3];
+  q[4] = 1;
+  q[3] = -(a1 + b1);
+  q[2] = a2 + b2 + a1 * b1;
+  q[1] = -(a1 * b2 + a2 * b1);
+  q[0] = a2 * b2;
+}
+
+// n / d += sum_j 1 / (alpha - v_j) over kAuditGroup values.
+__device__ __forceinline__ void audit_group(Frac& f, const AlphaPowers& ap, const int* v) {
+  constexpr int G = kAuditGroup;
+  long long c[G + 1];  // P(x) = sum_k c[k] x^k, c[G] = 1
+  if constexpr (G == 4) {
+    quartic(v, c);
+  } else {
+    long long x[5], y[5];
+    quartic(v, x);
+    quartic(v + 4, y);
+#pragma unroll
+    for (int k = 0; k <= 8; ++k) c[k] = 0;
+#pragma unroll
+    for (int i = 0; i <= 4; ++i)
+#pragma unroll
+      for (int j = 0; j <= 4; ++j) c[i + j] += x[i] * y[j];
+  }
+  // P(alpha) = alpha^G + sum_{k<G} c_k alpha^k and P'(alpha) = G alpha^(G-1) +
+  // sum_{1<=k<G} k c_k alpha^(k-1): per lane, products below 2^62 (KoalaBear:
+  // at most three of them and two canonical terms in one 64-bit sum; F65521:
+  // products below 2^35).
+  uint32_t m[G];
+#pragma unroll
+  for (int k = 0; k < G; ++k) m[k] = red_signed(c[k]);
   Fr P, D;
 #pragma unroll
   for (int j = 0; j < kC; ++j) {
-    uint64_t s = uint64_t(a[3].c[j]) + uint64_t(k3) * a[2].c[j] + uint64_t(k2) * a[1].c[j] + uint64_t(k1) * a[0].c[j];
-    uint64_t t = 4ull * a[2].c[j] + uint64_t(d2) * a[1].c[j] + uint64_t(d1) * a[0].c[j];
-    if (j == 0) { s += k0; t += k1; }
-    P.c[j] = red_sum(s);
-    D.c[j] = red_sum(t);
+    uint64_t s = ap.c[G - 1][j], t;
+    if constexpr (sizeof(Wt) == 1) {
+      t = uint64_t(G) * ap.c[G - 2][j];
+#pragma unroll
+      for (int k = 1; k < G; ++k) s += uint64_t(m[k]) * ap.c[k - 1][j];
+#pragma unroll
+      for (int k = 2; k < G; ++k) t += uint64_t(k * m[k]) * ap.c[k - 2][j];
+      if (j == 0) { s += m[0]; t += m[1]; }
+      P.c[j] = red_sum(s);
+      D.c[j] = red_sum(t);
+    } else {
+      // G = 4: P = a^4 + m3 a^3 + m2 a^2 + m1 a + m0, P' = 4 a^3 + 3 m3 a^2 + 2 m2 a + m1.
+      s += uint64_t(m[3]) * ap.c[2][j] + uint64_t(m[2]) * ap.c[1][j] + uint64_t(m[1]) * ap.c[0][j];
+      t = 4ull * ap.c[2][j] + uint64_t(red_signed(3 * c[3])) * ap.c[1][j] + uint64_t(red_signed(2 * c[2])) * ap.c[0][j];
+      if (j == 0) { s += m[0]; t += m[1]; }
+      P.c[j] = red_sum(s);
+      D.c[j] = red_sum(t);
+    }
   }
   Acc t = acc_zero();
   mul_acc(t, f.n, P);
@@ -110,11 +158,8 @@ k_range_audit(const Wt* __restrict__ vals, uint64_t n, AlphaPowers ap, unsigned 
   extern __shared__ uint32_t bins[];
   for (uint32_t i = threadIdx.x; i < kAuditSmemWords; i += blockDim.x) bins[i] = 0;
   __syncthreads();
-  Fr a[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) a[k] = load(&ap.p[k]);
-  Frac f{zero(), zero()};
-  f.d.c[0] = 1;
+  Frac f[2] = {{zero(), zero()}, {zero(), zero()}};
+  f[0].d.c[0] = f[1].d.c[0] = 1;
   uint32_t* wb = sizeof(Wt) == 1 ? bins + (threadIdx.x >> 5) * 256 : bins;
   const uint64_t chunks = n / kAuditPerChunk;
   const uint64_t per_round = uint64_t(gridDim.x) * kAuditThreads;
@@ -123,25 +168,19 @@ k_range_audit(const Wt* __restrict__ vals, uint64_t n, AlphaPowers ap, unsigned 
   for (uint64_t r = 0; r < rounds; ++r) {
     const uint64_t c = r * per_round + uint64_t(blockIdx.x) * kAuditThreads + threadIdx.x;
     if (c < chunks) {
-      // Four values per group: one word of int8 entries, two of int16.  The
-      // groups run one after the other (words rotate down) to keep few live.
-      uint4 u = __ldg(src + c);
-#pragma unroll 1
-      for (int g = 0; g < kAuditPerChunk / 4; ++g) {
-        int v[4];
-        if constexpr (sizeof(Wt) == 1) {
+      const uint4 u = __ldg(src + c);
+      const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+      int v[kAuditPerChunk];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) v[i] = int(int8_t(u.x >> (8 * i)));
-          u = make_uint4(u.y, u.z, u.w, 0);
-        } else {
-          v[0] = int(int16_t(u.x)); v[1] = int(int16_t(u.x >> 16));
-          v[2] = int(int16_t(u.y)); v[3] = int(int16_t(u.y >> 16));
-          u = make_uint4(u.z, u.w, 0, 0);
-        }
-        audit_group(f, a, v[0], v[1], v[2], v[3]);
-#pragma unroll
-        for (int i = 0; i < 4; ++i) audit_count(wb, v[i]);
+      for (int i = 0; i < kAuditPerChunk; ++i) {
+        if constexpr (sizeof(Wt) == 1) v[i] = int(int8_t(w[i >> 2] >> (8 * (i & 3))));
+        else v[i] = int(int16_t(w[i >> 1] >> (16 * (i & 1))));
       }
+      static_assert(kAuditPerChunk == 2 * kAuditGroup, "two groups per 16-byte chunk");
+      audit_group(f[0], ap, v);
+      audit_group(f[1], ap, v + kAuditGroup);
+#pragma unroll
+      for (int i = 0; i < kAuditPerChunk; ++i) audit_count(wb, v[i]);
     }
     if constexpr (sizeof(Wt) == 2)
       if ((r + 1) % kAuditEpochRounds == 0) audit_flush16(bins, hist);  // uniform over the CTA
@@ -150,7 +189,10 @@ k_range_audit(const Wt* __restrict__ vals, uint64_t n, AlphaPowers ap, unsigned 
   if (blockIdx.x == 0 && threadIdx.x == 0)
     for (uint64_t i = chunks * kAuditPerChunk; i < n; ++i) {
       const int v = int(vals[i]);
-      audit_one(f, a[0], v);
+      Fr alpha;
+#pragma unroll
+      for (int j = 0; j < kC; ++j) alpha.c[j] = ap.c[0][j];
+      audit_one(f[0], alpha, v);
       audit_count(wb, v);
     }
   if constexpr (sizeof(Wt) == 2) {
@@ -164,20 +206,22 @@ k_range_audit(const Wt* __restrict__ vals, uint64_t n, AlphaPowers ap, unsigned 
     }
     __syncthreads();
   }
-  // Fraction sum over the CTA: lanes, then warps (through the counters' memory).
+  // Fraction sum over the CTA: the thread's two, lanes, then warps (through
+  // the counters' memory).
+  Frac t = frac_add(f[0], f[1]);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    Frac g{shfl_xor(f.n, o), shfl_xor(f.d, o)};
-    f = frac_add(f, g);
+    Frac g{shfl_xor(t.n, o), shfl_xor(t.d, o)};
+    t = frac_add(t, g);
   }
   Fr* red = reinterpret_cast<Fr*>(bins);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { red[2 * warp] = f.n; red[2 * warp + 1] = f.d; }
+  if (lane == 0) { red[2 * warp] = t.n; red[2 * warp + 1] = t.d; }
   __syncthreads();
   if (threadIdx.x == 0) {
-    for (int w = 1; w < kAuditWarps; ++w) f = frac_add(f, Frac{red[2 * w], red[2 * w + 1]});
-    store(partials + 2 * blockIdx.x, f.n);
-    store(partials + 2 * blockIdx.x + 1, f.d);
+    for (int w = 1; w < kAuditWarps; ++w) t = frac_add(t, Frac{red[2 * w], red[2 * w + 1]});
+    store(partials + 2 * blockIdx.x, t.n);
+    store(partials + 2 * blockIdx.x + 1, t.d);
   }
 }
 

@@ -53,7 +53,7 @@ def test_audit_matches_the_oracle(field, mode):
 @pytest.mark.parametrize("field", ["f65521", "koalabear"])
 def test_audit_at_sixteen_million_values(field):
     """2^24 entries: every CTA runs many rounds (and flushes its int16
-    counters every 61,440 values)."""
+    counters every 64,512 values)."""
     fid, dt = FIELDS[field]
     shapes = [(4096, 4096)]
     params = qf.Parameters(shapes, qf.Config(20, 4), field=fid)
