@@ -1553,6 +1553,24 @@ bool GpuBackend::multi_eval(const PcsParams<F>& pp, size_t level, const std::vec
   return true;
 }
 
+// The carry's commit_extension_matrix (qafold_short_pc.rs:2327-2362) on the
+// device: the column-major message becomes the codeword's message halves,
+// then the same encode and extension-row hashing as a top round's next layer.
+std::unique_ptr<CodewordView<F>> GpuBackend::commit_carry(const PcsParams<F>& pp, size_t code_index,
+                                                          const std::vector<F>& message, size_t n_cols) {
+  const QaCode<F>& code = pp.seq.codes[code_index];
+  const uint64_t R = code.message_len, total = uint64_t(R) * n_cols;
+  if (R < 128 || message.size() != total || !is_pow2(n_cols)) return nullptr;
+  HostScope hs("decide_carry_commit_dev");
+  DBuf<Fe> msg(total);
+  QF_CK(cudaMemcpyAsync(msg.p, message.data(), total * 16, cudaMemcpyHostToDevice, s_));
+  auto ncw = alloc_codeword(R, n_cols, s_);
+  QF_LAUNCH(s_, "k_to_message_halves", total * 32,
+            qfd::k_to_message_halves<<<grid_for(total, kThreads), kThreads, 0, s_>>>(msg.p, total, ilog2(R), ncw->cw.p));
+  encode_and_hash(*ncw, tables_->alpha(pp, code_index, 1), ilog2(R), ilog2(total), true);
+  return ncw;
+}
+
 // prove_short_qa_direct_code_switch_carry (qafold_short_decide_carry.rs:940-1027)
 // with the message-length vectors in HBM.
 bool GpuBackend::direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,

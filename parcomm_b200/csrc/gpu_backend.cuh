@@ -172,6 +172,9 @@ class GpuBackend : public Backend<F>,
   bool direct_switch(const QaCode<F>& target, size_t target_level, size_t row_factor, const RowSelection& sel,
                      const std::vector<F>& iota, const std::vector<F>& folded_message, F merged_value,
                      const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) override;
+  // Decide carry commitment on the device for codes of at least 128 rows.
+  std::unique_ptr<CodewordView<F>> commit_carry(const PcsParams<F>& pp, size_t code_index, const std::vector<F>& message,
+                                                size_t n_cols) override;
 
   // EO
   void cross_terms(const Query<F>& q, size_t stride, std::vector<F>& pos, std::vector<F>& neg) override;

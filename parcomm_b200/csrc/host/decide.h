@@ -552,8 +552,8 @@ std::vector<F> iota_weights(const std::vector<F>& logical_w, size_t setup_cols, 
 // physical columns and encoded with the next lower code.
 template <class F>
 struct Carry {
-  std::vector<F> message;  // logical column
-  Codeword<F> cw;
+  std::vector<F> message;                // logical column
+  std::unique_ptr<CodewordView<F>> cw;   // on the host, or kept on a device
 };
 
 template <class F>
@@ -643,6 +643,21 @@ Rows<F> open_codeword_rows(const Codeword<F>& cw, const RowSelection& sel) {
   });
   return out;
 }
+// The same rows of a codeword held anywhere (a device codeword gathers them).
+template <class F>
+Rows<F> open_codeword_rows(const CodewordView<F>& cw, const RowSelection& sel) {
+  if (const auto* host = dynamic_cast<const Codeword<F>*>(&cw)) return open_codeword_rows(*host, sel);
+  Rows<F> out;
+  if (sel.all) { out.all = true; out.n_rows = cw.ext_rows(); out.n_cols = cw.cols(); out.encoded = cw.entries(); return out; }
+  auto rows = cw.rows(sel.rows);
+  auto paths = cw.paths(sel.rows);
+  out.partial.resize(sel.rows.size());
+  for (size_t i = 0; i < sel.rows.size(); ++i) {
+    out.partial[i].row = std::move(rows[i]);
+    out.partial[i].path.siblings = std::move(paths[i]);
+  }
+  return out;
+}
 
 template <class F>
 struct SwitchCarry {
@@ -728,6 +743,13 @@ struct DecideAccel {
                              const std::vector<F>& merged_left, PcsTranscript<F>& t, SwitchCarry<F>& out) {
     return false;
   }
+  // The carry commitment (commit_extension_matrix of `message` under
+  // pp.seq.codes[code_index], `n_cols` columns, extension-row leaves) kept on
+  // the device; null leaves it to the host.
+  virtual std::unique_ptr<CodewordView<F>> commit_carry(const PcsParams<F>& pp, size_t code_index,
+                                                        const std::vector<F>& message, size_t n_cols) {
+    return nullptr;
+  }
 };
 
 template <class F>
@@ -784,7 +806,7 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, Dec
     {
       Section sec("decide_open_rows");
       round.setup_rows = open_setup_rows(sl, sel);
-      if (carry) round.carry_rows = open_codeword_rows(carry->cw, sel);
+      if (carry) round.carry_rows = open_codeword_rows(*carry->cw, sel);
     }
     std::vector<F> iw = iota_weights(col_w, ps.setup_cols, ps.carry_cols, merged_left, rf);
     size_t auth_carry_cols = ps.carry_cols * rf;
@@ -820,8 +842,9 @@ DecideProof<F> prove_decide(const PcsParams<F>& pp, const Reduction<F>& red, Dec
       next_carry = std::make_unique<Carry<F>>();
       next_carry->message = recursive;
       Section sec("decide_carry_commit");
-      next_carry->cw = encode_and_commit(nt, recursive, rf, kLeafExtDomain);
-      next_root = next_carry->cw.root();
+      if (accel) next_carry->cw = accel->commit_carry(pp, level - 2, recursive, rf);
+      if (!next_carry->cw) next_carry->cw = std::make_unique<Codeword<F>>(encode_and_commit(nt, recursive, rf, kLeafExtDomain));
+      next_root = next_carry->cw->root();
     } else {
       terminal = recursive;
     }
