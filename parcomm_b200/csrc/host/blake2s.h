@@ -57,6 +57,8 @@ inline void blake2s_compress(uint32_t h[8], const uint8_t block[64], uint64_t t,
   v[d] = rotr32(v[d] ^ v[a], 8);      \
   v[c] = v[c] + v[d];                 \
   v[b] = rotr32(v[b] ^ v[c], 7);
+  // Unrolled, the schedule's indices are constants and m[] stays in registers.
+#pragma GCC unroll 10
   for (int r = 0; r < 10; ++r) {
     const uint8_t* s = kBlake2sSigma[r];
     QF_G(0, 4, 8, 12, m[s[0]], m[s[1]]);

@@ -97,9 +97,24 @@ struct Json {
   std::string s;
   void raw(const char* x) { s += x; }
   void num(uint64_t v) { s += std::to_string(v); }
+  // serde_json's byte arrays: "[b0,b1,...]" in decimal.  The digits of each
+  // byte value come from a table (a large collection's claims hold about
+  // 10^5 bytes).
   void bytes(const uint8_t* p, size_t n) {
+    static const std::array<std::array<char, 4>, 256> digits = [] {
+      std::array<std::array<char, 4>, 256> t{};
+      for (int v = 0; v < 256; ++v) {
+        const std::string d = std::to_string(v);
+        t[v][0] = char(d.size());
+        std::memcpy(&t[v][1], d.data(), d.size());
+      }
+      return t;
+    }();
     s += '[';
-    for (size_t i = 0; i < n; ++i) { if (i) s += ','; s += std::to_string(unsigned(p[i])); }
+    for (size_t i = 0; i < n; ++i) {
+      if (i) s += ',';
+      s.append(&digits[p[i]][1], size_t(digits[p[i]][0]));
+    }
     s += ']';
   }
   template <class F> void scalar(const F& v) { uint8_t e[F::kBytes]; v.to_bytes(e); bytes(e, F::kBytes); }
@@ -144,6 +159,9 @@ struct Claim {
 template <class F>
 std::string claims_json(const std::vector<Claim<F>>& claims) {
   Json j;
+  size_t coords = 0;
+  for (const auto& c : claims) coords += c.row.size() + c.col.size() + 1;
+  j.s.reserve(coords * (F::kBytes * 4 + 2) + claims.size() * 32 + 2);
   j.raw("[");
   for (size_t i = 0; i < claims.size(); ++i) {
     if (i) j.raw(",");
