@@ -791,10 +791,84 @@ F GpuBackend::sumcheck_final_weight() {
   return v;
 }
 
+// Wire records of the selected rows of codewords, gathered on the device
+// into one buffer and copied back once (k_binding_records).
+struct BindingRecords {
+  cudaStream_t s;
+  uint32_t count;
+  DBuf<uint64_t> idx;
+  std::vector<DBuf<uint64_t>> offsets;
+  std::vector<std::pair<uint64_t, uint64_t>> segs;  // (first word, words) per codeword
+  DBuf<uint64_t> buf;
+  uint64_t used = 0;
+  BindingRecords(cudaStream_t stream, const std::vector<size_t>& rows, uint64_t words_cap) : s(stream), count(uint32_t(rows.size())) {
+    std::vector<uint64_t> id(rows.begin(), rows.end());
+    idx.alloc(std::max<size_t>(id.size(), 1));
+    if (!id.empty()) QF_CK(cudaMemcpyAsync(idx.p, id.data(), id.size() * 8, cudaMemcpyHostToDevice, s));
+    buf.alloc(std::max<uint64_t>(words_cap, 1));
+  }
+  static uint64_t words(const DeviceCodeword& cw, size_t count) {
+    return uint64_t(count) * (2 + 2 * uint64_t(cw.n_cols) + 4 * uint64_t(ilog2(cw.n_ext)));
+  }
+  // Enqueues the records of `cw`; returns its segment's index.
+  size_t add(const DeviceCodeword& cw) {
+    const int depth = ilog2(cw.n_ext);
+    const uint64_t w = words(cw, count);
+    check(used + w <= buf.n, "binding record buffer");
+    offsets.emplace_back(cw.level_off.size());
+    QF_CK(cudaMemcpyAsync(offsets.back().p, cw.level_off.data(), cw.level_off.size() * 8, cudaMemcpyHostToDevice, s));
+    const uint64_t items = uint64_t(count) * (uint64_t(cw.n_cols) + depth + 2);
+    check(items <= (uint64_t(1) << 20) * kThreads, "binding records: too many items for one launch");
+    if (items)
+      QF_LAUNCH(s, "k_binding_records", w * 8 + uint64_t(count) * (cw.n_cols * 16 + depth * 32),
+                qfd::k_binding_records<<<grid_for(items, kThreads, 1 << 20), kThreads, 0, s>>>(
+                    cw.cw.p, cw.n_ext, int(cw.n_cols), cw.tree.p, offsets.back().p, depth, idx.p, count, buf.p + used));
+    segs.push_back({used, w});
+    used += w;
+    return segs.size() - 1;
+  }
+  // Copies every segment back (one copy, one synchronisation).
+  std::vector<uint64_t> fetch() {
+    std::vector<uint64_t> h(used);
+    if (used) QF_CK(cudaMemcpyAsync(h.data(), buf.p, used * 8, cudaMemcpyDeviceToHost, s));
+    QF_CK(cudaStreamSynchronize(s));
+    return h;
+  }
+};
+
 std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) {
   ByteWriter w;
   w.bytes("QAFOLDB1", 8);
   w.len(roots.size());
+  if (!sel.all && !src_) {
+    // Resident blocks: every block's records and the folded codeword's in
+    // one gather, then the payload in block order.
+    std::vector<const DeviceCodeword*> cws;
+    for (size_t b = 0; b < roots.size(); ++b) {
+      const DeviceCodeword* cw = b < blocks_.size() ? blocks_[b].get() : nullptr;
+      if (!cw) {  // a repeated zero block: the first committed zero block
+        for (size_t k = 0; k < blocks_.size() && !cw; ++k)
+          if (blocks_[k] && roots_[k] == roots[b]) cw = blocks_[k].get();
+      }
+      if (!cw || cw->root_ != roots[b]) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
+      cws.push_back(cw);
+    }
+    cws.push_back(folded_.get());
+    std::map<const DeviceCodeword*, size_t> seg_of;
+    uint64_t cap = 0;
+    for (const DeviceCodeword* cw : cws)
+      if (!seg_of.count(cw)) { seg_of[cw] = 0; cap += BindingRecords::words(*cw, sel.rows.size()); }
+    BindingRecords rec(s_, sel.rows, cap);
+    for (auto& [cw, seg] : seg_of) seg = rec.add(*cw);
+    const std::vector<uint64_t> h = rec.fetch();
+    for (const DeviceCodeword* cw : cws) {
+      const auto [first, n] = rec.segs[seg_of[cw]];
+      w.u8(0);
+      w.len(sel.rows.size());
+      w.bytes(h.data() + first, n * 8);
+    }
+    return std::move(w.out);
+  }
   auto emit_into = [&](ByteWriter& w, const DeviceCodeword& cw) {
     Rows<F> r;
     if (sel.all) {

@@ -362,6 +362,38 @@ __global__ void k_gather_paths(const uint4* __restrict__ tree, const uint64_t* _
   out[2 * t] = tree[2 * off];
   out[2 * t + 1] = tree[2 * off + 1];
 }
+// Wire records of sampled rows (the partial form of write_rows): per query,
+// u64 n_cols, the row's n_cols elements (16 canonical bytes each, which is
+// their device layout), u64 depth, then the depth sibling digests leaf level
+// first (32 bytes each, the tree's little-endian words).  Record q occupies
+// rec_words = 2 + 2 n_cols + 4 depth u64 words from out + q * rec_words; one
+// thread writes one element, one sibling or one length.
+__global__ void k_binding_records(const Fe* __restrict__ cw, uint64_t n_ext, int n_cols, const uint4* __restrict__ tree,
+                                  const uint64_t* __restrict__ level_off, int depth, const uint64_t* __restrict__ idx,
+                                  uint32_t count, uint64_t* __restrict__ out) {
+  const uint64_t per = uint64_t(n_cols) + uint64_t(depth) + 2;
+  const uint64_t rec_words = 2 + 2 * uint64_t(n_cols) + 4 * uint64_t(depth);
+  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= uint64_t(count) * per) return;
+  const uint64_t q = t / per, k = t % per;
+  uint64_t* rec = out + q * rec_words;
+  if (k < uint64_t(n_cols)) {
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(cw + k * n_ext + idx[q]);
+    rec[1 + 2 * k] = v.x;
+    rec[2 + 2 * k] = v.y;
+  } else if (k < uint64_t(n_cols) + depth) {
+    const int l = int(k - n_cols);
+    const uint64_t off = level_off[l] + ((idx[q] >> l) ^ 1);
+    const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(tree + 2 * off);
+    const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(tree + 2 * off + 1);
+    uint64_t* d = rec + 2 + 2 * uint64_t(n_cols) + 4 * uint64_t(l);
+    d[0] = a.x; d[1] = a.y; d[2] = b.x; d[3] = b.y;
+  } else if (k == uint64_t(n_cols) + depth) {
+    rec[0] = uint64_t(n_cols);
+  } else {
+    rec[1 + 2 * uint64_t(n_cols)] = uint64_t(depth);
+  }
+}
 // out[c] partials: sum_{r in chunk} w[r] * cw[c * n_ext + r], r < n_rows.
 __global__ void k_row_project(const Fe* __restrict__ cw, uint64_t n_ext, uint64_t n_rows, const Fe* __restrict__ hi,
                               const Fe* __restrict__ lo, int lb, Fe* __restrict__ partials) {
