@@ -827,12 +827,13 @@ struct BindingRecords {
     used += w;
     return segs.size() - 1;
   }
-  // Copies every segment back (one copy, one synchronisation).
-  std::vector<uint64_t> fetch() {
-    std::vector<uint64_t> h(used);
-    if (used) QF_CK(cudaMemcpyAsync(h.data(), buf.p, used * 8, cudaMemcpyDeviceToHost, s));
+  // Copies every segment back into page-locked memory (one copy, one
+  // synchronisation); the lease holds them until it is released.
+  PinnedStage::Lease fetch() {
+    PinnedStage::Lease l = PinnedStage::acquire(std::max<uint64_t>(used, 1) * 8);
+    if (used) QF_CK(cudaMemcpyAsync(l.p, buf.p, used * 8, cudaMemcpyDeviceToHost, s));
     QF_CK(cudaStreamSynchronize(s));
-    return h;
+    return l;
   }
 };
 
@@ -860,12 +861,16 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
       if (!seg_of.count(cw)) { seg_of[cw] = 0; cap += BindingRecords::words(*cw, sel.rows.size()); }
     BindingRecords rec(s_, sel.rows, cap);
     for (auto& [cw, seg] : seg_of) seg = rec.add(*cw);
-    const std::vector<uint64_t> h = rec.fetch();
+    uint64_t total = w.out.size();
+    for (const DeviceCodeword* cw : cws) total += 9 + rec.segs[seg_of[cw]].second * 8;
+    w.out.reserve(total);
+    const PinnedStage::Lease lease = rec.fetch();
+    const uint64_t* h = static_cast<const uint64_t*>(lease.p);
     for (const DeviceCodeword* cw : cws) {
       const auto [first, n] = rec.segs[seg_of[cw]];
       w.u8(0);
       w.len(sel.rows.size());
-      w.bytes(h.data() + first, n * 8);
+      w.bytes(h + first, n * 8);
     }
     return std::move(w.out);
   }

@@ -97,6 +97,22 @@ void DevicePool::trim() {
     }
   }
 }
+PinnedStage::Lease PinnedStage::acquire(size_t bytes) {
+  static std::mutex mu;
+  static void* buf = nullptr;
+  static size_t cap = 0;
+  Lease l{std::unique_lock<std::mutex>(mu), nullptr};
+  if (bytes > cap) {
+    if (buf) QF_CK(cudaFreeHost(buf));
+    buf = nullptr;
+    cap = 0;
+    QF_CK(cudaHostAlloc(&buf, bytes, cudaHostAllocPortable));
+    cap = bytes;
+  }
+  l.p = buf;
+  return l;
+}
+
 size_t DevicePool::cached_bytes() {
   const int dev = current_device();
   std::lock_guard<std::mutex> g(g_pool_mu);

@@ -80,6 +80,18 @@ struct DevicePool {
   }
 };
 
+// A process-wide page-locked host buffer for device-to-host copies of proof
+// payloads: a copy into it runs at link speed, where one into pageable memory
+// is staged by the driver.  One holder at a time (the lease keeps a lock);
+// it grows to the largest request and is portable across devices.
+struct PinnedStage {
+  struct Lease {
+    std::unique_lock<std::mutex> lock;
+    void* p = nullptr;
+  };
+  static Lease acquire(size_t bytes);
+};
+
 template <class T>
 struct DBuf {
   T* p = nullptr;

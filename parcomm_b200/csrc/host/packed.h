@@ -344,7 +344,11 @@ BatchOpening<F> open_batch(const PackedPcs<F>& pcs, Backend<F>& be, const std::v
   t0 = std::chrono::steady_clock::now();
   DecideProof<F> dp = prove_decide(*pcs.pp, op.reduction, be.decide_accel());
   out.times.decide_ms = ms_since(t0);
+  const std::vector<uint8_t> ob = opening_to_bytes(op.proof);
+  const std::vector<uint8_t> db = decide_to_bytes(dp);
   ByteWriter w;
+  w.out.reserve(64 + (1 + evaluations.size() + positive.size() + negative.size() + 2 * rounds.size() + 1) * F::kBytes +
+                binding.size() + ob.size() + db.size());
   w.bytes("QAPKBAT1", 8);
   w.field(claimed);
   for (const F& v : evaluations) w.field(v);
@@ -355,10 +359,8 @@ BatchOpening<F> open_batch(const PackedPcs<F>& pcs, Backend<F>& be, const std::v
   w.field(final_value);
   w.len(binding.size());
   w.bytes(binding.data(), binding.size());
-  std::vector<uint8_t> ob = opening_to_bytes(op.proof);
   w.len(ob.size());
   w.bytes(ob.data(), ob.size());
-  std::vector<uint8_t> db = decide_to_bytes(dp);
   w.len(db.size());
   w.bytes(db.data(), db.size());
   if (w.out.size() > 256u * 1024 * 1024) fail(QF_E_ENCODING, "oversize batch proof");
@@ -555,6 +557,8 @@ BatchOpening<F> open_single(const PackedPcs<F>& pcs, SingleBackend<F>& be, const
   t0 = std::chrono::steady_clock::now();
   DecideProof<F> dp = prove_decide(*pcs.pp, op.reduction, be.decide_accel());
   out.times.decide_ms = ms_since(t0);
+  const std::vector<uint8_t> ob = opening_to_bytes(op.proof);
+  const std::vector<uint8_t> db = decide_to_bytes(dp);
   ByteWriter w;
   w.bytes(F::kPackedMagic, 8);
   w.field(claimed);
@@ -562,10 +566,8 @@ BatchOpening<F> open_single(const PackedPcs<F>& pcs, SingleBackend<F>& be, const
   w.len(rounds.size());
   for (const auto& m : rounds) { w.field(m[0]); w.field(m[1]); }
   w.field(final_value);
-  std::vector<uint8_t> ob = opening_to_bytes(op.proof);
   w.len(ob.size());
   w.bytes(ob.data(), ob.size());
-  std::vector<uint8_t> db = decide_to_bytes(dp);
   w.len(db.size());
   w.bytes(db.data(), db.size());
   out.claimed_value = claimed;

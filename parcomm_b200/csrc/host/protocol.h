@@ -479,6 +479,8 @@ struct Proof {
 template <class F>
 std::vector<uint8_t> proof_to_bytes(const Proof<F>& p) {
   ByteWriter w;
+  w.out.reserve(64 + (p.eo.positive.size() + p.eo.negative.size() + 2 * p.eo.rounds.size() + 3) * F::kBytes +
+                p.opening_proof.size());
   w.len(p.eo.positive.size());
   for (const F& v : p.eo.positive) w.field(v);
   w.len(p.eo.negative.size());
