@@ -838,6 +838,7 @@ struct BindingRecords {
 };
 
 std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std::vector<Digest>& roots) {
+  HostScope hs("binding_rows");
   ByteWriter w;
   w.bytes("QAFOLDB1", 8);
   w.len(roots.size());
@@ -1433,6 +1434,7 @@ LiteBullet<F> GpuBackend::litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, Pc
 // Row projection of the systematic half at tensor_weights(point[col_log..]),
 // keeping the row weights in HBM for the top round.
 std::vector<F> GpuBackend::open_top(const DeviceCodeword& cw, const std::vector<F>& point, size_t col_log) {
+  HostScope hs("open_top");
   open_cw_ = &cw;
   const uint64_t n_rows = cw.n_ext / 2;
   tensor_table(std::vector<F>(point.begin() + col_log, point.end()), rw_d_);
