@@ -267,10 +267,10 @@ inline Digest derive_level_seed(const Digest& seed, size_t level) {
   return h.finalize();
 }
 
+// The hasher state after the frames shared by every row of one generator
+// column (domain, field, modulus, seed, message length, index, block).
 template <class F>
-F sample_generator_element(const Digest& seed, size_t message_len, size_t index, size_t block, size_t row) {
-  // Full-extension fields: UNIFORM_BYTES = 16, two 16-byte lanes per digest
-  // (qafold_short.rs:2219-2281).
+Blake2s generator_column_hasher(const Digest& seed, size_t message_len, size_t index, size_t block) {
   Blake2s base;
   const char* dom = "qafold-short/qa-generator-coefficient/v1";
   absorb_framed(base, "domain", dom, std::strlen(dom));
@@ -280,6 +280,13 @@ F sample_generator_element(const Digest& seed, size_t message_len, size_t index,
   absorb_framed_u64(base, "message-length", message_len);
   absorb_framed_u64(base, "index", index);
   absorb_framed_u64(base, "block", block);
+  return base;
+}
+// Full-extension fields: UNIFORM_BYTES = 16, two 16-byte lanes per digest
+// (qafold_short.rs:2219-2281).  `column` is generator_column_hasher's state.
+template <class F>
+F sample_generator_element_from(const Blake2s& column, size_t row) {
+  Blake2s base = column;
   absorb_framed_u64(base, "row", row);
   for (uint64_t attempt = 0;; ++attempt) {
     Blake2s h = base;
@@ -291,6 +298,10 @@ F sample_generator_element(const Digest& seed, size_t message_len, size_t index,
     }
   }
 }
+template <class F>
+F sample_generator_element(const Digest& seed, size_t message_len, size_t index, size_t block, size_t row) {
+  return sample_generator_element_from<F>(generator_column_hasher<F>(seed, message_len, index, block), row);
+}
 
 template <class F>
 Digest qa_generator_digest(const std::vector<std::vector<F>>& alphas) {
@@ -301,12 +312,24 @@ Digest qa_generator_digest(const std::vector<std::vector<F>>& alphas) {
   absorb_framed_u64(h, "modulus", F::modulus_u64());
   absorb_framed_u64(h, "columns", alphas.size());
   absorb_framed_u64(h, "rows", alphas.empty() ? 0 : alphas[0].size());
-  uint8_t enc[F::kBytes];
+  // Each coefficient's frame, u64(11) || "coefficient" || u64(16) || bytes,
+  // is assembled into a batch that is absorbed in one update.
+  static const char kLabel[] = "coefficient";
+  constexpr size_t kL = sizeof(kLabel) - 1, kFrame = 8 + kL + 8 + F::kBytes, kBatch = 256;
+  std::vector<uint8_t> batch(kFrame * kBatch);
+  for (size_t i = 0; i < kBatch; ++i) {
+    uint8_t* f = batch.data() + i * kFrame;
+    for (int k = 0; k < 8; ++k) f[k] = uint8_t(uint64_t(kL) >> (8 * k));
+    std::memcpy(f + 8, kLabel, kL);
+    for (int k = 0; k < 8; ++k) f[8 + kL + k] = uint8_t(uint64_t(F::kBytes) >> (8 * k));
+  }
   for (size_t col = 0; col < alphas.size(); ++col) {
     absorb_framed_u64(h, "column", col);
-    for (const F& v : alphas[col]) {
-      v.to_bytes(enc);
-      absorb_framed(h, "coefficient", enc, F::kBytes);
+    const std::vector<F>& a = alphas[col];
+    for (size_t i = 0; i < a.size(); i += kBatch) {
+      const size_t n = std::min(kBatch, a.size() - i);
+      for (size_t k = 0; k < n; ++k) a[i + k].to_bytes(batch.data() + k * kFrame + 16 + kL);
+      h.update(batch.data(), n * kFrame);
     }
   }
   return h.finalize();
@@ -318,8 +341,12 @@ QaCode<F> sample_systematic(size_t message_len, size_t index, const Digest& seed
   if (message_len == 0 || !is_pow2(message_len) || index <= 1 || !is_pow2(index)) fail(QF_E_ENCODING, "qa shape");
   std::vector<std::vector<F>> cols(index, std::vector<F>(message_len, F::zero()));
   cols[0][0] = F::one();
-  for (size_t b = 1; b < index; ++b)
-    for (size_t r = 0; r < message_len; ++r) cols[b][r] = sample_generator_element<F>(seed, message_len, index, b, r);
+  for (size_t b = 1; b < index; ++b) {
+    const Blake2s column = generator_column_hasher<F>(seed, message_len, index, b);
+    std::vector<F>& out = cols[b];
+#pragma omp parallel for schedule(static) if (message_len >= 4096)
+    for (long r = 0; r < long(message_len); ++r) out[size_t(r)] = sample_generator_element_from<F>(column, size_t(r));
+  }
   F n_inv = F::from_base(uint32_t(message_len % F::kPrime)).inverse();
   for (auto& a : cols) {
     wht_in_place(a.data(), message_len);
