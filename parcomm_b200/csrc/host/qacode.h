@@ -55,13 +55,17 @@ inline uint64_t next_pow2(uint64_t x) { return x <= 1 ? 1 : (uint64_t(1) << (64 
 // order.  Any stage order gives the same exact result.
 template <class F>
 void wht_in_place(F* v, size_t n) {
-  for (size_t half = 1; half < n; half <<= 1)
-    for (size_t blk = 0; blk < n; blk += 2 * half)
-      for (size_t i = blk; i < blk + half; ++i) {
-        F a = v[i], b = v[i + half];
-        v[i] = a + b;
-        v[i + half] = a - b;
-      }
+  // Butterfly k of a level pairs i = (k / half) * 2 half + k % half with
+  // i + half; large transforms spread each level over the OpenMP threads.
+  for (size_t half = 1, lh = 0; half < n; half <<= 1, ++lh) {
+#pragma omp parallel for schedule(static) if (n >= (size_t(1) << 18))
+    for (long k = 0; k < long(n / 2); ++k) {
+      const size_t i = ((size_t(k) >> lh) << (lh + 1)) | (size_t(k) & (half - 1));
+      F a = v[i], b = v[i + half];
+      v[i] = a + b;
+      v[i + half] = a - b;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- distances
@@ -350,7 +354,8 @@ QaCode<F> sample_systematic(size_t message_len, size_t index, const Digest& seed
   F n_inv = F::from_base(uint32_t(message_len % F::kPrime)).inverse();
   for (auto& a : cols) {
     wht_in_place(a.data(), message_len);
-    for (auto& v : a) v = v * n_inv;
+#pragma omp parallel for schedule(static) if (message_len >= 4096)
+    for (long r = 0; r < long(message_len); ++r) a[size_t(r)] = a[size_t(r)] * n_inv;
   }
   QaCode<F> code;
   code.message_len = message_len;
