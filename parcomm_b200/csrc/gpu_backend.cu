@@ -297,6 +297,7 @@ static unsigned tile_grid(uint64_t n_tiles) {
 // The first min(12, logR) WHT levels of a 2^logm-entry half, optionally
 // multiplying by alpha first (a CTA size per variant).
 static void wht_tile_launch(cudaStream_t s, const Fe* src, Fe* dst, const Fe* alpha, int logR, int logm, int wl) {
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   const uint32_t tiles = uint32_t(size_t(1) << (logm - wl));
   if (alpha)
     qfd::k_wht_tile<true><<<tile_grid(tiles), qfd::kAlphaTileThreads, qfd::kTileSmem, s>>>(src, dst, alpha, logR, wl, tiles);
@@ -404,6 +405,7 @@ template <int OP>
 static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int from, int to, bool timed = true,
                            bool allow_tuning = true) {
   if (to <= from) return;
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   if (allow_tuning && PassTuner::enabled() && !g_tuner.ready) g_tuner.tune(s);
   int lo = from;
   for (int k : g_tuner.plan(OP, to - from)) {

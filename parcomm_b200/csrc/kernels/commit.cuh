@@ -24,6 +24,12 @@ namespace QFD_NS {
 __device__ __forceinline__ size_t msg_addr(size_t i, int logR) {
   return ((i >> logR) << (logR + 1)) | (i & ((size_t(1) << logR) - 1));
 }
+// The same in 32 bits, for the transform passes: a block's codeword holds at
+// most 2^31 elements (the launchers check logm <= 30), so every index fits
+// and the per-element address arithmetic takes single-word instructions.
+__device__ __forceinline__ uint32_t msg_addr32(uint32_t i, int logR) {
+  return ((i >> logR) << (logR + 1)) | (i & ((1u << logR) - 1u));
+}
 
 enum ButterflyOp { kMobius = 0, kWht = 1 };
 
@@ -299,8 +305,13 @@ __global__ void __launch_bounds__(ALPHA ? kAlphaTileThreads : kTileThreads, 1)
     k_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha, int logR, int levels, uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
   // For a message-half address a = c * 2R + r, a & (R - 1) = r.
+  // 32-bit addressing, except with ALPHA, whose extension product leaves no
+  // registers for it (that variant spills with it).
   const size_t rmask = (size_t(1) << logR) - 1;
-  auto addr = [=](uint32_t tile, int t) { return msg_addr((size_t(tile) << levels) + t, logR); };
+  auto addr = [=](uint32_t tile, int t) -> size_t {
+    if constexpr (ALPHA) return msg_addr((size_t(tile) << levels) + t, logR);
+    else return msg_addr32((tile << levels) + uint32_t(t), logR);
+  };
   auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + addr(tile, t)); };
   auto conv = [=](uint32_t tile, int t, uint4 raw) {
     const Fr v = unpack_fe(raw);
@@ -319,11 +330,11 @@ template <int OP>
 __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k, int cb,
                                                                       uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  const size_t low_mask = (size_t(1) << lo) - 1;
+  const uint32_t low_mask = (1u << lo) - 1u;
   const int cmask = (1 << cb) - 1;
   auto addr = [=](uint32_t tile, int t) {
-    const size_t g = (size_t(tile) << cb) + (t & cmask);
-    return msg_addr((((g >> lo) << (lo + k)) | (g & low_mask)) + (size_t(t >> cb) << lo), logR);
+    const uint32_t g = (tile << cb) + uint32_t(t & cmask);
+    return msg_addr32((((g >> lo) << (lo + k)) | (g & low_mask)) + (uint32_t(t >> cb) << lo), logR);
   };
   auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(base + addr(tile, t)); };
   auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
