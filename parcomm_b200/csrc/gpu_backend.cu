@@ -479,6 +479,7 @@ Digest GpuBackend::encode_block(const W* bva, uint64_t active, uint64_t src_base
   const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * (F::kLanes * sizeof(W) + 16),
             qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
                 bva, active, src_base, cw.cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
@@ -556,6 +557,7 @@ void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, 
   QF_CK(cudaMemcpyAsync(alpha, top.alphas[1].data(), R * 16, cudaMemcpyHostToDevice, s));
   // Message half: pack + Mobius.
   const int l0 = std::min(qfd::kMaxTileLog, logm);
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
       d_bva, active, uint64_t(b) * P.block_len, cw, logR, l0, uint32_t(uint64_t(1) << (logm - l0)));
   QF_CK(cudaGetLastError());
@@ -741,6 +743,7 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
                 values_.p, folded_->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
   mobius_rest(folded_->cw.p, logm, logR, l0);

@@ -279,7 +279,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const Wt* 
   };
   auto conv = [](uint32_t, int, uint2 raw) { return weights_to_fr(raw); };
   auto st = [=](uint32_t tile, int t, uint4 u) {
-    *reinterpret_cast<uint4*>(cw + msg_addr((size_t(tile) << levels) + t, logR)) = u;
+    *reinterpret_cast<uint4*>(cw + msg_addr32((tile << levels) + uint32_t(t), logR)) = u;
   };
   tile_loop<kMobius, uint2>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
@@ -292,7 +292,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* 
   auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + (size_t(tile) << levels) + t); };
   auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
   auto st = [=](uint32_t tile, int t, uint4 u) {
-    *reinterpret_cast<uint4*>(cw + msg_addr((size_t(tile) << levels) + t, logR)) = u;
+    *reinterpret_cast<uint4*>(cw + msg_addr32((tile << levels) + uint32_t(t), logR)) = u;
   };
   tile_loop<kMobius, uint4>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
