@@ -76,7 +76,7 @@ __device__ __forceinline__ uint4 planar_get_packed(const uint32_t* planes, int e
 // groups); its plane offsets are computed once (pidx is XOR-linear over the
 // disjoint base and level bits).  Consecutive threads take consecutive groups
 // of the same planes.
-template <int OP, int R>
+template <int OP, int R, bool SWAP45 = false>
 __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b, int lvl) {
   const int lg = log_n - R;
   int split = 0;
@@ -87,7 +87,12 @@ __device__ __forceinline__ void planar_stage(uint32_t* planes, int log_n, int b,
 #pragma unroll
   for (int j = 0; j < (1 << R); ++j) off[j] = pidx(j << b);
   for (int item = threadIdx.x; item < (1 << (lg + split)); item += blockDim.x) {
-    const int g = item & ((1 << lg) - 1), c0 = (item >> lg) * ppi;
+    int g = item & ((1 << lg) - 1);
+    const int c0 = (item >> lg) * ppi;
+    // SWAP45 (a radix-4 stage on bits 4..5 of a full tile, lg = 10): swap
+    // group bits 4 and 5, a bijection of [0, 2^lg), so that a warp's groups
+    // cover tile bits 0..3 and 7 (see tile_loop).
+    if (SWAP45) g = (g & ~0x30) | ((g >> 1) & 0x10) | ((g << 1) & 0x20);
     const int pb = pidx((g & bmask) | ((g & ~bmask) << R));
     int q[1 << R];
 #pragma unroll
@@ -236,7 +241,13 @@ __device__ __forceinline__ void tile_loop(uint32_t* planes, int log_n, int b0, u
       if (next < n_tiles)
 #pragma unroll
         for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
-      planar_levels<OP>(planes, log_n, b0, rm, 3);
+      // A radix-4 stage on tile bits 4..5 (b0 = 4) would give a warp's 32
+      // groups tile bits 0..3 and 6; bit 6 enters the banks as swizzle
+      // column 9, which bits 0..3 also reach (2-way conflicts).  With group
+      // bits 4 and 5 swapped the warp covers bits 0..3 and 7 (column 18,
+      // bank bit 4): all 32 banks.
+      if (b0 == 4 && rm == 2) planar_stage<OP, 2, true>(planes, log_n, 4, 3);
+      else planar_levels<OP>(planes, log_n, b0, rm, 3);
       auto st_t = [&](int t, uint4 u) { st(tile, t, u); };
       switch (rz) {
         case 3: pass_tail<OP, 3>(planes, 9 - 3, 3 + rm, st_t); break;
