@@ -76,3 +76,23 @@ def test_reads_span_several_pieces(tmp_path, monkeypatch):
     stream.write_stream(tmp_path / "d.json", tmp_path / "s.bva", shapes, bva)
     m = stream.open_stream(tmp_path / "d.json", tmp_path / "s.bva", qf.Config(14, 4), pinned=False)
     assert np.array_equal(m.bva, bva)
+
+
+def test_reads_stdin_like_the_reference_cli(tmp_path):
+    """`--input -` (main.rs:155-157): the stream comes on standard input."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    d, data = cli_stream_case()
+    (tmp_path / "input.json").write_text(json.dumps(d))
+    code = ("import sys; import parcomm_b200 as qf; from parcomm_b200 import stream; "
+            "m = stream.open_stream(sys.argv[1], '-', qf.Config(10, 4), pinned=False); "
+            "sys.stdout.write(m.bva.tobytes().hex())")
+    root = Path(__file__).resolve().parents[1]
+    ok = subprocess.run([sys.executable, "-c", code, str(tmp_path / "input.json")], input=data, capture_output=True,
+                        cwd=root, timeout=120)
+    assert ok.returncode == 0, ok.stderr.decode()
+    assert bytes.fromhex(ok.stdout.decode()) == data
+    extra = subprocess.run([sys.executable, "-c", code, str(tmp_path / "input.json")], input=data + b"\0",
+                           capture_output=True, cwd=root, timeout=120)
+    assert extra.returncode != 0 and b"excess BVA input" in extra.stderr
