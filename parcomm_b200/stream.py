@@ -28,8 +28,9 @@ from . import FIELD_F65521, FIELD_KOALABEAR, Config, Parameters, QfError, QF_E_A
 from .layout import buckets
 
 FORMAT = "parcomm-dense-bva-stream-description"
-# Little-endian hosts only: int16 payloads are read in place as they lie in the stream.
-assert sys.byteorder == "little"
+# int16 payloads are read in place as they lie in the stream (little-endian).
+if sys.byteorder != "little":
+    raise ImportError("parcomm_b200.stream reads little-endian streams in place; this host is big-endian")
 _DTYPES = {"i8": (np.dtype(np.int8), FIELD_F65521), "i16": (np.dtype(np.int16), FIELD_KOALABEAR)}
 _PIECE = 8 << 20  # bytes per read, as the reference's 8 MiB buffer
 
