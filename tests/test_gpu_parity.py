@@ -357,3 +357,39 @@ def test_all_zero_weights_streamed():
     claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
     proof, _ = p.prove(c, claims)
     assert proof.to_bytes() == o_proof
+
+
+def test_greedy_pass_plan_runs_the_depth8_stage():
+    """QF_TUNE=0 (the greedy split, read before the tuner's first use, hence a
+    fresh process): the 8 Möbius levels above the tile of a chunk-23 statement
+    run as one depth-8 strided pass, whose radix-4 stage on tile bits 4..5
+    takes its groups in swapped order.  Roots and proof equal the oracle's."""
+    import os
+    import subprocess
+    import sys
+    import textwrap
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    code = textwrap.dedent("""
+        import sys
+        sys.path.insert(0, "oracle")
+        import numpy as np
+        import oracle
+        import parcomm_b200 as qf
+        from parcomm_b200 import layout
+        rng = np.random.default_rng(123)
+        w = np.clip(np.rint(rng.normal(0, 20, size=(2048, 4096))), -127, 127).astype(np.int8)
+        p = qf.Parameters([(2048, 4096)], qf.Config(23, 4))
+        bva = layout.encode(p.shapes, [w])
+        o_roots, o_claims, o_proof, _ = oracle.prove(p.shapes, 23, 4, bva)
+        c = p.commit(bva)
+        assert b"".join(c.roots) == o_roots, "roots differ"
+        claims = p.evaluate_claims(c, p.benchmark_points(c.roots))
+        assert qf.claims_to_bytes(claims) == o_claims, "claims differ"
+        proof, _ = p.prove(c, claims)
+        assert proof.to_bytes() == o_proof, "proof differs"
+        print("greedy-ok")
+    """)
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=dict(os.environ, QF_TUNE="0"),
+                       capture_output=True, timeout=900)
+    assert r.returncode == 0 and b"greedy-ok" in r.stdout, r.stderr.decode()[-3000:]
