@@ -37,9 +37,10 @@ enum ButterflyOp { kMobius = 0, kWht = 1 };
 // A shared-memory tile holds each of the 8 coefficients of its elements in a
 // separate 32-bit plane.  Entry e of a plane sits at e ^ swz(e >> 5), an XOR
 // of its bank bits with a GF(2)-linear image of bits 5..7 (columns 4, 9, 18):
-// every warp access of the butterfly stages below (groups at bit offsets 0,
-// 2 and 3, radix 2..8) and of the load/store loops then hits 32 distinct
-// banks.  Butterflies run in radix-8 register stages on lazily reduced
+// every warp access of the load/store loops and of the butterfly stages the
+// passes run (radix 8 at bit offsets 0, 2 and 3, radix 2 at bit 5, and radix
+// 4 at bit 4 with its groups' bits 4 and 5 swapped, see tile_loop) then hits
+// 32 distinct banks.  Butterflies run in radix-8 register stages on lazily reduced
 // values: a value entering level l of a pass is < 2^l * p, a difference is
 // formed as a + 2^l p - b, so twelve levels stay below 2^28 and one
 // reduction per pass suffices.  Both transforms act coefficient-wise over F_p.
