@@ -1,7 +1,8 @@
 """LogUp range audit on the CPU: the oracle against a pure-Python restatement
 (hashlib BLAKE2s for alpha, big-integer field arithmetic, a Fermat
 inversion), the identity on edge-value multisets, rejection of altered
-multiplicities, and the C ABI's argument checks without a device."""
+multiplicities, the library's host table sum (batched inversion) against
+the direct sum, and the C ABI's argument checks without a device."""
 import ctypes
 import hashlib
 import struct
@@ -152,3 +153,17 @@ def test_capi_checks_arguments_without_a_device():
     holds = ctypes.c_int(7)
     rc = L.qf_range_audit(None, None, b"\x00" * 32, None, 0, None, None, None, ctypes.byref(holds))
     assert rc == qf.QF_E_ARGUMENT and holds.value == 7
+
+
+def test_host_table_sum_batched_inversion(tmp_path):
+    """The library's host table sum (one batched inversion) against the direct
+    per-term sum, both fields, compiled with the host compiler."""
+    import json
+    import subprocess
+    from pathlib import Path
+    src = Path(__file__).resolve().parent / "range_audit_check.cpp"
+    exe = tmp_path / "range_audit_check"
+    subprocess.run(["/usr/bin/g++", "-std=c++17", "-O2", str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert r.returncode == 0 and out["mismatches"] == 0 and out["checked"] == 48, out
