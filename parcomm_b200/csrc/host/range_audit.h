@@ -59,16 +59,6 @@ F range_audit_alpha(const uint8_t seed[32]) {
   }
 }
 
-// A sum of fractions kept as numerator / denominator.
-template <class F>
-struct Fraction {
-  F num = F::zero(), den = F::one();
-};
-template <class F>
-Fraction<F> fraction_add(const Fraction<F>& a, const Fraction<F>& b) {
-  return {a.num * b.den + b.num * a.den, a.den * b.den};
-}
-
 // sum_t m_t / (alpha - t) over the nonzero multiplicities, with one field
 // inversion (prefix products, Montgomery's batch inversion).
 template <class F, class W>
