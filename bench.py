@@ -423,8 +423,11 @@ def run_reference(args):
     sixteen = args.workload in ("8b16", "layers16", "70b16")
     field = "koalabear" if sixteen else "f65521"
     packed_log = 6 if args.workload == "70b16" else 4
+    chunk_log = 24
     if args.workload == "70b16":  # one 70B decoder layer's attention projections
         shapes = [(8192, 8192), (1024, 8192), (1024, 8192)]
+    elif args.workload == "smoke":  # the whole smoke configuration
+        shapes, chunk_log = [(1024, 4096)], 20
     rng = np.random.default_rng(0)
     mats = []
     for r, c in shapes:
@@ -445,25 +448,26 @@ def run_reference(args):
     times = []
     for step in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, 24, packed_log, bva, field=field)
+        roots, claims, proof, (commit_ms, open_ms) = oracle.prove(shapes, chunk_log, packed_log, bva, field=field)
         dt = time.perf_counter() - t0
         if step >= args.warmup:
             times.append((commit_ms + open_ms) / 1000.0)
     sec = statistics.mean(times)
     value = weights / sec
-    layer = "3 matrices of one 70B decoder layer (q,k,v" if args.workload == "70b16" else \
-        "4 matrices of one 8B decoder layer (q,k,v,o"
+    layer = {"70b16": "3 matrices of one 70B decoder layer (q,k,v", "smoke": "the whole smoke workload (1024x4096"}.get(
+        args.workload, "4 matrices of one 8B decoder layer (q,k,v,o")
     sample = (f"{layer}: {weights} "
-              f"{'BF16 payloads' if sixteen else 'int8 weights'}), chunk_log 24, packed_log {packed_log}, "
+              f"{'BF16 payloads' if sixteen else 'int8 weights'}), chunk_log {chunk_log}, packed_log {packed_log}, "
               f"C++ restatement of the reference CPU prover (OpenMP, {threads} threads)")
     line = {
         "impl": "reference", "metric": "QAFold commit+open weights/s", "value": value, "unit": "weights/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int16" if sixteen else "int8",
-        "data": "synthetic", "config": {"workload": ("70B-shape 16-bit weights, streamed (sample)" if args.workload == "70b16"
-                                                     else f"8B-shape {16 if sixteen else 8}-bit weights, batched (sample)"),
+        "data": "synthetic", "config": {"workload": {"70b16": "70B-shape 16-bit weights, streamed (sample)",
+                                                     "smoke": "smoke 1024x4096 int8"}.get(
+                                            args.workload, f"8B-shape {16 if sixteen else 8}-bit weights, batched (sample)"),
                                         "field": "KoalaBear^4" if sixteen else "F65521^8",
-                                        "chunk_log": 24, "packed_log": packed_log, "sample": sample},
+                                        "chunk_log": chunk_log, "packed_log": packed_log, "sample": sample},
         "cpu_baseline": {"value": value, "unit": "weights/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "weights/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
