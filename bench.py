@@ -23,6 +23,9 @@ setup and claim generation are outside it.  The claims are computed once
            each committed and proven as its own single-matrix statement.
   range_audit : the LogUp range audit of the same weights (Committed.range_audit),
            a check beside the proof, timed once outside the step.
+  recompute : the same step in the reference's measured mode (--cache-mode
+           recompute, Parameters.commit_recomputed): only the roots stay on
+           the device and binding re-encodes every block; same proof bytes.
 
 `--impl reference` times the CPU restatement of the reference prover (the
 oracle; the Rust reference cannot be built in this image) with all host
@@ -499,7 +502,9 @@ def main():
     ap.add_argument("--no-per-matrix", action="store_true",
                     help="skip the per-matrix comparison (each matrix proven on its own)")
     ap.add_argument("--no-audit", action="store_true", help="skip the LogUp range audit measurement")
-    ap.add_argument("--out", default=str(ROOT / "gpurun_out"))
+    ap.add_argument("--no-recompute", action="store_true",
+                    help="skip the recompute-mode measurement (the reference's --cache-mode recompute)")
+    ap.add_argument("--out", default=str(ROOT / "bench_out"), help="directory for the clock samples and kernel stats")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -581,11 +586,13 @@ def main():
 
     res_blocks = [0, 0]
 
-    def step(on_device: bool):
-        cc = commit(on_device)
+    def step(on_device: bool, commit_fn=None):
+        cc = (commit_fn or commit)(on_device)
         pr, pf = params.prove(cc, claims)
         if streamed:
             h2d, res_blocks[0], res_blocks[1] = cc.stream_info()
+        elif commit_fn is not None:  # recompute mode: the copies the stream made (none for device weights)
+            h2d = cc.stream_info()[0]
         else:
             h2d = 0 if on_device else active * entry_bytes
         cc.close()
@@ -599,14 +606,14 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    def timed(on_device: bool, steps: int):
+    def timed(on_device: bool, steps: int, commit_fn=None):
         barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         launches0 = qf.kernel_launches()
         ev0.record()
         last = None
         for _ in range(steps):
-            last = step(on_device)
+            last = step(on_device, commit_fn)
         ev1.record()
         barrier()
         ms = max_over_ranks(ev0.elapsed_time(ev1), world)
@@ -621,6 +628,34 @@ def main():
     else:
         ms_e2e, (pr_e2e, pf_e2e, h2d_e2e), _ = timed(False, max(1, args.steps))
     assert pr_dev.to_bytes() == proof.to_bytes() == pr_e2e.to_bytes(), "proof bytes changed between steps"
+
+    # The reference's measured mode (--cache-mode recompute): only the roots
+    # stay on the device after the commit, and binding re-encodes every block
+    # and checks its root (qafold_short_batch.rs:118-160).  Same weights, same
+    # claims, same proof bytes; timed the same way, after its own warm-up.
+    recompute = None
+    if not args.no_recompute and not streamed:
+        def commit_rc(on_device: bool):
+            return params.commit_recomputed(bva_dev if on_device else bva_host, resident_bytes=None)
+
+        for _ in range(max(args.warmup, 1)):
+            step(True, commit_rc)
+        ms_rc, (pr_rc, pf_rc, _), _ = timed(True, args.steps, commit_rc)
+        ms_rc_e2e, (pr_rc_e2e, _, h2d_rc), _ = timed(False, max(1, args.steps), commit_rc)
+        assert pr_rc.to_bytes() == proof.to_bytes() == pr_rc_e2e.to_bytes(), "recompute-mode proof bytes differ"
+        rc_alg, rc_terms = step_alg_bytes(active, params.logical, cfg.chunk_log, cfg.packed_log, 4 if sixteen else 8,
+                                          entry_bytes, True)
+        recompute = {
+            "value": job_throughput(weights, world, ms_rc), "unit": "weights/s", "ms_per_step": ms_rc,
+            "e2e": {"value": job_throughput(weights, world, ms_rc_e2e), "unit": "weights/s", "ms_per_step": ms_rc_e2e,
+                    "h2d_bytes_per_step": h2d_rc, "d2h_bytes_per_step": len(pr_rc.to_bytes())},
+            "stage_ms": {k: getattr(pf_rc, k) for k in ("commit_ms", "eo_ms", "projection_ms", "folding_ms",
+                                                       "sumcheck_ms", "binding_ms", "native_opening_ms", "decide_ms",
+                                                       "open_ms")},
+            "step_alg_bytes": rc_alg, "binding_alg_gb": round(rc_terms["binding"] / 1e9, 2),
+            "what": "Parameters.commit_recomputed over the same weights (device-resident for value, pinned host "
+                    "memory for e2e): only roots kept, binding re-encodes and root-checks every block; proof bytes "
+                    "identical to the cache-mode step"}
 
     # Per-kernel device time (CUDA events on each launch's own stream), one extra step.
     qf.kernel_timing(True)
@@ -734,6 +769,7 @@ def main():
         "link_roofline": link,
         "cpu_baseline": cpu_baseline,
         "per_matrix": per_matrix,
+        "recompute": recompute,
         "range_audit": range_audit,
         "clocks": clocks.summary(local),
         "proof_bytes": proof_bytes,

@@ -181,13 +181,20 @@ size_t qf_last_error(char* buf, size_t cap);
  * Limit: F65521 blocks of at most 2^QF_NOALLOC_MAX_CHUNK_LOG weights
  * (config chunk_log <= 20); larger blocks return QF_E_ARGUMENT.  All working
  * buffers live in one static device array of QF_NOALLOC_SCRATCH_BYTES, which
- * every GPU that loads the library holds until the process exits.  The first
- * call on a device looks up that array's address there (cudaGetSymbolAddress);
- * make that first call before any stream capture.  Every call shares the
- * array, which keeps the last call's contents (nothing in it has to start at
- * zero: each word a call reads, the same call wrote first); calls that
- * overlap on the GPU (other streams or host threads on the same device) race,
- * so serialise them. */
+ * every GPU that loads the library holds until the process exits.  The call
+ * runs on the current device and uses that device's copy of the array:
+ * d_bva, d_root and the stream must belong to it (QF_E_ARGUMENT otherwise).
+ * The first call on a device looks up that array's address there
+ * (cudaGetSymbolAddress), and looks it up again if the device's context has
+ * changed since (after cudaDeviceReset); make that first call before any
+ * stream capture.  The array also holds the code's alpha table: a call whose
+ * parameter set differs from the previous call's on that device copies the
+ * table in from host memory and waits for that copy (the host blocks until
+ * the stream reaches it); calls with the same parameter set copy nothing.
+ * Every call shares the array, which keeps the last call's contents (nothing
+ * in it has to start at zero: each word a call reads, the same call or the
+ * table copy wrote first); calls that overlap on the GPU (other streams or
+ * host threads on the same device) race, so serialise them. */
 #define QF_NOALLOC_MAX_CHUNK_LOG 20
 #define QF_NOALLOC_SCRATCH_BYTES (5u << 20)
 int qf_commit_block_noalloc(const qf_params* params, const int8_t* d_bva, uint64_t n_values, uint64_t block,

@@ -546,15 +546,13 @@ static void strided_passes_plain(cudaStream_t s, Fe* base, int logR, int logm, i
 }
 
 void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
-                       Fe* alpha, uint8_t* d_root, cudaStream_t s) {
+                       const Fe* alpha, uint8_t* d_root, cudaStream_t s) {
   configure_tile_kernels();
   const int logm = ilog2(P.pcs.packed_len());
   const size_t cols = P.pcs.pp->extension_columns;
   const int logR = logm - ilog2(cols);
   const size_t R = size_t(1) << logR;
-  const auto& top = P.pcs.pp->seq.top();
-  check(top.message_len == R, "alpha table length");
-  QF_CK(cudaMemcpyAsync(alpha, top.alphas[1].data(), R * 16, cudaMemcpyHostToDevice, s));
+  check(P.pcs.pp->seq.top().message_len == R, "alpha table length");
   // Message half: pack + Mobius.
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");

@@ -102,11 +102,12 @@ class BlockStream {
 
 // Commitment root of block `b` of a device BVA (`active` entries), computed
 // only in the caller's device buffers: `cw` holds 2R x cols entries, `tree`
-// 4 x 2R words (2 x 2R digests), `alpha` R entries (overwritten with the
-// code's alpha table).  Launches on `s`, writes the 32-byte root to the device
-// bytes `d_root` and returns without synchronising; allocates no device memory.
+// 4 x 2R words (2 x 2R digests), `alpha` the R entries of the top code's
+// alpha table (alphas[1]), already on the device.  Launches on `s`, writes the
+// 32-byte root to the device bytes `d_root` and returns without
+// synchronising; allocates no device memory.
 void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
-                       Fe* alpha, uint8_t* d_root, cudaStream_t s);
+                       const Fe* alpha, uint8_t* d_root, cudaStream_t s);
 
 class GpuBackend : public Backend<F>,
                    public SingleBackend<F>,

@@ -53,4 +53,6 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: extract_reference_vectors.py <reference checkout>")
+    main(Path(sys.argv[1]))

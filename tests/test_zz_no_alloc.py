@@ -71,3 +71,43 @@ def test_noalloc_rejects_blocks_beyond_the_limit():
     with pytest.raises(qf.QfError) as e:
         p.block_root_noalloc(bva, 0, root)
     assert e.value.code == -9 and "exceeds the limit of 2^20" in str(e.value)
+
+
+def test_noalloc_back_to_back_on_a_caller_stream():
+    """Several calls queued on a caller-owned stream with no host sync in
+    between, each writing its own root slot, then one sync: every root equals
+    qf_commit's.  A parameter set change in the middle (chunk 16, then 20)
+    re-uploads the alpha table between calls."""
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    cases = []
+    for chunk, seed in ((16, 21), (20, 22)):
+        p = qf.Parameters(SHAPES, qf.Config(chunk_log=chunk, packed_log=4))
+        bva = device_bva(p, seed)
+        c = p.commit(bva, on_device=True)
+        cases.append((p, bva, list(c.roots)))
+        c.close()
+    slots = torch.zeros(sum(p.blocks for p, _, _ in cases), 32, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()  # the weights and the zeroed slots are complete before the caller's stream reads them
+    k = 0
+    for p, bva, _ in cases:
+        for b in range(p.blocks):
+            p.block_root_noalloc(bva, b, slots[k], stream.cuda_stream)
+            k += 1
+    stream.synchronize()
+    got = [bytes(r) for r in slots.cpu().numpy()]
+    k = 0
+    for p, _, roots in cases:
+        for b in range(p.blocks):
+            assert got[k] == roots[b], f"chunk {p.config.chunk_log} block {b}: root differs from qf_commit"
+            k += 1
+
+
+def test_noalloc_rejects_host_memory():
+    torch.cuda.set_device(0)
+    p = qf.Parameters(SHAPES, qf.Config(chunk_log=16, packed_log=4))
+    bva = device_bva(p, 4)
+    host_root = torch.zeros(32, dtype=torch.uint8)
+    with pytest.raises(qf.QfError) as e:
+        p.block_root_noalloc(bva, 0, host_root)
+    assert e.value.code == -9 and "current device" in str(e.value)
