@@ -673,11 +673,26 @@ def main():
 
     alg_total, alg_terms = step_alg_bytes(active, params.logical, cfg.chunk_log, cfg.packed_log,
                                           4 if sixteen else 8, entry_bytes, streamed)
+    # Integer roofline: the measured issue peaks (microbenchmark) against the
+    # algorithmic integer operations the library counts per launch.
+    int_peaks = qf.int_peaks()
+    issue_peak = int_peaks["issue_ops_per_s"]
+    kernel_stats = {k: v for k, v in stats.items() if not k.startswith(("host:", "_"))}
+    step_ops = sum(v.get("ops", 0) for v in kernel_stats.values())
+    counted_ms = sum(v["ms"] for v in kernel_stats.values() if v.get("ops", 0))
+    hbm_frac = alg_total / (ms_dev / 1000.0) / 1e9 / peak
+    alu_frac = step_ops / (ms_dev / 1000.0) / issue_peak
     step_roofline = {"bound": "hbm", "alg_bytes": alg_total, "achieved": alg_total / (ms_dev / 1000.0) / 1e9,
-                     "peak": peak, "unit": "GB/s", "frac": alg_total / (ms_dev / 1000.0) / 1e9 / peak,
+                     "peak": peak, "unit": "GB/s", "frac": hbm_frac,
                      "peak_source": peak_kind, "terms_gb": {k: round(v / 1e9, 2) for k, v in alg_terms.items()},
+                     "alu": {"alg_ops": step_ops, "achieved_ops_per_s": step_ops / (ms_dev / 1000.0),
+                             "peak_ops_per_s": issue_peak, "frac": alu_frac, "counted_kernel_ms": counted_ms,
+                             "what": "integer operations the arithmetic needs (transform butterflies, reductions, "
+                                     "extension products, BLAKE2s compressions) in the kernels that count them, over "
+                                     "the step time, against the measured issue peak of both integer pipes"},
+                     "max_frac": max(hbm_frac, alu_frac), "max_bound": "alu" if alu_frac > hbm_frac else "hbm",
                      "what": "the whole step's compulsory bytes (each materialised vector written once, read once "
-                             "per dependent pass) over its time; the step is bound by integer work, not by them"}
+                             "per dependent pass) and counted integer operations over its time"}
 
     link = None
     if streamed:  # the host link bounds a streamed step: bytes copied per step against a measured copy
@@ -764,7 +779,17 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic, "kernel_ms_per_step": d["ms"], "kernel_launches": d["launches"],
-                     "alg_bytes_per_launch": d["bytes"] / max(d["launches"], 1)},
+                     "alg_bytes_per_launch": d["bytes"] / max(d["launches"], 1),
+                     "alu": ({"alg_ops_per_launch": d["ops"] / max(d["launches"], 1),
+                              "achieved_ops_per_s": d["ops"] / (d["ms"] / 1000.0), "peak_ops_per_s": issue_peak,
+                              "frac": d["ops"] / (d["ms"] / 1000.0) / issue_peak, "peak_source": "measured in this run"}
+                             if d.get("ops") else None)},
+        "int_peaks": int_peaks,
+        "kernels": {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                        "hbm_frac": round(v["bytes"] / (v["ms"] / 1000.0) / 1e9 / peak, 3) if v["ms"] > 0 else None,
+                        "alu_frac": (round(v["ops"] / (v["ms"] / 1000.0) / issue_peak, 3)
+                                     if v.get("ops") and v["ms"] > 0 else None)}
+                    for k, v in sorted(kernel_stats.items(), key=lambda kv: -kv[1]["ms"])[:14]},
         "step_roofline": step_roofline,
         "link_roofline": link,
         "cpu_baseline": cpu_baseline,

@@ -62,7 +62,8 @@ EXPORTED = (
     "qf_params_new", "qf_params_free", "qf_params_info", "qf_commit", "qf_committed_free", "qf_statement_json",
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
     "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
-    "qf_committed_stream_info", "qf_open", "qf_device_cache_limit", "qf_range_audit",
+    "qf_committed_stream_info", "qf_open", "qf_device_cache_limit", "qf_range_audit", "qf_kernel_int_peaks",
+    "qf_kernel_option",
 )
 
 
@@ -100,6 +101,8 @@ def lib() -> ctypes.CDLL:
         L.qf_kernel_launches.argtypes = []
         L.qf_kernel_launches.restype = U64
         L.qf_device_cache_limit.argtypes = [U64]
+        L.qf_kernel_int_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        L.qf_kernel_option.argtypes = [ctypes.c_char_p, ctypes.c_int]
         L.qf_commit_block_noalloc.argtypes = [P, P, U64, U64, P, P]
         L.qf_range_audit.argtypes = [P, P, ctypes.c_char_p, P, S, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                      ctypes.POINTER(ctypes.c_int)]
@@ -447,6 +450,23 @@ def device_cache_limit(nbytes: int) -> None:
 
 def kernel_launches() -> int:
     return int(lib().qf_kernel_launches())
+
+
+def kernel_option(name: str, value: int) -> None:
+    """qf_kernel_option: "imma" (tensor-core weight passes, default on) or
+    "per_matrix" (one launch per term / bucket / block, default off); both
+    settings write identical bytes."""
+    _check(lib().qf_kernel_option(name.encode(), int(value)))
+
+
+def int_peaks() -> dict:
+    """The device's measured integer issue peaks (thread-level operations/s):
+    the ALU pipe (XOR chains), the FMA pipe (multiply-add chains), both
+    interleaved, and widening 32 x 32 -> 64-bit multiply-adds; the
+    denominators of the integer roofline."""
+    out = (ctypes.c_double * 4)()
+    _check(lib().qf_kernel_int_peaks(out))
+    return {"alu_ops_per_s": out[0], "fma_ops_per_s": out[1], "issue_ops_per_s": out[2], "mad_wide_per_s": out[3]}
 
 
 def demo_shapes() -> List[Shape]:

@@ -15,7 +15,7 @@ LIB = LIB_DIR / "libparcomm_qafold.so"
 # gpu_backend_kb.cu / capi_field_kb.cu recompile gpu_backend.cu / capi_field.cu
 # for KoalaBear^4 (QF_FIELD_KB); the others are F65521^8 or field-independent.
 SOURCES = [PKG / "csrc" / n for n in ("capi.cu", "gpu_common.cu", "gpu_backend.cu", "capi_field.cu", "noalloc.cu",
-                                      "gpu_backend_kb.cu", "capi_field_kb.cu")]
+                                      "intpeak.cu", "gpu_backend_kb.cu", "capi_field_kb.cu")]
 OBJ_DIR = PKG / "_build"
 HEADERS = sorted((PKG / "csrc").rglob("*.h")) + sorted((PKG / "csrc").rglob("*.cuh"))
 

@@ -179,6 +179,15 @@ int qf_kernel_timing(int enable) {
   return guarded([&] { qfg::KernelClock::reset(enable != 0); });
 }
 
+int qf_kernel_option(const char* name, int value) {
+  return guarded([&] {
+    const std::string n = name ? name : "";
+    if (n == "imma") qfg::KernelOptions::imma = value != 0;
+    else if (n == "per_matrix") qfg::KernelOptions::per_matrix = value != 0;
+    else fail(QF_E_ARGUMENT, "unknown kernel option: " + n);
+  });
+}
+
 int qf_kernel_stats(char* buf, size_t cap, size_t* len) {
   return guarded([&] {
     std::string j = qfg::KernelClock::stats_json();

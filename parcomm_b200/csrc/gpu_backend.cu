@@ -4,6 +4,10 @@
 #include "kernels/open.cuh"
 #include "kernels/vec.cuh"
 #include "kernels/audit.cuh"
+#if !defined(QF_FIELD_KB)
+#include "kernels/imma_f65521.cuh"
+#endif
+#include "intops.h"
 
 #include <algorithm>
 #include <map>
@@ -13,6 +17,31 @@
 namespace QFB_NS {
 
 static constexpr int kThreads = 256;
+// Operation counts of this field's arithmetic, for the integer roofline.
+#if defined(QF_FIELD_KB)
+static constexpr const qf_intops::FieldOps& kOps = qf_intops::kKoalaBear;
+#else
+static constexpr const qf_intops::FieldOps& kOps = qf_intops::kF65521;
+#endif
+
+// The exact integer-limb tensor-core kernels exist for F65521^8 (8-bit
+// weights); KoalaBear keeps its 64-bit IMAD kernels.
+static bool imma_on() {
+#if defined(QF_FIELD_KB)
+  return false;
+#else
+  return KernelOptions::imma.load() != 0;
+#endif
+}
+// Grid of the persistent tensor-core weight kernels: four CTAs per SM.
+static unsigned mma_grid() {
+  static const int sms = [] {
+    int d = 0, n = 148;
+    if (cudaGetDevice(&d) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d) != cudaSuccess) n = 148;
+    return n;
+  }();
+  return unsigned(sms * 4);
+}
 
 template <class K>
 static void set_smem(K kernel, size_t bytes) {
@@ -113,6 +142,8 @@ static void configure_tile_kernels() {
   set_smem(qfd::k_wht_tile<true>, bytes);
   set_smem(qfd::k_butterfly_strided<qfd::kMobius>, bytes);
   set_smem(qfd::k_butterfly_strided<qfd::kWht>, bytes);
+  set_smem(qfd::k_mobius_wht_strided, bytes);
+  set_smem(qfd::k_wht_alpha_wht_tile, bytes + qfd::kAlphaStageSmem);
   done.insert(dev);
 }
 
@@ -341,7 +372,8 @@ struct PassTuner {
     float best = 1e30f;
     for (int rep = 0; rep < 4; ++rep) {
       QF_CK(cudaEventRecord(a, s));
-      qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(buf, kLogm, kLo, k, cb, tiles);
+      qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(buf, buf, kLogm, kLo, k, cb,
+                                                                                                  tiles);
       QF_CK(cudaGetLastError());
       QF_CK(cudaEventRecord(b, s));
       QF_CK(cudaEventSynchronize(b));
@@ -397,12 +429,26 @@ struct PassTuner {
 PassTuner g_tuner;
 }  // namespace
 
-// Butterfly levels [from, to) over a half (message or parity at `base`) of
-// 2^logm entries, in strided passes of at most 10 levels (the tuner's split).
-// `to` is logR for the per-column WHT and logm for the Mobius transform of the
-// whole message.  `allow_tuning` is false on the allocation-free path.
+// One launch, recorded by the kernel clock (timed) or plain (the
+// allocation-free path).
+template <class Fn>
+static void launch(cudaStream_t s, bool timed, const char* name, uint64_t bytes, uint64_t ops, Fn&& fn) {
+  if (timed) {
+    QF_LAUNCH_OPS(s, name, bytes, ops, fn());
+  } else {
+    fn();
+    QF_CK(cudaGetLastError());
+  }
+}
+
+// Butterfly levels [from, to) over a half of 2^logm entries, in strided
+// passes of at most 10 levels (the tuner's split).  The first pass reads
+// `src` and writes `dst`; the others work in place on `dst` (src == dst: all
+// in place).  `to` is at most logR for the per-column WHT and logm for the
+// Mobius transform of the whole message.  `allow_tuning` is false on the
+// allocation-free path.
 template <int OP>
-static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int from, int to, bool timed = true,
+static void strided_passes(cudaStream_t s, const Fe* src, Fe* dst, int logR, int logm, int from, int to, bool timed = true,
                            bool allow_tuning = true) {
   if (to <= from) return;
   check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
@@ -411,49 +457,106 @@ static void strided_passes(cudaStream_t s, Fe* base, int logR, int logm, int fro
   for (int k : g_tuner.plan(OP, to - from)) {
     const int cb = strided_cb(k, logm);
     const uint32_t tiles = uint32_t(uint64_t(1) << (logm - k - cb));
-    if (timed) {
-      QF_LAUNCH(s, "k_butterfly_strided", (uint64_t(2) << logm) * 16,
-                qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(
-                    base, logR, lo, k, cb, tiles));
-    } else {
-      qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(base, logR, lo, k, cb, tiles);
-      QF_CK(cudaGetLastError());
-    }
+    const uint64_t n = uint64_t(1) << logm;
+    const uint64_t ops = qf_intops::transform_ops(kOps, n, OP == qfd::kWht ? k : 0, OP == qfd::kMobius ? k : 0, 1, 0);
+    launch(s, timed, "k_butterfly_strided", 2 * n * 16, ops, [&] {
+      qfd::k_butterfly_strided<OP><<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(src, dst, logR, lo, k, cb,
+                                                                                                tiles);
+    });
+    src = dst;
     lo += k;
   }
 }
 
-void GpuBackend::mobius_rest(Fe* cw, int logm, int logR, int from) { strided_passes<qfd::kMobius>(s_, cw, logR, logm, from, logm); }
-
-// Parity = WHT(alpha * WHT(message)) per column, then leaf hashes and tree.
-void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain) {
+// The transform passes of one codeword (2^logm message entries in 2^(logm -
+// logR) columns of R = 2^logR rows, message half at cw, parity at cw + R).
+// On entry the message half holds the packed message with its Mobius levels
+// [0, mob_from) applied; mob_from = logm when the message needs none (the
+// extension codewords).  On return the message half holds the Mobius
+// transform of the whole message (mobius_in_place, packed.rs:708-752) and
+// the parity half WHT(alpha * WHT(message)) per column (qafold_short.rs:
+// 975-1002).
+//
+// Every level is a 2 x 2 map on one index bit, and maps on different bits
+// commute, so the passes group them by the bits a tile covers (12 per tile;
+// the tile levels 0..11 of a column are its low 12 bits):
+//   1. Mobius on the bits above the fused span (the column bits [logR, logm),
+//      plus any within-column bits above 22), strided, in place;
+//   2. Mobius then WHT #1 on the fused span [12, min(logR, 22)) in one
+//      strided pass, writing the message (now final) and the parity;
+//   3. WHT #1 on within-column bits above 22 (KoalaBear, logR = 23);
+//   4. WHT #1 on bits 0..11, alpha, WHT #2 on bits 0..11: one tile pass;
+//   5. WHT #2 on [12, logR), strided.
+// A fused span of fewer than 6 levels leaves too few bits for the fused
+// pass's register stages; its Mobius levels then join pass 1 and its WHT
+// levels run as a strided pass from the message into the parity.  Columns
+// shorter than one tile (logR < 12) take one tile pass per WHT.
+static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int logm, int mob_from, bool timed,
+                          bool allow_tuning) {
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   const size_t R = size_t(1) << logR;
-  const int wl = std::min(qfd::kMaxTileLog, logR);
-  Fe* msg = out.cw.p;
-  Fe* par = out.cw.p + R;
-  for (int pass = 0; pass < 2; ++pass) {
-    QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logm) * 16,
-              wht_tile_launch(s_, pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, logm, wl));
-    strided_passes<qfd::kWht>(s_, par, logR, logm, wl, logR);
+  Fe* msg = cw;
+  Fe* par = cw + R;
+  const bool mobius = mob_from < logm;
+  if (logR < qfd::kMaxTileLog) {
+    if (mobius) strided_passes<qfd::kMobius>(s, msg, msg, logR, logm, mob_from, logm, timed, allow_tuning);
+    for (int pass = 0; pass < 2; ++pass)
+      launch(s, timed, "k_wht_tile", (uint64_t(2) << logm) * 16,
+             qf_intops::transform_ops(kOps, uint64_t(1) << logm, logR, 0, 1, pass),
+             [&] { wht_tile_launch(s, pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, logm, logR); });
+    return;
   }
+  constexpr int kT = qfd::kMaxTileLog;
+  check(!mobius || mob_from == kT, "the Mobius tile pass covers bits 0..11");
+  const int top = std::min(logR, kT + 10);  // fused span [kT, top)
+  const int k = top - kT;
+  const bool fused = mobius && k >= 6;
+  if (mobius) strided_passes<qfd::kMobius>(s, msg, msg, logR, logm, fused ? top : kT, logm, timed, allow_tuning);
+  if (fused) {
+    const int cb = strided_cb(k, logm);
+    const uint32_t tiles = uint32_t(uint64_t(1) << (logm - k - cb));
+    launch(s, timed, "k_mobius_wht_strided", (uint64_t(3) << logm) * 16,
+           qf_intops::transform_ops(kOps, uint64_t(1) << logm, k, k, 2, 0), [&] {
+             qfd::k_mobius_wht_strided<<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(cw, uint32_t(R), logR,
+                                                                                                 kT, k, cb, tiles);
+           });
+  } else {
+    strided_passes<qfd::kWht>(s, msg, par, logR, logm, kT, top, timed, allow_tuning);
+  }
+  strided_passes<qfd::kWht>(s, par, par, logR, logm, top, logR, timed, allow_tuning);
+  const uint32_t tiles = uint32_t(uint64_t(1) << (logm - kT));
+  const Fe* src = k > 0 ? par : msg;
+  launch(s, timed, "k_wht_alpha_wht_tile", (uint64_t(2) << logm) * 16 + uint64_t(R) * 16,
+         qf_intops::transform_ops(kOps, uint64_t(1) << logm, 2 * kT, 0, 2, 1), [&] {
+           qfd::k_wht_alpha_wht_tile<<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem + qfd::kAlphaStageSmem, s>>>(
+               src, par, alpha, logR, tiles);
+         });
+  strided_passes<qfd::kWht>(s, par, par, logR, logm, kT, logR, timed, allow_tuning);
+}
+
+// Encode (see encode_passes), then leaf hashes and tree.
+void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain, int mob_from) {
+  const size_t R = size_t(1) << logR;
+  encode_passes(s_, out.cw.p, alpha, logR, logm, mob_from < 0 ? logm : mob_from, true, true);
   // Leaves and inner levels.
   const uint64_t n_ext = 2 * R;
   ::qfd::LeafPrefix lp = leaf_prefix(out.n_cols, ext_domain);
   const unsigned lgrid = unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads);
+  const uint64_t leaf_ops = qf_intops::leaf_hash_ops(n_ext, ext_domain ? 80 : 75, out.n_cols * 16);
   if (ext_domain)
-    QF_LAUNCH(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32,
-              qfd::k_hash_leaves<16><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
+    QF_LAUNCH_OPS(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32, leaf_ops,
+                  qfd::k_hash_leaves<16><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
   else
-    QF_LAUNCH(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32,
-              qfd::k_hash_leaves<11><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
+    QF_LAUNCH_OPS(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32, leaf_ops,
+                  qfd::k_hash_leaves<11><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
   ::qfd::InnerPrefix ip = inner_prefix();
   out.level_off.clear();
   uint64_t off = 0, n = n_ext;
   while (n > 1) {
     out.level_off.push_back(off);
-    QF_LAUNCH(s_, "k_hash_inner", n * 32 + (n / 2) * 32,
-              qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s_>>>(out.tree.p + 2 * off, n / 2, ip,
-                                                                                             out.tree.p + 2 * (off + n)));
+    QF_LAUNCH_OPS(s_, "k_hash_inner", n * 32 + (n / 2) * 32, qf_intops::inner_hash_ops(n / 2),
+                  qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s_>>>(
+                      out.tree.p + 2 * off, n / 2, ip, out.tree.p + 2 * (off + n)));
     off += n;
     n /= 2;
   }
@@ -480,11 +583,11 @@ Digest GpuBackend::encode_block(const W* bva, uint64_t active, uint64_t src_base
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
   check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
-  QF_LAUNCH(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * (F::kLanes * sizeof(W) + 16),
+  QF_LAUNCH_OPS(s_, "k_pack_mobius_tile", (uint64_t(1) << logm) * (F::kLanes * sizeof(W) + 16),
+            qf_intops::transform_ops(kOps, uint64_t(1) << logm, 0, l0, 1, 0),
             qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
                 bva, active, src_base, cw.cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
-  mobius_rest(cw.cw.p, logm, logR, l0);
-  encode_and_hash(cw, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
+  encode_and_hash(cw, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false, l0);
   return cw.root_;
 }
 
@@ -540,11 +643,6 @@ std::vector<Digest> GpuBackend::commit_streamed(const BlockStream::BlockFn& per_
 
 // The same kernels as commit_block + encode_and_hash, launched without the
 // per-launch timers and into caller-owned buffers.
-template <int OP>
-static void strided_passes_plain(cudaStream_t s, Fe* base, int logR, int logm, int from, int to) {
-  strided_passes<OP>(s, base, logR, logm, from, to, false, false);
-}
-
 void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
                        const Fe* alpha, uint8_t* d_root, cudaStream_t s) {
   configure_tile_kernels();
@@ -553,20 +651,13 @@ void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, 
   const int logR = logm - ilog2(cols);
   const size_t R = size_t(1) << logR;
   check(P.pcs.pp->seq.top().message_len == R, "alpha table length");
-  // Message half: pack + Mobius.
+  // Message half: pack + Mobius levels 0..11, then the rest of the encode.
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
   qfd::k_pack_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, qfd::kTileSmem, s>>>(
       d_bva, active, uint64_t(b) * P.block_len, cw, logR, l0, uint32_t(uint64_t(1) << (logm - l0)));
   QF_CK(cudaGetLastError());
-  strided_passes_plain<qfd::kMobius>(s, cw, logR, logm, l0, logm);
-  // Parity half: WHT(alpha * WHT(message)) per column.
-  const int wl = std::min(qfd::kMaxTileLog, logR);
-  for (int pass = 0; pass < 2; ++pass) {
-    wht_tile_launch(s, pass == 0 ? cw : cw + R, cw + R, pass == 0 ? nullptr : alpha, logR, logm, wl);
-    QF_CK(cudaGetLastError());
-    strided_passes_plain<qfd::kWht>(s, cw + R, logR, logm, wl, logR);
-  }
+  encode_passes(s, cw, alpha, logR, logm, l0, false, false);
   // Row leaves, inner levels, root.
   const uint64_t n_ext = 2 * R;
   qfd::k_hash_leaves<11><<<unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads), qfd::kLeafThreads, 0, s>>>(
@@ -641,8 +732,9 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
                                                                            raw.p + kRaw * b));
     });
   }
-  for (size_t b0 = 0; !streaming() && b0 < live; b0 += qfd::kEqBlocks) {
-    const int nb = int(std::min<size_t>(qfd::kEqBlocks, live - b0));
+  const size_t per_launch = KernelOptions::per_matrix ? 1 : size_t(qfd::kEqBlocks);
+  for (size_t b0 = 0; !streaming() && b0 < live; b0 += per_launch) {
+    const int nb = int(std::min<size_t>(per_launch, live - b0));
     QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W) * uint64_t(nb),
               qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva_, active_, P_.block_len, b0, nb, m, weights_.p,
                                                                          raw.p + kRaw * b0));
@@ -678,6 +770,26 @@ const DeviceCodeword& GpuBackend::single_codeword() {
   return *single_cw_;
 }
 
+// values[i] (+)= sum_b sum_j v(b * block_len + 8i + j) T[b * L + j] over the
+// packed length m: the tensor-core kernel for F65521, else the dp4a / IMAD one.
+void GpuBackend::block_fold_launch(const W* bva, uint64_t active, int blocks, const Fe* T, int accumulate) {
+  constexpr int L = F::kLanes;
+  const uint64_t m = P_.pcs.packed_len();
+  const uint64_t bytes = m * (L * sizeof(W) * uint64_t(blocks) + (accumulate ? 32 : 16));
+#if !defined(QF_FIELD_KB)
+  if (imma_on()) {
+    QF_LAUNCH(s_, "k_block_fold_mma", bytes,
+              qfd::k_block_fold_mma<<<mma_grid(), qfd::kMmaThreads, 0, s_>>>(bva, active, P_.block_len, blocks, m, T,
+                                                                              values_.p, accumulate));
+    return;
+  }
+#endif
+  set_smem(qfd::k_block_fold, size_t(blocks) * L * 16);
+  QF_LAUNCH(s_, "k_block_fold", bytes,
+            qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, size_t(blocks) * L * 16, s_>>>(
+                bva, active, P_.block_len, blocks, m, T, values_.p, accumulate));
+}
+
 std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   single_cw_ = nullptr;  // a new opening
   std::vector<std::vector<F>> lanes = project_blocks(outer, 1);
@@ -692,12 +804,10 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   if (streaming()) {
     QF_CK(cudaMemsetAsync(values_.p, 0, m * 16, s_));
     src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
-      if (b == 0)
-        QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 32),
-                  qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(d, n, P_.block_len, 1, m, dT.p, values_.p, 1));
+      if (b == 0) block_fold_launch(d, n, 1, dT.p, 1);
     });
   } else {
-    QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(bva_, active_, P_.block_len, 1, m, dT.p, values_.p, 0));
+    block_fold_launch(bva_, active_, 1, dT.p, 0);
   }
   sum_len_ = m;
   msg_valid_ = false;
@@ -729,23 +839,24 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
     QF_CK(cudaMemsetAsync(values_.p, 0, m * 16, s_));
     src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
       if (b >= size_t(blocks)) return;
-      QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) + 32),
-                qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, L * 16, s_>>>(d, n, P_.block_len, 1, m, dT.p + b * L,
-                                                                                  values_.p, 1));
+      block_fold_launch(d, n, 1, dT.p + b * L, 1);
     });
+  } else if (KernelOptions::per_matrix) {  // one launch per block, accumulated
+    for (int b = 0; b < blocks; ++b) {
+      const uint64_t off = uint64_t(b) * P_.block_len;
+      block_fold_launch(off < active_ ? bva_ + off : bva_, off < active_ ? active_ - off : 0, 1, dT.p + b * L, b > 0);
+    }
   } else {
-    set_smem(qfd::k_block_fold, T.size() * 16);
-    QF_LAUNCH(s_, "k_block_fold", m * (L * sizeof(W) * uint64_t(blocks) + 16), qfd::k_block_fold<<<grid_for(m, kThreads), kThreads, T.size() * 16, s_>>>(bva_, active_, P_.block_len, blocks, m, dT.p,
-                                                                            values_.p, 0));
+    block_fold_launch(bva_, active_, blocks, dT.p, 0);
   }
   folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
   const int l0 = std::min(qfd::kMaxTileLog, logm);
   const size_t smem = qfd::kTileSmem;
   check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
-  QF_LAUNCH(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16, qfd::k_copy_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
+  QF_LAUNCH_OPS(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16,
+                qf_intops::transform_ops(kOps, uint64_t(1) << logm, 0, l0, 1, 0), qfd::k_copy_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
                 values_.p, folded_->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
-  mobius_rest(folded_->cw.p, logm, logR, l0);
-  encode_and_hash(*folded_, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false);
+  encode_and_hash(*folded_, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false, l0);
   sum_len_ = m;
   msg_valid_ = false;
   return folded_->root_;
@@ -1169,11 +1280,27 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
   tb.build(s_, tables);
   DBuf<qfd::TermTiles> dtt(tt.size());
   DBuf<uint32_t> dseg(seg.size());
-  QF_CK(cudaMemcpyAsync(dtt.p, tt.data(), tt.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
   QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 4, cudaMemcpyHostToDevice, s_));
-  QF_LAUNCH(s_, "k_project_terms", proj_bytes,
-            qfd::k_project_terms<<<unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0, s_>>>(
-                bva_, active_, dtt.p, int(tt.size()), uint32_t(tiles), tables.p, int(common_lanes), dtile.p));
+  if (KernelOptions::per_matrix) {
+    // One launch per term (a bucket's claim term, or a padding / suffix
+    // term): each term's tiles renumbered from 0, its outputs at its first tile.
+    std::vector<qfd::TermTiles> solo = tt;
+    for (auto& T : solo) T.first_tile = 0;
+    QF_CK(cudaMemcpyAsync(dtt.p, solo.data(), solo.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
+    for (size_t k = 0; k < tt.size(); ++k) {
+      const uint64_t n = term_tile_count(tt[k]);
+      QF_LAUNCH(s_, "k_project_terms", tt[k].rows * common_lanes * sizeof(W) + n * 16,
+                qfd::k_project_terms<<<unsigned((n + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0, s_>>>(
+                    bva_, active_, dtt.p + k, 1, uint32_t(n), tables.p, int(common_lanes),
+                    dtile.p + size_t(tt[k].first_tile) * common_lanes));
+    }
+  } else {
+    QF_CK(cudaMemcpyAsync(dtt.p, tt.data(), tt.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
+    QF_LAUNCH(s_, "k_project_terms", proj_bytes,
+              qfd::k_project_terms<<<unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0,
+                                     s_>>>(bva_, active_, dtt.p, int(tt.size()), uint32_t(tiles), tables.p,
+                                           int(common_lanes), dtile.p));
+  }
   QF_LAUNCH(s_, "k_sum_segments", tiles * common_lanes * 16, qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p));
   std::vector<F> h(terms.size() * common_lanes);
   QF_CK(cudaMemcpyAsync(h.data(), dterm.p, h.size() * 16, cudaMemcpyDeviceToHost, s_));
@@ -1228,6 +1355,22 @@ void GpuBackend::cross_terms(const Query<F>& q, size_t stride, std::vector<F>& p
   }
 }
 
+// Packed EO witness rows [0, rows) of the weights at `bva` (`active`
+// entries): the tensor-core kernel for F65521 at stride 16, else dp4a / IMAD.
+void GpuBackend::eo_witness_launch(const W* bva, uint64_t active, uint64_t rows, size_t stride, const Fe* powers,
+                                   Fe* out) {
+  const uint64_t bytes = std::min<uint64_t>(active, rows * stride) * sizeof(W) + rows * 16;
+#if !defined(QF_FIELD_KB)
+  if (imma_on() && stride == 16) {
+    QF_LAUNCH(s_, "k_eo_witness_mma", bytes,
+              qfd::k_eo_witness_mma<<<mma_grid(), qfd::kMmaThreads, 0, s_>>>(bva, active, rows, powers, out));
+    return;
+  }
+#endif
+  QF_LAUNCH(s_, "k_eo_witness", bytes,
+            qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva, active, rows, int(stride), powers, out));
+}
+
 F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t stride) {
   HostScope hs("eo_build");
   const uint64_t rows = logical / stride;
@@ -1246,11 +1389,27 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
       const uint64_t r0 = uint64_t(b) * rpb;
       if (r0 >= rows) return;
       const uint64_t rb = std::min(rpb, rows - r0);
-      QF_LAUNCH(s_, "k_eo_witness", n * sizeof(W) + rb * 16,
-                qfd::k_eo_witness<<<grid_for(rb, kThreads), kThreads, 0, s_>>>(d, n, rb, int(stride), dp.p, wit_.p + r0));
+      eo_witness_launch(d, n, rb, stride, dp.p, wit_.p + r0);
     });
+  } else if (KernelOptions::per_matrix) {
+    // One launch per bucket: the rows [offset / stride, end / stride) of
+    // each bucket, a run of small buckets sharing a row joined to the next.
+    uint64_t r0 = 0;
+    for (size_t k = 0; k < P_.layout.buckets.size() && r0 < rows; ++k) {
+      const auto& bk = P_.layout.buckets[k];
+      const uint64_t end = k + 1 < P_.layout.buckets.size() ? (bk.offset + bk.len()) / stride : rows;
+      if (end <= r0) continue;
+      const uint64_t r1 = std::min(end, rows);
+      const uint64_t g0 = r0 * stride;
+      eo_witness_launch(bva_ + std::min<uint64_t>(g0, active_), active_ > g0 ? active_ - g0 : 0, r1 - r0, stride, dp.p,
+                        wit_.p + r0);
+      r0 = r1;
+    }
+    if (r0 < rows)
+      eo_witness_launch(bva_ + std::min<uint64_t>(r0 * stride, active_), active_ > r0 * stride ? active_ - r0 * stride : 0,
+                        rows - r0, stride, dp.p, wit_.p + r0);
   } else {
-    QF_LAUNCH(s_, "k_eo_witness", std::min<uint64_t>(active_, rows * stride) * sizeof(W) + rows * 16, qfd::k_eo_witness<<<grid_for(rows, kThreads), kThreads, 0, s_>>>(bva_, active_, rows, int(stride), dp.p, wit_.p));
+    eo_witness_launch(bva_, active_, rows, stride, dp.p, wit_.p);
   }
   // Query fold (tbv.rs:393-428): zero, then two disjoint passes of large-term
   // tiles, then the merged small-term contributions.
@@ -1294,6 +1453,18 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
     auto& tl = pass_terms[pass];
     if (tl.empty()) continue;
     dtt[pass].alloc(tl.size());
+    if (KernelOptions::per_matrix) {  // one launch per term, tiles renumbered from 0
+      std::vector<qfd::TermTiles> solo = tl;
+      for (auto& T : solo) T.first_tile = 0;
+      QF_CK(cudaMemcpyAsync(dtt[pass].p, solo.data(), solo.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
+      for (size_t k = 0; k < tl.size(); ++k) {
+        const uint64_t n = term_tile_count(tl[k]);
+        QF_LAUNCH(s_, "k_query_terms", tl[k].rows * 32,
+                  qfd::k_query_terms<<<unsigned((n + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), kThreads, 0, s_>>>(
+                      dtt[pass].p + k, 1, uint32_t(n), tables.p, qv_.p));
+      }
+      continue;
+    }
     QF_CK(cudaMemcpyAsync(dtt[pass].p, tl.data(), tl.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
     QF_LAUNCH(s_, "k_query_terms", query_bytes[pass],
               qfd::k_query_terms<<<unsigned((pass_tiles[pass] + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), kThreads, 0, s_>>>(
@@ -1378,7 +1549,7 @@ void GpuBackend::tensor_table(const std::vector<F>& point, DBuf<Fe>& out) { devi
 void GpuBackend::wht_dev(Fe* v, int logn, const Fe* alpha) {
   const int wl = std::min(qfd::kMaxTileLog, logn);
   QF_LAUNCH(s_, "k_wht_tile", (uint64_t(2) << logn) * 16, wht_tile_launch(s_, v, v, alpha, logn, logn, wl));
-  strided_passes<qfd::kWht>(s_, v, logn, logn, wl, logn);
+  strided_passes<qfd::kWht>(s_, v, v, logn, logn, wl, logn);
 }
 
 F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {

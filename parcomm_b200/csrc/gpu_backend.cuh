@@ -200,8 +200,10 @@ class GpuBackend : public Backend<F>,
 
  private:
   // Encode the message halves of `out` with alpha (parity = WHT(alpha * WHT(msg)))
-  // and build its row tree with the base- or extension-row leaf domain.
-  void encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain);
+  // and build its row tree with the base- or extension-row leaf domain.  When
+  // mob_from >= 0 the message holds the packed message with only its Mobius
+  // levels [0, mob_from) applied, and the encode finishes the transform.
+  void encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain, int mob_from = -1);
   std::vector<F> open_top(const DeviceCodeword& cw, const std::vector<F>& point, size_t col_log);
   void tensor_table(const std::vector<F>& point, DBuf<Fe>& out);
   void wht_dev(Fe* v, int logn, const Fe* alpha);
@@ -223,8 +225,9 @@ class GpuBackend : public Backend<F>,
   const DeviceCodeword& single_codeword();
   std::vector<std::vector<std::vector<F>>> project_groups_streamed(const std::vector<std::vector<const Term<F>*>>& groups,
                                                                    size_t stride);
-  void mobius_rest(Fe* cw, int logm, int logR, int from);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
+  void block_fold_launch(const W* bva, uint64_t active, int blocks, const Fe* T, int accumulate);
+  void eo_witness_launch(const W* bva, uint64_t active, uint64_t rows, size_t stride, const Fe* powers, Fe* out);
 
   const Parameters<F>& P_;
   const W* bva_;              // resident weights, or null

@@ -122,12 +122,15 @@ size_t DevicePool::cached_bytes() {
   return n;
 }
 
+std::atomic<int> KernelOptions::imma{1};
+std::atomic<int> KernelOptions::per_matrix{0};
+
 bool KernelClock::enabled = false;
 std::mutex KernelClock::mu;
 std::vector<KernelClock::Rec> KernelClock::recs;
 std::atomic<uint64_t> KernelClock::launches{0};
 
-KernelClock::Scope::Scope(cudaStream_t s, const char* n, uint64_t b_) : stream(s), name(n), bytes(b_) {
+KernelClock::Scope::Scope(cudaStream_t s, const char* n, uint64_t b_, uint64_t o_) : stream(s), name(n), bytes(b_), ops(o_) {
   if (enabled) {
     QF_CK(cudaEventCreate(&a));
     QF_CK(cudaEventCreate(&b));
@@ -139,7 +142,7 @@ void KernelClock::Scope::done() {
   if (enabled) {
     QF_CK(cudaEventRecord(b, stream));
     std::lock_guard<std::mutex> g(mu);
-    recs.push_back({name, a, b, bytes});
+    recs.push_back({name, a, b, bytes, ops});
   }
 }
 void KernelClock::reset(bool on) {
@@ -161,7 +164,7 @@ void KernelClock::note(const std::string& key, const std::string& json_value) {
 std::string KernelClock::stats_json() {
   QF_CK(cudaDeviceSynchronize());
   std::lock_guard<std::mutex> g(mu);
-  struct Agg { uint64_t n = 0, bytes = 0; double ms = 0; };
+  struct Agg { uint64_t n = 0, bytes = 0, ops = 0; double ms = 0; };
   std::map<std::string, Agg> agg;
   for (auto& r : recs) {
     float ms = 0;
@@ -170,6 +173,7 @@ std::string KernelClock::stats_json() {
     e.n += 1;
     e.ms += ms;
     e.bytes += r.bytes;
+    e.ops += r.ops;
   }
   std::string s = "{";
   bool first = true;
@@ -177,8 +181,8 @@ std::string KernelClock::stats_json() {
     if (!first) s += ",";
     first = false;
     char buf[256];
-    std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu}", k.c_str(),
-                  (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes);
+    std::snprintf(buf, sizeof buf, "\"%s\":{\"launches\":%llu,\"ms\":%.6f,\"bytes\":%llu,\"ops\":%llu}", k.c_str(),
+                  (unsigned long long)v.n, v.ms, (unsigned long long)v.bytes, (unsigned long long)v.ops);
     s += buf;
   }
   // Idle time between consecutive recorded launches (in launch order), with

@@ -28,16 +28,27 @@ using namespace qf;
       ::qf::fail(QF_E_CUDA, std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #x); \
   } while (0)
 
+// Process-wide kernel choices, for comparisons that must write the same
+// bytes: `imma` runs the F65521 weight passes on the tensor cores (exact
+// integer limbs) instead of the dp4a / IMAD kernels; `per_matrix` issues the
+// weight passes one launch per term, bucket or block instead of one launch
+// over all of them.  Set through qf_kernel_option.
+struct KernelOptions {
+  static std::atomic<int> imma;
+  static std::atomic<int> per_matrix;
+};
+
 // Per-kernel device time: when enabled, every launch is bracketed by CUDA
 // events recorded on the launching stream; totals are read after a sync.
 struct KernelClock {
-  struct Rec { const char* name; cudaEvent_t a, b; uint64_t bytes; };
+  struct Rec { const char* name; cudaEvent_t a, b; uint64_t bytes, ops; };
   struct Scope {
     cudaStream_t stream;
     const char* name;
     uint64_t bytes;  // algorithmic bytes moved by this launch
+    uint64_t ops;    // algorithmic integer operations (thread level) of this launch, 0 if not counted
     cudaEvent_t a = nullptr, b = nullptr;
-    Scope(cudaStream_t s, const char* n, uint64_t bytes);
+    Scope(cudaStream_t s, const char* n, uint64_t bytes, uint64_t ops = 0);
     void done();
   };
   static bool enabled;
@@ -59,6 +70,14 @@ using HostScope = ::qf::Section;
     __VA_ARGS__;                                \
     QF_CK(cudaGetLastError());                  \
     qf_scope_.done();                           \
+  } while (0)
+// The same, with the launch's algorithmic integer operations (intops.h).
+#define QF_LAUNCH_OPS(stream, name, bytes, ops, ...)     \
+  do {                                                   \
+    ::qfg::KernelClock::Scope qf_scope_(stream, name, bytes, ops); \
+    __VA_ARGS__;                                         \
+    QF_CK(cudaGetLastError());                           \
+    qf_scope_.done();                                    \
   } while (0)
 
 // Process-wide cache of device allocations: released buffers are kept, keyed

@@ -333,25 +333,186 @@ __global__ void __launch_bounds__(ALPHA ? kAlphaTileThreads : kTileThreads, 1)
   tile_loop<kWht, uint4>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
-// Levels [lo, lo + k) over the logical index space, on the half starting at
-// `base` (cw for the message, cw + R for the parity).  Tile `tile` owns 2^cb
-// consecutive group bases g0 = tile << cb (64-byte runs in HBM at cb = 2,
-// longer above): tile element t = (j << cb) + c is logical index
-// base(g0 + c) + (j << lo), so the levels act on tile bits [cb, cb + k).
+// Codeword address of element t of tile `tile` of a strided pass: the tile
+// owns 2^cb consecutive group bases g0 = tile << cb (64-byte runs in HBM at
+// cb = 2, longer above), and tile element t = (j << cb) + c is logical index
+// base(g0 + c) + (j << lo), so the pass's k levels act on tile bits [cb, cb + k).
+__device__ __forceinline__ uint32_t strided_addr(uint32_t tile, int t, int logR, int lo, int k, int cb) {
+  const uint32_t g = (tile << cb) + uint32_t(t & ((1 << cb) - 1));
+  return msg_addr32((((g >> lo) << (lo + k)) | (g & ((1u << lo) - 1u))) + (uint32_t(t >> cb) << lo), logR);
+}
+
+// Levels [lo, lo + k) over the logical index space of a half: read at `src`
+// (cw for the message, cw + R for the parity), written at `dst` (src itself
+// for an in-place pass, or the parity half when the first pass of a span
+// turns the message into the parity).
 template <int OP>
-__global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(Fe* __restrict__ base, int logR, int lo, int k, int cb,
-                                                                      uint32_t n_tiles) {
+__global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(const Fe* src, Fe* dst, int logR, int lo, int k,
+                                                                      int cb, uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  const uint32_t low_mask = (1u << lo) - 1u;
-  const int cmask = (1 << cb) - 1;
-  auto addr = [=](uint32_t tile, int t) {
-    const uint32_t g = (tile << cb) + uint32_t(t & cmask);
-    return msg_addr32((((g >> lo) << (lo + k)) | (g & low_mask)) + (uint32_t(t >> cb) << lo), logR);
+  auto fetch = [=](uint32_t tile, int t) {
+    return *reinterpret_cast<const uint4*>(src + strided_addr(tile, t, logR, lo, k, cb));
   };
-  auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(base + addr(tile, t)); };
   auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
-  auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(base + addr(tile, t)) = u; };
+  auto st = [=](uint32_t tile, int t, uint4 u) {
+    *reinterpret_cast<uint4*>(dst + strided_addr(tile, t, logR, lo, k, cb)) = u;
+  };
   tile_loop<OP, uint4>(planes_s, cb + k, cb, n_tiles, fetch, conv, st);
+}
+
+// ---------------------------------------------------------------- fused passes
+// Two transforms on the same tile bits, with a step on the canonical values
+// in between, in one trip through HBM.  The transforms are tensor products of
+// 2 x 2 maps on the index bits, so the levels of either one can run in any
+// order and levels on different bits commute: a pass may take the message's
+// Mobius levels on bits [lo, lo + k) and then the first WHT's levels on the
+// same bits, or the first WHT's last levels, the alpha product and the second
+// WHT's first levels.
+
+// Registers -> planes: v[j] is tile element base + (j << zb).
+template <int R>
+__device__ __forceinline__ void regs_to_planes(uint32_t* planes, int base, int zb, const uint32_t (&v)[1 << R][kC]) {
+  const int pb = pidx(base);
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) {
+    const int q = pb ^ pidx(j << zb);
+#pragma unroll
+    for (int c = 0; c < kC; ++c) planes[c * kPlane + q] = v[j][c];
+  }
+}
+
+// Planar levels on tile bits [b0, 6) of a full tile (the levels between a
+// register head on bits 9..11 and a register tail on bits 6..8), lvl0 the
+// first level's lazy index.  A radix-4 stage on bits 4..5 takes its groups
+// with bits 4 and 5 swapped (conflict-free banks, see tile_loop).
+template <int OP>
+__device__ __forceinline__ void fused_middle(uint32_t* planes, int b0, int lvl0) {
+  if (b0 == 4) planar_stage<OP, 2, true>(planes, kMaxTileLog, 4, lvl0);
+  else planar_levels<OP>(planes, kMaxTileLog, b0, 6 - b0, lvl0);
+}
+
+// Runs OP1 on tile bits [b0, 12) of full 4096-element tiles, then for each
+// element mid(tile, t, Fr& v) on its canonical value, then OP2 on the same
+// bits, then st(tile, t, uint4).  512 threads, 6 >= b0 >= 0.  OP1: register
+// head on bits 9..11, planar levels on [b0, 6), register tail on bits 6..8;
+// mid on the tail's registers; OP2: register levels on bits 6..8 right
+// there, planar levels on [b0, 6), register tail on bits 9..11 and the
+// stores (consecutive threads take consecutive elements, as the loads).
+// stage(tile) runs first in each tile (to issue its cp.async side loads,
+// which each thread then waits for before the first planar stage's barrier).
+// The next tile's loads are issued after mid, so their registers are not live
+// across it.
+template <int OP1, int OP2, class Raw, class Fetch, class Conv, class Stage, class Mid, class St>
+__device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32_t n_tiles, Fetch fetch, Conv conv,
+                                                Stage stage, Mid mid, St st) {
+  const int g = threadIdx.x;
+  const int rm = 6 - b0;
+  const int tb = (g & 63) | ((g >> 6) << 9);  // the tail group: elements tb + (j << 6)
+  Raw raw[8];
+  uint32_t tile = blockIdx.x;
+  if (tile < n_tiles)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+  for (; tile < n_tiles; tile += gridDim.x) {
+    stage(tile);
+    {
+      uint32_t v[8][kC];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const Fr e = conv(tile, g + (j << 9), raw[j]);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
+      }
+      head_levels<OP1>(planes, v);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (rm > 0) fused_middle<OP1>(planes, b0, 3);
+    else __syncthreads();
+    {
+      uint32_t v[8][kC];
+      const int pb = pidx(tb);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int q = pb ^ pidx(j << 6);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = planes[c * kPlane + q];
+      }
+      reg_levels<OP1, 3>(v, 3 + rm);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        Fr w;
+#pragma unroll
+        for (int c = 0; c < kC; ++c) w.c[c] = tile_final(v[j][c]);
+        mid(tile, tb + (j << 6), w);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = w.c[c];
+      }
+      reg_levels<OP2, 3>(v, 0);
+      // The same thread read these positions: no other thread touches them
+      // until the barrier below.
+      regs_to_planes<3>(planes, tb, 6, v);
+    }
+    const uint32_t next = tile + gridDim.x;
+    if (next < n_tiles)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
+    __syncthreads();
+    if (rm > 0) fused_middle<OP2>(planes, b0, 3);
+    auto st_t = [&](int t, uint4 u) { st(tile, t, u); };
+    pass_tail<OP2, 3>(planes, 9, 3 + rm, st_t);
+    __syncthreads();  // the next head overwrites the planes
+  }
+}
+
+// Message half at cw: Mobius levels [lo, lo + k) (the message is final after
+// them), stored back; then the first WHT's levels [lo, lo + k) of the same
+// values, stored into the parity half at cw + R.  k in [6, 10], cb = 12 - k
+// (or 2 at k = 10).
+__global__ void __launch_bounds__(kTileThreads, 1) k_mobius_wht_strided(Fe* cw, uint32_t R, int logR, int lo, int k, int cb,
+                                                                       uint32_t n_tiles) {
+  extern __shared__ uint32_t planes_s[];
+  auto fetch = [=](uint32_t tile, int t) {
+    return *reinterpret_cast<const uint4*>(cw + strided_addr(tile, t, logR, lo, k, cb));
+  };
+  auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
+  auto stage = [](uint32_t) {};
+  auto mid = [=](uint32_t tile, int t, Fr& v) {
+    *reinterpret_cast<uint4*>(cw + strided_addr(tile, t, logR, lo, k, cb)) = pack_fe(v);
+  };
+  auto st = [=](uint32_t tile, int t, uint4 u) {
+    *reinterpret_cast<uint4*>(cw + R + strided_addr(tile, t, logR, lo, k, cb)) = u;
+  };
+  tile_loop_fused<kMobius, kWht, uint4>(planes_s, cb, n_tiles, fetch, conv, stage, mid, st);
+}
+
+// The parity tile pass: the first WHT's levels 0..11 of each column (read at
+// src, the message half when no strided WHT level came first, else the
+// parity half), times alpha[r], the second WHT's levels 0..11, written to the
+// parity half at dst.  Each tile's 4096 alphas are staged in shared memory
+// (cp.async) while the first WHT runs.
+constexpr size_t kAlphaStageSmem = size_t(1) << kMaxTileLog << 4;  // 64 KiB
+__global__ void __launch_bounds__(kTileThreads, 1) k_wht_alpha_wht_tile(const Fe* src, Fe* dst, const Fe* __restrict__ alpha,
+                                                                       int logR, uint32_t n_tiles) {
+  extern __shared__ uint32_t planes_s[];
+  uint4* alpha_s = reinterpret_cast<uint4*>(planes_s + kC * kPlane);
+  const uint32_t rmask = (1u << logR) - 1u;
+  auto addr = [=](uint32_t tile, int t) { return msg_addr32((tile << kMaxTileLog) + uint32_t(t), logR); };
+  auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + addr(tile, t)); };
+  auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
+  auto stage = [=](uint32_t tile) {
+    // Tile rows r0 .. r0 + 4095 (R is a multiple of 4096).
+    const Fe* a = alpha + ((tile << kMaxTileLog) & rmask);
+#pragma unroll
+    for (int i = 0; i < (1 << kMaxTileLog) / kTileThreads; ++i) {
+      const int e = int(threadIdx.x) + i * kTileThreads;
+      const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(alpha_s + e));
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(a + e) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  auto mid = [=](uint32_t, int t, Fr& v) { v = mul(v, unpack_fe(alpha_s[t])); };
+  auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(dst + addr(tile, t)) = u; };
+  tile_loop_fused<kWht, kWht, uint4>(planes_s, 0, n_tiles, fetch, conv, stage, mid, st);
 }
 
 // ---------------------------------------------------------------- hashing
