@@ -19,8 +19,11 @@ setup and claim generation are outside it.  The claims are computed once
   value  : weights/s with the BVA already in HBM (Parameters.commit(on_device)).
   e2e    : weights/s through the same public API from a pinned host BVA
            (host->device copy of the weights and proof bytes back per step).
-  per_matrix : the plain per-matrix path for comparison: the same 226 shapes,
-           each committed and proven as its own single-matrix statement.
+  per_matrix : the same statement and proof bytes with the weight passes
+           launched one term / bucket / PCS block at a time (the per-matrix
+           launch sequence) instead of once over all of them.
+  separate_statements : the same 226 shapes, each committed and proven as
+           its own single-matrix statement (its own proof).
   range_audit : the LogUp range audit of the same weights (Committed.range_audit),
            a check beside the proof, timed once outside the step.
   recompute : the same step in the reference's measured mode (--cache-mode
@@ -502,6 +505,8 @@ def main():
     ap.add_argument("--no-per-matrix", action="store_true",
                     help="skip the per-matrix comparison (each matrix proven on its own)")
     ap.add_argument("--no-audit", action="store_true", help="skip the LogUp range audit measurement")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the same-bytes comparisons (dp4a kernels, per-matrix launch sequence)")
     ap.add_argument("--no-recompute", action="store_true",
                     help="skip the recompute-mode measurement (the reference's --cache-mode recompute)")
     ap.add_argument("--out", default=str(ROOT / "bench_out"), help="directory for the clock samples and kernel stats")
@@ -702,6 +707,45 @@ def main():
                 "frac": h2d_achieved / h2d_peak, "bytes_per_step": h2d_dev,
                 "peak_source": "pinned 2 GiB host->device copy, best of 3, measured in this run"}
 
+    # The tensor-core weight passes against the dp4a / IMAD kernels they
+    # replace (F65521): one more profiled step with them switched off, same bytes.
+    imma_cmp = None
+    if not sixteen and not args.no_compare:
+        qf.kernel_option("imma", 0)
+        qf.kernel_timing(True)
+        pr_off, _, _ = step(True)
+        torch.cuda.synchronize()
+        off = qf.kernel_stats()
+        qf.kernel_timing(False)
+        qf.kernel_option("imma", 1)
+        assert pr_off.to_bytes() == proof.to_bytes(), "dp4a-path proof bytes differ"
+        pairs = {"eo_witness": ("k_eo_witness_mma", "k_eo_witness"), "block_fold": ("k_block_fold_mma", "k_block_fold")}
+        imma_cmp = {}
+        for name, (on_k, off_k) in pairs.items():
+            a, b = stats.get(on_k), off.get(off_k)
+            if a and b:
+                imma_cmp[name] = {"imma_ms": a["ms"], "dp4a_ms": b["ms"], "speedup": b["ms"] / a["ms"],
+                                  "imma_hbm_frac": a["bytes"] / (a["ms"] / 1000.0) / 1e9 / peak,
+                                  "dp4a_hbm_frac": b["bytes"] / (b["ms"] / 1000.0) / 1e9 / peak}
+        imma_cmp["what"] = ("per-step kernel time of the exact integer-limb tensor-core kernels (mma.sync s8 x u8 -> "
+                            "s32) against the dp4a / IMAD kernels, same proof bytes")
+
+    # The same statement with the weight passes issued one launch per term,
+    # bucket or block (the per-matrix launch sequence) instead of one launch
+    # over all of them: same bytes, timed the same way.
+    per_matrix_launches = None
+    if not args.no_compare and not streamed:
+        qf.kernel_option("per_matrix", 1)
+        step(True)
+        ms_pm, (pr_pm, _, _), launches_pm = timed(True, args.steps)
+        qf.kernel_option("per_matrix", 0)
+        assert pr_pm.to_bytes() == proof.to_bytes(), "per-matrix launch sequence proof bytes differ"
+        per_matrix_launches = {"value": job_throughput(weights, world, ms_pm), "unit": "weights/s", "ms_per_step": ms_pm,
+                               "gpu_launches": launches_pm // max(args.steps, 1),
+                               "batched_over_per_matrix": ms_pm / ms_dev,
+                               "what": "the same proof (identical bytes) with the weight passes launched per term, "
+                                       "bucket or PCS block instead of once over all of them"}
+
     # LogUp range audit of the same weights (beside the proof, outside the
     # timed region): one warm-up call, then one timed call.
     range_audit = None
@@ -793,8 +837,10 @@ def main():
         "step_roofline": step_roofline,
         "link_roofline": link,
         "cpu_baseline": cpu_baseline,
-        "per_matrix": per_matrix,
+        "per_matrix": per_matrix_launches,
+        "separate_statements": per_matrix,
         "recompute": recompute,
+        "imma_vs_dp4a": imma_cmp,
         "range_audit": range_audit,
         "clocks": clocks.summary(local),
         "proof_bytes": proof_bytes,
