@@ -719,7 +719,8 @@ def main():
         qf.kernel_timing(False)
         qf.kernel_option("imma", 1)
         assert pr_off.to_bytes() == proof.to_bytes(), "dp4a-path proof bytes differ"
-        pairs = {"eo_witness": ("k_eo_witness_mma", "k_eo_witness"), "block_fold": ("k_block_fold_mma", "k_block_fold")}
+        pairs = {"eo_witness": ("k_eo_witness_mma", "k_eo_witness"), "block_fold": ("k_block_fold_mma", "k_block_fold"),
+                 "eq_projection": ("k_eq_project_mma", "k_eq_project_blocks")}
         imma_cmp = {}
         for name, (on_k, off_k) in pairs.items():
             a, b = stats.get(on_k), off.get(off_k)

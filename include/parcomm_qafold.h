@@ -166,8 +166,9 @@ uint64_t qf_kernel_launches(void);
 int qf_kernel_int_peaks(double out[4]);
 /* Diagnostics, no reference counterpart: process-wide kernel choices that
  * write identical bytes, for comparisons.  "imma" (default 1): the F65521
- * weight passes (EO witness, block fold) contract on the tensor cores with
- * exact integer limbs; 0 selects the dp4a / IMAD kernels.  "per_matrix"
+ * weight passes (EO witness, block fold, equality-table lane sums) contract
+ * on the tensor cores with exact integer limbs; 0 selects the dp4a / IMAD
+ * kernels.  "per_matrix"
  * (default 0): 1 issues the weight passes one launch per term, bucket or
  * block instead of one launch over all of them.  Set it between calls, not
  * while another call runs. */

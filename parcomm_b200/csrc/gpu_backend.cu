@@ -713,6 +713,25 @@ static void device_point_table(cudaStream_t s, const std::vector<F>& point, W we
 static std::vector<F> eq_slice(const std::vector<F>& p) { return equality_table(p); }
 static std::vector<F> tensor_slice(const std::vector<F>& p) { return tensor_weights(p); }
 
+// Raw lane sums of blocks [b0, b0 + nb) (nb <= 8) against the equality table
+// in weights_: the tensor-core kernel for F65521, else the IMAD one.
+void GpuBackend::eq_project_launch(const W* bva, uint64_t active, uint64_t b0, int nb, unsigned long long* raw,
+                                   unsigned grid) {
+  constexpr int L = F::kLanes;
+  const uint64_t m = P_.pcs.packed_len();
+  const uint64_t bytes = m * 16 + m * L * sizeof(W) * uint64_t(nb);
+#if !defined(QF_FIELD_KB)
+  if (imma_on()) {
+    QF_LAUNCH(s_, "k_eq_project_mma", bytes,
+              qfd::k_eq_project_mma<<<mma_grid(), qfd::kMmaThreads, 0, s_>>>(bva, active, P_.block_len, b0, nb, m,
+                                                                              weights_.p, raw));
+    return;
+  }
+#endif
+  QF_LAUNCH(s_, "k_eq_project_blocks", bytes,
+            qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva, active, P_.block_len, b0, nb, m, weights_.p, raw));
+}
+
 std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& outer, size_t nblocks) {
   const uint64_t m = P_.pcs.packed_len();
   if (outer.size() != size_t(ilog2(m))) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "outer point");
@@ -727,17 +746,13 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
   if (streaming()) {  // one block per launch, as each lands in HBM
     src_->for_each(s_, [&](size_t b, const W* d, uint64_t n) {
       if (b >= nblocks) return;
-      QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W),
-                qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(d, n, P_.block_len, 0, 1, m, weights_.p,
-                                                                           raw.p + kRaw * b));
+      eq_project_launch(d, n, 0, 1, raw.p + kRaw * b, grid);
     });
   }
   const size_t per_launch = KernelOptions::per_matrix ? 1 : size_t(qfd::kEqBlocks);
   for (size_t b0 = 0; !streaming() && b0 < live; b0 += per_launch) {
     const int nb = int(std::min<size_t>(per_launch, live - b0));
-    QF_LAUNCH(s_, "k_eq_project_blocks", m * 16 + m * L * sizeof(W) * uint64_t(nb),
-              qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva_, active_, P_.block_len, b0, nb, m, weights_.p,
-                                                                         raw.p + kRaw * b0));
+    eq_project_launch(bva_, active_, b0, nb, raw.p + kRaw * b0, grid);
   }
   std::vector<unsigned long long> h(kRaw * nblocks);
   QF_CK(cudaMemcpyAsync(h.data(), raw.p, h.size() * 8, cudaMemcpyDeviceToHost, s_));

@@ -227,6 +227,7 @@ class GpuBackend : public Backend<F>,
                                                                    size_t stride);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
   void block_fold_launch(const W* bva, uint64_t active, int blocks, const Fe* T, int accumulate);
+  void eq_project_launch(const W* bva, uint64_t active, uint64_t b0, int nb, unsigned long long* raw, unsigned grid);
   void eo_witness_launch(const W* bva, uint64_t active, uint64_t rows, size_t stride, const Fe* powers, Fe* out);
 
   const Parameters<F>& P_;

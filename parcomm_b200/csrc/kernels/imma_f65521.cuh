@@ -1,6 +1,7 @@
-// Exact integer-limb tensor-core forms of two F65521^8 weight passes: the
-// packed EO witness (eo.rs:119-132) and the block fold (packed_batch.rs:
-// 213-236).  Both contract signed 8-bit weights against tables of extension
+// Exact integer-limb tensor-core forms of three F65521^8 weight passes: the
+// packed EO witness (eo.rs:119-132), the block fold (packed_batch.rs:
+// 213-236) and the batch opening's equality-table lane sums (packed_batch.rs:
+// 25-41).  Each contracts signed 8-bit weights against a table of extension
 // elements.  Each table coefficient (canonical, < 2^16) splits into its two
 // bytes, which are exactly the 16 bytes of the element's storage (byte 2k =
 // low byte of coefficient k, byte 2k + 1 = its high byte).  One
@@ -184,6 +185,104 @@ __global__ void __launch_bounds__(kMmaThreads) k_block_fold_mma(const int8_t* __
     }
     mma_store_rows(out_s[warp], acc, row0, m, values, accumulate != 0);
   }
+}
+
+// Batch-opening lane sums of up to 8 blocks against the equality weights
+// (project_lanes_from_fn, packed_batch.rs:25-41):
+//   raw[b][j * 8 + k] += sum_i v(b, 8 i + j) * weights[i].c[k].
+// The contraction runs over the element index i, which is the outer index
+// of both the weights (8 lanes j per element) and the table (16 limbs per
+// element), so each fragment register is gathered: four 32-bit loads (the
+// word holding byte j, or limb l, of four consecutive elements) and three
+// byte permutes.  Rows of the A tile are (block pair member, lane j): row g
+// is lane g of the pair's first block, row g + 8 lane g of the second.  Per
+// k32 step the limb sums are below 32 * 128 * 255 < 2^20; s32 accumulators
+// run 256 steps before they move into 64-bit totals.
+constexpr int kEqMmaSteps = 256;  // k32 steps between flushes into 64-bit totals
+__device__ __forceinline__ uint32_t gather_bytes(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3, int b) {
+  const uint32_t sel = uint32_t(b) | (uint32_t(4 + b) << 4);
+  return __byte_perm(__byte_perm(x0, x1, sel), __byte_perm(x2, x3, sel), 0x5410);
+}
+__global__ void __launch_bounds__(kMmaThreads) k_eq_project_mma(const int8_t* __restrict__ bva, uint64_t active,
+                                                                uint64_t block_len, uint64_t first_block, int nb, uint64_t m,
+                                                                const Fe* __restrict__ weights,
+                                                                unsigned long long* __restrict__ raw) {
+  __shared__ long long tot_s[8][64];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+  for (int i = threadIdx.x; i < 8 * 64; i += kMmaThreads) tot_s[i >> 6][i & 63] = 0;
+  __syncthreads();
+  const int pairs = (nb + 1) / 2;
+  int32_t acc[4][2][4];
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[p][nt][c] = 0;
+  const uint64_t steps = (m + 31) / 32;
+  const uint64_t wid = uint64_t(blockIdx.x) * kMmaWarps + warp, nw = uint64_t(gridDim.x) * kMmaWarps;
+  // Moves the s32 sums into the CTA's 64-bit totals: lane (g, t) holds, for
+  // block 2p + h, lane j = g, coefficient nt * 4 + t.
+  auto flush = [&]() {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+          const int64_t v = int64_t(acc[p][nt][2 * h]) + 256 * int64_t(acc[p][nt][2 * h + 1]);
+          acc[p][nt][2 * h] = acc[p][nt][2 * h + 1] = 0;
+          if (2 * p + h < nb)
+            atomicAdd(reinterpret_cast<unsigned long long*>(&tot_s[2 * p + h][g * 8 + nt * 4 + t]),
+                      (unsigned long long)v);
+        }
+  };
+  int since = 0;
+  for (uint64_t st = wid; st < steps; st += nw) {
+    const uint64_t i0 = st * 32;
+    // B: limb nt * 8 + g of elements i0 + 16 r + 4 t + e (word 2 nt + g / 4).
+    uint32_t bf[2][2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) {
+        uint32_t x[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const uint64_t i = i0 + 16 * r + 4 * t + e;
+          x[e] = i < m ? reinterpret_cast<const uint32_t*>(weights + i)[2 * nt + (g >> 2)] : 0u;
+        }
+        bf[nt][r] = gather_bytes(x[0], x[1], x[2], x[3], g & 3);
+      }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      if (p >= pairs) break;
+      uint32_t a[4];
+#pragma unroll
+      for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {  // A register 2 r + h: row half h (block 2p + h), K half r
+          const int b = 2 * p + h;
+          uint32_t x[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const uint64_t i = i0 + 16 * r + 4 * t + e;
+            x[e] = (b < nb && i < m) ? weight_word(bva, active, (first_block + b) * block_len + 8 * i + 4 * (g >> 2)) : 0u;
+          }
+          a[2 * r + h] = gather_bytes(x[0], x[1], x[2], x[3], g & 3);
+        }
+#pragma unroll
+      for (int nt = 0; nt < 2; ++nt) mma_s8u8_k32(acc[p][nt], a, bf[nt][0], bf[nt][1]);
+    }
+    if (++since == kEqMmaSteps) {
+      flush();
+      since = 0;
+    }
+  }
+  flush();
+  __syncthreads();
+  for (int i = threadIdx.x; i < nb * 64; i += kMmaThreads)
+    atomicAdd(raw + i, (unsigned long long)tot_s[i >> 6][i & 63]);  // two's complement sum
 }
 
 }  // namespace QFD_NS
