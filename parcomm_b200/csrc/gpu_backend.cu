@@ -151,16 +151,16 @@ static void configure_tile_kernels() {
 GpuBackend::GpuBackend(const Parameters<F>& p, const W* d_bva, size_t active, cudaStream_t s, DeviceTables* tables)
     : P_(p), bva_(d_bva), active_(active), s_(s), tables_(tables ? tables : &own_tables_) {
   configure_tile_kernels();
-  partials_.alloc(148 * 8 * 4);
-  result_.alloc(8);
+  partials_.alloc(qfd::kRedHeader + 148 * 8 * 3);
+  QF_CK(cudaMemsetAsync(partials_.p, 0, 16, s_));  // the reduction counter starts at zero
 }
 GpuBackend::GpuBackend(const Parameters<F>& p, BlockStream* src, cudaStream_t s, DeviceTables* tables)
     : P_(p), bva_(nullptr), src_(src), active_(src->active()), s_(s), tables_(tables ? tables : &own_tables_) {
   configure_tile_kernels();
   check(src->block_len() == P_.block_len, "block length of the weight stream");
   if (src->on_device()) bva_ = src->host();  // gathers read the resident weights directly
-  partials_.alloc(148 * 8 * 4);
-  result_.alloc(8);
+  partials_.alloc(qfd::kRedHeader + 148 * 8 * 3);
+  QF_CK(cudaMemsetAsync(partials_.p, 0, 16, s_));  // the reduction counter starts at zero
 }
 GpuBackend::~GpuBackend() {}
 
@@ -674,15 +674,12 @@ void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, 
   QF_CK(cudaMemcpyAsync(d_root, tree + 2 * off, 32, cudaMemcpyDeviceToDevice, s));
 }
 
-std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n) {
-  switch (n) {
-    case 1: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 16, qfd::k_reduce_partials<1><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;
-    case 2: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 32, qfd::k_reduce_partials<2><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;
-    case 3: QF_LAUNCH(s_, "k_reduce_partials", uint64_t(count) * 48, qfd::k_reduce_partials<3><<<1, kThreads, 0, s_>>>(partials.p, count, result_.p)); break;
-    default: fail(QF_E_ARGUMENT, "reduce arity");
-  }
+// The result of the last reduction kernel (finish_reduction): n elements of
+// the reduction buffer's header.
+std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t, int n) {
+  check(n >= 1 && n + 1 <= qfd::kRedHeader, "reduce arity");
   std::vector<F> out(n);
-  QF_CK(cudaMemcpyAsync(out.data(), result_.p, n * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaMemcpyAsync(out.data(), partials.p + 1, n * 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
   return out;
 }

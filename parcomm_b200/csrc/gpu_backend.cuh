@@ -254,7 +254,7 @@ class GpuBackend : public Backend<F>,
   DBuf<Fe> wit_, qv_, wit2_, qv2_;
   uint64_t eo_len_ = 0;
   std::array<F, 2> cross_;
-  DBuf<Fe> partials_, result_;
+  DBuf<Fe> partials_;  // reduction buffer: header (counter, result) + one slot per CTA
 };
 
 }  // namespace QFB_NS

@@ -44,19 +44,39 @@ __device__ void block_reduce(Fr (&v)[N]) {
       for (int n = 0; n < N; ++n) v[n] = add(v[n], red_s[w][n]);
   }
 }
-// partials[blockIdx][N] -> out[N] (single CTA).
+// One-launch reductions.  A reduction buffer holds a 4-element header and
+// then one slot of N elements per CTA: header word 0 counts the CTAs that
+// have finished (zero between launches), header elements 1..N receive the
+// result.  Each CTA stores its totals in its slot; the last one to finish
+// sums every slot, writes the result and re-arms the counter, so the host
+// reads the result right after the producing kernel with no reduction launch.
+constexpr int kRedHeader = 4;
 template <int N>
-__global__ void k_reduce_partials(const Fe* __restrict__ partials, uint32_t count, Fe* __restrict__ out) {
-  Fr v[N];
+__device__ void finish_reduction(Fr (&v)[N], Fe* __restrict__ buf) {
+  __shared__ bool last_s;
+  Fe* part = buf + kRedHeader;
+  if (threadIdx.x == 0) {
 #pragma unroll
-  for (int n = 0; n < N; ++n) v[n] = zero();
-  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x)
+    for (int n = 0; n < N; ++n) store(part + size_t(blockIdx.x) * N + n, v[n]);
+    __threadfence();
+    last_s = atomicAdd(reinterpret_cast<unsigned*>(buf), 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last_s) return;
+  __threadfence();
+  Fr s[N];
 #pragma unroll
-    for (int n = 0; n < N; ++n) v[n] = add(v[n], load(partials + size_t(i) * N + n));
-  block_reduce<N>(v);
-  if (threadIdx.x == 0)
+  for (int n = 0; n < N; ++n) s[n] = zero();
+  for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x)
 #pragma unroll
-    for (int n = 0; n < N; ++n) store(out + n, v[n]);
+    for (int n = 0; n < N; ++n)  // other CTAs' stores: read through L2
+      s[n] = add(s[n], unpack_fe(__ldcg(reinterpret_cast<const uint4*>(part + size_t(i) * N + n))));
+  block_reduce<N>(s);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) store(buf + 1 + n, s[n]);
+    *reinterpret_cast<unsigned*>(buf) = 0u;
+  }
 }
 
 // Two-level product table: t[i] = hi[i >> lb] * lo[i & (2^lb - 1)].
@@ -195,9 +215,7 @@ __global__ void k_eo_dot_cross(const Fe* __restrict__ w, const Fe* __restrict__ 
   }
   Fr v[3] = {acc_reduce(acc[0]), acc_reduce(acc[1]), acc_reduce(acc[2])};
   block_reduce<3>(v);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) store(partials + size_t(blockIdx.x) * 3 + k, v[k]);
+  finish_reduction<3>(v, partials);
 }
 // w'[i] = w[2i] + w[2i+1] * inv; q'[i] = q[2i] + q[2i+1] * ch, plus the next
 // cross pair of (w', q') (eo.rs:141-160, fold_in_place 57-79).
@@ -226,9 +244,7 @@ __global__ void k_eo_fold_cross(const Fe* __restrict__ w, const Fe* __restrict__
   }
   Fr v[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(v);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) store(partials + size_t(blockIdx.x) * 2 + k, v[k]);
+  finish_reduction<2>(v, partials);
 }
 
 // The same fold as k_eo_fold_cross, one vector at a time, so the full-length
@@ -259,9 +275,7 @@ __global__ void k_eo_fold_query_cross(const Fe* __restrict__ wf, const Fe* __res
   }
   Fr v[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(v);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < 2; ++k) store(partials + size_t(blockIdx.x) * 2 + k, v[k]);
+  finish_reduction<2>(v, partials);
 }
 
 // ---------------------------------------------------------------- batch opening
@@ -306,7 +320,7 @@ __global__ void k_sum_message(const Fe* __restrict__ v, const Fe* __restrict__ w
   }
   Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
-  if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
+  finish_reduction<2>(s, partials);
 }
 // Fold both vectors at ch (lo <- lo + ch (hi - lo), packed.rs:674-696) and
 // emit the next message of the folded vectors.  Thread i < n/4 produces
@@ -339,7 +353,7 @@ __global__ void k_sum_fold_message(const Fe* __restrict__ v, const Fe* __restric
   }
   Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
-  if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
+  finish_reduction<2>(s, partials);
 }
 
 // ---------------------------------------------------------------- codeword access

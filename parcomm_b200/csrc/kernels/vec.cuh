@@ -32,7 +32,7 @@ __global__ void k_dot(const Fe* __restrict__ a, const Fe* __restrict__ b, uint64
     mul_acc(acc, load(a + i), load(b + i));
   Fr s[1] = {acc_reduce(acc)};
   block_reduce<1>(s);
-  if (threadIdx.x == 0) store(partials + blockIdx.x, s[0]);
+  finish_reduction<1>(s, partials);
 }
 // LiteBullet cross pair of (L, R) with half h: sum L[i] R[h+i], sum L[h+i] R[i].
 __global__ void k_lb_cross(const Fe* __restrict__ L, const Fe* __restrict__ R, uint64_t n, Fe* __restrict__ partials) {
@@ -44,7 +44,7 @@ __global__ void k_lb_cross(const Fe* __restrict__ L, const Fe* __restrict__ R, u
   }
   Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
-  if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
+  finish_reduction<2>(s, partials);
 }
 // Fold L[i] += L[h+i] * wl, R[i] += R[h+i] * wr (h = n/2), in place, and emit
 // the cross pair of the folded length-h vectors.  Thread i < n/4 owns the
@@ -74,7 +74,7 @@ __global__ void k_lb_fold_cross(Fe* __restrict__ L, Fe* __restrict__ R, uint64_t
   }
   Fr s[2] = {acc_reduce(acc[0]), acc_reduce(acc[1])};
   block_reduce<2>(s);
-  if (threadIdx.x == 0) { store(partials + 2 * blockIdx.x, s[0]); store(partials + 2 * blockIdx.x + 1, s[1]); }
+  finish_reduction<2>(s, partials);
 }
 // out[r] = sum_b w[b] * in[b * rows + r]  (block coordinate fold, b < nb)
 __global__ void k_block_combine(const Fe* __restrict__ in, uint64_t rows, int nb, const Fe* __restrict__ w, Fe* __restrict__ out) {
