@@ -707,23 +707,25 @@ def main():
                 "frac": h2d_achieved / h2d_peak, "bytes_per_step": h2d_dev,
                 "peak_source": "pinned 2 GiB host->device copy, best of 3, measured in this run"}
 
-    # The tensor-core weight passes against the dp4a / IMAD kernels they
-    # replace (F65521): one more profiled step with them switched off, same bytes.
+    # The exact integer-limb tensor-core forms of the weight passes against
+    # the dp4a / IMAD kernels the library runs (F65521): one more profiled
+    # step with them switched on, same bytes.
     imma_cmp = None
     if not sixteen and not args.no_compare:
-        qf.kernel_option("imma", 0)
-        qf.kernel_timing(True)
-        pr_off, _, _ = step(True)
-        torch.cuda.synchronize()
-        off = qf.kernel_stats()
-        qf.kernel_timing(False)
         qf.kernel_option("imma", 1)
-        assert pr_off.to_bytes() == proof.to_bytes(), "dp4a-path proof bytes differ"
+        qf.kernel_timing(True)
+        pr_on, _, _ = step(True)
+        torch.cuda.synchronize()
+        on_stats = qf.kernel_stats()
+        qf.kernel_timing(False)
+        qf.kernel_option("imma", 0)
+        assert pr_on.to_bytes() == proof.to_bytes(), "tensor-core path proof bytes differ"
+        off = stats
         pairs = {"eo_witness": ("k_eo_witness_mma", "k_eo_witness"), "block_fold": ("k_block_fold_mma", "k_block_fold"),
                  "eq_projection": ("k_eq_project_mma", "k_eq_project_blocks")}
         imma_cmp = {}
         for name, (on_k, off_k) in pairs.items():
-            a, b = stats.get(on_k), off.get(off_k)
+            a, b = on_stats.get(on_k), off.get(off_k)
             if a and b:
                 imma_cmp[name] = {"imma_ms": a["ms"], "dp4a_ms": b["ms"], "speedup": b["ms"] / a["ms"],
                                   "imma_hbm_frac": a["bytes"] / (a["ms"] / 1000.0) / 1e9 / peak,

@@ -159,16 +159,17 @@ uint64_t qf_kernel_launches(void);
 /* Diagnostics, no reference counterpart: the current device's integer issue
  * peaks in thread-level operations per second, measured by a microbenchmark
  * (independent chains of 32-bit XORs, of 32-bit multiply-adds, of both
- * interleaved, and of 32 x 32 -> 64-bit multiply-adds): out[0] the ALU pipe,
- * out[1] the FMA pipe, out[2] both, out[3] widening multiply-adds.  They are
- * the denominators of the integer roofline; qf_kernel_stats reports each
- * kernel's algorithmic integer operations as "ops". */
-int qf_kernel_int_peaks(double out[4]);
+ * interleaved, of 32 x 32 -> 64-bit multiply-adds, of dp4a and of funnel-shift
+ * rotations): out[0] the ALU pipe, out[1] the FMA pipe, out[2] both, out[3]
+ * widening multiply-adds, out[4] dp4a, out[5] rotations.  They are the
+ * denominators of the integer roofline; qf_kernel_stats reports each kernel's
+ * algorithmic integer operations as "ops". */
+int qf_kernel_int_peaks(double out[6]);
 /* Diagnostics, no reference counterpart: process-wide kernel choices that
- * write identical bytes, for comparisons.  "imma" (default 1): the F65521
- * weight passes (EO witness, block fold, equality-table lane sums) contract
- * on the tensor cores with exact integer limbs; 0 selects the dp4a / IMAD
- * kernels.  "per_matrix"
+ * write identical bytes, for comparisons.  "imma" (default 0): 1 makes the
+ * F65521 weight passes (EO witness, block fold, equality-table lane sums)
+ * contract on the tensor cores with exact integer limbs instead of the dp4a
+ * / IMAD kernels (measured slower on B200; kept for the comparison).  "per_matrix"
  * (default 0): 1 issues the weight passes one launch per term, bucket or
  * block instead of one launch over all of them.  Set it between calls, not
  * while another call runs. */

@@ -453,7 +453,7 @@ def kernel_launches() -> int:
 
 
 def kernel_option(name: str, value: int) -> None:
-    """qf_kernel_option: "imma" (tensor-core weight passes, default on) or
+    """qf_kernel_option: "imma" (tensor-core weight passes, default off) or
     "per_matrix" (one launch per term / bucket / block, default off); both
     settings write identical bytes."""
     _check(lib().qf_kernel_option(name.encode(), int(value)))
@@ -464,9 +464,10 @@ def int_peaks() -> dict:
     the ALU pipe (XOR chains), the FMA pipe (multiply-add chains), both
     interleaved, and widening 32 x 32 -> 64-bit multiply-adds; the
     denominators of the integer roofline."""
-    out = (ctypes.c_double * 4)()
+    out = (ctypes.c_double * 6)()
     _check(lib().qf_kernel_int_peaks(out))
-    return {"alu_ops_per_s": out[0], "fma_ops_per_s": out[1], "issue_ops_per_s": out[2], "mad_wide_per_s": out[3]}
+    return {"alu_ops_per_s": out[0], "fma_ops_per_s": out[1], "issue_ops_per_s": out[2], "mad_wide_per_s": out[3],
+            "dp4a_per_s": out[4], "rotate_per_s": out[5]}
 
 
 def demo_shapes() -> List[Shape]:

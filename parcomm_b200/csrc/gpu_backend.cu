@@ -534,6 +534,46 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
   strided_passes<qfd::kWht>(s, par, par, logR, logm, kT, logR, timed, allow_tuning);
 }
 
+// Inner levels of a row tree over the n_leaves digests at tree[0..): level j
+// at digest offset level_off[j], the root last.  Launches of three levels
+// per thread (k_hash_subtrees: each thread hashes an 8-child subtree, no
+// barrier) while the level they reach keeps at least 2^11 nodes, then one CTA
+// for the levels above (k_hash_top): 5 launches for 2^23 leaves instead of 23.
+static void build_tree(cudaStream_t s, uint4* tree, uint64_t n_leaves, std::vector<uint64_t>& level_off, bool timed) {
+  level_off.clear();
+  for (uint64_t k = n_leaves, off = 0;; k /= 2) {
+    level_off.push_back(off);
+    off += k;
+    if (k <= 1) break;
+  }
+  const ::qfd::InnerPrefix ip = inner_prefix();
+  constexpr int kTopLog = 11;
+  size_t j = 0;
+  uint64_t n = n_leaves;
+  while (n > (uint64_t(1) << kTopLog)) {
+    const int L = std::min(3, ilog2(n) - kTopLog);
+    ::qfd::TreeLevels lv{};
+    for (int t = 0; t <= L; ++t) lv.off[t] = level_off[j + t];
+    const uint64_t top = n >> L;
+    const unsigned grid = unsigned((top + kThreads - 1) / kThreads);
+    launch(s, timed, "k_hash_inner", n * 32 + (n - top) * 32, qf_intops::inner_hash_ops(n - top), [&] {
+      switch (L) {
+        case 1: qfd::k_hash_subtrees<1><<<grid, kThreads, 0, s>>>(tree, top, lv, ip); break;
+        case 2: qfd::k_hash_subtrees<2><<<grid, kThreads, 0, s>>>(tree, top, lv, ip); break;
+        default: qfd::k_hash_subtrees<3><<<grid, kThreads, 0, s>>>(tree, top, lv, ip); break;
+      }
+    });
+    j += L;
+    n = top;
+  }
+  if (n > 1) {
+    ::qfd::TreeLevels lv{};
+    for (int t = 0; t <= ilog2(n); ++t) lv.off[t] = level_off[j + t];
+    launch(s, timed, "k_hash_inner", n * 32 + (n - 1) * 32, qf_intops::inner_hash_ops(n - 1),
+           [&] { qfd::k_hash_top<<<1, unsigned(std::min<uint64_t>(1024, n / 2)), 0, s>>>(tree, n, lv, ip); });
+  }
+}
+
 // Encode (see encode_passes), then leaf hashes and tree.
 void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR, int logm, bool ext_domain, int mob_from) {
   const size_t R = size_t(1) << logR;
@@ -549,20 +589,9 @@ void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR,
   else
     QF_LAUNCH_OPS(s_, "k_hash_leaves", n_ext * out.n_cols * 16 + n_ext * 32, leaf_ops,
                   qfd::k_hash_leaves<11><<<lgrid, qfd::kLeafThreads, 0, s_>>>(out.cw.p, n_ext, int(out.n_cols), lp, out.tree.p));
-  ::qfd::InnerPrefix ip = inner_prefix();
-  out.level_off.clear();
-  uint64_t off = 0, n = n_ext;
-  while (n > 1) {
-    out.level_off.push_back(off);
-    QF_LAUNCH_OPS(s_, "k_hash_inner", n * 32 + (n / 2) * 32, qf_intops::inner_hash_ops(n / 2),
-                  qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s_>>>(
-                      out.tree.p + 2 * off, n / 2, ip, out.tree.p + 2 * (off + n)));
-    off += n;
-    n /= 2;
-  }
-  out.level_off.push_back(off);
+  build_tree(s_, out.tree.p, n_ext, out.level_off, true);
   uint4 r[2];
-  QF_CK(cudaMemcpyAsync(r, out.tree.p + 2 * off, 32, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaMemcpyAsync(r, out.tree.p + 2 * out.level_off.back(), 32, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
   out.root_ = digest_from_words(r);
 }
@@ -663,15 +692,9 @@ void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, 
   qfd::k_hash_leaves<11><<<unsigned((n_ext + qfd::kLeafThreads - 1) / qfd::kLeafThreads), qfd::kLeafThreads, 0, s>>>(
       cw, n_ext, int(cols), leaf_prefix(cols, false), tree);
   QF_CK(cudaGetLastError());
-  const ::qfd::InnerPrefix ip = inner_prefix();
-  uint64_t off = 0, n = n_ext;
-  while (n > 1) {
-    qfd::k_hash_inner<<<unsigned((n / 2 + kThreads - 1) / kThreads), kThreads, 0, s>>>(tree + 2 * off, n / 2, ip, tree + 2 * (off + n));
-    QF_CK(cudaGetLastError());
-    off += n;
-    n /= 2;
-  }
-  QF_CK(cudaMemcpyAsync(d_root, tree + 2 * off, 32, cudaMemcpyDeviceToDevice, s));
+  std::vector<uint64_t> level_off;
+  build_tree(s, tree, n_ext, level_off, false);
+  QF_CK(cudaMemcpyAsync(d_root, tree + 2 * level_off.back(), 32, cudaMemcpyDeviceToDevice, s));
 }
 
 // The result of the last reduction kernel (finish_reduction): n elements of

@@ -122,7 +122,7 @@ size_t DevicePool::cached_bytes() {
   return n;
 }
 
-std::atomic<int> KernelOptions::imma{1};
+std::atomic<int> KernelOptions::imma{0};
 std::atomic<int> KernelOptions::per_matrix{0};
 
 bool KernelClock::enabled = false;

@@ -30,7 +30,8 @@ using namespace qf;
 
 // Process-wide kernel choices, for comparisons that must write the same
 // bytes: `imma` runs the F65521 weight passes on the tensor cores (exact
-// integer limbs) instead of the dp4a / IMAD kernels; `per_matrix` issues the
+// integer limbs) instead of the dp4a / IMAD kernels (off by default: slower
+// as measured on B200); `per_matrix` issues the
 // weight passes one launch per term, bucket or block instead of one launch
 // over all of them.  Set through qf_kernel_option.
 struct KernelOptions {

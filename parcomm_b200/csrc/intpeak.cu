@@ -1,8 +1,9 @@
 // Integer issue peaks of the device, the denominators of the integer
 // roofline: independent chains of 32-bit XORs (the ALU pipe), of 32-bit
 // multiply-adds (the FMA pipe), of both interleaved (the issue limit when
-// both pipes are fed), and of 32 x 32 -> 64-bit multiply-adds (the extension
-// products' inner operation).  Each thread runs 8 independent chains so that
+// both pipes are fed), of 32 x 32 -> 64-bit multiply-adds (the extension
+// products' inner operation), of dp4a (the weight passes) and of funnel-shift
+// rotations (BLAKE2s).  Each thread runs 8 independent chains so that
 // the dependent latency is hidden; the grid fills every SM with 4 CTAs of 256
 // threads.  The instructions are written as inline PTX so the compiler
 // neither folds nor reorders them into other forms.
@@ -35,8 +36,19 @@ __device__ __forceinline__ uint64_t op_mad_wide(uint32_t a, uint32_t b, uint64_t
   return d;
 }
 
+__device__ __forceinline__ uint32_t op_dp4a(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t d;
+  asm volatile("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+__device__ __forceinline__ uint32_t op_shf(uint32_t a, uint32_t n) {
+  uint32_t d;
+  asm volatile("shf.r.wrap.b32 %0, %1, %1, %2;" : "=r"(d) : "r"(a), "r"(n));
+  return d;
+}
+
 // KIND 0: XOR only; 1: multiply-add only; 2: alternating; 3: widening
-// multiply-add (64-bit accumulators).
+// multiply-add (64-bit accumulators); 4: dp4a; 5: funnel-shift rotations.
 template <int KIND>
 __global__ void __launch_bounds__(256) k_int_peak(uint32_t* sink, uint32_t iters, uint32_t seed) {
   uint32_t a[kChains];
@@ -55,7 +67,9 @@ __global__ void __launch_bounds__(256) k_int_peak(uint32_t* sink, uint32_t iters
         if (KIND == 0) a[c] = op_xor(a[c], b + uint32_t(u));
         else if (KIND == 1) a[c] = op_mad(a[c], b);
         else if (KIND == 2) a[c] = ((u + c) & 1) ? op_mad(a[c], b) : op_xor(a[c], b + uint32_t(u));
-        else w[c] = op_mad_wide(a[c], b + uint32_t(u), w[c]);
+        else if (KIND == 3) w[c] = op_mad_wide(a[c], b + uint32_t(u), w[c]);
+        else if (KIND == 4) a[c] = op_dp4a(b + uint32_t(u), b, a[c]);
+        else a[c] = op_shf(a[c], 7u + uint32_t(u));
       }
   }
   uint32_t x = 0;
@@ -105,6 +119,8 @@ extern "C" int qf_kernel_int_peaks(double* out) {
     out[1] = measure<1>(sink, sms);
     out[2] = measure<2>(sink, sms);
     out[3] = measure<3>(sink, sms);
+    out[4] = measure<4>(sink, sms);
+    out[5] = measure<5>(sink, sms);
     QF_CK(cudaFree(sink));
   });
 }

@@ -569,14 +569,9 @@ __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restri
   leaves[2 * r + 1] = make_uint4(h[4], h[5], h[6], h[7]);
 }
 
-// Inner node = BLAKE2s(50-byte prefix || left || right), 114 bytes.
-__global__ void k_hash_inner(const uint4* __restrict__ children, uint64_t n_parents, ::qfd::InnerPrefix pre, uint4* __restrict__ parents) {
-  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n_parents) return;
-  uint32_t d[16];
-  uint4 a = children[4 * i], b = children[4 * i + 1], c = children[4 * i + 2], e = children[4 * i + 3];
-  d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w; d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
-  d[8] = c.x; d[9] = c.y; d[10] = c.z; d[11] = c.w; d[12] = e.x; d[13] = e.y; d[14] = e.z; d[15] = e.w;
+// Inner node = BLAKE2s(50-byte prefix || left || right), 114 bytes.  d holds
+// the two children's 16 words; h receives the parent's 8.
+__device__ __forceinline__ void inner_hash(const uint32_t (&d)[16], const ::qfd::InnerPrefix& pre, uint32_t (&h)[8]) {
   uint32_t buf[32];
 #pragma unroll
   for (int k = 0; k < 12; ++k) buf[k] = pre.w[k];
@@ -588,14 +583,73 @@ __global__ void k_hash_inner(const uint4* __restrict__ children, uint64_t n_pare
   }
 #pragma unroll
   for (int k = 29; k < 32; ++k) buf[k] = 0;
-  uint32_t h[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) h[k] = ::qfd::kIv[k];
   h[0] ^= 0x01010020u;
   ::qfd::compress(h, buf, 64u, false, pre.one);
   ::qfd::compress(h, buf + 16, 114u, true, pre.one);
-  parents[2 * i] = make_uint4(h[0], h[1], h[2], h[3]);
-  parents[2 * i + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
+// Digest offsets (in digests, 2 uint4 each) of the levels a launch reads and
+// writes: off[0] the children's level, off[j] the level j above it.
+struct TreeLevels {
+  uint64_t off[12];
+};
+
+// The node at height D above level 0 with index `idx` in its level, from its
+// 2^D descendants at level 0; every node it makes is stored in its level.
+template <int D>
+__device__ __forceinline__ void subtree_hash(uint4* __restrict__ tree, const TreeLevels& lv, uint64_t idx,
+                                             const ::qfd::InnerPrefix& pre, uint32_t (&h)[8]) {
+  if constexpr (D == 0) {
+    const uint4 a = tree[2 * (lv.off[0] + idx)], b = tree[2 * (lv.off[0] + idx) + 1];
+    h[0] = a.x; h[1] = a.y; h[2] = a.z; h[3] = a.w; h[4] = b.x; h[5] = b.y; h[6] = b.z; h[7] = b.w;
+  } else {
+    uint32_t d[16];
+    {
+      uint32_t l[8], r[8];
+      subtree_hash<D - 1>(tree, lv, 2 * idx, pre, l);
+      subtree_hash<D - 1>(tree, lv, 2 * idx + 1, pre, r);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { d[k] = l[k]; d[8 + k] = r[k]; }
+    }
+    inner_hash(d, pre, h);
+    tree[2 * (lv.off[D] + idx)] = make_uint4(h[0], h[1], h[2], h[3]);
+    tree[2 * (lv.off[D] + idx) + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+  }
+}
+
+// L inner levels in one launch: thread i hashes the 2^L children [i 2^L,
+// (i + 1) 2^L) of level off[0] up to their common ancestor (2^L - 1 node
+// hashes, depth first, no barrier), for the n_top nodes of level off[L].
+template <int L>
+__global__ void k_hash_subtrees(uint4* __restrict__ tree, uint64_t n_top, TreeLevels lv, ::qfd::InnerPrefix pre) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n_top) return;
+  uint32_t h[8];
+  subtree_hash<L>(tree, lv, i, pre, h);
+}
+
+// The top of a tree in one CTA: from the n children at level off[0] (n a
+// power of two, n / 2 <= blockDim.x) every level up to the root, one node per
+// thread and level, a barrier between levels (the children a level reads are
+// the previous level's stores of other threads of this CTA).
+__global__ void k_hash_top(uint4* __restrict__ tree, uint64_t n, TreeLevels lv, ::qfd::InnerPrefix pre) {
+  int j = 0;
+  for (uint64_t parents = n / 2; parents >= 1; parents /= 2, ++j) {
+    for (uint64_t i = threadIdx.x; i < parents; i += blockDim.x) {
+      const uint4* c = tree + 2 * (lv.off[j] + 2 * i);
+      uint32_t d[16];
+      const uint4 a = __ldcg(c), b = __ldcg(c + 1), e = __ldcg(c + 2), f = __ldcg(c + 3);
+      d[0] = a.x; d[1] = a.y; d[2] = a.z; d[3] = a.w; d[4] = b.x; d[5] = b.y; d[6] = b.z; d[7] = b.w;
+      d[8] = e.x; d[9] = e.y; d[10] = e.z; d[11] = e.w; d[12] = f.x; d[13] = f.y; d[14] = f.z; d[15] = f.w;
+      uint32_t h[8];
+      inner_hash(d, pre, h);
+      tree[2 * (lv.off[j + 1] + i)] = make_uint4(h[0], h[1], h[2], h[3]);
+      tree[2 * (lv.off[j + 1] + i) + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+    }
+    __syncthreads();
+  }
 }
 
 }  // namespace QFD_NS

@@ -8,7 +8,7 @@ hashing of the deepest levels, the deepest strided transform passes over
 2^27-element codeword halves, and a half-live last block.  The weights are the
 benchmark's own synthetic draws (bench.make_bva_on_device, same seeds): the
 embedding matrix of the 8B set alone (one block), and embedding + output head
-(two blocks, the second partly live).  Each case compares roots, claims and
++ one MLP gate matrix (two blocks, the second partly live).  Each case compares roots, claims and
 proof bytes with the oracle (qafold/f65521/src/protocol.rs:201-263; the query
 counts of vendor/qafold/src/qafold.rs:75-178) and checks both verifiers.
 The oracle needs about a minute per 10^9 weights on 16 host threads."""
@@ -57,8 +57,9 @@ def test_f65521_embedding_one_block_chunk30():
     assert p.blocks == 1
 
 
-def test_f65521_embedding_and_head_two_blocks_chunk30():
-    p = prove_both([EMBED, EMBED], "f65521", False)
+def test_f65521_embedding_head_and_gate_two_blocks_chunk30():
+    # 1.11 G weights: two 2^30 blocks, the second about a tenth live.
+    p = prove_both([EMBED, EMBED, (14336, 4096)], "f65521", False)
     assert p.blocks == 2 and p.active > (1 << 30)
 
 
