@@ -552,7 +552,7 @@ static void build_tree(cudaStream_t s, uint4* tree, uint64_t n_leaves, std::vect
   uint64_t n = n_leaves;
   while (n > (uint64_t(1) << kTopLog)) {
     const int L = std::min(3, ilog2(n) - kTopLog);
-    ::qfd::TreeLevels lv{};
+    qfd::TreeLevels lv{};
     for (int t = 0; t <= L; ++t) lv.off[t] = level_off[j + t];
     const uint64_t top = n >> L;
     const unsigned grid = unsigned((top + kThreads - 1) / kThreads);
@@ -567,7 +567,7 @@ static void build_tree(cudaStream_t s, uint4* tree, uint64_t n_leaves, std::vect
     n = top;
   }
   if (n > 1) {
-    ::qfd::TreeLevels lv{};
+    qfd::TreeLevels lv{};
     for (int t = 0; t <= ilog2(n); ++t) lv.off[t] = level_off[j + t];
     launch(s, timed, "k_hash_inner", n * 32 + (n - 1) * 32, qf_intops::inner_hash_ops(n - 1),
            [&] { qfd::k_hash_top<<<1, unsigned(std::min<uint64_t>(1024, n / 2)), 0, s>>>(tree, n, lv, ip); });
