@@ -1259,10 +1259,8 @@ std::vector<std::vector<std::vector<F>>> GpuBackend::project_groups_streamed(
     for (size_t g = 0; g < G; ++g) {
       const uint64_t tiles = tiles_bg[b][g];
       if (!tiles) continue;
-      QF_LAUNCH(s_, "k_project_terms", n * sizeof(W),
-                qfd::k_project_terms<<<unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0, s_>>>(
-                    d, n, dall.p + piece_at[b][g], int(pieces[b][g].size()), uint32_t(tiles), tables.p, int(lanes_of[g]),
-                    dtile[g].p + tile_base[b][g] * lanes_of[g]));
+      project_terms_launch(d, n, dall.p + piece_at[b][g], int(pieces[b][g].size()), tiles, tables.p, lanes_of[g],
+                           dtile[g].p + tile_base[b][g] * lanes_of[g], n * sizeof(W));
     }
   });
   for (size_t g = 0; g < G; ++g) {
@@ -1280,6 +1278,24 @@ std::vector<std::vector<std::vector<F>>> GpuBackend::project_groups_streamed(
       for (size_t l = 0; l < lanes_of[g]; ++l) out[g][seg_term[g][k]][l] += h[k * lanes_of[g] + l];
   }
   return out;
+}
+
+// Lane projections of `n_terms` term tile lists (`tiles` tiles) into out:
+// the dp4a kernel for F65521 terms of 16 lanes, the general one otherwise.
+void GpuBackend::project_terms_launch(const W* bva, uint64_t active, const qfd::TermTiles* terms, int n_terms,
+                                      uint64_t tiles, const Fe* tables, size_t lanes, Fe* out, uint64_t bytes) {
+  const unsigned grid = unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta);
+#if !defined(QF_FIELD_KB)
+  if (lanes == 16) {
+    QF_LAUNCH(s_, "k_project_terms", bytes,
+              qfd::k_project_terms16<<<grid, qfd::kTermThreads, 0, s_>>>(bva, active, terms, n_terms, uint32_t(tiles),
+                                                                         tables, out));
+    return;
+  }
+#endif
+  QF_LAUNCH(s_, "k_project_terms", bytes,
+            qfd::k_project_terms<<<grid, qfd::kTermThreads, 0, s_>>>(bva, active, terms, n_terms, uint32_t(tiles), tables,
+                                                                     int(lanes), out));
 }
 
 std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Term<F>*>& terms, size_t stride) {
@@ -1324,17 +1340,12 @@ std::vector<std::vector<F>> GpuBackend::project_terms(const std::vector<const Te
     QF_CK(cudaMemcpyAsync(dtt.p, solo.data(), solo.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
     for (size_t k = 0; k < tt.size(); ++k) {
       const uint64_t n = term_tile_count(tt[k]);
-      QF_LAUNCH(s_, "k_project_terms", tt[k].rows * common_lanes * sizeof(W) + n * 16,
-                qfd::k_project_terms<<<unsigned((n + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0, s_>>>(
-                    bva_, active_, dtt.p + k, 1, uint32_t(n), tables.p, int(common_lanes),
-                    dtile.p + size_t(tt[k].first_tile) * common_lanes));
+      project_terms_launch(bva_, active_, dtt.p + k, 1, n, tables.p, common_lanes,
+                           dtile.p + size_t(tt[k].first_tile) * common_lanes, tt[k].rows * common_lanes * sizeof(W) + n * 16);
     }
   } else {
     QF_CK(cudaMemcpyAsync(dtt.p, tt.data(), tt.size() * sizeof(qfd::TermTiles), cudaMemcpyHostToDevice, s_));
-    QF_LAUNCH(s_, "k_project_terms", proj_bytes,
-              qfd::k_project_terms<<<unsigned((tiles + qfd::kTilesPerCta - 1) / qfd::kTilesPerCta), qfd::kTermThreads, 0,
-                                     s_>>>(bva_, active_, dtt.p, int(tt.size()), uint32_t(tiles), tables.p,
-                                           int(common_lanes), dtile.p));
+    project_terms_launch(bva_, active_, dtt.p, int(tt.size()), tiles, tables.p, common_lanes, dtile.p, proj_bytes);
   }
   QF_LAUNCH(s_, "k_sum_segments", tiles * common_lanes * 16, qfd::k_sum_segments<<<unsigned(terms.size()), kThreads, 0, s_>>>(dtile.p, dseg.p, int(common_lanes), dterm.p));
   std::vector<F> h(terms.size() * common_lanes);

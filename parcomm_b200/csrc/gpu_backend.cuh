@@ -10,6 +10,10 @@
 #include "field_select.h"
 #include "gpu_common.cuh"
 
+namespace QFD_NS {
+struct TermTiles;  // kernels/open.cuh
+}
+
 namespace QFB_NS {
 using namespace qf;
 using namespace qfg;
@@ -227,6 +231,8 @@ class GpuBackend : public Backend<F>,
                                                                    size_t stride);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
   void block_fold_launch(const W* bva, uint64_t active, int blocks, const Fe* T, int accumulate);
+  void project_terms_launch(const W* bva, uint64_t active, const qfd::TermTiles* terms, int n_terms, uint64_t tiles,
+                            const Fe* tables, size_t lanes, Fe* out, uint64_t bytes);
   void eq_project_launch(const W* bva, uint64_t active, uint64_t b0, int nb, unsigned long long* raw, unsigned grid);
   void eo_witness_launch(const W* bva, uint64_t active, uint64_t rows, size_t stride, const Fe* powers, Fe* out);
 

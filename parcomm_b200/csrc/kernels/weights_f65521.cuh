@@ -20,6 +20,16 @@ __device__ __forceinline__ int32_t dp4a_su(uint32_t a, uint32_t b, int32_t c) {
   asm("dp4a.s32.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
   return d;
 }
+// 4 x 4 byte transpose: out[b] = byte b of x0, x1, x2, x3 (in that order).
+__device__ __forceinline__ void transpose4(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3, uint32_t (&out)[4]) {
+  const uint32_t t0 = __byte_perm(x0, x1, 0x5140), t1 = __byte_perm(x0, x1, 0x7362);
+  const uint32_t t2 = __byte_perm(x2, x3, 0x5140), t3 = __byte_perm(x2, x3, 0x7362);
+  out[0] = __byte_perm(t0, t2, 0x5410);
+  out[1] = __byte_perm(t0, t2, 0x7632);
+  out[2] = __byte_perm(t1, t3, 0x5410);
+  out[3] = __byte_perm(t1, t3, 0x7632);
+}
+
 // Byte planes of the coefficient k of four elements e[0..3]: lo = the low
 // bytes, hi = the high bytes, lane i in byte i.
 __device__ __forceinline__ void byte_planes(const Fe* e, int k, uint32_t& lo, uint32_t& hi) {
@@ -128,6 +138,110 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms(const int8_t* __
   }
 }
 
+// Lane projections of terms with 16 lanes (stride 16), in dp4a form: a
+// thread takes groups of 4 rows, lanes 8 lh .. 8 lh + 7 and coefficients
+// 4 h .. 4 h + 3 (thread 4 g + 2 lh + h).  The 4 rows' weights of a lane and
+// the 4 rows' low (high) bytes of a table coefficient transpose into words,
+// so each dp4a adds 4 products.  A thread sums at most 16 rows of a tile
+// (16 * 128 * 65520 < 2^28), a warp reduce-scatter over the 8 lanes of the
+// same (lh, h) stays below 2^31, then i64 across warps and one reduction.
+__global__ void __launch_bounds__(kTermThreads) k_project_terms16(const int8_t* __restrict__ bva, uint64_t active,
+                                                                  const TermTiles* __restrict__ terms, int n_terms,
+                                                                  uint32_t n_tiles, const Fe* __restrict__ tables,
+                                                                  Fe* __restrict__ out) {
+  __shared__ int t_sel;
+  __shared__ int64_t part_s[kTermThreads / 32][16][8];
+  const uint32_t tile0 = blockIdx.x * kTilesPerCta;
+  if (threadIdx.x == 0) t_sel = find_term(terms, n_terms, tile0);
+  __syncthreads();
+  int ti = t_sel;
+  const int h = threadIdx.x & 1, lh = (threadIdx.x >> 1) & 1, grp = threadIdx.x >> 2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int kGroups = kTermThreads / 4;
+  for (uint32_t tile = tile0; tile < tile0 + kTilesPerCta && tile < n_tiles; ++tile) {
+    while (ti + 1 < n_terms && terms[ti + 1].first_tile <= tile) ++ti;
+    const TermTiles T = terms[ti];
+    const uint64_t i = tile - T.first_tile + T.tile_skip;
+    const uint64_t row0 = i << T.lb;
+    const uint64_t span = uint64_t(1) << T.lb, left = T.rows - row0;
+    const int nrows = int(left < span ? left : span);
+    const Fe* lot = tables + T.lo_off;
+    int32_t lo[8][4], hi[8][4];
+#pragma unroll
+    for (int l = 0; l < 8; ++l)
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) lo[l][kk] = hi[l][kk] = 0;
+    for (int r0 = 4 * grp; r0 < nrows; r0 += 4 * kGroups) {
+      uint32_t x[8], y[8];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const uint64_t g = T.offset + (row0 + r0 + r) * 16 + 8 * lh;
+        uint2 u = make_uint2(0, 0), w = make_uint2(0, 0);
+        if (r0 + r < nrows) {
+          w = reinterpret_cast<const uint2*>(lot + r0 + r)[h];
+          if (g + 8 <= active) {
+            u = *reinterpret_cast<const uint2*>(bva + g);
+          } else {
+            uint32_t b[2] = {0, 0};
+            for (int y2 = 0; y2 < 8; ++y2)
+              if (g + y2 < active) b[y2 >> 2] |= uint32_t(uint8_t(bva[g + y2])) << (8 * (y2 & 3));
+            u = make_uint2(b[0], b[1]);
+          }
+        }
+        x[2 * r] = u.x;
+        x[2 * r + 1] = u.y;
+        y[2 * r] = w.x;
+        y[2 * r + 1] = w.y;
+      }
+      uint32_t va[4], vb[4], pa[4], pb[4];
+      transpose4(x[0], x[2], x[4], x[6], va);  // lanes 8 lh + 0..3
+      transpose4(x[1], x[3], x[5], x[7], vb);  // lanes 8 lh + 4..7
+      transpose4(y[0], y[2], y[4], y[6], pa);  // {lo, hi} of coefficients 4h, 4h + 1
+      transpose4(y[1], y[3], y[5], y[7], pb);  // {lo, hi} of coefficients 4h + 2, 4h + 3
+      const uint32_t plo[4] = {pa[0], pa[2], pb[0], pb[2]}, phi[4] = {pa[1], pa[3], pb[1], pb[3]};
+#pragma unroll
+      for (int l = 0; l < 8; ++l) {
+        const uint32_t v = l < 4 ? va[l] : vb[l - 4];
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          lo[l][kk] = dp4a_su(v, plo[kk], lo[l][kk]);
+          hi[l][kk] = dp4a_su(v, phi[kk], hi[l][kk]);
+        }
+      }
+    }
+    int32_t acc[32];
+#pragma unroll
+    for (int f = 0; f < 32; ++f) acc[f] = lo[f >> 2][f & 3] + 256 * hi[f >> 2][f & 3];
+    // Reduce-scatter over the 8 lanes with the same (lh, h): the lane keeps
+    // entries (lane & 28) .. + 3, i.e. lane 8 lh + ((lane >> 2) & 7),
+    // coefficients 4 h .. 4 h + 3.
+#pragma unroll
+    for (int o = 16, n = 32; o >= 4; o >>= 1, n >>= 1) {
+      const bool upper = lane & o;
+#pragma unroll
+      for (int qq = 0; qq < n / 2; ++qq) {
+        const int32_t send = upper ? acc[qq] : acc[qq + n / 2];
+        const int32_t keep = upper ? acc[qq + n / 2] : acc[qq];
+        acc[qq] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+      }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) part_s[warp][8 * lh + ((lane >> 2) & 7)][4 * h + qq] = acc[qq];
+    __syncthreads();
+    if (threadIdx.x < 16) {
+      int64_t sum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int w = 0; w < kTermThreads / 32; ++w)
+#pragma unroll
+        for (int k = 0; k < 8; ++k) sum[k] += part_s[w][threadIdx.x][k];
+      Fr v;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v.c[k] = mod_i64(sum[k]);
+      store(out + size_t(tile) * 16 + threadIdx.x, mul(tile_high(T, tables, i), v));
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- EO
 // witness[row] = sum_lane v[row * stride + lane] * inv^lane (eo.rs:119-132).
 // Packed EO witness (eo.rs:119-132): witness[row] = sum_lane v(row * stride +
@@ -146,104 +260,164 @@ __global__ void k_eo_witness(const int8_t* __restrict__ bva, uint64_t active, ui
 #pragma unroll
       for (int q = 0; q < 4; ++q) byte_planes(pw + 4 * q, k, plo[k][q], phi[k][q]);
   }
-  for (uint64_t row = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; row < rows; row += uint64_t(gridDim.x) * blockDim.x) {
-    int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const uint64_t g0 = row * stride;
-    if (stride == 16 && g0 + 16 <= active) {
-      const uint4 raw = *reinterpret_cast<const uint4*>(bva + g0);
-      const uint32_t a[4] = {raw.x, raw.y, raw.z, raw.w};
+  // kWitRows rows per thread and iteration, their loads issued first, so that
+  // enough 16-byte loads are in flight to keep HBM busy.
+  constexpr int kWitRows = 4;
+  const uint64_t nthr = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t row0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; row0 < rows; row0 += kWitRows * nthr) {
+    uint4 raw[kWitRows];
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        int32_t lo = 0, hi = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          lo = dp4a_su(a[q], plo[k][q], lo);
-          hi = dp4a_su(a[q], phi[k][q], hi);
-        }
-        acc[k] = lo + hi * 256;
-      }
-    } else if (g0 < active) {
-      for (int lane = 0; lane < stride; ++lane) {
-        const uint64_t g = g0 + lane;
-        const int v = g < active ? int(bva[g]) : 0;
-        const Fr p = load(pw + lane);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] += int32_t(p.c[k]) * v;
-      }
+    for (int q = 0; q < kWitRows; ++q) {
+      const uint64_t row = row0 + q * nthr;
+      raw[q] = (stride == 16 && row < rows && row * 16 + 16 <= active)
+                   ? *reinterpret_cast<const uint4*>(bva + row * 16)
+                   : make_uint4(0, 0, 0, 0);
     }
-    Fr w;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) w.c[k] = mod_i32(acc[k]);
-    store(witness + row, w);
+    for (int q = 0; q < kWitRows; ++q) {
+      const uint64_t row = row0 + q * nthr;
+      if (row >= rows) break;
+      int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      const uint64_t g0 = row * stride;
+      if (stride == 16 && g0 + 16 <= active) {
+        const uint32_t a[4] = {raw[q].x, raw[q].y, raw[q].z, raw[q].w};
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          int32_t lo = 0, hi = 0;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            lo = dp4a_su(a[c], plo[k][c], lo);
+            hi = dp4a_su(a[c], phi[k][c], hi);
+          }
+          acc[k] = lo + hi * 256;
+        }
+      } else if (g0 < active) {
+        for (int lane = 0; lane < stride; ++lane) {
+          const uint64_t g = g0 + lane;
+          const int v = g < active ? int(bva[g]) : 0;
+          const Fr p = load(pw + lane);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) acc[k] += int32_t(p.c[k]) * v;
+        }
+      }
+      Fr w;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) w.c[k] = mod_i32(acc[k]);
+      store(witness + row, w);
+    }
   }
 }
+
 
 // Raw lane sums of up to kEqBlocks consecutive blocks against the equality
 // weights (project_lanes_from_fn, packed_batch.rs:25-41):
 //   raw[b][j * 8 + k] += sum_i v(b, 8i + j) * weights[i].c[k]
-// A CTA stages a chunk of kEqChunk weights in shared memory and runs every
-// block over it, so the table is read from HBM once for all blocks.  A thread
-// takes 8 elements per block (one 8-byte load each) into 64 i32 sums; a warp
-// reduce-scatter leaves lane l with entries 2l and 2l + 1 (each a sum of 256
-// products, |sum| <= 256 * 128 * 65520 < 2^31), and the CTA keeps i64 totals
-// per block that reach `raw` with one atomic add per entry at the end.
+// in dp4a form: four consecutive elements form a quad; the weights of a quad
+// transpose (byte permutes) into one word per lane j holding its 4 entries,
+// and the table's coefficient k of the quad into a low-byte and a high-byte
+// plane, so one dp4a adds 4 products of a (j, k, byte) entry.  A CTA stages
+// a chunk of kEqChunk table entries as byte planes in shared memory (read
+// from HBM once for all blocks).  Thread 2q + h takes quad q's lanes j = 0..7
+// and coefficients 4h..4h+3.  Per chunk and block a warp covers 256
+// elements; a warp reduce-scatter over the 16 lanes of a coefficient half
+// leaves each lane two entries (|sum| <= 256 * 128 * 65520 < 2^31), and the
+// CTA keeps i64 totals per block that reach `raw` with one atomic add per
+// entry at the end.
 __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_t* __restrict__ bva, uint64_t active,
                                                                     uint64_t block_len, uint64_t first_block, int nb,
                                                                     uint64_t m, const Fe* __restrict__ weights,
                                                                     unsigned long long* __restrict__ raw) {
-  __shared__ uint4 w_s[kEqChunk];
+  constexpr int kQuads = kEqChunk / 4;
+  // planes_s[q][g]: g = 0 low planes of k 0..3, 1 high planes of k 0..3, 2 and 3 the same for k 4..7.
+  __shared__ uint4 planes_s[kQuads][4];
   __shared__ int32_t stage_s[kEqThreads / 32][64];
   __shared__ long long tot_s[kEqBlocks][64];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = threadIdx.x & 1;
   for (int t = threadIdx.x; t < kEqBlocks * 64; t += kEqThreads) tot_s[t >> 6][t & 63] = 0;
   for (uint64_t c0 = uint64_t(blockIdx.x) * kEqChunk; c0 < m; c0 += uint64_t(gridDim.x) * kEqChunk) {
     __syncthreads();
-    for (int e = threadIdx.x; e < kEqChunk; e += kEqThreads)
-      w_s[e] = c0 + e < m ? *reinterpret_cast<const uint4*>(weights + c0 + e) : make_uint4(0, 0, 0, 0);
+    for (int q = threadIdx.x; q < kQuads; q += kEqThreads) {
+      uint4 e[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        e[r] = c0 + 4 * q + r < m ? *reinterpret_cast<const uint4*>(weights + c0 + 4 * q + r) : make_uint4(0, 0, 0, 0);
+      // Word w of the elements holds coefficients 2w (bytes 0, 1) and 2w + 1 (bytes 2, 3).
+      uint32_t pl[4][4];
+      transpose4(e[0].x, e[1].x, e[2].x, e[3].x, pl[0]);
+      transpose4(e[0].y, e[1].y, e[2].y, e[3].y, pl[1]);
+      transpose4(e[0].z, e[1].z, e[2].z, e[3].z, pl[2]);
+      transpose4(e[0].w, e[1].w, e[2].w, e[3].w, pl[3]);
+      // pl[w] = {lo k=2w, hi k=2w, lo k=2w+1, hi k=2w+1}
+      planes_s[q][0] = make_uint4(pl[0][0], pl[0][2], pl[1][0], pl[1][2]);
+      planes_s[q][1] = make_uint4(pl[0][1], pl[0][3], pl[1][1], pl[1][3]);
+      planes_s[q][2] = make_uint4(pl[2][0], pl[2][2], pl[3][0], pl[3][2]);
+      planes_s[q][3] = make_uint4(pl[2][1], pl[2][3], pl[3][1], pl[3][3]);
+    }
     __syncthreads();
     for (int b = 0; b < nb; ++b) {
       const uint64_t bbase = (first_block + b) * block_len;
-      int32_t acc[64];
+      int32_t lo[8][4], hi[8][4];
 #pragma unroll
-      for (int q = 0; q < 64; ++q) acc[q] = 0;
+      for (int jj = 0; jj < 8; ++jj)
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) lo[jj][kk] = hi[jj][kk] = 0;
 #pragma unroll 2
-      for (int u = 0; u < kEqChunk / kEqThreads; ++u) {
-        const int e = threadIdx.x + u * kEqThreads;
-        const uint64_t g = bbase + 8 * (c0 + e);
-        uint2 v8 = make_uint2(0, 0);
-        if (c0 + e < m) {
-          if (g + 8 <= active) {
-            v8 = *reinterpret_cast<const uint2*>(bva + g);
-          } else {
-            uint32_t w[2] = {0, 0};
-            for (int j = 0; j < 8; ++j)
-              if (g + j < active) w[j >> 2] |= uint32_t(uint8_t(bva[g + j])) << (8 * (j & 3));
-            v8 = make_uint2(w[0], w[1]);
+      for (int u = 0; u < kQuads / (kEqThreads / 2); ++u) {
+        const int q = (threadIdx.x >> 1) + u * (kEqThreads / 2);
+        const uint64_t i0 = c0 + 4 * uint64_t(q);
+        const uint64_t g = bbase + 8 * i0;
+        uint32_t x[8];
+        if (i0 + 4 <= m && g + 32 <= active) {
+          const uint4 a = *reinterpret_cast<const uint4*>(bva + g), bq = *reinterpret_cast<const uint4*>(bva + g + 16);
+          x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = bq.x; x[5] = bq.y; x[6] = bq.z; x[7] = bq.w;
+        } else {
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            uint32_t w = 0;
+            for (int y = 0; y < 4; ++y) {
+              const uint64_t gy = g + 4 * r + y;
+              if (i0 + r / 2 < m && gy < active) w |= uint32_t(uint8_t(bva[gy])) << (8 * y);
+            }
+            x[r] = w;
           }
         }
-        const uint4 wq = w_s[e];
-        const uint32_t wc[4] = {wq.x, wq.y, wq.z, wq.w};
+        // vj[jj]: lane jj of the quad's 4 elements (element r's lanes are x[2r], x[2r + 1]).
+        uint32_t v_lo[4], v_hi[4];
+        transpose4(x[0], x[2], x[4], x[6], v_lo);
+        transpose4(x[1], x[3], x[5], x[7], v_hi);
+        const uint4 pl = planes_s[q][2 * h], ph = planes_s[q][2 * h + 1];
+        const uint32_t plo[4] = {pl.x, pl.y, pl.z, pl.w}, phi[4] = {ph.x, ph.y, ph.z, ph.w};
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int v = int(int8_t(((j < 4 ? v8.x : v8.y) >> (8 * (j & 3))) & 0xffu));
+        for (int jj = 0; jj < 8; ++jj) {
+          const uint32_t v = jj < 4 ? v_lo[jj] : v_hi[jj - 4];
 #pragma unroll
-          for (int k = 0; k < 8; ++k) acc[j * 8 + k] += v * int32_t((wc[k >> 1] >> (16 * (k & 1))) & 0xffffu);
+          for (int kk = 0; kk < 4; ++kk) {
+            lo[jj][kk] = dp4a_su(v, plo[kk], lo[jj][kk]);
+            hi[jj][kk] = dp4a_su(v, phi[kk], hi[jj][kk]);
+          }
         }
       }
-      // Reduce-scatter over the warp: after offset o the lane keeps the half
-      // of its entries selected by (lane & o).
+      int32_t acc[32];
 #pragma unroll
-      for (int o = 16, n = 64; o >= 1; o >>= 1, n >>= 1) {
+      for (int f = 0; f < 32; ++f) acc[f] = lo[f >> 2][f & 3] + 256 * hi[f >> 2][f & 3];
+      // Reduce-scatter over the 16 lanes of this coefficient half: after
+      // offset o the lane keeps the half of its entries selected by (lane & o);
+      // it ends with entries (lane & 30) and (lane & 30) + 1.
+#pragma unroll
+      for (int o = 16, n = 32; o >= 2; o >>= 1, n >>= 1) {
         const bool upper = lane & o;
 #pragma unroll
-        for (int q = 0; q < n / 2; ++q) {
-          const int32_t send = upper ? acc[q] : acc[q + n / 2];
-          const int32_t keep = upper ? acc[q + n / 2] : acc[q];
-          acc[q] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        for (int qq = 0; qq < n / 2; ++qq) {
+          const int32_t send = upper ? acc[qq] : acc[qq + n / 2];
+          const int32_t keep = upper ? acc[qq + n / 2] : acc[qq];
+          acc[qq] = keep + __shfl_xor_sync(0xffffffffu, send, o);
         }
       }
-      stage_s[warp][2 * lane] = acc[0];
-      stage_s[warp][2 * lane + 1] = acc[1];
+#pragma unroll
+      for (int qq = 0; qq < 2; ++qq) {
+        const int f = (lane & 30) + qq;  // entry f: lane j = f / 4, coefficient 4h + f % 4
+        stage_s[warp][(f >> 2) * 8 + 4 * h + (f & 3)] = acc[qq];
+      }
       __syncthreads();
       if (threadIdx.x < 64) {
         long long t = 0;
@@ -281,6 +455,39 @@ __global__ void k_block_fold(const int8_t* __restrict__ bva, uint64_t active, ui
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < m; i += uint64_t(gridDim.x) * blockDim.x) {
     int32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (blocks <= 8) {
+      // Up to 8 blocks: every block's 8 weights are loaded before any is used.
+      uint2 v8[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const uint64_t g = uint64_t(b) * block_len + 8 * i;
+        v8[b] = make_uint2(0, 0);
+        if (b < blocks && g + 8 <= active) {
+          v8[b] = *reinterpret_cast<const uint2*>(bva + g);
+        } else if (b < blocks && g < active) {
+          uint32_t w[2] = {0, 0};
+          for (int j = 0; j < 8; ++j)
+            if (g + j < active) w[j >> 2] |= uint32_t(uint8_t(bva[g + j])) << (8 * (j & 3));
+          v8[b] = make_uint2(w[0], w[1]);
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        if (b >= blocks) break;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const uint4 pl = planes[b * 8 + k];
+          const int32_t lo = dp4a_su(v8[b].y, pl.y, dp4a_su(v8[b].x, pl.x, 0));
+          const int32_t hi = dp4a_su(v8[b].y, pl.w, dp4a_su(v8[b].x, pl.z, 0));
+          acc[k] += lo + hi * 256;
+        }
+      }
+      Fr o;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) o.c[k] = mod_i32(acc[k]);
+      store(values + i, accumulate ? add(load(values + i), o) : o);
+      continue;
+    }
     for (int b = 0; b < blocks; ++b) {
       if (b && (b & 7) == 0)
 #pragma unroll
