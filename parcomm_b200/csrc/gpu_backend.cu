@@ -535,10 +535,11 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
 }
 
 // Inner levels of a row tree over the n_leaves digests at tree[0..): level j
-// at digest offset level_off[j], the root last.  Launches of three levels
-// per thread (k_hash_subtrees: each thread hashes an 8-child subtree, no
-// barrier) while the level they reach keeps at least 2^11 nodes, then one CTA
-// for the levels above (k_hash_top): 5 launches for 2^23 leaves instead of 23.
+// at digest offset level_off[j], the root last.  Launches of two levels per
+// thread (k_hash_subtrees: each thread hashes a 4-child subtree, no barrier;
+// three levels measured slower, their registers cost occupancy) while the
+// level they reach keeps at least 2^11 nodes, then one CTA for the levels
+// above (k_hash_top): 7 launches for 2^23 leaves instead of 23.
 static void build_tree(cudaStream_t s, uint4* tree, uint64_t n_leaves, std::vector<uint64_t>& level_off, bool timed) {
   level_off.clear();
   for (uint64_t k = n_leaves, off = 0;; k /= 2) {
@@ -551,17 +552,14 @@ static void build_tree(cudaStream_t s, uint4* tree, uint64_t n_leaves, std::vect
   size_t j = 0;
   uint64_t n = n_leaves;
   while (n > (uint64_t(1) << kTopLog)) {
-    const int L = std::min(3, ilog2(n) - kTopLog);
+    const int L = std::min(2, ilog2(n) - kTopLog);
     qfd::TreeLevels lv{};
     for (int t = 0; t <= L; ++t) lv.off[t] = level_off[j + t];
     const uint64_t top = n >> L;
     const unsigned grid = unsigned((top + kThreads - 1) / kThreads);
     launch(s, timed, "k_hash_inner", n * 32 + (n - top) * 32, qf_intops::inner_hash_ops(n - top), [&] {
-      switch (L) {
-        case 1: qfd::k_hash_subtrees<1><<<grid, kThreads, 0, s>>>(tree, top, lv, ip); break;
-        case 2: qfd::k_hash_subtrees<2><<<grid, kThreads, 0, s>>>(tree, top, lv, ip); break;
-        default: qfd::k_hash_subtrees<3><<<grid, kThreads, 0, s>>>(tree, top, lv, ip); break;
-      }
+      if (L == 1) qfd::k_hash_subtrees<1><<<grid, kThreads, 0, s>>>(tree, top, lv, ip);
+      else qfd::k_hash_subtrees<2><<<grid, kThreads, 0, s>>>(tree, top, lv, ip);
     });
     j += L;
     n = top;
