@@ -271,6 +271,269 @@ __device__ __forceinline__ void tile_loop(uint32_t* planes, int log_n, int b0, u
 }
 
 
+// ---------------------------------------------------------------- element-major tiles
+// The transform passes over full 4096-element tiles.  A thread holds whole
+// elements (all coefficients, lazily reduced 32-bit values) in registers and
+// applies up to three levels to a group of 2^R elements that differ in one
+// window of R tile bits; the groups of the next window are formed through
+// shared memory.  Shared memory holds the tile element-major: element e's
+// coefficients as kUnits 16-byte units, so a thread moves an element with
+// kUnits 128-bit accesses.  Unit (e, h) sits at tunit(e, 0) ^ h with
+// tunit(e, 0) = (kUnits * e) ^ swz(e), swz XOR-linear in e (F65521: bit 0 =
+// e2 ^ e3 ^ e5, bit 1 = e4, bit 2 = e5; KoalaBear: the bits e3..e5).  The
+// eight lanes of every 128-bit access phase then hit eight distinct 16-byte
+// bank groups for every window the passes use (a simulation of the warps'
+// accesses checks [9,12), [0,3), [3,6), [6,9), [2,5), [5,7), [7,9) and the
+// windows of the other strided depths).
+//
+// A pass over tile bits [b0, 12) runs its first window on bits 9..11: a
+// thread owns elements g + (j << 9), so consecutive threads load consecutive
+// elements.  The remaining bits [b0, 9) are split into windows of at most
+// three bits, and the highest window runs last: its groups enumerate tile
+// bits 0..4 across the lanes, so the stores are coalesced too.
+constexpr int kUnits = kC / 4;
+constexpr int kTile = 1 << kMaxTileLog;
+__device__ __forceinline__ int tunit(int e) {
+  if constexpr (kUnits == 2) return (2 * e) ^ ((((e >> 2) ^ (e >> 3) ^ (e >> 5)) & 1) | ((e >> 3) & 6));
+  else return e ^ ((e >> 3) & 7);
+}
+
+// Windows of tile bits [b0, 9): at most three bits each, lowest first.
+struct Windows {
+  int n;
+  int b[3], r[3];
+};
+__device__ __forceinline__ Windows windows_below9(int b0) {
+  Windows w{};
+  const int span = 9 - b0;
+  w.n = (span + 2) / 3;
+  int b = b0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    const int left = 9 - b, parts = w.n - i;
+    const int r = parts > 0 ? (left + parts - 1) / parts : 0;
+    w.b[i] = b;
+    w.r[i] = r;
+    b += r;
+  }
+  return w;
+}
+
+// Group g of a window [b, b + R): the elements base + (j << b).
+__device__ __forceinline__ int group_base(int g, int b, int R) {
+  return (g & ((1 << b) - 1)) | ((g >> b) << (b + R));
+}
+template <int R>
+__device__ __forceinline__ void group_get(const uint4* t, int base, const int (&off)[1 << R], uint32_t (&v)[1 << R][kC]) {
+  const int u0 = tunit(base);
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+#pragma unroll
+    for (int h = 0; h < kUnits; ++h) {
+      const uint4 u = t[(u0 ^ off[j]) ^ h];
+      v[j][4 * h] = u.x;
+      v[j][4 * h + 1] = u.y;
+      v[j][4 * h + 2] = u.z;
+      v[j][4 * h + 3] = u.w;
+    }
+}
+template <int R>
+__device__ __forceinline__ void group_put(uint4* t, int base, const int (&off)[1 << R], const uint32_t (&v)[1 << R][kC]) {
+  const int u0 = tunit(base);
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j)
+#pragma unroll
+    for (int h = 0; h < kUnits; ++h)
+      t[(u0 ^ off[j]) ^ h] = make_uint4(v[j][4 * h], v[j][4 * h + 1], v[j][4 * h + 2], v[j][4 * h + 3]);
+}
+template <int R>
+__device__ __forceinline__ void window_offsets(int b, int (&off)[1 << R]) {
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) off[j] = tunit(j << b);
+}
+
+// One window of OP through shared memory (in place: a group is read and
+// written by one thread), then a barrier.
+template <int OP, int R>
+__device__ __forceinline__ void window_stage(uint4* t, int b, int lvl) {
+  int off[1 << R];
+  window_offsets<R>(b, off);
+  for (int g = threadIdx.x; g < (kTile >> R); g += blockDim.x) {
+    const int base = group_base(g, b, R);
+    uint32_t v[1 << R][kC];
+    group_get<R>(t, base, off, v);
+    reg_levels<OP, R>(v, lvl);
+    group_put<R>(t, base, off, v);
+  }
+  __syncthreads();
+}
+template <int OP>
+__device__ __forceinline__ void window_stage_r(uint4* t, int b, int r, int lvl) {
+  if (r == 3) window_stage<OP, 3>(t, b, lvl);
+  else if (r == 2) window_stage<OP, 2>(t, b, lvl);
+  else window_stage<OP, 1>(t, b, lvl);
+}
+
+// The last window of a pass: OP's levels, reduction to canonical form,
+// fin(e, Fr&) on each element (a store to HBM, or the step between two
+// transforms), and (PUT) the result back into the tile.
+template <int OP, int R, bool PUT, class Fin>
+__device__ __forceinline__ void window_last(uint4* t, int b, int lvl, Fin fin) {
+  int off[1 << R];
+  window_offsets<R>(b, off);
+  for (int g = threadIdx.x; g < (kTile >> R); g += blockDim.x) {
+    const int base = group_base(g, b, R);
+    uint32_t v[1 << R][kC];
+    group_get<R>(t, base, off, v);
+    reg_levels<OP, R>(v, lvl);
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      Fr w;
+#pragma unroll
+      for (int c = 0; c < kC; ++c) w.c[c] = tile_final(v[j][c]);
+      fin(base + (j << b), w);
+#pragma unroll
+      for (int c = 0; c < kC; ++c) v[j][c] = w.c[c];
+    }
+    if (PUT) group_put<R>(t, base, off, v);
+  }
+}
+template <int OP, bool PUT, class Fin>
+__device__ __forceinline__ void window_last_r(uint4* t, int b, int r, int lvl, Fin fin) {
+  if (r == 3) window_last<OP, 3, PUT>(t, b, lvl, fin);
+  else if (r == 2) window_last<OP, 2, PUT>(t, b, lvl, fin);
+  else window_last<OP, 1, PUT>(t, b, lvl, fin);
+}
+
+// The window where a fused pass changes transforms: OP1's levels, reduction,
+// step(e, Fr&) on each canonical element, OP2's first levels, back into the tile.
+template <int OP1, int OP2, int R, class Step>
+__device__ __forceinline__ void window_mid(uint4* t, int b, int lvl, Step step) {
+  int off[1 << R];
+  window_offsets<R>(b, off);
+  for (int g = threadIdx.x; g < (kTile >> R); g += blockDim.x) {
+    const int base = group_base(g, b, R);
+    uint32_t v[1 << R][kC];
+    group_get<R>(t, base, off, v);
+    reg_levels<OP1, R>(v, lvl);
+#pragma unroll
+    for (int j = 0; j < (1 << R); ++j) {
+      Fr x;
+#pragma unroll
+      for (int c = 0; c < kC; ++c) x.c[c] = tile_final(v[j][c]);
+      step(base + (j << b), x);
+#pragma unroll
+      for (int c = 0; c < kC; ++c) v[j][c] = x.c[c];
+    }
+    reg_levels<OP2, R>(v, 0);
+    group_put<R>(t, base, off, v);
+  }
+}
+template <int OP1, int OP2, class Step>
+__device__ __forceinline__ void window_mid_r(uint4* t, int b, int r, int lvl, Step step) {
+  if (r == 3) window_mid<OP1, OP2, 3>(t, b, lvl, step);
+  else if (r == 2) window_mid<OP1, OP2, 2>(t, b, lvl, step);
+  else window_mid<OP1, OP2, 1>(t, b, lvl, step);
+}
+
+// A pass of OP1 over tile bits [b0, 12) of full tiles (b0 <= 9, 512
+// threads), and, when FUSED (b0 <= 6), a step and a second transform OP2 on
+// the same bits in the same trip through HBM:
+//   fetch(tile, e) -> Raw and conv(tile, e, Raw) -> Fr read element e;
+//   stage(tile) runs first in each tile (it issues cp.async side loads, waited
+//   for before the first barrier);
+//   single pass: st(tile, e, uint4) stores element e (reduced, packed);
+//   fused pass: mid(tile, e, Fr&) runs on each canonical element after OP1,
+//   then OP2 and st.
+// The next tile's loads are issued after the first window (single) or after
+// the step (fused), so their registers are not live across the step.
+template <int OP1, int OP2, bool FUSED, class Raw, class Fetch, class Conv, class Stage, class Mid, class St>
+__device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles, Fetch fetch, Conv conv, Stage stage,
+                                             Mid mid, St st) {
+  const int g = threadIdx.x;
+  const Windows w = windows_below9(b0);
+  int off9[8];
+  window_offsets<3>(9, off9);
+  Raw raw[8];
+  uint32_t tile = blockIdx.x;
+  if (tile < n_tiles)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+  for (; tile < n_tiles; tile += gridDim.x) {
+    stage(tile);
+    const uint32_t next = tile + gridDim.x;
+    {
+      uint32_t v[8][kC];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const Fr e = conv(tile, g + (j << 9), raw[j]);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
+      }
+      reg_levels<OP1, 3>(v, 0);
+      if (w.n == 0 && !FUSED) {  // three levels: the first window is the last
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          Fr o;
+#pragma unroll
+          for (int c = 0; c < kC; ++c) o.c[c] = tile_final(v[j][c]);
+          st(tile, g + (j << 9), pack_fe(o));
+        }
+      } else {
+        group_put<3>(t, g, off9, v);
+      }
+    }
+    if (!FUSED && next < n_tiles)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
+    if (w.n == 0 && !FUSED) continue;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();
+    int lvl = 3;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      if (i + 1 < w.n) {
+        window_stage_r<OP1>(t, w.b[i], w.r[i], lvl);
+        lvl += w.r[i];
+      }
+    const int bl = w.n == 3 ? w.b[2] : (w.n == 2 ? w.b[1] : w.b[0]);
+    const int rl = w.n == 3 ? w.r[2] : (w.n == 2 ? w.r[1] : w.r[0]);
+    if (!FUSED) {
+      window_last_r<OP1, false>(t, bl, rl, lvl, [&](int e, Fr& v) { st(tile, e, pack_fe(v)); });
+      __syncthreads();  // the next tile's first window overwrites the tile
+      continue;
+    }
+    // Fused: OP1's last window, the step, and OP2's levels on the same
+    // window in registers.
+    window_mid_r<OP1, OP2>(t, bl, rl, lvl, [&](int e, Fr& v) { mid(tile, e, v); });
+    if (next < n_tiles)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
+    __syncthreads();
+    int lvl2 = rl;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+      if (i + 1 < w.n) {
+        window_stage_r<OP2>(t, w.b[i], w.r[i], lvl2);
+        lvl2 += w.r[i];
+      }
+    // OP2's last window: bits 9..11, the elements g + (j << 9), stored.
+    {
+      uint32_t v[8][kC];
+      group_get<3>(t, g, off9, v);
+      reg_levels<OP2, 3>(v, lvl2);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        Fr o;
+#pragma unroll
+        for (int c = 0; c < kC; ++c) o.c[c] = tile_final(v[j][c]);
+        st(tile, g + (j << 9), pack_fe(o));
+      }
+    }
+    __syncthreads();  // the next tile's first window overwrites the tile
+  }
+}
+
 // Pack eight signed weights per element, then Mobius levels [0, levels) in
 // tiles of 2^levels elements; write into the message half.  `src_base` is
 // the block's first BVA index.
@@ -293,6 +556,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const Wt* 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + msg_addr32((tile << levels) + uint32_t(t), logR)) = u;
   };
+  if (levels == kMaxTileLog) {
+    tile_pass_v2<kMobius, kMobius, false, uint2>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv,
+                                                 [](uint32_t) {}, [](uint32_t, int, Fr&) {}, st);
+    return;
+  }
   tile_loop<kMobius, uint2>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
@@ -306,6 +574,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + msg_addr32((tile << levels) + uint32_t(t), logR)) = u;
   };
+  if (levels == kMaxTileLog) {
+    tile_pass_v2<kMobius, kMobius, false, uint4>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv,
+                                                 [](uint32_t) {}, [](uint32_t, int, Fr&) {}, st);
+    return;
+  }
   tile_loop<kMobius, uint4>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
@@ -357,6 +630,11 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(const Fe*
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(dst + strided_addr(tile, t, logR, lo, k, cb)) = u;
   };
+  if (cb + k == kMaxTileLog && cb <= 9) {
+    tile_pass_v2<OP, OP, false, uint4>(reinterpret_cast<uint4*>(planes_s), cb, n_tiles, fetch, conv, [](uint32_t) {},
+                                       [](uint32_t, int, Fr&) {}, st);
+    return;
+  }
   tile_loop<OP, uint4>(planes_s, cb + k, cb, n_tiles, fetch, conv, st);
 }
 
@@ -368,101 +646,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(const Fe*
 // Mobius levels on bits [lo, lo + k) and then the first WHT's levels on the
 // same bits, or the first WHT's last levels, the alpha product and the second
 // WHT's first levels.
-
-// Registers -> planes: v[j] is tile element base + (j << zb).
-template <int R>
-__device__ __forceinline__ void regs_to_planes(uint32_t* planes, int base, int zb, const uint32_t (&v)[1 << R][kC]) {
-  const int pb = pidx(base);
-#pragma unroll
-  for (int j = 0; j < (1 << R); ++j) {
-    const int q = pb ^ pidx(j << zb);
-#pragma unroll
-    for (int c = 0; c < kC; ++c) planes[c * kPlane + q] = v[j][c];
-  }
-}
-
-// Planar levels on tile bits [b0, 6) of a full tile (the levels between a
-// register head on bits 9..11 and a register tail on bits 6..8), lvl0 the
-// first level's lazy index.  A radix-4 stage on bits 4..5 takes its groups
-// with bits 4 and 5 swapped (conflict-free banks, see tile_loop).
-template <int OP>
-__device__ __forceinline__ void fused_middle(uint32_t* planes, int b0, int lvl0) {
-  if (b0 == 4) planar_stage<OP, 2, true>(planes, kMaxTileLog, 4, lvl0);
-  else planar_levels<OP>(planes, kMaxTileLog, b0, 6 - b0, lvl0);
-}
-
-// Runs OP1 on tile bits [b0, 12) of full 4096-element tiles, then for each
-// element mid(tile, t, Fr& v) on its canonical value, then OP2 on the same
-// bits, then st(tile, t, uint4).  512 threads, 6 >= b0 >= 0.  OP1: register
-// head on bits 9..11, planar levels on [b0, 6), register tail on bits 6..8;
-// mid on the tail's registers; OP2: register levels on bits 6..8 right
-// there, planar levels on [b0, 6), register tail on bits 9..11 and the
-// stores (consecutive threads take consecutive elements, as the loads).
-// stage(tile) runs first in each tile (to issue its cp.async side loads,
-// which each thread then waits for before the first planar stage's barrier).
-// The next tile's loads are issued after mid, so their registers are not live
-// across it.
-template <int OP1, int OP2, class Raw, class Fetch, class Conv, class Stage, class Mid, class St>
-__device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32_t n_tiles, Fetch fetch, Conv conv,
-                                                Stage stage, Mid mid, St st) {
-  const int g = threadIdx.x;
-  const int rm = 6 - b0;
-  const int tb = (g & 63) | ((g >> 6) << 9);  // the tail group: elements tb + (j << 6)
-  Raw raw[8];
-  uint32_t tile = blockIdx.x;
-  if (tile < n_tiles)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
-  for (; tile < n_tiles; tile += gridDim.x) {
-    stage(tile);
-    {
-      uint32_t v[8][kC];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const Fr e = conv(tile, g + (j << 9), raw[j]);
-#pragma unroll
-        for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
-      }
-      head_levels<OP1>(planes, v);
-    }
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    if (rm > 0) fused_middle<OP1>(planes, b0, 3);
-    else __syncthreads();
-    {
-      uint32_t v[8][kC];
-      const int pb = pidx(tb);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int q = pb ^ pidx(j << 6);
-#pragma unroll
-        for (int c = 0; c < kC; ++c) v[j][c] = planes[c * kPlane + q];
-      }
-      reg_levels<OP1, 3>(v, 3 + rm);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        Fr w;
-#pragma unroll
-        for (int c = 0; c < kC; ++c) w.c[c] = tile_final(v[j][c]);
-        mid(tile, tb + (j << 6), w);
-#pragma unroll
-        for (int c = 0; c < kC; ++c) v[j][c] = w.c[c];
-      }
-      reg_levels<OP2, 3>(v, 0);
-      // The same thread read these positions: no other thread touches them
-      // until the barrier below.
-      regs_to_planes<3>(planes, tb, 6, v);
-    }
-    const uint32_t next = tile + gridDim.x;
-    if (next < n_tiles)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
-    __syncthreads();
-    if (rm > 0) fused_middle<OP2>(planes, b0, 3);
-    auto st_t = [&](int t, uint4 u) { st(tile, t, u); };
-    pass_tail<OP2, 3>(planes, 9, 3 + rm, st_t);
-    __syncthreads();  // the next head overwrites the planes
-  }
-}
 
 // Message half at cw: Mobius levels [lo, lo + k) (the message is final after
 // them), stored back; then the first WHT's levels [lo, lo + k) of the same
@@ -482,7 +665,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_mobius_wht_strided(Fe* cw, 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + R + strided_addr(tile, t, logR, lo, k, cb)) = u;
   };
-  tile_loop_fused<kMobius, kWht, uint4>(planes_s, cb, n_tiles, fetch, conv, stage, mid, st);
+  tile_pass_v2<kMobius, kWht, true, uint4>(reinterpret_cast<uint4*>(planes_s), cb, n_tiles, fetch, conv, stage, mid, st);
 }
 
 // The parity tile pass: the first WHT's levels 0..11 of each column (read at
@@ -512,7 +695,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_wht_alpha_wht_tile(const Fe
   };
   auto mid = [=](uint32_t, int t, Fr& v) { v = mul(v, unpack_fe(alpha_s[t])); };
   auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(dst + addr(tile, t)) = u; };
-  tile_loop_fused<kWht, kWht, uint4>(planes_s, 0, n_tiles, fetch, conv, stage, mid, st);
+  tile_pass_v2<kWht, kWht, true, uint4>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv, stage, mid, st);
 }
 
 // ---------------------------------------------------------------- hashing

@@ -171,41 +171,48 @@ __global__ void __launch_bounds__(kTermThreads) k_project_terms16(const int8_t* 
     for (int l = 0; l < 8; ++l)
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk) lo[l][kk] = hi[l][kk] = 0;
-    for (int r0 = 4 * grp; r0 < nrows; r0 += 4 * kGroups) {
-      uint32_t x[8], y[8];
+    // Two groups of 4 rows per iteration, all their loads issued first.
+    for (int r0 = 4 * grp; r0 < nrows; r0 += 8 * kGroups) {
+      uint32_t x[2][8], y[2][8];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const uint64_t g = T.offset + (row0 + r0 + r) * 16 + 8 * lh;
-        uint2 u = make_uint2(0, 0), w = make_uint2(0, 0);
-        if (r0 + r < nrows) {
-          w = reinterpret_cast<const uint2*>(lot + r0 + r)[h];
-          if (g + 8 <= active) {
-            u = *reinterpret_cast<const uint2*>(bva + g);
-          } else {
-            uint32_t b[2] = {0, 0};
-            for (int y2 = 0; y2 < 8; ++y2)
-              if (g + y2 < active) b[y2 >> 2] |= uint32_t(uint8_t(bva[g + y2])) << (8 * (y2 & 3));
-            u = make_uint2(b[0], b[1]);
+      for (int q = 0; q < 2; ++q)
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int rr = r0 + q * 4 * kGroups + r;
+          const uint64_t g = T.offset + (row0 + rr) * 16 + 8 * lh;
+          uint2 u = make_uint2(0, 0), w = make_uint2(0, 0);
+          if (rr < nrows) {
+            w = reinterpret_cast<const uint2*>(lot + rr)[h];
+            if (g + 8 <= active) {
+              u = *reinterpret_cast<const uint2*>(bva + g);
+            } else {
+              uint32_t b[2] = {0, 0};
+              for (int y2 = 0; y2 < 8; ++y2)
+                if (g + y2 < active) b[y2 >> 2] |= uint32_t(uint8_t(bva[g + y2])) << (8 * (y2 & 3));
+              u = make_uint2(b[0], b[1]);
+            }
           }
+          x[q][2 * r] = u.x;
+          x[q][2 * r + 1] = u.y;
+          y[q][2 * r] = w.x;
+          y[q][2 * r + 1] = w.y;
         }
-        x[2 * r] = u.x;
-        x[2 * r + 1] = u.y;
-        y[2 * r] = w.x;
-        y[2 * r + 1] = w.y;
-      }
-      uint32_t va[4], vb[4], pa[4], pb[4];
-      transpose4(x[0], x[2], x[4], x[6], va);  // lanes 8 lh + 0..3
-      transpose4(x[1], x[3], x[5], x[7], vb);  // lanes 8 lh + 4..7
-      transpose4(y[0], y[2], y[4], y[6], pa);  // {lo, hi} of coefficients 4h, 4h + 1
-      transpose4(y[1], y[3], y[5], y[7], pb);  // {lo, hi} of coefficients 4h + 2, 4h + 3
-      const uint32_t plo[4] = {pa[0], pa[2], pb[0], pb[2]}, phi[4] = {pa[1], pa[3], pb[1], pb[3]};
 #pragma unroll
-      for (int l = 0; l < 8; ++l) {
-        const uint32_t v = l < 4 ? va[l] : vb[l - 4];
+      for (int q = 0; q < 2; ++q) {
+        uint32_t va[4], vb[4], pa[4], pb[4];
+        transpose4(x[q][0], x[q][2], x[q][4], x[q][6], va);  // lanes 8 lh + 0..3
+        transpose4(x[q][1], x[q][3], x[q][5], x[q][7], vb);  // lanes 8 lh + 4..7
+        transpose4(y[q][0], y[q][2], y[q][4], y[q][6], pa);  // {lo, hi} of coefficients 4h, 4h + 1
+        transpose4(y[q][1], y[q][3], y[q][5], y[q][7], pb);  // {lo, hi} of coefficients 4h + 2, 4h + 3
+        const uint32_t plo[4] = {pa[0], pa[2], pb[0], pb[2]}, phi[4] = {pa[1], pa[3], pb[1], pb[3]};
 #pragma unroll
-        for (int kk = 0; kk < 4; ++kk) {
-          lo[l][kk] = dp4a_su(v, plo[kk], lo[l][kk]);
-          hi[l][kk] = dp4a_su(v, phi[kk], hi[l][kk]);
+        for (int l = 0; l < 8; ++l) {
+          const uint32_t v = l < 4 ? va[l] : vb[l - 4];
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            lo[l][kk] = dp4a_su(v, plo[kk], lo[l][kk]);
+            hi[l][kk] = dp4a_su(v, phi[kk], hi[l][kk]);
+          }
         }
       }
     }
@@ -348,10 +355,13 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
       transpose4(e[0].z, e[1].z, e[2].z, e[3].z, pl[2]);
       transpose4(e[0].w, e[1].w, e[2].w, e[3].w, pl[3]);
       // pl[w] = {lo k=2w, hi k=2w, lo k=2w+1, hi k=2w+1}
-      planes_s[q][0] = make_uint4(pl[0][0], pl[0][2], pl[1][0], pl[1][2]);
-      planes_s[q][1] = make_uint4(pl[0][1], pl[0][3], pl[1][1], pl[1][3]);
-      planes_s[q][2] = make_uint4(pl[2][0], pl[2][2], pl[3][0], pl[3][2]);
-      planes_s[q][3] = make_uint4(pl[2][1], pl[2][3], pl[3][1], pl[3][3]);
+      // Group g of quad q sits in slot g ^ ((q >> 1) & 1): a warp phase of 4
+      // quads x 2 coefficient halves then reads 8 distinct bank groups.
+      const int sw = (q >> 1) & 1;
+      planes_s[q][0 ^ sw] = make_uint4(pl[0][0], pl[0][2], pl[1][0], pl[1][2]);
+      planes_s[q][1 ^ sw] = make_uint4(pl[0][1], pl[0][3], pl[1][1], pl[1][3]);
+      planes_s[q][2 ^ sw] = make_uint4(pl[2][0], pl[2][2], pl[3][0], pl[3][2]);
+      planes_s[q][3 ^ sw] = make_uint4(pl[2][1], pl[2][3], pl[3][1], pl[3][3]);
     }
     __syncthreads();
     for (int b = 0; b < nb; ++b) {
@@ -385,7 +395,8 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
         uint32_t v_lo[4], v_hi[4];
         transpose4(x[0], x[2], x[4], x[6], v_lo);
         transpose4(x[1], x[3], x[5], x[7], v_hi);
-        const uint4 pl = planes_s[q][2 * h], ph = planes_s[q][2 * h + 1];
+        const int sw = (q >> 1) & 1;
+        const uint4 pl = planes_s[q][(2 * h) ^ sw], ph = planes_s[q][(2 * h + 1) ^ sw];
         const uint32_t plo[4] = {pl.x, pl.y, pl.z, pl.w}, phi[4] = {ph.x, ph.y, ph.z, ph.w};
 #pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
