@@ -447,7 +447,8 @@ __device__ __forceinline__ void window_mid_r(uint4* t, int b, int r, int lvl, St
 //   then OP2 and st.
 // The next tile's loads are issued after the first window (single) or after
 // the step (fused), so their registers are not live across the step.
-template <int OP1, int OP2, bool FUSED, class Raw, class Fetch, class Conv, class Stage, class Mid, class St>
+template <int OP1, int OP2, bool FUSED, bool PREFETCH, class Raw, class Fetch, class Conv, class Stage, class Mid,
+          class St>
 __device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles, Fetch fetch, Conv conv, Stage stage,
                                              Mid mid, St st) {
   const int g = threadIdx.x;
@@ -456,12 +457,15 @@ __device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles,
   window_offsets<3>(9, off9);
   Raw raw[8];
   uint32_t tile = blockIdx.x;
-  if (tile < n_tiles)
+  if (PREFETCH && tile < n_tiles)
 #pragma unroll
     for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
   for (; tile < n_tiles; tile += gridDim.x) {
     stage(tile);
     const uint32_t next = tile + gridDim.x;
+    if (!PREFETCH)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
     {
       uint32_t v[8][kC];
 #pragma unroll
@@ -483,7 +487,7 @@ __device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles,
         group_put<3>(t, g, off9, v);
       }
     }
-    if (!FUSED && next < n_tiles)
+    if (PREFETCH && !FUSED && next < n_tiles)
 #pragma unroll
       for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
     if (w.n == 0 && !FUSED) continue;
@@ -506,7 +510,7 @@ __device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles,
     // Fused: OP1's last window, the step, and OP2's levels on the same
     // window in registers.
     window_mid_r<OP1, OP2>(t, bl, rl, lvl, [&](int e, Fr& v) { mid(tile, e, v); });
-    if (next < n_tiles)
+    if (PREFETCH && next < n_tiles)
 #pragma unroll
       for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
     __syncthreads();
@@ -556,11 +560,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_pack_mobius_tile(const Wt* 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + msg_addr32((tile << levels) + uint32_t(t), logR)) = u;
   };
-  if (levels == kMaxTileLog) {
-    tile_pass_v2<kMobius, kMobius, false, uint2>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv,
-                                                 [](uint32_t) {}, [](uint32_t, int, Fr&) {}, st);
-    return;
-  }
   tile_loop<kMobius, uint2>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
@@ -574,11 +573,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_copy_mobius_tile(const Fe* 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + msg_addr32((tile << levels) + uint32_t(t), logR)) = u;
   };
-  if (levels == kMaxTileLog) {
-    tile_pass_v2<kMobius, kMobius, false, uint4>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv,
-                                                 [](uint32_t) {}, [](uint32_t, int, Fr&) {}, st);
-    return;
-  }
   tile_loop<kMobius, uint4>(planes_s, levels, 0, n_tiles, fetch, conv, st);
 }
 
@@ -630,11 +624,6 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(const Fe*
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(dst + strided_addr(tile, t, logR, lo, k, cb)) = u;
   };
-  if (cb + k == kMaxTileLog && cb <= 9) {
-    tile_pass_v2<OP, OP, false, uint4>(reinterpret_cast<uint4*>(planes_s), cb, n_tiles, fetch, conv, [](uint32_t) {},
-                                       [](uint32_t, int, Fr&) {}, st);
-    return;
-  }
   tile_loop<OP, uint4>(planes_s, cb + k, cb, n_tiles, fetch, conv, st);
 }
 
@@ -646,6 +635,101 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_butterfly_strided(const Fe*
 // Mobius levels on bits [lo, lo + k) and then the first WHT's levels on the
 // same bits, or the first WHT's last levels, the alpha product and the second
 // WHT's first levels.
+
+// Registers -> planes: v[j] is tile element base + (j << zb).
+template <int R>
+__device__ __forceinline__ void regs_to_planes(uint32_t* planes, int base, int zb, const uint32_t (&v)[1 << R][kC]) {
+  const int pb = pidx(base);
+#pragma unroll
+  for (int j = 0; j < (1 << R); ++j) {
+    const int q = pb ^ pidx(j << zb);
+#pragma unroll
+    for (int c = 0; c < kC; ++c) planes[c * kPlane + q] = v[j][c];
+  }
+}
+
+// Planar levels on tile bits [b0, 6) of a full tile (the levels between a
+// register head on bits 9..11 and a register tail on bits 6..8), lvl0 the
+// first level's lazy index.  A radix-4 stage on bits 4..5 takes its groups
+// with bits 4 and 5 swapped (conflict-free banks, see tile_loop).
+template <int OP>
+__device__ __forceinline__ void fused_middle(uint32_t* planes, int b0, int lvl0) {
+  if (b0 == 4) planar_stage<OP, 2, true>(planes, kMaxTileLog, 4, lvl0);
+  else planar_levels<OP>(planes, kMaxTileLog, b0, 6 - b0, lvl0);
+}
+
+// Runs OP1 on tile bits [b0, 12) of full 4096-element tiles, then for each
+// element mid(tile, t, Fr& v) on its canonical value, then OP2 on the same
+// bits, then st(tile, t, uint4).  512 threads, 6 >= b0 >= 0.  OP1: register
+// head on bits 9..11, planar levels on [b0, 6), register tail on bits 6..8;
+// mid on the tail's registers; OP2: register levels on bits 6..8 right
+// there, planar levels on [b0, 6), register tail on bits 9..11 and the
+// stores (consecutive threads take consecutive elements, as the loads).
+// stage(tile) runs first in each tile (to issue its cp.async side loads,
+// which each thread then waits for before the first planar stage's barrier).
+// The next tile's loads are issued after mid, so their registers are not live
+// across it.
+template <int OP1, int OP2, class Raw, class Fetch, class Conv, class Stage, class Mid, class St>
+__device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32_t n_tiles, Fetch fetch, Conv conv,
+                                                Stage stage, Mid mid, St st) {
+  const int g = threadIdx.x;
+  const int rm = 6 - b0;
+  const int tb = (g & 63) | ((g >> 6) << 9);  // the tail group: elements tb + (j << 6)
+  Raw raw[8];
+  uint32_t tile = blockIdx.x;
+  if (tile < n_tiles)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+  for (; tile < n_tiles; tile += gridDim.x) {
+    stage(tile);
+    {
+      uint32_t v[8][kC];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const Fr e = conv(tile, g + (j << 9), raw[j]);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
+      }
+      head_levels<OP1>(planes, v);
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    if (rm > 0) fused_middle<OP1>(planes, b0, 3);
+    else __syncthreads();
+    {
+      uint32_t v[8][kC];
+      const int pb = pidx(tb);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int q = pb ^ pidx(j << 6);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = planes[c * kPlane + q];
+      }
+      reg_levels<OP1, 3>(v, 3 + rm);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        Fr w;
+#pragma unroll
+        for (int c = 0; c < kC; ++c) w.c[c] = tile_final(v[j][c]);
+        mid(tile, tb + (j << 6), w);
+#pragma unroll
+        for (int c = 0; c < kC; ++c) v[j][c] = w.c[c];
+      }
+      reg_levels<OP2, 3>(v, 0);
+      // The same thread read these positions: no other thread touches them
+      // until the barrier below.
+      regs_to_planes<3>(planes, tb, 6, v);
+    }
+    const uint32_t next = tile + gridDim.x;
+    if (next < n_tiles)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
+    __syncthreads();
+    if (rm > 0) fused_middle<OP2>(planes, b0, 3);
+    auto st_t = [&](int t, uint4 u) { st(tile, t, u); };
+    pass_tail<OP2, 3>(planes, 9, 3 + rm, st_t);
+    __syncthreads();  // the next head overwrites the planes
+  }
+}
 
 // Message half at cw: Mobius levels [lo, lo + k) (the message is final after
 // them), stored back; then the first WHT's levels [lo, lo + k) of the same
@@ -665,7 +749,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_mobius_wht_strided(Fe* cw, 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + R + strided_addr(tile, t, logR, lo, k, cb)) = u;
   };
-  tile_pass_v2<kMobius, kWht, true, uint4>(reinterpret_cast<uint4*>(planes_s), cb, n_tiles, fetch, conv, stage, mid, st);
+  tile_loop_fused<kMobius, kWht, uint4>(planes_s, cb, n_tiles, fetch, conv, stage, mid, st);
 }
 
 // The parity tile pass: the first WHT's levels 0..11 of each column (read at
@@ -695,7 +779,10 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_wht_alpha_wht_tile(const Fe
   };
   auto mid = [=](uint32_t, int t, Fr& v) { v = mul(v, unpack_fe(alpha_s[t])); };
   auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(dst + addr(tile, t)) = u; };
-  tile_pass_v2<kWht, kWht, true, uint4>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv, stage, mid, st);
+  // No register prefetch of the next tile: with the product in the step, its
+  // registers would spill (measured); the tile's loads are issued at its start.
+  tile_pass_v2<kWht, kWht, true, false, uint4>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv, stage, mid,
+                                               st);
 }
 
 // ---------------------------------------------------------------- hashing
