@@ -1,5 +1,6 @@
 // BLAKE2s-256 compression on the device (RFC 7693), one message per thread.
-// Rotations are single funnel shifts.
+// Rotations by 12 and 7 are single funnel shifts, those by 16 and 8 byte
+// permutes.
 #pragma once
 #include <cstdint>
 
@@ -9,6 +10,9 @@ static __constant__ uint32_t kIv[8] = {0x6A09E667u, 0xBB67AE85u, 0x3C6EF372u, 0x
                                 0x510E527Fu, 0x9B05688Cu, 0x1F83D9ABu, 0x5BE0CD19u};
 
 __device__ __forceinline__ uint32_t rotr(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
+// Rotations by whole bytes as byte permutes (funnel shifts issue at half rate).
+__device__ __forceinline__ uint32_t rotr16(uint32_t x) { return __byte_perm(x, x, 0x1032); }
+__device__ __forceinline__ uint32_t rotr8(uint32_t x) { return __byte_perm(x, x, 0x0321); }
 // a + b as a 32-bit multiply-add by `one` (a runtime 1 from the kernel's
 // arguments): it issues to the FMA pipe, leaving the ALU pipe, which the
 // XORs and rotations keep busy, to them.
@@ -20,11 +24,11 @@ __device__ __forceinline__ uint32_t add_fma(uint32_t a, uint32_t b, uint32_t one
 
 #define QFD_G(a, b, c, d, x, y)                         \
   v[a] = add_fma(add_fma(v[a], v[b], one), (x), one);   \
-  v[d] = rotr(v[d] ^ v[a], 16);                         \
+  v[d] = rotr16(v[d] ^ v[a]);                           \
   v[c] = add_fma(v[c], v[d], one);                      \
   v[b] = rotr(v[b] ^ v[c], 12);                         \
   v[a] = add_fma(add_fma(v[a], v[b], one), (y), one);   \
-  v[d] = rotr(v[d] ^ v[a], 8);                          \
+  v[d] = rotr8(v[d] ^ v[a]);                            \
   v[c] = add_fma(v[c], v[d], one);                      \
   v[b] = rotr(v[b] ^ v[c], 7);
 

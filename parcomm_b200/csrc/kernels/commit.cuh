@@ -825,10 +825,10 @@ __global__ void __launch_bounds__(kLeafThreads) k_hash_leaves(const Fe* __restri
       } else if (s < 8) {
         word = pre.tail[w];
       } else if (s == 8) {
-        word = pre.tail[2] | (rw(0) << 24);
+        word = __byte_perm(pre.tail[2], rw(0), 0x4210);  // pre.tail[2] (3 bytes) | (rw(0) << 24)
       } else {
         const int q = (s - 12) >> 2;
-        word = (rw(q) >> 8) | (rw(q + 1) << 24);
+        word = __byte_perm(rw(q), rw(q + 1), 0x4321);  // (rw(q) >> 8) | (rw(q + 1) << 24)
       }
       m[w] = word;
     }
