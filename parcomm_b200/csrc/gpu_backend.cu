@@ -746,8 +746,14 @@ void GpuBackend::eq_project_launch(const W* bva, uint64_t active, uint64_t b0, i
     return;
   }
 #endif
+#if defined(QF_FIELD_KB)
   QF_LAUNCH(s_, "k_eq_project_blocks", bytes,
             qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, 0, s_>>>(bva, active, P_.block_len, b0, nb, m, weights_.p, raw));
+#else
+  QF_LAUNCH(s_, "k_eq_project_blocks", bytes,
+            qfd::k_eq_project_blocks<<<grid, qfd::kEqThreads, qfd::kEqWeightSmem, s_>>>(bva, active, P_.block_len, b0, nb, m,
+                                                                                     weights_.p, raw));
+#endif
 }
 
 std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& outer, size_t nblocks) {

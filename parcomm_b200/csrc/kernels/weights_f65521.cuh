@@ -330,6 +330,15 @@ __global__ void k_eo_witness(const int8_t* __restrict__ bva, uint64_t active, ui
 // leaves each lane two entries (|sum| <= 256 * 128 * 65520 < 2^31), and the
 // CTA keeps i64 totals per block that reach `raw` with one atomic add per
 // entry at the end.
+constexpr size_t kEqWeightSmem = 2 * (kEqChunk / 2) * 16;  // the weight double buffer of k_eq_project_blocks
+
+// 16 bytes of weights from global to shared memory, asynchronously; bytes at
+// or past `avail` (0..16) are zero-filled (and not read).
+__device__ __forceinline__ void cp_async16_zfill(void* smem, const void* gmem, uint32_t avail) {
+  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(avail) : "memory");
+}
+
 __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_t* __restrict__ bva, uint64_t active,
                                                                     uint64_t block_len, uint64_t first_block, int nb,
                                                                     uint64_t m, const Fe* __restrict__ weights,
@@ -337,12 +346,31 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
   constexpr int kQuads = kEqChunk / 4;
   // planes_s[q][g]: g = 0 low planes of k 0..3, 1 high planes of k 0..3, 2 and 3 the same for k 4..7.
   __shared__ uint4 planes_s[kQuads][4];
+  // The chunk's weights of the block being summed and of the next one
+  // (cp.async double buffer, kEqWeightSmem bytes of dynamic shared memory):
+  // element e's 8 lanes at bytes 8e .. 8e + 7 of a buffer.
+  extern __shared__ uint4 eq_dyn_s[];
+  uint4 (*wts_s)[kEqChunk / 2] = reinterpret_cast<uint4 (*)[kEqChunk / 2]>(eq_dyn_s);
   __shared__ int32_t stage_s[kEqThreads / 32][64];
   __shared__ long long tot_s[kEqBlocks][64];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, h = threadIdx.x & 1;
   for (int t = threadIdx.x; t < kEqBlocks * 64; t += kEqThreads) tot_s[t >> 6][t & 63] = 0;
+  // Issues the copies of block b's chunk into wts_s[buf].
+  auto stage_block = [&](uint64_t c0, int b, int buf) {
+    const uint64_t bbase = (first_block + b) * block_len;
+    for (int u = threadIdx.x; u < kEqChunk / 2; u += kEqThreads) {
+      const uint64_t i = c0 + 2 * uint64_t(u);  // the unit's first element
+      const uint64_t g = bbase + 8 * i;
+      uint32_t avail = 0;
+      if (i < m && g < active) avail = uint32_t(active - g < 16 ? active - g : 16);
+      if (i + 1 >= m && avail > 8) avail = 8;  // the second element is past the packed length
+      cp_async16_zfill(&wts_s[buf][u], avail ? static_cast<const void*>(bva + g) : static_cast<const void*>(bva), avail);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
   for (uint64_t c0 = uint64_t(blockIdx.x) * kEqChunk; c0 < m; c0 += uint64_t(gridDim.x) * kEqChunk) {
     __syncthreads();
+    if (nb > 0) stage_block(c0, 0, 0);
     for (int q = threadIdx.x; q < kQuads; q += kEqThreads) {
       uint4 e[4];
 #pragma unroll
@@ -354,7 +382,6 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
       transpose4(e[0].y, e[1].y, e[2].y, e[3].y, pl[1]);
       transpose4(e[0].z, e[1].z, e[2].z, e[3].z, pl[2]);
       transpose4(e[0].w, e[1].w, e[2].w, e[3].w, pl[3]);
-      // pl[w] = {lo k=2w, hi k=2w, lo k=2w+1, hi k=2w+1}
       // Group g of quad q sits in slot g ^ ((q >> 1) & 1): a warp phase of 4
       // quads x 2 coefficient halves then reads 8 distinct bank groups.
       const int sw = (q >> 1) & 1;
@@ -363,9 +390,15 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
       planes_s[q][2 ^ sw] = make_uint4(pl[2][0], pl[2][2], pl[3][0], pl[3][2]);
       planes_s[q][3 ^ sw] = make_uint4(pl[2][1], pl[2][3], pl[3][1], pl[3][3]);
     }
-    __syncthreads();
     for (int b = 0; b < nb; ++b) {
-      const uint64_t bbase = (first_block + b) * block_len;
+      if (b + 1 < nb) {
+        stage_block(c0, b + 1, (b + 1) & 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+      } else {
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+      }
+      __syncthreads();  // block b's weights (and, at b = 0, the planes) are in shared memory
+      const uint4* wb = wts_s[b & 1];
       int32_t lo[8][4], hi[8][4];
 #pragma unroll
       for (int jj = 0; jj < 8; ++jj)
@@ -374,27 +407,11 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
 #pragma unroll 2
       for (int u = 0; u < kQuads / (kEqThreads / 2); ++u) {
         const int q = (threadIdx.x >> 1) + u * (kEqThreads / 2);
-        const uint64_t i0 = c0 + 4 * uint64_t(q);
-        const uint64_t g = bbase + 8 * i0;
-        uint32_t x[8];
-        if (i0 + 4 <= m && g + 32 <= active) {
-          const uint4 a = *reinterpret_cast<const uint4*>(bva + g), bq = *reinterpret_cast<const uint4*>(bva + g + 16);
-          x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w; x[4] = bq.x; x[5] = bq.y; x[6] = bq.z; x[7] = bq.w;
-        } else {
-#pragma unroll
-          for (int r = 0; r < 8; ++r) {
-            uint32_t w = 0;
-            for (int y = 0; y < 4; ++y) {
-              const uint64_t gy = g + 4 * r + y;
-              if (i0 + r / 2 < m && gy < active) w |= uint32_t(uint8_t(bva[gy])) << (8 * y);
-            }
-            x[r] = w;
-          }
-        }
-        // vj[jj]: lane jj of the quad's 4 elements (element r's lanes are x[2r], x[2r + 1]).
+        const uint4 a = wb[2 * q], bq = wb[2 * q + 1];
+        // vj[jj]: lane jj of the quad's 4 elements (element r's lanes are words 2r, 2r + 1).
         uint32_t v_lo[4], v_hi[4];
-        transpose4(x[0], x[2], x[4], x[6], v_lo);
-        transpose4(x[1], x[3], x[5], x[7], v_hi);
+        transpose4(a.x, a.z, bq.x, bq.z, v_lo);
+        transpose4(a.y, a.w, bq.y, bq.w, v_hi);
         const int sw = (q >> 1) & 1;
         const uint4 pl = planes_s[q][(2 * h) ^ sw], ph = planes_s[q][(2 * h + 1) ^ sw];
         const uint32_t plo[4] = {pl.x, pl.y, pl.z, pl.w}, phi[4] = {ph.x, ph.y, ph.z, ph.w};
@@ -429,16 +446,16 @@ __global__ void __launch_bounds__(kEqThreads, 2) k_eq_project_blocks(const int8_
         const int f = (lane & 30) + qq;  // entry f: lane j = f / 4, coefficient 4h + f % 4
         stage_s[warp][(f >> 2) * 8 + 4 * h + (f & 3)] = acc[qq];
       }
-      __syncthreads();
+      __syncthreads();  // stage_s complete; every thread is done reading wts_s[b & 1]
       if (threadIdx.x < 64) {
         long long t = 0;
 #pragma unroll
         for (int w = 0; w < kEqThreads / 32; ++w) t += stage_s[w][threadIdx.x];
         tot_s[b][threadIdx.x] += t;
       }
-      __syncthreads();
     }
   }
+  __syncthreads();
   for (int t = threadIdx.x; t < nb * 64; t += kEqThreads)
     atomicAdd(raw + t, (unsigned long long)tot_s[t >> 6][t & 63]);  // two's complement sum
 }
