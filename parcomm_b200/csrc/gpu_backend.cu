@@ -144,6 +144,10 @@ static void configure_tile_kernels() {
   set_smem(qfd::k_butterfly_strided<qfd::kWht>, bytes);
   set_smem(qfd::k_mobius_wht_strided, bytes);
   set_smem(qfd::k_wht_alpha_wht_tile, bytes + qfd::kAlphaStageSmem);
+#if !defined(QF_FIELD_KB)
+  // 38 KiB of static shared memory plus the 32 KiB weight double buffer.
+  set_smem(qfd::k_eq_project_blocks, qfd::kEqWeightSmem);
+#endif
   done.insert(dev);
 }
 
