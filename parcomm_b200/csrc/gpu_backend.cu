@@ -502,12 +502,26 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
   Fe* msg = cw;
   Fe* par = cw + R;
   const bool mobius = mob_from < logm;
-  if (logR < qfd::kMaxTileLog) {
+  // The separate passes: the rest of the Mobius transform, then per WHT a
+  // tile pass (levels 0..11, alpha first for the second) and strided passes.
+  // KoalaBear keeps them: its butterflies reduce at every level (3 operations
+  // per element, coefficient and level), so its passes are compute-heavier
+  // and the fused plan measured slower on its 8B step (351 vs 337 ms).
+  // Columns shorter than a tile (logR < 12) take them in both fields.
+#if defined(QF_FIELD_KB)
+  constexpr bool kSeparate = true;
+#else
+  constexpr bool kSeparate = false;
+#endif
+  if (kSeparate || logR < qfd::kMaxTileLog) {
+    const int wl = std::min(qfd::kMaxTileLog, logR);
     if (mobius) strided_passes<qfd::kMobius>(s, msg, msg, logR, logm, mob_from, logm, timed, allow_tuning);
-    for (int pass = 0; pass < 2; ++pass)
+    for (int pass = 0; pass < 2; ++pass) {
       launch(s, timed, "k_wht_tile", (uint64_t(2) << logm) * 16,
-             qf_intops::transform_ops(kOps, uint64_t(1) << logm, logR, 0, 1, pass),
-             [&] { wht_tile_launch(s, pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, logm, logR); });
+             qf_intops::transform_ops(kOps, uint64_t(1) << logm, wl, 0, 1, pass),
+             [&] { wht_tile_launch(s, pass == 0 ? msg : par, par, pass == 0 ? nullptr : alpha, logR, logm, wl); });
+      strided_passes<qfd::kWht>(s, par, par, logR, logm, wl, logR, timed, allow_tuning);
+    }
     return;
   }
   constexpr int kT = qfd::kMaxTileLog;
