@@ -509,6 +509,9 @@ def main():
                     help="skip the same-bytes comparisons (dp4a kernels, per-matrix launch sequence)")
     ap.add_argument("--no-recompute", action="store_true",
                     help="skip the recompute-mode measurement (the reference's --cache-mode recompute)")
+    ap.add_argument("--profile-range", action="store_true",
+                    help="bracket the device-resident timed steps with cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--out", default=str(ROOT / "bench_out"), help="directory for the clock samples and kernel stats")
     args = ap.parse_args()
 
@@ -615,12 +618,17 @@ def main():
         barrier()
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         launches0 = qf.kernel_launches()
+        profiled = args.profile_range and on_device and commit_fn is None
+        if profiled:  # a profiler started with its capture off records only this region
+            torch.cuda.profiler.start()
         ev0.record()
         last = None
         for _ in range(steps):
             last = step(on_device, commit_fn)
         ev1.record()
         barrier()
+        if profiled:
+            torch.cuda.profiler.stop()
         ms = max_over_ranks(ev0.elapsed_time(ev1), world)
         return ms / steps, last, qf.kernel_launches() - launches0
 

@@ -17,6 +17,11 @@
 namespace QFB_NS {
 
 static constexpr int kThreads = 256;
+// Folding rounds over vectors of at most this many elements (LiteBullet,
+// sumcheck, EO binary rounds) run on the host: each device round costs a
+// launch and a synchronisation (about 20 us), more than the host's 2n
+// extension products at this length.
+static constexpr uint64_t kHostTail = 512;
 // Operation counts of this field's arithmetic, for the integer roofline.
 #if defined(QF_FIELD_KB)
 static constexpr const qf_intops::FieldOps& kOps = qf_intops::kKoalaBear;
@@ -178,6 +183,10 @@ void GpuBackend::release_opening_state() {
   sum_len_ = 0;
   eo_len_ = 0;
   msg_valid_ = false;
+  host_v_.clear();
+  host_w_.clear();
+  host_wit_.clear();
+  host_qv_.clear();
 }
 
 // ---------------------------------------------------------------- streamed weights
@@ -723,6 +732,61 @@ std::vector<F> GpuBackend::reduce_to_host(const DBuf<Fe>& partials, uint32_t, in
   return out;
 }
 
+std::vector<F> GpuBackend::copy_to_host(const Fe* p, uint64_t n) {
+  std::vector<F> out(n);
+  QF_CK(cudaMemcpyAsync(out.data(), p, n * 16, cudaMemcpyDeviceToHost, s_));
+  QF_CK(cudaStreamSynchronize(s_));
+  return out;
+}
+
+namespace {
+// The host rounds below mirror the device kernels of the same names
+// (k_sum_message, k_sum_fold_message, k_eo_fold_cross, k_lb_cross,
+// k_lb_fold_cross): the same field operations on canonical elements, so the
+// results are the same bytes.
+std::array<F, 2> sum_message_host(const std::vector<F>& v, const std::vector<F>& w) {
+  const size_t h = v.size() / 2;
+  F a = F::zero(), b = F::zero();
+  for (size_t i = 0; i < h; ++i) {
+    a += v[i] * w[i];
+    b += (v[i + h] - v[i]) * (w[i + h] - w[i]);
+  }
+  return {a, b};
+}
+void sum_fold_host(std::vector<F>& v, F ch) {
+  const size_t h = v.size() / 2;
+  for (size_t i = 0; i < h; ++i) v[i] += ch * (v[i + h] - v[i]);
+  v.resize(h);
+}
+std::array<F, 2> eo_cross_host(const std::vector<F>& w, const std::vector<F>& q) {
+  F a = F::zero(), b = F::zero();
+  for (size_t j = 0; j + 1 < w.size(); j += 2) {
+    a += w[j] * q[j + 1];
+    b += w[j + 1] * q[j];
+  }
+  return {a, b};
+}
+void eo_fold_host(std::vector<F>& v, F f) {
+  const size_t h = v.size() / 2;
+  for (size_t i = 0; i < h; ++i) v[i] = v[2 * i] + v[2 * i + 1] * f;
+  v.resize(h);
+}
+std::array<F, 2> lb_cross_host(const std::vector<F>& L, const std::vector<F>& R) {
+  const size_t h = L.size() / 2;
+  F a = F::zero(), b = F::zero();
+  for (size_t i = 0; i < h; ++i) {
+    a += L[i] * R[h + i];
+    b += L[h + i] * R[i];
+  }
+  return {a, b};
+}
+void lb_fold_host(std::vector<F>& v, F f) {
+  const size_t h = v.size() / 2;
+  for (size_t i = 0; i < h; ++i) v[i] += v[h + i] * f;
+  v.resize(h);
+}
+}  // namespace
+
 // Device table of the 2^n weights of an MSB-first point, `weights` giving the
 // host table of a coordinate slice (equality_table, packed.rs:525-545, or
 // tensor_weights, qafold_short_pc.rs:2826-2855; both factor over slices).
@@ -808,6 +872,8 @@ std::vector<std::vector<F>> GpuBackend::project_blocks(const std::vector<F>& out
         const int64_t r = v % int64_t(F::kPrime);
         out[b][j].c[k] = typename F::Coeff(r < 0 ? r + int64_t(F::kPrime) : r);
       }
+  host_v_.clear();
+  host_w_.clear();
   sum_len_ = 0;
   return out;
 }
@@ -866,6 +932,8 @@ std::vector<F> GpuBackend::project(const std::vector<F>& outer) {
   } else {
     block_fold_launch(bva_, active_, 1, dT.p, 0);
   }
+  host_v_.clear();
+  host_w_.clear();
   sum_len_ = m;
   msg_valid_ = false;
   return lanes[0];
@@ -914,12 +982,20 @@ Digest GpuBackend::fold_and_commit(const std::vector<F>& fw) {
                 qf_intops::transform_ops(kOps, uint64_t(1) << logm, 0, l0, 1, 0), qfd::k_copy_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, smem, s_>>>(
                 values_.p, folded_->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
   encode_and_hash(*folded_, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false, l0);
+  host_v_.clear();
+  host_w_.clear();
   sum_len_ = m;
   msg_valid_ = false;
   return folded_->root_;
 }
 
 void GpuBackend::sumcheck_message(F m[2]) {
+  if (!msg_valid_ && !host_v_.empty()) {
+    const std::array<F, 2> r = sum_message_host(host_v_, host_w_);
+    msg_[0] = r[0];
+    msg_[1] = r[1];
+    msg_valid_ = true;
+  }
   if (!msg_valid_) {
     const int g = grid_for(sum_len_ / 2, kThreads);
     QF_LAUNCH(s_, "k_sum_message", sum_len_ * 32, qfd::k_sum_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, partials_.p));
@@ -933,6 +1009,18 @@ void GpuBackend::sumcheck_message(F m[2]) {
 }
 
 void GpuBackend::sumcheck_fold(F ch) {
+  if (host_v_.empty() && sum_len_ <= kHostTail) {
+    host_v_ = copy_to_host(values_.p, sum_len_);
+    host_w_ = copy_to_host(weights_.p, sum_len_);
+  }
+  if (!host_v_.empty()) {
+    sum_fold_host(host_v_, ch);
+    sum_fold_host(host_w_, ch);
+    sum_len_ /= 2;
+    msg_valid_ = false;
+    if (sum_len_ >= 2) sumcheck_message(msg_);
+    return;
+  }
   if (tmp_v_.n < sum_len_ / 2) { tmp_v_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); tmp_w_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); }
   const int g = grid_for(std::max<uint64_t>(sum_len_ / 4, 1), kThreads);
   QF_LAUNCH(s_, "k_sum_fold_message", sum_len_ * 48, qfd::k_sum_fold_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p));
@@ -950,12 +1038,14 @@ void GpuBackend::sumcheck_fold(F ch) {
 }
 
 F GpuBackend::sumcheck_final_value() {
+  if (!host_v_.empty()) return host_v_[0];
   F v;
   QF_CK(cudaMemcpyAsync(&v, values_.p, 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
   return v;
 }
 F GpuBackend::sumcheck_final_weight() {
+  if (!host_w_.empty()) return host_w_[0];
   F v;
   QF_CK(cudaMemcpyAsync(&v, weights_.p, 16, cudaMemcpyDeviceToHost, s_));
   QF_CK(cudaStreamSynchronize(s_));
@@ -1443,6 +1533,8 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
   HostScope hs("eo_build");
   const uint64_t rows = logical / stride;
   eo_len_ = rows;
+  host_wit_.clear();
+  host_qv_.clear();
   wit_.alloc(rows);
   qv_.alloc(rows);
   std::vector<F> pinv = consecutive_powers(inv, stride);
@@ -1566,6 +1658,17 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
 void GpuBackend::eo_round_fold(F inv, F ch) {
   HostScope hs("eo_round_fold");
   const uint64_t n = eo_len_;
+  if (host_wit_.empty() && n <= kHostTail) {
+    host_wit_ = copy_to_host(wit_.p, n);
+    host_qv_ = copy_to_host(qv_.p, n);
+  }
+  if (!host_wit_.empty()) {
+    eo_fold_host(host_wit_, inv);
+    eo_fold_host(host_qv_, ch);
+    eo_len_ = n / 2;
+    if (eo_len_ >= 2) cross_ = eo_cross_host(host_wit_, host_qv_);
+    return;
+  }
   const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
   if (n >= (uint64_t(1) << 26)) {
     // Large rounds fold the two vectors one after the other: the full-length
@@ -1592,9 +1695,16 @@ void GpuBackend::eo_round_fold(F inv, F ch) {
 
 std::array<F, 2> GpuBackend::eo_terminal() {
   F w0, q0;
-  QF_CK(cudaMemcpyAsync(&w0, wit_.p, 16, cudaMemcpyDeviceToHost, s_));
-  QF_CK(cudaMemcpyAsync(&q0, qv_.p, 16, cudaMemcpyDeviceToHost, s_));
-  QF_CK(cudaStreamSynchronize(s_));
+  if (!host_wit_.empty()) {
+    w0 = host_wit_[0];
+    q0 = host_qv_[0];
+    host_wit_.clear();
+    host_qv_.clear();
+  } else {
+    QF_CK(cudaMemcpyAsync(&w0, wit_.p, 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaMemcpyAsync(&q0, qv_.p, 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaStreamSynchronize(s_));
+  }
   // The EO vectors (up to 2 x 1.5 x N/stride elements) are done: give their
   // memory back before the batch opening allocates its own.
   wit_.reset();
@@ -1638,20 +1748,45 @@ std::array<F, 2> GpuBackend::lb_cross(const Fe* L, const Fe* R, uint64_t n) {
 // domain label) and `claimed` is the running right-hand side.
 LiteBullet<F> GpuBackend::litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, PcsTranscript<F>& t, const char* label,
                                          const char* fold_label, bool check_and_absorb) {
+  // Vectors of at most kHostTail elements fold on the host from the start;
+  // longer ones switch there once they have folded down to that length.
+  std::vector<F> hl, hr;
+  if (n > 0 && n <= kHostTail) {
+    hl = copy_to_host(L, n);
+    hr = copy_to_host(R, n);
+  }
   if (check_and_absorb) {
-    if (n == 0 || !is_pow2(n) || dot_dev(L, R, n) != claimed) fail(QF_E_INVALID_COMMITMENT, "litebullet claim");
+    if (n == 0 || !is_pow2(n)) fail(QF_E_INVALID_COMMITMENT, "litebullet claim");
+    F dot = F::zero();
+    if (hl.empty()) dot = dot_dev(L, R, n);
+    else
+      for (uint64_t i = 0; i < n; ++i) dot += hl[i] * hr[i];
+    if (dot != claimed) fail(QF_E_INVALID_COMMITMENT, "litebullet claim");
     t.absorb_str("litebullet-domain", label);
   }
   F rhs = claimed;
   LiteBullet<F> out;
   std::array<F, 2> cr{F::zero(), F::zero()};
-  if (n > 1) cr = lb_cross(L, R, n);
+  if (n > 1) cr = hl.empty() ? lb_cross(L, R, n) : lb_cross_host(hl, hr);
   while (n > 1) {
     t.push_response(cr[0]);
     t.push_response(cr[1]);
     F ch = t.challenge_nonzero(fold_label);
     F inv = ch.inverse();
     rhs += cr[0] * ch + cr[1] * inv;
+    out.a_point.push_back(inv);
+    out.b_point.push_back(ch);
+    if (hl.empty() && n <= kHostTail) {
+      hl = copy_to_host(L, n);
+      hr = copy_to_host(R, n);
+    }
+    if (!hl.empty()) {
+      lb_fold_host(hl, inv);
+      lb_fold_host(hr, ch);
+      n /= 2;
+      if (n > 1) cr = lb_cross_host(hl, hr);
+      continue;
+    }
     const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
     QF_LAUNCH(s_, "k_lb_fold_cross", n * 48,
               qfd::k_lb_fold_cross<<<g, kThreads, 0, s_>>>(L, R, n, to_fe(inv), to_fe(ch), partials_.p));
@@ -1660,12 +1795,15 @@ LiteBullet<F> GpuBackend::litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, Pc
       std::vector<F> r = reduce_to_host(partials_, g, 2);
       cr = {r[0], r[1]};
     }
-    out.a_point.push_back(inv);
-    out.b_point.push_back(ch);
   }
-  QF_CK(cudaMemcpyAsync(&out.a_value, L, 16, cudaMemcpyDeviceToHost, s_));
-  QF_CK(cudaMemcpyAsync(&out.b_value, R, 16, cudaMemcpyDeviceToHost, s_));
-  QF_CK(cudaStreamSynchronize(s_));
+  if (!hl.empty()) {
+    out.a_value = hl[0];
+    out.b_value = hr[0];
+  } else {
+    QF_CK(cudaMemcpyAsync(&out.a_value, L, 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaMemcpyAsync(&out.b_value, R, 16, cudaMemcpyDeviceToHost, s_));
+    QF_CK(cudaStreamSynchronize(s_));
+  }
   t.push_response(out.a_value);
   t.push_response(out.b_value);
   if (check_and_absorb && out.a_value * out.b_value != rhs) fail(QF_E_INVALID_COMMITMENT, "litebullet terminal");

@@ -213,7 +213,9 @@ class GpuBackend : public Backend<F>,
   void wht_dev(Fe* v, int logn, const Fe* alpha);
   F dot_dev(const Fe* a, const Fe* b, uint64_t n);
   std::array<F, 2> lb_cross(const Fe* L, const Fe* R, uint64_t n);
-  // LiteBullet (or MultiEval row rounds) on device vectors, folded in place.
+  // LiteBullet (or MultiEval row rounds) on device vectors, folded in place
+  // down to 512 elements and on the host from there (L and R are left
+  // partly folded).
   LiteBullet<F> litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, PcsTranscript<F>& t, const char* label,
                                const char* fold_label, bool check_and_absorb);
   const Fe* level_alpha(size_t level, int which);
@@ -230,6 +232,7 @@ class GpuBackend : public Backend<F>,
   std::vector<std::vector<std::vector<F>>> project_groups_streamed(const std::vector<std::vector<const Term<F>*>>& groups,
                                                                    size_t stride);
   std::vector<F> reduce_to_host(const DBuf<Fe>& partials, uint32_t count, int n);
+  std::vector<F> copy_to_host(const Fe* p, uint64_t n);
   void block_fold_launch(const W* bva, uint64_t active, int blocks, const Fe* T, int accumulate);
   void project_terms_launch(const W* bva, uint64_t active, const qfd::TermTiles* terms, int n_terms, uint64_t tiles,
                             const Fe* tables, size_t lanes, Fe* out, uint64_t bytes);
@@ -256,10 +259,12 @@ class GpuBackend : public Backend<F>,
   uint64_t sum_len_ = 0;
   bool msg_valid_ = false;
   F msg_[2];
+  std::vector<F> host_v_, host_w_;  // the sumcheck's last rounds (length <= kHostTail), on the host
   // EO state
   DBuf<Fe> wit_, qv_, wit2_, qv2_;
   uint64_t eo_len_ = 0;
   std::array<F, 2> cross_;
+  std::vector<F> host_wit_, host_qv_;  // the EO's last binary rounds, on the host
   DBuf<Fe> partials_;  // reduction buffer: header (counter, result) + one slot per CTA
 };
 
