@@ -171,7 +171,10 @@ int qf_kernel_int_peaks(double out[6]);
  * contract on the tensor cores with exact integer limbs instead of the dp4a
  * / IMAD kernels (measured slower on B200; kept for the comparison).  "per_matrix"
  * (default 0): 1 issues the weight passes one launch per term, bucket or
- * block instead of one launch over all of them.  Set it between calls, not
+ * block instead of one launch over all of them.  "core_dots" (default 0): 1
+ * sums the extension products of the EO binary rounds, the sumcheck
+ * messages and the LiteBullet rounds with CUDA-core multiply-adds instead
+ * of exact integer-limb tensor-core products.  Set it between calls, not
  * while another call runs. */
 int qf_kernel_option(const char* name, int value);
 

@@ -184,6 +184,7 @@ int qf_kernel_option(const char* name, int value) {
     const std::string n = name ? name : "";
     if (n == "imma") qfg::KernelOptions::imma = value != 0;
     else if (n == "per_matrix") qfg::KernelOptions::per_matrix = value != 0;
+    else if (n == "core_dots") qfg::KernelOptions::core_dots = value != 0;
     else fail(QF_E_ARGUMENT, "unknown kernel option: " + n);
   });
 }

@@ -4,6 +4,7 @@
 #include "kernels/open.cuh"
 #include "kernels/vec.cuh"
 #include "kernels/audit.cuh"
+#include "kernels/dot_mma.cuh"
 #if !defined(QF_FIELD_KB)
 #include "kernels/imma_f65521.cuh"
 #endif
@@ -38,6 +39,9 @@ static bool imma_on() {
   return KernelOptions::imma.load() != 0;
 #endif
 }
+// The extension-product sums of the EO, sumcheck and LiteBullet rounds run
+// on the tensor cores (kernels/dot_mma.cuh) unless core_dots is set.
+static bool tc_dots() { return KernelOptions::core_dots.load() == 0; }
 // Grid of the persistent tensor-core weight kernels: four CTAs per SM.
 static unsigned mma_grid() {
   static const int sms = [] {
@@ -46,6 +50,11 @@ static unsigned mma_grid() {
     return n;
   }();
   return unsigned(sms * 4);
+}
+// Grid of a tensor-core product kernel over `count` indices (one per thread
+// and chunk), at most four CTAs per SM.
+static unsigned dot_grid(uint64_t count) {
+  return unsigned(std::max<uint64_t>(1, std::min<uint64_t>((count + qfd::kDotThreads - 1) / qfd::kDotThreads, mma_grid())));
 }
 
 template <class K>
@@ -998,7 +1007,12 @@ void GpuBackend::sumcheck_message(F m[2]) {
   }
   if (!msg_valid_) {
     const int g = grid_for(sum_len_ / 2, kThreads);
-    QF_LAUNCH(s_, "k_sum_message", sum_len_ * 32, qfd::k_sum_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, partials_.p));
+    if (tc_dots())
+      QF_LAUNCH(s_, "k_sum_message_mma", sum_len_ * 32,
+                qfd::k_sum_message_mma<<<dot_grid(sum_len_ / 2), qfd::kDotThreads, 0, s_>>>(values_.p, weights_.p, sum_len_,
+                                                                                             partials_.p));
+    else
+      QF_LAUNCH(s_, "k_sum_message", sum_len_ * 32, qfd::k_sum_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, partials_.p));
     std::vector<F> r = reduce_to_host(partials_, g, 2);
     msg_[0] = r[0];
     msg_[1] = r[1];
@@ -1023,7 +1037,12 @@ void GpuBackend::sumcheck_fold(F ch) {
   }
   if (tmp_v_.n < sum_len_ / 2) { tmp_v_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); tmp_w_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); }
   const int g = grid_for(std::max<uint64_t>(sum_len_ / 4, 1), kThreads);
-  QF_LAUNCH(s_, "k_sum_fold_message", sum_len_ * 48, qfd::k_sum_fold_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p));
+  if (tc_dots() && sum_len_ >= 4)
+    QF_LAUNCH(s_, "k_sum_fold_message_mma", sum_len_ * 48,
+              qfd::k_sum_fold_message_mma<<<dot_grid(sum_len_ / 4), qfd::kDotThreads, 0, s_>>>(
+                  values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p));
+  else
+    QF_LAUNCH(s_, "k_sum_fold_message", sum_len_ * 48, qfd::k_sum_fold_message<<<g, kThreads, 0, s_>>>(values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p));
   std::swap(values_, tmp_v_);
   std::swap(weights_, tmp_w_);
   sum_len_ /= 2;
@@ -1642,7 +1661,11 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
     QF_CK(cudaStreamSynchronize(s_));
   }
   const int g = grid_for(std::max<uint64_t>(rows / 2, 1), kThreads);
-  QF_LAUNCH(s_, "k_eo_dot_cross", rows * 32, qfd::k_eo_dot_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p));
+  if (tc_dots())
+    QF_LAUNCH(s_, "k_eo_dot_cross_mma", rows * 32,
+              qfd::k_eo_dot_cross_mma<<<dot_grid(rows / 2), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p));
+  else
+    QF_LAUNCH(s_, "k_eo_dot_cross", rows * 32, qfd::k_eo_dot_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p));
   std::vector<F> r = reduce_to_host(partials_, g, 3);
   cross_ = {r[1], r[2]};
   if (rows == 1) {  // a single packed row has no binary rounds
@@ -1678,11 +1701,22 @@ void GpuBackend::eo_round_fold(F inv, F ch) {
     QF_LAUNCH(s_, "k_eo_fold_vec", n * 24, qfd::k_eo_fold_vec<<<grid_for(n / 2, kThreads), kThreads, 0, s_>>>(wit_.p, n, to_fe(inv), w2.p));
     wit_ = std::move(w2);
     DBuf<Fe> q2(n / 2);
-    QF_LAUNCH(s_, "k_eo_fold_query_cross", n * 32, qfd::k_eo_fold_query_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch), q2.p, partials_.p));
+    if (tc_dots())
+      QF_LAUNCH(s_, "k_eo_fold_query_cross_mma", n * 32,
+                qfd::k_eo_fold_query_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch),
+                                                                                             q2.p, partials_.p));
+    else
+      QF_LAUNCH(s_, "k_eo_fold_query_cross", n * 32, qfd::k_eo_fold_query_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch), q2.p, partials_.p));
     qv_ = std::move(q2);
   } else {
     if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
-    QF_LAUNCH(s_, "k_eo_fold_cross", n * 48, qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p));
+    if (tc_dots() && n >= 4)
+      QF_LAUNCH(s_, "k_eo_fold_cross_mma", n * 48,
+                qfd::k_eo_fold_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv),
+                                                                                       to_fe(ch), wit2_.p, qv2_.p,
+                                                                                       partials_.p));
+    else
+      QF_LAUNCH(s_, "k_eo_fold_cross", n * 48, qfd::k_eo_fold_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv), to_fe(ch), wit2_.p, qv2_.p, partials_.p));
     std::swap(wit_, wit2_);
     std::swap(qv_, qv2_);
   }
@@ -1731,6 +1765,10 @@ void GpuBackend::wht_dev(Fe* v, int logn, const Fe* alpha) {
 }
 
 F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {
+  if (tc_dots()) {
+    QF_LAUNCH(s_, "k_dot_mma", n * 32, qfd::k_dot_mma<<<dot_grid(n), qfd::kDotThreads, 0, s_>>>(a, b, n, partials_.p));
+    return reduce_to_host(partials_, 0, 1)[0];
+  }
   const int g = grid_for(n, kThreads);
   QF_LAUNCH(s_, "k_dot", n * 32, qfd::k_dot<<<g, kThreads, 0, s_>>>(a, b, n, partials_.p));
   return reduce_to_host(partials_, g, 1)[0];
@@ -1738,7 +1776,10 @@ F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {
 
 std::array<F, 2> GpuBackend::lb_cross(const Fe* L, const Fe* R, uint64_t n) {
   const int g = grid_for(std::max<uint64_t>(n / 2, 1), kThreads);
-  QF_LAUNCH(s_, "k_lb_cross", n * 32, qfd::k_lb_cross<<<g, kThreads, 0, s_>>>(L, R, n, partials_.p));
+  if (tc_dots())
+    QF_LAUNCH(s_, "k_lb_cross_mma", n * 32, qfd::k_lb_cross_mma<<<dot_grid(n / 2), qfd::kDotThreads, 0, s_>>>(L, R, n, partials_.p));
+  else
+    QF_LAUNCH(s_, "k_lb_cross", n * 32, qfd::k_lb_cross<<<g, kThreads, 0, s_>>>(L, R, n, partials_.p));
   std::vector<F> r = reduce_to_host(partials_, g, 2);
   return {r[0], r[1]};
 }
@@ -1788,8 +1829,13 @@ LiteBullet<F> GpuBackend::litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, Pc
       continue;
     }
     const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
-    QF_LAUNCH(s_, "k_lb_fold_cross", n * 48,
-              qfd::k_lb_fold_cross<<<g, kThreads, 0, s_>>>(L, R, n, to_fe(inv), to_fe(ch), partials_.p));
+    if (tc_dots() && n >= 4)
+      QF_LAUNCH(s_, "k_lb_fold_cross_mma", n * 48,
+                qfd::k_lb_fold_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(L, R, n, to_fe(inv), to_fe(ch),
+                                                                                       partials_.p));
+    else
+      QF_LAUNCH(s_, "k_lb_fold_cross", n * 48,
+                qfd::k_lb_fold_cross<<<g, kThreads, 0, s_>>>(L, R, n, to_fe(inv), to_fe(ch), partials_.p));
     n /= 2;
     if (n > 1) {
       std::vector<F> r = reduce_to_host(partials_, g, 2);

@@ -124,6 +124,7 @@ size_t DevicePool::cached_bytes() {
 
 std::atomic<int> KernelOptions::imma{0};
 std::atomic<int> KernelOptions::per_matrix{0};
+std::atomic<int> KernelOptions::core_dots{0};
 
 bool KernelClock::enabled = false;
 std::mutex KernelClock::mu;
