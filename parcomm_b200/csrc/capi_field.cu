@@ -178,7 +178,14 @@ static std::vector<Claim<F>> device_eval_claims(const Parameters<F>& P, GpuBacke
 }
 
 void make_params(qf_params* out, const std::vector<Shape>& shapes, const Config& config) {
-  out->P = std::shared_ptr<Parameters<F>>(make_parameters<F>(shapes, config).release());
+  // The setup commitments run on the current device when there is one; a
+  // process without a device (parameter digests, statement checks) builds
+  // them on the host.
+  int devices = 0;
+  DeviceSetup ds;
+  SetupAccel<F>* accel = cudaGetDeviceCount(&devices) == cudaSuccess && devices > 0 ? &ds : nullptr;
+  if (!accel) cudaGetLastError();
+  out->P = std::shared_ptr<Parameters<F>>(make_parameters<F>(shapes, config, accel).release());
   out->tables = std::make_shared<DeviceTables>();
 }
 

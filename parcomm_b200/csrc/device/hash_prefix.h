@@ -14,6 +14,17 @@ struct LeafPrefix {
   uint32_t one = 1;  // the multiplier of the compression's multiply-add additions
 };
 
+// Setup-row leaf message = constant framed prefix || framed row index ||
+// row bytes.  The prefix's first t0 bytes (whole blocks) are absorbed into
+// `mid`; `tail` holds the n_tail (1..64) bytes after them.
+struct SetupLeafPrefix {
+  uint32_t mid[8];
+  uint32_t t0;
+  uint32_t n_tail;
+  uint32_t tail[16];
+  uint32_t one = 1;  // the multiplier of the compression's multiply-add additions
+};
+
 // Inner message = 50-byte framed domain || left || right.
 struct InnerPrefix {
   uint32_t w[13];  // last word holds 2 bytes

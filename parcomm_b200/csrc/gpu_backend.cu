@@ -630,6 +630,60 @@ void GpuBackend::encode_and_hash(DeviceCodeword& out, const Fe* alpha, int logR,
   out.root_ = digest_from_words(r);
 }
 
+// The setup-row leaf prefix: the prefix's whole 64-byte blocks (all but a
+// non-empty tail) are compressed here.
+static ::qfd::SetupLeafPrefix setup_leaf_prefix(const SetupShape& shape) {
+  const std::vector<uint8_t> pre = setup_row_prefix<F>(shape);
+  ::qfd::SetupLeafPrefix pf;
+  uint32_t h[8];
+  for (int i = 0; i < 8; ++i) h[i] = kBlake2sIv[i];
+  h[0] ^= 0x01010000u ^ 32u;
+  const size_t blocks = (pre.size() - 1) / 64;
+  for (size_t b = 0; b < blocks; ++b) blake2s_compress(h, pre.data() + 64 * b, 64 * (b + 1), false);
+  for (int i = 0; i < 8; ++i) pf.mid[i] = h[i];
+  pf.t0 = uint32_t(64 * blocks);
+  pf.n_tail = uint32_t(pre.size() - 64 * blocks);
+  uint8_t tail[64] = {0};
+  std::memcpy(tail, pre.data() + 64 * blocks, pf.n_tail);
+  for (int i = 0; i < 16; ++i)
+    pf.tail[i] = uint32_t(tail[4 * i]) | (uint32_t(tail[4 * i + 1]) << 8) | (uint32_t(tail[4 * i + 2]) << 16) |
+                 (uint32_t(tail[4 * i + 3]) << 24);
+  return pf;
+}
+
+bool DeviceSetup::encode_level(const QaCode<F>& target, const QaCode<F>& current, size_t rf, const SetupShape& shape,
+                               std::vector<F>& encoded, std::vector<Digest>& leaves) {
+  const size_t mr = shape.message_rows, er = shape.encoded_rows, hc = shape.h_cols;
+  if (shape.t_cols != 0 || er != 2 * mr || er * hc < (size_t(1) << 20) || !target.systematic_first ||
+      target.index != 2 || target.message_len != mr || current.message_len != mr * rf || !is_pow2(hc) ||
+      hc > current.alphas.size() * rf)
+    return false;
+  check(ilog2(mr * hc) <= 30, "setup level size");
+  cudaStream_t s;
+  QF_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  {
+    DBuf<Fe> cw(er * hc), alpha(mr);
+    DBuf<uint4> lv(2 * er);
+    // Column col is the message current.alphas[col / rf][(col % rf) mr ..][.. mr).
+    for (size_t col = 0; col < hc; ++col)
+      QF_CK(cudaMemcpyAsync(cw.p + col * er, current.alphas[col / rf].data() + (col % rf) * mr, mr * 16,
+                            cudaMemcpyHostToDevice, s));
+    QF_CK(cudaMemcpyAsync(alpha.p, target.alphas[1].data(), mr * 16, cudaMemcpyHostToDevice, s));
+    const int logm = ilog2(mr * hc);
+    encode_passes(s, cw.p, alpha.p, ilog2(mr), logm, logm, false, true);
+    const ::qfd::SetupLeafPrefix pf = setup_leaf_prefix(shape);
+    qfd::k_hash_setup_rows<<<unsigned((er + kThreads - 1) / kThreads), kThreads, 0, s>>>(cw.p, er, int(hc), pf, lv.p);
+    QF_CK(cudaGetLastError());
+    encoded.resize(er * hc);
+    leaves.resize(er);
+    QF_CK(cudaMemcpyAsync(encoded.data(), cw.p, er * hc * 16, cudaMemcpyDeviceToHost, s));
+    QF_CK(cudaMemcpyAsync(leaves.data(), lv.p, er * 32, cudaMemcpyDeviceToHost, s));
+    QF_CK(cudaStreamSynchronize(s));
+  }
+  QF_CK(cudaStreamDestroy(s));
+  return true;
+}
+
 static std::unique_ptr<DeviceCodeword> alloc_codeword(size_t R, size_t cols, cudaStream_t s) {
   auto cw = std::make_unique<DeviceCodeword>();
   cw->stream = s;

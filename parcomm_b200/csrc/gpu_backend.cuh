@@ -113,6 +113,18 @@ class BlockStream {
 void commit_block_into(const Parameters<F>& P, const W* d_bva, uint64_t active, size_t b, Fe* cw, uint4* tree,
                        const Fe* alpha, uint8_t* d_root, cudaStream_t s);
 
+// The setup commitments of a parameter set on the current device
+// (ShortQaFoldPC::setup, qafold_short_pc.rs:401-444; direct-interleaved
+// setup, qafold_short_setup.rs:427-536): each level's columns are encoded by
+// the commit's transform passes and its rows hashed by k_hash_setup_rows;
+// the host keeps the encoded matrix and builds the tree from the leaves.
+// Levels below 2^20 encoded entries stay on the host.
+class DeviceSetup final : public SetupAccel<F> {
+ public:
+  bool encode_level(const QaCode<F>& target, const QaCode<F>& current, size_t row_factor, const SetupShape& shape,
+                    std::vector<F>& encoded, std::vector<Digest>& leaves) override;
+};
+
 class GpuBackend : public Backend<F>,
                    public SingleBackend<F>,
                    public EoBackend<F>,

@@ -187,7 +187,8 @@ struct PackedPcs {
   // The setup depends only on (log_n, columns, security bits, seed), so one
   // process builds each distinct setup once and shares it between parameter
   // sets (a pool of many shapes with few distinct block sizes).
-  static PackedPcs create(size_t log_n, size_t columns, size_t security_bits, const std::array<uint8_t, 32>& seed) {
+  static PackedPcs create(size_t log_n, size_t columns, size_t security_bits, const std::array<uint8_t, 32>& seed,
+                          SetupAccel<F>* accel = nullptr) {
     if (log_n < 4 || log_n > 30) fail(QF_E_INVALID_NUMBER_OF_VARIABLES, "packed log_n");
     static std::mutex mu;
     static std::map<std::tuple<size_t, size_t, size_t, std::array<uint8_t, 32>>, std::shared_ptr<PcsParams<F>>> cache;
@@ -203,7 +204,8 @@ struct PackedPcs {
       }
     }
     StdRng rng(seed);
-    std::shared_ptr<PcsParams<F>> pp(pcs_setup<F>(size_t(1) << (log_n - ilog2(F::kLanes)), columns, security_bits, rng).release());
+    std::shared_ptr<PcsParams<F>> pp(
+        pcs_setup<F>(size_t(1) << (log_n - ilog2(F::kLanes)), columns, security_bits, rng, accel).release());
     std::lock_guard<std::mutex> g(mu);
     p.pp = cache.emplace(key, pp).first->second;
     return p;

@@ -276,15 +276,37 @@ inline void absorb_setup_shape(Blake2s& h, const SetupShape& s) {
   absorb_framed_u64(h, "t-last-length", s.t_last_len);
   absorb_framed_u64(h, "h-columns", s.h_cols);
 }
+// The bytes a setup row's leaf hash absorbs before its framed row index:
+// the domain, the field metadata (absorb_field_metadata), the setup mode and
+// the shape (absorb_setup_shape), framed.
+template <class F>
+std::vector<uint8_t> setup_row_prefix(const SetupShape& s) {
+  std::vector<uint8_t> b;
+  auto u64 = [&](const char* label, uint64_t v) {
+    const auto w = le64(v);
+    append_frame(b, label, w.data(), 8);
+  };
+  const char* dom = "qafold-short/setup-base-row/v1";
+  append_frame(b, "domain", dom, std::strlen(dom));
+  append_frame(b, "field-name", F::kName, std::strlen(F::kName));
+  u64("modulus", F::modulus_u64());
+  u64("canonical-bytes", F::kBytes);
+  u64("extension-degree", 1);
+  const char* mode = "direct-interleaved-v1";
+  append_frame(b, "decide-setup-mode", mode, std::strlen(mode));
+  u64("level", s.level);
+  u64("encoded-rows", s.encoded_rows);
+  u64("message-rows", s.message_rows);
+  u64("t-columns", s.t_cols);
+  u64("t-elements", s.t_elements);
+  u64("t-last-length", s.t_last_len);
+  u64("h-columns", s.h_cols);
+  return b;
+}
 template <class F>
 Blake2s setup_row_hasher(const SetupShape& s, size_t row) {
   Blake2s h;
-  const char* dom = "qafold-short/setup-base-row/v1";
-  absorb_framed(h, "domain", dom, std::strlen(dom));
-  absorb_field_metadata<F>(h);
-  const char* mode = "direct-interleaved-v1";
-  absorb_framed(h, "decide-setup-mode", mode, std::strlen(mode));
-  absorb_setup_shape(h, s);
+  h.update(setup_row_prefix<F>(s));
   absorb_framed_u64(h, "row", row);
   return h;
 }
@@ -309,6 +331,16 @@ MerkleTree build_setup_tree(const std::vector<F>& enc, const SetupShape& s) {
   }
   return tree_from_leaves(std::move(leaves));
 }
+
+// Device acceleration of the setup commitments: encode_level fills a
+// level's encoded matrix (column-major, encoded_rows x h_cols) and its row
+// leaves (hash_setup_row), or returns false to leave the level to the host.
+template <class F>
+struct SetupAccel {
+  virtual ~SetupAccel() {}
+  virtual bool encode_level(const QaCode<F>& target, const QaCode<F>& current, size_t row_factor, const SetupShape& shape,
+                            std::vector<F>& encoded, std::vector<Digest>& leaves) = 0;
+};
 
 template <class F>
 struct PcsParams {
@@ -338,7 +370,8 @@ double cardinality_log2() {
 
 // ShortQaFoldPC::new_with_recursive_index + setup (qafold_short_pc.rs:358-444).
 template <class F>
-std::unique_ptr<PcsParams<F>> pcs_setup(size_t n_witness, size_t extension_columns, size_t security_bits, StdRng& rng) {
+std::unique_ptr<PcsParams<F>> pcs_setup(size_t n_witness, size_t extension_columns, size_t security_bits, StdRng& rng,
+                                        SetupAccel<F>* accel = nullptr) {
   auto pp = std::make_unique<PcsParams<F>>();
   pp->card_log2 = cardinality_log2<F>();
   size_t capacity_bits = size_t(std::floor(pp->card_log2 * 1.0));
@@ -383,15 +416,22 @@ std::unique_ptr<PcsParams<F>> pcs_setup(size_t n_witness, size_t extension_colum
     sl->shape.message_rows = target.message_len;
     sl->shape.h_cols = current.alphas.size() * row_factor;
     sl->shape.validate();
-    const size_t er = sl->shape.encoded_rows, mr = sl->shape.message_rows;
-    sl->encoded.assign(er * sl->shape.h_cols, F::zero());
+    std::vector<Digest> leaves;
+    if (accel && accel->encode_level(target, current, row_factor, sl->shape, sl->encoded, leaves)) {
+      if (sl->encoded.size() != sl->shape.encoded_rows * sl->shape.h_cols || leaves.size() != sl->shape.encoded_rows)
+        fail(QF_E_ENCODING, "device setup level");
+      sl->tree = tree_from_leaves(std::move(leaves));
+    } else {
+      const size_t er = sl->shape.encoded_rows, mr = sl->shape.message_rows;
+      sl->encoded.assign(er * sl->shape.h_cols, F::zero());
 #pragma omp parallel for schedule(dynamic)
-    for (long col = 0; col < long(sl->shape.h_cols); ++col) {
-      const auto& alpha = current.alphas[col / row_factor];
-      size_t block = col % row_factor;
-      target.encode_into(alpha.data() + block * mr, sl->encoded.data() + col * er);
+      for (long col = 0; col < long(sl->shape.h_cols); ++col) {
+        const auto& alpha = current.alphas[col / row_factor];
+        size_t block = col % row_factor;
+        target.encode_into(alpha.data() + block * mr, sl->encoded.data() + col * er);
+      }
+      sl->tree = build_setup_tree<F>(sl->encoded, sl->shape);
     }
-    sl->tree = build_setup_tree<F>(sl->encoded, sl->shape);
     sl->root = sl->tree.root();
     pp->setup[level] = std::move(sl);
   }

@@ -544,7 +544,8 @@ struct Parameters {
 };
 
 template <class F>
-std::unique_ptr<Parameters<F>> make_parameters(const std::vector<Shape>& shapes, const Config& config) {
+std::unique_ptr<Parameters<F>> make_parameters(const std::vector<Shape>& shapes, const Config& config,
+                                               SetupAccel<F>* accel = nullptr) {
   check(config.chunk_log >= 10 && config.chunk_log <= 30 && config.packed_log >= 1 && config.packed_log <= 6 &&
             config.query_rf_bits >= 32 && config.query_rf_bits <= 120,
         "invalid ParComm config");
@@ -556,7 +557,7 @@ std::unique_ptr<Parameters<F>> make_parameters(const std::vector<Shape>& shapes,
   check(p->layout.logical / p->block_len <= 128, "at most 128 PCS blocks are supported");
   std::array<uint8_t, 32> seed;
   seed.fill(0x51);
-  p->pcs = PackedPcs<F>::create(chunk_log, 32, config.query_rf_bits, seed);
+  p->pcs = PackedPcs<F>::create(chunk_log, 32, config.query_rf_bits, seed, accel);
   return p;
 }
 

@@ -786,6 +786,53 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_wht_alpha_wht_tile(const Fe
 }
 
 // ---------------------------------------------------------------- hashing
+// Setup-row leaves (hash_setup_row; qafold_short_setup.rs:655-897): one
+// thread per row hashes the framed prefix tail, the framed row index and
+// the row's n_cols elements, entry (c, r) at cw[c * n_rows + r].  The message
+// is assembled byte by byte; the setup is built once per parameter set,
+// outside any proof.
+__global__ void k_hash_setup_rows(const Fe* __restrict__ cw, uint64_t n_rows, int n_cols, ::qfd::SetupLeafPrefix pf,
+                                  uint4* __restrict__ leaves) {
+  const uint64_t row = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  uint32_t h[8], m[16];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) h[i] = pf.mid[i];
+  uint32_t t = pf.t0;
+  int fill = 0;
+  auto push = [&](uint32_t b) {
+    if (fill == 64) {  // a full block is compressed once more input arrives
+      t += 64;
+      ::qfd::compress(h, m, t, false, pf.one);
+      fill = 0;
+    }
+    const int w = fill >> 2, sh = 8 * (fill & 3);
+    m[w] = sh ? (m[w] | (b << sh)) : b;
+    ++fill;
+  };
+  for (uint32_t i = 0; i < pf.n_tail; ++i) push((pf.tail[i >> 2] >> (8 * (i & 3))) & 0xffu);
+  // framed "row": u64(3) || "row" || u64(8) || u64(row)
+  push(3u);
+  for (int i = 0; i < 7; ++i) push(0u);
+  push('r');
+  push('o');
+  push('w');
+  push(8u);
+  for (int i = 0; i < 7; ++i) push(0u);
+  for (int i = 0; i < 8; ++i) push(uint32_t(row >> (8 * i)) & 0xffu);
+  for (int c = 0; c < n_cols; ++c) {
+    const uint4 u = *reinterpret_cast<const uint4*>(cw + uint64_t(c) * n_rows + row);
+    const uint32_t wd[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int k = 0; k < 16; ++k) push((wd[k >> 2] >> (8 * (k & 3))) & 0xffu);
+  }
+  t += uint32_t(fill);
+  for (int w = (fill + 3) >> 2; w < 16; ++w) m[w] = 0u;
+  ::qfd::compress(h, m, t, true, pf.one);
+  leaves[2 * row] = make_uint4(h[0], h[1], h[2], h[3]);
+  leaves[2 * row + 1] = make_uint4(h[4], h[5], h[6], h[7]);
+}
+
 constexpr int kLeafThreads = 64;
 constexpr int kRowWords = 128;  // 32 entries x 4 words
 constexpr int kRowStride = 129;  // padded: conflict-free per-thread rows

@@ -393,3 +393,32 @@ def test_greedy_pass_plan_runs_the_depth8_stage():
     r = subprocess.run([sys.executable, "-c", code], cwd=root, env=dict(os.environ, QF_TUNE="0"),
                        capture_output=True, timeout=900)
     assert r.returncode == 0 and b"greedy-ok" in r.stdout, r.stderr.decode()[-3000:]
+
+
+def test_device_setup_levels_chunk26():
+    """Chunk 26 is the smallest block whose top setup level (2^14 encoded rows
+    x 64 columns) is encoded and hashed on the device; the proof, which
+    absorbs the parameter digest, equals the oracle's host-built one."""
+    rng = np.random.default_rng(26)
+    mats = [gaussian_i8(rng, 8192 * 8192, forced=0.001).reshape(8192, 8192)]
+    run_both([(8192, 8192)], 26, 4, mats)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+@pytest.mark.parametrize("chunk_log", [26, 28, 30])
+def test_device_setup_digest_equals_host_setup(field, chunk_log):
+    """The parameter digest of a device-built setup equals the one a process
+    without a visible device builds on the host."""
+    import os
+    import subprocess
+    import sys
+    shapes = [(1 << 15, 1 << 15)]
+    p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=4), field=FIELDS[field])
+    code = ("import parcomm_b200 as qf; "
+            f"p = qf.Parameters({shapes!r}, qf.Config(chunk_log={chunk_log}, packed_log=4), field={FIELDS[field]!r}); "
+            "print(p.parameter_digest.hex())")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600,
+                         cwd=str(__import__("pathlib").Path(__file__).resolve().parents[1]))
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.strip() == p.parameter_digest.hex()
