@@ -1748,22 +1748,25 @@ void GpuBackend::eo_round_fold(F inv, F ch) {
   }
   const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
   if (n >= (uint64_t(1) << 26)) {
-    // Large rounds fold the two vectors one after the other: the full-length
-    // witness goes back to the pool before the query's output is allocated,
-    // so the round holds 2.5 rather than 3 vector lengths.
-    DBuf<Fe> w2(n / 2);
-    QF_LAUNCH(s_, "k_eo_fold_vec", n * 24, qfd::k_eo_fold_vec<<<grid_for(n / 2, kThreads), kThreads, 0, s_>>>(wit_.p, n, to_fe(inv), w2.p));
-    wit_ = std::move(w2);
-    DBuf<Fe> q2(n / 2);
+    // Large rounds fold the two vectors one after the other through one
+    // spare buffer (wit2_, n/2 entries at the first large round): the
+    // witness folds into the spare, its old buffer becomes the spare and
+    // takes the folded query, and the query's old buffer becomes the spare.
+    // The rounds hold 2.5 vector lengths and allocate nothing after the
+    // first (a nearly full HBM would otherwise evict and re-allocate).
+    if (wit2_.n < n / 2) wit2_.alloc(n / 2);
+    QF_LAUNCH(s_, "k_eo_fold_vec", n * 24, qfd::k_eo_fold_vec<<<grid_for(n / 2, kThreads), kThreads, 0, s_>>>(wit_.p, n, to_fe(inv), wit2_.p));
+    std::swap(wit_, wit2_);
     if (tc_dots())
       QF_LAUNCH(s_, "k_eo_fold_query_cross_mma", n * 32,
                 qfd::k_eo_fold_query_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch),
-                                                                                             q2.p, partials_.p));
+                                                                                             wit2_.p, partials_.p));
     else
-      QF_LAUNCH(s_, "k_eo_fold_query_cross", n * 32, qfd::k_eo_fold_query_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch), q2.p, partials_.p));
-    qv_ = std::move(q2);
+      QF_LAUNCH(s_, "k_eo_fold_query_cross", n * 32, qfd::k_eo_fold_query_cross<<<g, kThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch), wit2_.p, partials_.p));
+    std::swap(qv_, wit2_);
   } else {
-    if (wit2_.n < n / 2) { wit2_.alloc(n / 2); qv2_.alloc(n / 2); }
+    if (wit2_.n < n / 2) wit2_.alloc(n / 2);
+    if (qv2_.n < n / 2) qv2_.alloc(n / 2);
     if (tc_dots() && n >= 4)
       QF_LAUNCH(s_, "k_eo_fold_cross_mma", n * 48,
                 qfd::k_eo_fold_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv),
