@@ -659,6 +659,7 @@ bool DeviceSetup::encode_level(const QaCode<F>& target, const QaCode<F>& current
       hc > current.alphas.size() * rf)
     return false;
   check(ilog2(mr * hc) <= 30, "setup level size");
+  configure_tile_kernels();  // the setup may be a process's first device work
   cudaStream_t s;
   QF_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   {

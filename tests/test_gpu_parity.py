@@ -408,17 +408,22 @@ def test_device_setup_levels_chunk26():
 @pytest.mark.parametrize("chunk_log", [26, 28, 30])
 def test_device_setup_digest_equals_host_setup(field, chunk_log):
     """The parameter digest of a device-built setup equals the one a process
-    without a visible device builds on the host."""
+    without a visible device builds on the host; the device setup also runs
+    as a fresh process's first device work."""
     import os
     import subprocess
     import sys
+    from pathlib import Path
     shapes = [(1 << 15, 1 << 15)]
     p = qf.Parameters(shapes, qf.Config(chunk_log=chunk_log, packed_log=4), field=FIELDS[field])
     code = ("import parcomm_b200 as qf; "
             f"p = qf.Parameters({shapes!r}, qf.Config(chunk_log={chunk_log}, packed_log=4), field={FIELDS[field]!r}); "
             "print(p.parameter_digest.hex())")
-    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
-    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600,
-                         cwd=str(__import__("pathlib").Path(__file__).resolve().parents[1]))
-    assert out.returncode == 0, out.stderr[-2000:]
-    assert out.stdout.strip() == p.parameter_digest.hex()
+    root = str(Path(__file__).resolve().parents[1])
+    for visible in ("", None):
+        env = dict(os.environ)
+        if visible is not None:
+            env["CUDA_VISIBLE_DEVICES"] = visible
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600, cwd=root)
+        assert out.returncode == 0, out.stderr[-2000:]
+        assert out.stdout.strip() == p.parameter_digest.hex()
