@@ -156,7 +156,7 @@ static void configure_tile_kernels() {
   set_smem(qfd::k_wht_tile<true>, bytes);
   set_smem(qfd::k_butterfly_strided<qfd::kMobius>, bytes);
   set_smem(qfd::k_butterfly_strided<qfd::kWht>, bytes);
-  set_smem(qfd::k_mobius_wht_strided, bytes);
+  set_smem(qfd::k_mobius_wht_strided, bytes + qfd::kPrefetchSmem);
   set_smem(qfd::k_wht_alpha_wht_tile, bytes + qfd::kAlphaStageSmem);
 #if !defined(QF_FIELD_KB)
   // 38 KiB of static shared memory plus the 32 KiB weight double buffer.
@@ -553,7 +553,7 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
     const uint32_t tiles = uint32_t(uint64_t(1) << (logm - k - cb));
     launch(s, timed, "k_mobius_wht_strided", (uint64_t(3) << logm) * 16,
            qf_intops::transform_ops(kOps, uint64_t(1) << logm, k, k, 2, 0), [&] {
-             qfd::k_mobius_wht_strided<<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem, s>>>(cw, uint32_t(R), logR,
+             qfd::k_mobius_wht_strided<<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem + qfd::kPrefetchSmem, s>>>(cw, uint32_t(R), logR,
                                                                                                  kT, k, cb, tiles);
            });
   } else {

@@ -667,32 +667,49 @@ __device__ __forceinline__ void fused_middle(uint32_t* planes, int b0, int lvl0)
 // stores (consecutive threads take consecutive elements, as the loads).
 // stage(tile) runs first in each tile (to issue its cp.async side loads,
 // which each thread then waits for before the first planar stage's barrier).
-// The next tile's loads are issued after mid, so their registers are not live
-// across it.
-template <int OP1, int OP2, class Raw, class Fetch, class Conv, class Stage, class Mid, class St>
-__device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32_t n_tiles, Fetch fetch, Conv conv,
+// The tile's 16-byte elements (src(tile, t)) arrive by cp.async in a staging
+// area of kPrefetchSmem bytes after the planes: thread g copies elements
+// g + (j << 9) and reads back only its own copies, so the next tile's copies
+// are issued right after the head and land while the rest of the tile runs,
+// without holding registers.  Commit groups per tile: the side loads and an
+// always-present group closing them, then the next tile's elements.
+constexpr size_t kPrefetchSmem = size_t(1) << kMaxTileLog << 4;  // 64 KiB
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(src) : "memory");
+}
+template <int OP1, int OP2, class Src, class Conv, class Stage, class Mid, class St>
+__device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32_t n_tiles, Src src, Conv conv,
                                                 Stage stage, Mid mid, St st) {
   const int g = threadIdx.x;
   const int rm = 6 - b0;
   const int tb = (g & 63) | ((g >> 6) << 9);  // the tail group: elements tb + (j << 6)
-  Raw raw[8];
+  uint4* pre = reinterpret_cast<uint4*>(planes + kC * kPlane);
   uint32_t tile = blockIdx.x;
   if (tile < n_tiles)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+    for (int j = 0; j < 8; ++j) cp_async16(pre + g + (j << 9), src(tile, g + (j << 9)));
+  asm volatile("cp.async.commit_group;" ::: "memory");
   for (; tile < n_tiles; tile += gridDim.x) {
     stage(tile);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this tile's elements (and older groups) have landed
     {
       uint32_t v[8][kC];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const Fr e = conv(tile, g + (j << 9), raw[j]);
+        const Fr e = conv(tile, g + (j << 9), pre[g + (j << 9)]);
 #pragma unroll
         for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
       }
       head_levels<OP1>(planes, v);
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    const uint32_t next = tile + gridDim.x;
+    if (next < n_tiles)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) cp_async16(pre + g + (j << 9), src(next, g + (j << 9)));
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 1;" ::: "memory");  // the side loads; the next tile's copies may pend
     if (rm > 0) fused_middle<OP1>(planes, b0, 3);
     else __syncthreads();
     {
@@ -719,10 +736,6 @@ __device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32
       // until the barrier below.
       regs_to_planes<3>(planes, tb, 6, v);
     }
-    const uint32_t next = tile + gridDim.x;
-    if (next < n_tiles)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
     __syncthreads();
     if (rm > 0) fused_middle<OP2>(planes, b0, 3);
     auto st_t = [&](int t, uint4 u) { st(tile, t, u); };
@@ -738,9 +751,7 @@ __device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32
 __global__ void __launch_bounds__(kTileThreads, 1) k_mobius_wht_strided(Fe* cw, uint32_t R, int logR, int lo, int k, int cb,
                                                                        uint32_t n_tiles) {
   extern __shared__ uint32_t planes_s[];
-  auto fetch = [=](uint32_t tile, int t) {
-    return *reinterpret_cast<const uint4*>(cw + strided_addr(tile, t, logR, lo, k, cb));
-  };
+  auto src = [=](uint32_t tile, int t) -> const void* { return cw + strided_addr(tile, t, logR, lo, k, cb); };
   auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
   auto stage = [](uint32_t) {};
   auto mid = [=](uint32_t tile, int t, Fr& v) {
@@ -749,7 +760,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_mobius_wht_strided(Fe* cw, 
   auto st = [=](uint32_t tile, int t, uint4 u) {
     *reinterpret_cast<uint4*>(cw + R + strided_addr(tile, t, logR, lo, k, cb)) = u;
   };
-  tile_loop_fused<kMobius, kWht, uint4>(planes_s, cb, n_tiles, fetch, conv, stage, mid, st);
+  tile_loop_fused<kMobius, kWht>(planes_s, cb, n_tiles, src, conv, stage, mid, st);
 }
 
 // The parity tile pass: the first WHT's levels 0..11 of each column (read at
