@@ -171,11 +171,12 @@ int qf_kernel_int_peaks(double out[6]);
  * contract on the tensor cores with exact integer limbs instead of the dp4a
  * / IMAD kernels (measured slower on B200; kept for the comparison).  "per_matrix"
  * (default 0): 1 issues the weight passes one launch per term, bucket or
- * block instead of one launch over all of them.  "core_dots" (default 0): 1
- * sums the extension products of the EO binary rounds, the sumcheck
- * messages and the LiteBullet rounds with CUDA-core multiply-adds instead
- * of exact integer-limb tensor-core products.  Set it between calls, not
- * while another call runs. */
+ * block instead of one launch over all of them.  "core_dots" chooses where
+ * the sums of extension products of the EO binary rounds, the sumcheck
+ * messages and the LiteBullet rounds run: 0 (default) per kernel, as
+ * measured fastest on B200; 1 all with CUDA-core multiply-adds; 2 all as
+ * exact integer-limb tensor-core products.  Set it between calls, not while
+ * another call runs. */
 int qf_kernel_option(const char* name, int value);
 
 /* Device buffers released by the library are cached for reuse (no cudaMalloc

@@ -184,7 +184,10 @@ int qf_kernel_option(const char* name, int value) {
     const std::string n = name ? name : "";
     if (n == "imma") qfg::KernelOptions::imma = value != 0;
     else if (n == "per_matrix") qfg::KernelOptions::per_matrix = value != 0;
-    else if (n == "core_dots") qfg::KernelOptions::core_dots = value != 0;
+    else if (n == "core_dots") {
+      if (value < 0 || value > 2) fail(QF_E_ARGUMENT, "core_dots takes 0, 1 or 2");
+      qfg::KernelOptions::core_dots = value;
+    }
     else fail(QF_E_ARGUMENT, "unknown kernel option: " + n);
   });
 }

@@ -39,9 +39,24 @@ static bool imma_on() {
   return KernelOptions::imma.load() != 0;
 #endif
 }
-// The extension-product sums of the EO, sumcheck and LiteBullet rounds run
-// on the tensor cores (kernels/dot_mma.cuh) unless core_dots is set.
-static bool tc_dots() { return KernelOptions::core_dots.load() == 0; }
+// The extension-product sums of the EO, sumcheck and LiteBullet rounds:
+// on the tensor cores (kernels/dot_mma.cuh) where that measured faster on
+// B200 in the 8B-shape step, on the CUDA cores elsewhere (core_dots 0);
+// core_dots 1 takes the CUDA cores everywhere, 2 the tensor cores
+// everywhere.  The tensor-core sums win where the sum is the work (EO dot and
+// first cross pair 1.9x / 1.7x, sumcheck message 1.75x / 1.5x for F65521 /
+// KoalaBear); where a fold's scalar products dominate, or the vectors are
+// short, the chunked warp loop and its staging cost more than they save.
+enum class Dots { kEoDotCross, kEoFoldQueryCross, kEoFoldCross, kSumMessage, kSumFold, kLbCross, kLbFold, kDot };
+static bool tc_dots(Dots k) {
+  const int opt = KernelOptions::core_dots.load();
+  if (opt != 0) return opt == 2;
+#if defined(QF_FIELD_KB)
+  return k == Dots::kEoDotCross || k == Dots::kSumMessage || k == Dots::kLbCross;
+#else
+  return k == Dots::kEoDotCross || k == Dots::kEoFoldQueryCross || k == Dots::kSumMessage || k == Dots::kSumFold;
+#endif
+}
 // Grid of the persistent tensor-core weight kernels: four CTAs per SM.
 static unsigned mma_grid() {
   static const int sms = [] {
@@ -1062,7 +1077,7 @@ void GpuBackend::sumcheck_message(F m[2]) {
   }
   if (!msg_valid_) {
     const int g = grid_for(sum_len_ / 2, kThreads);
-    if (tc_dots())
+    if (tc_dots(Dots::kSumMessage))
       QF_LAUNCH(s_, "k_sum_message_mma", sum_len_ * 32,
                 qfd::k_sum_message_mma<<<dot_grid(sum_len_ / 2), qfd::kDotThreads, 0, s_>>>(values_.p, weights_.p, sum_len_,
                                                                                              partials_.p));
@@ -1092,7 +1107,7 @@ void GpuBackend::sumcheck_fold(F ch) {
   }
   if (tmp_v_.n < sum_len_ / 2) { tmp_v_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); tmp_w_.alloc(std::max<uint64_t>(sum_len_ / 2, 1)); }
   const int g = grid_for(std::max<uint64_t>(sum_len_ / 4, 1), kThreads);
-  if (tc_dots() && sum_len_ >= 4)
+  if (tc_dots(Dots::kSumFold) && sum_len_ >= 4)
     QF_LAUNCH(s_, "k_sum_fold_message_mma", sum_len_ * 48,
               qfd::k_sum_fold_message_mma<<<dot_grid(sum_len_ / 4), qfd::kDotThreads, 0, s_>>>(
                   values_.p, weights_.p, sum_len_, to_fe(ch), tmp_v_.p, tmp_w_.p, partials_.p));
@@ -1716,7 +1731,7 @@ F GpuBackend::eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t st
     QF_CK(cudaStreamSynchronize(s_));
   }
   const int g = grid_for(std::max<uint64_t>(rows / 2, 1), kThreads);
-  if (tc_dots())
+  if (tc_dots(Dots::kEoDotCross))
     QF_LAUNCH(s_, "k_eo_dot_cross_mma", rows * 32,
               qfd::k_eo_dot_cross_mma<<<dot_grid(rows / 2), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, rows, partials_.p));
   else
@@ -1758,7 +1773,7 @@ void GpuBackend::eo_round_fold(F inv, F ch) {
     if (wit2_.n < n / 2) wit2_.alloc(n / 2);
     QF_LAUNCH(s_, "k_eo_fold_vec", n * 24, qfd::k_eo_fold_vec<<<grid_for(n / 2, kThreads), kThreads, 0, s_>>>(wit_.p, n, to_fe(inv), wit2_.p));
     std::swap(wit_, wit2_);
-    if (tc_dots())
+    if (tc_dots(Dots::kEoFoldQueryCross))
       QF_LAUNCH(s_, "k_eo_fold_query_cross_mma", n * 32,
                 qfd::k_eo_fold_query_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(ch),
                                                                                              wit2_.p, partials_.p));
@@ -1768,7 +1783,7 @@ void GpuBackend::eo_round_fold(F inv, F ch) {
   } else {
     if (wit2_.n < n / 2) wit2_.alloc(n / 2);
     if (qv2_.n < n / 2) qv2_.alloc(n / 2);
-    if (tc_dots() && n >= 4)
+    if (tc_dots(Dots::kEoFoldCross) && n >= 4)
       QF_LAUNCH(s_, "k_eo_fold_cross_mma", n * 48,
                 qfd::k_eo_fold_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(wit_.p, qv_.p, n, to_fe(inv),
                                                                                        to_fe(ch), wit2_.p, qv2_.p,
@@ -1823,7 +1838,7 @@ void GpuBackend::wht_dev(Fe* v, int logn, const Fe* alpha) {
 }
 
 F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {
-  if (tc_dots()) {
+  if (tc_dots(Dots::kDot)) {
     QF_LAUNCH(s_, "k_dot_mma", n * 32, qfd::k_dot_mma<<<dot_grid(n), qfd::kDotThreads, 0, s_>>>(a, b, n, partials_.p));
     return reduce_to_host(partials_, 0, 1)[0];
   }
@@ -1834,7 +1849,7 @@ F GpuBackend::dot_dev(const Fe* a, const Fe* b, uint64_t n) {
 
 std::array<F, 2> GpuBackend::lb_cross(const Fe* L, const Fe* R, uint64_t n) {
   const int g = grid_for(std::max<uint64_t>(n / 2, 1), kThreads);
-  if (tc_dots())
+  if (tc_dots(Dots::kLbCross))
     QF_LAUNCH(s_, "k_lb_cross_mma", n * 32, qfd::k_lb_cross_mma<<<dot_grid(n / 2), qfd::kDotThreads, 0, s_>>>(L, R, n, partials_.p));
   else
     QF_LAUNCH(s_, "k_lb_cross", n * 32, qfd::k_lb_cross<<<g, kThreads, 0, s_>>>(L, R, n, partials_.p));
@@ -1887,7 +1902,7 @@ LiteBullet<F> GpuBackend::litebullet_dev(F claimed, Fe* L, Fe* R, uint64_t n, Pc
       continue;
     }
     const int g = grid_for(std::max<uint64_t>(n / 4, 1), kThreads);
-    if (tc_dots() && n >= 4)
+    if (tc_dots(Dots::kLbFold) && n >= 4)
       QF_LAUNCH(s_, "k_lb_fold_cross_mma", n * 48,
                 qfd::k_lb_fold_cross_mma<<<dot_grid(n / 4), qfd::kDotThreads, 0, s_>>>(L, R, n, to_fe(inv), to_fe(ch),
                                                                                        partials_.p));

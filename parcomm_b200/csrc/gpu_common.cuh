@@ -33,9 +33,10 @@ using namespace qf;
 // integer limbs) instead of the dp4a / IMAD kernels (off by default: slower
 // as measured on B200); `per_matrix` issues the
 // weight passes one launch per term, bucket or block instead of one launch
-// over all of them; `core_dots` sums the extension products of the EO,
-// sumcheck and LiteBullet rounds with CUDA-core 64-bit multiply-adds instead
-// of the tensor cores (off by default).  Set through qf_kernel_option.
+// over all of them; `core_dots` chooses where the extension-product sums of
+// the EO, sumcheck and LiteBullet rounds run: 0 (default) per kernel as
+// measured fastest, 1 all on the CUDA cores, 2 all on the tensor cores.  Set
+// through qf_kernel_option.
 struct KernelOptions {
   static std::atomic<int> imma;
   static std::atomic<int> per_matrix;

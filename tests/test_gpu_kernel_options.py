@@ -1,5 +1,6 @@
-"""Every kernel choice writes the same bytes: the tensor-core extension-product
-sums (default) against the CUDA-core kernels (core_dots), the tensor-core
+"""Every kernel choice writes the same bytes: the extension-product sums per
+kernel as measured fastest (default), all on the CUDA cores and all on the
+tensor cores (core_dots 1, 2), the tensor-core
 weight passes (imma, F65521) and the per-matrix launch sequence, each
 compared with the CPU oracle's proof.  Requires a B200."""
 import numpy as np
@@ -13,7 +14,7 @@ from test_gpu_parity import FIELDS, gaussian_i8, gaussian_i16
 
 pytestmark = pytest.mark.gpu
 
-OPTIONS = [{}, {"core_dots": 1}, {"imma": 1}, {"per_matrix": 1}, {"core_dots": 1, "per_matrix": 1}]
+OPTIONS = [{}, {"core_dots": 1}, {"core_dots": 2}, {"imma": 1}, {"per_matrix": 1}, {"core_dots": 2, "per_matrix": 1}]
 
 
 def prove_with(p, bva, options):
@@ -52,3 +53,5 @@ def test_kernel_options_write_oracle_bytes(field, chunk_log):
 def test_unknown_kernel_option_is_an_error():
     with pytest.raises(qf.QfError):
         qf.kernel_option("no_such_option", 1)
+    with pytest.raises(qf.QfError):
+        qf.kernel_option("core_dots", 3)
