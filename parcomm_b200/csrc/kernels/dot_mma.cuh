@@ -128,20 +128,34 @@ __device__ __forceinline__ void dot_flush(DotAcc& acc, Fr& out) {
 }
 
 // The warp-chunked loop of the tensor-core kernels.  Chunk c covers indices
-// [32c, 32c + 32) and lane j takes index 32c + j.  load(i, valid, x) fills
-// the NX staged operands of index i (zero when !valid) and performs the
-// kernel's own stores; step(f) issues the chunk's products from the
-// fragments; flush() moves the s32 sums out every kDotFlush chunks and once
-// at the end.  Every lane of a warp runs the same chunks (mma.sync).
-template <int NX, class Load, class Step, class Flush>
-__device__ __forceinline__ void dot_loop(uint32_t* s, uint64_t count, Load load, Step step, Flush flush) {
+// [32c, 32c + 32) and lane j takes index 32c + j.  fetch(i, ok, r) loads the
+// NR raw inputs of index i (zero when !ok); make(i, ok, r, x) forms the NX
+// staged operands from them and performs the kernel's own stores; step(f)
+// issues the chunk's products from the fragments; flush() moves the s32
+// sums out every kDotFlush chunks and once at the end.  The next chunk's
+// fetch is issued before the current chunk's staging and products, so its
+// loads are in flight meanwhile.  Every lane of a warp runs the same chunks
+// (mma.sync).
+template <int NX, int NR, class Fetch, class Make, class Step, class Flush>
+__device__ __forceinline__ void dot_loop(uint32_t* s, uint64_t count, Fetch fetch, Make make, Step step, Flush flush) {
   const int lane = threadIdx.x & 31;
   const uint64_t nw = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  uint64_t c = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  uint4 r[NR];
+  if (c * 32 < count) {
+    const uint64_t i = c * 32 + uint64_t(lane);
+    fetch(i, i < count, r);
+  }
   int since = 0;
-  for (uint64_t c = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; c * 32 < count; c += nw) {
+  for (; c * 32 < count; c += nw) {
     const uint64_t i = c * 32 + uint64_t(lane);
     uint4 x[NX];
-    load(i, i < count, x);
+    make(i, i < count, r, x);
+    const uint64_t cn = c + nw;
+    if (cn * 32 < count) {
+      const uint64_t in = cn * 32 + uint64_t(lane);
+      fetch(in, in < count, r);
+    }
     __syncwarp();  // the previous chunk's fragments are read
 #pragma unroll
     for (int k = 0; k < NX; ++k) dot_put(s, k, lane, x[k]);
@@ -160,29 +174,38 @@ __device__ __forceinline__ void dot_loop(uint32_t* s, uint64_t count, Load load,
 
 __device__ __forceinline__ uint4 ld4(const Fe* p) { return *reinterpret_cast<const uint4*>(p); }
 __device__ __forceinline__ uint4 zero4() { return make_uint4(0u, 0u, 0u, 0u); }
+// r[k] = ok ? p[k](index) : 0 for each of the N pointers.
+template <int N>
+__device__ __forceinline__ void fetch_n(bool ok, uint4 (&r)[N], const Fe* const (&p)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) r[k] = ok ? ld4(p[k]) : zero4();
+}
+template <int N>
+__device__ __forceinline__ void copy_n(const uint4 (&r)[N], uint4 (&x)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) x[k] = r[k];
+}
+__device__ __forceinline__ Fr fr(uint4 u) { return unpack_fe(u); }
 
 // ---------------------------------------------------------------- kernels
 // sum a_i b_i (k_dot).
-__global__ void __launch_bounds__(kDotThreads) k_dot_mma(const Fe* __restrict__ a, const Fe* __restrict__ b, uint64_t n,
+__global__ void __launch_bounds__(kDotThreads, 2) k_dot_mma(const Fe* __restrict__ a, const Fe* __restrict__ b, uint64_t n,
                                                          Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][2 * kDotStride];
   uint32_t* s = stage_s[threadIdx.x >> 5];
   DotAcc acc;
   dot_clear(acc);
   Fr v[1] = {zero()};
-  dot_loop<2>(
-      s, n,
-      [&](uint64_t i, bool ok, uint4 (&x)[2]) {
-        x[0] = ok ? ld4(a + i) : zero4();
-        x[1] = ok ? ld4(b + i) : zero4();
-      },
+  dot_loop<2, 2>(
+      s, n, [&](uint64_t i, bool ok, uint4 (&r)[2]) { fetch_n<2>(ok, r, {a + i, b + i}); },
+      [&](uint64_t, bool, const uint4 (&r)[2], uint4 (&x)[2]) { copy_n<2>(r, x); },
       [&](const DotFrag (&f)[2]) { dot_mma(acc, f[0], f[1]); }, [&] { dot_flush(acc, v[0]); });
   block_reduce<1>(v);
   finish_reduction<1>(v, partials);
 }
 
 // LiteBullet cross pair of (L, R) with half h: sum L[i] R[h+i], sum L[h+i] R[i] (k_lb_cross).
-__global__ void __launch_bounds__(kDotThreads) k_lb_cross_mma(const Fe* __restrict__ L, const Fe* __restrict__ R, uint64_t n,
+__global__ void __launch_bounds__(kDotThreads, 2) k_lb_cross_mma(const Fe* __restrict__ L, const Fe* __restrict__ R, uint64_t n,
                                                               Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
   uint32_t* s = stage_s[threadIdx.x >> 5];
@@ -191,14 +214,9 @@ __global__ void __launch_bounds__(kDotThreads) k_lb_cross_mma(const Fe* __restri
   dot_clear(acc[0]);
   dot_clear(acc[1]);
   Fr v[2] = {zero(), zero()};
-  dot_loop<4>(
-      s, h,
-      [&](uint64_t i, bool ok, uint4 (&x)[4]) {
-        x[0] = ok ? ld4(L + i) : zero4();
-        x[1] = ok ? ld4(L + h + i) : zero4();
-        x[2] = ok ? ld4(R + i) : zero4();
-        x[3] = ok ? ld4(R + h + i) : zero4();
-      },
+  dot_loop<4, 4>(
+      s, h, [&](uint64_t i, bool ok, uint4 (&r)[4]) { fetch_n<4>(ok, r, {L + i, L + h + i, R + i, R + h + i}); },
+      [&](uint64_t, bool, const uint4 (&r)[4], uint4 (&x)[4]) { copy_n<4>(r, x); },
       [&](const DotFrag (&f)[4]) {
         dot_mma(acc[0], f[0], f[3]);
         dot_mma(acc[1], f[1], f[2]);
@@ -213,36 +231,36 @@ __global__ void __launch_bounds__(kDotThreads) k_lb_cross_mma(const Fe* __restri
 
 // L[i] += L[h+i] * wl, R[i] += R[h+i] * wr for i < h = n/2, in place, and the
 // cross pair of the folded length-h vectors (k_lb_fold_cross).  Index i < n/4
-// owns positions {i, i + n/4, i + n/2, i + 3n/4}; n >= 4.
-__global__ void __launch_bounds__(kDotThreads) k_lb_fold_cross_mma(Fe* __restrict__ L, Fe* __restrict__ R, uint64_t n, Fe wl,
+// owns positions {i, i + n/4, i + n/2, i + 3n/4} (so the prefetch of a later
+// chunk never reads a position this chunk writes); n >= 4.
+__global__ void __launch_bounds__(kDotThreads, 2) k_lb_fold_cross_mma(Fe* __restrict__ L, Fe* __restrict__ R, uint64_t n, Fe wl,
                                                                    Fe wr, Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
   uint32_t* s = stage_s[threadIdx.x >> 5];
-  const Fr fl = load(&wl), fr = load(&wr);
+  const Fr fl = load(&wl), fw = load(&wr);
   const uint64_t h = n / 2, q = n / 4;
   DotAcc acc[2];
   dot_clear(acc[0]);
   dot_clear(acc[1]);
   Fr v[2] = {zero(), zero()};
-  dot_loop<4>(
+  dot_loop<4, 8>(
       s, q,
-      [&](uint64_t i, bool ok, uint4 (&x)[4]) {
-        if (!ok) {
-          x[0] = x[1] = x[2] = x[3] = zero4();
-          return;
-        }
-        const Fr l0 = add(load(L + i), mul(load(L + i + h), fl));
-        const Fr l1 = add(load(L + i + q), mul(load(L + i + q + h), fl));
-        const Fr r0 = add(load(R + i), mul(load(R + i + h), fr));
-        const Fr r1 = add(load(R + i + q), mul(load(R + i + q + h), fr));
-        store(L + i, l0);
-        store(L + i + q, l1);
-        store(R + i, r0);
-        store(R + i + q, r1);
+      [&](uint64_t i, bool ok, uint4 (&r)[8]) {
+        fetch_n<8>(ok, r, {L + i, L + i + h, L + i + q, L + i + q + h, R + i, R + i + h, R + i + q, R + i + q + h});
+      },
+      [&](uint64_t i, bool ok, const uint4 (&r)[8], uint4 (&x)[4]) {
+        const Fr l0 = add(fr(r[0]), mul(fr(r[1]), fl)), l1 = add(fr(r[2]), mul(fr(r[3]), fl));
+        const Fr r0 = add(fr(r[4]), mul(fr(r[5]), fw)), r1 = add(fr(r[6]), mul(fr(r[7]), fw));
         x[0] = pack_fe(l0);
         x[1] = pack_fe(l1);
         x[2] = pack_fe(r0);
         x[3] = pack_fe(r1);
+        if (ok) {
+          *reinterpret_cast<uint4*>(L + i) = x[0];
+          *reinterpret_cast<uint4*>(L + i + q) = x[1];
+          *reinterpret_cast<uint4*>(R + i) = x[2];
+          *reinterpret_cast<uint4*>(R + i + q) = x[3];
+        }
       },
       [&](const DotFrag (&f)[4]) {
         dot_mma(acc[0], f[0], f[3]);
@@ -258,7 +276,7 @@ __global__ void __launch_bounds__(kDotThreads) k_lb_fold_cross_mma(Fe* __restric
 
 // dot(w, q) and the first binary cross pair (k_eo_dot_cross): over pairs
 // j < n/2, sum w[2j] q[2j] + w[2j+1] q[2j+1], sum w[2j] q[2j+1], sum w[2j+1] q[2j].
-__global__ void __launch_bounds__(kDotThreads) k_eo_dot_cross_mma(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n,
+__global__ void __launch_bounds__(kDotThreads, 2) k_eo_dot_cross_mma(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n,
                                                                   Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
   uint32_t* s = stage_s[threadIdx.x >> 5];
@@ -266,14 +284,9 @@ __global__ void __launch_bounds__(kDotThreads) k_eo_dot_cross_mma(const Fe* __re
 #pragma unroll
   for (int k = 0; k < 3; ++k) dot_clear(acc[k]);
   Fr v[3] = {zero(), zero(), zero()};
-  dot_loop<4>(
-      s, n / 2,
-      [&](uint64_t j, bool ok, uint4 (&x)[4]) {
-        x[0] = ok ? ld4(w + 2 * j) : zero4();
-        x[1] = ok ? ld4(w + 2 * j + 1) : zero4();
-        x[2] = ok ? ld4(q + 2 * j) : zero4();
-        x[3] = ok ? ld4(q + 2 * j + 1) : zero4();
-      },
+  dot_loop<4, 4>(
+      s, n / 2, [&](uint64_t j, bool ok, uint4 (&r)[4]) { fetch_n<4>(ok, r, {w + 2 * j, w + 2 * j + 1, q + 2 * j, q + 2 * j + 1}); },
+      [&](uint64_t, bool, const uint4 (&r)[4], uint4 (&x)[4]) { copy_n<4>(r, x); },
       [&](const DotFrag (&f)[4]) {
         dot_mma(acc[0], f[0], f[2]);
         dot_mma(acc[0], f[1], f[3]);
@@ -290,7 +303,7 @@ __global__ void __launch_bounds__(kDotThreads) k_eo_dot_cross_mma(const Fe* __re
 
 // w'[i] = w[2i] + w[2i+1] inv, q'[i] = q[2i] + q[2i+1] ch and the next cross
 // pair of (w', q') (k_eo_fold_cross); n >= 4.
-__global__ void __launch_bounds__(kDotThreads) k_eo_fold_cross_mma(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n,
+__global__ void __launch_bounds__(kDotThreads, 2) k_eo_fold_cross_mma(const Fe* __restrict__ w, const Fe* __restrict__ q, uint64_t n,
                                                                    Fe inv, Fe ch, Fe* __restrict__ w_out, Fe* __restrict__ q_out,
                                                                    Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
@@ -300,25 +313,23 @@ __global__ void __launch_bounds__(kDotThreads) k_eo_fold_cross_mma(const Fe* __r
   dot_clear(acc[0]);
   dot_clear(acc[1]);
   Fr v[2] = {zero(), zero()};
-  dot_loop<4>(
+  dot_loop<4, 8>(
       s, n / 4,
-      [&](uint64_t j, bool ok, uint4 (&x)[4]) {
-        if (!ok) {
-          x[0] = x[1] = x[2] = x[3] = zero4();
-          return;
+      [&](uint64_t j, bool ok, uint4 (&r)[8]) {
+        fetch_n<8>(ok, r, {w + 4 * j, w + 4 * j + 1, w + 4 * j + 2, w + 4 * j + 3, q + 4 * j, q + 4 * j + 1, q + 4 * j + 2,
+                           q + 4 * j + 3});
+      },
+      [&](uint64_t j, bool ok, const uint4 (&r)[8], uint4 (&x)[4]) {
+        x[0] = pack_fe(add(fr(r[0]), mul(fr(r[1]), fi)));
+        x[1] = pack_fe(add(fr(r[2]), mul(fr(r[3]), fi)));
+        x[2] = pack_fe(add(fr(r[4]), mul(fr(r[5]), fc)));
+        x[3] = pack_fe(add(fr(r[6]), mul(fr(r[7]), fc)));
+        if (ok) {
+          *reinterpret_cast<uint4*>(w_out + 2 * j) = x[0];
+          *reinterpret_cast<uint4*>(w_out + 2 * j + 1) = x[1];
+          *reinterpret_cast<uint4*>(q_out + 2 * j) = x[2];
+          *reinterpret_cast<uint4*>(q_out + 2 * j + 1) = x[3];
         }
-        const Fr a0 = add(load(w + 4 * j), mul(load(w + 4 * j + 1), fi));
-        const Fr a1 = add(load(w + 4 * j + 2), mul(load(w + 4 * j + 3), fi));
-        const Fr b0 = add(load(q + 4 * j), mul(load(q + 4 * j + 1), fc));
-        const Fr b1 = add(load(q + 4 * j + 2), mul(load(q + 4 * j + 3), fc));
-        x[0] = pack_fe(a0);
-        x[1] = pack_fe(a1);
-        x[2] = pack_fe(b0);
-        x[3] = pack_fe(b1);
-        *reinterpret_cast<uint4*>(w_out + 2 * j) = x[0];
-        *reinterpret_cast<uint4*>(w_out + 2 * j + 1) = x[1];
-        *reinterpret_cast<uint4*>(q_out + 2 * j) = x[2];
-        *reinterpret_cast<uint4*>(q_out + 2 * j + 1) = x[3];
       },
       [&](const DotFrag (&f)[4]) {
         dot_mma(acc[0], f[0], f[3]);
@@ -334,7 +345,7 @@ __global__ void __launch_bounds__(kDotThreads) k_eo_fold_cross_mma(const Fe* __r
 
 // q'[i] = q[2i] + q[2i+1] ch next to the folded witness wf, and the cross
 // pair of (wf, q') (k_eo_fold_query_cross); n >= 4.
-__global__ void __launch_bounds__(kDotThreads) k_eo_fold_query_cross_mma(const Fe* __restrict__ wf, const Fe* __restrict__ q,
+__global__ void __launch_bounds__(kDotThreads, 2) k_eo_fold_query_cross_mma(const Fe* __restrict__ wf, const Fe* __restrict__ q,
                                                                          uint64_t n, Fe ch, Fe* __restrict__ q_out,
                                                                          Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
@@ -344,21 +355,20 @@ __global__ void __launch_bounds__(kDotThreads) k_eo_fold_query_cross_mma(const F
   dot_clear(acc[0]);
   dot_clear(acc[1]);
   Fr v[2] = {zero(), zero()};
-  dot_loop<4>(
+  dot_loop<4, 6>(
       s, n / 4,
-      [&](uint64_t j, bool ok, uint4 (&x)[4]) {
-        if (!ok) {
-          x[0] = x[1] = x[2] = x[3] = zero4();
-          return;
+      [&](uint64_t j, bool ok, uint4 (&r)[6]) {
+        fetch_n<6>(ok, r, {wf + 2 * j, wf + 2 * j + 1, q + 4 * j, q + 4 * j + 1, q + 4 * j + 2, q + 4 * j + 3});
+      },
+      [&](uint64_t j, bool ok, const uint4 (&r)[6], uint4 (&x)[4]) {
+        x[0] = r[0];
+        x[1] = r[1];
+        x[2] = pack_fe(add(fr(r[2]), mul(fr(r[3]), fc)));
+        x[3] = pack_fe(add(fr(r[4]), mul(fr(r[5]), fc)));
+        if (ok) {
+          *reinterpret_cast<uint4*>(q_out + 2 * j) = x[2];
+          *reinterpret_cast<uint4*>(q_out + 2 * j + 1) = x[3];
         }
-        x[0] = ld4(wf + 2 * j);
-        x[1] = ld4(wf + 2 * j + 1);
-        const Fr b0 = add(load(q + 4 * j), mul(load(q + 4 * j + 1), fc));
-        const Fr b1 = add(load(q + 4 * j + 2), mul(load(q + 4 * j + 3), fc));
-        x[2] = pack_fe(b0);
-        x[3] = pack_fe(b1);
-        *reinterpret_cast<uint4*>(q_out + 2 * j) = x[2];
-        *reinterpret_cast<uint4*>(q_out + 2 * j + 1) = x[3];
       },
       [&](const DotFrag (&f)[4]) {
         dot_mma(acc[0], f[0], f[3]);
@@ -374,7 +384,7 @@ __global__ void __launch_bounds__(kDotThreads) k_eo_fold_query_cross_mma(const F
 
 // Degree-2 sumcheck message on (v, w) of length n: sum_{i<h} v_i w_i and
 // sum (v_{i+h} - v_i)(w_{i+h} - w_i) (k_sum_message).
-__global__ void __launch_bounds__(kDotThreads) k_sum_message_mma(const Fe* __restrict__ v, const Fe* __restrict__ w, uint64_t n,
+__global__ void __launch_bounds__(kDotThreads, 2) k_sum_message_mma(const Fe* __restrict__ v, const Fe* __restrict__ w, uint64_t n,
                                                                  Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
   uint32_t* s = stage_s[threadIdx.x >> 5];
@@ -383,18 +393,13 @@ __global__ void __launch_bounds__(kDotThreads) k_sum_message_mma(const Fe* __res
   dot_clear(acc[0]);
   dot_clear(acc[1]);
   Fr out[2] = {zero(), zero()};
-  dot_loop<4>(
-      s, h,
-      [&](uint64_t i, bool ok, uint4 (&x)[4]) {
-        if (!ok) {
-          x[0] = x[1] = x[2] = x[3] = zero4();
-          return;
-        }
-        const Fr a = load(v + i), b = load(w + i), c = load(v + i + h), d = load(w + i + h);
-        x[0] = pack_fe(a);
-        x[1] = pack_fe(b);
-        x[2] = pack_fe(sub(c, a));
-        x[3] = pack_fe(sub(d, b));
+  dot_loop<4, 4>(
+      s, h, [&](uint64_t i, bool ok, uint4 (&r)[4]) { fetch_n<4>(ok, r, {v + i, w + i, v + i + h, w + i + h}); },
+      [&](uint64_t, bool, const uint4 (&r)[4], uint4 (&x)[4]) {
+        x[0] = r[0];
+        x[1] = r[1];
+        x[2] = pack_fe(sub(fr(r[2]), fr(r[0])));
+        x[3] = pack_fe(sub(fr(r[3]), fr(r[1])));
       },
       [&](const DotFrag (&f)[4]) {
         dot_mma(acc[0], f[0], f[1]);
@@ -411,7 +416,7 @@ __global__ void __launch_bounds__(kDotThreads) k_sum_message_mma(const Fe* __res
 // Fold both vectors at ch (lo <- lo + ch (hi - lo)) and the next message of
 // the folded vectors (k_sum_fold_message); index i < n/4 produces entries
 // i and i + n/4 of the length-n/2 outputs; n >= 4.
-__global__ void __launch_bounds__(kDotThreads) k_sum_fold_message_mma(const Fe* __restrict__ v, const Fe* __restrict__ w,
+__global__ void __launch_bounds__(kDotThreads, 2) k_sum_fold_message_mma(const Fe* __restrict__ v, const Fe* __restrict__ w,
                                                                       uint64_t n, Fe ch, Fe* __restrict__ v_out,
                                                                       Fe* __restrict__ w_out, Fe* __restrict__ partials) {
   __shared__ __align__(16) uint32_t stage_s[kDotThreads / 32][4 * kDotStride];
@@ -422,21 +427,21 @@ __global__ void __launch_bounds__(kDotThreads) k_sum_fold_message_mma(const Fe* 
   dot_clear(acc[0]);
   dot_clear(acc[1]);
   Fr out[2] = {zero(), zero()};
-  dot_loop<4>(
+  dot_loop<4, 8>(
       s, q,
-      [&](uint64_t i, bool ok, uint4 (&x)[4]) {
-        if (!ok) {
-          x[0] = x[1] = x[2] = x[3] = zero4();
-          return;
+      [&](uint64_t i, bool ok, uint4 (&r)[8]) {
+        fetch_n<8>(ok, r, {v + i, v + i + h, v + i + q, v + i + q + h, w + i, w + i + h, w + i + q, w + i + q + h});
+      },
+      [&](uint64_t i, bool ok, const uint4 (&r)[8], uint4 (&x)[4]) {
+        const Fr a0 = fr(r[0]), b0 = fr(r[2]), x0 = fr(r[4]), y0 = fr(r[6]);
+        const Fr nv0 = add(a0, mul(c, sub(fr(r[1]), a0))), nv1 = add(b0, mul(c, sub(fr(r[3]), b0)));
+        const Fr nw0 = add(x0, mul(c, sub(fr(r[5]), x0))), nw1 = add(y0, mul(c, sub(fr(r[7]), y0)));
+        if (ok) {
+          store(v_out + i, nv0);
+          store(v_out + i + q, nv1);
+          store(w_out + i, nw0);
+          store(w_out + i + q, nw1);
         }
-        const Fr a0 = load(v + i), a1 = load(v + i + h), b0 = load(v + i + q), b1 = load(v + i + q + h);
-        const Fr nv0 = add(a0, mul(c, sub(a1, a0))), nv1 = add(b0, mul(c, sub(b1, b0)));
-        const Fr x0 = load(w + i), x1 = load(w + i + h), y0 = load(w + i + q), y1 = load(w + i + q + h);
-        const Fr nw0 = add(x0, mul(c, sub(x1, x0))), nw1 = add(y0, mul(c, sub(y1, y0)));
-        store(v_out + i, nv0);
-        store(v_out + i + q, nv1);
-        store(w_out + i, nw0);
-        store(w_out + i + q, nw1);
         x[0] = pack_fe(nv0);
         x[1] = pack_fe(nw0);
         x[2] = pack_fe(sub(nv1, nv0));
