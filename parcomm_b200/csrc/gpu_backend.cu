@@ -43,16 +43,19 @@ static bool imma_on() {
 // on the tensor cores (kernels/dot_mma.cuh) where that measured faster on
 // B200 in the 8B-shape step, on the CUDA cores elsewhere (core_dots 0);
 // core_dots 1 takes the CUDA cores everywhere, 2 the tensor cores
-// everywhere.  The tensor-core sums win where the sum is the work (EO dot and
-// first cross pair 1.9x / 1.7x, sumcheck message 1.75x / 1.5x for F65521 /
-// KoalaBear); where a fold's scalar products dominate, or the vectors are
-// short, the chunked warp loop and its staging cost more than they save.
+// everywhere.  The tensor-core sums win on the long vectors: EO dot and
+// first cross pair 2.5x / 2.2x, EO query fold 1.4x / 1.13x, sumcheck message
+// 1.7x / 1.3x and fold 1.09x / 1.19x (F65521 / KoalaBear).  On the short
+// vectors of the LiteBullet rounds and the small EO rounds the chunked warp
+// loop and its staging cost more than they save (0.7x - 0.9x), except the
+// KoalaBear LiteBullet cross pair (1.03x).
 enum class Dots { kEoDotCross, kEoFoldQueryCross, kEoFoldCross, kSumMessage, kSumFold, kLbCross, kLbFold, kDot };
 static bool tc_dots(Dots k) {
   const int opt = KernelOptions::core_dots.load();
   if (opt != 0) return opt == 2;
 #if defined(QF_FIELD_KB)
-  return k == Dots::kEoDotCross || k == Dots::kSumMessage || k == Dots::kLbCross;
+  return k == Dots::kEoDotCross || k == Dots::kEoFoldQueryCross || k == Dots::kSumMessage || k == Dots::kSumFold ||
+         k == Dots::kLbCross;
 #else
   return k == Dots::kEoDotCross || k == Dots::kEoFoldQueryCross || k == Dots::kSumMessage || k == Dots::kSumFold;
 #endif
