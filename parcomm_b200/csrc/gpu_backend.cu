@@ -538,18 +538,10 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
   Fe* msg = cw;
   Fe* par = cw + R;
   const bool mobius = mob_from < logm;
-  // The separate passes: the rest of the Mobius transform, then per WHT a
-  // tile pass (levels 0..11, alpha first for the second) and strided passes.
-  // KoalaBear keeps them: its butterflies reduce at every level (3 operations
-  // per element, coefficient and level), so its passes are compute-heavier
-  // and the fused plan measured slower on its 8B step (351 vs 337 ms).
-  // Columns shorter than a tile (logR < 12) take them in both fields.
-#if defined(QF_FIELD_KB)
-  constexpr bool kSeparate = true;
-#else
-  constexpr bool kSeparate = false;
-#endif
-  if (kSeparate || logR < qfd::kMaxTileLog) {
+  // Columns shorter than a tile (logR < 12): the rest of the Mobius
+  // transform, then per WHT a tile pass (levels 0..logR, alpha first for the
+  // second) and strided passes.
+  if (logR < qfd::kMaxTileLog) {
     const int wl = std::min(qfd::kMaxTileLog, logR);
     if (mobius) strided_passes<qfd::kMobius>(s, msg, msg, logR, logm, mob_from, logm, timed, allow_tuning);
     for (int pass = 0; pass < 2; ++pass) {
@@ -564,7 +556,16 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
   check(!mobius || mob_from == kT, "the Mobius tile pass covers bits 0..11");
   const int top = std::min(logR, kT + 10);  // fused span [kT, top)
   const int k = top - kT;
+  // KoalaBear does not fuse the Mobius and WHT #1 strided levels: its
+  // butterflies reduce at every level (3 operations per element, coefficient
+  // and level), so a 20-level pass is issue-bound where its separate strided
+  // passes run at 0.95 of HBM (the fused plan measured 351 against 337 ms
+  // per 8B step).  It still takes the WHT-alpha-WHT tile pass.
+#if defined(QF_FIELD_KB)
+  const bool fused = false;
+#else
   const bool fused = mobius && k >= 6;
+#endif
   if (mobius) strided_passes<qfd::kMobius>(s, msg, msg, logR, logm, fused ? top : kT, logm, timed, allow_tuning);
   if (fused) {
     const int cb = strided_cb(k, logm);

@@ -57,6 +57,12 @@ __device__ __forceinline__ int pidx(int e) {
   return e ^ int(__byte_perm(uint32_t(kSwz), uint32_t(kSwz >> 32), (e >> 5) & 7) & 31);
 }
 
+// 16 bytes global -> shared memory, asynchronously (cp.async, L2 only).
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(src) : "memory");
+}
+
 __device__ __forceinline__ void planar_put(uint32_t* planes, int e, const Fr& v) {
   const int q = pidx(e);
 #pragma unroll
@@ -436,62 +442,48 @@ __device__ __forceinline__ void window_mid_r(uint4* t, int b, int r, int lvl, St
   else window_mid<OP1, OP2, 1>(t, b, lvl, step);
 }
 
-// A pass of OP1 over tile bits [b0, 12) of full tiles (b0 <= 9, 512
-// threads), and, when FUSED (b0 <= 6), a step and a second transform OP2 on
-// the same bits in the same trip through HBM:
-//   fetch(tile, e) -> Raw and conv(tile, e, Raw) -> Fr read element e;
-//   stage(tile) runs first in each tile (it issues cp.async side loads, waited
-//   for before the first barrier);
-//   single pass: st(tile, e, uint4) stores element e (reduced, packed);
-//   fused pass: mid(tile, e, Fr&) runs on each canonical element after OP1,
-//   then OP2 and st.
-// The next tile's loads are issued after the first window (single) or after
-// the step (fused), so their registers are not live across the step.
-template <int OP1, int OP2, bool FUSED, bool PREFETCH, class Raw, class Fetch, class Conv, class Stage, class Mid,
-          class St>
-__device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles, Fetch fetch, Conv conv, Stage stage,
+// A fused pass over full tiles (512 threads): OP1 on tile bits [b0, 12)
+// (b0 <= 6), a step on each canonical element, then OP2 on the same bits, in
+// one trip through HBM.
+//   src(tile, e) -> const void* is the 16-byte global element e of a tile,
+//   conv(tile, e, uint4) -> Fr its value;
+//   stage(tile) issues the cp.async side loads the step needs (one commit
+//   group) into `side`, each thread only to the positions e = g + (j << 9)
+//   it owns in the first window;
+//   mid(tile, e, Fr&) runs on each canonical element after OP1;
+//   st(tile, e, uint4) stores element e (reduced, packed) after OP2.
+// `side` (4096 x 16 bytes) also stages the tile's elements: once the step
+// has consumed the side loads, each thread copies the next tile's elements
+// it owns into its own positions there by cp.async, so they land while OP2
+// runs, and reads them back at the next tile's start before stage() reuses
+// the positions.  Commit groups: the next tile's elements, then the side
+// loads, each waited for in full.
+template <int OP1, int OP2, class Src, class Conv, class Stage, class Mid, class St>
+__device__ __forceinline__ void tile_pass_v2(uint4* t, uint4* side, int b0, uint32_t n_tiles, Src src, Conv conv, Stage stage,
                                              Mid mid, St st) {
   const int g = threadIdx.x;
   const Windows w = windows_below9(b0);
   int off9[8];
   window_offsets<3>(9, off9);
-  Raw raw[8];
   uint32_t tile = blockIdx.x;
-  if (PREFETCH && tile < n_tiles)
+  if (tile < n_tiles)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+    for (int j = 0; j < 8; ++j) cp_async16(side + g + (j << 9), src(tile, g + (j << 9)));
+  asm volatile("cp.async.commit_group;" ::: "memory");
   for (; tile < n_tiles; tile += gridDim.x) {
-    stage(tile);
-    const uint32_t next = tile + gridDim.x;
-    if (!PREFETCH)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) raw[j] = fetch(tile, g + (j << 9));
+    asm volatile("cp.async.wait_all;" ::: "memory");  // this tile's elements (own copies)
     {
       uint32_t v[8][kC];
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        const Fr e = conv(tile, g + (j << 9), raw[j]);
+        const Fr e = conv(tile, g + (j << 9), side[g + (j << 9)]);
 #pragma unroll
         for (int c = 0; c < kC; ++c) v[j][c] = e.c[c];
       }
       reg_levels<OP1, 3>(v, 0);
-      if (w.n == 0 && !FUSED) {  // three levels: the first window is the last
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          Fr o;
-#pragma unroll
-          for (int c = 0; c < kC; ++c) o.c[c] = tile_final(v[j][c]);
-          st(tile, g + (j << 9), pack_fe(o));
-        }
-      } else {
-        group_put<3>(t, g, off9, v);
-      }
+      group_put<3>(t, g, off9, v);
     }
-    if (PREFETCH && !FUSED && next < n_tiles)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
-    if (w.n == 0 && !FUSED) continue;
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    stage(tile);  // into this thread's positions, whose elements it has consumed
     __syncthreads();
     int lvl = 3;
 #pragma unroll
@@ -500,20 +492,19 @@ __device__ __forceinline__ void tile_pass_v2(uint4* t, int b0, uint32_t n_tiles,
         window_stage_r<OP1>(t, w.b[i], w.r[i], lvl);
         lvl += w.r[i];
       }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // the side loads
+    __syncthreads();
     const int bl = w.n == 3 ? w.b[2] : (w.n == 2 ? w.b[1] : w.b[0]);
     const int rl = w.n == 3 ? w.r[2] : (w.n == 2 ? w.r[1] : w.r[0]);
-    if (!FUSED) {
-      window_last_r<OP1, false>(t, bl, rl, lvl, [&](int e, Fr& v) { st(tile, e, pack_fe(v)); });
-      __syncthreads();  // the next tile's first window overwrites the tile
-      continue;
-    }
-    // Fused: OP1's last window, the step, and OP2's levels on the same
-    // window in registers.
+    // OP1's last window, the step, and OP2's levels on the same window in
+    // registers.
     window_mid_r<OP1, OP2>(t, bl, rl, lvl, [&](int e, Fr& v) { mid(tile, e, v); });
-    if (PREFETCH && next < n_tiles)
+    __syncthreads();  // every step has read the side loads
+    const uint32_t next = tile + gridDim.x;
+    if (next < n_tiles)
 #pragma unroll
-      for (int j = 0; j < 8; ++j) raw[j] = fetch(next, g + (j << 9));
-    __syncthreads();
+      for (int j = 0; j < 8; ++j) cp_async16(side + g + (j << 9), src(next, g + (j << 9)));
+    asm volatile("cp.async.commit_group;" ::: "memory");
     int lvl2 = rl;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -674,10 +665,6 @@ __device__ __forceinline__ void fused_middle(uint32_t* planes, int b0, int lvl0)
 // without holding registers.  Commit groups per tile: the side loads and an
 // always-present group closing them, then the next tile's elements.
 constexpr size_t kPrefetchSmem = size_t(1) << kMaxTileLog << 4;  // 64 KiB
-__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
-  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(src) : "memory");
-}
 template <int OP1, int OP2, class Src, class Conv, class Stage, class Mid, class St>
 __device__ __forceinline__ void tile_loop_fused(uint32_t* planes, int b0, uint32_t n_tiles, Src src, Conv conv,
                                                 Stage stage, Mid mid, St st) {
@@ -775,7 +762,7 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_wht_alpha_wht_tile(const Fe
   uint4* alpha_s = reinterpret_cast<uint4*>(planes_s + kC * kPlane);
   const uint32_t rmask = (1u << logR) - 1u;
   auto addr = [=](uint32_t tile, int t) { return msg_addr32((tile << kMaxTileLog) + uint32_t(t), logR); };
-  auto fetch = [=](uint32_t tile, int t) { return *reinterpret_cast<const uint4*>(src + addr(tile, t)); };
+  auto elem = [=](uint32_t tile, int t) -> const void* { return src + addr(tile, t); };
   auto conv = [](uint32_t, int, uint4 raw) { return unpack_fe(raw); };
   auto stage = [=](uint32_t tile) {
     // Tile rows r0 .. r0 + 4095 (R is a multiple of 4096).
@@ -783,17 +770,15 @@ __global__ void __launch_bounds__(kTileThreads, 1) k_wht_alpha_wht_tile(const Fe
 #pragma unroll
     for (int i = 0; i < (1 << kMaxTileLog) / kTileThreads; ++i) {
       const int e = int(threadIdx.x) + i * kTileThreads;
-      const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(alpha_s + e));
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(a + e) : "memory");
+      cp_async16(alpha_s + e, a + e);
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   auto mid = [=](uint32_t, int t, Fr& v) { v = mul(v, unpack_fe(alpha_s[t])); };
   auto st = [=](uint32_t tile, int t, uint4 u) { *reinterpret_cast<uint4*>(dst + addr(tile, t)) = u; };
-  // No register prefetch of the next tile: with the product in the step, its
-  // registers would spill (measured); the tile's loads are issued at its start.
-  tile_pass_v2<kWht, kWht, true, false, uint4>(reinterpret_cast<uint4*>(planes_s), 0, n_tiles, fetch, conv, stage, mid,
-                                               st);
+  // The next tile's elements are staged by cp.async in the alpha area once
+  // the step has used it (a register prefetch would spill: measured).
+  tile_pass_v2<kWht, kWht>(reinterpret_cast<uint4*>(planes_s), alpha_s, 0, n_tiles, elem, conv, stage, mid, st);
 }
 
 // ---------------------------------------------------------------- hashing
