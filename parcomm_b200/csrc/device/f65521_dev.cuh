@@ -77,6 +77,7 @@ QFD_HD uint32_t red_signed(int64_t v) {
   return red40(u);
 }
 QFD_HD Fr mul(const Fr& a, const Fr& b) {
+  // A loop's fixed factor goes second, so that 17 * b is computed once.
   // X^8 = 17: the wrap-around products take 17 * b_j (< 2^21, unreduced), so
   // output coefficient k is one sum of eight products a_i * b'_j < 2^37,
   // accumulated with 64-bit multiply-adds (< 2^40) and reduced once.

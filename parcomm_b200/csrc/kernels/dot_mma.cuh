@@ -434,8 +434,8 @@ __global__ void __launch_bounds__(kDotThreads, 2) k_sum_fold_message_mma(const F
       },
       [&](uint64_t i, bool ok, const uint4 (&r)[8], uint4 (&x)[4]) {
         const Fr a0 = fr(r[0]), b0 = fr(r[2]), x0 = fr(r[4]), y0 = fr(r[6]);
-        const Fr nv0 = add(a0, mul(c, sub(fr(r[1]), a0))), nv1 = add(b0, mul(c, sub(fr(r[3]), b0)));
-        const Fr nw0 = add(x0, mul(c, sub(fr(r[5]), x0))), nw1 = add(y0, mul(c, sub(fr(r[7]), y0)));
+        const Fr nv0 = add(a0, mul(sub(fr(r[1]), a0), c)), nv1 = add(b0, mul(sub(fr(r[3]), b0), c));
+        const Fr nw0 = add(x0, mul(sub(fr(r[5]), x0), c)), nw1 = add(y0, mul(sub(fr(r[7]), y0), c));
         if (ok) {
           store(v_out + i, nv0);
           store(v_out + i + q, nv1);

@@ -195,7 +195,7 @@ __global__ void k_query_terms(const TermTiles* __restrict__ terms, int n_terms, 
     const Fr hi = tile_high(T, tables, i);
     Fe* dst = q + T.offset + row0;
     for (uint32_t r = threadIdx.x; r < nrows; r += blockDim.x)
-      store(dst + r, add(load(dst + r), mul(hi, load(tables + T.lo_off + r))));
+      store(dst + r, add(load(dst + r), mul(load(tables + T.lo_off + r), hi)));
   }
 }
 __global__ void k_scatter_add(const uint64_t* __restrict__ idx, const Fe* __restrict__ vals, uint32_t n, Fe* __restrict__ q) {
@@ -333,16 +333,16 @@ __global__ void k_sum_fold_message(const Fe* __restrict__ v, const Fe* __restric
   if (n == 2) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       Fr a = load(v), b = load(v + 1);
-      store(v_out, add(a, mul(c, sub(b, a))));
+      store(v_out, add(a, mul(sub(b, a), c)));
       Fr x = load(w), y = load(w + 1);
-      store(w_out, add(x, mul(c, sub(y, x))));
+      store(w_out, add(x, mul(sub(y, x), c)));
     }
   } else {
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < q; i += uint64_t(gridDim.x) * blockDim.x) {
       Fr a0 = load(v + i), a1 = load(v + i + h), b0 = load(v + i + q), b1 = load(v + i + q + h);
-      Fr nv0 = add(a0, mul(c, sub(a1, a0))), nv1 = add(b0, mul(c, sub(b1, b0)));
+      Fr nv0 = add(a0, mul(sub(a1, a0), c)), nv1 = add(b0, mul(sub(b1, b0), c));
       Fr x0 = load(w + i), x1 = load(w + i + h), y0 = load(w + i + q), y1 = load(w + i + q + h);
-      Fr nw0 = add(x0, mul(c, sub(x1, x0))), nw1 = add(y0, mul(c, sub(y1, y0)));
+      Fr nw0 = add(x0, mul(sub(x1, x0), c)), nw1 = add(y0, mul(sub(y1, y0), c));
       store(v_out + i, nv0);
       store(v_out + i + q, nv1);
       store(w_out + i, nw0);

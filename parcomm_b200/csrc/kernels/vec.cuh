@@ -13,7 +13,7 @@ namespace QFD_NS {
 __global__ void k_axpy(Fe* __restrict__ a, const Fe* __restrict__ b, uint64_t n, Fe s) {
   const Fr fs = load(&s);
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
-    store(a + i, add(load(a + i), mul(fs, load(b + i))));
+    store(a + i, add(load(a + i), mul(load(b + i), fs)));
 }
 // a[i] += b[i]
 __global__ void k_add(Fe* __restrict__ a, const Fe* __restrict__ b, uint64_t n) {
