@@ -575,10 +575,12 @@ static void encode_passes(cudaStream_t s, Fe* cw, const Fe* alpha, int logR, int
              qfd::k_mobius_wht_strided<<<tile_grid(tiles), qfd::kTileThreads, qfd::kTileSmem + qfd::kPrefetchSmem, s>>>(cw, uint32_t(R), logR,
                                                                                                  kT, k, cb, tiles);
            });
+    strided_passes<qfd::kWht>(s, par, par, logR, logm, top, logR, timed, allow_tuning);
   } else {
-    strided_passes<qfd::kWht>(s, msg, par, logR, logm, kT, top, timed, allow_tuning);
+    // WHT #1's levels [12, logR) as one span (the tuner's split), message
+    // into parity.
+    strided_passes<qfd::kWht>(s, msg, par, logR, logm, kT, logR, timed, allow_tuning);
   }
-  strided_passes<qfd::kWht>(s, par, par, logR, logm, top, logR, timed, allow_tuning);
   const uint32_t tiles = uint32_t(uint64_t(1) << (logm - kT));
   const Fe* src = k > 0 ? par : msg;
   launch(s, timed, "k_wht_alpha_wht_tile", (uint64_t(2) << logm) * 16 + uint64_t(R) * 16,
