@@ -97,6 +97,21 @@ def make_bva_on_host(shapes, seed: int = 0, sigma: float = 0.02):
     return out, active, pinned
 
 
+def force_extremes(w, n_forced: int, g):
+    """Sets n_forced positions of the flat float tensor w, drawn with
+    generator g, to -127 or +127.  A position drawn more than once takes its
+    first draw's sign: a scatter with repeated indices would leave the winner
+    unspecified, and the weights would differ between runs."""
+    import torch
+    idx = torch.randint(0, w.numel(), (n_forced,), generator=g, device=w.device)
+    sign = torch.randint(0, 2, (n_forced,), generator=g, device=w.device).float().mul_(254.0).sub_(127.0)
+    order = torch.sort(idx, stable=True).indices
+    idx, sign = idx[order], sign[order]
+    first = torch.ones_like(idx, dtype=torch.bool)
+    first[1:] = idx[1:] != idx[:-1]
+    w[idx[first]] = sign[first]
+
+
 def make_bva_on_device(shapes, seed: int = 0, bf16: bool = False, embedding_first: bool = False):
     """Deterministic synthetic weights laid out as the BVA, generated on the GPU:
     int8 round(N(0, 20^2)) clipped to +-127 with 0.1% forced to +-127, or (bf16)
@@ -120,9 +135,7 @@ def make_bva_on_device(shapes, seed: int = 0, bf16: bool = False, embedding_firs
         else:
             w = w.mul_(20.0).round_().clamp_(-127, 127)
             n_forced = max(1, (rows * cols) // 1000)
-            idx = torch.randint(0, rows * cols, (n_forced,), generator=g, device="cuda")
-            sign = torch.randint(0, 2, (n_forced,), generator=g, device="cuda").float().mul_(254.0).sub_(127.0)
-            w[idx] = sign
+            force_extremes(w, n_forced, g)
             w = w.to(torch.int8).view(rows, cols)
         for b in by_matrix[m]:
             dst = out[b.offset: b.offset + b.rows * b.cols].view(b.rows, b.cols)
@@ -318,9 +331,7 @@ def int8_matrix(rows: int, cols: int, seed: int):
     g = torch.Generator(device="cuda")
     g.manual_seed(seed)
     w = torch.randn(rows * cols, generator=g, device="cuda", dtype=torch.float32).mul_(20.0).round_().clamp_(-127, 127)
-    n_forced = max(1, (rows * cols) // 1000)
-    idx = torch.randint(0, rows * cols, (n_forced,), generator=g, device="cuda")
-    w[idx] = torch.randint(0, 2, (n_forced,), generator=g, device="cuda").float().mul_(254.0).sub_(127.0)
+    force_extremes(w, max(1, (rows * cols) // 1000), g)
     return w.to(torch.int8).view(rows, cols)
 
 
