@@ -55,7 +55,11 @@ typedef struct {
   uint64_t kernel_launches;
 } qf_profile; /* ProverProfile (protocol.rs:67-80), milliseconds */
 
-/* Parameters::new(shapes, config) (protocol.rs:109-130). Setup runs on the host. */
+/* Parameters::new(shapes, config) (protocol.rs:109-130).  The setup's large
+ * levels are encoded and their rows hashed on the current device when the
+ * process has one (the rest of the setup, and all of it in a process
+ * without a device, runs on the host threads); either way the parameter
+ * digest is the same.  A parameter set's setup is built once per process. */
 int qf_params_new(int field, const qf_shape* shapes, size_t n_shapes, const qf_config* config, qf_params** out);
 void qf_params_free(qf_params* params);
 /* Layout facts and Commitment::parameter_digest (layout.rs:56-114, packed.rs:161). */
