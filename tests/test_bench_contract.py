@@ -31,3 +31,25 @@ def test_streamed_70b_step_bytes_include_binding():
     live = -(-a // (1 << 30))
     assert live == 66 and terms["binding"] == terms["commit"] == (live + 1) * (1 << 30) * 18
     assert 3.5e12 < t < 3.7e12
+
+
+def test_forced_extremes_are_deterministic_with_repeated_draws():
+    """A forced position drawn twice keeps its first draw's sign, so the
+    synthetic weights are the same on every run (CPU generator here)."""
+    import torch
+    draws = []
+    for _ in range(2):
+        g = torch.Generator()
+        g.manual_seed(7)
+        w = torch.zeros(64)
+        bench.force_extremes(w, 200, g)  # far more draws than positions: many repeats
+        draws.append(w.clone())
+    assert torch.equal(draws[0], draws[1])
+    assert set(draws[0].unique().tolist()) <= {-127.0, 0.0, 127.0}
+    g = torch.Generator()
+    g.manual_seed(7)
+    idx = torch.randint(0, 64, (200,), generator=g)
+    sign = torch.randint(0, 2, (200,), generator=g).float().mul_(254.0).sub_(127.0)
+    for pos in idx.unique().tolist():
+        first = int((idx == pos).nonzero()[0])
+        assert draws[0][pos] == sign[first]
