@@ -116,18 +116,30 @@ struct CpuBackend : Backend<F>, SingleBackend<F>, EoBackend<F> {
   }
   // round_message / fold_pair (packed.rs:652-696)
   void sumcheck_message(F msg[2]) override {
-    size_t h = sum_values.size() / 2;
+    const long h = long(sum_values.size() / 2);
     F a = F::zero(), b = F::zero();
-    for (size_t i = 0; i < h; ++i) {
-      a += sum_values[i] * weights[i];
-      b += (sum_values[i + h] - sum_values[i]) * (weights[i + h] - weights[i]);
+#pragma omp parallel if (h >= 4096)
+    {
+      F la = F::zero(), lb = F::zero();
+#pragma omp for nowait
+      for (long i = 0; i < h; ++i) {
+        la += sum_values[i] * weights[i];
+        lb += (sum_values[i + h] - sum_values[i]) * (weights[i + h] - weights[i]);
+      }
+#pragma omp critical
+      {
+        a += la;
+        b += lb;
+      }
     }
     msg[0] = a;
     msg[1] = b;
   }
   void sumcheck_fold(F ch) override {
-    size_t h = sum_values.size() / 2;
-    for (size_t i = 0; i < h; ++i) {
+    const long h = long(sum_values.size() / 2);
+    // Index i reads i and i + h and writes i < h: disjoint per i.
+#pragma omp parallel for if (h >= 4096)
+    for (long i = 0; i < h; ++i) {
       sum_values[i] = sum_values[i] + ch * (sum_values[i + h] - sum_values[i]);
       weights[i] = weights[i] + ch * (weights[i + h] - weights[i]);
     }
@@ -167,21 +179,20 @@ struct CpuBackend : Backend<F>, SingleBackend<F>, EoBackend<F> {
     if (term.offset >= active || term.scale.is_zero()) return out;
     std::vector<F> hw = factor_weights(term.factors.data() + low_bits, term.factors.size() - low_bits);
     size_t rows = std::min((active - term.offset + lanes - 1) / lanes, term.len() / lanes);
-    for (size_t lane = 0; lane < lanes; ++lane) {
-      F s = F::zero();
-#pragma omp parallel
-      {
-        F local = F::zero();
+    std::vector<F> sums(lanes, F::zero());
+#pragma omp parallel if (rows * lanes >= 4096)
+    {
+      std::vector<F> local(lanes, F::zero());
 #pragma omp for nowait
-        for (long r = 0; r < long(rows); ++r) {
+      for (long r = 0; r < long(rows); ++r)
+        for (size_t lane = 0; lane < lanes; ++lane) {
           size_t idx = term.offset + r * lanes + lane;
-          if (idx < active && values[idx] != 0) local += hw[r].mul_prime(F::small(int(values[idx])));
+          if (idx < active && values[idx] != 0) local[lane] += hw[r].mul_prime(F::small(int(values[idx])));
         }
 #pragma omp critical
-        s += local;
-      }
-      out[lane] = s * term.scale;
+      for (size_t lane = 0; lane < lanes; ++lane) sums[lane] += local[lane];
     }
+    for (size_t lane = 0; lane < lanes; ++lane) out[lane] = sums[lane] * term.scale;
     return out;
   }
   void cross_terms(const Query<F>& q, size_t stride, std::vector<F>& pos, std::vector<F>& neg) override {
@@ -231,32 +242,55 @@ struct CpuBackend : Backend<F>, SingleBackend<F>, EoBackend<F> {
         for (size_t j = 0; j < stride; ++j) sc += low[j] * powers[j];
         sc = term.scale * sc;
         std::vector<F> hw = factor_weights(term.factors.data() + lb, term.factors.size() - lb);
-        size_t start = term.offset / stride;
-        for (size_t i = 0; i < hw.size(); ++i) query_values[start + i] += sc * hw[i];
+        const size_t start = term.offset / stride;
+#pragma omp parallel for if (hw.size() >= 4096)
+        for (long i = 0; i < long(hw.size()); ++i) query_values[start + i] += sc * hw[i];
       } else {
         for (size_t i = 0; i < term.len(); ++i) query_values[term.offset / stride] += term.weight(i) * powers[(term.offset + i) % stride];
       }
     }
     F dot = F::zero();
-    for (size_t i = 0; i < witness.size(); ++i) dot += witness[i] * query_values[i];
+    const long nw = long(witness.size());
+#pragma omp parallel if (nw >= 4096)
+    {
+      F local = F::zero();
+#pragma omp for nowait
+      for (long i = 0; i < nw; ++i) local += witness[i] * query_values[i];
+#pragma omp critical
+      dot += local;
+    }
     return dot;
   }
   std::array<F, 2> eo_round_cross() override {
     F a = F::zero(), b = F::zero();
-    for (size_t i = 0; i + 1 < witness.size(); i += 2) {
-      a += witness[i] * query_values[i + 1];
-      b += witness[i + 1] * query_values[i];
+    const long pairs = long(witness.size() / 2);
+#pragma omp parallel if (pairs >= 4096)
+    {
+      F la = F::zero(), lb = F::zero();
+#pragma omp for nowait
+      for (long j = 0; j < pairs; ++j) {
+        la += witness[2 * j] * query_values[2 * j + 1];
+        lb += witness[2 * j + 1] * query_values[2 * j];
+      }
+#pragma omp critical
+      {
+        a += la;
+        b += lb;
+      }
     }
     return {a, b};
   }
   void eo_round_fold(F inv, F ch) override {
-    size_t h = witness.size() / 2;
-    for (size_t i = 0; i < h; ++i) {
-      witness[i] = witness[2 * i] + witness[2 * i + 1] * inv;
-      query_values[i] = query_values[2 * i] + query_values[2 * i + 1] * ch;
+    const long h = long(witness.size() / 2);
+    // Out of place: index i reads 2i and 2i + 1.
+    std::vector<F> w(h), q(h);
+#pragma omp parallel for if (h >= 4096)
+    for (long i = 0; i < h; ++i) {
+      w[i] = witness[2 * i] + witness[2 * i + 1] * inv;
+      q[i] = query_values[2 * i] + query_values[2 * i + 1] * ch;
     }
-    witness.resize(h);
-    query_values.resize(h);
+    witness.swap(w);
+    query_values.swap(q);
   }
   std::array<F, 2> eo_terminal() override { return {witness[0], query_values[0]}; }
 };

@@ -253,7 +253,8 @@ std::vector<F> factor_weights(const std::array<F, 2>* factors, size_t n) {
   for (size_t k = 0; k < n; ++k) {
     size_t len = r.size();
     r.resize(2 * len);
-    for (size_t i = 0; i < len; ++i) { r[len + i] = r[i] * factors[k][1]; r[i] = r[i] * factors[k][0]; }
+#pragma omp parallel for if (len >= 4096)
+    for (long i = 0; i < long(len); ++i) { r[len + i] = r[i] * factors[k][1]; r[i] = r[i] * factors[k][0]; }
   }
   return r;
 }
