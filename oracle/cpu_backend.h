@@ -64,17 +64,16 @@ struct CpuBackend : Backend<F>, SingleBackend<F>, EoBackend<F> {
   // ---- equality-table lane projection (project_lanes_from_fn, packed_batch.rs:25-41)
   std::vector<F> lanes_of(size_t b) const {
     std::vector<F> lanes(F::kLanes, F::zero());
-    for (int j = 0; j < F::kLanes; ++j) {
-      F s = F::zero();
 #pragma omp parallel
-      {
-        F local = F::zero();
+    {
+      std::vector<F> local(F::kLanes, F::zero());
 #pragma omp for nowait
-        for (long i = 0; i < long(m()); ++i) local += weights[i].mul_prime(packed(b, i).c[j]);
-#pragma omp critical
-        s += local;
+      for (long i = 0; i < long(m()); ++i) {
+        const F v = packed(b, i);
+        for (int j = 0; j < F::kLanes; ++j) local[j] += weights[i].mul_prime(v.c[j]);
       }
-      lanes[j] = s;
+#pragma omp critical
+      for (int j = 0; j < F::kLanes; ++j) lanes[j] += local[j];
     }
     return lanes;
   }

@@ -48,7 +48,8 @@ std::vector<F> equality_table(const std::vector<F>& point) {
   std::vector<F> t(1, F::one());
   for (const F& c : point) {
     std::vector<F> n(t.size() * 2);
-    for (size_t i = 0; i < t.size(); ++i) { n[2 * i + 1] = t[i] * c; n[2 * i] = t[i] - n[2 * i + 1]; }
+#pragma omp parallel for if (t.size() >= 4096)
+    for (long i = 0; i < long(t.size()); ++i) { n[2 * i + 1] = t[i] * c; n[2 * i] = t[i] - n[2 * i + 1]; }
     t.swap(n);
   }
   return t;
