@@ -21,10 +21,14 @@ using namespace qf;
 template <class F>
 void mobius(std::vector<F>& v) {
   size_t n = v.size();
-  for (size_t half = 1; half < n; half <<= 1)
-#pragma omp parallel for if (n >= (1u << 16))
-    for (long blk = 0; blk < long(n / (2 * half)); ++blk)
-      for (size_t i = blk * 2 * half; i < blk * 2 * half + half; ++i) v[i + half] -= v[i];
+  // Butterfly k of a level pairs i = (k / half) * 2 half + k % half with
+  // i + half, so every level spreads over the threads (the top levels too).
+  for (size_t half = 1, lh = 0; half < n; half <<= 1, ++lh)
+#pragma omp parallel for schedule(static) if (n >= (1u << 16))
+    for (long k = 0; k < long(n / 2); ++k) {
+      const size_t i = ((size_t(k) >> lh) << (lh + 1)) | (size_t(k) & (half - 1));
+      v[i + half] -= v[i];
+    }
 }
 
 template <class F, class T>
