@@ -14,6 +14,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "libqforacle.so"
 _lib = None
+# int gather(void* ctx, const void* in, size_t n, void* out)
+GATHER = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
 
 
 def build() -> Path:
@@ -45,6 +47,11 @@ def lib() -> ctypes.CDLL:
         for name in ("qfo_verify", "qfo_verify_kb"):
             getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
+        for name in ("qfo_prove_sharded", "qfo_prove_sharded_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_int,
+                                         ctypes.c_int, GATHER, P, BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S), BPP,
+                                         ctypes.POINTER(S)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -94,6 +101,35 @@ def prove(shapes, chunk_log, packed_log, values, claims: bytes | None = None, rf
                                             ctypes.byref(outs[1]), ctypes.byref(lens[1]), ctypes.byref(outs[2]),
                                             ctypes.byref(lens[2]), t))
     return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2]), (t[0], t[1])
+
+
+def prove_sharded(shapes, chunk_log, packed_log, values, rank, world, all_gather, claims: bytes | None = None,
+                  rf_bits=100, field="f65521"):
+    """One rank of a block-sharded proof, the CPU shard standing in for the
+    rank's device.  `all_gather(data: bytes) -> bytes` returns every rank's
+    bytes in rank order.  Returns (roots, claims, proof)."""
+    sfx, dt = _SUFFIX[field]
+    arr, n = _shapes(shapes)
+    v = np.ascontiguousarray(values, dtype=dt)
+
+    def gather(_ctx, src, size, dst):
+        try:
+            out = all_gather(ctypes.string_at(src, size))
+            if len(out) != size * world:
+                return 1
+            ctypes.memmove(dst, out, len(out))
+            return 0
+        except Exception:  # the C side turns a nonzero status into an error
+            return 1
+
+    cb = GATHER(gather)
+    outs = [ctypes.POINTER(ctypes.c_uint8)() for _ in range(3)]
+    lens = [ctypes.c_size_t() for _ in range(3)]
+    _check(getattr(lib(), "qfo_prove_sharded" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size,
+                                                    claims, len(claims) if claims else 0, rank, world, cb, None,
+                                                    ctypes.byref(outs[0]), ctypes.byref(lens[0]), ctypes.byref(outs[1]),
+                                                    ctypes.byref(lens[1]), ctypes.byref(outs[2]), ctypes.byref(lens[2])))
+    return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2])
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -10,6 +10,7 @@
 #include <string>
 
 #include "cpu_backend.h"
+#include "cpu_shard.h"
 #include "../parcomm_b200/csrc/host/range_audit.h"
 
 using namespace qf;
@@ -192,6 +193,57 @@ int verify_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uin
     verify_proof(*P, make_statement(*P, rs), cl, proof_from_bytes<G>(proof, proof_len));
   });
 }
+// One rank of a block-sharded proof (csrc/host/sharded.h) with the CPU shard
+// standing in for its device.  Every rank passes the whole BVA; the shard
+// keeps only its own blocks.  `claims` may be null: each rank then takes its
+// part of the benchmark claims and the parts are summed.
+template <class G, class T>
+int prove_sharded_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                       const T* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, int rank, int world,
+                       CallbackComm::Fn gather, void* gather_ctx, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
+                       size_t* claims_out_len, uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
+    validate_values(P->layout, bva, n_values);
+    CallbackComm comm(rank, world, gather, gather_ctx);
+    BlockShards shards(P->blocks(), world);
+    qf_oracle::CpuShard<G, T> shard(*P, bva, n_values, shards, rank);
+    ShardedBackend<G> be(*P, shard, comm);
+    std::vector<Digest> rs = be.commit_all();
+    std::vector<Claim<G>> cl;
+    if (claims_in) {
+      ByteReader r(claims_in, claims_len);
+      for (const Shape& s : P->layout.shapes) {
+        Claim<G> x;
+        for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) x.row.push_back(r.field<G>());
+        for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) x.col.push_back(r.field<G>());
+        x.value = r.field<G>();
+        cl.push_back(x);
+      }
+    } else {
+      cl = sum_claims(comm, qf_oracle::evaluate_claims(*P, shard.masked.data(), n_values,
+                                                       benchmark_points<G>(make_statement(*P, rs))));
+    }
+    std::vector<uint8_t> wire = prove_sharded(*P, be, rs, cl);
+    ByteWriter rw, cw;
+    for (const auto& d : rs) rw.digest(d);
+    for (const auto& x : cl) {
+      for (const G& v : x.row) cw.field(v);
+      for (const G& v : x.col) cw.field(v);
+      cw.field(x.value);
+    }
+    *roots = dup(rw.out);
+    *roots_len = rw.out.size();
+    *claims_out = dup(cw.out);
+    *claims_out_len = cw.out.size();
+    *proof = dup(wire);
+    *proof_len = wire.size();
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -284,6 +336,26 @@ int qfo_range_audit(const int8_t* values, uint64_t n, const uint8_t seed[32], ui
 int qfo_range_audit_kb(const int16_t* values, uint64_t n, const uint8_t seed[32], uint64_t* mult, uint8_t alpha[16],
                        uint8_t lhs[16], uint8_t rhs[16]) {
   return range_audit_impl<Kb4, int16_t>(values, n, seed, mult, alpha, lhs, rhs);
+}
+
+// One rank of a block-sharded proof; `gather(ctx, in, n, out)` is the
+// all-gather over the `world` ranks (out = every rank's n bytes, in rank
+// order; returns 0 on success).  Outputs as qfo_prove's.
+int qfo_prove_sharded(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                      const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, int rank, int world,
+                      CallbackComm::Fn gather, void* gather_ctx, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
+                      size_t* claims_out_len, uint8_t** proof, size_t* proof_len) {
+  return prove_sharded_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
+                                         claims_len, rank, world, gather, gather_ctx, roots, roots_len, claims_out,
+                                         claims_out_len, proof, proof_len);
+}
+int qfo_prove_sharded_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                         const int16_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, int rank,
+                         int world, CallbackComm::Fn gather, void* gather_ctx, uint8_t** roots, size_t* roots_len,
+                         uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len) {
+  return prove_sharded_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
+                                          claims_len, rank, world, gather, gather_ctx, roots, roots_len, claims_out,
+                                          claims_out_len, proof, proof_len);
 }
 
 }  // extern "C"

@@ -1,0 +1,92 @@
+"""Block-sharded proof over gloo ranks on CPU.
+
+Each rank holds a contiguous run of the BVA's PCS blocks and runs the
+sharding layer (csrc/host/sharded.h) with the oracle's CPU shard standing in
+for its device; the only exchange is an all-gather over torch.distributed.
+Every rank must write the proof that one rank holding all blocks writes,
+byte for byte, in both fields, with given and with summed benchmark claims,
+for world sizes that split the blocks evenly and unevenly."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import oracle
+from parcomm_b200 import layout
+
+SHAPES = [(300, 700), (129, 65), (1, 5000), (64, 64)]  # 228,801 active entries, 2^18 logical
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _bva(field: str) -> np.ndarray:
+    rng = np.random.default_rng(7)
+    lo, hi, dt = (-128, 128, np.int8) if field == "f65521" else (-32768, 32768, np.int16)
+    mats = [rng.integers(lo, hi, size=(r, c), dtype=dt) for r, c in SHAPES]
+    return layout.encode(SHAPES, mats)
+
+
+def _all_gather(world: int):
+    def gather(data: bytes) -> bytes:
+        t = torch.frombuffer(bytearray(data), dtype=torch.uint8)
+        parts = [torch.empty_like(t) for _ in range(world)]
+        dist.all_gather(parts, t)
+        return b"".join(p.numpy().tobytes() for p in parts)
+    return gather
+
+
+def _rank(rank: int, world: int, port: int, field: str, cases, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        bva = _bva(field)
+        for key, chunk_log, claims in cases:
+            out[(rank, key)] = oracle.prove_sharded(SHAPES, chunk_log, 4, bva, rank, world, _all_gather(world),
+                                                    claims=claims, field=field)
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+@pytest.mark.parametrize("world", [2, 3, 4])
+def test_sharded_proof_equals_single_rank_proof(field, world):
+    bva = _bva(field)
+    cases, expected = [], {}
+    for chunk_log in (14, 16):  # 16 and 4 blocks
+        roots, claims, proof, _ = oracle.prove(SHAPES, chunk_log, 4, bva, field=field)
+        cases.append((("benchmark", chunk_log), chunk_log, None))
+        cases.append((("given", chunk_log), chunk_log, claims))
+        expected[("benchmark", chunk_log)] = expected[("given", chunk_log)] = (roots, claims, proof)
+    manager = mp.get_context("spawn").Manager()
+    out = manager.dict()
+    mp.spawn(_rank, args=(world, _free_port(), field, cases, out), nprocs=world, join=True)
+    for key, want in expected.items():
+        for rank in range(world):
+            got = out[(rank, key)]
+            assert got[0] == want[0], f"rank {rank} {key}: roots differ"
+            assert got[1] == want[1], f"rank {rank} {key}: claims differ"
+            assert got[2] == want[2], f"rank {rank} {key}: proof bytes differ"
+        assert oracle.verify(SHAPES, key[1], 4, want[0], want[1], out[(0, key)][2], field=field)
+
+
+def test_more_ranks_than_blocks_is_an_error():
+    bva = _bva("f65521")
+    with pytest.raises(oracle.OracleError, match="ranks <= blocks"):
+        # chunk 16 gives 4 blocks; a fifth rank would hold none.  The error is
+        # raised before the first exchange, so one process can check it alone.
+        oracle.prove_sharded(SHAPES, 16, 4, bva, 0, 5, lambda b: b * 5)
+
+
+def test_failed_exchange_is_an_error():
+    bva = _bva("f65521")
+    with pytest.raises(oracle.OracleError, match="all_gather"):
+        oracle.prove_sharded(SHAPES, 16, 4, bva, 0, 2, lambda b: b)  # returns one rank's bytes, not two
