@@ -5,7 +5,8 @@ sharding layer (csrc/host/sharded.h) with the oracle's CPU shard standing in
 for its device; the only exchange is an all-gather over torch.distributed.
 Every rank must write the proof that one rank holding all blocks writes,
 byte for byte, in both fields, with given and with summed benchmark claims,
-for world sizes that split the blocks evenly and unevenly."""
+for world sizes that split the blocks evenly and unevenly.  A rank that
+leaves, or an exchange that fails, ends the proof with an error."""
 import os
 import socket
 
@@ -90,3 +91,40 @@ def test_failed_exchange_is_an_error():
     bva = _bva("f65521")
     with pytest.raises(oracle.OracleError, match="all_gather"):
         oracle.prove_sharded(SHAPES, 16, 4, bva, 0, 2, lambda b: b)  # returns one rank's bytes, not two
+
+
+def _rank_with_a_lost_peer(rank: int, world: int, port: int, out):
+    import datetime
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        os._exit(0)  # leaves between steps, before its first exchange
+    try:
+        oracle.prove_sharded(SHAPES, 16, 4, _bva("f65521"), rank, world, _all_gather(world))
+        out[rank] = "proved"
+    except oracle.OracleError as e:
+        out[rank] = str(e)
+
+
+def test_lost_rank_ends_the_proof_with_an_error():
+    """A rank that leaves before the first exchange: the survivor's gather
+    fails (peer gone or the process group's timeout) and the prover returns
+    an error instead of waiting."""
+    world = 2
+    manager = mp.get_context("spawn").Manager()
+    out = manager.dict()
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_with_a_lost_peer, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    try:
+        for p in procs:
+            p.join(timeout=120)
+        assert all(p.exitcode is not None for p in procs), "a rank did not end"
+    finally:
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+                p.join()
+    assert "all_gather" in out.get(0, ""), out.get(0)
