@@ -52,6 +52,10 @@ def lib() -> ctypes.CDLL:
                                          ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_int,
                                          ctypes.c_int, GATHER, P, BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S), BPP,
                                          ctypes.POINTER(S)]
+        for name in ("qfo_tbv_dense", "qfo_tbv_dense_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_uint32, BPP,
+                                         ctypes.POINTER(S)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -130,6 +134,29 @@ def prove_sharded(shapes, chunk_log, packed_log, values, rank, world, all_gather
                                                     ctypes.byref(outs[0]), ctypes.byref(lens[0]), ctypes.byref(outs[1]),
                                                     ctypes.byref(lens[1]), ctypes.byref(outs[2]), ctypes.byref(lens[2])))
     return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2])
+
+
+def tbv_dense(shapes, chunk_log, packed_log, values, claims: bytes, stride=16, rf_bits=100, field="f65521"):
+    """The query that tbv::compile makes of `claims` from a fresh transcript, in
+    dense form: (dense weights, query claim, point, evaluation at the point,
+    positive cross terms, negative cross terms), each element 16 canonical bytes."""
+    sfx, dt = _SUFFIX[field]
+    arr, n = _shapes(shapes)
+    v = np.ascontiguousarray(values, dtype=dt)
+    out, size = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+    _check(getattr(lib(), "qfo_tbv_dense" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size, claims,
+                                                len(claims), stride, ctypes.byref(out), ctypes.byref(size)))
+    blob = _take(out, size)
+    logical = 1 << (max(v.size, 1024) - 1).bit_length()
+    bits = logical.bit_length() - 1
+    cut = [logical, 1, bits, 1, stride - 1, stride - 1]
+    assert len(blob) == 16 * sum(cut)
+    parts, pos = [], 0
+    for k in cut:
+        parts.append([blob[pos + 16 * i: pos + 16 * (i + 1)] for i in range(k)])
+        pos += 16 * k
+    dense, (claim,), point, (evaluation,), positive, negative = parts
+    return dense, claim, point, evaluation, positive, negative
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -244,6 +244,53 @@ int prove_sharded_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_l
     *proof_len = wire.size();
   });
 }
+// The compiled query of `claims` (tbv::compile from a fresh transcript) in
+// dense form, for a check against its definition: one blob of
+//   dense weights (logical x 16 B) || query claim || the point of log2(logical)
+//   "evaluation" challenges drawn next || Query::evaluation at it ||
+//   cross terms at `stride`: positive (stride - 1) || negative (stride - 1).
+template <class G, class T>
+int tbv_dense_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                   const T* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint32_t stride,
+                   uint8_t** out, size_t* out_len) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
+    validate_values(P->layout, bva, n_values);
+    if (stride < 2 || !is_pow2(stride)) fail(-9, "stride");
+    ByteReader r(claims_in, claims_len);
+    std::vector<Claim<G>> cl;
+    for (const Shape& s : P->layout.shapes) {
+      Claim<G> x;
+      for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) x.row.push_back(r.field<G>());
+      for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) x.col.push_back(r.field<G>());
+      x.value = r.field<G>();
+      cl.push_back(x);
+    }
+    Transcript<G> t;
+    Query<G> q = compile(P->layout, cl, t);
+    std::vector<G> dense(P->layout.logical, G::zero());
+    for (const Term<G>& term : q.terms)
+      for (size_t i = 0; i < term.len(); ++i) dense[term.offset + i] += term.weight(i);
+    std::vector<G> point;
+    for (int i = 0; i < ilog2(P->layout.logical); ++i) point.push_back(t.challenge("evaluation"));
+    qf_oracle::CpuBackend<G, T> be(*P, bva, n_values);
+    std::vector<G> pos, neg;
+    be.cross_terms(q, stride, pos, neg);
+    ByteWriter w;
+    for (const G& v : dense) w.field(v);
+    w.field(q.claim);
+    for (const G& v : point) w.field(v);
+    w.field(q.evaluation(point));
+    for (const G& v : pos) w.field(v);
+    for (const G& v : neg) w.field(v);
+    *out = dup(w.out);
+    *out_len = w.out.size();
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -356,6 +403,21 @@ int qfo_prove_sharded_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk
   return prove_sharded_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
                                           claims_len, rank, world, gather, gather_ctx, roots, roots_len, claims_out,
                                           claims_out_len, proof, proof_len);
+}
+
+// The compiled query in dense form beside its claim, evaluation and cross
+// terms (layout above tbv_dense_impl), for a check against the definitions.
+int qfo_tbv_dense(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                  const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint32_t stride,
+                  uint8_t** out, size_t* out_len) {
+  return tbv_dense_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
+                                     claims_len, stride, out, out_len);
+}
+int qfo_tbv_dense_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                     const int16_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint32_t stride,
+                     uint8_t** out, size_t* out_len) {
+  return tbv_dense_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
+                                      claims_len, stride, out, out_len);
 }
 
 }  // extern "C"

@@ -143,3 +143,31 @@ def test_rows_above_the_characteristic_are_not_aliased():
     assert np.array_equal(claim_value(mats[0], row, col, "f65521"), value)
     assert oracle.verify(shapes, 10, 4, roots, claims, proof)
     assert product_verifies(shapes, 10, 4, roots, claims, proof, "f65521")
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_compact_query_equals_its_dense_form(field):
+    """tbv::compile's compact terms, written out densely, give the query's
+    claim against the BVA, its evaluation at a point (the dense vector folded
+    pair by pair) and the Laurent cross terms at stride 16 (end_to_end.rs:216-262)."""
+    p = FIELDS[field][0]
+    shapes = [(31, 31), (3, 2)]
+    mats = layout.demo_matrices(shapes, dtype=FIELDS[field][4])
+    bva = layout.encode(shapes, mats)
+    _, claims, _, _ = oracle.prove(shapes, 10, 4, bva, field=field)
+    dense, claim, point, evaluation, positive, negative = oracle.tbv_dense(shapes, 10, 4, bva, claims, 16, field=field)
+    q = np.array([ext_from_bytes(b, field) for b in dense])
+    v = np.zeros(len(dense), dtype=np.int64)
+    v[: bva.size] = bva
+    assert np.count_nonzero(q.any(axis=1)) >= bva.size // 2 and v.any()
+    assert np.array_equal(((v[:, None] * q) % p).sum(axis=0) % p, ext_from_bytes(claim, field))
+    reduced = q
+    for b in point:
+        reduced = (reduced[0::2] + ext_mul(reduced[1::2], ext_from_bytes(b, field)[None, :], field)) % p
+    assert np.array_equal(reduced[0], ext_from_bytes(evaluation, field))
+    vs, qs = v.reshape(-1, 16), q.reshape(-1, 16, q.shape[1])
+    for d in range(1, 16):
+        pos = ((vs[:, : 16 - d, None] * qs[:, d:, :]) % p).sum(axis=(0, 1)) % p
+        neg = ((vs[:, d:, None] * qs[:, : 16 - d, :]) % p).sum(axis=(0, 1)) % p
+        assert np.array_equal(pos, ext_from_bytes(positive[d - 1], field)), d
+        assert np.array_equal(neg, ext_from_bytes(negative[d - 1], field)), d
