@@ -1,4 +1,5 @@
-"""The C-ABI library loads, exports every declared symbol, and fails loudly without a GPU."""
+"""The C-ABI library loads, exports every declared symbol, refuses malformed
+inputs, and fails loudly without a GPU."""
 import re
 from pathlib import Path
 
@@ -81,3 +82,31 @@ def test_wrong_weight_width_rejected():
     p = qf.Parameters(qf.demo_shapes(), qf.Config(chunk_log=10, packed_log=4), field=qf.FIELD_KOALABEAR)
     with pytest.raises(qf.QfError, match="int16"):
         p.commit_recomputed(torch.zeros(p.active, dtype=torch.int8))
+
+
+@pytest.mark.parametrize("field", [qf.FIELD_F65521, qf.FIELD_KOALABEAR])
+def test_malformed_inputs_rejected(field):
+    """end_to_end.rs:194-213: no matrices, a zero dimension and a dimension
+    whose size overflows are refused; a BVA one value short and a claim with a
+    missing coordinate are rejected."""
+    import dataclasses
+    import oracle
+    from parcomm_b200 import layout
+    cfg = qf.Config(chunk_log=10, packed_log=4)
+    for shapes, msg in (([], "invalid matrix count"), ([(0, 1)], "invalid matrix shape"),
+                        ([(2**64 - 1, 2)], "invalid matrix shape")):
+        with pytest.raises(qf.QfError, match=msg):
+            qf.Parameters(shapes, cfg, field=field)
+    name = "f65521" if field == qf.FIELD_F65521 else "koalabear"
+    shapes = [(3, 5)]
+    import numpy as np
+    bva = layout.encode(shapes, layout.demo_matrices(shapes, dtype=np.int8 if name == "f65521" else np.int16))
+    with pytest.raises(oracle.OracleError, match="active BVA length"):
+        oracle.prove(shapes, 10, 4, bva[:-1], field=name)
+    roots, claims, proof, _ = oracle.prove(shapes, 10, 4, bva, field=name)
+    p = qf.Parameters(shapes, cfg, field=field)
+    c = qf.claims_from_bytes(p.shapes, claims)[0]
+    with pytest.raises(qf.QfError):
+        p.verify([roots], [dataclasses.replace(c, row=c.row[:-1])], proof)
+    assert not oracle.verify(shapes, 10, 4, roots, claims[16:], proof, field=name)
+    p.verify([roots], [c], proof)
