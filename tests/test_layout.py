@@ -27,3 +27,16 @@ def test_intervals_last_doubled():
     assert layout.intervals(31) == [(0, 16), (16, 8), (24, 4), (28, 4)]
     assert layout.intervals(37) == [(0, 32), (32, 4), (36, 1)]
     assert layout.intervals(128256) == [(0, 65536), (65536, 32768), (98304, 16384), (114688, 16384)]
+
+
+def test_layout_of_a_70b_scale_matrix_without_its_weights():
+    """cpu_optimization.rs:33-40: a 2^18 x (2^18 + 16) matrix lays out to more
+    than 2^36 active entries in 2^37 logical ones, 128 blocks of 2^30; a
+    2^20 x 2^20 matrix exceeds the 2^37-entry capacity and is refused."""
+    _, active, logical = layout.buckets([(1 << 18, (1 << 18) + 16)])
+    assert active > 1 << 36 and logical == 1 << 37 and logical // (1 << 30) == 128
+    p = qf.Parameters([(1 << 18, (1 << 18) + 16)], qf.Config(chunk_log=30, packed_log=4))
+    assert (p.active, p.logical, p.blocks) == (active, logical, 128)
+    import pytest
+    with pytest.raises(qf.QfError, match="matrix exceeds supported capacity"):
+        qf.Parameters([(1 << 20, 1 << 20)], qf.Config(chunk_log=30, packed_log=4))
