@@ -56,6 +56,8 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_uint32, BPP,
                                          ctypes.POINTER(S)]
+        for name in ("qfo_field_ops", "qfo_field_ops_kb"):
+            getattr(L, name).argtypes = [ctypes.c_char_p, ctypes.c_char_p, S, P, P, P]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -157,6 +159,15 @@ def tbv_dense(shapes, chunk_log, packed_log, values, claims: bytes, stride=16, r
         pos += 16 * k
     dense, (claim,), point, (evaluation,), positive, negative = parts
     return dense, claim, point, evaluation, positive, negative
+
+
+def field_ops(a: bytes, b: bytes, field="f65521"):
+    """Element-wise (a * b, a^-1 with 0 for 0, a^p) of canonical 16-byte
+    elements, as concatenated bytes."""
+    assert len(a) == len(b) and len(a) % 16 == 0
+    out = [ctypes.create_string_buffer(len(a)) for _ in range(3)]
+    _check(getattr(lib(), "qfo_field_ops" + _SUFFIX[field][0])(a, b, len(a) // 16, *out))
+    return tuple(o.raw for o in out)
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

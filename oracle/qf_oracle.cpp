@@ -291,6 +291,20 @@ int tbv_dense_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, 
     *out_len = w.out.size();
   });
 }
+// Element-wise a * b, a^-1 (0 for a = 0) and a^p (one Frobenius step) of n
+// canonical 16-byte elements each, for checks against the definitions.
+template <class G>
+int field_ops_impl(const uint8_t* a, const uint8_t* b, size_t n, uint8_t* prod, uint8_t* inv, uint8_t* frob) {
+  return guarded([&] {
+    for (size_t i = 0; i < n; ++i) {
+      G x, y;
+      if (!G::from_bytes(a + 16 * i, x) || !G::from_bytes(b + 16 * i, y)) fail(-9, "non-canonical element");
+      (x * y).to_bytes(prod + 16 * i);
+      (x.is_zero() ? G::zero() : x.inverse()).to_bytes(inv + 16 * i);
+      x.frobenius(1).to_bytes(frob + 16 * i);
+    }
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -418,6 +432,14 @@ int qfo_tbv_dense_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log
                      uint8_t** out, size_t* out_len) {
   return tbv_dense_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
                                       claims_len, stride, out, out_len);
+}
+
+// The extension fields' product, inverse and Frobenius step, element-wise.
+int qfo_field_ops(const uint8_t* a, const uint8_t* b, size_t n, uint8_t* prod, uint8_t* inv, uint8_t* frob) {
+  return field_ops_impl<Fp8>(a, b, n, prod, inv, frob);
+}
+int qfo_field_ops_kb(const uint8_t* a, const uint8_t* b, size_t n, uint8_t* prod, uint8_t* inv, uint8_t* frob) {
+  return field_ops_impl<Kb4>(a, b, n, prod, inv, frob);
 }
 
 }  // extern "C"
