@@ -58,6 +58,14 @@ def lib() -> ctypes.CDLL:
                                          ctypes.POINTER(S)]
         for name in ("qfo_field_ops", "qfo_field_ops_kb"):
             getattr(L, name).argtypes = [ctypes.c_char_p, ctypes.c_char_p, S, P, P, P]
+        for name in ("qfo_packed_open", "qfo_packed_open_kb"):
+            getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, P,
+                                         ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, ctypes.c_char_p, BPP,
+                                         ctypes.POINTER(S)]
+        for name in ("qfo_packed_verify", "qfo_packed_verify_kb"):
+            getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p,
+                                         ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, S,
+                                         ctypes.c_char_p, S]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -168,6 +176,26 @@ def field_ops(a: bytes, b: bytes, field="f65521"):
     out = [ctypes.create_string_buffer(len(a)) for _ in range(3)]
     _check(getattr(lib(), "qfo_field_ops" + _SUFFIX[field][0])(a, b, len(a) // 16, *out))
     return tuple(o.raw for o in out)
+
+
+def packed_open(log_n, columns, bits, seed: bytes, values, point: bytes, ctx: bytes, field="f65521"):
+    """Single-block packed PCS: commit the 2^log_n canonical base values, open
+    at `point` (log_n elements).  Returns (root, claimed value, proof bytes)."""
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    assert v.size == 1 << log_n and len(seed) == 32 and len(point) == 16 * log_n
+    root, value = ctypes.create_string_buffer(32), ctypes.create_string_buffer(16)
+    out, size = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+    _check(getattr(lib(), "qfo_packed_open" + _SUFFIX[field][0])(log_n, columns, bits, seed, v.ctypes.data, point, ctx,
+                                                                len(ctx), root, value, ctypes.byref(out),
+                                                                ctypes.byref(size)))
+    return root.raw, value.raw, _take(out, size)
+
+
+def packed_verify(log_n, columns, bits, seed: bytes, root: bytes, point: bytes, value: bytes, proof: bytes, ctx: bytes,
+                  field="f65521") -> bool:
+    rc = getattr(lib(), "qfo_packed_verify" + _SUFFIX[field][0])(log_n, columns, bits, seed, root, point, value, proof,
+                                                                len(proof), ctx, len(ctx))
+    return rc == 0
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -305,6 +305,53 @@ int field_ops_impl(const uint8_t* a, const uint8_t* b, size_t n, uint8_t* prod, 
     }
   });
 }
+// The single-block packed PCS (PackedPcs::{new, commit, open, verify},
+// packed.rs:132-484) over a table of 2^log_n base-field values given as
+// canonical integers: commit, open at `point` (log_n elements) under `ctx`;
+// outputs the root, the claimed value and the opening's bytes.
+template <class G>
+int packed_open_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], const int32_t* values,
+                     const uint8_t* point, const uint8_t* ctx, size_t ctx_len, uint8_t root[32], uint8_t value[16],
+                     uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    std::array<uint8_t, 32> sd;
+    std::memcpy(sd.data(), seed, 32);
+    Parameters<G> P;
+    P.pcs = PackedPcs<G>::create(log_n, columns, bits, sd);
+    P.block_len = size_t(1) << log_n;
+    for (size_t i = 0; i < P.block_len; ++i)
+      if (values[i] < 0 || uint64_t(values[i]) >= G::modulus_u64()) fail(-9, "non-canonical base value");
+    qf_oracle::CpuBackend<G, int32_t> be(P, values, P.block_len);
+    const Digest d = be.commit();
+    std::vector<G> pt;
+    ByteReader r(point, 16 * size_t(log_n));
+    for (uint32_t i = 0; i < log_n; ++i) pt.push_back(r.field<G>());
+    BatchOpening<G> op = open_single(P.pcs, be, d, pt, std::vector<uint8_t>(ctx, ctx + ctx_len));
+    std::memcpy(root, d.data(), 32);
+    op.claimed_value.to_bytes(value);
+    *proof = dup(op.wire);
+    *proof_len = op.wire.size();
+  });
+}
+template <class G>
+int packed_verify_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], const uint8_t root[32],
+                       const uint8_t* point, const uint8_t value[16], const uint8_t* proof, size_t proof_len,
+                       const uint8_t* ctx, size_t ctx_len) {
+  return guarded([&] {
+    std::array<uint8_t, 32> sd;
+    std::memcpy(sd.data(), seed, 32);
+    PackedPcs<G> pcs = PackedPcs<G>::create(log_n, columns, bits, sd);
+    Digest d;
+    std::memcpy(d.data(), root, 32);
+    std::vector<G> pt;
+    ByteReader r(point, 16 * size_t(log_n));
+    for (uint32_t i = 0; i < log_n; ++i) pt.push_back(r.field<G>());
+    ByteReader rv(value, 16);
+    const G v = rv.field<G>();
+    if (!verify_single(pcs, d, pt, v, proof, proof_len, std::vector<uint8_t>(ctx, ctx + ctx_len)))
+      fail(QF_E_INVALID_COMMITMENT, "packed opening rejected");
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -440,6 +487,28 @@ int qfo_field_ops(const uint8_t* a, const uint8_t* b, size_t n, uint8_t* prod, u
 }
 int qfo_field_ops_kb(const uint8_t* a, const uint8_t* b, size_t n, uint8_t* prod, uint8_t* inv, uint8_t* frob) {
   return field_ops_impl<Kb4>(a, b, n, prod, inv, frob);
+}
+
+// Single-block packed PCS open and verify over canonical base values.
+int qfo_packed_open(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], const int32_t* values,
+                    const uint8_t* point, const uint8_t* ctx, size_t ctx_len, uint8_t root[32], uint8_t value[16],
+                    uint8_t** proof, size_t* proof_len) {
+  return packed_open_impl<Fp8>(log_n, columns, bits, seed, values, point, ctx, ctx_len, root, value, proof, proof_len);
+}
+int qfo_packed_open_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], const int32_t* values,
+                       const uint8_t* point, const uint8_t* ctx, size_t ctx_len, uint8_t root[32], uint8_t value[16],
+                       uint8_t** proof, size_t* proof_len) {
+  return packed_open_impl<Kb4>(log_n, columns, bits, seed, values, point, ctx, ctx_len, root, value, proof, proof_len);
+}
+int qfo_packed_verify(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], const uint8_t root[32],
+                      const uint8_t* point, const uint8_t value[16], const uint8_t* proof, size_t proof_len,
+                      const uint8_t* ctx, size_t ctx_len) {
+  return packed_verify_impl<Fp8>(log_n, columns, bits, seed, root, point, value, proof, proof_len, ctx, ctx_len);
+}
+int qfo_packed_verify_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], const uint8_t root[32],
+                         const uint8_t* point, const uint8_t value[16], const uint8_t* proof, size_t proof_len,
+                         const uint8_t* ctx, size_t ctx_len) {
+  return packed_verify_impl<Kb4>(log_n, columns, bits, seed, root, point, value, proof, proof_len, ctx, ctx_len);
 }
 
 }  // extern "C"

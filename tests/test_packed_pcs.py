@@ -1,0 +1,96 @@
+"""The single-block packed PCS against the multilinear extension of the
+original base table, computed here from its definition without the packing
+helpers (after vendor/qafold/tests/packed.rs:10-112): an extension-field
+point, each of the eight lanes packed into one element (the last three
+coordinates, most significant first), and Boolean points that select single
+entries.  Each opening must claim the table's value and verify; another
+value or a flipped proof byte must not."""
+import numpy as np
+import pytest
+
+import oracle
+from test_oracle_claims import FIELDS, ext_from_bytes, ext_mul, ext_to_bytes
+
+SEED = bytes([91]) * 32
+CTX = b"packed-pcs/integration-tests/v1"
+
+
+def table(field, log_n, seed):
+    return np.random.default_rng(seed).integers(0, FIELDS[field][0], size=1 << log_n, dtype=np.int64)
+
+
+def ext_point(field, log_n, seed):
+    """Coordinates with a nonzero coefficient above the base field."""
+    p, d, _, _, _ = FIELDS[field]
+    pt = np.random.default_rng(seed).integers(0, p, size=(log_n, d), dtype=np.int64)
+    pt[:, 1] = np.maximum(pt[:, 1], 1)
+    return pt
+
+
+def base_point(field, bits):
+    d = FIELDS[field][1]
+    pt = np.zeros((len(bits), d), dtype=np.int64)
+    pt[:, 0] = bits
+    return pt
+
+
+def original_mle(values, point, field):
+    """Fold the table on its most significant index bit first:
+    t[i] <- t[i] (1 - x) + t[half + i] x."""
+    p, d, _, _, _ = FIELDS[field]
+    t = np.zeros((values.size, d), dtype=np.int64)
+    t[:, 0] = values % p
+    one = np.zeros(d, dtype=np.int64)
+    one[0] = 1
+    for x in point:
+        half = len(t) // 2
+        t = (ext_mul(t[:half], ((one - x) % p)[None, :], field) + ext_mul(t[half:], x[None, :], field)) % p
+    return t[0]
+
+
+def open_and_check(field, log_n, values, point):
+    pb = b"".join(ext_to_bytes(x, field) for x in point)
+    root, value, proof = oracle.packed_open(log_n, 4, 32, SEED, values, pb, CTX, field=field)
+    assert np.array_equal(ext_from_bytes(value, field), original_mle(values, point, field))
+    assert oracle.packed_verify(log_n, 4, 32, SEED, root, pb, value, proof, CTX, field=field)
+    return root, pb, value, proof
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_extension_point_authenticates_the_original_table(field):
+    log_n = 9
+    values = table(field, log_n, 1)
+    root, pb, value, proof = open_and_check(field, log_n, values, ext_point(field, log_n, 2))
+    other = bytearray(value)
+    other[0] ^= 1
+    assert not oracle.packed_verify(log_n, 4, 32, SEED, root, pb, bytes(other), proof, CTX, field=field)
+    for pos in (0, 40, len(proof) // 2, len(proof) - 1):
+        bad = bytearray(proof)
+        bad[pos] ^= 0x10
+        assert not oracle.packed_verify(log_n, 4, 32, SEED, root, pb, value, bytes(bad), CTX, field=field)
+    assert not oracle.packed_verify(log_n, 4, 32, SEED, root, pb, value, proof, CTX + b"x", field=field)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_each_lane_is_selected_by_the_last_coordinates(field):
+    """An element packs 2^k adjacent entries (k = 3 for F65521^8, 2 for
+    KoalaBear^4); Boolean values of the last k coordinates, most significant
+    first, pick one lane."""
+    log_n = 7
+    lane_bits = FIELDS[field][1].bit_length() - 1
+    values = table(field, log_n, 3)
+    for lane in range(1 << lane_bits):
+        pt = ext_point(field, log_n, 4)
+        for bit in range(lane_bits):
+            pt[log_n - lane_bits + bit] = base_point(field, [(lane >> (lane_bits - 1 - bit)) & 1])[0]
+        open_and_check(field, log_n, values, pt)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_boolean_points_select_the_original_entry(field):
+    log_n = 6
+    values = table(field, log_n, 5)
+    for index in (0, 1, 7, 8, (1 << log_n) - 1):
+        bits = [(index >> (log_n - 1 - b)) & 1 for b in range(log_n)]
+        root, pb, value, proof = open_and_check(field, log_n, values, base_point(field, bits))
+        assert ext_from_bytes(value, field)[0] == values[index] and not ext_from_bytes(value, field)[1:].any()
