@@ -66,6 +66,17 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p,
                                          ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, S,
                                          ctypes.c_char_p, S]
+        for name in ("qfo_packed_open_batch", "qfo_packed_open_batch_kb"):
+            getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p,
+                                         ctypes.c_uint32, P, ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p,
+                                         ctypes.c_char_p, BPP, ctypes.POINTER(S)]
+        for name in ("qfo_packed_verify_batch", "qfo_packed_verify_batch_kb"):
+            getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p,
+                                         ctypes.c_uint32, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32,
+                                         ctypes.c_char_p, ctypes.c_char_p, S, ctypes.c_char_p, S]
+        for name in ("qfo_codeword_fold", "qfo_codeword_fold_kb"):
+            getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p,
+                                         ctypes.c_uint32, P, P, ctypes.c_char_p, P, ctypes.POINTER(ctypes.c_int)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -196,6 +207,43 @@ def packed_verify(log_n, columns, bits, seed: bytes, root: bytes, point: bytes, 
     rc = getattr(lib(), "qfo_packed_verify" + _SUFFIX[field][0])(log_n, columns, bits, seed, root, point, value, proof,
                                                                 len(proof), ctx, len(ctx))
     return rc == 0
+
+
+def packed_open_batch(log_n, columns, bits, seed: bytes, blocks, values, point: bytes, ctx: bytes, field="f65521"):
+    """Batched packed PCS over `blocks` tables of 2^log_n canonical base
+    values (block after block): returns (roots, claimed value, proof bytes)."""
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    assert v.size == blocks << log_n and len(seed) == 32
+    roots, value = ctypes.create_string_buffer(32 * blocks), ctypes.create_string_buffer(16)
+    out, size = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+    _check(getattr(lib(), "qfo_packed_open_batch" + _SUFFIX[field][0])(log_n, columns, bits, seed, blocks, v.ctypes.data,
+                                                                      point, ctx, len(ctx), roots, value,
+                                                                      ctypes.byref(out), ctypes.byref(size)))
+    return roots.raw, value.raw, _take(out, size)
+
+
+def packed_verify_batch(log_n, columns, bits, seed: bytes, roots: bytes, point: bytes, value: bytes, proof: bytes,
+                        ctx: bytes, field="f65521") -> bool:
+    rc = getattr(lib(), "qfo_packed_verify_batch" + _SUFFIX[field][0])(log_n, columns, bits, seed, len(roots) // 32,
+                                                                      roots, point, len(point) // 16, value, proof,
+                                                                      len(proof), ctx, len(ctx))
+    return rc == 0
+
+
+def codeword_fold_accepted(log_n, columns, bits, pcs_seed: bytes, blocks, values, fold_weights, seed: bytes,
+                           check_weights, field="f65521") -> bool:
+    """Fold the blocks with `fold_weights`, write the binding rows that `seed`
+    samples, and return whether the verifier accepts them under `check_weights`
+    (base-field weights, one per block)."""
+    v = np.ascontiguousarray(values, dtype=np.int32)
+    fw = np.ascontiguousarray(fold_weights, dtype=np.uint32)
+    cw = np.ascontiguousarray(check_weights, dtype=np.uint32)
+    assert v.size == blocks << log_n and fw.size == cw.size == blocks
+    ok = ctypes.c_int()
+    _check(getattr(lib(), "qfo_codeword_fold" + _SUFFIX[field][0])(log_n, columns, bits, pcs_seed, blocks,
+                                                                  v.ctypes.data, fw.ctypes.data, seed, cw.ctypes.data,
+                                                                  ctypes.byref(ok)))
+    return bool(ok.value)
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -352,6 +352,91 @@ int packed_verify_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const ui
       fail(QF_E_INVALID_COMMITMENT, "packed opening rejected");
   });
 }
+// The batched packed PCS (open_batch_impl, packed_batch.rs:139-319) over
+// `blocks` tables of 2^log_n canonical base values each: every block
+// committed, then one opening at `point` (log_n + log2(blocks) elements, the
+// block coordinates first).  Outputs the blocks' roots, the claimed value
+// and the opening's bytes.
+template <class G>
+int packed_open_batch_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], uint32_t blocks,
+                           const int32_t* values, const uint8_t* point, const uint8_t* ctx, size_t ctx_len,
+                           uint8_t* roots, uint8_t value[16], uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    if (blocks < 2 || !is_pow2(blocks)) fail(-9, "blocks");
+    std::array<uint8_t, 32> sd;
+    std::memcpy(sd.data(), seed, 32);
+    Parameters<G> P;
+    P.pcs = PackedPcs<G>::create(log_n, columns, bits, sd);
+    P.block_len = size_t(1) << log_n;
+    const size_t n = P.block_len * blocks;
+    for (size_t i = 0; i < n; ++i)
+      if (values[i] < 0 || uint64_t(values[i]) >= G::modulus_u64()) fail(-9, "non-canonical base value");
+    qf_oracle::CpuBackend<G, int32_t> be(P, values, n);
+    std::vector<Digest> rs;
+    for (uint32_t b = 0; b < blocks; ++b) rs.push_back(be.commit_block(b));
+    const size_t k = log_n + ilog2(blocks);
+    std::vector<G> pt;
+    ByteReader r(point, 16 * k);
+    for (size_t i = 0; i < k; ++i) pt.push_back(r.field<G>());
+    BatchOpening<G> op = open_batch(P.pcs, be, rs, pt, std::vector<uint8_t>(ctx, ctx + ctx_len));
+    for (uint32_t b = 0; b < blocks; ++b) std::memcpy(roots + 32 * b, rs[b].data(), 32);
+    op.claimed_value.to_bytes(value);
+    *proof = dup(op.wire);
+    *proof_len = op.wire.size();
+  });
+}
+template <class G>
+int packed_verify_batch_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], uint32_t blocks,
+                             const uint8_t* roots, const uint8_t* point, uint32_t point_len, const uint8_t value[16],
+                             const uint8_t* proof, size_t proof_len, const uint8_t* ctx, size_t ctx_len) {
+  return guarded([&] {
+    std::array<uint8_t, 32> sd;
+    std::memcpy(sd.data(), seed, 32);
+    PackedPcs<G> pcs = PackedPcs<G>::create(log_n, columns, bits, sd);
+    std::vector<Digest> rs(blocks);
+    for (uint32_t b = 0; b < blocks; ++b) std::memcpy(rs[b].data(), roots + 32 * b, 32);
+    std::vector<G> pt;
+    ByteReader r(point, 16 * size_t(point_len));
+    for (uint32_t i = 0; i < point_len; ++i) pt.push_back(r.field<G>());
+    ByteReader rv(value, 16);
+    const G v = rv.field<G>();
+    if (!verify_batch(pcs, rs, pt, v, proof, proof_len, std::vector<uint8_t>(ctx, ctx + ctx_len)))
+      fail(QF_E_INVALID_COMMITMENT, "batch opening rejected");
+  });
+}
+// The codeword-fold binding (prove/verify_codeword_fold,
+// qafold_short_batch.rs:77-240): the blocks are folded with the base weights
+// `fold_w`, the folded codeword committed, and the binding rows sampled by
+// `seed` written; the verifier then checks them against the block roots
+// under the weights `check_w`.  `accepted` <- the verifier's answer.
+template <class G>
+int codeword_fold_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t pcs_seed[32], uint32_t blocks,
+                       const int32_t* values, const uint32_t* fold_w, const uint8_t seed[32], const uint32_t* check_w,
+                       int* accepted) {
+  return guarded([&] {
+    if (blocks < 2 || !is_pow2(blocks)) fail(-9, "blocks");
+    std::array<uint8_t, 32> sd;
+    std::memcpy(sd.data(), pcs_seed, 32);
+    Parameters<G> P;
+    P.pcs = PackedPcs<G>::create(log_n, columns, bits, sd);
+    P.block_len = size_t(1) << log_n;
+    qf_oracle::CpuBackend<G, int32_t> be(P, values, P.block_len * blocks);
+    std::vector<Digest> rs;
+    for (uint32_t b = 0; b < blocks; ++b) rs.push_back(be.commit_block(b));
+    std::vector<G> fw, cw;
+    for (uint32_t b = 0; b < blocks; ++b) {
+      fw.push_back(G::from_base(fold_w[b] % uint32_t(G::modulus_u64())));
+      cw.push_back(G::from_base(check_w[b] % uint32_t(G::modulus_u64())));
+    }
+    const Digest folded = be.fold_and_commit(fw);
+    Digest s;
+    std::memcpy(s.data(), seed, 32);
+    const auto& pp = *P.pcs.pp;
+    RowSelection sel = make_selection(pp.num_queries(pp.levels() - 1, pp.top_ext_rows()), pp.top_ext_rows(), s);
+    const std::vector<uint8_t> binding = be.binding_rows(sel, rs);
+    *accepted = verify_codeword_fold(pp, rs, cw, folded, s, binding.data(), binding.size()) ? 1 : 0;
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -509,6 +594,44 @@ int qfo_packed_verify_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const 
                          const uint8_t* point, const uint8_t value[16], const uint8_t* proof, size_t proof_len,
                          const uint8_t* ctx, size_t ctx_len) {
   return packed_verify_impl<Kb4>(log_n, columns, bits, seed, root, point, value, proof, proof_len, ctx, ctx_len);
+}
+
+// Batched packed PCS open and verify over canonical base values.
+int qfo_packed_open_batch(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], uint32_t blocks,
+                          const int32_t* values, const uint8_t* point, const uint8_t* ctx, size_t ctx_len, uint8_t* roots,
+                          uint8_t value[16], uint8_t** proof, size_t* proof_len) {
+  return packed_open_batch_impl<Fp8>(log_n, columns, bits, seed, blocks, values, point, ctx, ctx_len, roots, value, proof,
+                                     proof_len);
+}
+int qfo_packed_open_batch_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], uint32_t blocks,
+                             const int32_t* values, const uint8_t* point, const uint8_t* ctx, size_t ctx_len,
+                             uint8_t* roots, uint8_t value[16], uint8_t** proof, size_t* proof_len) {
+  return packed_open_batch_impl<Kb4>(log_n, columns, bits, seed, blocks, values, point, ctx, ctx_len, roots, value, proof,
+                                     proof_len);
+}
+int qfo_packed_verify_batch(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], uint32_t blocks,
+                            const uint8_t* roots, const uint8_t* point, uint32_t point_len, const uint8_t value[16],
+                            const uint8_t* proof, size_t proof_len, const uint8_t* ctx, size_t ctx_len) {
+  return packed_verify_batch_impl<Fp8>(log_n, columns, bits, seed, blocks, roots, point, point_len, value, proof, proof_len,
+                                       ctx, ctx_len);
+}
+int qfo_packed_verify_batch_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t seed[32], uint32_t blocks,
+                               const uint8_t* roots, const uint8_t* point, uint32_t point_len, const uint8_t value[16],
+                               const uint8_t* proof, size_t proof_len, const uint8_t* ctx, size_t ctx_len) {
+  return packed_verify_batch_impl<Kb4>(log_n, columns, bits, seed, blocks, roots, point, point_len, value, proof, proof_len,
+                                       ctx, ctx_len);
+}
+
+// Codeword-fold binding made under one set of block weights, checked under another.
+int qfo_codeword_fold(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t pcs_seed[32], uint32_t blocks,
+                      const int32_t* values, const uint32_t* fold_w, const uint8_t seed[32], const uint32_t* check_w,
+                      int* accepted) {
+  return codeword_fold_impl<Fp8>(log_n, columns, bits, pcs_seed, blocks, values, fold_w, seed, check_w, accepted);
+}
+int qfo_codeword_fold_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const uint8_t pcs_seed[32], uint32_t blocks,
+                         const int32_t* values, const uint32_t* fold_w, const uint8_t seed[32], const uint32_t* check_w,
+                         int* accepted) {
+  return codeword_fold_impl<Kb4>(log_n, columns, bits, pcs_seed, blocks, values, fold_w, seed, check_w, accepted);
 }
 
 }  // extern "C"

@@ -94,3 +94,61 @@ def test_boolean_points_select_the_original_entry(field):
         bits = [(index >> (log_n - 1 - b)) & 1 for b in range(log_n)]
         root, pb, value, proof = open_and_check(field, log_n, values, base_point(field, bits))
         assert ext_from_bytes(value, field)[0] == values[index] and not ext_from_bytes(value, field)[1:].any()
+
+
+def source(field, blocks, log_n):
+    """index * 7927 + block * 65519 + 31, reduced (packed_batch_tests.rs:3-9)."""
+    p = FIELDS[field][0]
+    idx = np.arange(1 << log_n, dtype=np.int64)
+    return np.concatenate([(idx * 7927 + b * 65519 + 31) % p for b in range(blocks)])
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+@pytest.mark.parametrize("blocks,log_n", [(2, 10), (4, 10), (8, 10), (64, 10), (2, 16)])
+def test_batch_opening_equals_the_concatenated_tables_extension(field, blocks, log_n):
+    """After packed_batch_tests.rs:40-140: the batch opening claims the
+    multilinear extension of the blocks' tables laid end to end (the block
+    coordinates first), Boolean coordinates included, and verifies; another
+    context, a missing or altered root, a flipped byte in each wire section,
+    and a wire one byte longer or shorter are rejected."""
+    lanes = FIELDS[field][1]
+    values = source(field, blocks, log_n)
+    k = log_n + blocks.bit_length() - 1
+    pt = ext_point(field, k, 10 * blocks + log_n)
+    if blocks == 4:
+        pt[0], pt[1], pt[log_n] = base_point(field, [0, 1, 1])
+    pb = b"".join(ext_to_bytes(x, field) for x in pt)
+    seed = bytes([0x51]) * 32
+    ctx = b"batch-test"
+    roots, value, wire = oracle.packed_open_batch(log_n, 32, 100, seed, blocks, values, pb, ctx, field=field)
+    assert np.array_equal(ext_from_bytes(value, field), original_mle(values, pt, field))
+    verify = lambda r=roots, w=wire, c=ctx: oracle.packed_verify_batch(log_n, 32, 100, seed, r, pb, value, w, c,
+                                                                      field=field)
+    assert verify()
+    assert not verify(c=b"different-context")
+    assert not verify(r=roots[:-32])
+    for b in range(blocks):
+        bad = bytearray(roots)
+        bad[32 * b] ^= 1
+        assert not verify(r=bytes(bad))
+    cross = 8 + 16 + lanes * 16
+    folded_root = cross + 2 * (blocks - 1) * 16
+    final = folded_root + 32 + (log_n - (lanes.bit_length() - 1)) * 32
+    binding = final + 16 + 8
+    for offset in (0, 8, 24, cross, folded_root, final, binding, len(wire) - 1):
+        bad = bytearray(wire)
+        bad[offset] ^= 1
+        assert not verify(w=bytes(bad)), f"accepted a flipped byte at {offset}"
+    assert not verify(w=wire + b"\0")
+    assert not verify(w=wire[:-1])
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_fold_binding_under_other_weights_is_rejected(field):
+    """packed_batch_tests.rs:142-165: a folded commitment made with the block
+    weights (1, 1) binds under (1, 1) and is rejected under (1, 2)."""
+    values = source(field, 2, 10)
+    seed, pcs_seed = bytes([0x78]) * 32, bytes([0x51]) * 32
+    assert oracle.codeword_fold_accepted(10, 32, 100, pcs_seed, 2, values, [1, 1], seed, [1, 1], field=field)
+    assert not oracle.codeword_fold_accepted(10, 32, 100, pcs_seed, 2, values, [1, 1], seed, [1, 2], field=field)
+    assert oracle.codeword_fold_accepted(10, 32, 100, pcs_seed, 2, values, [1, 2], seed, [1, 2], field=field)
