@@ -16,6 +16,8 @@ LIB = HERE / "libqforacle.so"
 _lib = None
 # int gather(void* ctx, const void* in, size_t n, void* out)
 GATHER = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+# int reduce(void* ctx, uint64_t* data, size_t n)
+REDUCE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_size_t)
 
 
 def build() -> Path:
@@ -50,8 +52,8 @@ def lib() -> ctypes.CDLL:
         for name in ("qfo_prove_sharded", "qfo_prove_sharded_kb"):
             getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_int,
-                                         ctypes.c_int, GATHER, P, BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S), BPP,
-                                         ctypes.POINTER(S)]
+                                         ctypes.c_int, GATHER, REDUCE, P, BPP, ctypes.POINTER(S), BPP,
+                                         ctypes.POINTER(S), BPP, ctypes.POINTER(S)]
         for name in ("qfo_tbv_dense", "qfo_tbv_dense_kb"):
             getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_uint32, BPP,
@@ -129,10 +131,12 @@ def prove(shapes, chunk_log, packed_log, values, claims: bytes | None = None, rf
 
 
 def prove_sharded(shapes, chunk_log, packed_log, values, rank, world, all_gather, claims: bytes | None = None,
-                  rf_bits=100, field="f65521"):
+                  rf_bits=100, field="f65521", all_reduce=None):
     """One rank of a block-sharded proof, the CPU shard standing in for the
     rank's device.  `all_gather(data: bytes) -> bytes` returns every rank's
-    bytes in rank order.  Returns (roots, claims, proof)."""
+    bytes in rank order; `all_reduce(a: np.ndarray)`, if given, sums a uint64
+    array over the ranks in place (else sums go through the gather).
+    Returns (roots, claims, proof)."""
     sfx, dt = _SUFFIX[field]
     arr, n = _shapes(shapes)
     v = np.ascontiguousarray(values, dtype=dt)
@@ -147,11 +151,19 @@ def prove_sharded(shapes, chunk_log, packed_log, values, rank, world, all_gather
         except Exception:  # the C side turns a nonzero status into an error
             return 1
 
+    def reduce(_ctx, data, size):
+        try:
+            all_reduce(np.ctypeslib.as_array(data, shape=(size,)))
+            return 0
+        except Exception:
+            return 1
+
     cb = GATHER(gather)
+    rcb = REDUCE(reduce) if all_reduce is not None else ctypes.cast(None, REDUCE)
     outs = [ctypes.POINTER(ctypes.c_uint8)() for _ in range(3)]
     lens = [ctypes.c_size_t() for _ in range(3)]
     _check(getattr(lib(), "qfo_prove_sharded" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size,
-                                                    claims, len(claims) if claims else 0, rank, world, cb, None,
+                                                    claims, len(claims) if claims else 0, rank, world, cb, rcb, None,
                                                     ctypes.byref(outs[0]), ctypes.byref(lens[0]), ctypes.byref(outs[1]),
                                                     ctypes.byref(lens[1]), ctypes.byref(outs[2]), ctypes.byref(lens[2])))
     return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2])

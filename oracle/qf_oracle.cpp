@@ -200,8 +200,9 @@ int verify_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uin
 template <class G, class T>
 int prove_sharded_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
                        const T* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, int rank, int world,
-                       CallbackComm::Fn gather, void* gather_ctx, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
-                       size_t* claims_out_len, uint8_t** proof, size_t* proof_len) {
+                       CallbackComm::Fn gather, CallbackComm::ReduceFn reduce, void* comm_ctx, uint8_t** roots,
+                       size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof,
+                       size_t* proof_len) {
   return guarded([&] {
     Config c;
     c.chunk_log = chunk_log;
@@ -209,7 +210,7 @@ int prove_sharded_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_l
     c.query_rf_bits = rf_bits;
     auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
     validate_values(P->layout, bva, n_values);
-    CallbackComm comm(rank, world, gather, gather_ctx);
+    CallbackComm comm(rank, world, gather, comm_ctx, reduce);
     BlockShards shards(P->blocks(), world);
     qf_oracle::CpuShard<G, T> shard(*P, bva, n_values, shards, rank);
     ShardedBackend<G> be(*P, shard, comm);
@@ -533,21 +534,24 @@ int qfo_range_audit_kb(const int16_t* values, uint64_t n, const uint8_t seed[32]
 
 // One rank of a block-sharded proof; `gather(ctx, in, n, out)` is the
 // all-gather over the `world` ranks (out = every rank's n bytes, in rank
-// order; returns 0 on success).  Outputs as qfo_prove's.
+// order) and `reduce(ctx, data, n)`, which may be null, the sum of n 64-bit
+// integers over the ranks; both return 0 on success.  Outputs as qfo_prove's.
 int qfo_prove_sharded(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
                       const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, int rank, int world,
-                      CallbackComm::Fn gather, void* gather_ctx, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
-                      size_t* claims_out_len, uint8_t** proof, size_t* proof_len) {
+                      CallbackComm::Fn gather, CallbackComm::ReduceFn reduce, void* comm_ctx, uint8_t** roots,
+                      size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof,
+                      size_t* proof_len) {
   return prove_sharded_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
-                                         claims_len, rank, world, gather, gather_ctx, roots, roots_len, claims_out,
+                                         claims_len, rank, world, gather, reduce, comm_ctx, roots, roots_len, claims_out,
                                          claims_out_len, proof, proof_len);
 }
 int qfo_prove_sharded_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
                          const int16_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, int rank,
-                         int world, CallbackComm::Fn gather, void* gather_ctx, uint8_t** roots, size_t* roots_len,
-                         uint8_t** claims_out, size_t* claims_out_len, uint8_t** proof, size_t* proof_len) {
+                         int world, CallbackComm::Fn gather, CallbackComm::ReduceFn reduce, void* comm_ctx,
+                         uint8_t** roots, size_t* roots_len, uint8_t** claims_out, size_t* claims_out_len,
+                         uint8_t** proof, size_t* proof_len) {
   return prove_sharded_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
-                                          claims_len, rank, world, gather, gather_ctx, roots, roots_len, claims_out,
+                                          claims_len, rank, world, gather, reduce, comm_ctx, roots, roots_len, claims_out,
                                           claims_out_len, proof, proof_len);
 }
 

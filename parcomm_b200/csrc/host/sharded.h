@@ -32,30 +32,48 @@
 
 namespace qf {
 
-// The one collective the sharded proof uses.
+// The collectives the sharded proof uses.
 struct Comm {
   virtual ~Comm() {}
   virtual int rank() const = 0;
   virtual int size() const = 0;
   // out[r n, (r + 1) n) <- rank r's n bytes `in`; every rank passes the same n.
   virtual void all_gather(const void* in, size_t n, void* out) = 0;
+  // data[i] <- the sum over the ranks of data[i] (every rank passes the same
+  // n; the sums used here stay below 2^63).  The form of an integer
+  // all-reduce (NCCL's uint64 sum); by default built on all_gather.
+  virtual void all_reduce_sum(uint64_t* data, size_t n) {
+    std::vector<uint64_t> all(n * size_t(size()));
+    all_gather(data, 8 * n, all.data());
+    for (size_t i = 0; i < n; ++i) {
+      uint64_t t = 0;
+      for (int k = 0; k < size(); ++k) t += all[size_t(k) * n + i];
+      data[i] = t;
+    }
+  }
 };
 
-// A Comm over a C callback, the form a caller outside C++ provides (MPI,
-// torch.distributed, NCCL over host buffers).  The callback returns 0 on
-// success.
+// A Comm over C callbacks, the form a caller outside C++ provides (MPI,
+// torch.distributed, NCCL over host buffers).  Each callback returns 0 on
+// success; without `reduce`, sums go through the gather.
 struct CallbackComm : Comm {
   using Fn = int (*)(void* ctx, const void* in, size_t n, void* out);
+  using ReduceFn = int (*)(void* ctx, uint64_t* data, size_t n);
   int r, n;
   Fn fn;
+  ReduceFn reduce;
   void* ctx;
-  CallbackComm(int rank, int size, Fn f, void* c) : r(rank), n(size), fn(f), ctx(c) {
+  CallbackComm(int rank, int size, Fn f, void* c, ReduceFn red = nullptr) : r(rank), n(size), fn(f), reduce(red), ctx(c) {
     if (size < 1 || rank < 0 || rank >= size || !f) fail(QF_E_ARGUMENT, "communicator rank/size/callback");
   }
   int rank() const override { return r; }
   int size() const override { return n; }
   void all_gather(const void* in, size_t bytes, void* out) override {
     if (fn(ctx, in, bytes, out) != 0) fail(QF_E_PROTOCOL, "all_gather callback failed");
+  }
+  void all_reduce_sum(uint64_t* data, size_t count) override {
+    if (!reduce) return Comm::all_reduce_sum(data, count);
+    if (reduce(ctx, data, count) != 0) fail(QF_E_PROTOCOL, "all_reduce callback failed");
   }
 };
 
@@ -83,19 +101,21 @@ struct BlockShards {
 };
 
 // Sum over the ranks of each rank's vector `part` (the same length on every
-// rank).  Field addition is exact, so the sum is the same on every rank.
+// rank): the canonical coefficients (each below p < 2^31) are summed as
+// 64-bit integers, which cannot overflow below 2^32 ranks, and reduced mod p
+// once, so every rank gets the same canonical elements.
 template <class F>
 std::vector<F> sum_over_ranks(Comm& c, const std::vector<F>& part) {
   if (part.empty() || c.size() == 1) return part;
-  ByteWriter w;
-  w.out.reserve(part.size() * F::kBytes);
-  for (const F& v : part) w.field(v);
-  std::vector<uint8_t> all(w.out.size() * size_t(c.size()));
-  c.all_gather(w.out.data(), w.out.size(), all.data());
-  std::vector<F> total(part.size(), F::zero());
-  ByteReader r(all.data(), all.size());
-  for (int k = 0; k < c.size(); ++k)
-    for (F& t : total) t += r.field<F>();
+  constexpr int kD = F::kLanes;  // coefficients per element
+  std::vector<uint64_t> wide(part.size() * kD);
+  for (size_t i = 0; i < part.size(); ++i)
+    for (int k = 0; k < kD; ++k) wide[i * kD + k] = uint64_t(part[i].c[k]);
+  c.all_reduce_sum(wide.data(), wide.size());
+  std::vector<F> total(part.size());
+  const uint64_t p = F::modulus_u64();
+  for (size_t i = 0; i < part.size(); ++i)
+    for (int k = 0; k < kD; ++k) total[i].c[k] = typename F::Coeff(wide[i * kD + k] % p);
   return total;
 }
 

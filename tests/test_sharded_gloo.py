@@ -2,9 +2,11 @@
 
 Each rank holds a contiguous run of the BVA's PCS blocks and runs the
 sharding layer (csrc/host/sharded.h) with the oracle's CPU shard standing in
-for its device; the only exchange is an all-gather over torch.distributed.
+for its device; the exchanges are an all-gather and an integer all-reduce
+over torch.distributed.
 Every rank must write the proof that one rank holding all blocks writes,
 byte for byte, in both fields, with given and with summed benchmark claims,
+with the sums taken through the gather or through an integer all-reduce,
 for world sizes that split the blocks evenly and unevenly.  A rank that
 leaves, or an exchange that fails, ends the proof with an error."""
 import os
@@ -44,14 +46,22 @@ def _all_gather(world: int):
     return gather
 
 
+def _all_reduce(a: np.ndarray) -> None:
+    """In-place integer sum over the ranks (the sums stay below 2^63)."""
+    dist.all_reduce(torch.from_numpy(a.view(np.int64)), op=dist.ReduceOp.SUM)
+
+
 def _rank(rank: int, world: int, port: int, field: str, cases, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         bva = _bva(field)
         for key, chunk_log, claims in cases:
+            calls = []
+            reduce = (lambda a: (calls.append(a.size), _all_reduce(a))) if key[0] == "reduce" else None
             out[(rank, key)] = oracle.prove_sharded(SHAPES, chunk_log, 4, bva, rank, world, _all_gather(world),
-                                                    claims=claims, field=field)
+                                                    claims=claims, field=field, all_reduce=reduce)
+            out[(rank, key, "reduce_calls")] = len(calls)
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -66,7 +76,9 @@ def test_sharded_proof_equals_single_rank_proof(field, world):
         roots, claims, proof, _ = oracle.prove(SHAPES, chunk_log, 4, bva, field=field)
         cases.append((("benchmark", chunk_log), chunk_log, None))
         cases.append((("given", chunk_log), chunk_log, claims))
-        expected[("benchmark", chunk_log)] = expected[("given", chunk_log)] = (roots, claims, proof)
+        cases.append((("reduce", chunk_log), chunk_log, None))  # sums through the integer all-reduce
+        for kind in ("benchmark", "given", "reduce"):
+            expected[(kind, chunk_log)] = (roots, claims, proof)
     manager = mp.get_context("spawn").Manager()
     out = manager.dict()
     mp.spawn(_rank, args=(world, _free_port(), field, cases, out), nprocs=world, join=True)
@@ -76,6 +88,7 @@ def test_sharded_proof_equals_single_rank_proof(field, world):
             assert got[0] == want[0], f"rank {rank} {key}: roots differ"
             assert got[1] == want[1], f"rank {rank} {key}: claims differ"
             assert got[2] == want[2], f"rank {rank} {key}: proof bytes differ"
+            assert (out[(rank, key, "reduce_calls")] > 0) == (key[0] == "reduce")
         assert oracle.verify(SHAPES, key[1], 4, want[0], want[1], out[(0, key)][2], field=field)
 
 
