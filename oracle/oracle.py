@@ -79,6 +79,10 @@ def lib() -> ctypes.CDLL:
         for name in ("qfo_codeword_fold", "qfo_codeword_fold_kb"):
             getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p,
                                          ctypes.c_uint32, P, P, ctypes.c_char_p, P, ctypes.POINTER(ctypes.c_int)]
+        for name in ("qfo_prove_unchecked", "qfo_prove_unchecked_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, BPP,
+                                         ctypes.POINTER(S)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -256,6 +260,18 @@ def codeword_fold_accepted(log_n, columns, bits, pcs_seed: bytes, blocks, values
                                                                   v.ctypes.data, fw.ctypes.data, seed, cw.ctypes.data,
                                                                   ctypes.byref(ok)))
     return bool(ok.value)
+
+
+def prove_unchecked(shapes, chunk_log, packed_log, values, claims: bytes, rf_bits=100, field="f65521") -> bytes:
+    """The prover over `values` (up to the logical length) without the layout
+    check of the weights, against the given claims; returns the proof bytes."""
+    sfx, dt = _SUFFIX[field]
+    arr, n = _shapes(shapes)
+    v = np.ascontiguousarray(values, dtype=dt)
+    out, size = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+    _check(getattr(lib(), "qfo_prove_unchecked" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size,
+                                                      claims, len(claims), ctypes.byref(out), ctypes.byref(size)))
+    return _take(out, size)
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -438,6 +438,50 @@ int codeword_fold_impl(uint32_t log_n, uint32_t columns, uint32_t bits, const ui
     *accepted = verify_codeword_fold(pp, rs, cw, folded, s, binding.data(), binding.size()) ? 1 : 0;
   });
 }
+// The prover without the layout check of the weights (the reference's
+// commit_unchecked, protocol.rs:333-369): `n_values` entries (up to the
+// logical length, so the implicit zero suffix can be overwritten) are
+// committed as given and proved against the given claims.  A nonzero entry
+// in a bucket's padding or in the suffix must make the proof fail.
+template <class G, class T>
+int prove_unchecked_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log,
+                         uint32_t rf_bits, const T* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len,
+                         uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
+    if (n_values > P->layout.logical) fail(-9, "more values than the logical length");
+    ByteReader r(claims_in, claims_len);
+    std::vector<Claim<G>> cl;
+    for (const Shape& s : P->layout.shapes) {
+      Claim<G> x;
+      for (int i = 0; i < ilog2(next_pow2(s.rows)); ++i) x.row.push_back(r.field<G>());
+      for (int i = 0; i < ilog2(next_pow2(s.cols)); ++i) x.col.push_back(r.field<G>());
+      x.value = r.field<G>();
+      cl.push_back(x);
+    }
+    qf_oracle::CpuBackend<G, T> be(*P, bva, n_values);
+    std::vector<Digest> rs;
+    for (size_t b = 0; b < P->blocks(); ++b) rs.push_back(be.commit_block(b));
+    Transcript<G> t = statement_transcript(*P, make_statement(*P, rs), cl);
+    Query<G> q = compile(P->layout, cl, t);
+    auto [eo, term] = eo_prove<G>(be, P->layout.logical, size_t(1) << P->config.packed_log, q, t);
+    std::vector<uint8_t> ctx = opening_context<G>(t.state, 0);
+    BatchOpening<G> op = rs.size() > 1 ? open_batch(P->pcs, be, rs, term.point_msb, ctx)
+                                       : open_single(P->pcs, be, rs[0], term.point_msb, ctx);
+    check(op.claimed_value * term.scale == term.value, "QAFold/EO terminal mismatch");
+    Proof<G> pr;
+    pr.eo = eo;
+    pr.opening_value = op.claimed_value;
+    pr.opening_proof = std::move(op.wire);
+    const std::vector<uint8_t> wire = proof_to_bytes(pr);
+    *proof = dup(wire);
+    *proof_len = wire.size();
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -636,6 +680,20 @@ int qfo_codeword_fold_kb(uint32_t log_n, uint32_t columns, uint32_t bits, const 
                          const int32_t* values, const uint32_t* fold_w, const uint8_t seed[32], const uint32_t* check_w,
                          int* accepted) {
   return codeword_fold_impl<Kb4>(log_n, columns, bits, pcs_seed, blocks, values, fold_w, seed, check_w, accepted);
+}
+
+// The prover without the weights' layout check (outputs: the proof bytes).
+int qfo_prove_unchecked(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log, uint32_t rf_bits,
+                        const int8_t* bva, uint64_t n_values, const uint8_t* claims_in, size_t claims_len, uint8_t** proof,
+                        size_t* proof_len) {
+  return prove_unchecked_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
+                                           claims_len, proof, proof_len);
+}
+int qfo_prove_unchecked_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log,
+                           uint32_t rf_bits, const int16_t* bva, uint64_t n_values, const uint8_t* claims_in,
+                           size_t claims_len, uint8_t** proof, size_t* proof_len) {
+  return prove_unchecked_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values, claims_in,
+                                            claims_len, proof, proof_len);
 }
 
 }  // extern "C"

@@ -171,3 +171,43 @@ def test_compact_query_equals_its_dense_form(field):
         neg = ((vs[:, d:, None] * qs[:, : 16 - d, :]) % p).sum(axis=(0, 1)) % p
         assert np.array_equal(pos, ext_from_bytes(positive[d - 1], field)), d
         assert np.array_equal(neg, ext_from_bytes(negative[d - 1], field)), d
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_padding_is_a_proved_predicate(field):
+    """protocol.rs:332-353: a nonzero entry in a bucket's padding is refused
+    by the layout check and, with the check skipped, by the proof itself."""
+    shapes = [(31, 31)]
+    mat = np.ones((31, 31), dtype=FIELDS[field][4])
+    row, col = [base(3, field)] * 5, [base(7, field)] * 5
+    claims = b"".join(ext_to_bytes(e, field) for e in row + col + [claim_value(mat, row, col, field)])
+    bva = layout.encode(shapes, [mat])
+    _, _, proof, _ = oracle.prove(shapes, 30, 4, bva, claims=claims, field=field)
+    assert oracle.prove_unchecked(shapes, 30, 4, bva, claims, field=field) == proof
+    b = next(b for b in layout.buckets(shapes)[0] if b.rows > b.physical_rows or b.cols > b.physical_cols)
+    index = b.offset + b.physical_cols if b.cols > b.physical_cols else b.offset + b.physical_rows * b.cols
+    corrupt = bva.copy()
+    corrupt[index] = 1
+    with pytest.raises(oracle.OracleError, match="padding"):
+        oracle.prove(shapes, 30, 4, corrupt, claims=claims, field=field)
+    with pytest.raises(oracle.OracleError, match="packed reduction claim mismatch"):
+        oracle.prove_unchecked(shapes, 30, 4, corrupt, claims, field=field)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_implicit_suffix_is_checked_by_the_same_relation(field):
+    """protocol.rs:354-368: the entries past the active ones are zero by the
+    proof's relation; a 1 in the last logical entry makes the proof fail."""
+    shapes = [(3, 5)]
+    mat = np.full((3, 5), 2, dtype=FIELDS[field][4])
+    row, col = [base(3, field)] * 2, [base(7, field)] * 3
+    claims = b"".join(ext_to_bytes(e, field) for e in row + col + [claim_value(mat, row, col, field)])
+    bva = layout.encode(shapes, [mat])
+    logical = layout.buckets(shapes)[2]
+    full = np.zeros(logical, dtype=bva.dtype)
+    full[: bva.size] = bva
+    _, _, proof, _ = oracle.prove(shapes, 30, 4, bva, claims=claims, field=field)
+    assert oracle.prove_unchecked(shapes, 30, 4, full, claims, field=field) == proof
+    full[-1] = 1
+    with pytest.raises(oracle.OracleError, match="packed reduction claim mismatch"):
+        oracle.prove_unchecked(shapes, 30, 4, full, claims, field=field)
