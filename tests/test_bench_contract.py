@@ -1,6 +1,7 @@
 """The bench's whole-step compulsory-byte count on the CPU: the 8B int8 and
 int16 workloads and the streamed 70B set, whose binding re-encodes every
-block (the formulas of the survey's measurement section)."""
+block (each materialised vector written once and read once per dependent
+pass)."""
 import sys
 from pathlib import Path
 
