@@ -7,7 +7,7 @@
 //
 // Each function follows the reference loop it names; exact field arithmetic
 // makes evaluation order irrelevant.  Only tests, `__graft_entry__.smoke()`
-// and the bench's CPU-baseline leg may load this code, as the checker.
+// and the bench's CPU-baseline leg may load this code, to compare results with.
 #pragma once
 #include <memory>
 #include <vector>

@@ -1,7 +1,7 @@
 """ORACLE (test infrastructure only): ctypes wrapper of oracle/libqforacle.so.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
-this module, as the checker.  The product package never imports it.
+this module, to compare results with.  The product package never imports it.
 """
 from __future__ import annotations
 

@@ -1,6 +1,6 @@
 // ORACLE (test infrastructure only): C entry points over the CPU restatement
 // in cpu_backend.h, used by tests/, __graft_entry__.smoke() and the bench's
-// CPU-baseline leg as the checker.  Never linked into the product library.
+// CPU-baseline leg to compare results with.  Never linked into the product library.
 //
 // Pinned by the reference's own golden vectors:
 //   * demo proof (qafold/f65521/src/main.rs:108-145, validation/qafold8-smoke-final/run.log)
