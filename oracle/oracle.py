@@ -83,6 +83,8 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
                                          ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, BPP,
                                          ctypes.POINTER(S)]
+        L.qfo_blake2s_stream.argtypes = [ctypes.c_char_p, S, P, S, ctypes.c_char_p]
+        L.qfo_blake2s_compress.argtypes = [P, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, P]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -272,6 +274,23 @@ def prove_unchecked(shapes, chunk_log, packed_log, values, claims: bytes, rf_bit
     _check(getattr(lib(), "qfo_prove_unchecked" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data, v.size,
                                                       claims, len(claims), ctypes.byref(out), ctypes.byref(size)))
     return _take(out, size)
+
+
+def blake2s_stream(data: bytes, cuts=()) -> bytes:
+    """The host BLAKE2s-256 of `data`, fed in pieces ending at `cuts`."""
+    c = np.ascontiguousarray(cuts, dtype=np.uint64)
+    out = ctypes.create_string_buffer(32)
+    _check(lib().qfo_blake2s_stream(data, len(data), c.ctypes.data, c.size, out))
+    return out.raw
+
+
+def blake2s_compress(h, block: bytes, t: int, last: bool, ssse3: bool):
+    """One host BLAKE2s compression (scalar or SSSE3 path) of the 8-word state h."""
+    hi = np.ascontiguousarray(h, dtype=np.uint32)
+    ho = np.zeros(8, dtype=np.uint32)
+    assert hi.size == 8 and len(block) == 64
+    _check(lib().qfo_blake2s_compress(hi.ctypes.data, block, t, int(last), int(ssse3), ho.ctypes.data))
+    return ho
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -696,4 +696,42 @@ int qfo_prove_unchecked_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chu
                                             claims_len, proof, proof_len);
 }
 
+// BLAKE2s-256 of `n` bytes fed to one hasher in pieces that end at the
+// `n_cuts` ascending offsets `cuts` (then the rest).
+int qfo_blake2s_stream(const uint8_t* data, size_t n, const uint64_t* cuts, size_t n_cuts, uint8_t out[32]) {
+  return guarded([&] {
+    Blake2s h;
+    size_t at = 0;
+    for (size_t i = 0; i < n_cuts; ++i) {
+      if (cuts[i] < at || cuts[i] > n) fail(-9, "cuts");
+      h.update(data + at, size_t(cuts[i] - at));
+      at = size_t(cuts[i]);
+    }
+    h.update(data + at, n - at);
+    const Digest d = h.finalize();
+    std::memcpy(out, d.data(), 32);
+  });
+}
+// One compression of `block` into the state h (t = the byte count after the
+// block, `last` the final-block flag) by the scalar or the SSSE3 path.
+int qfo_blake2s_compress(const uint32_t h_in[8], const uint8_t block[64], uint64_t t, int last, int ssse3,
+                         uint32_t h_out[8]) {
+  return guarded([&] {
+    uint32_t h[8];
+    std::memcpy(h, h_in, sizeof h);
+#if defined(__x86_64__)
+    if (ssse3) {
+      if (!__builtin_cpu_supports("ssse3")) fail(-9, "no SSSE3 on this host");
+      blake2s_compress_ssse3(h, block, t, last != 0);
+    } else {
+      blake2s_compress_scalar(h, block, t, last != 0);
+    }
+#else
+    if (ssse3) fail(-9, "no SSSE3 on this host");
+    blake2s_compress_scalar(h, block, t, last != 0);
+#endif
+    std::memcpy(h_out, h, sizeof h);
+  });
+}
+
 }  // extern "C"
