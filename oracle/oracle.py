@@ -85,6 +85,7 @@ def lib() -> ctypes.CDLL:
                                          ctypes.POINTER(S)]
         L.qfo_blake2s_stream.argtypes = [ctypes.c_char_p, S, P, S, ctypes.c_char_p]
         L.qfo_blake2s_compress.argtypes = [P, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, P]
+        L.qfo_stdrng.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, P, S, ctypes.c_char_p, S]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -291,6 +292,16 @@ def blake2s_compress(h, block: bytes, t: int, last: bool, ssse3: bool):
     assert hi.size == 8 and len(block) == 64
     _check(lib().qfo_blake2s_compress(hi.ctypes.data, block, t, int(last), int(ssse3), ho.ctypes.data))
     return ho
+
+
+def stdrng(ops, seed: bytes | None = None, seed_u64: int | None = None) -> bytes:
+    """Draws from the host StdRng: op k > 0 is fill_bytes(k), -1 next_u32,
+    -2 next_u64; the outputs concatenated (little-endian)."""
+    o = np.ascontiguousarray(ops, dtype=np.int32)
+    size = sum(k if k > 0 else (4 if k == -1 else 8) for k in ops)
+    out = ctypes.create_string_buffer(max(size, 1))
+    _check(lib().qfo_stdrng(seed, seed_u64 or 0, int(seed_u64 is not None), o.ctypes.data, o.size, out, size))
+    return out.raw[:size]
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

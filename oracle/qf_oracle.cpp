@@ -734,4 +734,37 @@ int qfo_blake2s_compress(const uint32_t h_in[8], const uint8_t block[64], uint64
   });
 }
 
+// The setup's generator (rand 0.8 StdRng) driven by a list of draws: a
+// positive op k is fill_bytes of k bytes, -1 is next_u32 and -2 next_u64
+// (little-endian); the outputs are concatenated into `out`.  With
+// `use_u64` the generator is StdRng::seed_from_u64(seed_u64), else
+// StdRng::from_seed(seed).
+int qfo_stdrng(const uint8_t seed[32], uint64_t seed_u64, int use_u64, const int32_t* ops, size_t n_ops, uint8_t* out,
+               size_t cap) {
+  return guarded([&] {
+    std::array<uint8_t, 32> sd{};
+    if (seed) std::memcpy(sd.data(), seed, 32);
+    StdRng rng = use_u64 ? StdRng::seed_from_u64(seed_u64) : StdRng(sd);
+    size_t at = 0;
+    auto room = [&](size_t k) { if (at + k > cap) fail(-9, "output buffer too small"); };
+    for (size_t i = 0; i < n_ops; ++i) {
+      if (ops[i] > 0) {
+        room(size_t(ops[i]));
+        rng.fill_bytes(out + at, size_t(ops[i]));
+        at += size_t(ops[i]);
+      } else if (ops[i] == -1) {
+        room(4);
+        const uint32_t v = rng.next_u32();
+        for (int j = 0; j < 4; ++j) out[at++] = uint8_t(v >> (8 * j));
+      } else if (ops[i] == -2) {
+        room(8);
+        const uint64_t v = rng.next_u64();
+        for (int j = 0; j < 8; ++j) out[at++] = uint8_t(v >> (8 * j));
+      } else {
+        fail(-9, "unknown draw");
+      }
+    }
+  });
+}
+
 }  // extern "C"
