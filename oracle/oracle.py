@@ -86,6 +86,9 @@ def lib() -> ctypes.CDLL:
         L.qfo_blake2s_stream.argtypes = [ctypes.c_char_p, S, P, S, ctypes.c_char_p]
         L.qfo_blake2s_compress.argtypes = [P, ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, P]
         L.qfo_stdrng.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int, P, S, ctypes.c_char_p, S]
+        for name in ("qfo_query_counts", "qfo_query_counts_kb"):
+            getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, P, S, ctypes.POINTER(S),
+                                         ctypes.POINTER(ctypes.c_double)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -302,6 +305,17 @@ def stdrng(ops, seed: bytes | None = None, seed_u64: int | None = None) -> bytes
     out = ctypes.create_string_buffer(max(size, 1))
     _check(lib().qfo_stdrng(seed, seed_u64 or 0, int(seed_u64 is not None), o.ctypes.data, o.size, out, size))
     return out.raw[:size]
+
+
+def query_counts(log_n, columns=32, bits=100, field="f65521"):
+    """Per level of the packed PCS code sequence: (message_len, index,
+    codeword_len, queries with the codeword's rows available, queries
+    unlimited); and log2 of the field's size."""
+    rows = np.zeros(5 * 64, dtype=np.uint64)
+    n, card = ctypes.c_size_t(), ctypes.c_double()
+    _check(getattr(lib(), "qfo_query_counts" + _SUFFIX[field][0])(log_n, columns, bits, rows.ctypes.data, rows.size,
+                                                                 ctypes.byref(n), ctypes.byref(card)))
+    return [tuple(int(x) for x in rows[5 * i: 5 * i + 5]) for i in range(n.value)], card.value
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

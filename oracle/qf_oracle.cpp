@@ -482,6 +482,36 @@ int prove_unchecked_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk
     *proof_len = wire.size();
   });
 }
+// The code sequence of a packed PCS over 2^log_n base values with
+// `columns` extension columns at `bits` of security: per level (ascending
+// message length) the message length, the index, the codeword length and the
+// query counts num_queries(level, available) with the codeword's rows
+// available and with no limit.  `card_log2` <- log2 of the field's size.
+template <class G>
+int query_counts_impl(uint32_t log_n, uint32_t columns, uint32_t bits, uint64_t* rows, size_t cap, size_t* levels,
+                      double* card_log2) {
+  return guarded([&] {
+    const size_t n_witness = size_t(1) << (log_n - ilog2(G::kLanes));
+    Digest seed;
+    seed.fill(0x51);
+    PcsParams<G> pp;
+    pp.card_log2 = cardinality_log2<G>();
+    pp.security_bits = bits;
+    pp.extension_columns = columns;
+    pp.seq = build_sequence<G>(n_witness, columns, seed);
+    *levels = pp.levels();
+    *card_log2 = pp.card_log2;
+    if (cap < 5 * pp.levels()) fail(-9, "output buffer too small");
+    for (size_t l = 0; l < pp.levels(); ++l) {
+      const QaCode<G>& c = pp.seq.codes[l];
+      rows[5 * l + 0] = c.message_len;
+      rows[5 * l + 1] = c.index;
+      rows[5 * l + 2] = c.codeword_len();
+      rows[5 * l + 3] = pp.num_queries(l, c.codeword_len());
+      rows[5 * l + 4] = pp.num_queries(l, SIZE_MAX);
+    }
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -765,6 +795,16 @@ int qfo_stdrng(const uint8_t seed[32], uint64_t seed_u64, int use_u64, const int
       }
     }
   });
+}
+
+// The query counts of every level of a packed PCS's code sequence.
+int qfo_query_counts(uint32_t log_n, uint32_t columns, uint32_t bits, uint64_t* rows, size_t cap, size_t* levels,
+                     double* card_log2) {
+  return query_counts_impl<Fp8>(log_n, columns, bits, rows, cap, levels, card_log2);
+}
+int qfo_query_counts_kb(uint32_t log_n, uint32_t columns, uint32_t bits, uint64_t* rows, size_t cap, size_t* levels,
+                        double* card_log2) {
+  return query_counts_impl<Kb4>(log_n, columns, bits, rows, cap, levels, card_log2);
 }
 
 }  // extern "C"
