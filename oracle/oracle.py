@@ -89,6 +89,7 @@ def lib() -> ctypes.CDLL:
         for name in ("qfo_query_counts", "qfo_query_counts_kb"):
             getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, P, S, ctypes.POINTER(S),
                                          ctypes.POINTER(ctypes.c_double)]
+        L.qfo_layout.argtypes = [ctypes.POINTER(ctypes.c_uint64), S, P, S, ctypes.POINTER(S)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -316,6 +317,18 @@ def query_counts(log_n, columns=32, bits=100, field="f65521"):
     _check(getattr(lib(), "qfo_query_counts" + _SUFFIX[field][0])(log_n, columns, bits, rows.ctypes.data, rows.size,
                                                                  ctypes.byref(n), ctypes.byref(card)))
     return [tuple(int(x) for x in rows[5 * i: 5 * i + 5]) for i in range(n.value)], card.value
+
+
+def host_layout(shapes):
+    """The host C++ layout: (bucket rows of (matrix, offset, row_offset,
+    col_offset, rows, cols, physical_rows, physical_cols), active, logical)."""
+    arr, n = _shapes(shapes)
+    cap = 8 * 16 * max(n, 1) + 2
+    out = np.zeros(cap, dtype=np.uint64)
+    nb = ctypes.c_size_t()
+    _check(lib().qfo_layout(arr, n, out.ctypes.data, cap, ctypes.byref(nb)))
+    rows = [tuple(int(x) for x in out[8 * i: 8 * i + 8]) for i in range(nb.value)]
+    return rows, int(out[8 * nb.value]), int(out[8 * nb.value + 1])
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -807,4 +807,21 @@ int qfo_query_counts_kb(uint32_t log_n, uint32_t columns, uint32_t bits, uint64_
   return query_counts_impl<Kb4>(log_n, columns, bits, rows, cap, levels, card_log2);
 }
 
+// The host layout of `shapes` (Layout::new, layout.rs:34-155): per bucket,
+// in layout order, matrix, offset, row offset, column offset, rows, columns,
+// physical rows, physical columns; then active and logical.
+int qfo_layout(const uint64_t* shapes, size_t n_shapes, uint64_t* out, size_t cap, size_t* n_buckets) {
+  return guarded([&] {
+    const Layout L = make_layout(shapes_of(shapes, n_shapes));
+    if (cap < 8 * L.buckets.size() + 2) fail(-9, "output buffer too small");
+    size_t at = 0;
+    for (const Bucket& b : L.buckets)
+      for (size_t v : {b.matrix, b.offset, b.row_offset, b.col_offset, b.rows, b.cols, b.physical_rows, b.physical_cols})
+        out[at++] = v;
+    out[at++] = L.active;
+    out[at++] = L.logical;
+    *n_buckets = L.buckets.size();
+  });
+}
+
 }  // extern "C"

@@ -8,6 +8,9 @@ Sources:
   * validation/qafold16-smoke/run.log       (KoalaBear demo bundle)
   * qafold/f65521/vendor/qafold/src/qafold_short_pc.rs  (native opening +
     Decide wire fixture digest, test `native_opening_and_decide_wire_fixture`)
+  * qafold/f65521/tests/fixtures/llama8b-layout.json  (the real 8B layout of
+    end_to_end.rs:262-298: its 291 shapes, the counts, and a BLAKE2s of the
+    bucket table, eight little-endian u64 per bucket in layout order)
 """
 import json
 import re
@@ -40,12 +43,35 @@ def wire_fixture(path: Path) -> dict:
             "rng_seed_u64": "0x706172616c6c656c"}
 
 
+BUCKET_FIELDS = ("tensor_index", "dense_offset", "row_offset", "col_offset", "row_len", "col_len",
+                 "physical_row_len", "physical_col_len")
+
+
+def bucket_table_digest(rows) -> str:
+    """BLAKE2s-256 of the bucket table: per bucket the eight fields above as u64 LE."""
+    import hashlib
+    import struct
+    h = hashlib.blake2s()
+    for r in rows:
+        h.update(struct.pack("<8Q", *r))
+    return h.hexdigest()
+
+
+def layout_fixture(path: Path) -> dict:
+    fx = json.loads(path.read_text())
+    rows = [[b[k] for k in BUCKET_FIELDS] for b in fx["buckets"]]
+    return {"shapes": fx["shapes"], "bucket_count": len(rows), "active_entries": fx["layout"]["active_entries"],
+            "logical_entries": fx["layout"]["logical_entries"], "buckets_blake2s": bucket_table_digest(rows),
+            "source": "qafold/f65521/tests/fixtures/llama8b-layout.json"}
+
+
 def main(ref: Path) -> None:
     out = {
         "f65521_demo": smoke(ref / "validation/qafold8-smoke-final/run.log"),
         "koalabear_demo": smoke(ref / "validation/qafold16-smoke/run.log"),
         "f65521_wire_fixture": wire_fixture(ref / "qafold/f65521/vendor/qafold/src/qafold_short_pc.rs"),
         "demo_command": "demo --chunk-log 10 --packed-log 4 --cache-mode recompute",
+        "llama8b_layout": layout_fixture(ref / "qafold/f65521/tests/fixtures/llama8b-layout.json"),
     }
     dst = Path(__file__).with_name("reference_vectors.json")
     dst.write_text(json.dumps(out, indent=2) + "\n")

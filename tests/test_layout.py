@@ -40,3 +40,29 @@ def test_layout_of_a_70b_scale_matrix_without_its_weights():
     import pytest
     with pytest.raises(qf.QfError, match="matrix exceeds supported capacity"):
         qf.Parameters([(1 << 20, 1 << 20)], qf.Config(chunk_log=30, packed_log=4))
+
+
+def test_real_8b_layout_matches_the_reference_fixture(vectors):
+    """end_to_end.rs:262-298: the reference's 291-tensor 8B layout fixture,
+    bucket by bucket (matrix, offset, row and column offsets, lengths and
+    physical lengths), through the table's BLAKE2s, and the counts, for the
+    Python layout and the host C++ layout; the library agrees on the counts."""
+    import hashlib
+    import struct
+    g = vectors["llama8b_layout"]
+    shapes = [tuple(s) for s in g["shapes"]]
+    bs, active, logical = layout.buckets(shapes)
+    assert (len(shapes), len(bs), active, logical) == (291, g["bucket_count"], g["active_entries"], g["logical_entries"])
+    h = hashlib.blake2s()
+    for b in bs:
+        h.update(struct.pack("<8Q", b.matrix, b.offset, b.row_offset, b.col_offset, b.rows, b.cols,
+                             b.physical_rows, b.physical_cols))
+    assert h.hexdigest() == g["buckets_blake2s"]
+    import oracle
+    rows, h_active, h_logical = oracle.host_layout(shapes)
+    h = hashlib.blake2s()
+    for r in rows:
+        h.update(struct.pack("<8Q", *r))
+    assert (h.hexdigest(), h_active, h_logical) == (g["buckets_blake2s"], active, logical)
+    p = qf.Parameters(shapes, qf.Config(chunk_log=30, packed_log=4))
+    assert (p.active, p.logical, p.buckets) == (active, logical, len(bs))
