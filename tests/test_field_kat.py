@@ -115,3 +115,22 @@ def test_non_canonical_encoding_rejected(field):
         bad[w * i: w * (i + 1)] = p.to_bytes(w, "little")
         with pytest.raises(oracle.OracleError, match="non-canonical"):
             oracle.field_ops(bytes(bad), good, field=field)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_products_of_edge_coefficients(field):
+    """full_extension.rs:118-137: every pair of edge coefficient values, with
+    one lane (or all) of the left factor set and the rest at p - 1."""
+    p, d, _, _, _ = FIELDS[field]
+    edge = [0, 1, 15, 32_760, 32_761, 65_519, 65_520] if field == "f65521" else [0, 1, 15, p // 2, p // 2 + 1, p - 2, p - 1]
+    a, b = [], []
+    for left in edge:
+        for right in edge:
+            for lane in range(d + 1):
+                a.append([left if lane == d or i == lane else p - 1 for i in range(d)])
+                b.append([right] * d)
+    a, b = np.array(a, dtype=np.int64), np.array(b, dtype=np.int64)
+    blob = lambda x: b"".join(ext_to_bytes(e, field) for e in x)
+    prod, _, _ = oracle.field_ops(blob(a), blob(b), field=field)
+    got = np.array([ext_from_bytes(prod[16 * i: 16 * (i + 1)], field) for i in range(len(a))])
+    assert np.array_equal(got, ext_mul(a, b, field))
