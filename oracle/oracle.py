@@ -90,6 +90,11 @@ def lib() -> ctypes.CDLL:
             getattr(L, name).argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, P, S, ctypes.POINTER(S),
                                          ctypes.POINTER(ctypes.c_double)]
         L.qfo_layout.argtypes = [ctypes.POINTER(ctypes.c_uint64), S, P, S, ctypes.POINTER(S)]
+        for name in ("qfo_prove_sharded_threads", "qfo_prove_sharded_threads_kb"):
+            getattr(L, name).argtypes = [ctypes.POINTER(ctypes.c_uint64), S, ctypes.c_uint32, ctypes.c_uint32,
+                                         ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_int, BPP,
+                                         ctypes.POINTER(S), BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S),
+                                         ctypes.POINTER(ctypes.c_int)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -329,6 +334,26 @@ def host_layout(shapes):
     _check(lib().qfo_layout(arr, n, out.ctypes.data, cap, ctypes.byref(nb)))
     rows = [tuple(int(x) for x in out[8 * i: 8 * i + 8]) for i in range(nb.value)]
     return rows, int(out[8 * nb.value]), int(out[8 * nb.value + 1])
+
+
+def prove_sharded_threads(shapes, chunk_log, packed_log, values, world, claims: bytes | None = None, rf_bits=100,
+                          field="f65521"):
+    """Every rank of a block-sharded proof as a thread of this process (CPU
+    shards).  Returns (roots, claims, proof) of rank 0 and whether all ranks
+    wrote the same."""
+    sfx, dt = _SUFFIX[field]
+    arr, n = _shapes(shapes)
+    v = np.ascontiguousarray(values, dtype=dt)
+    outs = [ctypes.POINTER(ctypes.c_uint8)() for _ in range(3)]
+    lens = [ctypes.c_size_t() for _ in range(3)]
+    same = ctypes.c_int()
+    _check(getattr(lib(), "qfo_prove_sharded_threads" + sfx)(arr, n, chunk_log, packed_log, rf_bits, v.ctypes.data,
+                                                            v.size, claims, len(claims) if claims else 0, world,
+                                                            ctypes.byref(outs[0]), ctypes.byref(lens[0]),
+                                                            ctypes.byref(outs[1]), ctypes.byref(lens[1]),
+                                                            ctypes.byref(outs[2]), ctypes.byref(lens[2]),
+                                                            ctypes.byref(same)))
+    return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2]), bool(same.value)
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

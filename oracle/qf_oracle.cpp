@@ -6,6 +6,9 @@
 //   * demo proof (qafold/f65521/src/main.rs:108-145, validation/qafold8-smoke-final/run.log)
 //   * native opening + Decide wire fixture (qafold_short_pc.rs:3605-3647)
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
 #include <cstdlib>
 #include <string>
 
@@ -512,6 +515,128 @@ int query_counts_impl(uint32_t log_n, uint32_t columns, uint32_t bits, uint64_t*
     }
   });
 }
+// Ranks as threads of one process, for the sharding layer's tests at world
+// sizes that would be slow as processes: an all-gather through shared slots
+// between two barriers.  A rank that fails marks the group, so the others
+// stop at their next barrier instead of waiting; every wait is bounded.
+struct ThreadGroup {
+  explicit ThreadGroup(int n) : n(n), slots(size_t(n)) {}
+  const int n;
+  std::mutex mu;
+  std::condition_variable cv;
+  int arrived = 0;
+  uint64_t generation = 0;
+  bool aborted = false;
+  std::vector<std::vector<uint8_t>> slots;
+  void barrier() {
+    std::unique_lock<std::mutex> lk(mu);
+    if (aborted) fail(QF_E_PROTOCOL, "another rank failed");
+    const uint64_t g = generation;
+    if (++arrived == n) {
+      arrived = 0;
+      ++generation;
+      cv.notify_all();
+      return;
+    }
+    if (!cv.wait_for(lk, std::chrono::seconds(120), [&] { return generation != g || aborted; }))
+      fail(QF_E_PROTOCOL, "barrier timed out");
+    if (aborted) fail(QF_E_PROTOCOL, "another rank failed");
+  }
+  void abort() {
+    std::lock_guard<std::mutex> lk(mu);
+    aborted = true;
+    cv.notify_all();
+  }
+};
+struct ThreadComm : Comm {
+  ThreadGroup& g;
+  int r;
+  ThreadComm(ThreadGroup& group, int rank) : g(group), r(rank) {}
+  int rank() const override { return r; }
+  int size() const override { return g.n; }
+  void all_gather(const void* in, size_t n, void* out) override {
+    g.slots[size_t(r)].assign(static_cast<const uint8_t*>(in), static_cast<const uint8_t*>(in) + n);
+    g.barrier();
+    for (int k = 0; k < g.n; ++k) {
+      if (g.slots[size_t(k)].size() != n) fail(QF_E_PROTOCOL, "all_gather sizes differ");
+      if (n) std::memcpy(static_cast<uint8_t*>(out) + size_t(k) * n, g.slots[size_t(k)].data(), n);
+    }
+    g.barrier();
+  }
+};
+
+// Every rank of a block-sharded proof as a thread, each with its CPU shard;
+// outputs rank 0's roots, claims and proof and whether every rank wrote the
+// same three.  `claims` may be null (each rank's part of the benchmark
+// claims, summed).
+template <class G, class T>
+int prove_sharded_threads_impl(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log,
+                               uint32_t rf_bits, const T* bva, uint64_t n_values, const uint8_t* claims_in,
+                               size_t claims_len, int world, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
+                               size_t* claims_out_len, uint8_t** proof, size_t* proof_len, int* all_equal) {
+  return guarded([&] {
+    if (world < 1 || world > 256) fail(-9, "world");
+    Config c;
+    c.chunk_log = chunk_log;
+    c.packed_log = packed_log;
+    c.query_rf_bits = rf_bits;
+    auto P = make_parameters<G>(shapes_of(shapes, n_shapes), c);
+    validate_values(P->layout, bva, n_values);
+    const BlockShards shards(P->blocks(), world);
+    ThreadGroup group(world);
+    const size_t n_ranks = static_cast<size_t>(world);
+    std::vector<std::array<std::vector<uint8_t>, 3>> out(n_ranks);
+    std::vector<std::string> errors(n_ranks);
+    std::vector<std::thread> ranks;
+    for (int r = 0; r < world; ++r)
+      ranks.emplace_back([&, r] {
+        try {
+          ThreadComm comm(group, r);
+          qf_oracle::CpuShard<G, T> shard(*P, bva, n_values, shards, r);
+          ShardedBackend<G> be(*P, shard, comm);
+          std::vector<Digest> rs = be.commit_all();
+          std::vector<Claim<G>> cl;
+          if (claims_in) {
+            ByteReader rd(claims_in, claims_len);
+            for (const Shape& sh : P->layout.shapes) {
+              Claim<G> x;
+              for (int i = 0; i < ilog2(next_pow2(sh.rows)); ++i) x.row.push_back(rd.field<G>());
+              for (int i = 0; i < ilog2(next_pow2(sh.cols)); ++i) x.col.push_back(rd.field<G>());
+              x.value = rd.field<G>();
+              cl.push_back(x);
+            }
+          } else {
+            cl = sum_claims(comm, qf_oracle::evaluate_claims(*P, shard.masked.data(), n_values,
+                                                             benchmark_points<G>(make_statement(*P, rs))));
+          }
+          const std::vector<uint8_t> wire = prove_sharded(*P, be, rs, cl);
+          ByteWriter rw, cw;
+          for (const auto& d : rs) rw.digest(d);
+          for (const auto& x : cl) {
+            for (const G& v : x.row) cw.field(v);
+            for (const G& v : x.col) cw.field(v);
+            cw.field(x.value);
+          }
+          out[size_t(r)] = {std::move(rw.out), std::move(cw.out), wire};
+        } catch (const std::exception& e) {
+          errors[size_t(r)] = e.what();
+          group.abort();
+        }
+      });
+    for (auto& t : ranks) t.join();
+    for (int r = 0; r < world; ++r)
+      if (!errors[size_t(r)].empty()) fail(QF_E_PROTOCOL, "rank " + std::to_string(r) + ": " + errors[size_t(r)]);
+    *all_equal = 1;
+    for (int r = 1; r < world; ++r)
+      if (out[size_t(r)] != out[0]) *all_equal = 0;
+    *roots = dup(out[0][0]);
+    *roots_len = out[0][0].size();
+    *claims_out = dup(out[0][1]);
+    *claims_out_len = out[0][1].size();
+    *proof = dup(out[0][2]);
+    *proof_len = out[0][2].size();
+  });
+}
 }  // namespace
 
 extern "C" {
@@ -822,6 +947,24 @@ int qfo_layout(const uint64_t* shapes, size_t n_shapes, uint64_t* out, size_t ca
     out[at++] = L.logical;
     *n_buckets = L.buckets.size();
   });
+}
+
+// Every rank of a block-sharded proof as a thread of this process.
+int qfo_prove_sharded_threads(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log,
+                              uint32_t rf_bits, const int8_t* bva, uint64_t n_values, const uint8_t* claims_in,
+                              size_t claims_len, int world, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
+                              size_t* claims_out_len, uint8_t** proof, size_t* proof_len, int* all_equal) {
+  return prove_sharded_threads_impl<Fp8, int8_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values,
+                                                 claims_in, claims_len, world, roots, roots_len, claims_out,
+                                                 claims_out_len, proof, proof_len, all_equal);
+}
+int qfo_prove_sharded_threads_kb(const uint64_t* shapes, size_t n_shapes, uint32_t chunk_log, uint32_t packed_log,
+                                 uint32_t rf_bits, const int16_t* bva, uint64_t n_values, const uint8_t* claims_in,
+                                 size_t claims_len, int world, uint8_t** roots, size_t* roots_len, uint8_t** claims_out,
+                                 size_t* claims_out_len, uint8_t** proof, size_t* proof_len, int* all_equal) {
+  return prove_sharded_threads_impl<Kb4, int16_t>(shapes, n_shapes, chunk_log, packed_log, rf_bits, bva, n_values,
+                                                  claims_in, claims_len, world, roots, roots_len, claims_out,
+                                                  claims_out_len, proof, proof_len, all_equal);
 }
 
 }  // extern "C"

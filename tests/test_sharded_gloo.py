@@ -8,7 +8,8 @@ Every rank must write the proof that one rank holding all blocks writes,
 byte for byte, in both fields, with given and with summed benchmark claims,
 with the sums taken through the gather or through an integer all-reduce,
 for world sizes that split the blocks evenly and unevenly.  A rank that
-leaves, or an exchange that fails, ends the proof with an error."""
+leaves, or an exchange that fails, ends the proof with an error.  World
+sizes up to 8 and up to 128 blocks run as threads of one process."""
 import os
 import socket
 
@@ -141,3 +142,17 @@ def test_lost_rank_ends_the_proof_with_an_error():
                 p.kill()
                 p.join()
     assert "all_gather" in out.get(0, ""), out.get(0)
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_sharded_proof_with_ranks_as_threads(field):
+    """World sizes 1 to 8 as threads of one process (the same layer and CPU
+    shards, an all-gather through shared memory) over 16, 64 and 128 blocks:
+    every rank writes the single-rank proof."""
+    bva = _bva(field)
+    for chunk_log in (14, 12, 11):  # 16, 64 and 128 blocks
+        want = oracle.prove(SHAPES, chunk_log, 4, bva, field=field)[:3]
+        for world in (1, 2, 5, 7, 8):
+            roots, claims, proof, same = oracle.prove_sharded_threads(SHAPES, chunk_log, 4, bva, world, field=field)
+            assert same, (chunk_log, world)
+            assert (roots, claims, proof) == want, (chunk_log, world)
