@@ -156,3 +156,16 @@ def test_sharded_proof_with_ranks_as_threads(field):
             roots, claims, proof, same = oracle.prove_sharded_threads(SHAPES, chunk_log, 4, bva, world, field=field)
             assert same, (chunk_log, world)
             assert (roots, claims, proof) == want, (chunk_log, world)
+
+
+def test_sharded_proof_at_2_24_blocks():
+    """One 8B decoder layer's attention projections (4 matrices, 41.9 M
+    weights) at chunk 24: four ranks, one block each, write the single-rank
+    proof."""
+    shapes = [(4096, 4096), (1024, 4096), (1024, 4096), (4096, 4096)]
+    rng = np.random.default_rng(0)
+    mats = [np.clip(np.rint(rng.normal(0, 20, r * c)), -127, 127).astype(np.int8).reshape(r, c) for r, c in shapes]
+    bva = layout.encode(shapes, mats)
+    want = oracle.prove(shapes, 24, 4, bva)[:3]
+    roots, claims, proof, same = oracle.prove_sharded_threads(shapes, 24, 4, bva, 4)
+    assert same and (roots, claims, proof) == want
