@@ -152,3 +152,57 @@ def test_fold_binding_under_other_weights_is_rejected(field):
     assert oracle.codeword_fold_accepted(10, 32, 100, pcs_seed, 2, values, [1, 1], seed, [1, 1], field=field)
     assert not oracle.codeword_fold_accepted(10, 32, 100, pcs_seed, 2, values, [1, 1], seed, [1, 2], field=field)
     assert oracle.codeword_fold_accepted(10, 32, 100, pcs_seed, 2, values, [1, 2], seed, [1, 2], field=field)
+
+
+def _plus_one(b: bytes, field) -> bytes:
+    p, _, _, w, _ = FIELDS[field]
+    return ((int.from_bytes(b[:w], "little") + 1) % p).to_bytes(w, "little") + b[w:16]
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_single_opening_rejects_modified_statements_and_wires(field):
+    """vendor/qafold/tests/packed.rs:126-262: another root, claim, point
+    coordinate, context or setup; every wrapper field changed to another
+    canonical value; a byte of each native payload; lengths set to 2^64 - 1;
+    a non-canonical conjugate; truncations; a trailing byte; the magic.  And
+    a PCS of 2^3 values is refused."""
+    log_n = 9
+    p, lanes, _, w, _ = FIELDS[field]
+    values = table(field, log_n, 11)
+    pt = ext_point(field, log_n, 12)
+    pb = b"".join(ext_to_bytes(x, field) for x in pt)
+    root, value, wire = oracle.packed_open(log_n, 4, 32, SEED, values, pb, CTX, field=field)
+    ok = lambda r=root, q=pb, v=value, b=wire, c=CTX, s=SEED: oracle.packed_verify(log_n, 4, 32, s, r, q, v, b, c,
+                                                                                   field=field)
+    assert ok()
+    assert not ok(r=bytes([root[0] ^ 1]) + root[1:])
+    assert not ok(v=_plus_one(value, field))
+    for k in (0, log_n - 1):
+        assert not ok(q=pb[: 16 * k] + _plus_one(pb[16 * k: 16 * k + 16], field) + pb[16 * k + 16:])
+    assert not ok(c=b"another context")
+    assert not ok(s=bytes([92]) * 32)
+    rd = lambda at: int.from_bytes(wire[at: at + 8], "little")
+    count_at = 8 + 16 + lanes * 16
+    rounds = log_n - (lanes.bit_length() - 1)
+    assert rd(count_at) == rounds
+    rounds_at = count_at + 8
+    final_at = rounds_at + 32 * rounds
+    opening_len_at = final_at + 16
+    opening_at = opening_len_at + 8
+    decide_len_at = opening_at + rd(opening_len_at)
+    decide_at = decide_len_at + 8
+    assert decide_at + rd(decide_len_at) == len(wire) and rd(opening_len_at) > 16 and rd(decide_len_at) > 16
+    fields = [8, final_at] + [8 + 16 + 16 * i for i in range(lanes)] + [rounds_at + 16 * i for i in range(2 * rounds)]
+    for at in fields:
+        assert not ok(b=wire[:at] + _plus_one(wire[at: at + 16], field) + wire[at + 16:]), at
+    for at in (opening_at + rd(opening_len_at) // 2, decide_at + rd(decide_len_at) // 2):
+        assert not ok(b=wire[:at] + bytes([wire[at] ^ 1]) + wire[at + 1:]), at
+    for at in (count_at, opening_len_at, decide_len_at):
+        assert not ok(b=wire[:at] + b"\xff" * 8 + wire[at + 8:]), at
+    assert not ok(b=wire[:24] + p.to_bytes(w, "little") + wire[24 + w:])
+    for end in (0, 7, 8, count_at, final_at, opening_at, decide_at, len(wire) - 1):
+        assert not ok(b=wire[:end]), end
+    assert not ok(b=wire + b"\0")
+    assert not ok(b=bytes([wire[0] ^ 1]) + wire[1:])
+    with pytest.raises(oracle.OracleError, match="log_n"):
+        oracle.packed_open(3, 4, 32, SEED, table(field, 3, 1), b"\0" * 48, CTX, field=field)
