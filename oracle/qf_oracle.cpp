@@ -594,7 +594,14 @@ int prove_sharded_threads_impl(const uint64_t* shapes, size_t n_shapes, uint32_t
           ThreadComm comm(group, r);
           qf_oracle::CpuShard<G, T> shard(*P, bva, n_values, shards, r);
           ShardedBackend<G> be(*P, shard, comm);
-          std::vector<Digest> rs = be.commit_all();
+          // Odd world sizes commit block by block (one root exchange per
+          // block), even ones through commit_all (one exchange).
+          std::vector<Digest> rs;
+          if (world % 2) {
+            for (size_t b = 0; b < P->blocks(); ++b) rs.push_back(be.commit_block(b));
+          } else {
+            rs = be.commit_all();
+          }
           std::vector<Claim<G>> cl;
           if (claims_in) {
             ByteReader rd(claims_in, claims_len);

@@ -148,7 +148,8 @@ def test_lost_rank_ends_the_proof_with_an_error():
 def test_sharded_proof_with_ranks_as_threads(field):
     """World sizes 1 to 8 as threads of one process (the same layer and CPU
     shards, an all-gather through shared memory) over 16, 64 and 128 blocks:
-    every rank writes the single-rank proof."""
+    every rank writes the single-rank proof.  Odd world sizes commit block by
+    block, even ones all blocks at once."""
     bva = _bva(field)
     for chunk_log in (14, 12, 11):  # 16, 64 and 128 blocks
         want = oracle.prove(SHAPES, chunk_log, 4, bva, field=field)[:3]
