@@ -591,7 +591,11 @@ int prove_sharded_threads_impl(const uint64_t* shapes, size_t n_shapes, uint32_t
     for (int r = 0; r < world; ++r)
       ranks.emplace_back([&, r] {
         try {
-          ThreadComm comm(group, r);
+          // One rank alone takes the copy-only communicator.
+          std::unique_ptr<Comm> owned;
+          if (world == 1) owned = std::make_unique<LocalComm>();
+          else owned = std::make_unique<ThreadComm>(group, r);
+          Comm& comm = *owned;
           qf_oracle::CpuShard<G, T> shard(*P, bva, n_values, shards, r);
           ShardedBackend<G> be(*P, shard, comm);
           // Odd world sizes commit block by block (one root exchange per
