@@ -107,7 +107,7 @@ struct BlockShards {
 template <class F>
 std::vector<F> sum_over_ranks(Comm& c, const std::vector<F>& part) {
   if (part.empty() || c.size() == 1) return part;
-  constexpr int kD = F::kLanes;  // coefficients per element
+  constexpr int kD = int(sizeof(F::c) / sizeof(typename F::Coeff));  // coefficients per element
   std::vector<uint64_t> wide(part.size() * kD);
   for (size_t i = 0; i < part.size(); ++i)
     for (int k = 0; k < kD; ++k) wide[i * kD + k] = uint64_t(part[i].c[k]);
