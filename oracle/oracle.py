@@ -95,6 +95,8 @@ def lib() -> ctypes.CDLL:
                                          ctypes.c_uint32, P, ctypes.c_uint64, ctypes.c_char_p, S, ctypes.c_int, BPP,
                                          ctypes.POINTER(S), BPP, ctypes.POINTER(S), BPP, ctypes.POINTER(S),
                                          ctypes.POINTER(ctypes.c_int)]
+        L.qfo_encode_column.argtypes = [ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_char_p, S,
+                                        ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(S)]
         for name in ("qfo_range_audit", "qfo_range_audit_kb"):
             getattr(L, name).argtypes = [P, ctypes.c_uint64, ctypes.c_char_p, P, ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.c_char_p]
@@ -354,6 +356,22 @@ def prove_sharded_threads(shapes, chunk_log, packed_log, values, world, claims: 
                                                             ctypes.byref(outs[2]), ctypes.byref(lens[2]),
                                                             ctypes.byref(same)))
     return _take(outs[0], lens[0]), _take(outs[1], lens[1]), _take(outs[2], lens[2]), bool(same.value)
+
+
+def encode_column(log_n, message: bytes, bits=100, field="f65521"):
+    """The top code of the packed PCS over 2^log_n values: (alphas[1], the
+    codeword of `message`), each a list of 16-byte elements."""
+    n = len(message) // 16
+    alpha, cw, rows = ctypes.create_string_buffer(16 * n), ctypes.create_string_buffer(32 * n), ctypes.c_size_t()
+    _check(lib().qfo_encode_column(int(field == "koalabear"), log_n, bits, message, n, alpha, cw, ctypes.byref(rows)))
+    split = lambda raw, k: [raw[16 * i: 16 * (i + 1)] for i in range(k)]
+    return split(alpha.raw, n), split(cw.raw, 2 * n)
+
+
+def top_rows(log_n, field="f65521"):
+    """Message length of the top code (the codeword rows' count is twice it)."""
+    lanes = 8 if field == "f65521" else 4
+    return 1 << (log_n - (lanes.bit_length() - 1) - 5)
 
 
 def commit_roots(shapes, chunk_log, packed_log, values, rf_bits=100, field="f65521"):

@@ -978,4 +978,32 @@ int qfo_prove_sharded_threads_kb(const uint64_t* shapes, size_t n_shapes, uint32
                                                   claims_out_len, proof, proof_len, all_equal);
 }
 
+// The top QA code of a packed PCS over 2^log_n base values (columns 32,
+// `bits` of security, setup seed 0x51..): its message length R, its alpha
+// table alphas[1] (R elements) and the codeword of the R-element message
+// column `message` (2R elements), for a check against the encoding's
+// definition (qafold_short.rs:975-1002).
+int qfo_encode_column(int kb, uint32_t log_n, uint32_t bits, const uint8_t* message, size_t message_len, uint8_t* alpha,
+                      uint8_t* codeword, size_t* rows) {
+  return guarded([&] {
+    auto run = [&](auto tag) {
+      using G = decltype(tag);
+      std::array<uint8_t, 32> sd;
+      sd.fill(0x51);
+      PackedPcs<G> pcs = PackedPcs<G>::create(log_n, 32, bits, sd);
+      const QaCode<G>& code = pcs.pp->seq.top();
+      *rows = code.message_len;
+      if (message_len != code.message_len) fail(-9, "message length");
+      std::vector<G> msg(message_len), out(code.codeword_len());
+      ByteReader r(message, 16 * message_len);
+      for (auto& m : msg) m = r.field<G>();
+      code.encode_into(msg.data(), out.data());
+      for (size_t i = 0; i < message_len; ++i) code.alphas[1][i].to_bytes(alpha + 16 * i);
+      for (size_t i = 0; i < out.size(); ++i) out[i].to_bytes(codeword + 16 * i);
+    };
+    if (kb) run(Kb4{});
+    else run(Fp8{});
+  });
+}
+
 }  // extern "C"

@@ -206,3 +206,31 @@ def test_single_opening_rejects_modified_statements_and_wires(field):
     assert not ok(b=bytes([wire[0] ^ 1]) + wire[1:])
     with pytest.raises(oracle.OracleError, match="log_n"):
         oracle.packed_open(3, 4, 32, SEED, table(field, 3, 1), b"\0" * 48, CTX, field=field)
+
+
+def wht(v, field):
+    """Unnormalised Walsh-Hadamard transform of an (n, d) array, (a, b) -> (a + b, a - b)."""
+    p = FIELDS[field][0]
+    v = v.copy()
+    h = 1
+    while h < len(v):
+        v = v.reshape(-1, 2, h, v.shape[-1])
+        a, b = v[:, 0].copy(), v[:, 1].copy()
+        v[:, 0], v[:, 1] = (a + b) % p, (a - b) % p
+        v = v.reshape(-1, v.shape[-1])
+        h *= 2
+    return v
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+@pytest.mark.parametrize("log_n", [12, 16])
+def test_top_code_encoding_is_the_index_two_systematic_code(field, log_n):
+    """qafold_short.rs:975-1002: a column's codeword is the message followed
+    by WHT(alpha (.) WHT(message)) with the code's alpha table."""
+    rows = oracle.top_rows(log_n, field)
+    msg = ext_point(field, rows, 20 + log_n)
+    alpha, cw = oracle.encode_column(log_n, b"".join(ext_to_bytes(x, field) for x in msg), field=field)
+    a = np.array([ext_from_bytes(x, field) for x in alpha])
+    got = np.array([ext_from_bytes(x, field) for x in cw])
+    assert np.array_equal(got[:rows], msg)
+    assert np.array_equal(got[rows:], wht(ext_mul(wht(msg, field), a, field), field))
