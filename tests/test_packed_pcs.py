@@ -234,3 +234,67 @@ def test_top_code_encoding_is_the_index_two_systematic_code(field, log_n):
     got = np.array([ext_from_bytes(x, field) for x in cw])
     assert np.array_equal(got[:rows], msg)
     assert np.array_equal(got[rows:], wht(ext_mul(wht(msg, field), a, field), field))
+
+
+def _framed(label: bytes, data: bytes) -> bytes:
+    return len(label).to_bytes(8, "little") + label + len(data).to_bytes(8, "little") + data
+
+
+def _mobius(v, field):
+    """high[i] -= low[i] at every level (packed.rs:708-752)."""
+    p = FIELDS[field][0]
+    v = v.copy()
+    h = 1
+    while h < len(v):
+        v = v.reshape(-1, 2, h, v.shape[-1])
+        v[:, 1] = (v[:, 1] - v[:, 0]) % p
+        v = v.reshape(-1, v.shape[-1])
+        h *= 2
+    return v
+
+
+def block_root(values, b, chunk_log, alpha, field):
+    """A PCS block's commitment root from the definitions: pack the block's
+    2^chunk_log entries into elements of `lanes` coefficients, Mobius
+    transform, encode each of the 32 message columns, hash each codeword
+    row (framed base-row domain, width, canonical values) and pair the
+    digests under the framed inner domain (qafold_short_pc.rs:2372-2517)."""
+    import hashlib
+    p, lanes = FIELDS[field][0], FIELDS[field][1]
+    n = 1 << chunk_log
+    blk = np.zeros(n, dtype=np.int64)
+    seg = values[b * n: (b + 1) * n].astype(np.int64)
+    blk[: seg.size] = seg % p
+    msg = _mobius(blk.reshape(-1, lanes), field)
+    R = len(msg) // 32
+    cols = [np.concatenate([msg[c * R:(c + 1) * R], wht(ext_mul(wht(msg[c * R:(c + 1) * R], field), alpha, field), field)])
+            for c in range(32)]
+    width = _framed(b"width", (32).to_bytes(8, "little"))
+    dom = _framed(b"domain", b"qafold-short/base-row/v1")
+    level = [hashlib.blake2s(dom + width + b"".join(ext_to_bytes(cols[c][r], field) for c in range(32))).digest()
+             for r in range(2 * R)]
+    inner = _framed(b"domain", b"qafold-short/merkle-inner/v1")
+    while len(level) > 1:
+        level = [hashlib.blake2s(inner + level[i] + level[i + 1]).digest() for i in range(0, len(level), 2)]
+    return level[0]
+
+
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_block_roots_from_the_definitions(field):
+    """Every block root of a ragged collection, including the zero blocks past
+    the active entries, recomputed in numpy and hashlib equals the oracle's."""
+    from parcomm_b200 import layout
+    dt = FIELDS[field][4]
+    shapes = [(31, 37), (65, 17), (1, 7), (9, 1), (300, 40)]
+    info = np.iinfo(dt)
+    rng = np.random.default_rng(30)
+    bva = layout.encode(shapes, [rng.integers(info.min, info.max + 1, size=s, dtype=dt) for s in shapes])
+    for chunk_log in (10, 13):
+        roots = oracle.commit_roots(shapes, chunk_log, 4, bva, field=field)
+        rows = oracle.top_rows(chunk_log, field)
+        alpha, _ = oracle.encode_column(chunk_log, bytes(16 * rows), field=field)
+        a = np.array([ext_from_bytes(x, field) for x in alpha])
+        blocks = layout.buckets(shapes)[2] >> chunk_log
+        assert blocks >= 2
+        for b in range(blocks):
+            assert block_root(bva, b, chunk_log, a, field) == roots[32 * b: 32 * (b + 1)], (chunk_log, b)
