@@ -110,3 +110,25 @@ def test_malformed_inputs_rejected(field):
         p.verify([roots], [dataclasses.replace(c, row=c.row[:-1])], proof)
     assert not oracle.verify(shapes, 10, 4, roots, claims[16:], proof, field=name)
     p.verify([roots], [c], proof)
+
+
+@pytest.mark.parametrize("field", [qf.FIELD_F65521, qf.FIELD_KOALABEAR])
+def test_library_points_and_claim_codec_match_the_oracle(field):
+    """The library's benchmark points for a multi-block statement (main.rs:190-204)
+    are the points of the oracle's claims, and the claim codec round-trips
+    the oracle's claim bytes."""
+    import numpy as np
+    import oracle
+    from parcomm_b200 import layout
+    name = "f65521" if field == qf.FIELD_F65521 else "koalabear"
+    shapes = [(31, 37), (65, 17), (1, 7), (9, 1), (300, 40)]
+    dt = np.int8 if name == "f65521" else np.int16
+    bva = layout.encode(shapes, layout.demo_matrices(shapes, dtype=dt))
+    roots, claims, _, _ = oracle.prove(shapes, 10, 4, bva, field=name)
+    p = qf.Parameters(shapes, qf.Config(chunk_log=10, packed_log=4), field=field)
+    rs = [roots[i:i + 32] for i in range(0, len(roots), 32)]
+    assert len(rs) == p.blocks > 1
+    cl = qf.claims_from_bytes(p.shapes, claims)
+    assert qf.claims_to_bytes(cl) == claims
+    points = qf.claims_from_bytes(p.shapes, p.benchmark_points(rs), with_value=False)
+    assert [(c.row, c.col) for c in points] == [(c.row, c.col) for c in cl]
