@@ -8,6 +8,7 @@ import parcomm_b200 as qf
 from parcomm_b200 import layout
 
 CFG = qf.Config(chunk_log=10, packed_log=4)
+ROOT = __import__("pathlib").Path(__file__).resolve().parents[1]
 
 
 @pytest.fixture(scope="module")
@@ -177,3 +178,36 @@ def test_statement_and_claim_mutations_are_rejected(collection):
     assert not oracle.verify(fewer, 10, 4, roots, claims, proof, field=field)
     assert not _accepts(field, shapes, roots, claims, proof[:-1])
     assert not _accepts(field, shapes, roots, claims, proof + b"\0")
+
+
+def test_fresh_process_verifies_from_public_bytes(tmp_path):
+    """cli_stream.py:1-40: a process with no prover state (only the shapes,
+    the config, the roots, the claims and the proof bytes on disk) accepts
+    the proof, and rejects it with its last byte flipped."""
+    import subprocess
+    import sys
+    shapes = [(32, 32)]
+    mat = (np.arange(1024, dtype=np.int64) * 73 % 256).astype(np.uint8).view(np.int8).reshape(32, 32)
+    bva = layout.encode(shapes, [mat])
+    roots, claims, proof, _ = oracle.prove(shapes, 10, 4, bva)
+    for name, data in (("roots", roots), ("claims", claims), ("proof", proof)):
+        (tmp_path / name).write_bytes(data)
+    script = (
+        "import sys; from pathlib import Path; import parcomm_b200 as qf\n"
+        "d = Path(sys.argv[1]); r = (d / 'roots').read_bytes()\n"
+        "p = qf.Parameters([(32, 32)], qf.Config(chunk_log=10, packed_log=4))\n"
+        "try:\n"
+        "    p.verify([r[i:i + 32] for i in range(0, len(r), 32)],\n"
+        "             qf.claims_from_bytes(p.shapes, (d / 'claims').read_bytes()), (d / 'proof').read_bytes())\n"
+        "    print('verified')\n"
+        "except qf.QfError as e:\n"
+        "    print('rejected', e.code)\n")
+    run = lambda: subprocess.run([sys.executable, "-c", script, str(tmp_path)], capture_output=True, text=True,
+                                 cwd=str(ROOT), timeout=300)
+    r = run()
+    assert r.returncode == 0 and r.stdout.strip() == "verified", r.stderr
+    bad = bytearray(proof)
+    bad[-1] ^= 1
+    (tmp_path / "proof").write_bytes(bytes(bad))
+    r = run()
+    assert r.returncode == 0 and r.stdout.startswith("rejected"), r.stderr
