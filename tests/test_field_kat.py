@@ -108,13 +108,21 @@ def test_host_field_matches_the_definitions(field):
 
 @pytest.mark.parametrize("field", ["f65521", "koalabear"])
 def test_non_canonical_encoding_rejected(field):
+    """full_extension.rs:181-218: a coefficient at or above p in any lane is
+    refused (every such 16-bit value for F65521; p, p + 1 and 2^32 - 1 for
+    KoalaBear), while p - 1 in every lane, an integer above the field's size,
+    is a valid element."""
     p, d, _, w, _ = FIELDS[field]
     good = ext_to_bytes(np.ones(d, np.int64), field)
+    invalid = range(p, 1 << 16) if w == 2 else (p, p + 1, (1 << 32) - 1)
     for i in range(d):
-        bad = bytearray(good)
-        bad[w * i: w * (i + 1)] = p.to_bytes(w, "little")
-        with pytest.raises(oracle.OracleError, match="non-canonical"):
-            oracle.field_ops(bytes(bad), good, field=field)
+        for v in invalid:
+            bad = bytearray(good)
+            bad[w * i: w * (i + 1)] = v.to_bytes(w, "little")
+            with pytest.raises(oracle.OracleError, match="non-canonical"):
+                oracle.field_ops(bytes(bad), good, field=field)
+    top = ext_to_bytes(np.full(d, p - 1, np.int64), field)
+    assert oracle.field_ops(top, good, field=field)[0]
 
 
 @pytest.mark.parametrize("field", ["f65521", "koalabear"])

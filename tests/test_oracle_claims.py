@@ -132,17 +132,19 @@ def test_packing_widths_at_zero_one_minus_one_points(field, packed_log):
     assert not oracle.verify(shapes, 30, packed_log, roots, bytes(bad), proof, field=field)
 
 
-def test_rows_above_the_characteristic_are_not_aliased():
-    """65523 rows > p = 65521: row indices 65521 and 65522 must not alias 0 and 1."""
+@pytest.mark.parametrize("field", ["f65521", "koalabear"])
+def test_rows_above_the_characteristic_are_not_aliased(field):
+    """65523 rows > 65521: row indices 65521 and 65522 must not alias 0 and 1
+    (end_to_end.rs:299-310 in both crates)."""
     shapes = [(65523, 1)]
-    mats = layout.demo_matrices(shapes)
+    mats = layout.demo_matrices(shapes, dtype=FIELDS[field][4])
     bva = layout.encode(shapes, mats)
-    roots, claims, proof, _ = oracle.prove(shapes, 10, 4, bva)
-    (row, col, value), = parse_claims(shapes, claims, "f65521")
+    roots, claims, proof, _ = oracle.prove(shapes, 10, 4, bva, field=field)
+    (row, col, value), = parse_claims(shapes, claims, field)
     assert len(row) == 16 and len(col) == 0
-    assert np.array_equal(claim_value(mats[0], row, col, "f65521"), value)
-    assert oracle.verify(shapes, 10, 4, roots, claims, proof)
-    assert product_verifies(shapes, 10, 4, roots, claims, proof, "f65521")
+    assert np.array_equal(claim_value(mats[0], row, col, field), value)
+    assert oracle.verify(shapes, 10, 4, roots, claims, proof, field=field)
+    assert product_verifies(shapes, 10, 4, roots, claims, proof, field)
 
 
 @pytest.mark.parametrize("field", ["f65521", "koalabear"])
