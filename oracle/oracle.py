@@ -234,6 +234,7 @@ def packed_open(log_n, columns, bits, seed: bytes, values, point: bytes, ctx: by
 
 def packed_verify(log_n, columns, bits, seed: bytes, root: bytes, point: bytes, value: bytes, proof: bytes, ctx: bytes,
                   field="f65521") -> bool:
+    assert len(seed) == 32 and len(root) == 32 and len(point) == 16 * log_n and len(value) == 16
     rc = getattr(lib(), "qfo_packed_verify" + _SUFFIX[field][0])(log_n, columns, bits, seed, root, point, value, proof,
                                                                 len(proof), ctx, len(ctx))
     return rc == 0
@@ -244,6 +245,7 @@ def packed_open_batch(log_n, columns, bits, seed: bytes, blocks, values, point: 
     values (block after block): returns (roots, claimed value, proof bytes)."""
     v = np.ascontiguousarray(values, dtype=np.int32)
     assert v.size == blocks << log_n and len(seed) == 32
+    assert blocks >= 2 and blocks & (blocks - 1) == 0 and len(point) == 16 * (log_n + blocks.bit_length() - 1)
     roots, value = ctypes.create_string_buffer(32 * blocks), ctypes.create_string_buffer(16)
     out, size = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
     _check(getattr(lib(), "qfo_packed_open_batch" + _SUFFIX[field][0])(log_n, columns, bits, seed, blocks, v.ctypes.data,
@@ -254,6 +256,7 @@ def packed_open_batch(log_n, columns, bits, seed: bytes, blocks, values, point: 
 
 def packed_verify_batch(log_n, columns, bits, seed: bytes, roots: bytes, point: bytes, value: bytes, proof: bytes,
                         ctx: bytes, field="f65521") -> bool:
+    assert len(seed) == 32 and len(roots) % 32 == 0 and len(point) % 16 == 0 and len(value) == 16
     rc = getattr(lib(), "qfo_packed_verify_batch" + _SUFFIX[field][0])(log_n, columns, bits, seed, len(roots) // 32,
                                                                       roots, point, len(point) // 16, value, proof,
                                                                       len(proof), ctx, len(ctx))
