@@ -152,6 +152,27 @@ int qf_range_audit(const qf_params* params, const qf_committed* committed, const
 
 void qf_free_bytes(uint8_t* bytes);
 
+/* One proof over PCS blocks spread across ranks (one process per device), no
+ * reference counterpart: the batch opening of Parameters::prove
+ * (protocol.rs:201-263) with rank `rank` of `world` holding the contiguous
+ * run of blocks [B rank / world, B (rank + 1) / world).  Every rank passes the
+ * same host BVA and claims (null: the benchmark points, each rank's part of
+ * the claim values summed); only its blocks are copied to the current
+ * device.  The ranks exchange through the caller's collectives:
+ *   gather(ctx, in, n, out): out = every rank's n bytes of `in`, in rank order;
+ *   reduce(ctx, data, n): data[i] = the sum over the ranks of data[i]
+ *     (64-bit, below 2^63); may be null, the sums then use `gather`.
+ * Both return 0 on success.  Every rank gets the roots (blocks x 32 bytes)
+ * and the proof that one device holding all blocks writes (malloc'd; free
+ * with qf_free_bytes).  Calls on the ranks must be made together: a rank that
+ * fails leaves the others waiting in their collectives until those time
+ * out.  Needs 1 <= world <= blocks. */
+typedef int (*qf_gather_fn)(void* ctx, const void* in, size_t n, void* out);
+typedef int (*qf_reduce_fn)(void* ctx, uint64_t* data, size_t n);
+int qf_prove_sharded(const qf_params* params, const void* host_bva, uint64_t n_values, int rank, int world,
+                     qf_gather_fn gather, qf_reduce_fn reduce, void* ctx, const uint8_t* claims, size_t claims_len,
+                     uint8_t* roots_out, uint8_t** proof, size_t* proof_len);
+
 /* Diagnostics (no reference counterpart): per-kernel device time measured with
  * CUDA events on each kernel's launching stream.  qf_kernel_timing(1) resets
  * and enables recording; qf_kernel_stats writes JSON

@@ -63,8 +63,12 @@ EXPORTED = (
     "qf_benchmark_points", "qf_eval_claims", "qf_prove", "qf_verify", "qf_free_bytes", "qf_last_error",
     "qf_kernel_timing", "qf_kernel_stats", "qf_kernel_launches", "qf_commit_block_noalloc", "qf_commit_streamed",
     "qf_committed_stream_info", "qf_open", "qf_device_cache_limit", "qf_range_audit", "qf_kernel_int_peaks",
-    "qf_kernel_option",
+    "qf_kernel_option", "qf_prove_sharded",
 )
+
+# int gather(void* ctx, const void* in, size_t n, void* out); int reduce(void* ctx, uint64_t* data, size_t n)
+GATHER_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p)
+REDUCE_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_size_t)
 
 
 def lib() -> ctypes.CDLL:
@@ -106,6 +110,8 @@ def lib() -> ctypes.CDLL:
         L.qf_commit_block_noalloc.argtypes = [P, P, U64, U64, P, P]
         L.qf_range_audit.argtypes = [P, P, ctypes.c_char_p, P, S, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
                                      ctypes.POINTER(ctypes.c_int)]
+        L.qf_prove_sharded.argtypes = [P, P, U64, ctypes.c_int, ctypes.c_int, GATHER_FN, REDUCE_FN, P, ctypes.c_char_p,
+                                       S, ctypes.c_char_p, ctypes.POINTER(BP), ctypes.POINTER(S)]
         for name in EXPORTED:
             if not hasattr(L, name):
                 raise QfError(-9, f"library does not export {name}")
@@ -419,6 +425,49 @@ class Parameters:
         finally:
             lib().qf_free_bytes(ctypes.cast(out, ctypes.c_void_p))
         return Proof(data), ProverProfile(*[getattr(prof, f) for f, _ in _Profile._fields_])
+
+    def prove_sharded(self, values, rank: int, world: int, all_gather, all_reduce=None,
+                      claims: Optional[Sequence[Claim]] = None) -> Tuple[List[bytes], Proof]:
+        """One rank of a proof whose PCS blocks are spread over `world` ranks
+        (qf_prove_sharded): rank r holds blocks [B r / world, B (r + 1) /
+        world) of the host BVA `values` (every rank passes the same array) on
+        the current device.  `all_gather(data: bytes) -> bytes` returns every
+        rank's bytes in rank order; `all_reduce(a)`, if given, sums a uint64
+        numpy array over the ranks in place.  `claims` None takes the
+        benchmark points.  Every rank returns the roots and the proof that
+        one device holding all blocks writes."""
+        v = np.ascontiguousarray(values, dtype=self.weight_dtype)
+
+        def gather(_ctx, src, size, dst):
+            try:
+                out = all_gather(ctypes.string_at(src, size))
+                if len(out) != size * world:
+                    return 1
+                ctypes.memmove(dst, out, len(out))
+                return 0
+            except Exception:  # the library turns a nonzero status into an error
+                return 1
+
+        def reduce(_ctx, data, size):
+            try:
+                all_reduce(np.ctypeslib.as_array(data, shape=(size,)))
+                return 0
+            except Exception:
+                return 1
+
+        g = GATHER_FN(gather)
+        r = REDUCE_FN(reduce) if all_reduce is not None else ctypes.cast(None, REDUCE_FN)
+        cb = claims_to_bytes(claims) if claims is not None else None
+        roots = ctypes.create_string_buffer(32 * self.blocks)
+        out = ctypes.POINTER(ctypes.c_uint8)()
+        n = ctypes.c_size_t()
+        _check(lib().qf_prove_sharded(self._h, v.ctypes.data, v.size, rank, world, g, r, None, cb,
+                                      len(cb) if cb else 0, roots, ctypes.byref(out), ctypes.byref(n)))
+        try:
+            data = ctypes.string_at(out, n.value)
+        finally:
+            lib().qf_free_bytes(ctypes.cast(out, ctypes.c_void_p))
+        return [roots.raw[32 * b: 32 * (b + 1)] for b in range(self.blocks)], Proof(data)
 
     def verify(self, statement: Commitment | Sequence[bytes], claims: Sequence[Claim], proof: Proof | bytes) -> None:
         """Raises QfError when the proof is rejected (protocol.rs:266-320)."""

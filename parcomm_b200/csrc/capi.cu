@@ -173,6 +173,23 @@ int qf_range_audit(const qf_params* params, const qf_committed* committed, const
   });
 }
 
+int qf_prove_sharded(const qf_params* params, const void* host_bva, uint64_t n_values, int rank, int world,
+                     qf_gather_fn gather, qf_reduce_fn reduce, void* ctx, const uint8_t* claims, size_t claims_len,
+                     uint8_t* roots_out, uint8_t** proof, size_t* proof_len) {
+  return guarded([&] {
+    if (!params || (!host_bva && n_values) || !gather || !proof || !proof_len) fail(QF_E_ARGUMENT, "null argument");
+    if (world < 1 || rank < 0 || rank >= world) fail(QF_E_ARGUMENT, "rank and world: need 0 <= rank < world");
+    require_device();
+    std::vector<uint8_t> bytes = api(params->field).prove_sharded(params, host_bva, n_values, rank, world, gather, reduce,
+                                                                  ctx, claims, claims_len, roots_out);
+    uint8_t* buf = static_cast<uint8_t*>(std::malloc(bytes.size()));
+    if (!buf) fail(QF_E_ARGUMENT, "host allocation failed");
+    std::memcpy(buf, bytes.data(), bytes.size());
+    *proof = buf;
+    *proof_len = bytes.size();
+  });
+}
+
 void qf_free_bytes(uint8_t* bytes) { std::free(bytes); }
 
 int qf_kernel_timing(int enable) {

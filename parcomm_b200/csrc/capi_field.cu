@@ -13,6 +13,7 @@
 #include "capi_internal.h"
 #include "gpu_backend.cuh"
 #include "host/range_audit.h"
+#include "host/sharded.h"
 
 namespace QFB_NS {
 namespace {
@@ -389,6 +390,113 @@ void stream_info(const qf_committed* committed, uint64_t* h2d_bytes, uint64_t* r
   if (live_blocks) *live_blocks = fc->src ? fc->src->live_blocks() : 0;
 }
 
+// One rank's device work in a block-sharded proof: a GPU backend over a copy
+// of the BVA that holds only this rank's blocks (zero elsewhere), so every
+// weight-linear sum it returns is the rank's part.
+class GpuShard final : public ShardBackend<F> {
+ public:
+  explicit GpuShard(GpuBackend& be) : be_(be) {}
+  Digest commit_block(size_t b) override { return be_.commit_block(b); }
+  std::vector<std::vector<F>> project_blocks(const std::vector<F>& outer, size_t blocks) override {
+    return be_.project_blocks(outer, blocks);
+  }
+  void apply_images(const std::vector<F>& images) override { be_.apply_images(images); }
+  std::vector<F> fold_part(const std::vector<F>& fold_weights) override { return be_.fold_values(fold_weights); }
+  Digest commit_folded(std::vector<F> values) override { return be_.commit_folded_values(values); }
+  void sumcheck_message(F m[2]) override { be_.sumcheck_message(m); }
+  void sumcheck_fold(F ch) override { be_.sumcheck_fold(ch); }
+  F sumcheck_final_value() override { return be_.sumcheck_final_value(); }
+  F sumcheck_final_weight() override { return be_.sumcheck_final_weight(); }
+  void write_block_rows(ByteWriter& w, size_t b, const RowSelection& sel, const Digest& root) override {
+    be_.write_block_rows(w, b, sel, root);
+  }
+  void write_folded_rows(ByteWriter& w, const RowSelection& sel) override { be_.write_folded_rows(w, sel); }
+  const CodewordView<F>& folded_codeword() override { return be_.folded_codeword(); }
+  std::vector<F> folded_opening(const std::vector<F>& point, size_t col_log, std::vector<F>& rw) override {
+    return be_.folded_opening(point, col_log, rw);
+  }
+  TopRoundAccel<F>* top_round_accel() override { return be_.top_round_accel(); }
+  DecideAccel<F>* decide_accel() override { return be_.decide_accel(); }
+  void cross_terms(const Query<F>& q, size_t stride, std::vector<F>& pos, std::vector<F>& neg) override {
+    be_.cross_terms(q, stride, pos, neg);
+  }
+  F eo_build(const Query<F>& q, F ch, F inv, size_t logical, size_t stride) override {
+    return be_.eo_build(q, ch, inv, logical, stride);
+  }
+  std::array<F, 2> eo_round_cross() override { return be_.eo_round_cross(); }
+  void eo_round_fold(F inv, F ch) override { be_.eo_round_fold(inv, ch); }
+  std::array<F, 2> eo_terminal() override { return be_.eo_terminal(); }
+
+ private:
+  GpuBackend& be_;
+};
+
+// Whether any zero-padding entry in [lo, hi) of the device BVA is nonzero.
+static bool padding_nonzero(const Parameters<F>& P, const W* d_bva, uint64_t lo, uint64_t hi, cudaStream_t s) {
+  const std::vector<uint64_t> seg = padding_segments(P, lo, hi);
+  if (seg.empty()) return false;
+  DBuf<uint64_t> dseg(seg.size());
+  DBuf<unsigned int> flag(1);
+  QF_CK(cudaMemcpyAsync(dseg.p, seg.data(), seg.size() * 8, cudaMemcpyHostToDevice, s));
+  QF_CK(cudaMemsetAsync(flag.p, 0, 4, s));
+  QF_LAUNCH(s, "k_check_zero_segments", 0,
+            k_check_zero_segments<<<unsigned(std::min<size_t>(seg.size() / 2, 148 * 8)), 256, 0, s>>>(
+                reinterpret_cast<const uint8_t*>(d_bva + lo), dseg.p, uint32_t(seg.size() / 2), flag.p));
+  unsigned int h = 0;
+  QF_CK(cudaMemcpyAsync(&h, flag.p, 4, cudaMemcpyDeviceToHost, s));
+  QF_CK(cudaStreamSynchronize(s));
+  return h != 0;
+}
+
+// A rank of a block-sharded proof: its blocks of the host BVA copied to the
+// current device (the rest of the copy zero), the padding of its range
+// checked (the verdict summed over the ranks, so all stop together), its
+// blocks committed and the roots gathered, the claims given or summed from
+// every rank's part, then the outer prover over the sharding layer.
+std::vector<uint8_t> prove_sharded(const qf_params* params, const void* host_bva, uint64_t n_values, int rank, int world,
+                                   qf_gather_fn gather, qf_reduce_fn reduce, void* ctx, const uint8_t* claims,
+                                   size_t claims_len, uint8_t* roots_out) {
+  const auto& P = params_of(params);
+  check(n_values == P.layout.active, "active BVA length mismatch");
+  CallbackComm comm(rank, world, gather, ctx, reduce);
+  const BlockShards shards(P.blocks(), world);
+  struct Stream {
+    cudaStream_t s = nullptr;
+    ~Stream() { if (s) cudaStreamDestroy(s); }
+  } st;
+  QF_CK(cudaStreamCreateWithFlags(&st.s, cudaStreamNonBlocking));
+  DBuf<W> bva(std::max<uint64_t>(n_values, 8));
+  QF_CK(cudaMemsetAsync(bva.p, 0, bva.n * sizeof(W), st.s));
+  const uint64_t lo = std::min<uint64_t>(n_values, uint64_t(shards.first(rank)) * P.block_len);
+  const uint64_t hi = std::min<uint64_t>(n_values, uint64_t(shards.first(rank + 1)) * P.block_len);
+  if (hi > lo)
+    QF_CK(cudaMemcpyAsync(bva.p + lo, static_cast<const W*>(host_bva) + lo, (hi - lo) * sizeof(W), cudaMemcpyHostToDevice,
+                          st.s));
+  uint64_t bad = padding_nonzero(P, bva.p, lo, hi, st.s) ? 1 : 0;
+  comm.all_reduce_sum(&bad, 1);
+  check(bad == 0, "nonzero boundary padding");
+  std::vector<uint8_t> wire;
+  {
+    GpuBackend be(P, bva.p, n_values, st.s, static_cast<DeviceTables*>(params->tables.get()));
+    GpuShard shard(be);
+    ShardedBackend<F> sharded(P, shard, comm);
+    const std::vector<Digest> roots = sharded.commit_all();
+    std::vector<Claim<F>> cl;
+    if (claims) {
+      cl = parse_claims(P, claims, claims_len, true);
+    } else {
+      std::vector<Claim<F>> pts;
+      for (const auto& [r, c] : benchmark_points<F>(make_statement(P, roots))) pts.push_back({r, c, F::zero()});
+      cl = sum_claims(comm, device_eval_claims(P, be, std::move(pts)));
+    }
+    wire = qf::prove_sharded(P, sharded, roots, cl);
+    if (roots_out)
+      for (size_t b = 0; b < roots.size(); ++b) std::memcpy(roots_out + 32 * b, roots[b].data(), 32);
+    QF_CK(cudaStreamSynchronize(st.s));  // the backend's buffers go back to the pool next
+  }
+  return wire;
+}
+
 }  // namespace
 
 // LogUp range audit: alpha from the seed, the weights' fraction sum on the
@@ -411,7 +519,8 @@ void range_audit(const qf_params* params, const qf_committed* committed, const u
   if (holds) *holds = (lhs == rhs && total == fc->active) ? 1 : 0;
 }
 
-const qfc::FieldApi kFieldApi = {sizeof(W), make_params, info, commit, commit_streamed, statement_json,
-                                 benchmark_points_bytes, eval_claims, prove, verify, stream_info, range_audit};
+const qfc::FieldApi kFieldApi = {sizeof(W),  make_params, info,   commit,      commit_streamed,
+                                 statement_json, benchmark_points_bytes, eval_claims, prove, verify,
+                                 stream_info, prove_sharded, range_audit};
 
 }  // namespace QFB_NS

@@ -52,6 +52,10 @@ struct FieldApi {
                  size_t proof_len);
   // Streamed weights: host->device bytes copied so far, resident and live blocks.
   void (*stream_info)(const qf_committed* c, uint64_t* h2d_bytes, uint64_t* resident_blocks, uint64_t* live_blocks);
+  // One rank of a block-sharded proof (host/sharded.h) on the current device.
+  std::vector<uint8_t> (*prove_sharded)(const qf_params* p, const void* host_bva, uint64_t n_values, int rank, int world,
+                                        qf_gather_fn gather, qf_reduce_fn reduce, void* ctx, const uint8_t* claims,
+                                        size_t claims_len, uint8_t* roots_out);
   // LogUp range audit of the committed weights (not part of the proof).
   void (*range_audit)(const qf_params* p, const qf_committed* c, const uint8_t seed[32], uint64_t* mult, size_t n_bins,
                       uint8_t alpha[16], uint8_t lhs[16], uint8_t rhs[16], int* holds);

@@ -1292,6 +1292,86 @@ std::vector<uint8_t> GpuBackend::binding_rows(const RowSelection& sel, const std
   return std::move(w.out);
 }
 
+// ---------------------------------------------------------------- block shards
+std::vector<F> GpuBackend::fold_values(const std::vector<F>& fw) {
+  HostScope hs("fold_values");
+  check(!src_, "sharded fold on streamed weights");
+  const uint64_t m = P_.pcs.packed_len();
+  const int blocks = int(fw.size());
+  constexpr int L = F::kLanes;
+  std::vector<F> T(size_t(blocks) * L);
+  for (int b = 0; b < blocks; ++b)
+    for (int j = 0; j < L; ++j) T[b * L + j] = fw[b] * basis<F>(j);
+  DBuf<Fe> dT(T.size());
+  QF_CK(cudaMemcpyAsync(dT.p, T.data(), T.size() * 16, cudaMemcpyHostToDevice, s_));
+  values_.alloc(m);
+  block_fold_launch(bva_, active_, blocks, dT.p, 0);
+  return copy_to_host(values_.p, m);
+}
+
+Digest GpuBackend::commit_folded_values(const std::vector<F>& values) {
+  HostScope hs("commit_folded_values");
+  const uint64_t m = P_.pcs.packed_len();
+  check(values.size() == m, "folded values length");
+  const int logm = ilog2(m);
+  const int logR = logm - ilog2(P_.pcs.pp->extension_columns);
+  values_.alloc(m);
+  QF_CK(cudaMemcpyAsync(values_.p, values.data(), m * 16, cudaMemcpyHostToDevice, s_));
+  folded_ = alloc_codeword(size_t(1) << logR, P_.pcs.pp->extension_columns, s_);
+  const int l0 = std::min(qfd::kMaxTileLog, logm);
+  check(logm <= 30, "transform passes index a codeword of at most 2^31 elements");
+  QF_LAUNCH_OPS(s_, "k_copy_mobius_tile", (uint64_t(2) << logm) * 16,
+                qf_intops::transform_ops(kOps, uint64_t(1) << logm, 0, l0, 1, 0), qfd::k_copy_mobius_tile<<<tile_grid(uint64_t(1) << (logm - l0)), qfd::kTileThreads, qfd::kTileSmem, s_>>>(
+                values_.p, folded_->cw.p, logR, l0, uint32_t(uint64_t(1) << (logm - l0))));
+  encode_and_hash(*folded_, tables_->top_alpha1(*P_.pcs.pp), logR, logm, false, l0);
+  QF_CK(cudaStreamSynchronize(s_));  // the host copy of `values` may go once this returns
+  host_v_.clear();
+  host_w_.clear();
+  sum_len_ = m;
+  msg_valid_ = false;
+  return folded_->root_;
+}
+
+namespace {
+// One codeword's rows in the binding payload: all rows, or the sampled rows
+// with their Merkle paths (write_rows).
+void write_device_rows(ByteWriter& w, const DeviceCodeword& cw, const RowSelection& sel) {
+  Rows<F> r;
+  if (sel.all) {
+    r.all = true;
+    r.n_rows = cw.n_ext;
+    r.n_cols = cw.n_cols;
+    r.encoded = cw.entries();
+  } else {
+    auto rws = cw.rows(sel.rows);
+    auto pth = cw.paths(sel.rows);
+    for (size_t i = 0; i < sel.rows.size(); ++i) {
+      RowQuery<F> q;
+      q.row = std::move(rws[i]);
+      q.path.siblings = std::move(pth[i]);
+      r.partial.push_back(std::move(q));
+    }
+  }
+  write_rows(w, r);
+}
+}  // namespace
+
+void GpuBackend::write_block_rows(ByteWriter& w, size_t b, const RowSelection& sel, const Digest& root) {
+  check(!src_, "sharded binding on streamed weights");
+  const DeviceCodeword* cw = b < blocks_.size() ? blocks_[b].get() : nullptr;
+  if (!cw) {  // a repeated zero block: the first committed zero block
+    for (size_t k = 0; k < blocks_.size() && !cw; ++k)
+      if (blocks_[k] && roots_[k] == root) cw = blocks_[k].get();
+  }
+  if (!cw || cw->root_ != root) fail(QF_E_INVALID_COMMITMENT, "block root mismatch");
+  write_device_rows(w, *cw, sel);
+}
+
+void GpuBackend::write_folded_rows(ByteWriter& w, const RowSelection& sel) {
+  check(folded_ != nullptr, "no folded codeword");
+  write_device_rows(w, *folded_, sel);
+}
+
 // ---------------------------------------------------------------- TBV / EO
 std::vector<W> GpuBackend::windows(const std::vector<uint64_t>& starts, size_t stride) {
   std::vector<W> out(starts.size() * stride);

@@ -208,6 +208,18 @@ class GpuBackend : public Backend<F>,
                                                                size_t stride);
   // Raw window values of small terms.
   std::vector<W> windows(const std::vector<uint64_t>& starts, size_t stride);
+  // Block-sharded proofs (host/sharded.h).  The backend then holds a copy of
+  // the BVA in which the blocks its rank does not hold are zero.
+  // This rank's part of sum_b fold[b] * packed(b, .), on the host.
+  std::vector<F> fold_values(const std::vector<F>& fold_weights);
+  // The folded values summed over the ranks: kept for the sumcheck, Mobius
+  // transformed, encoded and hashed as fold_and_commit does; returns the root.
+  Digest commit_folded_values(const std::vector<F>& values);
+  // The binding rows of committed block b (whose root must be `root`) and of
+  // the folded codeword, in the batch payload's format.
+  void write_block_rows(ByteWriter& w, size_t b, const RowSelection& sel, const Digest& root);
+  void write_folded_rows(ByteWriter& w, const RowSelection& sel);
+
   // LogUp range audit (not part of the proof): sum_i 1 / (alpha - v_i) over
   // the weights as {numerator, denominator}, and `mult` = the multiplicity of
   // each table value (bin k: the value k - 128 for int8, k - 32768 for int16).

@@ -132,3 +132,21 @@ def test_library_points_and_claim_codec_match_the_oracle(field):
     assert qf.claims_to_bytes(cl) == claims
     points = qf.claims_from_bytes(p.shapes, p.benchmark_points(rs), with_value=False)
     assert [(c.row, c.col) for c in points] == [(c.row, c.col) for c in cl]
+
+
+def test_sharded_prove_checks_its_arguments_and_needs_a_device():
+    """qf_prove_sharded refuses a rank outside [0, world) and, with valid
+    arguments, fails loudly without a device (no CPU fallback)."""
+    import numpy as np
+    import torch
+    p = qf.Parameters([(300, 700), (129, 65)], qf.Config(chunk_log=14, packed_log=4))
+    v = np.zeros(p.active, dtype=np.int8)
+    for rank, world in ((2, 2), (-1, 2), (0, 0)):
+        with pytest.raises(qf.QfError) as e:
+            p.prove_sharded(v, rank, world, lambda b: b * max(world, 1))
+        assert e.value.code == qf.QF_E_ARGUMENT
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(qf.QfError) as e:
+        p.prove_sharded(v, 0, 2, lambda b: b * 2)
+    assert e.value.code == qf.QF_E_NO_DEVICE
