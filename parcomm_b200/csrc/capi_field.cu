@@ -450,7 +450,7 @@ static bool padding_nonzero(const Parameters<F>& P, const W* d_bva, uint64_t lo,
 
 // A rank of a block-sharded proof: its blocks of the host BVA copied to the
 // current device (the rest of the copy zero), the padding of its range
-// checked (the verdict summed over the ranks, so all stop together), its
+// checked (the flags summed over the ranks, so all stop together), its
 // blocks committed and the roots gathered, the claims given or summed from
 // every rank's part, then the outer prover over the sharding layer.
 std::vector<uint8_t> prove_sharded(const qf_params* params, const void* host_bva, uint64_t n_values, int rank, int world,
